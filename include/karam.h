@@ -1,0 +1,277 @@
+/*
+ * karam.h -- C ABI of the B200 Newton-Raphson inner loop (device evaluation,
+ * MNA stamping, sparse LU refactorisation + triangular solves, convergence test).
+ *
+ * The reference engine has no extern "C" surface: its solver entry points are
+ * C++ member functions hidden behind the ENGINE_API visibility macros
+ * (engine_export.h:19-39). This header is the flat boundary that replaces them:
+ *
+ *   CircuitSim::solveDC(TensorNetlist&)        physics/circuitsim.h:1110,
+ *                                              solvers/circuitsim_solver.cpp:176-555
+ *   CircuitSim::solveDC(const CompiledTensorBlock&)      circuitsim_solver.cpp:790-807
+ *   CircuitSim::stepTransient(TensorNetlist&, dt, t)     circuitsim_solver.cpp:559-780
+ *   SessionImpl::runMonteCarlo (sequential DC loop)      engine_impl.cpp:259-281
+ *
+ * Conventions
+ *   - Plain pointers and sizes only; the caller owns every host buffer and the
+ *     library never keeps a caller pointer after a call returns.
+ *   - Node ids are 1-based, 0 is ground (netlist/circuit.h:1056-1216).
+ *   - Every function returns KARAM_OK (0) or a negative KARAM_E_* code; the text
+ *     of the last error of a context is available from karam_last_error().
+ *   - No exceptions cross this boundary. Per-instance solver outcomes are
+ *     reported as KARAM_ST_* codes in the caller's status array.
+ *   - A context owns one CUDA device and one stream; a context and the problems
+ *     made from it must not be used from two threads at once.
+ */
+#ifndef KARAM_H
+#define KARAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define KARAM_API __attribute__((visibility("default")))
+#else
+#define KARAM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------ */
+#define KARAM_OK 0
+#define KARAM_E_INVALID (-1)     /* bad argument or malformed netlist        */
+#define KARAM_E_CUDA (-2)        /* CUDA runtime error or no usable device    */
+#define KARAM_E_NOMEM (-3)       /* host or device allocation failed          */
+#define KARAM_E_UNSUPPORTED (-4) /* netlist uses something this path lacks   */
+#define KARAM_E_STATE (-5)       /* call out of order (e.g. no DC solution)   */
+
+/* ---- per-instance solver status (the reference reports converged=false +
+ *      error_detail, rankDeficient, and falls back to the CPU; this path has
+ *      no fallback and reports one of these instead) ------------------------ */
+#define KARAM_ST_CONVERGED 0
+#define KARAM_ST_NOCONV 1   /* NR did not converge within its iteration budget */
+#define KARAM_ST_SINGULAR 2 /* a pivot fell below the singularity threshold     */
+#define KARAM_ST_NAN 3      /* non-finite values met in the residual            */
+#define KARAM_ST_TIMEOUT 4  /* round budget of the launch exhausted             */
+
+/* ---- precision / schedule / method selectors ---------------------------- */
+#define KARAM_PREC_FP64 0  /* FP64 evaluation, FP64 LU                        */
+#define KARAM_PREC_MIXED 1 /* FP32 Jacobian + FP32 LU, FP64 residual + refinement */
+
+#define KARAM_TRAN_BE 0    /* backward Euler (Gear1, math/integration_method.h:83-115) */
+#define KARAM_TRAN_TRAP 1  /* trapezoidal (math/integration_method.h:47-81)           */
+
+#define KARAM_SRC_DC 0
+#define KARAM_SRC_PULSE 1  /* PULSE(v1 v2 td tr tf pw per), physics/circuitsim.h:2155-2170 */
+
+#define KARAM_MODEL_NMOS 0
+#define KARAM_MODEL_PMOS 1
+#define KARAM_MODEL_DIODE 2
+
+/*
+ * Flat netlist in netlist (insertion) order: the global block of a
+ * TensorNetlist (netlist/circuit.h:1056-1216) without hierarchy. The library
+ * performs the reference's tensorisation itself (device regrouping by model
+ * name, tensors/physics_tensors.cpp:305-493). Optional arrays may be NULL.
+ */
+typedef struct karam_netlist {
+  int32_t n_nodes; /* highest node id; unknowns are nodes 1..n_nodes            */
+  double temp_k;   /* ambient temperature [K]; reference default 300.15         */
+
+  /* independent voltage sources, Norton model G = 1e3 S (physics/circuitsim.h:2441-2467) */
+  int32_t n_vsrc;
+  const int32_t *vs_pos, *vs_neg;
+  const double *vs_dc;   /* DC value (also the DC operating-point value)        */
+  const int32_t *vs_kind; /* KARAM_SRC_*; NULL = all DC                          */
+  const double *vs_pulse; /* [n_vsrc][7] v1 v2 td tr tf pw per; NULL if none     */
+
+  /* independent current sources (physics/circuitsim.h:2470-2477) */
+  int32_t n_isrc;
+  const int32_t *is_pos, *is_neg;
+  const double *is_amp;
+
+  /* resistors (physics/circuitsim.h:2417-2438) */
+  int32_t n_res;
+  const int32_t *r_n1, *r_n2;
+  const double *r_ohm;
+
+  /* capacitors (companions in transient only) */
+  int32_t n_cap;
+  const int32_t *c_n1, *c_n2;
+  const double *c_farad;
+
+  /* diodes: Is, N, Vt as in TensorBlock::addDiode (netlist/circuit.h:815-826) */
+  int32_t n_dio;
+  const int32_t *d_anode, *d_cathode;
+  const double *d_is, *d_n, *d_vt;
+  const int32_t *d_model; /* model index, -1 = "diode_generic"; NULL = all -1     */
+
+  /* level-1 MOSFETs (netlist/circuit.h:832-843); model index required */
+  int32_t n_mos;
+  const int32_t *m_d, *m_g, *m_s, *m_b;
+  const double *m_w, *m_l;
+  const int32_t *m_model;
+
+  /* model cards (netlist/circuit.h:31-42); a NaN parameter means "not given",
+   * so the reference default of tensors/physics_tensors.cpp:424-441 applies */
+  int32_t n_models;
+  const char *const *model_name;
+  const int32_t *model_type; /* KARAM_MODEL_* */
+  const double *model_kp, *model_vto, *model_lambda;
+} karam_netlist;
+
+/*
+ * Per-instance parameters of a Monte-Carlo / corner batch. Every instance shares
+ * the netlist's topology. Arrays are instance-major; NULL means "use the
+ * netlist value for every instance". MOSFET KP/VTO are FP32-representable by
+ * contract (the sampler quantises them), so FP32 device storage is exact.
+ */
+typedef struct karam_instances {
+  int32_t n_instances;
+  const float *mos_kp;  /* [n_instances][n_mos], netlist MOSFET order          */
+  const float *mos_vto; /* [n_instances][n_mos]                                */
+  const double *vs_dc;  /* [n_instances][n_vsrc]: DC value; for PULSE sources the
+                           value scales v1 and v2 by vs_dc/netlist vs_dc when the
+                           netlist value is non-zero                           */
+} karam_instances;
+
+/* Solver options; karam_default_opts() fills the reference's constants
+ * (physics/physics_constants.h:62-85, physics/circuitsim.h:1206-1207). */
+typedef struct karam_solver_opts {
+  int32_t precision;     /* KARAM_PREC_*                                        */
+  int32_t max_nr_iter;   /* per GMIN step / per time step (reference: 50)       */
+  int32_t gmin_steps;    /* half-decade GMIN schedule length (reference: 19)    */
+  double reltol, vntol;  /* 1e-3, 1e-6                                          */
+  double kcl_shortcut;   /* converged outright below this KCL residual (1e-9 A)  */
+  double kcl_tol;        /* KCL tolerance at the final GMIN step / transient (1e-12 A) */
+  int32_t polish_max;    /* extra NR iterations after the reference criterion;
+                            0 keeps the reference stopping rule                  */
+  double polish_rel;     /* polishing stops once |dv_i| <= polish_rel*|v_i| + polish_abs */
+  double polish_abs;     /*   for every node, or when |dv| stops shrinking        */
+  int32_t ir_steps;      /* FP64 refinement steps per FP32 linear solve (mixed)  */
+  int32_t seeded;        /* 1: start from the caller's guess at the final GMIN
+                            step; fall back to full GMIN stepping if it has not
+                            converged after seed_max_iter iterations              */
+  int32_t seed_max_iter; /* K of the seeded fallback                              */
+  int32_t schedule;      /* 0 = autotuned; 1 = thread-per-instance; 2 = warp-per-instance */
+  int32_t max_rounds;    /* device round budget per launch (0 = unlimited)        */
+} karam_solver_opts;
+
+/* Sizes of the symbolic analysis of a problem. */
+typedef struct karam_problem_info {
+  int32_t n;           /* unknowns (node voltages)                              */
+  int32_t nnz;         /* CSR non-zeros of the Jacobian pattern                  */
+  int32_t nnz_filled;  /* non-zeros of L+U on the translated Min-Fill ordering   */
+  int32_t fill_in;     /* symbolicFactorize's estimatedFillIn                     */
+  int32_t treewidth;   /* TreewidthAnalyzer's estimatedTreewidth                  */
+  int32_t n_triplets;  /* stamp slots (triplets) per iteration incl. gmin         */
+  int32_t n_instances;
+  int32_t n_mos, n_dio, n_res, n_cap, n_vsrc, n_isrc;
+  int32_t lu_ops;      /* scaled + update operations of the LU program           */
+} karam_problem_info;
+
+/* Per-instance counters returned by the solves. */
+typedef struct karam_instance_stats {
+  int32_t status;       /* KARAM_ST_*                                            */
+  int32_t iterations;   /* NR iterations counted as the reference counts them    */
+  int32_t polish_iters; /* extra iterations spent polishing                       */
+  int32_t damped;       /* damping re-evaluations                                 */
+  int32_t gmin_step;    /* GMIN step reached (DC)                                 */
+  int32_t seeded_ok;    /* 1 if the seeded start converged without fallback       */
+  double residual;      /* final max KCL residual [A]                             */
+} karam_instance_stats;
+
+typedef struct karam_ctx karam_ctx;
+typedef struct karam_problem karam_problem;
+
+/* ---- context ------------------------------------------------------------ */
+KARAM_API int karam_ctx_create(int device, karam_ctx **out);
+KARAM_API void karam_ctx_destroy(karam_ctx *ctx);
+/* Text of the last error recorded on ctx (or of a failed karam_ctx_create when ctx is NULL). */
+KARAM_API const char *karam_last_error(const karam_ctx *ctx);
+KARAM_API void karam_default_opts(karam_solver_opts *opts);
+
+/* ---- problems ------------------------------------------------------------
+ * karam_problem_create runs the host symbolic analysis once per topology
+ * (the reference's NetlistCompiler::compile, infrastructure/netlist_compiler.cpp:17-90):
+ * tensorisation, stamp-slot -> CSR map, Min-Fill ordering, symbolic fill, LU
+ * program; it uploads the shared topology and sizes device state for
+ * max_instances instances. */
+KARAM_API int karam_problem_create(karam_ctx *ctx, const karam_netlist *nl,
+                                   int32_t max_instances, karam_problem **out);
+KARAM_API void karam_problem_destroy(karam_problem *p);
+KARAM_API int karam_problem_info_get(const karam_problem *p, karam_problem_info *out);
+/* Copies per-instance parameters host -> device (the batch to solve next). */
+KARAM_API int karam_set_instances(karam_problem *p, const karam_instances *inst);
+
+/* ---- solves (host buffers; copies are part of the call) ------------------
+ * DC operating point of every instance (circuitsim_solver.cpp:176-555).
+ * seed_v: [n_instances][n] initial guesses when opts->seeded, else NULL.
+ * out_v:  [n_instances][n]; stats: [n_instances] (either may be NULL). */
+KARAM_API int karam_solve_dc(karam_problem *p, const karam_solver_opts *opts,
+                             const double *seed_v, double *out_v,
+                             karam_instance_stats *stats);
+
+/* Fixed-step transient from the current DC (or previous transient) solution:
+ * n_steps steps of dt with the chosen companion (KARAM_TRAN_*).
+ * wave_nodes/n_wave: optional node ids recorded after every step into
+ * wave_out[n_instances][n_steps][n_wave]. out_v receives the final voltages. */
+KARAM_API int karam_step_transient(karam_problem *p, const karam_solver_opts *opts,
+                                   double dt, int32_t n_steps, int32_t method,
+                                   const int32_t *wave_nodes, int32_t n_wave,
+                                   double *wave_out, double *out_v,
+                                   karam_instance_stats *stats);
+
+/* One Monte-Carlo job: set the instances, DC, then the transient, with results
+ * copied back. It is the call a SessionImpl::runMonteCarlo caller replaces its
+ * sequential loop with. out_v: [n_instances][n] final voltages. */
+KARAM_API int karam_run_mc(karam_problem *p, const karam_instances *inst,
+                           const karam_solver_opts *opts, double dt, int32_t n_steps,
+                           int32_t method, double *out_v, karam_instance_stats *stats);
+
+/* ---- device-resident variants (inputs already in HBM; results stay there) --
+ * Same work as karam_run_mc after karam_set_instances, with no host copies;
+ * karam_read_results copies the device results back afterwards. */
+KARAM_API int karam_run_mc_device(karam_problem *p, const karam_solver_opts *opts,
+                                  double dt, int32_t n_steps, int32_t method);
+KARAM_API int karam_read_results(karam_problem *p, double *out_v,
+                                 karam_instance_stats *stats);
+/* Blocks until the problem's stream is idle. */
+KARAM_API int karam_sync(karam_problem *p);
+
+/* ---- symbolic queries (for bit-exact checks against the reference) -------- */
+/* CSR pattern of the Jacobian: row_ptr[n+1], col[nnz]. */
+KARAM_API int karam_get_pattern(const karam_problem *p, int32_t *row_ptr, int32_t *col);
+/* Stamp slot -> CSR index, in stampSoABlock triplet order (transient pattern,
+ * gmin diagonal last): slot_csr[n_triplets]. */
+KARAM_API int karam_get_stamp_map(const karam_problem *p, int32_t *slot_csr);
+/* Raw Min-Fill ordering (with the reference's branch ids) and its translation
+ * to a 0-based permutation of the n unknowns: raw[*raw_len], perm[n]. */
+KARAM_API int karam_get_ordering(const karam_problem *p, uint32_t *raw, int32_t *raw_len,
+                                 int32_t *perm);
+/* Filled L+U pattern in permuted order: f_row_ptr[n+1], f_col[nnz_filled]. */
+KARAM_API int karam_get_filled_pattern(const karam_problem *p, int32_t *f_row_ptr,
+                                       int32_t *f_col);
+/* SoA order of the tensorised devices: soa index -> netlist index. */
+KARAM_API int karam_get_device_order(const karam_problem *p, int32_t *mos_order,
+                                     int32_t *dio_order);
+
+/* ---- single-kernel access for measurement and parity ----------------------
+ * Runs the evaluation + stamping kernel once for every instance at the given
+ * voltages v[n_instances][n] and returns the Jacobian values without the gmin
+ * diagonal (jac[n_instances][nnz], FP64 or FP32 cast up per precision) and the
+ * device part of the KCL residual (f[n_instances][n]). h > 0 adds the
+ * capacitor companions of the chosen method with history v_prev = i_prev = 0. */
+KARAM_API int karam_eval_stamp(karam_problem *p, int32_t precision, const double *v,
+                               double *jac, double *f);
+/* Device timing of the last solve call, per kernel family, in milliseconds. */
+KARAM_API int karam_last_timing(const karam_problem *p, double *eval_ms, double *lu_ms,
+                                int32_t *eval_launches, int32_t *lu_launches,
+                                int32_t *rounds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KARAM_H */
