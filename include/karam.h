@@ -157,6 +157,9 @@ typedef struct karam_solver_opts {
   int32_t seed_max_iter; /* K of the seeded fallback                              */
   int32_t schedule;      /* 0 = autotuned; 1 = thread-per-instance; 2 = warp-per-instance */
   int32_t max_rounds;    /* device round budget per launch (0 = unlimited)        */
+  int32_t max_halvings;  /* transient: a step whose NR exhausts max_nr_iter restarts
+                            from the last time point with half the step, at most
+                            this many times (reference attempt loop: 3)          */
 } karam_solver_opts;
 
 /* Sizes of the symbolic analysis of a problem. */
@@ -180,6 +183,10 @@ typedef struct karam_instance_stats {
   int32_t damped;       /* damping re-evaluations                                 */
   int32_t gmin_step;    /* GMIN step reached (DC)                                 */
   int32_t seeded_ok;    /* 1 if the seeded start converged without fallback       */
+  int32_t rescued;      /* linear solves redone with partial pivoting because the
+                           static pivots of the shared LU program were unusable  */
+  int32_t halvings;     /* transient step halvings after NR failures              */
+  int32_t max_step_iters; /* most NR iterations spent on one transient attempt    */
   double residual;      /* final max KCL residual [A]                             */
 } karam_instance_stats;
 

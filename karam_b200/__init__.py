@@ -1,0 +1,262 @@
+"""karam_b200 -- B200-native Newton-Raphson inner loop of the Karam circuit engine.
+
+Python binding of the in-tree C ABI (include/karam.h, libkaram_b200.so). The
+classes mirror how the reference drives its solver: a ``Problem`` is the
+analog of a compiled block (CircuitSim + NetlistCompiler::compile) for one
+topology, batched over Monte-Carlo instances; ``solve_dc`` / ``step_transient``
+are CircuitSim::solveDC / stepTransient (physics/circuitsim.h:1110-1115) for
+every instance at once; ``run_mc`` replaces SessionImpl::runMonteCarlo's
+sequential loop (engine_impl.cpp:259-281).
+
+There is no CPU fallback: loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi as A
+from .circuits import Instances, Netlist  # noqa: F401  (re-exported)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkaram_b200.so")
+
+_lib = None
+
+
+class KaramError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"karam error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """The loaded libkaram_b200.so (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m karam_b200.build` "
+                          "(the product has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp = C.c_void_p
+    sig = {
+        "karam_ctx_create": (C.c_int, [C.c_int, P(vp)]),
+        "karam_ctx_destroy": (None, [vp]),
+        "karam_last_error": (C.c_char_p, [vp]),
+        "karam_default_opts": (None, [P(A.KaramSolverOpts)]),
+        "karam_problem_create": (C.c_int, [vp, P(A.KaramNetlist), C.c_int32, P(vp)]),
+        "karam_problem_destroy": (None, [vp]),
+        "karam_problem_info_get": (C.c_int, [vp, P(A.KaramProblemInfo)]),
+        "karam_set_instances": (C.c_int, [vp, P(A.KaramInstances)]),
+        "karam_solve_dc": (C.c_int, [vp, P(A.KaramSolverOpts), P(C.c_double), P(C.c_double),
+                                     P(A.KaramInstanceStats)]),
+        "karam_step_transient": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_double, C.c_int32,
+                                           C.c_int32, P(C.c_int32), C.c_int32, P(C.c_double),
+                                           P(C.c_double), P(A.KaramInstanceStats)]),
+        "karam_run_mc": (C.c_int, [vp, P(A.KaramInstances), P(A.KaramSolverOpts), C.c_double,
+                                   C.c_int32, C.c_int32, P(C.c_double),
+                                   P(A.KaramInstanceStats)]),
+        "karam_run_mc_device": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_double, C.c_int32,
+                                          C.c_int32]),
+        "karam_read_results": (C.c_int, [vp, P(C.c_double), P(A.KaramInstanceStats)]),
+        "karam_sync": (C.c_int, [vp]),
+        "karam_get_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+        "karam_get_stamp_map": (C.c_int, [vp, P(C.c_int32)]),
+        "karam_get_ordering": (C.c_int, [vp, P(C.c_uint32), P(C.c_int32), P(C.c_int32)]),
+        "karam_get_filled_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+        "karam_get_device_order": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+        "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
+                                       P(C.c_double)]),
+        "karam_last_timing": (C.c_int, [vp, P(C.c_double), P(C.c_double), P(C.c_int32),
+                                        P(C.c_int32), P(C.c_int32)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def options(**kw) -> A.KaramSolverOpts:
+    """Solver options: the reference constants, overridden by keyword."""
+    o = A.KaramSolverOpts()
+    lib().karam_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise AttributeError(f"unknown solver option {k}")
+        setattr(o, k, v)
+    return o
+
+
+class Context:
+    """One CUDA device + stream (karam_ctx)."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        rc = lib().karam_ctx_create(device, C.byref(h))
+        if rc != A.KARAM_OK:
+            raise KaramError(rc, lib().karam_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().karam_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Problem:
+    """One topology + its batch of instances (karam_problem).
+
+    With ``ctx=None`` only the host symbolic analysis is built (no device
+    memory); the symbolic queries work, solves raise.
+    """
+
+    def __init__(self, ctx: Context | None, nl: Netlist, max_instances=1):
+        self.ctx = ctx
+        self.nl = nl
+        self._nls = nl.as_struct()
+        h = C.c_void_p()
+        rc = lib().karam_problem_create(ctx.h if ctx else None, C.byref(self._nls),
+                                        max_instances, C.byref(h))
+        if rc != A.KARAM_OK:
+            raise KaramError(rc, lib().karam_last_error(ctx.h if ctx else None).decode())
+        self.h = h
+        self.info = self._info()
+        self.n = self.info["n"]
+        self.ni = 1
+
+    def _check(self, rc):
+        if rc != A.KARAM_OK:
+            raise KaramError(rc, lib().karam_last_error(self.ctx.h if self.ctx else None).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().karam_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _info(self):
+        inf = A.KaramProblemInfo()
+        self._check(lib().karam_problem_info_get(self.h, C.byref(inf)))
+        return {k: getattr(inf, k) for k, _ in A.KaramProblemInfo._fields_}
+
+    # -- symbolic queries ---------------------------------------------------
+    def pattern(self):
+        rp = np.zeros(self.n + 1, np.int32)
+        col = np.zeros(self.info["nnz"], np.int32)
+        self._check(lib().karam_get_pattern(self.h, A.ptr(rp, C.c_int32), A.ptr(col, C.c_int32)))
+        return rp, col
+
+    def stamp_map(self):
+        out = np.zeros(self.info["n_triplets"], np.int32)
+        self._check(lib().karam_get_stamp_map(self.h, A.ptr(out, C.c_int32)))
+        return out
+
+    def ordering(self):
+        raw = np.zeros(2 * self.n + self.info["n_vsrc"] + 8, np.uint32)
+        rl = C.c_int32(0)
+        perm = np.zeros(self.n, np.int32)
+        self._check(lib().karam_get_ordering(self.h, raw.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                             C.byref(rl), A.ptr(perm, C.c_int32)))
+        return raw[: rl.value], perm, self.info["treewidth"]
+
+    def filled_pattern(self):
+        rp = np.zeros(self.n + 1, np.int32)
+        col = np.zeros(self.info["nnz_filled"], np.int32)
+        self._check(lib().karam_get_filled_pattern(self.h, A.ptr(rp, C.c_int32),
+                                                   A.ptr(col, C.c_int32)))
+        return rp, col
+
+    def device_order(self):
+        mo = np.zeros(max(1, self.info["n_mos"]), np.int32)
+        do = np.zeros(max(1, self.info["n_dio"]), np.int32)
+        self._check(lib().karam_get_device_order(self.h, A.ptr(mo, C.c_int32),
+                                                 A.ptr(do, C.c_int32)))
+        return mo[: self.info["n_mos"]], do[: self.info["n_dio"]]
+
+    # -- batches and solves -------------------------------------------------
+    def set_instances(self, inst: Instances | None):
+        self._inst = inst.as_struct() if inst is not None else None
+        self._check(lib().karam_set_instances(self.h, C.byref(self._inst) if inst else None))
+        self.ni = inst.n if inst is not None else 1
+
+    @staticmethod
+    def _stats(st):
+        return [{k: getattr(s, k) for k, _ in A.KaramInstanceStats._fields_} for s in st]
+
+    def solve_dc(self, opts=None, seed=None):
+        opts = opts or options()
+        v = np.zeros((self.ni, self.n))
+        st = (A.KaramInstanceStats * self.ni)()
+        sd = None if seed is None else np.ascontiguousarray(seed, np.float64)
+        self._check(lib().karam_solve_dc(self.h, C.byref(opts), A.ptr(sd, C.c_double),
+                                         A.ptr(v, C.c_double), st))
+        return v, self._stats(st)
+
+    def step_transient(self, dt, n_steps, method=A.TRAN_BE, opts=None, wave_nodes=None):
+        opts = opts or options()
+        v = np.zeros((self.ni, self.n))
+        st = (A.KaramInstanceStats * self.ni)()
+        wn = None if wave_nodes is None else np.ascontiguousarray(wave_nodes, np.int32)
+        nw = 0 if wn is None else len(wn)
+        wave = np.zeros((self.ni, n_steps, max(1, nw)))
+        self._check(lib().karam_step_transient(self.h, C.byref(opts), dt, n_steps, method,
+                                               A.ptr(wn, C.c_int32), nw,
+                                               A.ptr(wave, C.c_double) if nw else None,
+                                               A.ptr(v, C.c_double), st))
+        return v, self._stats(st), wave[:, :, :nw]
+
+    def run_mc(self, inst: Instances, dt=0.0, n_steps=0, method=A.TRAN_BE, opts=None):
+        opts = opts or options()
+        self._inst = inst.as_struct()
+        self.ni = inst.n
+        v = np.zeros((self.ni, self.n))
+        st = (A.KaramInstanceStats * self.ni)()
+        self._check(lib().karam_run_mc(self.h, C.byref(self._inst), C.byref(opts), dt, n_steps,
+                                       method, A.ptr(v, C.c_double), st))
+        return v, self._stats(st)
+
+    def run_mc_device(self, dt=0.0, n_steps=0, method=A.TRAN_BE, opts=None):
+        opts = opts or options()
+        self._check(lib().karam_run_mc_device(self.h, C.byref(opts), dt, n_steps, method))
+
+    def read_results(self, want_stats=True):
+        v = np.zeros((self.ni, self.n))
+        st = (A.KaramInstanceStats * self.ni)() if want_stats else None
+        self._check(lib().karam_read_results(self.h, A.ptr(v, C.c_double), st))
+        return v, (self._stats(st) if want_stats else None)
+
+    def sync(self):
+        self._check(lib().karam_sync(self.h))
+
+    def eval_stamp(self, v, precision=A.PREC_FP64):
+        v = np.ascontiguousarray(v, np.float64).reshape(self.ni, self.n)
+        jac = np.zeros((self.ni, self.info["nnz"]))
+        f = np.zeros((self.ni, self.n))
+        self._check(lib().karam_eval_stamp(self.h, precision, A.ptr(v, C.c_double),
+                                           A.ptr(jac, C.c_double), A.ptr(f, C.c_double)))
+        return jac, f
+
+    def timing(self):
+        e, l = C.c_double(), C.c_double()
+        ne, nl_, r = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(lib().karam_last_timing(self.h, C.byref(e), C.byref(l), C.byref(ne),
+                                            C.byref(nl_), C.byref(r)))
+        return dict(eval_ms=e.value, lu_ms=l.value, eval_launches=ne.value,
+                    lu_launches=nl_.value, rounds=r.value)

@@ -58,6 +58,7 @@ class KaramSolverOpts(C.Structure):
         ("kcl_tol", C.c_double), ("polish_max", C.c_int32), ("polish_rel", C.c_double),
         ("polish_abs", C.c_double), ("ir_steps", C.c_int32), ("seeded", C.c_int32),
         ("seed_max_iter", C.c_int32), ("schedule", C.c_int32), ("max_rounds", C.c_int32),
+        ("max_halvings", C.c_int32),
     ]
 
 
@@ -71,7 +72,8 @@ class KaramInstanceStats(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32),
                 ("polish_iters", C.c_int32), ("damped", C.c_int32),
                 ("gmin_step", C.c_int32), ("seeded_ok", C.c_int32),
-                ("residual", C.c_double)]
+                ("rescued", C.c_int32), ("halvings", C.c_int32),
+                ("max_step_iters", C.c_int32), ("residual", C.c_double)]
 
 
 def ptr(arr, ctype):

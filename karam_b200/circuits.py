@@ -39,12 +39,15 @@ class Netlist:
     mos: list = field(default_factory=list)      # (d, g, s, b, w, l, model)
     models: list = field(default_factory=list)   # (name, type, kp, vto, lam)
     _keep: list = field(default_factory=list, repr=False)
+    _struct: object = field(default=None, repr=False)
 
     # -- builders ---------------------------------------------------------
     def _touch(self, *nodes):
+        self._struct = None
         self.n_nodes = max([self.n_nodes, *nodes])
 
     def model(self, name, mtype, kp=math.nan, vto=math.nan, lam=math.nan):
+        self._struct = None
         self.models.append((name, mtype, kp, vto, lam))
         return len(self.models) - 1
 
@@ -75,6 +78,7 @@ class Netlist:
         self._touch(d, g, s, b)
 
     def new_node(self):
+        self._struct = None
         self.n_nodes += 1
         return self.n_nodes
 
@@ -110,6 +114,9 @@ class Netlist:
         return out
 
     def as_struct(self) -> A.KaramNetlist:
+        """The karam_netlist view; cached, and valid while this object lives."""
+        if self._struct is not None:
+            return self._struct
         a = self.arrays()
         names = (C.c_char_p * max(1, len(self.models)))(*[x[0].encode() for x in self.models])
         self._keep = [a, names]
@@ -123,6 +130,7 @@ class Netlist:
             ctype = C.c_int32 if arr.dtype == np.int32 else C.c_double
             setattr(s, key, A.ptr(arr if arr.size else None, ctype))
         s.model_name = C.cast(names, C.POINTER(C.c_char_p))
+        self._struct = s
         return s
 
     @property

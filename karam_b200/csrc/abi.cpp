@@ -1,0 +1,835 @@
+// abi.cpp -- implementation of the C ABI (include/karam.h): contexts, problems,
+// device buffers and the round driver that replays CUDA graphs of NR rounds.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/karam.h"
+#include "device.hpp"
+#include "topology.hpp"
+
+using namespace karam;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw CudaError(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+// Owning device allocation.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t b) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = b;
+    if (b) ck(cudaMalloc(&p, b), "cudaMalloc");
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DBuf& b, const std::vector<T>& v) {
+  b.alloc(std::max<size_t>(v.size(), 1) * sizeof(T));
+  if (!v.empty()) ck(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
+
+}  // namespace
+
+struct karam_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  int max_smem = 0;
+  std::string err;
+};
+
+struct karam_problem {
+  karam_ctx* ctx = nullptr;
+  Topology topo;
+  int max_inst = 0;
+  int ni = 0;
+  bool inst_kp = false, inst_vth = false;  // per-instance MOSFET values present
+  bool have_dc = false;
+  bool tran_started = false;  // capacitor history holds a transient in progress
+  double t_now = 0.0, tran_h = 0.0;
+  int tran_method = KARAM_TRAN_BE;
+
+  // topology buffers
+  DBuf t_mos_term, t_mos_geo, t_mos_pmos, t_dio_term, t_dio_par, t_res_term, t_res_g, t_cap_term,
+      t_cap_c, t_mos_card, t_f_row, t_f_colp, t_vs_term, t_vs_kind, t_vs_pulse, t_is_term, t_is_amp, t_jt_off, t_jt_code,
+      t_jlin, t_jcap_off, t_jcap_code, t_ft_off, t_ft_code, t_lu_hdr, t_lu_data, t_seed_vs,
+      t_seed_anode, t_perm;
+  DevTopo dt{};
+  // instance buffers
+  DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_Fmax, i_J, i_cvp, i_cip, i_st, i_seed,
+      i_out, d_active, r_ws, r_list, r_count, i_vtp;
+  int rescue_slots = 0;
+  int* h_active = nullptr;  // pinned
+
+  // timing of the last solve call
+  double eval_ms = 0, lu_ms = 0;
+  int eval_launches = 0, lu_launches = 0, rounds = 0;
+
+  std::vector<int> csr_to_f;  // CSR position -> filled position
+
+  ~karam_problem() {
+    if (h_active) cudaFreeHost(h_active);
+  }
+};
+
+namespace {
+
+void set_err(karam_ctx* c, const std::string& m) {
+  if (c)
+    c->err = m;
+  else
+    g_create_error = m;
+}
+
+// Solves need a problem made with a context; a context-less problem carries
+// only the host symbolic analysis.
+void need_device(const karam_problem* p) {
+  if (!p->ctx) throw std::logic_error("problem was created without a context (symbolic only)");
+}
+
+template <class F>
+int guarded(karam_ctx* c, F f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    set_err(c, e.what());
+    return KARAM_E_CUDA;
+  } catch (const std::bad_alloc&) {
+    set_err(c, "out of host memory");
+    return KARAM_E_NOMEM;
+  } catch (const std::logic_error& e) {
+    set_err(c, e.what());
+    return KARAM_E_STATE;
+  } catch (const std::exception& e) {
+    set_err(c, e.what());
+    return KARAM_E_INVALID;
+  }
+}
+
+void upload_topology(karam_problem* p) {
+  const Topology& T = p->topo;
+  std::vector<int4> mt;
+  std::vector<double2> mg;
+  std::vector<int> mp;
+  std::vector<double2> mc;
+  for (size_t i = 0; i < T.mos.size(); ++i) {
+    mc.push_back(make_double2(T.mos[i].kp_card, T.mos[i].vto_card));
+    mt.push_back(make_int4(T.mos_term[4 * i], T.mos_term[4 * i + 1], T.mos_term[4 * i + 2],
+                           T.mos_term[4 * i + 3]));
+    mg.push_back(make_double2(T.mos[i].wl, T.mos[i].lam));
+    mp.push_back(T.mos[i].pmos ? 1 : 0);
+  }
+  std::vector<int2> dtm, rtm, ctm, vtm, itm;
+  std::vector<double4> dpar;
+  for (size_t i = 0; i < T.dio.size(); ++i) {
+    dtm.push_back(make_int2(T.dio_term[2 * i], T.dio_term[2 * i + 1]));
+    dpar.push_back(make_double4(T.dio[i].is, T.dio[i].n, T.dio[i].vt, 0.0));
+  }
+  std::vector<double> rg, cc, vpulse, ia;
+  for (size_t i = 0; i < T.res.size(); ++i) {
+    rtm.push_back(make_int2(T.res_term[2 * i], T.res_term[2 * i + 1]));
+    rg.push_back(1.0 / T.res[i].val);
+  }
+  for (size_t i = 0; i < T.cap.size(); ++i) {
+    ctm.push_back(make_int2(T.cap_term[2 * i], T.cap_term[2 * i + 1]));
+    cc.push_back(T.cap[i].val);
+  }
+  std::vector<int> vk, seed_vs;
+  for (size_t i = 0; i < T.vs.size(); ++i) {
+    vtm.push_back(make_int2(T.vs_term[2 * i], T.vs_term[2 * i + 1]));
+    vk.push_back(T.vs[i].kind);
+    for (int k = 0; k < 7; ++k) vpulse.push_back(T.vs[i].pulse[k]);
+    seed_vs.push_back(T.vs[i].pos > 0 ? T.iperm[T.vs[i].pos - 1] : -1);
+  }
+  for (size_t i = 0; i < T.isrc.size(); ++i) {
+    itm.push_back(make_int2(T.is_term[2 * i], T.is_term[2 * i + 1]));
+    ia.push_back(T.isrc[i].val);
+  }
+  std::vector<int> seed_an;
+  for (int a : T.seed_anodes) seed_an.push_back(a > 0 ? T.iperm[a - 1] : -1);
+  std::vector<int4> hdr;
+  for (int k = 0; k < T.n; ++k)
+    hdr.push_back(make_int4(T.lu_hdr[4 * k], T.lu_hdr[4 * k + 1], T.lu_hdr[4 * k + 2], 0));
+
+  upload(p->t_mos_term, mt);
+  upload(p->t_mos_geo, mg);
+  upload(p->t_mos_pmos, mp);
+  upload(p->t_mos_card, mc);
+  upload(p->t_dio_term, dtm);
+  upload(p->t_dio_par, dpar);
+  upload(p->t_res_term, rtm);
+  upload(p->t_res_g, rg);
+  upload(p->t_cap_term, ctm);
+  upload(p->t_cap_c, cc);
+  upload(p->t_vs_term, vtm);
+  upload(p->t_vs_kind, vk);
+  upload(p->t_vs_pulse, vpulse);
+  upload(p->t_is_term, itm);
+  upload(p->t_is_amp, ia);
+  upload(p->t_jt_off, T.jt_off);
+  upload(p->t_jt_code, T.jt_code);
+  upload(p->t_jlin, T.jlin_dc);
+  upload(p->t_jcap_off, T.jcap_off);
+  upload(p->t_jcap_code, T.jcap_code);
+  upload(p->t_ft_off, T.ft_off);
+  upload(p->t_ft_code, T.ft_code);
+  upload(p->t_lu_hdr, hdr);
+  upload(p->t_lu_data, T.lu_data);
+  upload(p->t_seed_vs, seed_vs);
+  upload(p->t_seed_anode, seed_an);
+  upload(p->t_perm, T.perm);
+  std::vector<int> frow(T.nnz_filled());
+  for (int i = 0; i < T.n; ++i)
+    for (int k = T.f_row_ptr[i]; k < T.f_row_ptr[i + 1]; ++k) frow[k] = i;
+  upload(p->t_f_row, frow);
+  upload(p->t_f_colp, T.f_col);
+
+  DevTopo& d = p->dt;
+  d.n = T.n;
+  d.nf = T.nnz_filled();
+  d.n_mos = (int)T.mos.size();
+  d.n_dio = (int)T.dio.size();
+  d.n_res = (int)T.res.size();
+  d.n_cap = (int)T.cap.size();
+  d.n_vs = (int)T.vs.size();
+  d.n_is = (int)T.isrc.size();
+  d.temp_k = T.temp_k;
+  d.mos_term = p->t_mos_term.as<int4>();
+  d.mos_geo = p->t_mos_geo.as<double2>();
+  d.mos_pmos = p->t_mos_pmos.as<int>();
+  d.mos_card = p->t_mos_card.as<double2>();
+  d.dio_term = p->t_dio_term.as<int2>();
+  d.dio_par = p->t_dio_par.as<double4>();
+  d.res_term = p->t_res_term.as<int2>();
+  d.res_g = p->t_res_g.as<double>();
+  d.cap_term = p->t_cap_term.as<int2>();
+  d.cap_c = p->t_cap_c.as<double>();
+  d.vs_term = p->t_vs_term.as<int2>();
+  d.vs_kind = p->t_vs_kind.as<int>();
+  d.vs_pulse = p->t_vs_pulse.as<double>();
+  d.is_term = p->t_is_term.as<int2>();
+  d.is_amp = p->t_is_amp.as<double>();
+  d.jt_off = p->t_jt_off.as<int>();
+  d.jt_code = p->t_jt_code.as<int>();
+  d.jlin_dc = p->t_jlin.as<double>();
+  d.jcap_off = p->t_jcap_off.as<int>();
+  d.jcap_code = p->t_jcap_code.as<int>();
+  d.ft_off = p->t_ft_off.as<int>();
+  d.ft_code = p->t_ft_code.as<int>();
+  d.lu_hdr = p->t_lu_hdr.as<int4>();
+  d.lu_data = p->t_lu_data.as<int>();
+  d.f_row = p->t_f_row.as<int>();
+  d.f_colp = p->t_f_colp.as<int>();
+  d.seed_vs = p->t_seed_vs.as<int>();
+  d.seed_anode = p->t_seed_anode.as<int>();
+  d.n_seed_anode = (int)seed_an.size();
+
+  // CSR position -> filled position (for karam_eval_stamp)
+  p->csr_to_f.assign(T.nnz(), -1);
+  for (size_t k = 0; k < T.trip.size(); ++k) p->csr_to_f[T.slot_csr[k]] = T.trip[k].f;
+}
+
+void alloc_instances(karam_problem* p) {
+  const Topology& T = p->topo;
+  const size_t M = (size_t)p->max_inst, n = T.n, nm = T.mos.size(), nv = T.vs.size();
+  p->i_kp.alloc(std::max<size_t>(1, M * nm) * sizeof(float));
+  p->i_vth.alloc(std::max<size_t>(1, M * nm) * sizeof(float));
+  p->i_vsdc.alloc(std::max<size_t>(1, M * nv) * sizeof(double));
+  p->i_v1.alloc(std::max<size_t>(1, M * nv) * sizeof(double));
+  p->i_v2.alloc(std::max<size_t>(1, M * nv) * sizeof(double));
+  p->i_v.alloc(M * n * sizeof(double));
+  p->i_x.alloc(M * n * sizeof(double));
+  p->i_F.alloc(M * n * sizeof(double));
+  p->i_Fmax.alloc(M * sizeof(double));
+  p->i_J.alloc(M * (size_t)T.nnz_filled() * sizeof(double));
+  p->i_cvp.alloc(std::max<size_t>(1, M * T.cap.size()) * sizeof(double));
+  p->i_cip.alloc(std::max<size_t>(1, M * T.cap.size()) * sizeof(double));
+  p->i_st.alloc(M * sizeof(InstState));
+  p->i_seed.alloc(M * n * sizeof(double));
+  p->i_vtp.alloc(M * n * sizeof(double));
+  p->i_out.alloc(M * n * sizeof(double));
+  p->d_active.alloc(sizeof(int));
+  // Partial-pivoting rescue: one dense n x n FP64 workspace per concurrently
+  // running rescue CTA, bounded by a 2 GiB budget.
+  const size_t dense = n * n * sizeof(double);
+  const size_t budget = size_t(2) << 30;
+  size_t slots = std::min<size_t>({M, (size_t)8 * std::max(1, p->ctx->num_sms), budget / dense});
+  p->rescue_slots = (int)slots;
+  if (slots > 0) {
+    p->r_ws.alloc(slots * dense);
+    p->r_list.alloc(M * sizeof(RescueItem));
+    p->r_count.alloc(sizeof(int));
+    ck(cudaMemset(p->r_count.p, 0, sizeof(int)), "memset rescue count");
+  }
+  ck(cudaMallocHost(&p->h_active, sizeof(int)), "cudaMallocHost");
+}
+
+DevInst dev_inst(karam_problem* p) {
+  DevInst I{};
+  I.ni = p->ni;
+  I.kp = p->inst_kp ? p->i_kp.as<float>() : nullptr;
+  I.vth = p->inst_vth ? p->i_vth.as<float>() : nullptr;
+  I.vs_dc = p->i_vsdc.as<double>();
+  I.vs_v1 = p->i_v1.as<double>();
+  I.vs_v2 = p->i_v2.as<double>();
+  I.v = p->i_v.as<double>();
+  I.x = p->i_x.as<double>();
+  I.F = p->i_F.as<double>();
+  I.Fmax = p->i_Fmax.as<double>();
+  I.J = p->i_J.p;
+  I.cap_vp = p->i_cvp.as<double>();
+  I.cap_ip = p->i_cip.as<double>();
+  I.v_tp = p->i_vtp.as<double>();
+  I.st = p->i_st.as<InstState>();
+  I.seed = nullptr;
+  I.rescue_ws = p->rescue_slots > 0 ? p->r_ws.as<double>() : nullptr;
+  I.rescue_list = p->rescue_slots > 0 ? p->r_list.as<RescueItem>() : nullptr;
+  I.rescue_count = p->rescue_slots > 0 ? p->r_count.as<int>() : nullptr;
+  I.rescue_slots = p->rescue_slots;
+  I.wave = nullptr;
+  I.wave_pos = nullptr;
+  I.n_wave = 0;
+  I.wave_steps = 0;
+  return I;
+}
+
+void set_instances_impl(karam_problem* p, const karam_instances* inst) {
+  const Topology& T = p->topo;
+  int ni = inst ? inst->n_instances : 1;
+  if (ni < 1 || ni > p->max_inst) throw std::runtime_error("n_instances out of range");
+  const size_t nm = T.mos.size(), nv = T.vs.size();
+  std::vector<float> kp((size_t)ni * nm), vth((size_t)ni * nm);
+  std::vector<double> vdc((size_t)ni * nv), v1((size_t)ni * nv), v2((size_t)ni * nv);
+  for (int i = 0; i < ni; ++i) {
+    for (size_t j = 0; j < nm; ++j) {
+      const size_t src = (size_t)i * nm + T.mos_order[j];
+      kp[(size_t)i * nm + j] = (inst && inst->mos_kp) ? inst->mos_kp[src] : (float)T.mos[j].kp_card;
+      vth[(size_t)i * nm + j] = (inst && inst->mos_vto) ? inst->mos_vto[src] : (float)T.mos[j].vto_card;
+    }
+    for (size_t s = 0; s < nv; ++s) {
+      const auto& V = T.vs[s];
+      double dc = V.dc, sc = 1.0;
+      if (inst && inst->vs_dc) {
+        dc = inst->vs_dc[(size_t)i * nv + s];
+        if (V.dc != 0.0) sc = dc / V.dc;
+      }
+      vdc[(size_t)i * nv + s] = dc;
+      v1[(size_t)i * nv + s] = V.kind == KARAM_SRC_PULSE ? V.pulse[0] * sc : dc;
+      v2[(size_t)i * nv + s] = V.kind == KARAM_SRC_PULSE ? V.pulse[1] * sc : dc;
+    }
+  }
+  // Without per-instance values the kernel reads the FP64 model-card table.
+  p->inst_kp = inst && inst->mos_kp;
+  p->inst_vth = inst && inst->mos_vto;
+  cudaStream_t s = p->ctx->stream;
+  if (nm) {
+    ck(cudaMemcpyAsync(p->i_kp.p, kp.data(), kp.size() * sizeof(float), cudaMemcpyHostToDevice, s), "H2D kp");
+    ck(cudaMemcpyAsync(p->i_vth.p, vth.data(), vth.size() * sizeof(float), cudaMemcpyHostToDevice, s), "H2D vth");
+  }
+  if (nv) {
+    ck(cudaMemcpyAsync(p->i_vsdc.p, vdc.data(), vdc.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D vs");
+    ck(cudaMemcpyAsync(p->i_v1.p, v1.data(), v1.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D v1");
+    ck(cudaMemcpyAsync(p->i_v2.p, v2.data(), v2.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D v2");
+  }
+  ck(cudaStreamSynchronize(s), "set_instances sync");
+  p->ni = ni;
+  p->have_dc = false;
+}
+
+JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int method) {
+  JobParams P{};
+  karam_solver_opts d;
+  karam_default_opts(&d);
+  if (!o) o = &d;
+  P.precision = o->precision;
+  P.max_nr_iter = o->max_nr_iter;
+  P.gmin_steps = o->gmin_steps;
+  P.reltol = o->reltol;
+  P.vntol = o->vntol;
+  P.kcl_shortcut = o->kcl_shortcut;
+  P.kcl_tol = o->kcl_tol;
+  P.polish_max = o->polish_max;
+  P.polish_rel = o->polish_rel;
+  P.polish_abs = o->polish_abs;
+  P.n_steps = n_steps;
+  P.h = h;
+  P.method = method;
+  P.seeded = o->seeded;
+  P.seed_max_iter = o->seed_max_iter;
+  P.max_halvings = o->max_halvings;
+  if (P.max_halvings < 0 || P.max_halvings > 10) throw std::runtime_error("max_halvings must be in 0..10");
+  if (P.max_nr_iter < 1 || P.gmin_steps < 1 || P.polish_max < 0)
+    throw std::runtime_error("invalid solver options");
+  if (P.precision != KARAM_PREC_FP64 && P.precision != KARAM_PREC_MIXED)
+    throw std::runtime_error("unknown precision");
+  if (n_steps > 0 && !(h > 0)) throw std::runtime_error("transient step must be > 0");
+  if (method != KARAM_TRAN_BE && method != KARAM_TRAN_TRAP) throw std::runtime_error("unknown method");
+  return P;
+}
+
+// Runs NR rounds until every instance is done (or the round budget ends).
+// Rounds are captured in a CUDA graph of kRounds (eval, lu) pairs with event
+// records around each kernel; the last round's LU kernel counts the live
+// instances into d_active, which is read back after every replay.
+void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
+                const DevInst* inst = nullptr) {
+  constexpr int kRounds = 16;
+  cudaStream_t s = p->ctx->stream;
+  DevInst I = inst ? *inst : dev_inst(p);
+  const int prec = P.precision;
+  LuLaunch L = plan_lu(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms);
+  if (L.ni_per_cta < 1)
+    throw std::runtime_error("instance too large for the thread-per-instance schedule");
+  configure_kernels(p->dt, L);
+  ck(cudaGetLastError(), "configure kernels");
+  std::vector<cudaEvent_t> ev(3 * kRounds);
+  for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+  struct EvGuard {
+    std::vector<cudaEvent_t>& v;
+    ~EvGuard() {
+      for (auto e : v) cudaEventDestroy(e);
+    }
+  } eg{ev};
+  int* active = p->d_active.as<int>();
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  // External event records become event-record nodes of the graph (a plain
+  // record inside capture would only order work within the capture).
+  for (int r = 0; r < kRounds; ++r) {
+    cudaEventRecordWithFlags(ev[3 * r], s, cudaEventRecordExternal);
+    launch_eval(p->dt, I, P, prec, s);
+    cudaEventRecordWithFlags(ev[3 * r + 1], s, cudaEventRecordExternal);
+    if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
+    launch_lu(p->dt, I, P, L, prec, active, s);
+    if (I.rescue_list) launch_rescue(p->dt, I, P, prec, I.rescue_slots, s);
+    cudaEventRecordWithFlags(ev[3 * r + 2], s, cudaEventRecordExternal);
+  }
+  const cudaError_t launch_err = cudaGetLastError();
+  ck(cudaStreamEndCapture(s, &graph), "end capture");
+  ck(launch_err, "kernel launch in capture");
+  struct GraphGuard {
+    cudaGraph_t& g;
+    cudaGraphExec_t& e;
+    ~GraphGuard() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+    }
+  } gg{graph, exec};
+  ck(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+
+  p->eval_ms = p->lu_ms = 0;
+  p->eval_launches = p->lu_launches = p->rounds = 0;
+  const int budget = max_rounds > 0 ? max_rounds : (1 << 30);
+  while (true) {
+    ck(cudaGraphLaunch(exec, s), "graph launch");
+    ck(cudaMemcpyAsync(p->h_active, active, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
+    ck(cudaStreamSynchronize(s), "round sync");
+    for (int r = 0; r < kRounds; ++r) {
+      float a = 0, b = 0;
+      ck(cudaEventElapsedTime(&a, ev[3 * r], ev[3 * r + 1]), "event time");
+      ck(cudaEventElapsedTime(&b, ev[3 * r + 1], ev[3 * r + 2]), "event time");
+      p->eval_ms += a;
+      p->lu_ms += b;
+    }
+    p->eval_launches += kRounds;
+    p->lu_launches += kRounds;
+    p->rounds += kRounds;
+    if (*p->h_active == 0 || p->rounds >= budget) break;
+  }
+}
+
+void read_stats(karam_problem* p, karam_instance_stats* stats, bool dc_only) {
+  if (!stats) return;
+  std::vector<InstState> st(p->ni);
+  ck(cudaMemcpy(st.data(), p->i_st.p, st.size() * sizeof(InstState), cudaMemcpyDeviceToHost), "D2H state");
+  for (int i = 0; i < p->ni; ++i) {
+    const InstState& s = st[i];
+    karam_instance_stats& o = stats[i];
+    o.status = s.mode == MODE_DONE ? s.status : KARAM_ST_TIMEOUT;
+    o.iterations = dc_only ? s.iters : s.iters + s.tran_iters;
+    o.polish_iters = s.polish;
+    o.damped = s.damped;
+    o.gmin_step = s.g;
+    o.seeded_ok = s.seeded_ok;
+    o.rescued = s.rescued;
+    o.halvings = s.halvings;
+    o.max_step_iters = s.max_step_it;
+    o.residual = s.resid;
+  }
+}
+
+void read_voltages(karam_problem* p, double* out_v) {
+  if (!out_v) return;
+  const int n = p->topo.n;
+  unpermute(p->i_v.as<double>(), p->t_perm.as<int>(), p->i_out.as<double>(), p->ni, n, p->ctx->stream);
+  ck(cudaMemcpyAsync(out_v, p->i_out.p, (size_t)p->ni * n * sizeof(double), cudaMemcpyDeviceToHost,
+                     p->ctx->stream),
+     "D2H v");
+  ck(cudaStreamSynchronize(p->ctx->stream), "read sync");
+}
+
+void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
+  DevInst I = dev_inst(p);
+  if (P.seeded && seed_v) {
+    // caller guesses arrive in node order; the device works in permuted order
+    const int n = p->topo.n;
+    std::vector<double> perm_seed((size_t)p->ni * n);
+    for (int i = 0; i < p->ni; ++i)
+      for (int k = 0; k < n; ++k) perm_seed[(size_t)i * n + k] = seed_v[(size_t)i * n + p->topo.perm[k]];
+    ck(cudaMemcpyAsync(p->i_seed.p, perm_seed.data(), perm_seed.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, p->ctx->stream),
+       "H2D seed");
+    I.seed = p->i_seed.as<double>();
+  }
+  launch_init(p->dt, I, P, p->ctx->stream);
+  ck(cudaGetLastError(), "init launch");
+  p->tran_started = P.n_steps > 0;
+  p->t_now = P.n_steps > 0 ? P.n_steps * P.h : 0.0;
+  p->tran_h = P.h;
+  p->tran_method = P.method;
+}
+
+}  // namespace
+
+extern "C" {
+
+void karam_default_opts(karam_solver_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = KARAM_PREC_FP64;
+  o->max_nr_iter = 50;
+  o->gmin_steps = 19;
+  o->reltol = 1e-3;
+  o->vntol = 1e-6;
+  o->kcl_shortcut = 1e-9;
+  o->kcl_tol = 1e-12;
+  o->polish_max = 0;
+  o->polish_rel = 0.0;
+  o->polish_abs = 0.0;
+  o->ir_steps = 0;
+  o->seeded = 0;
+  o->seed_max_iter = 10;
+  o->schedule = 0;
+  o->max_rounds = 0;
+  o->max_halvings = 3;
+}
+
+int karam_ctx_create(int device, karam_ctx** out) {
+  if (!out) return KARAM_E_INVALID;
+  *out = nullptr;
+  try {
+    int count = 0;
+    ck(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (device < 0 || device >= count) throw CudaError("no CUDA device with that index");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    auto c = std::make_unique<karam_ctx>();
+    c->device = device;
+    ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "attr");
+    ck(cudaDeviceGetAttribute(&c->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attr");
+    *out = c.release();
+    return KARAM_OK;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    return KARAM_E_CUDA;
+  }
+}
+
+void karam_ctx_destroy(karam_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* karam_last_error(const karam_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int karam_problem_create(karam_ctx* ctx, const karam_netlist* nl, int32_t max_instances,
+                         karam_problem** out) {
+  if (!out) return KARAM_E_INVALID;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    if (max_instances < 1) throw std::runtime_error("max_instances must be >= 1");
+    auto p = std::make_unique<karam_problem>();
+    p->topo = build_topology(nl);
+    p->max_inst = max_instances;
+    if (!ctx) {  // symbolic analysis only
+      *out = p.release();
+      return KARAM_OK;
+    }
+    ck(cudaSetDevice(ctx->device), "cudaSetDevice");
+    p->ctx = ctx;
+    upload_topology(p.get());
+    alloc_instances(p.get());
+    set_instances_impl(p.get(), nullptr);
+    *out = p.release();
+    return KARAM_OK;
+  });
+}
+
+void karam_problem_destroy(karam_problem* p) { delete p; }
+
+int karam_problem_info_get(const karam_problem* p, karam_problem_info* o) {
+  if (!p || !o) return KARAM_E_INVALID;
+  const Topology& T = p->topo;
+  o->n = T.n;
+  o->nnz = T.nnz();
+  o->nnz_filled = T.nnz_filled();
+  o->fill_in = T.fill_in;
+  o->treewidth = T.treewidth;
+  o->n_triplets = (int)T.trip.size();
+  o->n_instances = p->ni;
+  o->n_mos = (int)T.mos.size();
+  o->n_dio = (int)T.dio.size();
+  o->n_res = (int)T.res.size();
+  o->n_cap = (int)T.cap.size();
+  o->n_vsrc = (int)T.vs.size();
+  o->n_isrc = (int)T.isrc.size();
+  o->lu_ops = T.lu_ops;
+  return KARAM_OK;
+}
+
+int karam_set_instances(karam_problem* p, const karam_instances* inst) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    set_instances_impl(p, inst);
+    return KARAM_OK;
+  });
+}
+
+int karam_solve_dc(karam_problem* p, const karam_solver_opts* opts, const double* seed_v,
+                   double* out_v, karam_instance_stats* stats) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    JobParams P = job_params(opts, 0, 0.0, KARAM_TRAN_BE);
+    if (P.seeded && !seed_v) throw std::runtime_error("seeded solve without seed_v");
+    start_job(p, P, seed_v);
+    run_rounds(p, P, opts ? opts->max_rounds : 0);
+    p->have_dc = true;
+    read_voltages(p, out_v);
+    read_stats(p, stats, true);
+    return KARAM_OK;
+  });
+}
+
+int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double dt,
+                        int32_t n_steps, int32_t method) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    JobParams P = job_params(opts, n_steps, dt, method);
+    if (P.seeded) throw std::runtime_error("seeded starts need karam_solve_dc");
+    start_job(p, P, nullptr);
+    run_rounds(p, P, opts ? opts->max_rounds : 0);
+    p->have_dc = true;
+    return KARAM_OK;
+  });
+}
+
+int karam_read_results(karam_problem* p, double* out_v, karam_instance_stats* stats) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    read_voltages(p, out_v);
+    read_stats(p, stats, false);
+    return KARAM_OK;
+  });
+}
+
+int karam_run_mc(karam_problem* p, const karam_instances* inst, const karam_solver_opts* opts,
+                 double dt, int32_t n_steps, int32_t method, double* out_v,
+                 karam_instance_stats* stats) {
+  if (!p) return KARAM_E_INVALID;
+  int rc = karam_set_instances(p, inst);
+  if (rc != KARAM_OK) return rc;
+  rc = karam_run_mc_device(p, opts, dt, n_steps, method);
+  if (rc != KARAM_OK) return rc;
+  return karam_read_results(p, out_v, stats);
+}
+
+int karam_step_transient(karam_problem* p, const karam_solver_opts* opts, double dt,
+                         int32_t n_steps, int32_t method, const int32_t* wave_nodes,
+                         int32_t n_wave, double* wave_out, double* out_v,
+                         karam_instance_stats* stats) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    if (!p->have_dc) throw std::runtime_error("karam_step_transient needs a DC solution first");
+    if (n_steps < 1) throw std::runtime_error("n_steps must be >= 1");
+    if (n_wave > 0 && (!wave_nodes || !wave_out)) throw std::runtime_error("wave buffers missing");
+    if (p->tran_started && (dt != p->tran_h || method != p->tran_method))
+      throw std::runtime_error("a transient continues with the step and method it started with");
+    JobParams P = job_params(opts, n_steps, dt, method);
+    P.t0 = p->t_now;
+    DevInst I = dev_inst(p);
+    DBuf wave, wpos;
+    if (n_wave > 0) {
+      std::vector<int> pos(n_wave);
+      for (int k = 0; k < n_wave; ++k) {
+        int node = wave_nodes[k];
+        if (node < 0 || node > p->topo.n) throw std::runtime_error("wave node out of range");
+        pos[k] = node > 0 ? p->topo.iperm[node - 1] : -1;
+      }
+      upload(wpos, pos);
+      wave.alloc((size_t)p->ni * n_steps * n_wave * sizeof(double));
+      ck(cudaMemset(wave.p, 0, wave.bytes), "memset wave");
+    }
+    I.wave = wave.as<double>();
+    I.wave_pos = wpos.as<int>();
+    I.n_wave = n_wave;
+    I.wave_steps = n_steps;
+    launch_tran_start(p->dt, I, p->tran_started ? 0 : 1, p->ctx->stream);
+    ck(cudaGetLastError(), "tran start");
+    run_rounds(p, P, opts ? opts->max_rounds : 0, &I);
+    p->tran_started = true;
+    p->tran_h = dt;
+    p->tran_method = method;
+    p->t_now += n_steps * dt;
+    if (n_wave > 0)
+      ck(cudaMemcpy(wave_out, wave.p, wave.bytes, cudaMemcpyDeviceToHost), "D2H wave");
+    read_voltages(p, out_v);
+    read_stats(p, stats, false);
+    return KARAM_OK;
+  });
+}
+
+int karam_sync(karam_problem* p) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    ck(cudaStreamSynchronize(p->ctx->stream), "sync");
+    return KARAM_OK;
+  });
+}
+
+int karam_get_pattern(const karam_problem* p, int32_t* row_ptr, int32_t* col) {
+  if (!p) return KARAM_E_INVALID;
+  if (row_ptr) std::copy(p->topo.row_ptr.begin(), p->topo.row_ptr.end(), row_ptr);
+  if (col) std::copy(p->topo.col.begin(), p->topo.col.end(), col);
+  return KARAM_OK;
+}
+
+int karam_get_stamp_map(const karam_problem* p, int32_t* slot_csr) {
+  if (!p || !slot_csr) return KARAM_E_INVALID;
+  std::copy(p->topo.slot_csr.begin(), p->topo.slot_csr.end(), slot_csr);
+  return KARAM_OK;
+}
+
+int karam_get_ordering(const karam_problem* p, uint32_t* raw, int32_t* raw_len, int32_t* perm) {
+  if (!p) return KARAM_E_INVALID;
+  if (raw) std::copy(p->topo.raw_order.begin(), p->topo.raw_order.end(), raw);
+  if (raw_len) *raw_len = (int32_t)p->topo.raw_order.size();
+  if (perm) std::copy(p->topo.perm.begin(), p->topo.perm.end(), perm);
+  return KARAM_OK;
+}
+
+int karam_get_filled_pattern(const karam_problem* p, int32_t* f_row_ptr, int32_t* f_col) {
+  if (!p) return KARAM_E_INVALID;
+  if (f_row_ptr) std::copy(p->topo.f_row_ptr.begin(), p->topo.f_row_ptr.end(), f_row_ptr);
+  if (f_col) std::copy(p->topo.f_col.begin(), p->topo.f_col.end(), f_col);
+  return KARAM_OK;
+}
+
+int karam_get_device_order(const karam_problem* p, int32_t* mos_order, int32_t* dio_order) {
+  if (!p) return KARAM_E_INVALID;
+  if (mos_order) std::copy(p->topo.mos_order.begin(), p->topo.mos_order.end(), mos_order);
+  if (dio_order) std::copy(p->topo.dio_order.begin(), p->topo.dio_order.end(), dio_order);
+  return KARAM_OK;
+}
+
+int karam_eval_stamp(karam_problem* p, int32_t precision, const double* v, double* jac, double* f) {
+  if (!p || !v) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    const Topology& T = p->topo;
+    const int n = T.n, nf = T.nnz_filled(), ni = p->ni;
+    std::vector<double> vp((size_t)ni * n);
+    for (int i = 0; i < ni; ++i)
+      for (int k = 0; k < n; ++k) vp[(size_t)i * n + k] = v[(size_t)i * n + T.perm[k]];
+    cudaStream_t s = p->ctx->stream;
+    ck(cudaMemcpyAsync(p->i_x.p, vp.data(), vp.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D x");
+    std::vector<InstState> st(ni);
+    for (auto& e : st) {
+      e = InstState{};
+      e.mode = MODE_DC;
+    }
+    ck(cudaMemcpyAsync(p->i_st.p, st.data(), st.size() * sizeof(InstState), cudaMemcpyHostToDevice, s), "H2D st");
+    JobParams P = job_params(nullptr, 0, 0.0, KARAM_TRAN_BE);
+    DevInst I = dev_inst(p);
+    configure_kernels(p->dt, plan_lu(p->dt, ni, precision, p->ctx->max_smem, p->ctx->num_sms));
+    launch_eval(p->dt, I, P, precision, s);
+    ck(cudaGetLastError(), "eval launch");
+    std::vector<double> F((size_t)ni * n);
+    ck(cudaMemcpyAsync(F.data(), p->i_F.p, F.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H F");
+    std::vector<double> J64;
+    std::vector<float> J32;
+    if (precision == KARAM_PREC_MIXED) {
+      J32.resize((size_t)ni * nf);
+      ck(cudaMemcpyAsync(J32.data(), p->i_J.p, J32.size() * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H J");
+    } else {
+      J64.resize((size_t)ni * nf);
+      ck(cudaMemcpyAsync(J64.data(), p->i_J.p, J64.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H J");
+    }
+    ck(cudaStreamSynchronize(s), "eval sync");
+    p->have_dc = false;
+    const int nnz = T.nnz();
+    for (int i = 0; i < ni; ++i) {
+      if (jac)
+        for (int j = 0; j < nnz; ++j) {
+          const size_t src = (size_t)i * nf + p->csr_to_f[j];
+          jac[(size_t)i * nnz + j] = precision == KARAM_PREC_MIXED ? (double)J32[src] : J64[src];
+        }
+      if (f)
+        for (int k = 0; k < n; ++k) f[(size_t)i * n + T.perm[k]] = F[(size_t)i * n + k];
+    }
+    return KARAM_OK;
+  });
+}
+
+int karam_last_timing(const karam_problem* p, double* eval_ms, double* lu_ms,
+                      int32_t* eval_launches, int32_t* lu_launches, int32_t* rounds) {
+  if (!p) return KARAM_E_INVALID;
+  if (eval_ms) *eval_ms = p->eval_ms;
+  if (lu_ms) *lu_ms = p->lu_ms;
+  if (eval_launches) *eval_launches = p->eval_launches;
+  if (lu_launches) *lu_launches = p->lu_launches;
+  if (rounds) *rounds = p->rounds;
+  return KARAM_OK;
+}
+
+}  // extern "C"

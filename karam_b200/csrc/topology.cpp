@@ -1,0 +1,507 @@
+// topology.cpp -- host symbolic layer (see topology.hpp).
+#include "topology.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <unordered_set>
+
+namespace karam {
+namespace {
+
+void require(bool ok, const std::string& msg) {
+  if (!ok) throw std::runtime_error(msg);
+}
+
+inline int64_t key(int r, int c) { return (int64_t(r) << 32) | int64_t(uint32_t(c)); }
+
+// Two-terminal conductance stamp: 4 triplets, or 1 when a terminal is ground
+// (the pattern of every linear and diode stamp in stampSoABlock).
+void stamp_g(std::vector<Triplet>& t, int n1, int n2, int kind, int idx) {
+  if (n1 != 0 && n2 != 0) {
+    t.push_back({n1 - 1, n1 - 1, -1, kind, idx, false});
+    t.push_back({n2 - 1, n2 - 1, -1, kind, idx, false});
+    t.push_back({n1 - 1, n2 - 1, -1, kind, idx, true});
+    t.push_back({n2 - 1, n1 - 1, -1, kind, idx, true});
+  } else if (n1 != 0) {
+    t.push_back({n1 - 1, n1 - 1, -1, kind, idx, false});
+  } else if (n2 != 0) {
+    t.push_back({n2 - 1, n2 - 1, -1, kind, idx, false});
+  }
+}
+
+void tensorize(const karam_netlist* nl, Topology& T) {
+  require(nl != nullptr, "netlist is NULL");
+  require(nl->n_nodes >= 0, "n_nodes must not be negative");
+  require(nl->n_models >= 0 && nl->n_mos >= 0 && nl->n_dio >= 0 && nl->n_res >= 0 &&
+              nl->n_cap >= 0 && nl->n_vsrc >= 0 && nl->n_isrc >= 0,
+          "negative device count");
+  int nmax = nl->n_nodes;
+  auto node = [&](int x, const char* what) {
+    require(x >= 0, std::string("negative node id in ") + what);
+    nmax = std::max(nmax, x);
+    return x;
+  };
+  auto model_name = [&](int m) {
+    require(m >= 0 && m < nl->n_models && nl->model_name && nl->model_name[m],
+            "model index out of range");
+    return std::string(nl->model_name[m]);
+  };
+  T.temp_k = nl->temp_k > 0 ? nl->temp_k : 300.15;
+  const double tscale = T.temp_k / 300.15;
+
+  // Devices regrouped per model name, std::map order (physics_tensors.cpp:481-490).
+  std::map<std::string, std::vector<int>> mb, db;
+  for (int i = 0; i < nl->n_mos; ++i) {
+    int m = nl->m_model ? nl->m_model[i] : -1;
+    std::string nm = model_name(m);
+    int ty = nl->model_type[m];
+    require(ty == KARAM_MODEL_NMOS || ty == KARAM_MODEL_PMOS, "MOSFET model is not NMOS/PMOS");
+    mb[nm].push_back(i);
+  }
+  for (int i = 0; i < nl->n_dio; ++i) {
+    int m = nl->d_model ? nl->d_model[i] : -1;
+    db[m >= 0 ? model_name(m) : std::string("diode_generic")].push_back(i);
+  }
+  for (auto& kv : db)
+    for (int i : kv.second) {
+      require(nl->d_is[i] > 0 && nl->d_n[i] > 0 && nl->d_vt[i] > 0, "diode Is/N/Vt must be > 0");
+      T.dio.push_back({node(nl->d_anode[i], "diode"), node(nl->d_cathode[i], "diode"), nl->d_is[i],
+                       nl->d_n[i], nl->d_vt[i] * tscale});
+      T.dio_order.push_back(i);
+    }
+  for (auto& kv : mb)
+    for (int i : kv.second) {
+      int m = nl->m_model[i];
+      bool pmos = nl->model_type[m] == KARAM_MODEL_PMOS;
+      auto card = [&](const double* a, double dflt) {
+        return (a && !std::isnan(a[m])) ? a[m] : dflt;
+      };
+      require(nl->m_w[i] > 0 && nl->m_l[i] > 0, "MOSFET W and L must be > 0");
+      Topology::Mos q;
+      q.d = node(nl->m_d[i], "mosfet");
+      q.g = node(nl->m_g[i], "mosfet");
+      q.s = node(nl->m_s[i], "mosfet");
+      q.b = node(nl->m_b[i], "mosfet");
+      q.w = nl->m_w[i];
+      q.l = nl->m_l[i];
+      q.wl = q.w / q.l;
+      q.kp_card = card(nl->model_kp, pmos ? 100e-6 : 200e-6);
+      q.vto_card = card(nl->model_vto, pmos ? -0.7 : 0.7);
+      q.lam = card(nl->model_lambda, 0.02);
+      q.pmos = pmos;
+      T.mos.push_back(q);
+      T.mos_order.push_back(i);
+    }
+  for (int i = 0; i < nl->n_res; ++i) {
+    require(nl->r_ohm[i] > 0 && std::isfinite(nl->r_ohm[i]), "resistance must be finite and > 0");
+    T.res.push_back({node(nl->r_n1[i], "resistor"), node(nl->r_n2[i], "resistor"), nl->r_ohm[i]});
+  }
+  for (int i = 0; i < nl->n_cap; ++i) {
+    require(nl->c_farad[i] >= 0 && std::isfinite(nl->c_farad[i]), "capacitance must be >= 0");
+    T.cap.push_back({node(nl->c_n1[i], "capacitor"), node(nl->c_n2[i], "capacitor"), nl->c_farad[i]});
+  }
+  for (int i = 0; i < nl->n_isrc; ++i)
+    T.isrc.push_back({node(nl->is_pos[i], "isource"), node(nl->is_neg[i], "isource"), nl->is_amp[i]});
+  for (int i = 0; i < nl->n_vsrc; ++i) {
+    Topology::Vs v{};
+    v.pos = node(nl->vs_pos[i], "vsource");
+    v.neg = node(nl->vs_neg[i], "vsource");
+    v.kind = nl->vs_kind ? nl->vs_kind[i] : KARAM_SRC_DC;
+    require(v.kind == KARAM_SRC_DC || v.kind == KARAM_SRC_PULSE, "unknown source kind");
+    v.dc = nl->vs_dc[i];
+    if (v.kind == KARAM_SRC_PULSE) {
+      require(nl->vs_pulse != nullptr, "PULSE source without parameters");
+      for (int k = 0; k < 7; ++k) v.pulse[k] = nl->vs_pulse[7 * i + k];
+    }
+    T.vs.push_back(v);
+  }
+  for (int i = 0; i < nl->n_dio; ++i) T.seed_anodes.push_back(nl->d_anode[i]);
+  T.n = nmax;
+  require(T.n >= 1, "netlist has no unknowns");
+}
+
+// Stamp slots in stampSoABlock order (transient pattern: capacitor companions
+// included) followed by the gmin diagonal of addDiagonalConditioning.
+void stamps(Topology& T) {
+  auto& t = T.trip;
+  for (size_t i = 0; i < T.res.size(); ++i) stamp_g(t, T.res[i].n1, T.res[i].n2, SS_RES, (int)i);
+  for (size_t i = 0; i < T.vs.size(); ++i) stamp_g(t, T.vs[i].pos, T.vs[i].neg, SS_VS, (int)i);
+  for (size_t i = 0; i < T.cap.size(); ++i) stamp_g(t, T.cap[i].n1, T.cap[i].n2, SS_CAP, (int)i);
+  for (size_t i = 0; i < T.dio.size(); ++i) stamp_g(t, T.dio[i].a, T.dio[i].c, SS_DIO, (int)i);
+  for (size_t i = 0; i < T.mos.size(); ++i) {
+    const auto& q = T.mos[i];
+    int d = q.d, g = q.g, s = q.s, b = q.b, k = (int)i;
+    stamp_g(t, d, s, SS_MOS_GDS, k);
+    if (d != 0) {
+      if (g != 0) t.push_back({d - 1, g - 1, -1, SS_MOS_GM, k, false});
+      if (s != 0) t.push_back({d - 1, s - 1, -1, SS_MOS_GM, k, true});
+    }
+    if (s != 0) {
+      if (g != 0) t.push_back({s - 1, g - 1, -1, SS_MOS_GM, k, true});
+      t.push_back({s - 1, s - 1, -1, SS_MOS_GM, k, false});
+    }
+    if (d != 0) {
+      if (b != 0) t.push_back({d - 1, b - 1, -1, SS_MOS_GMB, k, false});
+      if (s != 0) t.push_back({d - 1, s - 1, -1, SS_MOS_GMB, k, true});
+    }
+    if (s != 0) {
+      if (b != 0) t.push_back({s - 1, b - 1, -1, SS_MOS_GMB, k, true});
+      t.push_back({s - 1, s - 1, -1, SS_MOS_GMB, k, false});
+    }
+  }
+  for (int i = 0; i < T.n; ++i) t.push_back({i, i, -1, SS_GMIN, i, false});
+
+  // CSR pattern: sorted (row, col), duplicates merged (createCsr, linalg.h:281-411).
+  std::vector<int64_t> keys;
+  keys.reserve(t.size());
+  for (auto& x : t) keys.push_back(key(x.row, x.col));
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  T.row_ptr.assign(T.n + 1, 0);
+  T.col.resize(keys.size());
+  std::unordered_map<int64_t, int> pos;
+  pos.reserve(keys.size() * 2);
+  for (size_t k = 0; k < keys.size(); ++k) {
+    int r = int(keys[k] >> 32);
+    T.row_ptr[r + 1]++;
+    T.col[k] = int(uint32_t(keys[k]));
+    pos[keys[k]] = (int)k;
+  }
+  for (int i = 0; i < T.n; ++i) T.row_ptr[i + 1] += T.row_ptr[i];
+  T.slot_csr.resize(t.size());
+  for (size_t k = 0; k < t.size(); ++k) T.slot_csr[k] = pos[key(t[k].row, t[k].col)];
+}
+
+// Factor graph of FactorGraph::fromTensorizedBlock: one factor per device over
+// its non-ground terminals; voltage sources add a branch-current variable whose
+// id starts at the node count (so the first one shares its id with node n).
+void ordering(Topology& T) {
+  std::vector<std::vector<uint32_t>> factors;
+  std::set<uint32_t> volt;
+  uint32_t bid = (uint32_t)T.n, nbranch = 0;
+  auto add = [&](std::initializer_list<int> nodes, bool branch) {
+    std::vector<uint32_t> f;
+    for (int x : nodes)
+      if (x > 0) {
+        f.push_back((uint32_t)x);
+        volt.insert((uint32_t)x);
+      }
+    if (branch) {
+      f.push_back(bid++);
+      ++nbranch;
+    }
+    factors.push_back(std::move(f));
+  };
+  for (auto& d : T.dio) add({d.a, d.c}, false);
+  for (auto& m : T.mos) add({m.d, m.g, m.s, m.b}, false);
+  for (auto& r : T.res) add({r.n1, r.n2}, false);
+  for (auto& c : T.cap) add({c.n1, c.n2}, false);
+  for (auto& v : T.vs) add({v.pos, v.neg}, true);
+  for (auto& c : T.isrc) add({c.n1, c.n2}, false);
+  std::vector<uint32_t> vars(volt.begin(), volt.end());
+  for (uint32_t k = 0; k < nbranch; ++k) vars.push_back((uint32_t)T.n + k);
+  MinFillResult mf = min_fill(factors, vars);
+  T.raw_order = mf.ordering;
+  T.treewidth = mf.treewidth;
+  // Translation to a 0-based permutation of the unknowns: ids 1..n kept in
+  // order of first appearance, branch ids and repeats dropped; unknowns no
+  // device touches go last.
+  std::vector<char> seen(T.n + 1, 0);
+  T.perm.clear();
+  for (uint32_t id : mf.ordering)
+    if (id >= 1 && id <= (uint32_t)T.n && !seen[id]) {
+      seen[id] = 1;
+      T.perm.push_back((int)id - 1);
+    }
+  for (int i = 1; i <= T.n; ++i)
+    if (!seen[i]) T.perm.push_back(i - 1);
+  T.iperm.assign(T.n, 0);
+  for (int i = 0; i < T.n; ++i) T.iperm[T.perm[i]] = i;
+}
+
+// symbolicFactorize (math/sparse_lu.cpp:14-128): eliminate in permuted order
+// on the undirected CSR graph; row k of U (and column k of L) holds the
+// permuted indices of the neighbours of the k-th eliminated unknown.
+void symbolic(Topology& T, std::vector<std::vector<int>>& urow) {
+  const int n = T.n;
+  std::vector<std::unordered_set<int>> adj(n);
+  for (int r = 0; r < n; ++r)
+    for (int k = T.row_ptr[r]; k < T.row_ptr[r + 1]; ++k) {
+      int c = T.col[k];
+      if (c != r) {
+        adj[r].insert(c);
+        adj[c].insert(r);
+      }
+    }
+  urow.assign(n, {});
+  int fill = 0;
+  std::vector<int> nb;
+  for (int step = 0; step < n; ++step) {
+    int v = T.perm[step];
+    nb.assign(adj[v].begin(), adj[v].end());
+    std::sort(nb.begin(), nb.end());
+    auto& ur = urow[step];
+    for (int u : nb) ur.push_back(T.iperm[u]);
+    std::sort(ur.begin(), ur.end());
+    for (size_t i = 0; i < nb.size(); ++i)
+      for (size_t j = i + 1; j < nb.size(); ++j)
+        if (adj[nb[i]].insert(nb[j]).second) {
+          adj[nb[j]].insert(nb[i]);
+          ++fill;
+        }
+    for (int u : nb) adj[u].erase(v);
+    adj[v].clear();
+  }
+  T.fill_in = fill;
+  // filled CSR (symmetric structure): row i = {k < i : i in urow[k]} + {i} + urow[i]
+  std::vector<std::vector<int>> lcols(n);
+  for (int k = 0; k < n; ++k)
+    for (int j : urow[k]) lcols[j].push_back(k);
+  T.f_row_ptr.assign(n + 1, 0);
+  T.f_col.clear();
+  T.f_diag.assign(n, -1);
+  for (int i = 0; i < n; ++i) {
+    T.f_row_ptr[i] = (int)T.f_col.size();
+    for (int k : lcols[i]) T.f_col.push_back(k);  // ascending by construction
+    T.f_diag[i] = (int)T.f_col.size();
+    T.f_col.push_back(i);
+    for (int j : urow[i]) T.f_col.push_back(j);
+  }
+  T.f_row_ptr[n] = (int)T.f_col.size();
+}
+
+void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
+  const int n = T.n, nf = T.nnz_filled();
+  std::unordered_map<int64_t, int> fpos;
+  fpos.reserve((size_t)nf * 2);
+  for (int i = 0; i < n; ++i)
+    for (int k = T.f_row_ptr[i]; k < T.f_row_ptr[i + 1]; ++k) fpos[key(i, T.f_col[k])] = k;
+  auto fp = [&](int pr, int pc) {
+    auto it = fpos.find(key(pr, pc));
+    require(it != fpos.end(), "filled pattern misses a position");
+    return it->second;
+  };
+  for (auto& x : T.trip) x.f = fp(T.iperm[x.row], T.iperm[x.col]);
+
+  // Evaluation gather tables, summation order = triplet order.
+  std::vector<std::vector<int>> jt(nf), jc(nf);
+  T.jlin_dc.assign(nf, 0.0);
+  for (auto& x : T.trip) {
+    switch (x.kind) {
+      case SS_RES: {
+        double g = 1.0 / T.res[x.idx].val;
+        T.jlin_dc[x.f] += x.neg ? -g : g;
+        break;
+      }
+      case SS_VS:
+        T.jlin_dc[x.f] += x.neg ? -1.0e3 : 1.0e3;
+        break;
+      case SS_CAP:
+        jc[x.f].push_back(term(0, x.idx, x.neg));
+        break;
+      case SS_DIO:
+        jt[x.f].push_back(term(JK_DIO_G, x.idx, x.neg));
+        break;
+      case SS_MOS_GDS:
+        jt[x.f].push_back(term(JK_MOS_GDS, x.idx, x.neg));
+        break;
+      case SS_MOS_GM:
+        jt[x.f].push_back(term(JK_MOS_GM, x.idx, x.neg));
+        break;
+      default:
+        break;  // gmb (always 0 in the level-1 kernel) and gmin are not gathered
+    }
+  }
+  auto flatten = [](const std::vector<std::vector<int>>& v, std::vector<int>& off,
+                    std::vector<int>& code) {
+    off.assign(v.size() + 1, 0);
+    code.clear();
+    for (size_t i = 0; i < v.size(); ++i) {
+      off[i] = (int)code.size();
+      code.insert(code.end(), v[i].begin(), v[i].end());
+    }
+    off[v.size()] = (int)code.size();
+  };
+  flatten(jt, T.jt_off, T.jt_code);
+  flatten(jc, T.jcap_off, T.jcap_code);
+
+  // KCL gather tables per permuted node: currents leaving the node.
+  std::vector<std::vector<int>> ft(n);
+  auto two = [&](int n1, int n2, int kind, int idx) {
+    if (n1 > 0) ft[T.iperm[n1 - 1]].push_back(term(kind, idx, false));
+    if (n2 > 0) ft[T.iperm[n2 - 1]].push_back(term(kind, idx, true));
+  };
+  for (size_t i = 0; i < T.res.size(); ++i) two(T.res[i].n1, T.res[i].n2, FK_RES, (int)i);
+  for (size_t i = 0; i < T.vs.size(); ++i) two(T.vs[i].pos, T.vs[i].neg, FK_VS, (int)i);
+  for (size_t i = 0; i < T.isrc.size(); ++i) two(T.isrc[i].n1, T.isrc[i].n2, FK_IS, (int)i);
+  for (size_t i = 0; i < T.cap.size(); ++i) two(T.cap[i].n1, T.cap[i].n2, FK_CAP, (int)i);
+  for (size_t i = 0; i < T.dio.size(); ++i) two(T.dio[i].a, T.dio[i].c, FK_DIO, (int)i);
+  for (size_t i = 0; i < T.mos.size(); ++i) two(T.mos[i].d, T.mos[i].s, FK_MOS, (int)i);
+  flatten(ft, T.ft_off, T.ft_code);
+
+  // LU program.
+  T.lu_hdr.assign(4 * (size_t)n, 0);
+  T.lu_data.clear();
+  T.lu_ops = 0;
+  T.max_d = 0;
+  for (int k = 0; k < n; ++k) {
+    const auto& nb = urow[k];
+    int d = (int)nb.size();
+    T.max_d = std::max(T.max_d, d);
+    T.lu_hdr[4 * k + 0] = (int)T.lu_data.size();
+    T.lu_hdr[4 * k + 1] = d;
+    T.lu_hdr[4 * k + 2] = T.f_diag[k];
+    for (int a = 0; a < d; ++a) T.lu_data.push_back(nb[a]);
+    for (int a = 0; a < d; ++a) T.lu_data.push_back(fp(nb[a], k));
+    for (int b = 0; b < d; ++b) T.lu_data.push_back(fp(k, nb[b]));
+    for (int a = 0; a < d; ++a)
+      for (int b = 0; b < d; ++b) T.lu_data.push_back(fp(nb[a], nb[b]));
+    T.lu_ops += d + d * d;
+  }
+
+  auto pn = [&](int node) { return node > 0 ? T.iperm[node - 1] : -1; };
+  for (auto& m : T.mos) {
+    T.mos_term.push_back(pn(m.d));
+    T.mos_term.push_back(pn(m.g));
+    T.mos_term.push_back(pn(m.s));
+    T.mos_term.push_back(pn(m.b));
+  }
+  for (auto& d : T.dio) {
+    T.dio_term.push_back(pn(d.a));
+    T.dio_term.push_back(pn(d.c));
+  }
+  for (auto& r : T.res) { T.res_term.push_back(pn(r.n1)); T.res_term.push_back(pn(r.n2)); }
+  for (auto& c : T.cap) { T.cap_term.push_back(pn(c.n1)); T.cap_term.push_back(pn(c.n2)); }
+  for (auto& v : T.vs) { T.vs_term.push_back(pn(v.pos)); T.vs_term.push_back(pn(v.neg)); }
+  for (auto& c : T.isrc) { T.is_term.push_back(pn(c.n1)); T.is_term.push_back(pn(c.n2)); }
+}
+
+}  // namespace
+
+// Min-Fill elimination with the reference's choice rule: at every step the
+// vertex with the fewest missing neighbour pairs, ties to the smallest id
+// (treewidth_analyzer.cpp:72-102). Instead of rescanning every vertex, fill
+// counts live in an ordered set keyed (fill, id) and only vertices whose
+// neighbourhood changed are updated: the eliminated vertex's neighbours are
+// recounted, and every other vertex adjacent to both ends of a new fill edge
+// loses one missing pair. A variable id listed twice (the reference's branch
+// id that equals the node count) is eliminated twice, the second time as an
+// isolated vertex, which is what the reference's map-keyed adjacency does.
+MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
+                       const std::vector<uint32_t>& variables) {
+  std::unordered_map<uint32_t, int> dense;
+  std::vector<uint32_t> ids;
+  std::vector<int> extra;  // repeated listings per dense vertex
+  for (uint32_t id : variables) {
+    auto it = dense.find(id);
+    if (it == dense.end()) {
+      dense[id] = (int)ids.size();
+      ids.push_back(id);
+      extra.push_back(0);
+    } else {
+      extra[it->second]++;
+    }
+  }
+  const int nv = (int)ids.size();
+  std::vector<std::unordered_set<int>> adj(nv);
+  for (const auto& f : factors)
+    for (size_t i = 0; i < f.size(); ++i)
+      for (size_t j = i + 1; j < f.size(); ++j) {
+        if (f[i] == f[j]) continue;
+        int a = dense.at(f[i]), b = dense.at(f[j]);
+        adj[a].insert(b);
+        adj[b].insert(a);
+      }
+  auto count_fill = [&](int u) {
+    uint32_t c = 0;
+    std::vector<int> nb(adj[u].begin(), adj[u].end());
+    for (size_t i = 0; i < nb.size(); ++i) {
+      const auto& ai = adj[nb[i]];
+      for (size_t j = i + 1; j < nb.size(); ++j)
+        if (!ai.count(nb[j])) ++c;
+    }
+    return c;
+  };
+  std::vector<uint32_t> fill(nv);
+  std::set<std::pair<uint32_t, uint32_t>> pq;  // (fill, id)
+  for (int u = 0; u < nv; ++u) {
+    fill[u] = count_fill(u);
+    pq.insert({fill[u], ids[u]});
+  }
+  std::vector<char> alive(nv, 1);
+  std::vector<int> ghosts(nv, 0);
+  MinFillResult out;
+  out.ordering.reserve(variables.size());
+  uint32_t maxclique = 0;
+  std::vector<int> nb, touched;
+  std::unordered_set<int> nbset;
+  std::unordered_map<int, uint32_t> dec;
+  while (!pq.empty()) {
+    auto top = *pq.begin();
+    pq.erase(pq.begin());
+    int u = dense.at(top.second);
+    out.ordering.push_back(top.second);
+    if (!alive[u]) {  // repeated listing: isolated by now
+      maxclique = std::max<uint32_t>(maxclique, 1);
+      if (--ghosts[u] > 0) pq.insert({0u, ids[u]});
+      continue;
+    }
+    nb.assign(adj[u].begin(), adj[u].end());
+    std::sort(nb.begin(), nb.end());
+    maxclique = std::max<uint32_t>(maxclique, (uint32_t)nb.size() + 1);
+    nbset.clear();
+    nbset.insert(nb.begin(), nb.end());
+    dec.clear();
+    for (size_t i = 0; i < nb.size(); ++i)
+      for (size_t j = i + 1; j < nb.size(); ++j) {
+        int a = nb[i], b = nb[j];
+        if (adj[a].insert(b).second) {
+          adj[b].insert(a);
+          // vertices outside N(u) adjacent to both a and b lose a missing pair
+          const auto& sa = adj[a].size() <= adj[b].size() ? adj[a] : adj[b];
+          const auto& sb = adj[a].size() <= adj[b].size() ? adj[b] : adj[a];
+          for (int w : sa)
+            if (w != a && w != b && w != u && !nbset.count(w) && sb.count(w)) dec[w]++;
+        }
+      }
+    for (int w : nb) adj[w].erase(u);
+    adj[u].clear();
+    alive[u] = 0;
+    for (auto& kv : dec) {
+      int w = kv.first;
+      pq.erase({fill[w], ids[w]});
+      fill[w] -= kv.second;
+      pq.insert({fill[w], ids[w]});
+    }
+    for (int w : nb) {
+      pq.erase({fill[w], ids[w]});
+      fill[w] = count_fill(w);
+      pq.insert({fill[w], ids[w]});
+    }
+    if (extra[u] > 0) {
+      ghosts[u] = extra[u];
+      pq.insert({0u, ids[u]});
+      extra[u] = 0;
+    }
+  }
+  out.treewidth = maxclique > 0 ? (int)maxclique - 1 : 0;
+  return out;
+}
+
+Topology build_topology(const karam_netlist* nl) {
+  Topology T;
+  tensorize(nl, T);
+  stamps(T);
+  ordering(T);
+  std::vector<std::vector<int>> urow;
+  symbolic(T, urow);
+  device_tables(T, urow);
+  return T;
+}
+
+}  // namespace karam

@@ -1,0 +1,104 @@
+// topology.hpp -- host symbolic layer of the NR inner loop (run once per topology).
+//
+// Produces everything the device kernels need from a karam_netlist:
+//   * the SoA device tables in tensorizeNetlist order (tensors/physics_tensors.cpp:305-493);
+//   * the stamp triplets in stampSoABlock order (physics/circuitsim.h:2413-2666,
+//     + addDiagonalConditioning :2857) and the CSR pattern/slot map of
+//     MatrixConstructor::buildPattern / CachedCsrPattern::indexOf (math/linalg.h:82-107, 281-465);
+//   * the Min-Fill ordering of FactorGraph + TreewidthAnalyzer
+//     (infrastructure/factor_graph.cpp:9-162, treewidth_analyzer.cpp:14-141), computed by an
+//     incremental priority-queue variant with the same (fill, id) tie-break, and its
+//     translation to a permutation of the unknowns;
+//   * the filled L+U pattern of symbolicFactorize (math/sparse_lu.cpp:14-128);
+//   * the gather tables of the evaluation kernel and the LU program of the factor kernel,
+//     all expressed in the permuted index space the device works in.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/karam.h"
+
+namespace karam {
+
+// Term codes of the gather tables: bit 31 = negative sign, bits 24..30 = kind,
+// bits 0..23 = device index.
+enum JKind { JK_MOS_GDS = 0, JK_MOS_GM = 1, JK_DIO_G = 2 };
+enum FKind { FK_RES = 0, FK_VS = 1, FK_IS = 2, FK_CAP = 3, FK_DIO = 4, FK_MOS = 5 };
+inline int32_t term(int kind, int idx, bool neg) {
+  return (neg ? int32_t(0x80000000u) : 0) | (kind << 24) | (idx & 0xFFFFFF);
+}
+
+struct Triplet {
+  int row, col;     // 0-based original node indices
+  int f;            // position in the filled, permuted pattern
+  int kind;         // stamp source (see StampSrc)
+  int idx;          // device index within its table
+  bool neg;
+};
+enum StampSrc { SS_RES, SS_VS, SS_CAP, SS_DIO, SS_MOS_GDS, SS_MOS_GM, SS_MOS_GMB, SS_GMIN };
+
+struct Topology {
+  int n = 0;  // unknowns
+  double temp_k = 300.15;
+
+  // ---- SoA device tables (tensorised order); node ids 1-based, 0 = ground ----
+  struct Mos { int d, g, s, b; double wl, w, l, kp_card, vto_card, lam; bool pmos; };
+  struct Dio { int a, c; double is, n, vt; };
+  struct Two { int n1, n2; double val; };
+  struct Vs { int pos, neg, kind; double dc; double pulse[7]; };
+  std::vector<Mos> mos;
+  std::vector<Dio> dio;
+  std::vector<Two> res, cap, isrc;
+  std::vector<Vs> vs;
+  std::vector<int> mos_order, dio_order;   // soa index -> netlist index
+  std::vector<int> seed_anodes;            // netlist-order diode anodes (seedInitialGuess)
+
+  // ---- CSR pattern (original order, transient pattern incl. gmin diagonal) ----
+  std::vector<int> row_ptr, col;
+  std::vector<Triplet> trip;  // stamp slots in reference order
+  std::vector<int> slot_csr;  // slot -> CSR index
+
+  // ---- ordering ----
+  std::vector<uint32_t> raw_order;
+  int treewidth = 0;
+  std::vector<int> perm, iperm;  // perm[new] = old (0-based), iperm[old] = new
+
+  // ---- filled pattern (permuted) ----
+  std::vector<int> f_row_ptr, f_col;
+  int fill_in = 0;
+  std::vector<int> f_diag;  // filled position of (k, k)
+
+  // ---- gather tables (permuted space) ----
+  std::vector<int> jt_off, jt_code;          // per filled position
+  std::vector<double> jlin_dc;               // R + V stamps per filled position
+  std::vector<int> jcap_off, jcap_code;      // capacitor stamps per filled position (G = C * scale)
+  std::vector<int> ft_off, ft_code;          // per permuted node
+
+  // ---- LU program: per pivot (off, d, dpos); data = nbr[d] lpos[d] upos[d] tpos[d*d] ----
+  std::vector<int> lu_hdr;   // 4 ints per pivot
+  std::vector<int> lu_data;
+  int lu_ops = 0;
+  int max_d = 0;
+
+  // ---- device tables in permuted node indices (-1 = ground) ----
+  std::vector<int> mos_term;  // 4 per MOSFET: d g s b
+  std::vector<int> dio_term;  // 2 per diode
+  std::vector<int> res_term, cap_term, vs_term, is_term;
+
+  int nnz() const { return (int)col.size(); }
+  int nnz_filled() const { return (int)f_col.size(); }
+};
+
+// Builds the full topology; throws std::runtime_error with a message on bad input.
+Topology build_topology(const karam_netlist* nl);
+
+// Min-Fill on an explicit factor list (exposed for tests of the ordering).
+struct MinFillResult {
+  std::vector<uint32_t> ordering;
+  int treewidth = 0;
+};
+MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
+                       const std::vector<uint32_t>& variables);
+
+}  // namespace karam

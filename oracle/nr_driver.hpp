@@ -7,10 +7,13 @@
 // of CircuitSim::stepTransient (circuitsim_solver.cpp:600-635) with these
 // documented deviations:
 //   * KCL residual. calculatePhysicalResiduals (physics/circuitsim.h:1250-1671)
-//     hardcodes MOSFET KP/VTO/LAMBDA by model-name substring, so it disagrees
-//     with the stamps whenever model cards are used and the reference never
-//     converges. The oracle uses F(v) = J(v) v - rhs(v) from the same stamps
-//     (without the gmin diagonal), i.e. the KCL sum of the stamped device laws.
+//     sums device currents per node but hardcodes MOSFET KP/VTO/LAMBDA by
+//     model-name substring, so it disagrees with the stamps whenever model
+//     cards are used and the reference never converges. The oracle keeps its
+//     structure (a KCL sum of device currents, no gmin) with the currents of
+//     the SoA kernels at the tensorised parameters, so it is exactly J(v) v -
+//     rhs(v) of the same stamps in real arithmetic, without the cancellation of
+//     forming J v and rhs separately (1e3 S source rows).
 //   * Transient. The reference re-tensorises every step (which zeroes the SoA
 //     capacitor history), has no PULSE in the SoA path and picks dt adaptively.
 //     The oracle runs fixed steps with the companions of
@@ -161,6 +164,8 @@ inline bool polish_done(const oracle_opts& o, const std::vector<double>& vn,
 //   void stamp(const std::vector<double>& v, double h, int method,
 //              const std::vector<double>& cvp, const std::vector<double>& cip,
 //              double t, std::vector<double>& vals, std::vector<double>& rhs);
+//   void kcl(v, h, method, cvp, cip, t, F): node currents at the point of the
+//              last stamp() call (device kernel outputs of that call);
 //   bool solve(const std::vector<double>& vals_gmin, const std::vector<double>& rhs,
 //              std::vector<double>& x, int solver);
 template <class B>
@@ -175,10 +180,19 @@ struct Driver {
     for (int i = 0; i < b.n; ++i) v[b.pat.diag[i]] += gmin;
   }
 
-  // KCL residual at x (DC: h = 0).
+  std::vector<double> fvec;
+
+  // KCL residual at x (DC: h = 0): currents leaving every node through the
+  // devices, evaluated by the backend from the device-kernel outputs at x.
   double kcl_at(const std::vector<double>& x, double h, int method, double t, bool* nf) {
     b.stamp(x, h, method, cvp, cip, t, tmp_vals, tmp_rhs);
-    return residual_max(b.pat, tmp_vals, x, tmp_rhs, nf);
+    b.kcl(x, h, method, cvp, cip, t, fvec);
+    double m = 0.0;
+    for (double f : fvec) {
+      if (!std::isfinite(f)) *nf = true;
+      m = std::max(m, std::fabs(f));
+    }
+    return m;
   }
 
   // seedInitialGuess, circuitsim_solver.cpp:32-116 (no BJTs on this path).
@@ -299,12 +313,30 @@ struct Driver {
   }
 
   // Polishing Newton steps at the final gmin (DC: h = 0; transient: companions).
+  // Each step is the reference's linear solve applied to the residual
+  // (dx = J^-1 (rhs - J v), v += dx), i.e. iterative refinement of the
+  // reference solution, so the fixed point is set by the FP64 residual rather
+  // than by the rounding of a solve for v itself.
+  bool refine_step(const std::vector<double>& v, double h, int method, double t,
+                   std::vector<double>& x) {
+    b.stamp(v, h, method, cvp, cip, t, vals, rhs);
+    b.kcl(v, h, method, cvp, cip, t, fvec);
+    add_gmin(vals, 1e-12);
+    std::vector<double> r(b.n);
+    for (int i = 0; i < b.n; ++i) r[i] = -(fvec[i] + 1e-12 * v[i]);
+    std::vector<double> dx;
+    if (!b.solve(vals, r, dx, o.linear_solver)) return false;
+    x.resize(b.n);
+    for (int i = 0; i < b.n; ++i) x[i] = v[i] + dx[i];
+    return true;
+  }
+
   void polish(std::vector<double>& v, double h, int method, double t, oracle_stats* st) {
     if (o.polish_max <= 0) return;
     std::vector<double> x(b.n);
     double prev = -1.0;
     for (int p = 0; p < o.polish_max; ++p) {
-      if (!newton_point(v, 1e-12, h, method, t, x)) break;
+      if (!refine_step(v, h, method, t, x)) break;
       double dv = 0.0;
       bool ok = polish_done(o, x, v, &dv);
       v = x;
@@ -352,7 +384,36 @@ struct Driver {
     return 0;
   }
 
-  // Fixed-step transient (see header comment).
+  // NR of one transient (sub-)step from guess at time t with step h.
+  // Returns the number of iterations used; conv tells whether it converged.
+  int tran_nr(std::vector<double>& guess, double h, int method, double t, bool* conv,
+              oracle_stats* st) {
+    std::vector<double> x(b.n);
+    *conv = false;
+    int it = 0;
+    for (; it < o.max_nr_iter; ++it) {
+      if (!newton_point(guess, 1e-12, h, method, t, x)) {
+        st->singular = 1;
+        return it + 1;
+      }
+      bool nf = false;
+      double kcl = kcl_at(x, h, method, t, &nf);
+      if (check_convergence(o, x, guess, kcl, o.kcl_tol)) {
+        guess = x;
+        *conv = true;
+        return it + 1;
+      }
+      guess = x;
+    }
+    return it + 1;
+  }
+
+  // Fixed-step transient (see header comment). A step whose NR does not
+  // converge within max_nr_iter is retried from the last accepted time point
+  // with half the step, as the attempt loop of CircuitSim::stepTransient does
+  // (circuitsim_solver.cpp:587-660, MAX_ATTEMPTS = 4, i.e. three halvings;
+  // o.max_halvings sets the count); the halved sub-steps then complete the
+  // step, so results stay on the output grid.
   int transient(const std::vector<double>& v_start, double dt, int n_steps, int method,
                 const int32_t* wave_nodes, int n_wave, double* wave_out,
                 std::vector<double>& v, oracle_stats* st) {
@@ -365,53 +426,48 @@ struct Driver {
       return node > 0 ? vv[node - 1] : 0.0;
     };
     for (size_t i = 0; i < nc; ++i) cvp[i] = vnode(v, b.cap_n1[i]) - vnode(v, b.cap_n2[i]);
-    std::vector<double> x(b.n), guess;
+    std::vector<double> guess;
     st->converged = 1;
-    for (int s = 1; s <= n_steps; ++s) {
-      double t = s * dt;
-      guess = v;
-      bool conv = false;
-      int it = 0;
-      for (; it < o.max_nr_iter; ++it) {
-        if (!newton_point(guess, 1e-12, dt, method, t, x)) {
-          st->singular = 1;
-          break;
+    const int H = o.max_halvings, units = 1 << H;
+    const double unit = dt / units;
+    for (int s = 1; s <= n_steps && st->converged; ++s) {
+      int depth = 0, frac = 0;
+      while (frac < units) {
+        const int size = units >> depth;
+        const double h = dt * size / units;
+        const double t = (double)((s - 1) * units + frac + size) * unit;
+        guess = v;
+        bool conv = false;
+        int its = tran_nr(guess, h, method, t, &conv, st);
+        st->iterations += its;
+        st->max_step_iters = std::max(st->max_step_iters, its);
+        if (!conv) {
+          if (st->singular || depth == H) {
+            st->converged = 0;
+            v = guess;
+            break;
+          }
+          depth++;
+          continue;
         }
-        bool nf = false;
-        double kcl = kcl_at(x, dt, method, t, &nf);
-        if (check_convergence(o, x, guess, kcl, o.kcl_tol)) {
-          guess = x;
-          conv = true;
-          break;
+        polish(guess, h, method, t, st);
+        // capacitor history, circuitsim_solver.cpp:669-699
+        for (size_t i = 0; i < nc; ++i) {
+          double vc = vnode(guess, b.cap_n1[i]) - vnode(guess, b.cap_n2[i]);
+          double C = b.cap_c[i];
+          double ic = (method == KARAM_TRAN_TRAP) ? (2.0 * C / h) * (vc - cvp[i]) - cip[i]
+                                                  : (C / h) * (vc - cvp[i]);
+          cvp[i] = vc;
+          cip[i] = ic;
         }
-        guess = x;
-      }
-      st->iterations += it + 1;
-      st->max_step_iters = std::max(st->max_step_iters, it + 1);
-      if (!conv) {
-        st->converged = 0;
         v = guess;
-        break;
+        frac += size;
       }
-      polish(guess, dt, method, t, st);
-      // capacitor history, circuitsim_solver.cpp:669-699
-      for (size_t i = 0; i < nc; ++i) {
-        double vc = vnode(guess, b.cap_n1[i]) - vnode(guess, b.cap_n2[i]);
-        double C = b.cap_c[i];
-        double ic = (method == KARAM_TRAN_TRAP) ? (2.0 * C / dt) * (vc - cvp[i]) - cip[i]
-                                                : (C / dt) * (vc - cvp[i]);
-        cvp[i] = vc;
-        cip[i] = ic;
-      }
-      v = guess;
-      if (wave_out && n_wave > 0)
+      if (st->converged && wave_out && n_wave > 0)
         for (int k = 0; k < n_wave; ++k)
           wave_out[(size_t)(s - 1) * n_wave + k] = vnode(v, wave_nodes[k]);
     }
-    if (st->converged) {
-      // residual of the last step's companions, evaluated before the update
-      st->residual = 0.0;
-    }
+    st->residual = 0.0;
     return 0;
   }
 };

@@ -37,6 +37,8 @@ typedef struct oracle_opts {
   int32_t linear_solver; /* ORACLE_LS_* */
   int32_t seeded;        /* start from v0 at the final GMIN step */
   int32_t seed_max_iter; /* fall back to full GMIN stepping after this many */
+  int32_t max_halvings;  /* transient step halvings after NR failure (3 = the
+                            reference's 4 attempts, circuitsim_solver.cpp:583) */
 } oracle_opts;
 
 typedef struct oracle_stats {

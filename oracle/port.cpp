@@ -594,6 +594,52 @@ struct PortBackend {
     rhs = st.rhs;
   }
 
+  // Currents leaving every node at v (the stamp() just run at v left the
+  // device-kernel outputs in ev): R (v1 - v2)/R, Norton sources
+  // 1e3 ((v+ - v-) - V), current sources, capacitor companions, diodes, MOSFETs.
+  void kcl(const std::vector<double>& v, double h, int method, const std::vector<double>& cvp,
+           const std::vector<double>& cip, double t, std::vector<double>& F) {
+    F.assign(n, 0.0);
+    auto vn = [&](int node) { return node > 0 ? v[node - 1] : 0.0; };
+    auto add = [&](int node, double cur) {
+      if (node > 0) F[node - 1] += cur;
+    };
+    const bool tran = h > 0.0;
+    for (const Two& r : soa.res) {
+      double i = (vn(r.n1) - vn(r.n2)) / r.val;
+      add(r.n1, i);
+      add(r.n2, -i);
+    }
+    for (size_t k = 0; k < soa.vs_pos.size(); ++k) {
+      double i = 1.0e3 * ((vn(soa.vs_pos[k]) - vn(soa.vs_neg[k])) - src.value_at((int)k, t, tran));
+      add(soa.vs_pos[k], i);
+      add(soa.vs_neg[k], -i);
+    }
+    for (const Two& c : soa.isrc) {
+      add(c.n1, c.val);
+      add(c.n2, -c.val);
+    }
+    if (tran) {
+      const double heff = method == KARAM_TRAN_TRAP ? h : 2.0 * h;
+      for (size_t k = 0; k < soa.cap.size(); ++k) {
+        const Two& c = soa.cap[k];
+        double g = (2.0 * c.val) / heff;
+        double i = g * ((vn(c.n1) - vn(c.n2)) - cvp[k]);
+        if (method == KARAM_TRAN_TRAP) i -= cip[k];
+        add(c.n1, i);
+        add(c.n2, -i);
+      }
+    }
+    for (size_t k = 0; k < soa.dio.size(); ++k) {
+      add(soa.dio[k].a, ev.id[k]);
+      add(soa.dio[k].c, -ev.id[k]);
+    }
+    for (size_t k = 0; k < soa.mos.size(); ++k) {
+      add(soa.mos[k].d, ev.ids[k]);
+      add(soa.mos[k].s, -ev.ids[k]);
+    }
+  }
+
   void ensure_symbolic() {
     if (have_sym) return;
     MinFill mf = min_fill(soa, n);
@@ -658,6 +704,7 @@ void oracle_default_opts(oracle_opts* o) {
   o->linear_solver = ORACLE_LS_DENSE;
   o->seeded = 0;
   o->seed_max_iter = 10;
+  o->max_halvings = 3;
 }
 
 int oracle_tensorize(const karam_netlist* nl, int32_t* mos_order, int32_t* dio_order) {

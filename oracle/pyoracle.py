@@ -30,7 +30,8 @@ class OracleOpts(C.Structure):
                 ("kcl_shortcut", C.c_double), ("kcl_tol", C.c_double),
                 ("polish_max", C.c_int32), ("polish_rel", C.c_double),
                 ("polish_abs", C.c_double), ("linear_solver", C.c_int32),
-                ("seeded", C.c_int32), ("seed_max_iter", C.c_int32)]
+                ("seeded", C.c_int32), ("seed_max_iter", C.c_int32),
+                ("max_halvings", C.c_int32)]
 
 
 class OracleStats(C.Structure):

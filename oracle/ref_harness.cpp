@@ -208,6 +208,56 @@ struct RefBackend {
     rhs = sim->rhsVector;
   }
 
+  // Currents leaving every node at v, with the device currents the
+  // reference kernels left in the SoA tensors during the last stamp() at v.
+  void kcl(const std::vector<double>& v, double h, int method, const std::vector<double>& cvp,
+           const std::vector<double>& cip, double t, std::vector<double>& F) {
+    F.assign(n, 0.0);
+    auto vn = [&](int node) { return node > 0 ? v[node - 1] : 0.0; };
+    auto add = [&](int node, double cur) {
+      if (node > 0) F[node - 1] += cur;
+    };
+    const bool tran = h > 0.0;
+    const auto& R = soa.resistors;
+    for (size_t k = 0; k < R.size(); ++k) {
+      double i = (vn(R.nodes1[k]) - vn(R.nodes2[k])) / R.R[k];
+      add(R.nodes1[k], i);
+      add(R.nodes2[k], -i);
+    }
+    const auto& V = soa.voltageSources;
+    for (size_t k = 0; k < V.size(); ++k) {
+      double i = 1.0e3 * ((vn(V.nodesPos[k]) - vn(V.nodesNeg[k])) - src.value_at((int)k, t, tran));
+      add(V.nodesPos[k], i);
+      add(V.nodesNeg[k], -i);
+    }
+    const auto& I = soa.currentSources;
+    for (size_t k = 0; k < I.size(); ++k) {
+      add(I.nodesPos[k], I.currents[k]);
+      add(I.nodesNeg[k], -I.currents[k]);
+    }
+    if (tran) {
+      const double heff = method == KARAM_TRAN_TRAP ? h : 2.0 * h;
+      const auto& Cp = soa.capacitors;
+      for (size_t k = 0; k < Cp.size(); ++k) {
+        double g = (2.0 * Cp.C[k]) / heff;
+        double i = g * ((vn(Cp.plates1[k]) - vn(Cp.plates2[k])) - cvp[k]);
+        if (method == KARAM_TRAN_TRAP) i -= cip[k];
+        add(Cp.plates1[k], i);
+        add(Cp.plates2[k], -i);
+      }
+    }
+    const auto& D = soa.diodes;
+    for (size_t k = 0; k < D.size(); ++k) {
+      add(D.node_a[k], D.i_d[k]);
+      add(D.node_c[k], -D.i_d[k]);
+    }
+    const auto& M = soa.mosfets;
+    for (size_t k = 0; k < M.size(); ++k) {
+      add(M.drains[k], M.ids[k]);
+      add(M.sources[k], -M.ids[k]);
+    }
+  }
+
   Csr_matrix as_csr(const std::vector<double>& vals) const {
     Csr_matrix m;
     m.rows = n;
@@ -295,6 +345,7 @@ void oracle_default_opts(oracle_opts* o) {
   o->linear_solver = ORACLE_LS_DENSE;
   o->seeded = 0;
   o->seed_max_iter = 10;
+  o->max_halvings = 3;
 }
 
 int oracle_tensorize(const karam_netlist* nl, int32_t* mos_order, int32_t* dio_order) {
