@@ -1,0 +1,457 @@
+#!/usr/bin/env python
+"""Headline benchmark: converged NR solves/s of the Monte-Carlo DC + transient job.
+
+Workload (one "step"): 4096 seeded Monte-Carlo instances of a 256-stage CMOS
+inverter chain with 64 diode clamps (IS 1e-14 A, N 1, RS 10 ohm) and 1 fF node
+caps (n = 322 unknowns); per-device VTO ~ N(card, 30 mV), KP ~ N(card, 5 %).
+Every instance solves its DC operating point, then a 200-step backward-Euler
+transient (1 ps) of a 0 -> 1.8 V input ramp. A "solve" is one converged
+nonlinear solve of one instance at one time point (DC point or transient step),
+so a fully converged step is 4096 * 201 solves. Synthetic inputs, fixed seeds.
+
+value  : mixed precision (FP32 Jacobian + FP32 LU, FP64 residual/refinement),
+         inputs resident in HBM, device time from CUDA events around each job,
+         L2 flushed (512 MiB write) between timed steps.
+e2e    : the same job through the C ABI with host buffers (karam_run_mc: H2D of
+         the per-instance parameters, D2H of voltages + stats), wall clock.
+fp64   : the plain FP64 GPU Newton path on the same job, for the comparison
+         the headline metric names.
+--impl reference : the reference CPU implementation of the path (compiled from
+         the reference sources: generic device kernels, stampSoABlock, CSR
+         assembly, solveSparse_LU) on all host threads, a bounded sample of
+         instances per step.
+
+Multi-GPU (torchrun): every rank solves its own batch of instances (weak
+scaling, no collective on the data path); timings are reduced with MAX.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STAGES, CLAMPS = 256, 64
+TRAN_STEPS, DT = 200, 1e-12
+POLISH = dict(polish_max=8, polish_rel=1e-11, polish_abs=1e-14)
+MAX_HALVINGS = 6
+METRIC = "solves/sec at <=1e-9 rel err: seeded mixed-precision vs plain FP64 NR, 1xB200"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="karam", choices=["karam", "reference"])
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="instances in the CPU-baseline sample (0 = sized to ~15 s)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, want_gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.td = td
+            self.torch = torch
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64,
+                              device="cuda" if self.torch.cuda.is_available() else "cpu")
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64,
+                              device="cuda" if self.torch.cuda.is_available() else "cpu")
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.td.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per eval launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "eval_stamp_config2.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_full_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def workload(n_inst, first):
+    from karam_b200 import circuits
+    nl = circuits.config2()
+    inst = circuits.mc_instances(nl, n_inst, first_instance=first)
+    return nl, inst
+
+
+def cpu_sample_run(nl, inst, count, threads):
+    """Reference CPU implementation (oracle/_ref when built, else the restatement)
+    on `count` instances with `threads` host threads; returns (seconds, solves, kind)."""
+    from oracle import pyoracle
+    kind = "reference" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    orc = pyoracle.Oracle("ref" if kind == "reference" else "port")
+    t0 = time.perf_counter()
+    _, st = orc.run_batch(nl, inst, 0, count, dt=DT, n_steps=TRAN_STEPS, n_threads=threads,
+                          linear_solver=pyoracle.LS_SPARSE, max_halvings=MAX_HALVINGS, **POLISH)
+    el = time.perf_counter() - t0
+    solves = sum(TRAN_STEPS + 1 for s in st if s["converged"])
+    return el, solves, kind
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nl, inst = workload(max(threads * 4, 32), 0)
+    count = args.cpu_sample or threads * 2
+    for _ in range(args.warmup):
+        cpu_sample_run(nl, inst, min(count, threads), threads)
+    total_t = total_s = 0.0
+    kind = "reference"
+    for _ in range(args.steps):
+        el, solves, kind = cpu_sample_run(nl, inst, count, threads)
+        total_t += el
+        total_s += solves
+    value = total_s / total_t
+    sample = f"{count} instances x (DC + {TRAN_STEPS} BE steps) per step, {threads} threads"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "MC inverter chain 256 stages + 64 diode clamps, n=322, "
+                               "DC + 200 BE steps of 1 ps", "instances_per_step": count,
+                   "solver": "oracle/_ref: reference sources, solveSparse_LU"
+                   if kind == "reference" else "oracle port (restatement)"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def eval_bytes(info, mixed, method_trap=False):
+    """Algorithmic bytes one evaluation + stamping of one instance moves:
+    per-instance KP/VTO (FP32), the voltages read, the Jacobian values
+    written (CSR entries, FP32 or FP64), the KCL residual and its maximum
+    written, the state record read, and in transient the capacitor history."""
+    n, nnz, nm, nc = info["n"], info["nnz"], info["n_mos"], info["n_cap"]
+    base = 8 * nm + 8 * n + (4 if mixed else 8) * nnz + 8 * n + 8 + 16
+    tran = base + 8 * nc * (2 if method_trap else 1)
+    return base, tran
+
+
+def run_karam(args, dist):
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+
+    ni = args.instances
+    nl, inst = workload(ni, dist.rank * ni)
+    ctx = K.Context(dist.local)
+    prob = K.Problem(ctx, nl, max_instances=ni)
+    prob.set_instances(inst)
+    info = prob.info
+
+    flush = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32,
+                                device=f"cuda:{dist.local}")
+    except Exception:
+        flush = None
+
+    def l2_flush():
+        if flush is not None:
+            flush.zero_()
+            import torch
+            torch.cuda.synchronize()
+
+    def job(opts):
+        prob.run_mc_device(DT, TRAN_STEPS, A.TRAN_BE, opts)
+        t = prob.timing()
+        _, st = prob.read_results()
+        conv = sum(1 for s in st if s["status"] == A.ST_CONVERGED)
+        return t, conv, st
+
+    mixed = K.options(precision=A.PREC_MIXED, max_halvings=MAX_HALVINGS, **POLISH)
+    fp64 = K.options(precision=A.PREC_FP64, max_halvings=MAX_HALVINGS, **POLISH)
+
+    for _ in range(args.warmup):
+        l2_flush()
+        job(mixed)
+
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    clocks.start()
+    tot_ms = 0.0
+    solves = 0
+    eval_ms = 0.0
+    evals_dc = evals_tran = 0
+    launches = 0
+    lu_ms = 0.0
+    rescues = 0
+    conv_min = ni
+    for _ in range(args.steps):
+        l2_flush()
+        t, conv, st = job(mixed)
+        tot_ms += t["job_ms"]
+        solves += conv * (TRAN_STEPS + 1)
+        eval_ms += t["eval_ms"]
+        lu_ms += t["lu_ms"]
+        evals_dc += t["evals_dc"]
+        evals_tran += t["evals_tran"]
+        rescues += t["rescues"]
+        launches += (t["eval_launches"] + t["lu_launches"] + t["rescue_launches"]
+                     + t["other_launches"])
+        conv_min = min(conv_min, conv)
+    clk = clocks.stop()
+    dist.barrier()
+    v_mixed, st_mixed = prob.read_results()
+    t_max = dist.max(tot_ms)
+    all_solves = dist.sum(solves)
+    value = all_solves / (t_max / 1e3)
+
+    # plain FP64 GPU Newton path, same job and timing rules
+    fp_ms = 0.0
+    fp_solves = 0
+    for _ in range(max(1, args.warmup // 3)):
+        job(fp64)
+    for _ in range(args.steps):
+        l2_flush()
+        t, conv, _ = job(fp64)
+        fp_ms += t["job_ms"]
+        fp_solves += conv * (TRAN_STEPS + 1)
+    v_fp64, _ = prob.read_results()
+    fp_value = dist.sum(fp_solves) / (dist.max(fp_ms) / 1e3)
+
+    # end to end through the C ABI with host buffers
+    h2d = inst.mos_kp.nbytes + inst.mos_vto.nbytes
+    d2h = ni * info["n"] * 8 + ni * A.C.sizeof(A.KaramInstanceStats)
+    e2e_t = 0.0
+    e2e_solves = 0
+    for _ in range(args.steps):
+        l2_flush()
+        dist.barrier()
+        t0 = time.perf_counter()
+        v, st = prob.run_mc(inst, DT, TRAN_STEPS, A.TRAN_BE, mixed)
+        e2e_t += time.perf_counter() - t0
+        e2e_solves += sum(TRAN_STEPS + 1 for s in st if s["status"] == A.ST_CONVERGED)
+    e2e_value = dist.sum(e2e_solves) / dist.max(e2e_t)
+
+    # roofline of the evaluation + stamping kernel
+    b_dc, b_tran = eval_bytes(info, mixed=True)
+    eval_bytes_total = evals_dc * b_dc + evals_tran * b_tran
+    peak, peak_kind = measured_peaks()
+    achieved = eval_bytes_total / (eval_ms / 1e3) / 1e9 if eval_ms > 0 else 0.0
+    full_launch_bytes = ni * b_tran
+    roofline = {
+        "kernel": "k_eval (device evaluation + stamping)", "bound": "hbm",
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "peak_source": peak_kind,
+        "traffic": profiled_traffic(),
+        "algorithmic_bytes_per_full_launch": full_launch_bytes,
+        "time_share": eval_ms / (eval_ms + lu_ms) if eval_ms + lu_ms > 0 else None,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {
+            "workload": "MC inverter chain 256 stages + 64 diode clamps, n=322, nnz=1219; "
+                        "DC + 200 BE steps of 1 ps",
+            "instances_per_gpu": ni, "solves_per_instance": TRAN_STEPS + 1,
+            "precision": "mixed: FP32 Jacobian/LU, FP64 residual + Newton refinement",
+            "seeder": "none",
+            "polish": POLISH, "max_halvings": MAX_HALVINGS,
+            "l2": "flushed (512 MiB write) between timed steps",
+            "converged_fraction": conv_min / ni,
+        },
+        "fp64": {"value": fp_value, "unit": "solves/s",
+                 "speedup_mixed_vs_fp64": value / fp_value if fp_value else None},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": roofline,
+        "gpu_launches": launches,
+        "rescues_per_step": rescues / args.steps,
+        "clocks": clk,
+    }
+
+    if dist.rank == 0 and not args.no_accuracy:
+        line["accuracy"] = accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed)
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        count = args.cpu_sample or threads * 2
+        el, cs, kind = cpu_sample_run(nl, inst, count, threads)
+        line["cpu_baseline"] = {
+            "value": cs / el, "unit": "solves/s", "cores": threads, "kind": kind,
+            "sample": f"{count} instances x (DC + {TRAN_STEPS} BE steps), {threads} threads, "
+                      f"{el:.1f} s"}
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    prob.close()
+    ctx.close()
+
+
+def accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, sample=6):
+    """Max relative error of the final transient voltages against the FP64
+    oracle (fully polished) on a few instances, and mixed vs FP64 GPU paths on
+    every instance."""
+    from karam_b200 import _abi as A
+    from oracle import pyoracle
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    orc = pyoracle.Oracle(kind)
+    idx = [i for i, s in enumerate(st_mixed) if s["status"] == A.ST_CONVERGED][:sample]
+    sub = inst.slice(min(idx), max(idx) + 1) if idx else None
+    worst = 0.0
+    worst_rel = 0.0
+    if idx:
+        v_ref, st = orc.run_batch(nl, sub, 0, sub.n, dt=DT, n_steps=TRAN_STEPS,
+                                  n_threads=os.cpu_count() or 1, linear_solver=pyoracle.LS_SPARSE,
+                                  max_halvings=MAX_HALVINGS, polish_max=8)
+        for i in idx:
+            r = v_ref[i - min(idx)]
+            d = np.abs(v_mixed[i] - r)
+            worst = max(worst, float(np.max(d / (1e-9 * np.abs(r) + 1e-12))))
+            big = np.abs(r) > 1e-3
+            if big.any():
+                worst_rel = max(worst_rel, float(np.max(d[big] / np.abs(r[big]))))
+    both = [i for i, s in enumerate(st_mixed) if s["status"] == A.ST_CONVERGED]
+    d = np.abs(v_mixed[both] - v_fp64[both])
+    diff = float(np.max(d / (1e-9 * np.abs(v_fp64[both]) + 1e-12))) if both else None
+    return {"max_scaled_err_vs_oracle": worst, "max_rel_err_vs_oracle_above_1mV": worst_rel,
+            "oracle": kind, "instances_checked": len(idx),
+            "max_scaled_diff_mixed_vs_fp64": diff,
+            "scaled": "|dv| / (1e-9 |v| + 1e-12 V); <= 1 meets the 1e-9 relative bar"}
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_karam(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -273,10 +273,20 @@ KARAM_API int karam_get_device_order(const karam_problem *p, int32_t *mos_order,
  * capacitor companions of the chosen method with history v_prev = i_prev = 0. */
 KARAM_API int karam_eval_stamp(karam_problem *p, int32_t precision, const double *v,
                                double *jac, double *f);
-/* Device timing of the last solve call, per kernel family, in milliseconds. */
-KARAM_API int karam_last_timing(const karam_problem *p, double *eval_ms, double *lu_ms,
-                                int32_t *eval_launches, int32_t *lu_launches,
-                                int32_t *rounds);
+/* Device-side accounting of the last solve call (CUDA events on the problem's
+ * stream; counters kept by the kernels). */
+typedef struct karam_timing {
+  double job_ms;            /* first kernel of the call to its last one             */
+  double eval_ms;           /* summed duration of the evaluation + stamping launches */
+  double lu_ms;             /* summed duration of the factor/solve (+ rescue) launches */
+  int32_t rounds;           /* NR rounds (one evaluation + one factor launch each)   */
+  int32_t eval_launches, lu_launches, rescue_launches, other_launches;
+  int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
+  int64_t evals_tran;       /* instance evaluations in transient mode                */
+  int64_t solves;           /* linear solves by the static-pivot LU                  */
+  int64_t rescues;          /* linear solves redone by the partial-pivoting rescue   */
+} karam_timing;
+KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 
 #ifdef __cplusplus
 }

@@ -71,8 +71,7 @@ def lib():
         "karam_get_device_order": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
         "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
                                        P(C.c_double)]),
-        "karam_last_timing": (C.c_int, [vp, P(C.c_double), P(C.c_double), P(C.c_int32),
-                                        P(C.c_int32), P(C.c_int32)]),
+        "karam_last_timing": (C.c_int, [vp, P(A.KaramTiming)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -254,9 +253,7 @@ class Problem:
         return jac, f
 
     def timing(self):
-        e, l = C.c_double(), C.c_double()
-        ne, nl_, r = C.c_int32(), C.c_int32(), C.c_int32()
-        self._check(lib().karam_last_timing(self.h, C.byref(e), C.byref(l), C.byref(ne),
-                                            C.byref(nl_), C.byref(r)))
-        return dict(eval_ms=e.value, lu_ms=l.value, eval_launches=ne.value,
-                    lu_launches=nl_.value, rounds=r.value)
+        """Device accounting of the last solve call (karam_timing as a dict)."""
+        t = A.KaramTiming()
+        self._check(lib().karam_last_timing(self.h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in A.KaramTiming._fields_}

@@ -76,6 +76,14 @@ class KaramInstanceStats(C.Structure):
                 ("max_step_iters", C.c_int32), ("residual", C.c_double)]
 
 
+class KaramTiming(C.Structure):
+    _fields_ = [("job_ms", C.c_double), ("eval_ms", C.c_double), ("lu_ms", C.c_double),
+                ("rounds", C.c_int32), ("eval_launches", C.c_int32), ("lu_launches", C.c_int32),
+                ("rescue_launches", C.c_int32), ("other_launches", C.c_int32),
+                ("evals_dc", C.c_int64), ("evals_tran", C.c_int64), ("solves", C.c_int64),
+                ("rescues", C.c_int64)]
+
+
 def ptr(arr, ctype):
     """Pointer to a contiguous numpy array (or NULL for None)."""
     if arr is None:

@@ -87,18 +87,20 @@ struct karam_problem {
   DevTopo dt{};
   // instance buffers
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_Fmax, i_J, i_cvp, i_cip, i_st, i_seed,
-      i_out, d_active, r_ws, r_list, r_count, i_vtp;
+      i_out, d_active, r_ws, r_list, r_count, i_vtp, d_counters;
+  cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   int* h_active = nullptr;  // pinned
 
-  // timing of the last solve call
-  double eval_ms = 0, lu_ms = 0;
-  int eval_launches = 0, lu_launches = 0, rounds = 0;
+  // accounting of the last solve call
+  karam_timing timing{};
 
   std::vector<int> csr_to_f;  // CSR position -> filled position
 
   ~karam_problem() {
     if (h_active) cudaFreeHost(h_active);
+    if (ev_job0) cudaEventDestroy(ev_job0);
+    if (ev_job1) cudaEventDestroy(ev_job1);
   }
 };
 
@@ -279,6 +281,9 @@ void alloc_instances(karam_problem* p) {
   p->i_vtp.alloc(M * n * sizeof(double));
   p->i_out.alloc(M * n * sizeof(double));
   p->d_active.alloc(sizeof(int));
+  p->d_counters.alloc(4 * sizeof(unsigned long long));
+  ck(cudaEventCreate(&p->ev_job0), "cudaEventCreate");
+  ck(cudaEventCreate(&p->ev_job1), "cudaEventCreate");
   // Partial-pivoting rescue: one dense n x n FP64 workspace per concurrently
   // running rescue CTA, bounded by a 2 GiB budget.
   const size_t dense = n * n * sizeof(double);
@@ -316,6 +321,7 @@ DevInst dev_inst(karam_problem* p) {
   I.rescue_list = p->rescue_slots > 0 ? p->r_list.as<RescueItem>() : nullptr;
   I.rescue_count = p->rescue_slots > 0 ? p->r_count.as<int>() : nullptr;
   I.rescue_slots = p->rescue_slots;
+  I.counters = p->d_counters.as<unsigned long long>();
   I.wave = nullptr;
   I.wave_pos = nullptr;
   I.n_wave = 0;
@@ -449,8 +455,6 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
   } gg{graph, exec};
   ck(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
 
-  p->eval_ms = p->lu_ms = 0;
-  p->eval_launches = p->lu_launches = p->rounds = 0;
   const int budget = max_rounds > 0 ? max_rounds : (1 << 30);
   while (true) {
     ck(cudaGraphLaunch(exec, s), "graph launch");
@@ -460,13 +464,14 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
       float a = 0, b = 0;
       ck(cudaEventElapsedTime(&a, ev[3 * r], ev[3 * r + 1]), "event time");
       ck(cudaEventElapsedTime(&b, ev[3 * r + 1], ev[3 * r + 2]), "event time");
-      p->eval_ms += a;
-      p->lu_ms += b;
+      p->timing.eval_ms += a;
+      p->timing.lu_ms += b;
     }
-    p->eval_launches += kRounds;
-    p->lu_launches += kRounds;
-    p->rounds += kRounds;
-    if (*p->h_active == 0 || p->rounds >= budget) break;
+    p->timing.eval_launches += kRounds;
+    p->timing.lu_launches += kRounds;
+    if (I.rescue_list) p->timing.rescue_launches += kRounds;
+    p->timing.rounds += kRounds;
+    if (*p->h_active == 0 || p->timing.rounds >= budget) break;
   }
 }
 
@@ -500,6 +505,28 @@ void read_voltages(karam_problem* p, double* out_v) {
   ck(cudaStreamSynchronize(p->ctx->stream), "read sync");
 }
 
+// Job accounting: counters cleared and a start event recorded before the
+// first kernel of a solve call; end_job records the end event and reads back.
+void begin_job(karam_problem* p) {
+  p->timing = karam_timing{};
+  ck(cudaMemsetAsync(p->d_counters.p, 0, 4 * sizeof(unsigned long long), p->ctx->stream), "memset counters");
+  ck(cudaEventRecord(p->ev_job0, p->ctx->stream), "event record");
+}
+
+void end_job(karam_problem* p) {
+  ck(cudaEventRecord(p->ev_job1, p->ctx->stream), "event record");
+  unsigned long long c[4];
+  ck(cudaMemcpyAsync(c, p->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream), "D2H counters");
+  ck(cudaStreamSynchronize(p->ctx->stream), "job sync");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, p->ev_job0, p->ev_job1), "job time");
+  p->timing.job_ms = ms;
+  p->timing.evals_dc = (int64_t)c[0];
+  p->timing.evals_tran = (int64_t)c[1];
+  p->timing.solves = (int64_t)c[2];
+  p->timing.rescues = (int64_t)c[3];
+}
+
 void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
   DevInst I = dev_inst(p);
   if (P.seeded && seed_v) {
@@ -515,6 +542,7 @@ void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
   }
   launch_init(p->dt, I, P, p->ctx->stream);
   ck(cudaGetLastError(), "init launch");
+  p->timing.other_launches += 1;
   p->tran_started = P.n_steps > 0;
   p->t_now = P.n_steps > 0 ? P.n_steps * P.h : 0.0;
   p->tran_h = P.h;
@@ -638,8 +666,10 @@ int karam_solve_dc(karam_problem* p, const karam_solver_opts* opts, const double
     need_device(p);
     JobParams P = job_params(opts, 0, 0.0, KARAM_TRAN_BE);
     if (P.seeded && !seed_v) throw std::runtime_error("seeded solve without seed_v");
+    begin_job(p);
     start_job(p, P, seed_v);
     run_rounds(p, P, opts ? opts->max_rounds : 0);
+    end_job(p);
     p->have_dc = true;
     read_voltages(p, out_v);
     read_stats(p, stats, true);
@@ -654,8 +684,10 @@ int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double 
     need_device(p);
     JobParams P = job_params(opts, n_steps, dt, method);
     if (P.seeded) throw std::runtime_error("seeded starts need karam_solve_dc");
+    begin_job(p);
     start_job(p, P, nullptr);
     run_rounds(p, P, opts ? opts->max_rounds : 0);
+    end_job(p);
     p->have_dc = true;
     return KARAM_OK;
   });
@@ -713,9 +745,12 @@ int karam_step_transient(karam_problem* p, const karam_solver_opts* opts, double
     I.wave_pos = wpos.as<int>();
     I.n_wave = n_wave;
     I.wave_steps = n_steps;
+    begin_job(p);
     launch_tran_start(p->dt, I, p->tran_started ? 0 : 1, p->ctx->stream);
     ck(cudaGetLastError(), "tran start");
+    p->timing.other_launches += 1;
     run_rounds(p, P, opts ? opts->max_rounds : 0, &I);
+    end_job(p);
     p->tran_started = true;
     p->tran_h = dt;
     p->tran_method = method;
@@ -821,14 +856,9 @@ int karam_eval_stamp(karam_problem* p, int32_t precision, const double* v, doubl
   });
 }
 
-int karam_last_timing(const karam_problem* p, double* eval_ms, double* lu_ms,
-                      int32_t* eval_launches, int32_t* lu_launches, int32_t* rounds) {
-  if (!p) return KARAM_E_INVALID;
-  if (eval_ms) *eval_ms = p->eval_ms;
-  if (lu_ms) *lu_ms = p->lu_ms;
-  if (eval_launches) *eval_launches = p->eval_launches;
-  if (lu_launches) *lu_launches = p->lu_launches;
-  if (rounds) *rounds = p->rounds;
+int karam_last_timing(const karam_problem* p, karam_timing* out) {
+  if (!p || !out) return KARAM_E_INVALID;
+  *out = p->timing;
   return KARAM_OK;
 }
 

@@ -104,6 +104,7 @@ struct DevInst {
   struct RescueItem* rescue_list;  // [ni]
   int* rescue_count;
   int rescue_slots;
+  unsigned long long* counters;  // [4]: evaluations DC, evaluations transient, solves, rescues
   double* wave;         // [ni][wave_steps][n_wave] node voltages after each step
   const int* wave_pos;  // permuted positions of the recorded nodes (-1 = ground)
   int n_wave, wave_steps;

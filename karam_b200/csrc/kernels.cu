@@ -97,6 +97,7 @@ __global__ void k_init(DevTopo T, DevInst I, JobParams P) {
   __syncthreads();
   for (int i = threadIdx.x; i < T.n; i += blockDim.x) x[i] = v[i];
   if (threadIdx.x == 0) {
+    if (I.counters) atomicAdd(&I.counters[0], 1ull);
     InstState s = {};
     s.mode = MODE_DC;
     s.sub = SUB_NR;
@@ -780,10 +781,21 @@ __global__ void __launch_bounds__(kLuThreads) k_lu(DevTopo Tp, DevInst I, JobPar
       } else if ((a & ACT_SOLVE) && (a & ACT_LIMIT) && Tp.n_dio > 0) {
         limit_junctions(Tp, I.x + (size_t)inst * n, I.v + (size_t)inst * n);
       }
-      live = I.st[inst].mode != MODE_DONE;
+      const int md = I.st[inst].mode;
+      live = (md != MODE_DONE) ? (md == MODE_TRAN ? 2 : 1) : 0;
     }
-    const unsigned m = __ballot_sync(kFull, live);
-    if (tid == 0 && m) atomicAdd(active, __popc(m));
+    const unsigned m = __ballot_sync(kFull, live != 0);
+    const unsigned mt = __ballot_sync(kFull, live == 2);
+    const unsigned ms = __ballot_sync(kFull, tid < cnt && (act[tid] & ACT_SOLVE) && !sing_s[tid]);
+    if (tid == 0) {
+      if (m) atomicAdd(active, __popc(m));
+      if (I.counters) {
+        // instances alive now are evaluated by the next round
+        if (m & ~mt) atomicAdd(&I.counters[0], (unsigned long long)__popc(m & ~mt));
+        if (mt) atomicAdd(&I.counters[1], (unsigned long long)__popc(mt));
+        if (ms) atomicAdd(&I.counters[2], (unsigned long long)__popc(ms));
+      }
+    }
   }
 }
 
@@ -929,6 +941,7 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
       if (tid == 0) {
         if (sanitize && Tp.n_dio > 0) limit_junctions(Tp, x, v);
         I.st[inst].rescued += 1;
+        if (I.counters) atomicAdd(&I.counters[3], 1ull);
       }
     } else if (tid == 0) {
       on_singular(Tp, I, inst);
@@ -956,6 +969,7 @@ __global__ void k_tran_start(DevTopo T, DevInst I, int init_caps) {
   double* vtp = I.v_tp + (size_t)inst * T.n;
   for (int i = threadIdx.x; i < T.n; i += blockDim.x) vtp[i] = v[i];
   if (threadIdx.x == 0) {
+    if (I.counters) atomicAdd(&I.counters[1], 1ull);
     s.mode = MODE_TRAN;
     s.sub = SUB_NR;
     s.step = 1;
