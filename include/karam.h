@@ -173,6 +173,7 @@ typedef struct karam_problem_info {
   int32_t n_instances;
   int32_t n_mos, n_dio, n_res, n_cap, n_vsrc, n_isrc;
   int32_t lu_ops;      /* scaled + update operations of the LU program           */
+  int32_t lu_jit;      /* 1 when the LU round runs as code compiled for this topology */
 } karam_problem_info;
 
 /* Per-instance counters returned by the solves. */
@@ -210,6 +211,9 @@ KARAM_API int karam_problem_create(karam_ctx *ctx, const karam_netlist *nl,
                                    int32_t max_instances, karam_problem **out);
 KARAM_API void karam_problem_destroy(karam_problem *p);
 KARAM_API int karam_problem_info_get(const karam_problem *p, karam_problem_info *out);
+/* How the LU round runs for this problem: compiled for its topology (NVRTC),
+ * or the program interpreter and why. */
+KARAM_API const char *karam_problem_lu_status(const karam_problem *p);
 /* Copies per-instance parameters host -> device (the batch to solve next). */
 KARAM_API int karam_set_instances(karam_problem *p, const karam_instances *inst);
 

@@ -72,6 +72,7 @@ def lib():
         "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
                                        P(C.c_double)]),
         "karam_last_timing": (C.c_int, [vp, P(A.KaramTiming)]),
+        "karam_problem_lu_status": (C.c_char_p, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -132,6 +133,7 @@ class Problem:
             raise KaramError(rc, lib().karam_last_error(ctx.h if ctx else None).decode())
         self.h = h
         self.info = self._info()
+        self.info["lu_status"] = lib().karam_problem_lu_status(self.h).decode()
         self.n = self.info["n"]
         self.ni = 1
 

@@ -65,7 +65,7 @@ class KaramSolverOpts(C.Structure):
 class KaramProblemInfo(C.Structure):
     _fields_ = [(name, C.c_int32) for name in (
         "n", "nnz", "nnz_filled", "fill_in", "treewidth", "n_triplets", "n_instances",
-        "n_mos", "n_dio", "n_res", "n_cap", "n_vsrc", "n_isrc", "lu_ops")]
+        "n_mos", "n_dio", "n_res", "n_cap", "n_vsrc", "n_isrc", "lu_ops", "lu_jit")]
 
 
 class KaramInstanceStats(C.Structure):

@@ -81,7 +81,7 @@ struct karam_problem {
 
   // topology buffers
   DBuf t_mos_term, t_mos_geo, t_mos_pmos, t_dio_term, t_dio_par, t_res_term, t_res_g, t_cap_term,
-      t_cap_c, t_mos_card, t_f_row, t_f_colp, t_vs_term, t_vs_kind, t_vs_pulse, t_is_term, t_is_amp, t_jt_off, t_jt_code,
+      t_cap_c, t_mos_card, t_f_row, t_f_colp, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse, t_is_term, t_is_amp, t_jt_off, t_jt_code,
       t_jlin, t_jcap_off, t_jcap_code, t_ft_off, t_ft_code, t_lu_hdr, t_lu_data, t_seed_vs,
       t_seed_anode, t_perm;
   DevTopo dt{};
@@ -96,8 +96,10 @@ struct karam_problem {
   karam_timing timing{};
 
   std::vector<int> csr_to_f;  // CSR position -> filled position
+  JitLu jit;                  // LU round compiled for this topology
 
   ~karam_problem() {
+    jit_release(jit);
     if (h_active) cudaFreeHost(h_active);
     if (ev_job0) cudaEventDestroy(ev_job0);
     if (ev_job1) cudaEventDestroy(ev_job1);
@@ -181,7 +183,11 @@ void upload_topology(karam_problem* p) {
   for (int a : T.seed_anodes) seed_an.push_back(a > 0 ? T.iperm[a - 1] : -1);
   std::vector<int4> hdr;
   for (int k = 0; k < T.n; ++k)
-    hdr.push_back(make_int4(T.lu_hdr[4 * k], T.lu_hdr[4 * k + 1], T.lu_hdr[4 * k + 2], 0));
+    hdr.push_back(make_int4(T.lu_hdr[4 * k], T.lu_hdr[4 * k + 1], T.lu_hdr[4 * k + 2],
+                            T.lu_hdr[4 * k + 3]));
+  std::vector<double2> dlim;
+  for (size_t i = 0; i < T.dio.size(); ++i)
+    dlim.push_back(make_double2(T.dio_lim[2 * i], T.dio_lim[2 * i + 1]));
 
   upload(p->t_mos_term, mt);
   upload(p->t_mos_geo, mg);
@@ -189,6 +195,8 @@ void upload_topology(karam_problem* p) {
   upload(p->t_mos_card, mc);
   upload(p->t_dio_term, dtm);
   upload(p->t_dio_par, dpar);
+  upload(p->t_dio_lim, dlim);
+  upload(p->t_dio_level, T.dio_level);
   upload(p->t_res_term, rtm);
   upload(p->t_res_g, rg);
   upload(p->t_cap_term, ctm);
@@ -232,6 +240,9 @@ void upload_topology(karam_problem* p) {
   d.mos_card = p->t_mos_card.as<double2>();
   d.dio_term = p->t_dio_term.as<int2>();
   d.dio_par = p->t_dio_par.as<double4>();
+  d.dio_lim = p->t_dio_lim.as<double2>();
+  d.dio_level = p->t_dio_level.as<int>();
+  d.n_dio_levels = T.n_dio_levels;
   d.res_term = p->t_res_term.as<int2>();
   d.res_g = p->t_res_g.as<double>();
   d.cap_term = p->t_cap_term.as<int2>();
@@ -417,6 +428,7 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
   if (L.ni_per_cta < 1)
     throw std::runtime_error("instance too large for the thread-per-instance schedule");
   configure_kernels(p->dt, L);
+  configure_jit(p->jit, L);
   ck(cudaGetLastError(), "configure kernels");
   std::vector<cudaEvent_t> ev(3 * kRounds);
   for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
@@ -438,7 +450,10 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
     launch_eval(p->dt, I, P, prec, s);
     cudaEventRecordWithFlags(ev[3 * r + 1], s, cudaEventRecordExternal);
     if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
-    launch_lu(p->dt, I, P, L, prec, active, s);
+    if (p->jit.ok)
+      launch_lu_jit(p->jit, p->dt, I, P, L, prec, active, s);
+    else
+      launch_lu(p->dt, I, P, L, prec, active, s);
     if (I.rescue_list) launch_rescue(p->dt, I, P, prec, I.rescue_slots, s);
     cudaEventRecordWithFlags(ev[3 * r + 2], s, cudaEventRecordExternal);
   }
@@ -623,12 +638,18 @@ int karam_problem_create(karam_ctx* ctx, const karam_netlist* nl, int32_t max_in
     upload_topology(p.get());
     alloc_instances(p.get());
     set_instances_impl(p.get(), nullptr);
+    jit_build(p->topo, p->jit);
     *out = p.release();
     return KARAM_OK;
   });
 }
 
 void karam_problem_destroy(karam_problem* p) { delete p; }
+
+const char* karam_problem_lu_status(const karam_problem* p) {
+  if (!p) return "";
+  return p->jit.ok ? "straight-line LU compiled for this topology" : p->jit.status.c_str();
+}
 
 int karam_problem_info_get(const karam_problem* p, karam_problem_info* o) {
   if (!p || !o) return KARAM_E_INVALID;
@@ -647,6 +668,7 @@ int karam_problem_info_get(const karam_problem* p, karam_problem_info* o) {
   o->n_vsrc = (int)T.vs.size();
   o->n_isrc = (int)T.isrc.size();
   o->lu_ops = T.lu_ops;
+  o->lu_jit = p->jit.ok ? 1 : 0;
   return KARAM_OK;
 }
 

@@ -344,24 +344,73 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   for (size_t i = 0; i < T.mos.size(); ++i) two(T.mos[i].d, T.mos[i].s, FK_MOS, (int)i);
   flatten(ft, T.ft_off, T.ft_code);
 
-  // LU program.
+  // LU program on the numerically non-zero part of the filled pattern. The
+  // filled pattern of symbolicFactorize is symmetric, but the MNA stamps are
+  // not (a MOSFET stamps its drain/source rows, never its gate row), so many
+  // positions of it hold zeros that stay zero through the elimination. The
+  // program keeps the reference's ordering and pattern and skips those: it
+  // eliminates on the unsymmetric structure of the stamps (gmb stamps, always
+  // zero in the level-1 kernel, excluded), which is a subset of the filled
+  // pattern, so results equal the full static elimination's.
+  std::vector<std::vector<int>> nzr(n), nzc(n);  // row -> cols, col -> rows (permuted)
+  auto add_nz = [&](int r, int c) {
+    auto& row = nzr[r];
+    auto it = std::lower_bound(row.begin(), row.end(), c);
+    if (it != row.end() && *it == c) return;
+    row.insert(it, c);
+    auto& col = nzc[c];
+    col.insert(std::lower_bound(col.begin(), col.end(), r), r);
+  };
+  for (auto& x : T.trip)
+    if (x.kind != SS_MOS_GMB) add_nz(T.iperm[x.row], T.iperm[x.col]);
   T.lu_hdr.assign(4 * (size_t)n, 0);
   T.lu_data.clear();
   T.lu_ops = 0;
   T.max_d = 0;
+  std::vector<int> L, U;
   for (int k = 0; k < n; ++k) {
-    const auto& nb = urow[k];
-    int d = (int)nb.size();
-    T.max_d = std::max(T.max_d, d);
+    L.clear();
+    U.clear();
+    for (int i : nzc[k])
+      if (i > k) L.push_back(i);
+    for (int j : nzr[k])
+      if (j > k) U.push_back(j);
+    for (int i : L)
+      for (int j : U) add_nz(i, j);
+    const int nl = (int)L.size(), nu = (int)U.size();
+    T.max_d = std::max({T.max_d, nl, nu});
     T.lu_hdr[4 * k + 0] = (int)T.lu_data.size();
-    T.lu_hdr[4 * k + 1] = d;
-    T.lu_hdr[4 * k + 2] = T.f_diag[k];
-    for (int a = 0; a < d; ++a) T.lu_data.push_back(nb[a]);
-    for (int a = 0; a < d; ++a) T.lu_data.push_back(fp(nb[a], k));
-    for (int b = 0; b < d; ++b) T.lu_data.push_back(fp(k, nb[b]));
-    for (int a = 0; a < d; ++a)
-      for (int b = 0; b < d; ++b) T.lu_data.push_back(fp(nb[a], nb[b]));
-    T.lu_ops += d + d * d;
+    T.lu_hdr[4 * k + 1] = nl;
+    T.lu_hdr[4 * k + 2] = nu;
+    T.lu_hdr[4 * k + 3] = T.f_diag[k];
+    for (int i : L) T.lu_data.push_back(i);
+    for (int i : L) T.lu_data.push_back(fp(i, k));
+    for (int j : U) T.lu_data.push_back(j);
+    for (int j : U) T.lu_data.push_back(fp(k, j));
+    for (int i : L)
+      for (int j : U) T.lu_data.push_back(fp(i, j));
+    T.lu_ops += nl + nl * nu;
+  }
+
+  // Junction limiting constants (applyPnJunctionLimits, circuitsim_solver.cpp:118-169):
+  // the reference recomputes them on every call with these expressions.
+  const double ts = T.temp_k / 300.15;
+  std::vector<int> last(n + 1, -1);
+  T.dio_lim.clear();
+  T.dio_level.clear();
+  T.n_dio_levels = 0;
+  for (const auto& d : T.dio) {
+    double vt = d.vt * ts;
+    double is = d.is * std::pow(ts, 3.0) * std::exp(1.11 / (vt / ts) - 1.11 / vt);
+    T.dio_lim.push_back(vt);
+    T.dio_lim.push_back(vt * std::log(vt / (std::sqrt(2.0) * is)));
+    int lvl = 0;
+    if (d.a > 0) lvl = std::max(lvl, last[d.a] + 1);
+    if (d.c > 0) lvl = std::max(lvl, last[d.c] + 1);
+    if (d.a > 0) last[d.a] = lvl;
+    if (d.c > 0) last[d.c] = lvl;
+    T.dio_level.push_back(lvl);
+    T.n_dio_levels = std::max(T.n_dio_levels, lvl + 1);
   }
 
   auto pn = [&](int node) { return node > 0 ? T.iperm[node - 1] : -1; };

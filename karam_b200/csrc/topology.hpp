@@ -75,11 +75,17 @@ struct Topology {
   std::vector<int> jcap_off, jcap_code;      // capacitor stamps per filled position (G = C * scale)
   std::vector<int> ft_off, ft_code;          // per permuted node
 
-  // ---- LU program: per pivot (off, d, dpos); data = nbr[d] lpos[d] upos[d] tpos[d*d] ----
+  // ---- LU program: per pivot k (off, nL, nU, dpos); data at off =
+  //      Lrow[nL] Lpos[nL] Ucol[nU] Upos[nU] T[nL*nU] (update targets, row-major) ----
   std::vector<int> lu_hdr;   // 4 ints per pivot
   std::vector<int> lu_data;
   int lu_ops = 0;
   int max_d = 0;
+
+  // ---- junction limiting (SoA diode order) ----
+  std::vector<double> dio_lim;  // 2 per diode: Vt * T/Tnom, vcrit
+  std::vector<int> dio_level;   // diodes of one level share no node
+  int n_dio_levels = 0;
 
   // ---- device tables in permuted node indices (-1 = ground) ----
   std::vector<int> mos_term;  // 4 per MOSFET: d g s b
