@@ -18,6 +18,7 @@
 #include "acutesim_engine/infrastructure/factor_graph.h"
 #include "acutesim_engine/infrastructure/treewidth_analyzer.h"
 #include "acutesim_engine/math/sparse_lu.h"
+#include "acutesim_engine/math/portable_rng.h"
 
 #include <algorithm>
 #include <cmath>
@@ -511,6 +512,16 @@ int oracle_run_batch(const karam_netlist* nl, const karam_instances* inst, int32
     for (auto& th : pool) th.join();
     return 0;
   });
+}
+
+// Draws of the reference's seeded normal sampler (math/portable_rng.h:15-95):
+// PortableRNG(seed) feeding PortableNormalDist(mean, sd), `count` calls in a row.
+// Used to pin the Monte-Carlo parameter sampler of the test circuits.
+int oracle_ref_normals(uint64_t seed, double mean, double sd, int32_t count, double* out) {
+  acutesim::math::PortableRNG rng(seed);
+  acutesim::math::PortableNormalDist dist(mean, sd);
+  for (int32_t i = 0; i < count; ++i) out[i] = dist(rng);
+  return 0;
 }
 
 }  // extern "C"

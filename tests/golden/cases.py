@@ -1,0 +1,67 @@
+"""Netlists of the golden fixtures: the two benchmark circuits plus small edge
+cases of the symbolic layer and the NR loop (ragged device mixes, duplicate
+stamp slots, a floating source, a capacitor-only node)."""
+from karam_b200 import circuits
+from karam_b200.circuits import Netlist
+
+
+def divider():
+    """Resistive divider with a current source: linear, one NR step."""
+    nl = Netlist()
+    nl.vsource(1, 0, 1.0)
+    nl.resistor(1, 2, 1e3)
+    nl.resistor(2, 0, 2e3)
+    nl.isource(0, 2, 1e-4)
+    return nl
+
+
+def floating_source():
+    """A voltage source between two non-ground nodes (branch id collision case)."""
+    nl = Netlist()
+    nl.vsource(1, 0, 1.2)
+    nl.vsource(2, 1, 0.5)
+    nl.resistor(2, 3, 500.0)
+    nl.resistor(3, 0, 1e3)
+    nl.diode(3, 0)
+    return nl
+
+
+def parallel_duplicates():
+    """Identical devices in parallel: every stamp slot of the pair collides."""
+    nl = Netlist()
+    nmos = nl.model("NCH", 0, kp=110e-6, vto=0.7, lam=0.04)
+    pmos = nl.model("PCH", 1, kp=40e-6, vto=-0.7, lam=0.05)
+    nl.vsource(1, 0, 1.8)
+    nl.vsource(2, 0, 0.6)
+    for _ in range(2):
+        nl.mosfet(3, 2, 0, 0, nmos, 2e-6, 0.18e-6)
+        nl.mosfet(3, 2, 1, 1, pmos, 4e-6, 0.18e-6)
+    nl.resistor(3, 0, 1e5)
+    nl.resistor(3, 0, 1e5)
+    return nl
+
+
+def diode_rc():
+    """Diode clamp through a series resistor with node caps; node 4 is reached
+    only through a capacitor (DC: held by gmin alone)."""
+    nl = Netlist()
+    nl.vsource(1, 0, 0.0, pulse=(0.0, 1.0, 0.0, 5e-12, 5e-12, 50e-12, 0.0))
+    nl.resistor(1, 2, 100.0)
+    nl.diode(2, 3)
+    nl.resistor(3, 0, 10.0)
+    nl.capacitor(2, 0, 1e-15)
+    nl.capacitor(3, 4, 1e-15)
+    nl.capacitor(4, 0, 1e-15)
+    return nl
+
+
+SMALL = {
+    "divider": divider,
+    "floating_source": floating_source,
+    "parallel_duplicates": parallel_duplicates,
+    "diode_rc": diode_rc,
+}
+BENCH = {"config1": circuits.config1, "config2": circuits.config2}
+
+RNG_SEEDS = (circuits.BASE_SEED, circuits.BASE_SEED + 1, circuits.BASE_SEED + 4095, 1)
+RNG_COUNT = 64

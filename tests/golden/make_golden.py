@@ -1,0 +1,122 @@
+#!/usr/bin/env python
+"""Generates the golden fixtures of the NR inner loop from the oracle library
+compiled from the reference's own sources (oracle/_ref/libkaram_ref.so, built
+by ``make -C oracle ref`` where the reference tree is present).
+
+Every array comes from reference code: the stamp pattern and slot map
+(MatrixConstructor::buildPattern / CachedCsrPattern::indexOf), the SoA order of
+tensorizeNetlist, the Min-Fill ordering (FactorGraph + TreewidthAnalyzer), the
+filled pattern of symbolicFactorize, the stamps of stampSoABlock, the NR
+solutions of the oracle driver over those stamps and solveLU_Pivoted /
+solveSparse_LU, and PortableNormalDist draws.
+
+    python tests/golden/make_golden.py      # rewrites tests/golden/*.npz
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+import ctypes as C  # noqa: E402
+
+import cases  # noqa: E402
+from karam_b200 import _abi as A  # noqa: E402
+from karam_b200 import circuits  # noqa: E402
+from oracle import pyoracle  # noqa: E402
+
+POLISH = dict(polish_max=8)
+WAVE_NODES = {"config2": [2, 3, 4, 5, 10, 20, 259], "diode_rc": [1, 2, 3, 4]}
+
+
+def probe_voltages(n, seed=11):
+    return np.random.default_rng(seed).uniform(-0.2, 2.0, size=n)
+
+
+def symbolic(ref, nl):
+    out = {}
+    out["rp_tran"], out["col_tran"] = ref.pattern(nl, transient=True)
+    out["rp_dc"], out["col_dc"] = ref.pattern(nl, transient=False)
+    out["stamp_map"] = ref.stamp_map(nl)
+    out["mos_order"], out["dio_order"] = ref.tensorize(nl)
+    raw, perm, tw = ref.ordering(nl)
+    out["raw_order"], out["perm_translated"], out["treewidth"] = raw, perm, np.int32(tw)
+    sym = ref.symbolic(nl)
+    out["perm"], out["iperm"] = sym["perm"], sym["iperm"]
+    out["f_row_ptr"], out["f_col"], out["fill_in"] = sym["row_ptr"], sym["col"], np.int32(sym["fill_in"])
+    return out
+
+
+def stamps(ref, nl, inst=None):
+    n = nl.n_nodes
+    v = probe_voltages(n)
+    out = {"probe_v": v}
+    out["stamp_dc_vals"], out["stamp_dc_rhs"] = ref.stamp(nl, v, inst, 0)
+    if nl.cap:
+        cv = np.linspace(-0.1, 0.3, len(nl.cap))
+        out["cap_vprev"] = cv
+        out["stamp_tr_vals"], out["stamp_tr_rhs"] = ref.stamp(nl, v, inst, 0, h=1e-12,
+                                                              method=A.TRAN_BE, cap_vprev=cv,
+                                                              t=2e-12)
+    return out
+
+
+def stats_arr(st):
+    keys = ("converged", "iterations", "polish_iters", "damped", "gmin_step", "singular")
+    return np.array([st[k] for k in keys], np.int64)
+
+
+def main():
+    if not os.path.isdir("/root/reference"):
+        sys.exit("the reference tree is needed to build the reference oracle")
+    pyoracle.build("ref")
+    ref = pyoracle.Oracle("ref")
+
+    seeds = np.array(cases.RNG_SEEDS, np.uint64)
+    normals = np.zeros((len(seeds), cases.RNG_COUNT))
+    for k, s in enumerate(seeds):
+        ref.lib.oracle_ref_normals.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_int32,
+                                               C.POINTER(C.c_double)]
+        ref.lib.oracle_ref_normals(int(s), 0.0, 1.0, cases.RNG_COUNT,
+                                   normals[k].ctypes.data_as(C.POINTER(C.c_double)))
+    np.savez_compressed(os.path.join(HERE, "rng_normals.npz"), seeds=seeds, normals=normals)
+
+    for name, make in {**cases.SMALL, **cases.BENCH}.items():
+        nl = make()
+        inst = circuits.mc_instances(nl, 2) if name == "config2" else None
+        out = symbolic(ref, nl)
+        out.update(stamps(ref, nl, inst))
+        if name == "config2":
+            out["mc_kp"], out["mc_vto"] = inst.mos_kp, inst.mos_vto
+            vs, sts = [], []
+            for i in range(2):
+                v, st = ref.solve_dc(nl, inst, i, linear_solver=pyoracle.LS_SPARSE, **POLISH)
+                vs.append(v)
+                sts.append(stats_arr(st))
+            out["dc_v"], out["dc_stats"] = np.array(vs), np.array(sts)
+            vt, st, wave = ref.transient(nl, vs[0], 1e-12, 20, A.TRAN_BE, inst, 0,
+                                         wave_nodes=WAVE_NODES[name],
+                                         linear_solver=pyoracle.LS_SPARSE, **POLISH)
+            out["tran_v"], out["tran_stats"], out["tran_wave"] = vt, stats_arr(st), wave
+            out["tran_wave_nodes"] = np.array(WAVE_NODES[name], np.int32)
+        else:
+            v, st = ref.solve_dc(nl)
+            out["dc_v_ref_rule"], out["dc_stats_ref_rule"] = v, stats_arr(st)
+            v, st = ref.solve_dc(nl, **POLISH)
+            out["dc_v"], out["dc_stats"] = v, stats_arr(st)
+            if name in WAVE_NODES:
+                vt, st, wave = ref.transient(nl, v, 1e-12, 40, A.TRAN_BE,
+                                             wave_nodes=WAVE_NODES[name], **POLISH)
+                out["tran_v"], out["tran_stats"], out["tran_wave"] = vt, stats_arr(st), wave
+                out["tran_wave_nodes"] = np.array(WAVE_NODES[name], np.int32)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, "n =", nl.n_nodes, "nnz =", len(out["col_tran"]),
+              "dc stats", out["dc_stats"].tolist())
+
+
+if __name__ == "__main__":
+    main()

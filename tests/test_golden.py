@@ -1,0 +1,159 @@
+"""The oracle restatement and the product's host symbolic layer against the
+golden fixtures generated from the reference's own code (tests/golden/).
+
+The reference ships no tests or known-answer vectors for this path; the
+fixtures come from the oracle library compiled from the reference sources
+(see tests/golden/make_golden.py), so they pin both the restatement and the
+product without the reference tree present. CPU only.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import cases  # noqa: E402
+from karam_b200 import _abi as A  # noqa: E402
+from karam_b200 import circuits  # noqa: E402
+
+ALL = {**cases.SMALL, **cases.BENCH}
+STAT_KEYS = ("converged", "iterations", "polish_iters", "damped", "gmin_step", "singular")
+
+
+def golden(name):
+    with np.load(os.path.join(HERE, "golden", f"{name}.npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+def stats_arr(st):
+    return np.array([st[k] for k in STAT_KEYS], np.int64)
+
+
+def instances_for(name, nl, g):
+    if name != "config2":
+        return None
+    return circuits.Instances(2, g["mc_kp"], g["mc_vto"])
+
+
+# ---------------------------------------------------------------------------
+# Monte-Carlo sampler vs PortableRNG / PortableNormalDist (math/portable_rng.h)
+# ---------------------------------------------------------------------------
+def test_sampler_matches_reference_rng():
+    g = golden("rng_normals")
+    rng = circuits.PCG32(g["seeds"])
+    draws = []
+    for _ in range(g["normals"].shape[1] // 2):
+        c, s = circuits.normal_pairs(rng)
+        draws += [c, s]
+    ours = np.stack(draws, axis=1)
+    # libm vs numpy transcendental rounding: a few ulp at most
+    assert np.allclose(ours, g["normals"], rtol=4e-15, atol=4e-15)
+
+
+def test_mc_parameters_are_reproducible():
+    g = golden("config2")
+    inst = circuits.mc_instances(circuits.config2(), 2)
+    assert np.array_equal(inst.mos_kp, g["mc_kp"]) and np.array_equal(inst.mos_vto, g["mc_vto"])
+
+
+# ---------------------------------------------------------------------------
+# oracle restatement (port) vs the reference-generated fixtures
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", list(ALL))
+def test_port_symbolic(port, name):
+    nl, g = ALL[name](), golden(name)
+    rp, col = port.pattern(nl, transient=True)
+    assert np.array_equal(rp, g["rp_tran"]) and np.array_equal(col, g["col_tran"])
+    rp, col = port.pattern(nl, transient=False)
+    assert np.array_equal(rp, g["rp_dc"]) and np.array_equal(col, g["col_dc"])
+    assert np.array_equal(port.stamp_map(nl), g["stamp_map"])
+    mo, do = port.tensorize(nl)
+    assert np.array_equal(mo, g["mos_order"]) and np.array_equal(do, g["dio_order"])
+    raw, perm, tw = port.ordering(nl)
+    assert np.array_equal(raw, g["raw_order"]) and np.array_equal(perm, g["perm_translated"])
+    assert tw == int(g["treewidth"])
+    sym = port.symbolic(nl)
+    for k, gk in (("perm", "perm"), ("iperm", "iperm"), ("row_ptr", "f_row_ptr"), ("col", "f_col")):
+        assert np.array_equal(sym[k], g[gk]), k
+    assert sym["fill_in"] == int(g["fill_in"])
+
+
+@pytest.mark.parametrize("name", list(ALL))
+def test_port_stamps(port, name):
+    nl, g = ALL[name](), golden(name)
+    inst = instances_for(name, nl, g)
+    vals, rhs = port.stamp(nl, g["probe_v"], inst, 0)
+    assert np.array_equal(vals, g["stamp_dc_vals"]) and np.array_equal(rhs, g["stamp_dc_rhs"])
+    if "stamp_tr_vals" in g:
+        vals, rhs = port.stamp(nl, g["probe_v"], inst, 0, h=1e-12, method=A.TRAN_BE,
+                               cap_vprev=g["cap_vprev"], t=2e-12)
+        assert np.array_equal(vals, g["stamp_tr_vals"]) and np.array_equal(rhs, g["stamp_tr_rhs"])
+
+
+@pytest.mark.parametrize("name", list(cases.SMALL) + ["config1"])
+def test_port_dc(port, name):
+    nl, g = ALL[name](), golden(name)
+    v, st = port.solve_dc(nl)
+    assert np.array_equal(stats_arr(st), g["dc_stats_ref_rule"])
+    assert np.allclose(v, g["dc_v_ref_rule"], rtol=1e-12, atol=1e-15)
+    v, st = port.solve_dc(nl, polish_max=8)
+    assert np.array_equal(stats_arr(st), g["dc_stats"])
+    assert np.allclose(v, g["dc_v"], rtol=1e-12, atol=1e-15)
+
+
+def test_port_dc_config2(port):
+    from oracle import pyoracle
+    nl, g = circuits.config2(), golden("config2")
+    inst = instances_for("config2", nl, g)
+    for i in range(2):
+        v, st = port.solve_dc(nl, inst, i, linear_solver=pyoracle.LS_SPARSE, polish_max=8)
+        assert np.array_equal(stats_arr(st), g["dc_stats"][i])
+        assert np.allclose(v, g["dc_v"][i], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["diode_rc", "config2"])
+def test_port_transient(port, name):
+    from oracle import pyoracle
+    nl, g = ALL[name](), golden(name)
+    inst = instances_for(name, nl, g)
+    v0 = g["dc_v"][0] if name == "config2" else g["dc_v"]
+    steps = 20 if name == "config2" else 40
+    v, st, wave = port.transient(nl, v0, 1e-12, steps, A.TRAN_BE, inst, 0,
+                                 wave_nodes=g["tran_wave_nodes"],
+                                 linear_solver=pyoracle.LS_SPARSE if inst is not None else 0,
+                                 polish_max=8)
+    assert np.array_equal(stats_arr(st), g["tran_stats"])
+    assert np.allclose(v, g["tran_v"], rtol=1e-12, atol=1e-15)
+    assert np.allclose(wave, g["tran_wave"], rtol=1e-12, atol=1e-15)
+
+
+def test_reference_build_reproduces_fixtures(ref):
+    """Where the reference-built oracle exists, the fixtures are current."""
+    nl, g = circuits.config1(), golden("config1")
+    assert np.array_equal(ref.stamp_map(nl), g["stamp_map"])
+    v, st = ref.solve_dc(nl)
+    assert np.array_equal(stats_arr(st), g["dc_stats_ref_rule"])
+    assert np.array_equal(v, g["dc_v_ref_rule"])
+
+
+# ---------------------------------------------------------------------------
+# product host symbolic layer (no device needed) vs the fixtures: bit-exact
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", list(ALL))
+def test_product_symbolic(product, name):
+    nl, g = ALL[name](), golden(name)
+    prob = product.Problem(None, nl)
+    rp, col = prob.pattern()
+    assert np.array_equal(rp, g["rp_tran"]) and np.array_equal(col, g["col_tran"])
+    assert np.array_equal(prob.stamp_map(), g["stamp_map"])
+    raw, perm, tw = prob.ordering()
+    assert np.array_equal(raw, g["raw_order"]) and np.array_equal(perm, g["perm_translated"])
+    assert tw == int(g["treewidth"])
+    frp, fcol = prob.filled_pattern()
+    assert np.array_equal(frp, g["f_row_ptr"]) and np.array_equal(fcol, g["f_col"])
+    assert prob.info["fill_in"] == int(g["fill_in"])
+    mo, do = prob.device_order()
+    assert np.array_equal(mo, g["mos_order"]) and np.array_equal(do, g["dio_order"])
