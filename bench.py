@@ -171,13 +171,18 @@ def measured_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per eval launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "eval_stamp_config2.md")
+def profiled_traffic(kernel):
+    """DRAM bytes (read + write) of one launch of `kernel` at the full
+    4096-instance batch, from the committed ncu summaries: lines of the form
+    `traffic_bytes_per_full_launch <kernel>: <bytes>` under profiles/."""
+    key = f"traffic_bytes_per_full_launch {kernel}:"
+    pdir = os.path.join(ROOT, "profiles")
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_full_launch:"):
-                return float(line.split(":")[1])
+        for name in sorted(os.listdir(pdir)):
+            if name.endswith(".md"):
+                for line in open(os.path.join(pdir, name)):
+                    if line.startswith(key):
+                        return float(line.split(":", 1)[1])
     except OSError:
         pass
     return None
@@ -242,15 +247,24 @@ def run_reference(args, dist):
     print(json.dumps(line), flush=True)
 
 
-def eval_bytes(info, mixed, method_trap=False):
-    """Algorithmic bytes one evaluation + stamping of one instance moves:
-    per-instance KP/VTO (FP32), the voltages read, the Jacobian values
-    written (CSR entries, FP32 or FP64), the KCL residual and its maximum
-    written, the state record read, and in transient the capacitor history."""
-    n, nnz, nm, nc = info["n"], info["nnz"], info["n_mos"], info["n_cap"]
-    base = 8 * nm + 8 * n + (4 if mixed else 8) * nnz + 8 * n + 8 + 16
-    tran = base + 8 * nc * (2 if method_trap else 1)
-    return base, tran
+def eval_stamp_bytes(info, mixed, tran=False):
+    """Algorithmic HBM bytes of one evaluation + stamping of one instance
+    (k_eval + k_stamp): KP/VTO read (FP32), the trial point x and the accepted
+    point v read (FP64; v for the convergence test), the Jacobian value slots
+    written (FP32 or FP64), the KCL residual written (FP64), and in transient
+    the capacitor history v_prev read. Device values pass through an
+    L2-resident scratch and are not counted."""
+    n, nm, nv, nc = info["n"], info["n_mos"], info["n_slots"], info["n_cap"]
+    b = 8 * nm + 8 * n + 8 * n + (4 if mixed else 8) * nv + 8 * n
+    return b + (8 * nc if tran else 0)
+
+
+def lu_bytes(info, mixed):
+    """Algorithmic HBM bytes of one control-flow + factor/solve pass of one
+    instance (k_lu): the Jacobian value slots and the KCL residual read, x and
+    v read and written back, the state record read and written."""
+    n, nv = info["n"], info["n_slots"]
+    return (4 if mixed else 8) * nv + 8 * n + 4 * 8 * n + 2 * 104
 
 
 def run_karam(args, dist):
@@ -298,11 +312,11 @@ def run_karam(args, dist):
     clocks.start()
     tot_ms = 0.0
     solves = 0
-    eval_ms = 0.0
+    eval_ms = lu_ms = rescue_ms = 0.0
     evals_dc = evals_tran = 0
     launches = 0
-    lu_ms = 0.0
     rescues = 0
+    rounds = 0
     conv_min = ni
     for _ in range(args.steps):
         l2_flush()
@@ -311,11 +325,14 @@ def run_karam(args, dist):
         solves += conv * (TRAN_STEPS + 1)
         eval_ms += t["eval_ms"]
         lu_ms += t["lu_ms"]
+        rescue_ms += t["rescue_ms"]
+        rounds += t["rounds"]
         evals_dc += t["evals_dc"]
         evals_tran += t["evals_tran"]
         rescues += t["rescues"]
         launches += (t["eval_launches"] + t["lu_launches"] + t["rescue_launches"]
                      + t["other_launches"])
+        lanes = t["lanes"]
         conv_min = min(conv_min, conv)
     clk = clocks.stop()
     dist.barrier()
@@ -351,20 +368,214 @@ def run_karam(args, dist):
         e2e_solves += sum(TRAN_STEPS + 1 for s in st if s["status"] == A.ST_CONVERGED)
     e2e_value = dist.sum(e2e_solves) / dist.max(e2e_t)
 
-    # roofline of the evaluation + stamping kernel
-    b_dc, b_tran = eval_bytes(info, mixed=True)
-    eval_bytes_total = evals_dc * b_dc + evals_tran * b_tran
+    # rooflines: evaluation + stamping (k_eval + k_stamp) and factor/solve
+    # (k_lu), algorithmic bytes per live instance-round over their event time
     peak, peak_kind = measured_peaks()
-    achieved = eval_bytes_total / (eval_ms / 1e3) / 1e9 if eval_ms > 0 else 0.0
-    full_launch_bytes = ni * b_tran
+    es_b = evals_dc * eval_stamp_bytes(info, True) + evals_tran * eval_stamp_bytes(info, True, True)
+    lu_b = (evals_dc + evals_tran) * lu_bytes(info, True)
+    es_gbs = es_b / (eval_ms / 1e3) / 1e9 if eval_ms else 0.0
+    lu_gbs = lu_b / (lu_ms / 1e3) / 1e9 if lu_ms else 0.0
+    tot_k = eval_ms + lu_ms + rescue_ms
+    kernels = {
+        "k_eval+k_stamp<float>": {"ms_per_step": eval_ms / args.steps, "share": eval_ms / tot_k,
+                                  "achieved_gbs": es_gbs, "frac": es_gbs / peak,
+                                  "bytes_per_instance_eval": eval_stamp_bytes(info, True, True)},
+        "k_lu<float>": {"ms_per_step": lu_ms / args.steps, "share": lu_ms / tot_k,
+                        "achieved_gbs": lu_gbs, "frac": lu_gbs / peak,
+                        "bytes_per_instance_round": lu_bytes(info, True), "lanes_per_cta": lanes},
+        "k_rescue": {"ms_per_step": rescue_ms / args.steps, "share": rescue_ms / tot_k},
+    }
+    dom = "k_lu<float>" if lu_ms >= eval_ms else "k_eval+k_stamp<float>"
     roofline = {
-        "kernel": "k_eval (device evaluation + stamping)", "bound": "hbm",
+        "kernel": dom, "bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak,
+        "unit": "GB/s", "frac": kernels[dom]["frac"], "peak_source": peak_kind,
+        "traffic": profiled_traffic(dom),
+        "algorithmic_bytes_per_full_launch": ni * (lu_bytes(info, True) if dom == "k_lu<float>"
+                                                   else eval_stamp_bytes(info, True, True)),
+        "avg_launch_us": 1e3 * (lu_ms if dom == "k_lu<float>" else eval_ms) / rounds,
+    }
+
+    # evaluation + stamping alone at full batch (every instance live), CUDA events
+    v_probe = np.repeat(v_mixed[:1], ni, axis=0)
+    es_us = []
+    for _ in range(5):
+        l2_flush()
+        prob.eval_stamp(v_probe, A.PREC_MIXED)
+        es_us.append(1e3 * prob.timing()["eval_ms"])
+    es_us = statistics.median(es_us[1:])
+    es_bytes = ni * eval_stamp_bytes(info, mixed=True)
+    eval_roofline = {"kernel": "k_eval + k_stamp<float>, all instances live", "bound": "hbm",
+                     "achieved": es_bytes / (es_us / 1e6) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": es_bytes / (es_us / 1e6) / 1e9 / peak, "launch_pair_us": es_us,
+                     "algorithmic_bytes": es_bytes}
+
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "MC inverter chain 256 stages + 64 diode clamps, n=322, "
+                               "DC + 200 BE steps of 1 ps", "instances_per_step": count,
+                   "solver": "oracle/_ref: reference sources, solveSparse_LU"
+                   if kind == "reference" else "oracle port (restatement)"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def eval_stamp_bytes(info, mixed, tran=False):
+    """Algorithmic HBM bytes of one evaluation + stamping of one instance
+    (k_eval + k_stamp): KP/VTO read (FP32), the trial point x and the accepted
+    point v read (FP64; v for the convergence test), the Jacobian value slots
+    written (FP32 or FP64), the KCL residual written (FP64), and in transient
+    the capacitor history v_prev read. Device values pass through an
+    L2-resident scratch and are not counted."""
+    n, nm, nv, nc = info["n"], info["n_mos"], info["n_slots"], info["n_cap"]
+    b = 8 * nm + 8 * n + 8 * n + (4 if mixed else 8) * nv + 8 * n
+    return b + (8 * nc if tran else 0)
+
+
+def lu_bytes(info, mixed):
+    """Algorithmic HBM bytes of one control-flow + factor/solve pass of one
+    instance (k_lu): the Jacobian value slots and the KCL residual read, x and
+    v read and written back, the state record read and written."""
+    n, nv = info["n"], info["n_slots"]
+    return (4 if mixed else 8) * nv + 8 * n + 4 * 8 * n + 2 * 104
+
+
+def run_karam(args, dist):
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+
+    ni = args.instances
+    nl, inst = workload(ni, dist.rank * ni)
+    ctx = K.Context(dist.local)
+    prob = K.Problem(ctx, nl, max_instances=ni)
+    prob.set_instances(inst)
+    info = prob.info
+
+    flush = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32,
+                                device=f"cuda:{dist.local}")
+    except Exception:
+        flush = None
+
+    def l2_flush():
+        if flush is not None:
+            flush.zero_()
+            import torch
+            torch.cuda.synchronize()
+
+    def job(opts):
+        prob.run_mc_device(DT, TRAN_STEPS, A.TRAN_BE, opts)
+        t = prob.timing()
+        _, st = prob.read_results()
+        conv = sum(1 for s in st if s["status"] == A.ST_CONVERGED)
+        return t, conv, st
+
+    mixed = K.options(precision=A.PREC_MIXED, max_halvings=MAX_HALVINGS, **POLISH)
+    fp64 = K.options(precision=A.PREC_FP64, max_halvings=MAX_HALVINGS, **POLISH)
+
+    for _ in range(args.warmup):
+        l2_flush()
+        job(mixed)
+
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    clocks.start()
+    tot_ms = 0.0
+    solves = 0
+    eval_ms = lu_ms = rescue_ms = 0.0
+    evals_dc = evals_tran = 0
+    launches = 0
+    rescues = 0
+    rounds = 0
+    conv_min = ni
+    for _ in range(args.steps):
+        l2_flush()
+        t, conv, st = job(mixed)
+        tot_ms += t["job_ms"]
+        solves += conv * (TRAN_STEPS + 1)
+        eval_ms += t["eval_ms"]
+        lu_ms += t["lu_ms"]
+        rescue_ms += t["rescue_ms"]
+        rounds += t["rounds"]
+        evals_dc += t["evals_dc"]
+        evals_tran += t["evals_tran"]
+        rescues += t["rescues"]
+        launches += (t["eval_launches"] + t["lu_launches"] + t["rescue_launches"]
+                     + t["other_launches"])
+        lanes = t["lanes"]
+        conv_min = min(conv_min, conv)
+    clk = clocks.stop()
+    dist.barrier()
+    v_mixed, st_mixed = prob.read_results()
+    t_max = dist.max(tot_ms)
+    all_solves = dist.sum(solves)
+    value = all_solves / (t_max / 1e3)
+
+    # plain FP64 GPU Newton path, same job and timing rules
+    fp_ms = 0.0
+    fp_solves = 0
+    for _ in range(max(1, args.warmup // 3)):
+        job(fp64)
+    for _ in range(args.steps):
+        l2_flush()
+        t, conv, _ = job(fp64)
+        fp_ms += t["job_ms"]
+        fp_solves += conv * (TRAN_STEPS + 1)
+    v_fp64, _ = prob.read_results()
+    fp_value = dist.sum(fp_solves) / (dist.max(fp_ms) / 1e3)
+
+    # end to end through the C ABI with host buffers
+    h2d = inst.mos_kp.nbytes + inst.mos_vto.nbytes
+    d2h = ni * info["n"] * 8 + ni * A.C.sizeof(A.KaramInstanceStats)
+    e2e_t = 0.0
+    e2e_solves = 0
+    for _ in range(args.steps):
+        l2_flush()
+        dist.barrier()
+        t0 = time.perf_counter()
+        v, st = prob.run_mc(inst, DT, TRAN_STEPS, A.TRAN_BE, mixed)
+        e2e_t += time.perf_counter() - t0
+        e2e_solves += sum(TRAN_STEPS + 1 for s in st if s["status"] == A.ST_CONVERGED)
+    e2e_value = dist.sum(e2e_solves) / dist.max(e2e_t)
+
+    # roofline of the dominant kernel: the fused NR round
+    b_dc, b_tran = round_bytes(info)
+    peak, peak_kind = measured_peaks()
+    achieved = (evals_dc * b_dc + evals_tran * b_tran) / (round_ms / 1e3) / 1e9 if round_ms else 0.0
+    roofline = {
+        "kernel": "k_round<float> (evaluation + stamping + control + LU, fused)", "bound": "hbm",
         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "peak_source": peak_kind,
         "traffic": profiled_traffic(),
-        "algorithmic_bytes_per_full_launch": full_launch_bytes,
-        "time_share": eval_ms / (eval_ms + lu_ms) if eval_ms + lu_ms > 0 else None,
+        "algorithmic_bytes_per_instance_round": {"dc": b_dc, "tran": b_tran},
+        "avg_launch_us": 1e3 * round_ms / rounds if rounds else None,
+        "time_share": round_ms / (round_ms + rescue_ms) if round_ms + rescue_ms > 0 else None,
+        "lanes_per_cta": lanes,
     }
+
+    # evaluation + stamping alone at full batch (an evaluation-only launch of
+    # k_round writing the Jacobian and residual to HBM), timed with CUDA events
+    v_probe = np.repeat(v_mixed[:1], ni, axis=0) if len(v_mixed) else None
+    es_us = []
+    for _ in range(5):
+        l2_flush()
+        prob.eval_stamp(v_probe, A.PREC_MIXED)
+        es_us.append(1e3 * prob.timing()["round_ms"])
+    es_us = statistics.median(es_us[1:])
+    es_bytes = ni * eval_stamp_bytes(info, mixed=True)
+    eval_roofline = {"kernel": "k_round<float>, evaluation-only launch", "bound": "hbm",
+                     "achieved": es_bytes / (es_us / 1e6) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": es_bytes / (es_us / 1e6) / 1e9 / peak, "launch_us": es_us,
+                     "algorithmic_bytes_per_launch": es_bytes}
 
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": dist.world,
@@ -386,6 +597,9 @@ def run_karam(args, dist):
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": roofline,
+        "kernels": kernels,
+        "eval_stamp_full_batch": eval_roofline,
+        "rounds_per_step": rounds / args.steps,
         "gpu_launches": launches,
         "rescues_per_step": rescues / args.steps,
         "clocks": clk,

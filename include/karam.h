@@ -155,7 +155,8 @@ typedef struct karam_solver_opts {
                             step; fall back to full GMIN stepping if it has not
                             converged after seed_max_iter iterations              */
   int32_t seed_max_iter; /* K of the seeded fallback                              */
-  int32_t schedule;      /* 0 = autotuned; 1 = thread-per-instance; 2 = warp-per-instance */
+  int32_t schedule;      /* instances per CTA of the factor/solve kernel (1, 2, 4, ..., 32);
+                            0 = chosen from shared memory, occupancy and batch size */
   int32_t max_rounds;    /* device round budget per launch (0 = unlimited)        */
   int32_t max_halvings;  /* transient: a step whose NR exhausts max_nr_iter restarts
                             from the last time point with half the step, at most
@@ -173,7 +174,11 @@ typedef struct karam_problem_info {
   int32_t n_instances;
   int32_t n_mos, n_dio, n_res, n_cap, n_vsrc, n_isrc;
   int32_t lu_ops;      /* scaled + update operations of the LU program           */
-  int32_t lu_jit;      /* 1 when the LU round runs as code compiled for this topology */
+  int32_t n_slots;     /* value slots: filled positions the static-pivot LU can
+                          make non-zero (what the device stores and factors)     */
+  int32_t es_blocks;   /* evaluation + stamping blocks (one CTA each per 32 instances) */
+  int32_t es_device_evals; /* device evaluations per instance and round, counting
+                          devices shared by two blocks twice                     */
 } karam_problem_info;
 
 /* Per-instance counters returned by the solves. */
@@ -184,8 +189,9 @@ typedef struct karam_instance_stats {
   int32_t damped;       /* damping re-evaluations                                 */
   int32_t gmin_step;    /* GMIN step reached (DC)                                 */
   int32_t seeded_ok;    /* 1 if the seeded start converged without fallback       */
-  int32_t rescued;      /* linear solves redone with partial pivoting because the
-                           static pivots of the shared LU program were unusable  */
+  int32_t rescued;      /* linear solves redone by the rescue path (FP64 static
+                           pivots, then dense partial pivoting) because the
+                           static pivots of the working precision were unusable */
   int32_t halvings;     /* transient step halvings after NR failures              */
   int32_t max_step_iters; /* most NR iterations spent on one transient attempt    */
   double residual;      /* final max KCL residual [A]                             */
@@ -211,9 +217,6 @@ KARAM_API int karam_problem_create(karam_ctx *ctx, const karam_netlist *nl,
                                    int32_t max_instances, karam_problem **out);
 KARAM_API void karam_problem_destroy(karam_problem *p);
 KARAM_API int karam_problem_info_get(const karam_problem *p, karam_problem_info *out);
-/* How the LU round runs for this problem: compiled for its topology (NVRTC),
- * or the program interpreter and why. */
-KARAM_API const char *karam_problem_lu_status(const karam_problem *p);
 /* Copies per-instance parameters host -> device (the batch to solve next). */
 KARAM_API int karam_set_instances(karam_problem *p, const karam_instances *inst);
 
@@ -268,6 +271,13 @@ KARAM_API int karam_get_filled_pattern(const karam_problem *p, int32_t *f_row_pt
 /* SoA order of the tensorised devices: soa index -> netlist index. */
 KARAM_API int karam_get_device_order(const karam_problem *p, int32_t *mos_order,
                                      int32_t *dio_order);
+/* The static-pivot LU program on the value slots (permuted space), as the
+ * device runs it: hdr[4 n] = (offset, nL, nU, diagonal slot) per pivot; data
+ * at offset = Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL * nU] (update target
+ * slots); slot_rc[2 n_slots] = (row, col) of every value slot. With data NULL
+ * only *data_len is written. */
+KARAM_API int karam_get_lu_program(const karam_problem *p, int32_t *hdr, int32_t *data,
+                                   int32_t *data_len, int32_t *slot_rc);
 
 /* ---- single-kernel access for measurement and parity ----------------------
  * Runs the evaluation + stamping kernel once for every instance at the given
@@ -277,18 +287,23 @@ KARAM_API int karam_get_device_order(const karam_problem *p, int32_t *mos_order,
  * capacitor companions of the chosen method with history v_prev = i_prev = 0. */
 KARAM_API int karam_eval_stamp(karam_problem *p, int32_t precision, const double *v,
                                double *jac, double *f);
-/* Device-side accounting of the last solve call (CUDA events on the problem's
- * stream; counters kept by the kernels). */
+/* Device-side accounting of the last solve or evaluation call (CUDA events on
+ * the problem's stream; counters kept by the kernels). */
 typedef struct karam_timing {
   double job_ms;            /* first kernel of the call to its last one             */
-  double eval_ms;           /* summed duration of the evaluation + stamping launches */
-  double lu_ms;             /* summed duration of the factor/solve (+ rescue) launches */
-  int32_t rounds;           /* NR rounds (one evaluation + one factor launch each)   */
+  double eval_ms;           /* summed duration of the device evaluation + stamping
+                               launches (one per round)                             */
+  double lu_ms;             /* summed duration of the control flow + factor/solve
+                               launches (one per round)                             */
+  double rescue_ms;         /* summed duration of the rescue launches (one per round) */
+  int32_t rounds;           /* NR rounds                                             */
   int32_t eval_launches, lu_launches, rescue_launches, other_launches;
+  int32_t lanes;            /* instances per CTA of the factor/solve kernel          */
   int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */
-  int64_t rescues;          /* linear solves redone by the partial-pivoting rescue   */
+  int64_t rescues;          /* linear solves redone by the rescue path               */
+  int64_t rescues_dense;    /* of those, the ones that needed dense partial pivoting */
 } karam_timing;
 KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 

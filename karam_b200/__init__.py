@@ -69,10 +69,11 @@ def lib():
         "karam_get_ordering": (C.c_int, [vp, P(C.c_uint32), P(C.c_int32), P(C.c_int32)]),
         "karam_get_filled_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
         "karam_get_device_order": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+        "karam_get_lu_program": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(C.c_int32),
+                                           P(C.c_int32)]),
         "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
                                        P(C.c_double)]),
         "karam_last_timing": (C.c_int, [vp, P(A.KaramTiming)]),
-        "karam_problem_lu_status": (C.c_char_p, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -133,7 +134,6 @@ class Problem:
             raise KaramError(rc, lib().karam_last_error(ctx.h if ctx else None).decode())
         self.h = h
         self.info = self._info()
-        self.info["lu_status"] = lib().karam_problem_lu_status(self.h).decode()
         self.n = self.info["n"]
         self.ni = 1
 
@@ -190,6 +190,19 @@ class Problem:
         self._check(lib().karam_get_device_order(self.h, A.ptr(mo, C.c_int32),
                                                  A.ptr(do, C.c_int32)))
         return mo[: self.info["n_mos"]], do[: self.info["n_dio"]]
+
+    def lu_program(self):
+        """(hdr[n, 4], data, slot_rc[n_slots, 2]) of the static-pivot LU program."""
+        n, nv = self.n, self.info["n_slots"]
+        ln = C.c_int32(0)
+        self._check(lib().karam_get_lu_program(self.h, None, None, C.byref(ln), None))
+        hdr = np.zeros(4 * n, np.int32)
+        data = np.zeros(max(1, ln.value), np.int32)
+        rc = np.zeros(2 * nv, np.int32)
+        self._check(lib().karam_get_lu_program(self.h, A.ptr(hdr, C.c_int32),
+                                               A.ptr(data, C.c_int32), C.byref(ln),
+                                               A.ptr(rc, C.c_int32)))
+        return hdr.reshape(n, 4), data[: ln.value], rc.reshape(nv, 2)
 
     # -- batches and solves -------------------------------------------------
     def set_instances(self, inst: Instances | None):

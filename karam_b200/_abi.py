@@ -65,7 +65,8 @@ class KaramSolverOpts(C.Structure):
 class KaramProblemInfo(C.Structure):
     _fields_ = [(name, C.c_int32) for name in (
         "n", "nnz", "nnz_filled", "fill_in", "treewidth", "n_triplets", "n_instances",
-        "n_mos", "n_dio", "n_res", "n_cap", "n_vsrc", "n_isrc", "lu_ops", "lu_jit")]
+        "n_mos", "n_dio", "n_res", "n_cap", "n_vsrc", "n_isrc", "lu_ops", "n_slots", "es_blocks",
+        "es_device_evals")]
 
 
 class KaramInstanceStats(C.Structure):
@@ -78,10 +79,12 @@ class KaramInstanceStats(C.Structure):
 
 class KaramTiming(C.Structure):
     _fields_ = [("job_ms", C.c_double), ("eval_ms", C.c_double), ("lu_ms", C.c_double),
-                ("rounds", C.c_int32), ("eval_launches", C.c_int32), ("lu_launches", C.c_int32),
-                ("rescue_launches", C.c_int32), ("other_launches", C.c_int32),
-                ("evals_dc", C.c_int64), ("evals_tran", C.c_int64), ("solves", C.c_int64),
-                ("rescues", C.c_int64)]
+                ("rescue_ms", C.c_double), ("rounds", C.c_int32), ("eval_launches", C.c_int32),
+                ("lu_launches", C.c_int32), ("rescue_launches", C.c_int32),
+                ("other_launches", C.c_int32),
+                ("lanes", C.c_int32), ("evals_dc", C.c_int64), ("evals_tran", C.c_int64),
+                ("solves", C.c_int64), ("rescues", C.c_int64),
+                ("rescues_dense", C.c_int64)]
 
 
 def ptr(arr, ctype):

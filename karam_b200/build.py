@@ -14,22 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libkaram_b200.so")
-SOURCES = ["kernels.cu", "topology.cpp", "abi.cpp", "jit.cpp"]
-JIT_INC = os.path.join(CSRC, "jit_sources.inc")
-
-
-def write_jit_sources():
-    """Embeds nr_types.h and nr_device.cuh as string literals for the run-time
-    compiled LU round (jit.cpp)."""
-    parts = []
-    for var, fname in (("kNrTypesSource", "nr_types.h"), ("kNrDeviceSource", "nr_device.cuh")):
-        text = open(os.path.join(CSRC, fname)).read()
-        assert ")KARAMSRC\"" not in text
-        parts.append(f'static const char {var}[] = R"KARAMSRC({text})KARAMSRC";\n')
-    new = "// generated by karam_b200/build.py from nr_types.h and nr_device.cuh\n" + "".join(parts)
-    if not os.path.exists(JIT_INC) or open(JIT_INC).read() != new:
-        with open(JIT_INC, "w") as fh:
-            fh.write(new)
+SOURCES = ["kernels.cu", "topology.cpp", "abi.cpp"]
 HEADERS = ["device.hpp", "topology.hpp", "nr_types.h", "nr_device.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -55,11 +40,10 @@ def build(force=False, verbose=False):
     """Compiles libkaram_b200.so when a source is newer than the library."""
     if not force and not _stale():
         return LIB
-    write_jit_sources()
     cmd = [nvcc(), "-O3", "-std=c++17", "-shared", "-lineinfo", *ARCH,
            "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
            "-Xptxas", "-v", "-I", os.path.join(ROOT, "include"),
-           "-o", LIB + ".tmp", *[os.path.join(CSRC, f) for f in SOURCES], "-ldl"]
+           "-o", LIB + ".tmp", *[os.path.join(CSRC, f) for f in SOURCES]]
     res = subprocess.run(cmd, capture_output=True, text=True)
     log = os.path.join(HERE, "build.log")
     with open(log, "w") as fh:

@@ -81,13 +81,15 @@ struct karam_problem {
 
   // topology buffers
   DBuf t_mos_term, t_mos_geo, t_mos_pmos, t_dio_term, t_dio_par, t_res_term, t_res_g, t_cap_term,
-      t_cap_c, t_mos_card, t_f_row, t_f_colp, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse, t_is_term, t_is_amp, t_jt_off, t_jt_code,
-      t_jlin, t_jcap_off, t_jcap_code, t_ft_off, t_ft_code, t_lu_hdr, t_lu_data, t_seed_vs,
-      t_seed_anode, t_perm;
+      t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
+      t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
+      t_es_jt, t_es_ft, t_es_fc, t_lu_hdr, t_lu_data, t_lu_rec, t_seed_vs, t_seed_anode, t_perm;
   DevTopo dt{};
-  // instance buffers
-  DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_Fmax, i_J, i_cvp, i_cip, i_st, i_seed,
-      i_out, d_active, r_ws, r_list, r_count, i_vtp, d_counters;
+  // instance buffers, [item][ld] (instance-interleaved)
+  int ld = 0;
+  DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
+      i_redf, i_reddv, i_redfl, i_evt, i_evh,
+      d_active, r_ws, r_list, r_count, i_vtp, d_counters;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   int* h_active = nullptr;  // pinned
@@ -95,11 +97,9 @@ struct karam_problem {
   // accounting of the last solve call
   karam_timing timing{};
 
-  std::vector<int> csr_to_f;  // CSR position -> filled position
-  JitLu jit;                  // LU round compiled for this topology
+  std::vector<int> csr_to_slot;  // CSR position -> value slot (-1: structurally zero)
 
   ~karam_problem() {
-    jit_release(jit);
     if (h_active) cudaFreeHost(h_active);
     if (ev_job0) cudaEventDestroy(ev_job0);
     if (ev_job1) cudaEventDestroy(ev_job1);
@@ -206,27 +206,35 @@ void upload_topology(karam_problem* p) {
   upload(p->t_vs_pulse, vpulse);
   upload(p->t_is_term, itm);
   upload(p->t_is_amp, ia);
-  upload(p->t_jt_off, T.jt_off);
-  upload(p->t_jt_code, T.jt_code);
   upload(p->t_jlin, T.jlin_dc);
   upload(p->t_jcap_off, T.jcap_off);
   upload(p->t_jcap_code, T.jcap_code);
-  upload(p->t_ft_off, T.ft_off);
-  upload(p->t_ft_code, T.ft_code);
+  {
+    auto int4s = [](const std::vector<int>& v) {
+      std::vector<int4> o(v.size() / 4);
+      for (size_t k = 0; k < o.size(); ++k) o[k] = make_int4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+      return o;
+    };
+    upload(p->t_es_block, int4s(T.es_block));
+    upload(p->t_es_item, int4s(T.es_item));
+    upload(p->t_es_ft, int4s(T.es_ft));
+  }
+  upload(p->t_es_dev, T.es_dev);
+  upload(p->t_es_jt, T.es_jt);
+  upload(p->t_es_fc, T.es_fc);
   upload(p->t_lu_hdr, hdr);
   upload(p->t_lu_data, T.lu_data);
+  upload(p->t_lu_rec, T.lu_rec);
   upload(p->t_seed_vs, seed_vs);
   upload(p->t_seed_anode, seed_an);
   upload(p->t_perm, T.perm);
-  std::vector<int> frow(T.nnz_filled());
-  for (int i = 0; i < T.n; ++i)
-    for (int k = T.f_row_ptr[i]; k < T.f_row_ptr[i + 1]; ++k) frow[k] = i;
-  upload(p->t_f_row, frow);
-  upload(p->t_f_colp, T.f_col);
+  std::vector<int2> src;
+  for (int s = 0; s < T.nv; ++s) src.push_back(make_int2(T.slot_row[s], T.slot_col[s]));
+  upload(p->t_slot_rc, src);
 
   DevTopo& d = p->dt;
   d.n = T.n;
-  d.nf = T.nnz_filled();
+  d.nv = T.nv;
   d.n_mos = (int)T.mos.size();
   d.n_dio = (int)T.dio.size();
   d.n_res = (int)T.res.size();
@@ -252,47 +260,62 @@ void upload_topology(karam_problem* p) {
   d.vs_pulse = p->t_vs_pulse.as<double>();
   d.is_term = p->t_is_term.as<int2>();
   d.is_amp = p->t_is_amp.as<double>();
-  d.jt_off = p->t_jt_off.as<int>();
-  d.jt_code = p->t_jt_code.as<int>();
   d.jlin_dc = p->t_jlin.as<double>();
   d.jcap_off = p->t_jcap_off.as<int>();
   d.jcap_code = p->t_jcap_code.as<int>();
-  d.ft_off = p->t_ft_off.as<int>();
-  d.ft_code = p->t_ft_code.as<int>();
+  d.n_es_blocks = (int)T.es_block.size() / 4;
+  d.es_block = p->t_es_block.as<int4>();
+  d.es_item = p->t_es_item.as<int4>();
+  d.es_dev = p->t_es_dev.as<int>();
+  d.es_jt = p->t_es_jt.as<int>();
+  d.es_ft = p->t_es_ft.as<int4>();
+  d.es_fc = p->t_es_fc.as<double>();
   d.lu_hdr = p->t_lu_hdr.as<int4>();
   d.lu_data = p->t_lu_data.as<int>();
-  d.f_row = p->t_f_row.as<int>();
-  d.f_colp = p->t_f_colp.as<int>();
+  d.lu_small = T.lu_small ? 1 : 0;
+  d.lu_rec = T.lu_small ? p->t_lu_rec.as<int4>() : nullptr;
+  d.slot_rc = p->t_slot_rc.as<int2>();
   d.seed_vs = p->t_seed_vs.as<int>();
   d.seed_anode = p->t_seed_anode.as<int>();
   d.n_seed_anode = (int)seed_an.size();
 
-  // CSR position -> filled position (for karam_eval_stamp)
-  p->csr_to_f.assign(T.nnz(), -1);
-  for (size_t k = 0; k < T.trip.size(); ++k) p->csr_to_f[T.slot_csr[k]] = T.trip[k].f;
+  // CSR position -> value slot (for karam_eval_stamp)
+  p->csr_to_slot.assign(T.nnz(), -1);
+  for (size_t k = 0; k < T.trip.size(); ++k) p->csr_to_slot[T.slot_csr[k]] = T.f_slot[T.trip[k].f];
 }
 
 void alloc_instances(karam_problem* p) {
   const Topology& T = p->topo;
   const size_t M = (size_t)p->max_inst, n = T.n, nm = T.mos.size(), nv = T.vs.size();
-  p->i_kp.alloc(std::max<size_t>(1, M * nm) * sizeof(float));
-  p->i_vth.alloc(std::max<size_t>(1, M * nm) * sizeof(float));
-  p->i_vsdc.alloc(std::max<size_t>(1, M * nv) * sizeof(double));
-  p->i_v1.alloc(std::max<size_t>(1, M * nv) * sizeof(double));
-  p->i_v2.alloc(std::max<size_t>(1, M * nv) * sizeof(double));
-  p->i_v.alloc(M * n * sizeof(double));
-  p->i_x.alloc(M * n * sizeof(double));
-  p->i_F.alloc(M * n * sizeof(double));
-  p->i_Fmax.alloc(M * sizeof(double));
-  p->i_J.alloc(M * (size_t)T.nnz_filled() * sizeof(double));
-  p->i_cvp.alloc(std::max<size_t>(1, M * T.cap.size()) * sizeof(double));
-  p->i_cip.alloc(std::max<size_t>(1, M * T.cap.size()) * sizeof(double));
+  p->ld = lane_stride(p->max_inst);
+  const size_t ld = (size_t)p->ld;
+  p->i_kp.alloc(std::max<size_t>(1, ld * nm) * sizeof(float));
+  p->i_vth.alloc(std::max<size_t>(1, ld * nm) * sizeof(float));
+  p->i_vsdc.alloc(std::max<size_t>(1, ld * nv) * sizeof(double));
+  p->i_v1.alloc(std::max<size_t>(1, ld * nv) * sizeof(double));
+  p->i_v2.alloc(std::max<size_t>(1, ld * nv) * sizeof(double));
+  p->i_v.alloc(ld * n * sizeof(double));
+  p->i_x.alloc(ld * n * sizeof(double));
+  p->i_F.alloc(ld * n * sizeof(double));
+  p->i_J.alloc(std::max<size_t>(1, ld * (size_t)T.nv) * sizeof(double));
+  p->i_redf.alloc(ld * sizeof(unsigned long long));
+  p->i_reddv.alloc(ld * sizeof(unsigned long long));
+  p->i_redfl.alloc(ld * sizeof(int));
+  p->i_evt.alloc(ld * sizeof(double));
+  p->i_evh.alloc(ld * sizeof(double));
+  {
+    // lanes beyond the batch never evaluate
+    std::vector<double> neg(ld, -1.0);
+    ck(cudaMemcpy(p->i_evh.p, neg.data(), ld * sizeof(double), cudaMemcpyHostToDevice), "init ev");
+  }
+  p->i_cvp.alloc(std::max<size_t>(1, ld * T.cap.size()) * sizeof(double));
+  p->i_cip.alloc(std::max<size_t>(1, ld * T.cap.size()) * sizeof(double));
   p->i_st.alloc(M * sizeof(InstState));
-  p->i_seed.alloc(M * n * sizeof(double));
-  p->i_vtp.alloc(M * n * sizeof(double));
-  p->i_out.alloc(M * n * sizeof(double));
+  p->i_seed.alloc(ld * n * sizeof(double));
+  p->i_vtp.alloc(ld * n * sizeof(double));
+  p->i_out.alloc(ld * n * sizeof(double));
   p->d_active.alloc(sizeof(int));
-  p->d_counters.alloc(4 * sizeof(unsigned long long));
+  p->d_counters.alloc(5 * sizeof(unsigned long long));
   ck(cudaEventCreate(&p->ev_job0), "cudaEventCreate");
   ck(cudaEventCreate(&p->ev_job1), "cudaEventCreate");
   // Partial-pivoting rescue: one dense n x n FP64 workspace per concurrently
@@ -313,6 +336,7 @@ void alloc_instances(karam_problem* p) {
 DevInst dev_inst(karam_problem* p) {
   DevInst I{};
   I.ni = p->ni;
+  I.ld = p->ld;
   I.kp = p->inst_kp ? p->i_kp.as<float>() : nullptr;
   I.vth = p->inst_vth ? p->i_vth.as<float>() : nullptr;
   I.vs_dc = p->i_vsdc.as<double>();
@@ -321,8 +345,12 @@ DevInst dev_inst(karam_problem* p) {
   I.v = p->i_v.as<double>();
   I.x = p->i_x.as<double>();
   I.F = p->i_F.as<double>();
-  I.Fmax = p->i_Fmax.as<double>();
   I.J = p->i_J.p;
+  I.red_f = p->i_redf.as<unsigned long long>();
+  I.red_dv = p->i_reddv.as<unsigned long long>();
+  I.red_flags = p->i_redfl.as<int>();
+  I.ev_t = p->i_evt.as<double>();
+  I.ev_heff = p->i_evh.as<double>();
   I.cap_vp = p->i_cvp.as<double>();
   I.cap_ip = p->i_cip.as<double>();
   I.v_tp = p->i_vtp.as<double>();
@@ -344,14 +372,15 @@ void set_instances_impl(karam_problem* p, const karam_instances* inst) {
   const Topology& T = p->topo;
   int ni = inst ? inst->n_instances : 1;
   if (ni < 1 || ni > p->max_inst) throw std::runtime_error("n_instances out of range");
-  const size_t nm = T.mos.size(), nv = T.vs.size();
-  std::vector<float> kp((size_t)ni * nm), vth((size_t)ni * nm);
-  std::vector<double> vdc((size_t)ni * nv), v1((size_t)ni * nv), v2((size_t)ni * nv);
+  const size_t nm = T.mos.size(), nv = T.vs.size(), ld = (size_t)p->ld;
+  // instance-interleaved: item k of instance i at [k * ld + i]
+  std::vector<float> kp(ld * nm, 0.0f), vth(ld * nm, 0.0f);
+  std::vector<double> vdc(ld * nv, 0.0), v1(ld * nv, 0.0), v2(ld * nv, 0.0);
   for (int i = 0; i < ni; ++i) {
     for (size_t j = 0; j < nm; ++j) {
       const size_t src = (size_t)i * nm + T.mos_order[j];
-      kp[(size_t)i * nm + j] = (inst && inst->mos_kp) ? inst->mos_kp[src] : (float)T.mos[j].kp_card;
-      vth[(size_t)i * nm + j] = (inst && inst->mos_vto) ? inst->mos_vto[src] : (float)T.mos[j].vto_card;
+      kp[j * ld + i] = (inst && inst->mos_kp) ? inst->mos_kp[src] : (float)T.mos[j].kp_card;
+      vth[j * ld + i] = (inst && inst->mos_vto) ? inst->mos_vto[src] : (float)T.mos[j].vto_card;
     }
     for (size_t s = 0; s < nv; ++s) {
       const auto& V = T.vs[s];
@@ -360,9 +389,9 @@ void set_instances_impl(karam_problem* p, const karam_instances* inst) {
         dc = inst->vs_dc[(size_t)i * nv + s];
         if (V.dc != 0.0) sc = dc / V.dc;
       }
-      vdc[(size_t)i * nv + s] = dc;
-      v1[(size_t)i * nv + s] = V.kind == KARAM_SRC_PULSE ? V.pulse[0] * sc : dc;
-      v2[(size_t)i * nv + s] = V.kind == KARAM_SRC_PULSE ? V.pulse[1] * sc : dc;
+      vdc[s * ld + i] = dc;
+      v1[s * ld + i] = V.kind == KARAM_SRC_PULSE ? V.pulse[0] * sc : dc;
+      v2[s * ld + i] = V.kind == KARAM_SRC_PULSE ? V.pulse[1] * sc : dc;
     }
   }
   // Without per-instance values the kernel reads the FP64 model-card table.
@@ -415,22 +444,22 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
 }
 
 // Runs NR rounds until every instance is done (or the round budget ends).
-// Rounds are captured in a CUDA graph of kRounds (eval, lu) pairs with event
-// records around each kernel; the last round's LU kernel counts the live
-// instances into d_active, which is read back after every replay.
-void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
+// Rounds (k_eval, k_stamp, k_lu, k_rescue) are captured in a CUDA graph of
+// kRounds rounds with event records between the phases; the last k_lu of the
+// graph counts the live instances into d_active, which is read back after
+// every replay.
+void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_lanes,
                 const DevInst* inst = nullptr) {
   constexpr int kRounds = 16;
   cudaStream_t s = p->ctx->stream;
   DevInst I = inst ? *inst : dev_inst(p);
   const int prec = P.precision;
-  LuLaunch L = plan_lu(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms);
-  if (L.ni_per_cta < 1)
-    throw std::runtime_error("instance too large for the thread-per-instance schedule");
-  configure_kernels(p->dt, L);
-  configure_jit(p->jit, L);
+  RoundLaunch L = plan_round(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms, want_lanes);
+  if (L.L < 1)
+    throw std::runtime_error("one instance's matrix does not fit the shared memory of a CTA");
   ck(cudaGetLastError(), "configure kernels");
-  std::vector<cudaEvent_t> ev(3 * kRounds);
+  p->timing.lanes = L.L;
+  std::vector<cudaEvent_t> ev(4 * kRounds);
   for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
   struct EvGuard {
     std::vector<cudaEvent_t>& v;
@@ -446,16 +475,15 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
   // External event records become event-record nodes of the graph (a plain
   // record inside capture would only order work within the capture).
   for (int r = 0; r < kRounds; ++r) {
-    cudaEventRecordWithFlags(ev[3 * r], s, cudaEventRecordExternal);
-    launch_eval(p->dt, I, P, prec, s);
-    cudaEventRecordWithFlags(ev[3 * r + 1], s, cudaEventRecordExternal);
     if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
-    if (p->jit.ok)
-      launch_lu_jit(p->jit, p->dt, I, P, L, prec, active, s);
-    else
-      launch_lu(p->dt, I, P, L, prec, active, s);
-    if (I.rescue_list) launch_rescue(p->dt, I, P, prec, I.rescue_slots, s);
-    cudaEventRecordWithFlags(ev[3 * r + 2], s, cudaEventRecordExternal);
+    if (I.rescue_count) cudaMemsetAsync(I.rescue_count, 0, sizeof(int), s);
+    cudaEventRecordWithFlags(ev[4 * r], s, cudaEventRecordExternal);
+    launch_eval_stamp(p->dt, I, P, L, prec, s);
+    cudaEventRecordWithFlags(ev[4 * r + 1], s, cudaEventRecordExternal);
+    launch_lu(p->dt, I, P, L, prec, active, s);
+    cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
+    if (I.rescue_list) launch_rescue(p->dt, I, P, I.rescue_slots, s);
+    cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
   }
   const cudaError_t launch_err = cudaGetLastError();
   ck(cudaStreamEndCapture(s, &graph), "end capture");
@@ -476,11 +504,13 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds,
     ck(cudaMemcpyAsync(p->h_active, active, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
     ck(cudaStreamSynchronize(s), "round sync");
     for (int r = 0; r < kRounds; ++r) {
-      float a = 0, b = 0;
-      ck(cudaEventElapsedTime(&a, ev[3 * r], ev[3 * r + 1]), "event time");
-      ck(cudaEventElapsedTime(&b, ev[3 * r + 1], ev[3 * r + 2]), "event time");
+      float a = 0, b = 0, c = 0;
+      ck(cudaEventElapsedTime(&a, ev[4 * r], ev[4 * r + 1]), "event time");
+      ck(cudaEventElapsedTime(&b, ev[4 * r + 1], ev[4 * r + 2]), "event time");
+      ck(cudaEventElapsedTime(&c, ev[4 * r + 2], ev[4 * r + 3]), "event time");
       p->timing.eval_ms += a;
       p->timing.lu_ms += b;
+      p->timing.rescue_ms += c;
     }
     p->timing.eval_launches += kRounds;
     p->timing.lu_launches += kRounds;
@@ -513,7 +543,8 @@ void read_stats(karam_problem* p, karam_instance_stats* stats, bool dc_only) {
 void read_voltages(karam_problem* p, double* out_v) {
   if (!out_v) return;
   const int n = p->topo.n;
-  unpermute(p->i_v.as<double>(), p->t_perm.as<int>(), p->i_out.as<double>(), p->ni, n, p->ctx->stream);
+  unpermute(p->i_v.as<double>(), p->t_perm.as<int>(), p->i_out.as<double>(), p->ni, p->ld, n,
+            p->ctx->stream);
   ck(cudaMemcpyAsync(out_v, p->i_out.p, (size_t)p->ni * n * sizeof(double), cudaMemcpyDeviceToHost,
                      p->ctx->stream),
      "D2H v");
@@ -524,13 +555,13 @@ void read_voltages(karam_problem* p, double* out_v) {
 // first kernel of a solve call; end_job records the end event and reads back.
 void begin_job(karam_problem* p) {
   p->timing = karam_timing{};
-  ck(cudaMemsetAsync(p->d_counters.p, 0, 4 * sizeof(unsigned long long), p->ctx->stream), "memset counters");
+  ck(cudaMemsetAsync(p->d_counters.p, 0, 5 * sizeof(unsigned long long), p->ctx->stream), "memset counters");
   ck(cudaEventRecord(p->ev_job0, p->ctx->stream), "event record");
 }
 
 void end_job(karam_problem* p) {
   ck(cudaEventRecord(p->ev_job1, p->ctx->stream), "event record");
-  unsigned long long c[4];
+  unsigned long long c[5];
   ck(cudaMemcpyAsync(c, p->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost, p->ctx->stream), "D2H counters");
   ck(cudaStreamSynchronize(p->ctx->stream), "job sync");
   float ms = 0;
@@ -540,19 +571,21 @@ void end_job(karam_problem* p) {
   p->timing.evals_tran = (int64_t)c[1];
   p->timing.solves = (int64_t)c[2];
   p->timing.rescues = (int64_t)c[3];
+  p->timing.rescues_dense = (int64_t)c[4];
 }
 
 void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
   DevInst I = dev_inst(p);
   if (P.seeded && seed_v) {
-    // caller guesses arrive in node order; the device works in permuted order
+    // caller guesses arrive instance-major in node order; the device works
+    // instance-interleaved in permuted order
     const int n = p->topo.n;
-    std::vector<double> perm_seed((size_t)p->ni * n);
-    for (int i = 0; i < p->ni; ++i)
-      for (int k = 0; k < n; ++k) perm_seed[(size_t)i * n + k] = seed_v[(size_t)i * n + p->topo.perm[k]];
-    ck(cudaMemcpyAsync(p->i_seed.p, perm_seed.data(), perm_seed.size() * sizeof(double),
+    ck(cudaMemcpyAsync(p->i_out.p, seed_v, (size_t)p->ni * n * sizeof(double),
                        cudaMemcpyHostToDevice, p->ctx->stream),
        "H2D seed");
+    interleave(p->i_out.as<double>(), p->t_perm.as<int>(), p->i_seed.as<double>(), p->ni, p->ld,
+               n, p->ctx->stream);
+    p->timing.other_launches += 1;
     I.seed = p->i_seed.as<double>();
   }
   launch_init(p->dt, I, P, p->ctx->stream);
@@ -638,18 +671,12 @@ int karam_problem_create(karam_ctx* ctx, const karam_netlist* nl, int32_t max_in
     upload_topology(p.get());
     alloc_instances(p.get());
     set_instances_impl(p.get(), nullptr);
-    jit_build(p->topo, p->jit);
     *out = p.release();
     return KARAM_OK;
   });
 }
 
 void karam_problem_destroy(karam_problem* p) { delete p; }
-
-const char* karam_problem_lu_status(const karam_problem* p) {
-  if (!p) return "";
-  return p->jit.ok ? "straight-line LU compiled for this topology" : p->jit.status.c_str();
-}
 
 int karam_problem_info_get(const karam_problem* p, karam_problem_info* o) {
   if (!p || !o) return KARAM_E_INVALID;
@@ -668,7 +695,9 @@ int karam_problem_info_get(const karam_problem* p, karam_problem_info* o) {
   o->n_vsrc = (int)T.vs.size();
   o->n_isrc = (int)T.isrc.size();
   o->lu_ops = T.lu_ops;
-  o->lu_jit = p->jit.ok ? 1 : 0;
+  o->n_slots = T.nv;
+  o->es_blocks = (int32_t)T.es_block.size() / 4;
+  o->es_device_evals = (int32_t)T.es_dev.size();
   return KARAM_OK;
 }
 
@@ -690,7 +719,7 @@ int karam_solve_dc(karam_problem* p, const karam_solver_opts* opts, const double
     if (P.seeded && !seed_v) throw std::runtime_error("seeded solve without seed_v");
     begin_job(p);
     start_job(p, P, seed_v);
-    run_rounds(p, P, opts ? opts->max_rounds : 0);
+    run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
     end_job(p);
     p->have_dc = true;
     read_voltages(p, out_v);
@@ -708,7 +737,7 @@ int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double 
     if (P.seeded) throw std::runtime_error("seeded starts need karam_solve_dc");
     begin_job(p);
     start_job(p, P, nullptr);
-    run_rounds(p, P, opts ? opts->max_rounds : 0);
+    run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
     end_job(p);
     p->have_dc = true;
     return KARAM_OK;
@@ -768,10 +797,10 @@ int karam_step_transient(karam_problem* p, const karam_solver_opts* opts, double
     I.n_wave = n_wave;
     I.wave_steps = n_steps;
     begin_job(p);
-    launch_tran_start(p->dt, I, p->tran_started ? 0 : 1, p->ctx->stream);
+    launch_tran_start(p->dt, I, P, p->tran_started ? 0 : 1, p->ctx->stream);
     ck(cudaGetLastError(), "tran start");
     p->timing.other_launches += 1;
-    run_rounds(p, P, opts ? opts->max_rounds : 0, &I);
+    run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0, &I);
     end_job(p);
     p->tran_started = true;
     p->tran_h = dt;
@@ -829,50 +858,82 @@ int karam_get_device_order(const karam_problem* p, int32_t* mos_order, int32_t* 
   return KARAM_OK;
 }
 
+int karam_get_lu_program(const karam_problem* p, int32_t* hdr, int32_t* data, int32_t* data_len,
+                         int32_t* slot_rc) {
+  if (!p) return KARAM_E_INVALID;
+  const Topology& T = p->topo;
+  if (hdr) std::copy(T.lu_hdr.begin(), T.lu_hdr.end(), hdr);
+  if (data_len) *data_len = (int32_t)T.lu_data.size();
+  if (data) std::copy(T.lu_data.begin(), T.lu_data.end(), data);
+  if (slot_rc)
+    for (int s = 0; s < T.nv; ++s) {
+      slot_rc[2 * s] = T.slot_row[s];
+      slot_rc[2 * s + 1] = T.slot_col[s];
+    }
+  return KARAM_OK;
+}
+
 int karam_eval_stamp(karam_problem* p, int32_t precision, const double* v, double* jac, double* f) {
   if (!p || !v) return KARAM_E_INVALID;
   return guarded(p->ctx, [&] {
     need_device(p);
+    if (precision != KARAM_PREC_FP64 && precision != KARAM_PREC_MIXED)
+      throw std::runtime_error("unknown precision");
     const Topology& T = p->topo;
-    const int n = T.n, nf = T.nnz_filled(), ni = p->ni;
-    std::vector<double> vp((size_t)ni * n);
-    for (int i = 0; i < ni; ++i)
-      for (int k = 0; k < n; ++k) vp[(size_t)i * n + k] = v[(size_t)i * n + T.perm[k]];
+    const int n = T.n, nvs = T.nv, ni = p->ni;
+    const size_t ld = (size_t)p->ld;
     cudaStream_t s = p->ctx->stream;
-    ck(cudaMemcpyAsync(p->i_x.p, vp.data(), vp.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D x");
-    std::vector<InstState> st(ni);
-    for (auto& e : st) {
-      e = InstState{};
-      e.mode = MODE_DC;
-    }
-    ck(cudaMemcpyAsync(p->i_st.p, st.data(), st.size() * sizeof(InstState), cudaMemcpyHostToDevice, s), "H2D st");
+    ck(cudaMemcpyAsync(p->i_out.p, v, (size_t)ni * n * sizeof(double), cudaMemcpyHostToDevice, s), "H2D v");
+    interleave(p->i_out.as<double>(), p->t_perm.as<int>(), p->i_x.as<double>(), ni, p->ld, n, s);
+    // every instance evaluates a DC point
+    std::vector<double> evh(ld, -1.0), evt(ld, 0.0);
+    std::fill(evh.begin(), evh.begin() + ni, 0.0);
+    ck(cudaMemcpyAsync(p->i_evh.p, evh.data(), ld * sizeof(double), cudaMemcpyHostToDevice, s), "H2D ev");
+    ck(cudaMemcpyAsync(p->i_evt.p, evt.data(), ld * sizeof(double), cudaMemcpyHostToDevice, s), "H2D ev");
     JobParams P = job_params(nullptr, 0, 0.0, KARAM_TRAN_BE);
+    P.precision = precision;
     DevInst I = dev_inst(p);
-    configure_kernels(p->dt, plan_lu(p->dt, ni, precision, p->ctx->max_smem, p->ctx->num_sms));
-    launch_eval(p->dt, I, P, precision, s);
+    const RoundLaunch L = plan_round(p->dt, ni, precision, p->ctx->max_smem, p->ctx->num_sms, 0);
+    p->timing = karam_timing{};
+    ck(cudaEventRecord(p->ev_job0, s), "event record");
+    launch_eval_stamp(p->dt, I, P, L, precision, s);
     ck(cudaGetLastError(), "eval launch");
-    std::vector<double> F((size_t)ni * n);
+    ck(cudaEventRecord(p->ev_job1, s), "event record");
+    std::vector<double> F((size_t)n * ld);
     ck(cudaMemcpyAsync(F.data(), p->i_F.p, F.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H F");
     std::vector<double> J64;
     std::vector<float> J32;
     if (precision == KARAM_PREC_MIXED) {
-      J32.resize((size_t)ni * nf);
+      J32.resize((size_t)nvs * ld);
       ck(cudaMemcpyAsync(J32.data(), p->i_J.p, J32.size() * sizeof(float), cudaMemcpyDeviceToHost, s), "D2H J");
     } else {
-      J64.resize((size_t)ni * nf);
+      J64.resize((size_t)nvs * ld);
       ck(cudaMemcpyAsync(J64.data(), p->i_J.p, J64.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H J");
     }
     ck(cudaStreamSynchronize(s), "eval sync");
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, p->ev_job0, p->ev_job1), "eval time");
+    p->timing.job_ms = p->timing.eval_ms = ms;
+    p->timing.eval_launches = 1;
+    p->timing.other_launches = 1;  // the interleave of the caller's voltages
+    // the device state no longer holds a solution
     p->have_dc = false;
+    std::vector<double> neg(ld, -1.0);
+    ck(cudaMemcpy(p->i_evh.p, neg.data(), ld * sizeof(double), cudaMemcpyHostToDevice), "reset ev");
     const int nnz = T.nnz();
     for (int i = 0; i < ni; ++i) {
       if (jac)
         for (int j = 0; j < nnz; ++j) {
-          const size_t src = (size_t)i * nf + p->csr_to_f[j];
-          jac[(size_t)i * nnz + j] = precision == KARAM_PREC_MIXED ? (double)J32[src] : J64[src];
+          const int sl = p->csr_to_slot[j];
+          double val = 0.0;
+          if (sl >= 0) {
+            const size_t src = (size_t)sl * ld + i;
+            val = precision == KARAM_PREC_MIXED ? (double)J32[src] : J64[src];
+          }
+          jac[(size_t)i * nnz + j] = val;
         }
       if (f)
-        for (int k = 0; k < n; ++k) f[(size_t)i * n + T.perm[k]] = F[(size_t)i * n + k];
+        for (int k = 0; k < n; ++k) f[(size_t)i * n + T.perm[k]] = F[(size_t)k * ld + i];
     }
     return KARAM_OK;
   });

@@ -4,57 +4,48 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
-#include <string>
 
 #include "nr_types.h"
 
 namespace karam {
 
-struct Topology;
-
-// Launch geometry of the LU round: NI instances per CTA, one lane each.
-struct LuLaunch {
-  int ni_per_cta;  // instances per CTA
-  int S;           // odd stride of the value rows
-  int Sv;          // odd stride of the vector rows
-  size_t smem;     // dynamic shared memory bytes
-  int grid;
+// Launch geometry of the factor/solve kernel of an NR round: one CTA per tile
+// of L instances.
+struct RoundLaunch {
+  int L = 0;          // lanes (instances) per CTA, a power of two <= 32
+  int grid = 0;       // CTAs
+  size_t smem = 0;    // dynamic shared memory bytes (value slots + right-hand side)
+  int ctas_per_sm = 0;
 };
 
+// Lane stride of the instance-interleaved arrays for ni instances.
+inline int lane_stride(int ni) { return (ni + 31) / 32 * 32; }
+
+// Picks L (or takes `want_lanes` when it is a valid power of two) so the
+// tiles fit shared memory and spread over the SMs in the fewest waves;
+// sets the kernels' shared-memory limits (call outside stream capture).
+RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num_sms,
+                       int want_lanes);
 void launch_init(const DevTopo& T, const DevInst& I, const JobParams& P, cudaStream_t s);
 // Moves every converged instance into the transient at step 1 (capacitor
 // history from the accepted point when init_caps).
-void launch_tran_start(const DevTopo& T, const DevInst& I, int init_caps, cudaStream_t s);
-void launch_eval(const DevTopo& T, const DevInst& I, const JobParams& P, int prec,
-                 cudaStream_t s);
-void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const LuLaunch& L,
+void launch_tran_start(const DevTopo& T, const DevInst& I, const JobParams& P, int init_caps,
+                       cudaStream_t s);
+// Device evaluation + stamping of every live instance at x (k_es): Jacobian
+// value slots, KCL residual and the per-instance reductions.
+void launch_eval_stamp(const DevTopo& T, const DevInst& I, const JobParams& P,
+                       const RoundLaunch& L, int prec, cudaStream_t s);
+// Control flow + static-pivot factor/solve of every live instance (k_lu).
+void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const RoundLaunch& L,
                int prec, int* active, cudaStream_t s);
-size_t eval_smem_bytes(const DevTopo& T);
-// Sets the dynamic shared-memory limits of the kernels (call outside stream capture).
-void configure_kernels(const DevTopo& T, const LuLaunch& L);
-LuLaunch plan_lu(const DevTopo& T, int ni, int prec, int max_smem, int num_sms);
-void unpermute(const double* v_perm, const int* perm, double* out, int ni, int n, cudaStream_t s);
-// Dense FP64 partial-pivoting solves for the instances the LU kernel flagged.
-void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, int prec, int grid,
+// Rescue of the solves whose static pivots failed (FP64 static, then dense
+// partial pivoting); one CTA per workspace slot.
+void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, int grid,
                    cudaStream_t s);
 size_t rescue_smem_bytes(const DevTopo& T);
-
-// ---- LU round compiled at run time for one topology (jit.cpp) --------------
-// Straight-line factor + solve code generated from the topology's LU program,
-// compiled with NVRTC for sm_100a together with nr_device.cuh and loaded as a
-// CUDA library. The interpreter is used when NVRTC is unavailable.
-struct JitLu {
-  bool ok = false;
-  std::string status;          // "ready", or why the interpreter is used
-  void* kernel_f32 = nullptr;  // cudaKernel_t
-  void* kernel_f64 = nullptr;
-  void* library = nullptr;     // cudaLibrary_t
-  double compile_ms = 0.0;
-};
-void jit_build(const Topology& T, JitLu& out);
-void jit_release(JitLu& j);
-void launch_lu_jit(const JitLu& J, const DevTopo& T, const DevInst& I, const JobParams& P,
-                   const LuLaunch& L, int prec, int* active, cudaStream_t s);
-void configure_jit(const JitLu& J, const LuLaunch& L);
+void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
+               cudaStream_t s);
+void interleave(const double* src, const int* perm, double* dst, int ni, int ld, int n,
+                cudaStream_t s);
 
 }  // namespace karam

@@ -1,29 +1,26 @@
 // nr_device.cuh -- device code of the batched Newton-Raphson inner loop.
 //
-// One NR "round" = k_eval (device evaluation + stamping at the point x of every
-// live instance) followed by an LU round (per-instance control flow, assembly,
-// static pivot LU on the filled pattern, triangular solves, junction limiting)
-// and, for the rare solves whose static pivots fail, k_rescue (dense partial
-// pivoting). The control flow reproduces CircuitSim::solveDC's GMIN / damping /
-// pnjlim / convergence logic (solvers/circuitsim_solver.cpp:237-485) and the
-// transient NR loop with its attempt loop (circuitsim_solver.cpp:587-660) as a
-// per-instance state machine, one decision per round.
-//
-// This text is compiled twice: by nvcc into the library (with the program
-// interpreter InterpFS), and at run time by NVRTC together with a factor-solve
-// policy generated for one topology (KARAM_JIT defined), so it includes no
-// standard headers.
+// One NR round over the batch is two kernels:
+//   k_es  device evaluation at the trial point x (level-1 MOSFET, diode) into
+//         shared memory and stamping: the Jacobian value slots (FP32 or FP64)
+//         and the KCL residual F (FP64) with its per-instance reductions;
+//   k_lu  per tile of L instances: the control flow (CircuitSim::solveDC's
+//         GMIN / damping / convergence logic, circuitsim_solver.cpp:237-485,
+//         and the transient NR loop with its attempt loop, :587-660), one
+//         decision per round; static-pivot LU of each instance's matrix in
+//         shared memory with the forward substitution fused into the
+//         elimination, back substitution, x = v + dx, and junction limiting
+//         (pnjlim) for DC NR iterations.
+// Solves whose static pivots fail go to k_rescue (FP64 static pivots, then
+// dense partial pivoting), launched after every round.
 #ifndef KARAM_NR_DEVICE_CUH
 #define KARAM_NR_DEVICE_CUH
-#if !defined(__CUDACC_RTC__)
 #include "nr_types.h"
-#endif
 
 namespace knr {
 
-
-constexpr int kEvalThreads = 256;
-constexpr int kLuThreads = 256;
+constexpr int kRoundThreads = 512;
+constexpr int kMaxLanes = 32;
 constexpr unsigned kFull = 0xffffffffu;
 
 enum Act : int {
@@ -32,7 +29,7 @@ enum Act : int {
   ACT_ACCEPT = 4,
   ACT_TRAN_INIT = 8,
   ACT_STEP = 16,
-  ACT_LIMIT = 32,  // sanitize + pnjlim after the solve (DC NR iterations)
+  ACT_LIMIT = 32,    // sanitize + pnjlim after the solve (DC NR iterations)
   ACT_RESEED = 64,   // seeded start failed: restart from the reference seed
   ACT_RESTART = 128, // transient NR failed: retry from the last time point, halved step
   ACT_WAVE = 256     // a full output step completed: record the waveform
@@ -54,72 +51,69 @@ __device__ double pulse_at(const double* p7, double v1, double v2, double time) 
   return v1;
 }
 
-__device__ __forceinline__ double source_value(const DevTopo& T, const DevInst& I, int inst,
-                                               int s, bool tran, double t) {
-  const size_t k = (size_t)inst * T.n_vs + s;
+__device__ __forceinline__ double source_value(const DevTopo& T, const DevInst& I, int g, int s,
+                                               bool tran, double t) {
+  const size_t k = (size_t)s * I.ld + g;
   if (!tran || T.vs_kind[s] != KSRC_PULSE) return I.vs_dc[k];
   return pulse_at(T.vs_pulse + 7 * s, I.vs_v1[k], I.vs_v2[k], t);
 }
 
-// seedInitialGuess (circuitsim_solver.cpp:32-116) in the permuted space;
-// single thread.
-__device__ void reference_seed(const DevTopo& T, const DevInst& I, int inst, double* v) {
-  for (int i = 0; i < T.n; ++i) v[i] = 0.0;
+// seedInitialGuess (circuitsim_solver.cpp:32-116) for instance g into v, in
+// the permuted space; one thread.
+__device__ void reference_seed(const DevTopo& T, const DevInst& I, int g, double* v) {
+  const int ld = I.ld;
+  for (int i = 0; i < T.n; ++i) v[(size_t)i * ld + g] = 0.0;
   double vsup = 5.0;
   for (int s = 0; s < T.n_vs; ++s) {
-    const double val = I.vs_dc[(size_t)inst * T.n_vs + s];
+    const double val = I.vs_dc[(size_t)s * ld + g];
     const int p = T.seed_vs[s];
-    if (p >= 0) v[p] = val;
+    if (p >= 0) v[(size_t)p * ld + g] = val;
     if (val > vsup) vsup = val;
   }
   for (int d = 0; d < T.n_seed_anode; ++d) {
     const int p = T.seed_anode[d];
-    if (p >= 0) v[p] = fmax(v[p], 0.6);
+    if (p >= 0) v[(size_t)p * ld + g] = fmax(v[(size_t)p * ld + g], 0.6);
   }
   for (int s = 0; s < T.n_is; ++s) {
     const int p = T.is_term[s].x;
-    if (p >= 0 && v[p] == 0.0) v[p] = vsup * 0.5;
+    if (p >= 0 && v[(size_t)p * ld + g] == 0.0) v[(size_t)p * ld + g] = vsup * 0.5;
   }
 }
 
 // ---------------------------------------------------------------------------
-// init: seed, state
+// init: seed, state (thread per instance; item loops are coalesced across lanes)
 // ---------------------------------------------------------------------------
-#if !defined(KARAM_JIT)
 __global__ void k_init(DevTopo T, DevInst I, JobParams P) {
-  const int inst = blockIdx.x;
-  if (inst >= I.ni) return;
-  double* v = I.v + (size_t)inst * T.n;
-  double* x = I.x + (size_t)inst * T.n;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= I.ni) return;
+  const size_t ld = I.ld;
   const bool seeded = P.seeded && I.seed != nullptr;
   if (seeded) {
-    for (int i = threadIdx.x; i < T.n; i += blockDim.x) v[i] = I.seed[(size_t)inst * T.n + i];
-  } else if (threadIdx.x == 0) {
-    reference_seed(T, I, inst, v);
+    for (int i = 0; i < T.n; ++i) I.v[i * ld + g] = I.seed[i * ld + g];
+  } else {
+    reference_seed(T, I, g, I.v);
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < T.n; i += blockDim.x) x[i] = v[i];
-  if (threadIdx.x == 0) {
-    if (I.counters) atomicAdd(&I.counters[0], 1ull);
-    InstState s = {};
-    s.mode = MODE_DC;
-    s.sub = SUB_NR;
-    s.g = seeded ? P.gmin_steps - 1 : 0;
-    s.first = 1;
-    s.status = KST_NOCONV;
-    s.seeded = seeded ? 1 : 0;
-    s.prevF = 0.0;
-    s.prev_dv = -1.0;
-    I.st[inst] = s;
-  }
+  for (int i = 0; i < T.n; ++i) I.x[i * ld + g] = I.v[i * ld + g];
+  InstState s = {};
+  s.mode = MODE_DC;
+  s.sub = SUB_NR;
+  s.g = seeded ? P.gmin_steps - 1 : 0;
+  s.first = 1;
+  s.status = KST_NOCONV;
+  s.seeded = seeded ? 1 : 0;
+  s.prevF = 0.0;
+  s.prev_dv = -1.0;
+  I.st[g] = s;
+  I.ev_t[g] = 0.0;
+  I.ev_heff[g] = 0.0;
+  I.red_f[g] = 0ull;
+  I.red_dv[g] = 0ull;
+  I.red_flags[g] = 3;
 }
-#endif  // !KARAM_JIT
 
 // ---------------------------------------------------------------------------
-// evaluation + stamping
+// device physics
 // ---------------------------------------------------------------------------
-constexpr int kMaxEvalInst = 8;
-
 // Level-1 MOSFET of batchMosfetPhysics_generic (tensors/physics_tensors.cpp:53-104).
 // Products are kept unfused (__dmul_rn / __dadd_rn) where the reference's
 // expression would otherwise be contracted into an FMA, so conductances match
@@ -162,208 +156,43 @@ __device__ __forceinline__ void diode_eval(double vdd, double4 par, double& id, 
   gd = fmax(1e-12, gbase);
 }
 
-#if !defined(KARAM_JIT)
-// One CTA evaluates up to NE instances: every gather-table load (device
-// terminals, stamp codes) is made once and applied to all of them, so the
-// index latency is amortised and the per-instance accumulations run side by
-// side. Shared memory per instance: x (n), MOSFET gm/gds/ids, diode g/i.
-// Summation order per Jacobian entry is the stamp order (bit-exact FP64).
-template <typename TJ>
-__global__ void __launch_bounds__(kEvalThreads) k_eval(DevTopo T, DevInst I, JobParams P, int NE) {
-  if (blockIdx.x == 0 && threadIdx.x == 0 && I.rescue_count) *I.rescue_count = 0;
-  extern __shared__ double sm[];
-  __shared__ int s_inst[kMaxEvalInst], s_tran[kMaxEvalInst];
-  __shared__ double s_t[kMaxEvalInst], s_heff[kMaxEvalInst];
-  __shared__ double red[kEvalThreads / 32][kMaxEvalInst];
-  __shared__ int s_cnt;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    int cnt = 0;
-    const int units = 1 << P.max_halvings;
-    for (int k = 0; k < NE; ++k) {
-      const int inst = blockIdx.x * NE + k;
-      if (inst >= I.ni) break;
-      const InstState st = I.st[inst];
-      if (st.mode == MODE_DONE) continue;
-      const bool tran = st.mode == MODE_TRAN;
-      // transient sub-step: size h / 2^depth ending at
-      // ((step - 1) * units + frac + size) * h / units
-      const int size = units >> st.depth;
-      const double hsub = P.h * size / units;
-      s_inst[cnt] = inst;
-      s_tran[cnt] = tran;
-      s_t[cnt] = tran ? P.t0 + (double)((st.step - 1) * units + st.frac + size) * (P.h / units) : 0.0;
-      s_heff[cnt] = P.method == KTRAN_TRAP ? hsub : 2.0 * hsub;
-      cnt++;
+// Device d (MOSFETs first, then diodes) of instance g at x into out[0..2]
+// (stride 32 doubles): MOSFET gm, gds, ids; diode g, i.
+__device__ __forceinline__ void eval_device(const DevTopo& T, const DevInst& I, int d, int g,
+                                            double* out) {
+  const size_t ld = I.ld;
+  const int nm = T.n_mos;
+  const double* x = I.x;
+  if (d < nm) {
+    const int4 tm = __ldg(&T.mos_term[d]);
+    const double2 geo = __ldg(&T.mos_geo[d]);
+    const double sign = __ldg(&T.mos_pmos[d]) ? -1.0 : 1.0;
+    double kpm, vthm;
+    if (I.kp) {
+      kpm = (double)I.kp[d * ld + g];
+      vthm = (double)I.vth[d * ld + g];
+    } else {
+      const double2 card = __ldg(&T.mos_card[d]);
+      kpm = card.x;
+      vthm = card.y;
     }
-    s_cnt = cnt;
-  }
-  __syncthreads();
-  const int ne = s_cnt;
-  if (ne == 0) return;
-  const int n = T.n, nm = T.n_mos, nd = T.n_dio;
-  const int per = n + 3 * nm + 2 * nd;
-  auto xs = [&](int k) { return sm + (size_t)k * per; };
-  for (int e = tid; e < ne * n; e += blockDim.x) {
-    const int k = e / n, i = e - k * n;
-    xs(k)[i] = I.x[(size_t)s_inst[k] * n + i];
-  }
-  __syncthreads();
-
-  for (int m = tid; m < nm; m += blockDim.x) {
-    const int4 tm = T.mos_term[m];
-    const double2 geo = T.mos_geo[m];
-    const double2 card = T.mos_card[m];
-    const double sign = T.mos_pmos[m] ? -1.0 : 1.0;
-#pragma unroll
-    for (int k = 0; k < kMaxEvalInst; ++k) {
-      if (k >= ne) break;
-      const double* x = xs(k);
-      const size_t pi = (size_t)s_inst[k] * nm + m;
-      const double kpm = I.kp ? (double)I.kp[pi] : card.x;
-      const double vthm = I.vth ? (double)I.vth[pi] : card.y;
-      double ids, gm, gds;
-      mosfet_eval(tm.x >= 0 ? x[tm.x] : 0.0, tm.y >= 0 ? x[tm.y] : 0.0, tm.z >= 0 ? x[tm.z] : 0.0,
-                  sign, kpm, vthm, geo.x, geo.y, ids, gm, gds);
-      double* dv = xs(k) + n;
-      dv[m] = gm;
-      dv[nm + m] = gds;
-      dv[2 * nm + m] = ids;
-    }
-  }
-  for (int d = tid; d < nd; d += blockDim.x) {
-    const int2 tt = T.dio_term[d];
-    const double4 par = T.dio_par[d];
-#pragma unroll
-    for (int k = 0; k < kMaxEvalInst; ++k) {
-      if (k >= ne) break;
-      const double* x = xs(k);
-      double id, gd;
-      diode_eval((tt.x >= 0 ? x[tt.x] : 0.0) - (tt.y >= 0 ? x[tt.y] : 0.0), par, id, gd);
-      double* dv = xs(k) + n + 3 * nm;
-      dv[d] = gd;
-      dv[nd + d] = id;
-    }
-  }
-  __syncthreads();
-
-  // Jacobian at x: linear part + gathered device terms, in stamp order.
-  for (int f = tid; f < T.nf; f += blockDim.x) {
-    double acc[kMaxEvalInst];
-    const double base = T.jlin_dc[f];
-#pragma unroll
-    for (int k = 0; k < kMaxEvalInst; ++k) acc[k] = base;
-    for (int q = T.jcap_off[f]; q < T.jcap_off[f + 1]; ++q) {
-      const int c = T.jcap_code[q];
-      const double cc = 2.0 * T.cap_c[code_idx(c)];
-#pragma unroll
-      for (int k = 0; k < kMaxEvalInst; ++k) {
-        if (k >= ne || !s_tran[k]) continue;
-        const double g = cc / s_heff[k];
-        acc[k] = c < 0 ? acc[k] - g : acc[k] + g;
-      }
-    }
-    for (int q = T.jt_off[f]; q < T.jt_off[f + 1]; ++q) {
-      const int c = T.jt_code[q];
-      const int idx = code_idx(c), kind = code_kind(c);
-      const int off = kind == 0 ? n + nm + idx : (kind == 1 ? n + idx : n + 3 * nm + idx);
-#pragma unroll
-      for (int k = 0; k < kMaxEvalInst; ++k) {
-        if (k >= ne) break;
-        const double val = xs(k)[off];
-        acc[k] = c < 0 ? acc[k] - val : acc[k] + val;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < kMaxEvalInst; ++k) {
-      if (k >= ne) break;
-      reinterpret_cast<TJ*>(I.J)[(size_t)s_inst[k] * T.nf + f] = (TJ)acc[k];
-    }
-  }
-
-  // KCL residual at x: currents leaving every node (no gmin).
-  double lmax[kMaxEvalInst];
-  bool bad = false;
-#pragma unroll
-  for (int k = 0; k < kMaxEvalInst; ++k) lmax[k] = 0.0;
-  for (int i = tid; i < n; i += blockDim.x) {
-    double acc[kMaxEvalInst];
-#pragma unroll
-    for (int k = 0; k < kMaxEvalInst; ++k) acc[k] = 0.0;
-    for (int q = T.ft_off[i]; q < T.ft_off[i + 1]; ++q) {
-      const int c = T.ft_code[q];
-      const int idx = code_idx(c), kind = code_kind(c);
-      int2 tt = make_int2(-1, -1);
-      double g = 0.0;
-      if (kind == 0) {
-        tt = T.res_term[idx];
-        g = T.res_g[idx];
-      } else if (kind == 1) {
-        tt = T.vs_term[idx];
-      } else if (kind == 3) {
-        tt = T.cap_term[idx];
-        g = 2.0 * T.cap_c[idx];
-      }
-#pragma unroll
-      for (int k = 0; k < kMaxEvalInst; ++k) {
-        if (k >= ne) break;
-        const double* x = xs(k);
-        const double va = tt.x >= 0 ? x[tt.x] : 0.0, vb = tt.y >= 0 ? x[tt.y] : 0.0;
-        double cur = 0.0;
-        switch (kind) {
-          case 0:  // resistor
-            cur = g * (va - vb);
-            break;
-          case 1:  // Norton voltage source, G = 1e3 S
-            cur = 1.0e3 * ((va - vb) - source_value(T, I, s_inst[k], idx, s_tran[k], s_t[k]));
-            break;
-          case 2:
-            cur = T.is_amp[idx];
-            break;
-          case 3:  // capacitor companion
-            if (s_tran[k]) {
-              const size_t ci = (size_t)s_inst[k] * T.n_cap + idx;
-              cur = (g / s_heff[k]) * ((va - vb) - I.cap_vp[ci]);
-              if (P.method == KTRAN_TRAP) cur -= I.cap_ip[ci];
-            }
-            break;
-          case 4:
-            cur = x[n + 3 * nm + nd + idx];
-            break;
-          default:
-            cur = x[n + 2 * nm + idx];
-            break;
-        }
-        acc[k] = c < 0 ? acc[k] - cur : acc[k] + cur;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < kMaxEvalInst; ++k) {
-      if (k >= ne) break;
-      I.F[(size_t)s_inst[k] * n + i] = acc[k];
-      if (!isfinite(acc[k])) bad = true;
-      lmax[k] = fmax(lmax[k], fabs(acc[k]));
-    }
-  }
-  bad = __any_sync(kFull, bad);
-#pragma unroll
-  for (int k = 0; k < kMaxEvalInst; ++k) {
-    double m = lmax[k];
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(kFull, m, o));
-    if ((tid & 31) == 0) red[tid >> 5][k] = bad ? __longlong_as_double(0x7ff0000000000000LL) : m;
-  }
-  __syncthreads();
-  if (tid < ne) {
-    double m = 0.0;
-    bool nf = false;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      if (isinf(red[w][tid])) nf = true;
-      m = fmax(m, red[w][tid]);
-    }
-    I.Fmax[s_inst[tid]] = nf ? __longlong_as_double(0x7ff8000000000000LL) : m;
+    double ids, gm, gds;
+    mosfet_eval(tm.x >= 0 ? x[tm.x * ld + g] : 0.0, tm.y >= 0 ? x[tm.y * ld + g] : 0.0,
+                tm.z >= 0 ? x[tm.z * ld + g] : 0.0, sign, kpm, vthm, geo.x, geo.y, ids, gm, gds);
+    out[0] = gm;
+    out[32] = gds;
+    out[64] = ids;
+  } else {
+    const int k = d - nm;
+    const int2 tt = __ldg(&T.dio_term[k]);
+    const double4 par = T.dio_par[k];
+    double id, gd;
+    diode_eval((tt.x >= 0 ? x[tt.x * ld + g] : 0.0) - (tt.y >= 0 ? x[tt.y * ld + g] : 0.0), par,
+               id, gd);
+    out[0] = gd;
+    out[32] = id;
   }
 }
-#endif  // !KARAM_JIT
 
 // ---------------------------------------------------------------------------
 // per-instance control flow
@@ -530,18 +359,38 @@ __device__ int decide(InstState& s, double F, bool vconv, bool pok, double dv,
   return ACT_ACCEPT | ACT_SOLVE;
 }
 
-// applyPnJunctionLimits (circuitsim_solver.cpp:118-169) for diode d on x
-// against v. The temperature-scaled Vt and vcrit (pnjlim's compute_vcrit,
-// physics/device_physics.h:175-179) are per-diode constants the host computes
-// with the reference's expressions once per topology.
-__device__ __forceinline__ void limit_one(const DevTopo& T, int d, double* x, const double* v) {
-  const int2 tt = T.dio_term[d];
+// Time and capacitor-companion step of the point an instance evaluates: DC
+// (heff = 0), or the end of the current transient sub-step of size h/2^depth,
+// ((step - 1) * units + frac + size) * h / units; heff is the trapezoidal
+// companion's step (backward Euler = trapezoidal stamp at 2 h).
+__device__ __forceinline__ void eval_point(const InstState& st, const JobParams& P, double& t,
+                                           double& heff) {
+  if (st.mode != MODE_TRAN) {
+    t = 0.0;
+    heff = 0.0;
+    return;
+  }
+  const int units = 1 << P.max_halvings;
+  const int size = units >> st.depth;
+  const double hsub = P.h * size / units;
+  t = P.t0 + (double)((st.step - 1) * units + st.frac + size) * (P.h / units);
+  heff = P.method == KTRAN_TRAP ? hsub : 2.0 * hsub;
+}
+
+// applyPnJunctionLimits (circuitsim_solver.cpp:118-169) for diode d of
+// instance g on x against v. The temperature-scaled Vt and vcrit (pnjlim's
+// compute_vcrit, physics/device_physics.h:175-179) are per-diode constants the
+// host computes with the reference's expressions once per topology.
+__device__ __forceinline__ void limit_one(const DevTopo& T, int d, double* x, const double* v,
+                                          size_t ld, int g) {
+  const int2 tt = __ldg(&T.dio_term[d]);
   const int p = tt.x, q = tt.y;
   if (p < 0 && q < 0) return;
-  const double2 lim = T.dio_lim[d];
+  const double2 lim = __ldg(&T.dio_lim[d]);
   const double vt = lim.x, vcrit = lim.y;
-  const double vjo = (p >= 0 ? v[p] : 0.0) - (q >= 0 ? v[q] : 0.0);
-  const double vjn = (p >= 0 ? x[p] : 0.0) - (q >= 0 ? x[q] : 0.0);
+  const size_t pp = (size_t)p * ld + g, qq = (size_t)q * ld + g;
+  const double vjo = (p >= 0 ? v[pp] : 0.0) - (q >= 0 ? v[qq] : 0.0);
+  const double vjn = (p >= 0 ? x[pp] : 0.0) - (q >= 0 ? x[qq] : 0.0);
   double vl = vjn;
   if (vjo > 30.0 * vt && vjn > 30.0 * vt) {
     vl = vjn;
@@ -560,540 +409,865 @@ __device__ __forceinline__ void limit_one(const DevTopo& T, int d, double* x, co
   const double corr = vjn - vl;
   if (fabs(corr) > 1e-12) {
     if (p >= 0 && q >= 0) {
-      x[p] -= corr * 0.5;
-      x[q] += corr * 0.5;
+      x[pp] -= corr * 0.5;
+      x[qq] += corr * 0.5;
     } else if (p >= 0) {
-      x[p] -= corr;
+      x[pp] -= corr;
     } else {
-      x[q] += corr;
+      x[qq] += corr;
     }
   }
 }
 
-// The reference limits diodes one after another; diodes of one level share
-// no node with each other, and every earlier diode sharing a node has a lower
-// level, so level-by-level parallel limiting gives the sequential result.
-__device__ void limit_junctions_warp(const DevTopo& T, double* x, const double* v, int lane) {
-  for (int lvl = 0; lvl < T.n_dio_levels; ++lvl) {
-    for (int d = lane; d < T.n_dio; d += 32)
-      if (T.dio_level[d] == lvl) limit_one(T, d, x, v);
-    __syncwarp();
-  }
+// Static-pivot LU + solve of one instance on the value slots. A: the slot
+// values (gmin already on the diagonal), y: right-hand side in, solution out;
+// element k of either sits at [k * L] (L = lanes of the tile). Pivot k of the
+// program lists Lrow/Lslot (rows i > k with A[i][k] != 0), Ucol/Uslot (columns
+// j > k of row k) and the update target of every (i, j) pair. The forward
+// substitution runs inside the elimination (y[k] is final when pivot k is
+// reached), which leaves the back substitution as the only second pass.
+// Returns false when the static pivots are unusable: a tiny or non-finite
+// pivot, a multiplier above growth_limit, or a non-finite solution.
+//
+// Two schedules with identical arithmetic: when every pivot has nL <= 2 and
+// nU <= 2 (chain-like circuits) the program arrives as packed records in
+// shared memory (rec), the record of pivot k + 1 is decoded while pivot k
+// computes, and all value loads of a pivot are issued before its stores (its
+// L, U, diagonal and target slots are distinct), so a pivot costs about one
+// shared-memory round trip plus the reciprocal; otherwise (rec == 0) a
+// generic loop walks the program in global memory.
+struct SmallPivot {
+  int d, nl, nu, lr0, lr1, ls0, ls1, us0, us1, t00, t01, t10, t11, uc0, uc1;
+};
+
+// Decodes a packed pivot record (see pack_small_pivots in topology.cpp).
+__device__ __forceinline__ SmallPivot decode_pivot(int4 a, int4 b) {
+  SmallPivot q;
+  const unsigned w0 = (unsigned)a.x;
+  q.d = (int)(w0 & 0xffffffu);
+  q.nl = (int)((w0 >> 24) & 15u);
+  q.nu = (int)(w0 >> 28);
+  q.lr0 = a.y & 0xffff;
+  q.lr1 = (int)((unsigned)a.y >> 16);
+  q.ls0 = a.z & 0xffff;
+  q.ls1 = (int)((unsigned)a.z >> 16);
+  q.us0 = a.w & 0xffff;
+  q.us1 = (int)((unsigned)a.w >> 16);
+  q.t00 = b.x & 0xffff;
+  q.t01 = (int)((unsigned)b.x >> 16);
+  q.t10 = b.y & 0xffff;
+  q.t11 = (int)((unsigned)b.y >> 16);
+  q.uc0 = b.z & 0xffff;
+  q.uc1 = (int)((unsigned)b.z >> 16);
+  return q;
 }
 
-__device__ void limit_junctions(const DevTopo& T, double* x, const double* v) {
-  for (int d = 0; d < T.n_dio; ++d) limit_one(T, d, x, v);
-}
+// Correctly rounded reciprocal (the value of 1 / x).
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }
 
-// Static-pivot LU + forward/back substitution, one instance per thread, on
-// the numerically non-zero part of the filled pattern. A: the instance's value
-// row (gmin already on the diagonal); y: right-hand side in, solution out.
-// Pivot k of the program lists Lrow/Lpos (rows i > k with A[i][k] != 0 and
-// their positions), Ucol/Upos (columns j > k of row k) and the update targets
-// A[i][j] for every (i, j) pair. Returns false when the static pivots are
-// unusable: a tiny or non-finite pivot, a multiplier above growth_limit (the
-// elimination order amplifies rounding, e.g. a supply hub eliminated after a
-// chain of high-gain stages), or a non-finite solution; such solves are redone
-// with partial pivoting. InterpFS reads the program from memory; a policy
-// generated per topology replaces it with straight-line code.
-struct InterpFS {
-  template <typename T>
-  __device__ static bool run(T* __restrict__ A, T* __restrict__ y, const DevTopo& Tp, T tiny,
-                             T growth_limit) {
-    const int4* __restrict__ hdr = Tp.lu_hdr;
-    const int* __restrict__ data = Tp.lu_data;
-    const int n = Tp.n;
-    bool ok = true;
-    T lmax = T(0);
+template <typename T>
+__device__ bool lu_solve(T* __restrict__ A, T* __restrict__ y, int L, const DevTopo& Tp,
+                         const int4* __restrict__ rec, T tiny, T growth_limit) {
+  const int n = Tp.n;
+  bool ok = true;
+  T lmax = T(0);
+  if (rec) {
+    SmallPivot q = decode_pivot(rec[0], rec[1]);
     for (int k = 0; k < n; ++k) {
-      const int4 h = __ldg(hdr + k);
-      const int nl = h.y, nu = h.z;
-      const int* lp = data + h.x + nl;
-      const int* up = lp + nl + nu;
-      const int* tp = up + nu;
-      const T piv = A[h.w];
+      const int kn = k + 1 < n ? k + 1 : k;
+      const SmallPivot nq = decode_pivot(rec[2 * kn], rec[2 * kn + 1]);
+      const int nl = q.nl, nu = q.nu;
+      const T piv = A[q.d * L];
+      const T yk = y[k * L];
+      const T u0 = nu > 0 ? A[q.us0 * L] : T(0);
+      const T u1 = nu > 1 ? A[q.us1 * L] : T(0);
+      const T a0 = nl > 0 ? A[q.ls0 * L] : T(0);
+      const T a1 = nl > 1 ? A[q.ls1 * L] : T(0);
+      const T y0 = nl > 0 ? y[q.lr0 * L] : T(0);
+      const T y1 = nl > 1 ? y[q.lr1 * L] : T(0);
+      const T b00 = (nl > 0 && nu > 0) ? A[q.t00 * L] : T(0);
+      const T b01 = (nl > 0 && nu > 1) ? A[q.t01 * L] : T(0);
+      const T b10 = (nl > 1 && nu > 0) ? A[q.t10 * L] : T(0);
+      const T b11 = (nl > 1 && nu > 1) ? A[q.t11 * L] : T(0);
       ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
-      const T r = T(1) / piv;
-      A[h.w] = r;
-      for (int a = 0; a < nl; ++a) {
-        const int la = __ldg(lp + a);
-        const T l = A[la] * r;
+      const T r = recip(piv);
+      A[q.d * L] = r;
+      if (nl > 0) {
+        const T l = a0 * r;
         lmax = fmax(lmax, fabs(l));
-        A[la] = l;
-        const int* trow = tp + a * nu;
-        for (int b2 = 0; b2 < nu; ++b2) A[__ldg(trow + b2)] -= l * A[__ldg(up + b2)];
+        A[q.ls0 * L] = l;
+        y[q.lr0 * L] = y0 - l * yk;
+        if (nu > 0) A[q.t00 * L] = b00 - l * u0;
+        if (nu > 1) A[q.t01 * L] = b01 - l * u1;
       }
-    }
-    for (int k = 0; k < n; ++k) {
-      const int4 h = __ldg(hdr + k);
-      const int nl = h.y;
-      const int* lr = data + h.x;
-      const int* lp = lr + nl;
-      const T yk = y[k];
-      for (int a = 0; a < nl; ++a) y[__ldg(lr + a)] -= A[__ldg(lp + a)] * yk;
+      if (nl > 1) {
+        const T l = a1 * r;
+        lmax = fmax(lmax, fabs(l));
+        A[q.ls1 * L] = l;
+        y[q.lr1 * L] = y1 - l * yk;
+        if (nu > 0) A[q.t10 * L] = b10 - l * u0;
+        if (nu > 1) A[q.t11 * L] = b11 - l * u1;
+      }
+      q = nq;
     }
     bool finite = true;
+    q = decode_pivot(rec[2 * (n - 1)], rec[2 * (n - 1) + 1]);
     for (int k = n - 1; k >= 0; --k) {
-      const int4 h = __ldg(hdr + k);
-      const int nl = h.y, nu = h.z;
-      const int* uc = data + h.x + 2 * nl;
-      const int* up = uc + nu;
-      T s = y[k];
-      for (int b2 = 0; b2 < nu; ++b2) s -= A[__ldg(up + b2)] * y[__ldg(uc + b2)];
-      y[k] = s * A[h.w];
-      finite = finite && isfinite(y[k]);
+      const int kn = k > 0 ? k - 1 : 0;
+      const SmallPivot nq = decode_pivot(rec[2 * kn], rec[2 * kn + 1]);
+      const int nu = q.nu;
+      T s = y[k * L];
+      const T r = A[q.d * L];
+      if (nu > 0) s -= A[q.us0 * L] * y[q.uc0 * L];
+      if (nu > 1) s -= A[q.us1 * L] * y[q.uc1 * L];
+      s *= r;
+      y[k * L] = s;
+      finite = finite && isfinite(s);
+      q = nq;
     }
     return ok && finite && !(lmax > growth_limit);
   }
-};
+  const int4* __restrict__ hdr = Tp.lu_hdr;
+  const int* __restrict__ data = Tp.lu_data;
+  int4 h = __ldg(hdr);
+  for (int k = 0; k < n; ++k) {
+    const int4 hn = __ldg(hdr + (k + 1 < n ? k + 1 : k));
+    const int nl = h.y, nu = h.z;
+    const int* lr = data + h.x;
+    const int* ls = lr + nl;
+    const int* us = ls + nl + nu;
+    const int* ts = us + nu;
+    const T piv = A[h.w * L];
+    ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
+    const T r = recip(piv);
+    A[h.w * L] = r;
+    const T yk = y[k * L];
+    for (int a = 0; a < nl; ++a) {
+      const int sl = __ldg(ls + a);
+      const T l = A[sl * L] * r;
+      lmax = fmax(lmax, fabs(l));
+      A[sl * L] = l;
+      y[__ldg(lr + a) * L] -= l * yk;
+      const int* trow = ts + a * nu;
+      for (int b = 0; b < nu; ++b) A[__ldg(trow + b) * L] -= l * A[__ldg(us + b) * L];
+    }
+    h = hn;
+  }
+  bool finite = true;
+  for (int k = n - 1; k >= 0; --k) {
+    const int4 hk = __ldg(hdr + k);
+    const int nl = hk.y, nu = hk.z;
+    const int* uc = data + hk.x + 2 * nl;
+    const int* us = uc + nu;
+    T s = y[k * L];
+    for (int b = 0; b < nu; ++b) s -= A[__ldg(us + b) * L] * y[__ldg(uc + b) * L];
+    s *= A[hk.w * L];
+    y[k * L] = s;
+    finite = finite && isfinite(s);
+  }
+  return ok && finite && !(lmax > growth_limit);
+}
 
 // What the control flow does when a linear solve of a DC NR iteration fails
 // for good (the reference's singular-matrix branch, circuitsim_solver.cpp:358-366):
 // a seeded start falls back to the reference seed, anything else stops.
-__device__ void on_singular(const DevTopo& Tp, const DevInst& I, int inst) {
-  InstState s = I.st[inst];
+// Returns false when the instance stopped.
+__device__ bool on_singular(const DevTopo& Tp, const DevInst& I, int g) {
+  InstState s = I.st[g];
   if (s.mode == MODE_DC && s.sub == SUB_NR) s.iters += 2 * (s.it + 1);
+  bool alive = false;
   if (s.mode == MODE_DC && s.sub == SUB_NR && s.seeded) {
-    double* v = I.v + (size_t)inst * Tp.n;
-    double* x = I.x + (size_t)inst * Tp.n;
-    reference_seed(Tp, I, inst, v);
-    for (int i = 0; i < Tp.n; ++i) x[i] = v[i];
+    reference_seed(Tp, I, g, I.v);
+    for (int i = 0; i < Tp.n; ++i) I.x[(size_t)i * I.ld + g] = I.v[(size_t)i * I.ld + g];
     s.g = 0;
     s.it = 0;
     s.first = 1;
     s.damp = 0;
     s.prevF = 0.0;
     s.seeded = 0;
+    alive = true;
   } else {
     s.status = KST_SINGULAR;
     s.mode = MODE_DONE;
   }
-  I.st[inst] = s;
+  I.st[g] = s;
+  return alive;
 }
 
-// One round of the control flow + linear solve for NI instances (one CTA).
-template <typename T, typename FS>
-__device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, const JobParams& P,
-                                         int NI, int S, int Sv, int* active) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* vals = reinterpret_cast<T*>(smem_raw);
-  T* vec = vals + (size_t)NI * S;
-  __shared__ int act[32];
-  __shared__ int vconv_s[32], pok_s[32], sing_s[32], solve_list[32];
-  __shared__ double dv_s[32], gmin_s[32], hsub_s[32];
-  __shared__ int n_solve;
+// ---------------------------------------------------------------------------
+// the NR round: k_es -> k_lu (-> k_rescue)
+// ---------------------------------------------------------------------------
+// One KCL term of record q (es_ft / es_fc) for instance g; device terms read
+// the CTA's device values sd ([local][3][32] doubles, lane offset applied).
+__device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, const JobParams& P,
+                                            int4 tm, double coef, int g, bool tran, double t,
+                                            double heff, const double* sd, int dev_base) {
+  const size_t ld = I.ld;
+  const int idx = code_idx(tm.x), kind = code_kind(tm.x);
+  if (kind >= 4) return sd[(idx - dev_base) * 96 + (kind == 4 ? 32 : 64)];  // diode i / MOSFET ids
+  if (kind == 2) return coef;                                                // current source
+  const double va = tm.y >= 0 ? I.x[tm.y * ld + g] : 0.0;
+  const double vb = tm.z >= 0 ? I.x[tm.z * ld + g] : 0.0;
+  if (kind == 0) return coef * (va - vb);                                    // resistor
+  if (kind == 1) return 1.0e3 * ((va - vb) - source_value(T, I, g, idx, tran, t));  // Norton V source
+  if (!tran) return 0.0;                                                     // capacitor companion
+  const size_t ci = (size_t)idx * ld + g;
+  double cur = (coef / heff) * ((va - vb) - I.cap_vp[ci]);
+  if (P.method == KTRAN_TRAP) cur -= I.cap_ip[ci];
+  return cur;
+}
 
-  const int n = Tp.n, nf = Tp.nf;
-  const int base = blockIdx.x * NI;
-  const int cnt = min(NI, I.ni - base);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+// Device evaluation + stamping at x: blockIdx.x picks 32 consecutive
+// instances (one per lane; every warp of the CTA holds the same 32),
+// blockIdx.y a block of stamp items. The CTA evaluates the block's devices
+// into shared memory, then writes the Jacobian value of each of its slots
+// (linear stamps, capacitor companions, device terms, in stamp order) and the
+// KCL residual of each of its nodes (terms in node order), and folds max |F|,
+// max |x - v| and the convergence flags of its nodes into the instance's
+// reductions with one atomic each. A hub node (more devices than shared memory
+// holds) walks its terms in chunks of KES_MAX_DEV devices.
+template <typename TJ>
+__global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
+  __shared__ double s_dev[KES_MAX_DEV * 3 * 32];
+  __shared__ unsigned long long s_f[8][32], s_dv[8][32];
+  __shared__ int s_fl[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = blockIdx.x * 32 + lane;
+  const size_t ld = I.ld;
+  const int nv = T.nv;
+  const double heff = g < I.ni ? I.ev_heff[g] : -1.0;
+  const bool live = heff >= 0.0;
+  if (!__syncthreads_or(live)) return;
+  const int4 blk = __ldg(&T.es_block[blockIdx.y]);  // item off, items, device off, devices
+  const bool tran = heff > 0.0;
+  const double t = live ? I.ev_t[g] : 0.0;
+  const double* sd = s_dev + lane;
+  double fmx = 0.0, dvm = 0.0;
+  bool bad = false;
+  int flags = 3, node_seen = 0;
+  auto node_done = [&](int i, double f) {
+    const size_t o = (size_t)i * ld + g;
+    I.F[o] = f;
+    if (!isfinite(f)) bad = true;
+    fmx = fmax(fmx, fabs(f));
+    const double xi = I.x[o], vi = I.v[o];
+    const double dd = fabs(xi - vi), m = fmax(fabs(xi), fabs(vi));
+    if (dd > P.reltol * m + P.vntol) flags &= ~1;
+    if (dd > P.polish_rel * m + P.polish_abs) flags &= ~2;
+    dvm = fmax(dvm, dd);
+    node_seen = 1;
+  };
+  if (blk.y > 0) {
+    if (live)
+      for (int k = warp; k < blk.w; k += 8)
+        eval_device(T, I, __ldg(&T.es_dev[blk.z + k]), g, s_dev + k * 96 + lane);
+    __syncthreads();
+    if (live)
+      for (int k = warp; k < blk.y; k += 8) {
+        const int4 it = __ldg(&T.es_item[blk.x + k]);
+        if (it.x < nv) {
+          const int s = it.x;
+          double acc = __ldg(&T.jlin_dc[s]);
+          if (tran) {
+            const int q1 = __ldg(&T.jcap_off[s + 1]);
+            for (int q = __ldg(&T.jcap_off[s]); q < q1; ++q) {
+              const int c = __ldg(&T.jcap_code[q]);
+              const double gq = (2.0 * __ldg(&T.cap_c[code_idx(c)])) / heff;
+              acc = c < 0 ? acc - gq : acc + gq;
+            }
+          }
+          for (int q = it.y; q < it.y + it.z; ++q) {
+            const int c = __ldg(&T.es_jt[q]);
+            const int kind = code_kind(c);  // 0 gds, 1 gm, 2 diode g
+            const double val = sd[code_idx(c) * 96 + (kind == 0 ? 32 : 0)];
+            acc = c < 0 ? acc - val : acc + val;
+          }
+          reinterpret_cast<TJ*>(I.J)[(size_t)s * ld + g] = (TJ)acc;
+        } else {
+          double acc = 0.0;
+          for (int q = it.y; q < it.y + it.z; ++q) {
+            const int4 tm = __ldg(&T.es_ft[q]);
+            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
+            acc = tm.x < 0 ? acc - cur : acc + cur;
+          }
+          node_done(it.x - nv, acc);
+        }
+      }
+  } else {
+    // hub item: devices in chunks of KES_MAX_DEV in term order; warp 0 sums
+    const int4 it = __ldg(&T.es_item[blk.x]);
+    const bool slot = it.x < nv;
+    int q = it.y;
+    const int qe = it.y + it.z;
+    double acc = 0.0;
+    if (slot) {
+      acc = __ldg(&T.jlin_dc[it.x]);
+      if (tran) {
+        const int q1 = __ldg(&T.jcap_off[it.x + 1]);
+        for (int c = __ldg(&T.jcap_off[it.x]); c < q1; ++c) {
+          const int cc = __ldg(&T.jcap_code[c]);
+          const double gq = (2.0 * __ldg(&T.cap_c[code_idx(cc)])) / heff;
+          acc = cc < 0 ? acc - gq : acc + gq;
+        }
+      }
+    }
+    for (int c0 = 0; c0 < blk.w; c0 += KES_MAX_DEV) {
+      const int cn = min(KES_MAX_DEV, blk.w - c0);
+      if (live)
+        for (int k = warp; k < cn; k += 8)
+          eval_device(T, I, __ldg(&T.es_dev[blk.z + c0 + k]), g, s_dev + k * 96 + lane);
+      __syncthreads();
+      if (warp == 0 && live) {
+        if (slot) {
+          for (; q < qe; ++q) {  // every slot term is a device term
+            const int c = __ldg(&T.es_jt[q]);
+            if (code_idx(c) >= c0 + cn) break;
+            const double val = sd[(code_idx(c) - c0) * 96 + (code_kind(c) == 0 ? 32 : 0)];
+            acc = c < 0 ? acc - val : acc + val;
+          }
+        } else {
+          for (; q < qe; ++q) {
+            const int4 tm = __ldg(&T.es_ft[q]);
+            if (code_kind(tm.x) >= 4 && code_idx(tm.x) >= c0 + cn) break;
+            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, c0);
+            acc = tm.x < 0 ? acc - cur : acc + cur;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (warp == 0 && live) {
+      if (slot) {
+        reinterpret_cast<TJ*>(I.J)[(size_t)it.x * ld + g] = (TJ)acc;
+      } else {
+        for (; q < qe; ++q) {
+          const int4 tm = __ldg(&T.es_ft[q]);
+          const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
+          acc = tm.x < 0 ? acc - cur : acc + cur;
+        }
+        node_done(it.x - nv, acc);
+      }
+    }
+  }
+  // non-negative doubles order like their bit patterns; NaN sorts above +inf
+  s_f[warp][lane] = bad ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(fmx);
+  s_dv[warp][lane] = (unsigned long long)__double_as_longlong(dvm);
+  s_fl[warp][lane] = flags;
+  const bool has_nodes = __syncthreads_or(node_seen);
+  if (warp == 0 && live && has_nodes) {
+    unsigned long long f = s_f[0][lane], d = s_dv[0][lane];
+    int fl = s_fl[0][lane];
+    for (int w = 1; w < 8; ++w) {
+      f = max(f, s_f[w][lane]);
+      d = max(d, s_dv[w][lane]);
+      fl &= s_fl[w][lane];
+    }
+    atomicMax(&I.red_f[g], f);
+    atomicMax(&I.red_dv[g], d);
+    if (fl != 3) atomicAnd(&I.red_flags[g], fl);
+  }
+}
+
+// Reductions of an instance back to their neutral values.
+__device__ __forceinline__ void reset_reductions(const DevInst& I, int g) {
+  I.red_f[g] = 0ull;
+  I.red_dv[g] = 0ull;
+  I.red_flags[g] = 3;
+}
+
+// Evaluation point of the next round from the instance's state.
+__device__ __forceinline__ void set_eval_point(const DevInst& I, const JobParams& P, int g,
+                                               const InstState& st) {
+  if (st.mode == MODE_DONE) {
+    I.ev_heff[g] = -1.0;
+    I.ev_t[g] = 0.0;
+    return;
+  }
+  double t, heff;
+  eval_point(st, P, t, heff);
+  I.ev_t[g] = t;
+  I.ev_heff[g] = heff;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Control flow + linear solve of a tile of L instances (one CTA): decisions
+// from the reductions of k_es, vector updates, the Jacobian tile staged
+// into shared memory with cp.async, static-pivot LU with the forward
+// substitution fused, x = v + dx, junction limiting, bookkeeping.
+template <typename T>
+__global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, JobParams P, int L,
+                                                      int* active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);  // [nv][L]
+  T* Y = A + (size_t)Tp.nv * L;            // [n][L]
+  int4* rec = Tp.lu_rec ? reinterpret_cast<int4*>(
+                              smem_raw + (((size_t)(Tp.nv + Tp.n) * L * sizeof(T) + 15) & ~size_t(15)))
+                        : nullptr;         // [2 n] packed pivot records
+  __shared__ int s_live[kMaxLanes], s_act[kMaxLanes], s_sing[kMaxLanes], s_trev[kMaxLanes];
+  __shared__ double s_gmin[kMaxLanes], s_hsub[kMaxLanes];
+
+  const int n = Tp.n, nv = Tp.nv;
+  const size_t ld = I.ld;
+  const int tid = threadIdx.x;
+  const int lane = tid % L, row = tid / L, R = blockDim.x / L;
+  const int base = blockIdx.x * L;
+  const int g = base + lane;
+  const int cnt = min(L, I.ni - base);
   if (cnt <= 0) return;
 
-  // 1. compare the trial point x with the accepted point v (warp per instance)
-  for (int k = warp; k < cnt; k += nw) {
-    const int inst = base + k;
-    bool vc = true, pk = true;
-    double dvm = 0.0;
-    if (I.st[inst].mode != MODE_DONE) {
-      const double* x = I.x + (size_t)inst * n;
-      const double* v = I.v + (size_t)inst * n;
-      for (int i = lane; i < n; i += 32) {
-        const double xi = x[i], vi = v[i];
-        const double d = fabs(xi - vi), m = fmax(fabs(xi), fabs(vi));
-        if (d > P.reltol * m + P.vntol) vc = false;
-        if (d > P.polish_rel * m + P.polish_abs) pk = false;
-        dvm = fmax(dvm, d);
-      }
-      vc = __all_sync(kFull, vc);
-      pk = __all_sync(kFull, pk);
-      for (int o = 16; o > 0; o >>= 1) dvm = fmax(dvm, __shfl_xor_sync(kFull, dvm, o));
-    }
-    if (lane == 0) {
-      vconv_s[k] = vc;
-      pok_s[k] = pk;
-      dv_s[k] = dvm;
-    }
-  }
-  __syncthreads();
-
-  // 2. decisions (thread per instance)
-  if (tid < 32) {
+  // 1. decisions (thread per lane) from the reductions of k_es
+  int my_live = 0;
+  if (tid < L) {
     int a = 0;
     if (tid < cnt) {
-      const int inst = base + tid;
-      InstState s = I.st[inst];
-      double gm = 1e-12, hs = P.h;
-      a = decide(s, I.Fmax[inst], vconv_s[tid], pok_s[tid], dv_s[tid], P, gm, hs);
-      hsub_s[tid] = hs;
-      if (a & ACT_RESEED) {
-        s.g = 0;
-        s.it = 0;
-        s.first = 1;
-        s.damp = 0;
-        s.prevF = 0.0;
-        s.seeded = 0;
+      InstState s = I.st[g];
+      s_trev[tid] = s.mode == MODE_TRAN;  // what this round evaluated
+      if (s.mode != MODE_DONE) {
+        my_live = 1;
+        const unsigned long long fb = I.red_f[g];
+        const double Fm = __longlong_as_double((long long)fb);
+        const double dvm = __longlong_as_double((long long)I.red_dv[g]);
+        const int fl = I.red_flags[g];
+        reset_reductions(I, g);
+        double gm = 1e-12, hs = P.h;
+        a = decide(s, Fm, fl & 1, (fl & 2) != 0, dvm, P, gm, hs);
+        if (a & ACT_RESEED) {
+          s.g = 0;
+          s.it = 0;
+          s.first = 1;
+          s.damp = 0;
+          s.prevF = 0.0;
+          s.seeded = 0;
+          reference_seed(Tp, I, g, I.v);
+        }
+        I.st[g] = s;
+        s_gmin[tid] = gm;
+        s_hsub[tid] = hs;
       }
-      gmin_s[tid] = gm;
-      I.st[inst] = s;
     }
-    act[tid] = a;
-    sing_s[tid] = 0;
-    const unsigned m = __ballot_sync(kFull, a & ACT_SOLVE);
-    if (a & ACT_SOLVE) solve_list[__popc(m & ((1u << tid) - 1u))] = tid;
-    if (tid == 0) n_solve = __popc(m);
+    s_live[tid] = my_live;
+    s_act[tid] = a;
+    s_sing[tid] = 0;
+  }
+  if (!__syncthreads_or(my_live)) return;
+
+  // 2. vector updates and the right-hand side of the instances that solve
+  const int a = s_act[lane];
+  int any_solve = 0;
+  if (a) {
+    const double gmin = s_gmin[lane];
+    for (int i = row; i < n; i += R) {
+      const size_t o = (size_t)i * ld + g;
+      double vi;
+      if (a & ACT_RESTART) {
+        vi = I.v_tp[o];
+        I.v[o] = vi;
+        I.x[o] = vi;
+      } else if (a & ACT_RESEED) {
+        vi = I.v[o];
+        I.x[o] = vi;
+      } else {
+        double xi = I.x[o];
+        vi = I.v[o];
+        if (a & ACT_DAMP) {
+          xi = vi + 0.5 * (xi - vi);
+          I.x[o] = xi;
+        }
+        if (a & ACT_ACCEPT) {
+          vi = xi;
+          I.v[o] = vi;
+        }
+        if (a & (ACT_STEP | ACT_TRAN_INIT)) I.v_tp[o] = vi;
+      }
+      if (a & ACT_SOLVE) Y[i * L + lane] = (T)(-(I.F[o] + gmin * vi));
+    }
+    any_solve = (a & ACT_SOLVE) != 0;
+  }
+  any_solve = __syncthreads_or(any_solve);
+
+  // 2b. the Jacobian tile of the solving instances into shared memory
+  if (any_solve) {
+    const T* J = reinterpret_cast<const T*>(I.J);
+    const int row_bytes = L * (int)sizeof(T);
+    if (row_bytes % 16 == 0) {
+      const int cpr = row_bytes / 16;  // 16-byte chunks per slot row
+      const int chunks = nv * cpr;
+      for (int c = tid; c < chunks; c += blockDim.x) {
+        const int s = c / cpr, part = c - s * cpr;
+        cp_async16(reinterpret_cast<char*>(A + (size_t)s * L) + 16 * part,
+                   reinterpret_cast<const char*>(J + (size_t)s * ld + base) + 16 * part);
+      }
+    } else {
+      for (int s = row; s < nv; s += R) A[s * L + lane] = J[(size_t)s * ld + g];
+    }
+    if (rec)
+      for (int k = tid; k < 2 * n; k += blockDim.x) rec[k] = __ldg(&Tp.lu_rec[k]);
+    cp_async_wait_all();
+  }
+
+  // 2c. capacitor history after a completed (sub-)step, waveform samples
+  if (a & (ACT_TRAN_INIT | ACT_STEP)) {
+    for (int c = row; c < Tp.n_cap; c += R) {
+      const int2 tt = __ldg(&Tp.cap_term[c]);
+      const double vc = (tt.x >= 0 ? I.v[tt.x * ld + g] : 0.0) - (tt.y >= 0 ? I.v[tt.y * ld + g] : 0.0);
+      const size_t ci = (size_t)c * ld + g;
+      if (a & ACT_TRAN_INIT) {
+        I.cap_vp[ci] = vc;
+        I.cap_ip[ci] = 0.0;
+      } else {
+        const double C = __ldg(&Tp.cap_c[c]);
+        const double h = s_hsub[lane];
+        const double ic = P.method == KTRAN_TRAP ? (2.0 * C / h) * (vc - I.cap_vp[ci]) - I.cap_ip[ci]
+                                                 : (C / h) * (vc - I.cap_vp[ci]);
+        I.cap_vp[ci] = vc;
+        I.cap_ip[ci] = ic;
+      }
+    }
+  }
+  if ((a & ACT_WAVE) && I.n_wave > 0) {
+    const int done_step = I.st[g].step - 1;  // 1-based step just completed
+    if (done_step >= 1 && done_step <= I.wave_steps)
+      for (int w = row; w < I.n_wave; w += R) {
+        const int q = I.wave_pos[w];
+        I.wave[((size_t)g * I.wave_steps + (done_step - 1)) * I.n_wave + w] = q >= 0 ? I.v[q * ld + g] : 0.0;
+      }
   }
   __syncthreads();
 
-  // 3. vector updates (warp per instance)
-  for (int k = warp; k < cnt; k += nw) {
-    const int a = act[k];
-    if (!(a & (ACT_DAMP | ACT_ACCEPT | ACT_TRAN_INIT | ACT_STEP | ACT_RESEED | ACT_RESTART)))
-      continue;
-    const int inst = base + k;
-    double* x = I.x + (size_t)inst * n;
-    double* v = I.v + (size_t)inst * n;
-    if (a & ACT_RESEED) {
-      if (lane == 0) reference_seed(Tp, I, inst, v);
-      __syncwarp();
-      for (int i = lane; i < n; i += 32) x[i] = v[i];
-      continue;
-    }
-    if (a & ACT_RESTART) {
-      const double* vtp = I.v_tp + (size_t)inst * n;
-      for (int i = lane; i < n; i += 32) {
-        v[i] = vtp[i];
-        x[i] = vtp[i];
-      }
-      continue;
-    }
-    if (a & ACT_DAMP)
-      for (int i = lane; i < n; i += 32) x[i] = v[i] + 0.5 * (x[i] - v[i]);
-    if (a & ACT_ACCEPT)
-      for (int i = lane; i < n; i += 32) v[i] = x[i];
-    __syncwarp();
-    if (a & (ACT_STEP | ACT_TRAN_INIT)) {
-      double* vtp = I.v_tp + (size_t)inst * n;
-      for (int i = lane; i < n; i += 32) vtp[i] = v[i];
-    }
-    if ((a & ACT_WAVE) && I.n_wave > 0) {
-      const int done_step = I.st[inst].step - 1;  // 1-based step just completed
-      if (done_step >= 1 && done_step <= I.wave_steps)
-        for (int w = lane; w < I.n_wave; w += 32) {
-          const int q = I.wave_pos[w];
-          I.wave[((size_t)inst * I.wave_steps + (done_step - 1)) * I.n_wave + w] = q >= 0 ? v[q] : 0.0;
-        }
-    }
-    if (a & (ACT_TRAN_INIT | ACT_STEP)) {
-      for (int c = lane; c < Tp.n_cap; c += 32) {
-        const int2 tt = Tp.cap_term[c];
-        const double vc = (tt.x >= 0 ? v[tt.x] : 0.0) - (tt.y >= 0 ? v[tt.y] : 0.0);
-        const size_t ci = (size_t)inst * Tp.n_cap + c;
-        if (a & ACT_TRAN_INIT) {
-          I.cap_vp[ci] = vc;
-          I.cap_ip[ci] = 0.0;
-        } else {
-          const double C = Tp.cap_c[c];
-          const double h = hsub_s[k];
-          const double ic = P.method == KTRAN_TRAP
-                                ? (2.0 * C / h) * (vc - I.cap_vp[ci]) - I.cap_ip[ci]
-                                : (C / h) * (vc - I.cap_vp[ci]);
-          I.cap_vp[ci] = vc;
-          I.cap_ip[ci] = ic;
-        }
-      }
-    }
-  }
-  __syncthreads();
-
-  // 4. assembly of the instances that solve this round
-  const int ns = n_solve;
-  if (ns > 0) {
-    const T* Jall = reinterpret_cast<const T*>(I.J);
-    for (int e = tid; e < ns * nf; e += blockDim.x) {
-      const int j = e / nf, f = e - j * nf;
-      const int k = solve_list[j];
-      vals[(size_t)k * S + f] = Jall[(size_t)(base + k) * nf + f];
-    }
-    for (int e = tid; e < ns * n; e += blockDim.x) {
-      const int j = e / n, i = e - j * n;
-      const int k = solve_list[j];
-      const size_t o = (size_t)(base + k) * n + i;
-      vec[(size_t)k * Sv + i] = (T)(-(I.F[o] + gmin_s[k] * I.v[o]));
-    }
-    __syncthreads();
-    for (int e = tid; e < ns * n; e += blockDim.x) {
-      const int j = e / n, i = e - j * n;
-      const int k = solve_list[j];
-      vals[(size_t)k * S + __ldg(&Tp.lu_hdr[i].w)] += (T)gmin_s[k];
+  if (any_solve) {
+    if (a & ACT_SOLVE) {
+      const T gmin = (T)s_gmin[lane];
+      for (int i = row; i < n; i += R) A[__ldg(&Tp.lu_hdr[i].w) * L + lane] += gmin;
     }
     __syncthreads();
 
-    // 5. factor + solve: one instance per lane of warp 0
-    if (warp == 0 && lane < cnt && (act[lane] & ACT_SOLVE)) {
+    // 3. factor + solve: one lane per instance
+    if (tid < L && (s_act[tid] & ACT_SOLVE)) {
       const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
       const T growth = sizeof(T) == 8 ? (T)1e10 : (T)1e4;
-      const bool ok = FS::template run<T>(vals + (size_t)lane * S, vec + (size_t)lane * Sv, Tp,
-                                          tiny, growth);
-      sing_s[lane] = ok ? 0 : 1;
+      s_sing[tid] = lu_solve<T>(A + tid, Y + tid, L, Tp, rec, tiny, growth) ? 0 : 1;
     }
     __syncthreads();
 
-    // 6. x = v + dx
-    for (int k = warp; k < cnt; k += nw) {
-      const int a = act[k];
-      if (!(a & ACT_SOLVE) || sing_s[k]) continue;
-      const int inst = base + k;
-      double* x = I.x + (size_t)inst * n;
-      const double* v = I.v + (size_t)inst * n;
-      const T* dx = vec + (size_t)k * Sv;
-      const bool sanitize = (a & ACT_LIMIT) != 0;
-      for (int i = lane; i < n; i += 32) {
-        double xi = v[i] + (double)dx[i];
+    // 4. x = v + dx, then junction limiting level by level
+    const bool upd = (a & ACT_SOLVE) && !s_sing[lane];
+    const bool sanitize = (a & ACT_LIMIT) != 0;
+    if (upd)
+      for (int i = row; i < n; i += R) {
+        const size_t o = (size_t)i * ld + g;
+        double xi = I.v[o] + (double)Y[i * L + lane];
         if (sanitize && !isfinite(xi)) xi = 0.0;  // SafeUtils::sanitize_vector
-        x[i] = xi;
+        I.x[o] = xi;
       }
-      __syncwarp();
-      if (sanitize && Tp.n_dio > 0) limit_junctions_warp(Tp, x, v, lane);
+    if (Tp.n_dio > 0) {
+      const int lim = upd && sanitize;
+      if (__syncthreads_or(lim)) {
+        for (int lvl = 0; lvl < Tp.n_dio_levels; ++lvl) {
+          if (lim)
+            for (int d = row; d < Tp.n_dio; d += R)
+              if (__ldg(&Tp.dio_level[d]) == lvl) limit_one(Tp, d, I.x, I.v, ld, g);
+          __syncthreads();
+        }
+      }
     }
-    __syncthreads();
   }
 
-  // 7. singular pivots, junction limiting, bookkeeping (thread per instance)
-  if (tid < 32) {
-    int live = 0;
-    if (tid < cnt) {
-      const int inst = base + tid;
-      const int a = act[tid];
-      if ((a & ACT_SOLVE) && sing_s[tid]) {
-        // static pivots unusable: hand the solve to the partial-pivoting rescue
+  // 5. rescue hand-off, next evaluation point, bookkeeping (thread per lane,
+  //    all in warp 0)
+  if (tid < L) {
+    const unsigned mask = L == 32 ? kFull : ((1u << L) - 1u);
+    int live = 0, solved = 0, dcev = 0, trev = 0;
+    if (tid < cnt && s_live[tid]) {
+      const int act = s_act[tid];
+      trev = s_trev[tid];
+      dcev = !trev;
+      if ((act & ACT_SOLVE) && s_sing[tid]) {
         if (I.rescue_list) {
           const int slot = atomicAdd(I.rescue_count, 1);
           RescueItem it;
-          it.inst = inst;
-          it.act = a;
-          it.gmin = gmin_s[tid];
+          it.inst = g;
+          it.act = act;
+          it.gmin = s_gmin[tid];
           I.rescue_list[slot] = it;
         } else {
-          on_singular(Tp, I, inst);
+          on_singular(Tp, I, g);
         }
       }
-      const int md = I.st[inst].mode;
-      live = (md != MODE_DONE) ? (md == MODE_TRAN ? 2 : 1) : 0;
+      const InstState st2 = I.st[g];
+      solved = (act & ACT_SOLVE) && !s_sing[tid];
+      live = st2.mode != MODE_DONE;
+      set_eval_point(I, P, g, st2);
     }
-    const unsigned m = __ballot_sync(kFull, live != 0);
-    const unsigned mt = __ballot_sync(kFull, live == 2);
-    const unsigned ms = __ballot_sync(kFull, tid < cnt && (act[tid] & ACT_SOLVE) && !sing_s[tid]);
+    const int nlive = __popc(__ballot_sync(mask, live));
+    const int nsol = __popc(__ballot_sync(mask, solved));
+    const int ndc = __popc(__ballot_sync(mask, dcev));
+    const int ntr = __popc(__ballot_sync(mask, trev));
     if (tid == 0) {
-      if (m) atomicAdd(active, __popc(m));
+      if (nlive) atomicAdd(active, nlive);
       if (I.counters) {
-        // instances alive now are evaluated by the next round
-        if (m & ~mt) atomicAdd(&I.counters[0], (unsigned long long)__popc(m & ~mt));
-        if (mt) atomicAdd(&I.counters[1], (unsigned long long)__popc(mt));
-        if (ms) atomicAdd(&I.counters[2], (unsigned long long)__popc(ms));
+        if (ndc) atomicAdd(&I.counters[0], (unsigned long long)ndc);
+        if (ntr) atomicAdd(&I.counters[1], (unsigned long long)ntr);
+        if (nsol) atomicAdd(&I.counters[2], (unsigned long long)nsol);
       }
     }
   }
 }
 
-// Dense FP64 LU with partial pivoting for the flagged instances: the
-// semantics of solveSparse_LU's numeric phase (math/sparse_lu.cpp:216-312) on
-// the permuted system: pivot = largest |a| in the column (ties to the lower
-// row), singular below 1e-25, rows with |a| < 1e-30 skipped. One CTA per
-// solve, matrix in a global workspace slot, right-hand side in shared memory.
-#if !defined(KARAM_JIT)
+// ---------------------------------------------------------------------------
+// rescue of the solves whose static pivots failed: FP64 static pivots on the
+// Jacobian (working precision, widened), and when those fail too, dense FP64
+// LU with partial pivoting
+// -- the semantics of solveSparse_LU's numeric phase (math/sparse_lu.cpp:216-312)
+// on the permuted system: pivot = largest |a| in the column (ties to the
+// lower row), singular below 1e-25, rows with |a| < 1e-30 skipped. One CTA per
+// solve; the dense matrix in a global workspace slot, vectors in shared memory.
+// ---------------------------------------------------------------------------
 template <typename TJ>
 __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams P) {
-  extern __shared__ double rs[];
-  const int n = Tp.n, nf = Tp.nf;
-  double* b = rs;                                  // n
-  double* lval = b + n;                            // n
-  int* rows = reinterpret_cast<int*>(lval + n);    // n
+  extern __shared__ __align__(16) double rs[];
+  const int n = Tp.n, nv = Tp.nv;
+  // packed pivot records behind the vectors: rs + n + max(nv, n) doubles, n ints
+  int4* rec = nullptr;
+  if (Tp.lu_rec) {
+    rec = reinterpret_cast<int4*>(
+        (reinterpret_cast<uintptr_t>(rs + n + max(nv, n)) + sizeof(int) * n + 15) & ~uintptr_t(15));
+  }
+  const size_t ld = I.ld;
   __shared__ double red_v[8];
   __shared__ int red_r[8];
-  __shared__ int s_piv, s_cnt, s_sing;
+  __shared__ int s_piv, s_cnt, s_sing, s_ok;
   __shared__ double s_aii;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int total = *I.rescue_count;
+  if (blockIdx.x >= total) return;
+  if (rec) {
+    for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) rec[k] = __ldg(&Tp.lu_rec[k]);
+    __syncthreads();
+  }
   double* A = I.rescue_ws + (size_t)blockIdx.x * n * n;
   for (int e = blockIdx.x; e < total; e += gridDim.x) {
     const RescueItem item = I.rescue_list[e];
-    const int inst = item.inst;
+    const int g = item.inst;
     const double gmin = item.gmin;
-    const TJ* J = reinterpret_cast<const TJ*>(I.J) + (size_t)inst * nf;
-    for (size_t q = tid; q < (size_t)n * n; q += blockDim.x) A[q] = 0.0;
-    __syncthreads();
-    for (int f = tid; f < nf; f += blockDim.x)
-      A[(size_t)Tp.f_row[f] * n + Tp.f_colp[f]] = (double)J[f];
-    for (int i = tid; i < n; i += blockDim.x) {
-      const size_t o = (size_t)inst * n + i;
-      b[i] = -(I.F[o] + gmin * I.v[o]);
+    const TJ* J = reinterpret_cast<const TJ*>(I.J);
+    double* b = rs;  // n
+    // -- level 1 (mixed precision only; the FP64 path already ran it): static
+    //    pivots in FP64 on the value slots
+    if (tid == 0) s_ok = 0;
+    if (P.precision == KPREC_MIXED) {
+      double* As = rs + n;  // nv
+      for (int s = tid; s < nv; s += blockDim.x) As[s] = (double)J[(size_t)s * ld + g];
+      for (int i = tid; i < n; i += blockDim.x) {
+        const size_t o = (size_t)i * ld + g;
+        b[i] = -(I.F[o] + gmin * I.v[o]);
+      }
+      __syncthreads();
+      for (int i = tid; i < n; i += blockDim.x) As[Tp.lu_hdr[i].w] += gmin;
+      __syncthreads();
+      if (tid == 0) s_ok = lu_solve<double>(As, b, 1, Tp, rec, 1e-25, 1e10) ? 1 : 0;
     }
     __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) A[(size_t)i * n + i] += gmin;
-    if (tid == 0) s_sing = 0;
-    __syncthreads();
-
-    for (int i = 0; i < n; ++i) {
-      // pivot search + rows to eliminate
-      if (tid == 0) s_cnt = 0;
+    if (!s_ok) {
+      // -- level 2: dense partial pivoting
+      double* lval = rs + n;                          // n
+      int* rows = reinterpret_cast<int*>(lval + n);  // n
+      for (size_t q = tid; q < (size_t)n * n; q += blockDim.x) A[q] = 0.0;
       __syncthreads();
-      double best = -1.0;
-      int brow = n;
-      for (int r = i + tid; r < n; r += blockDim.x) {
-        const double a = fabs(A[(size_t)r * n + i]);
-        if (a > best || (a == best && r < brow)) {
-          best = a;
-          brow = r;
-        }
-        if (r > i && a >= 1e-30) rows[atomicAdd(&s_cnt, 1)] = r;
+      for (int s = tid; s < nv; s += blockDim.x) {
+        const int2 rc = Tp.slot_rc[s];
+        A[(size_t)rc.x * n + rc.y] = (double)J[(size_t)s * ld + g];
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(kFull, best, o);
-        const int orow = __shfl_xor_sync(kFull, brow, o);
-        if (ob > best || (ob == best && orow < brow)) {
-          best = ob;
-          brow = orow;
-        }
-      }
-      if (lane == 0) {
-        red_v[warp] = best;
-        red_r[warp] = brow;
+      for (int i = tid; i < n; i += blockDim.x) {
+        const size_t o = (size_t)i * ld + g;
+        b[i] = -(I.F[o] + gmin * I.v[o]);
       }
       __syncthreads();
-      if (tid == 0) {
-        double bv = red_v[0];
-        int br = red_r[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-          if (red_v[w] > bv || (red_v[w] == bv && red_r[w] < br)) {
-            bv = red_v[w];
-            br = red_r[w];
+      for (int i = tid; i < n; i += blockDim.x) A[(size_t)i * n + i] += gmin;
+      if (tid == 0) s_sing = 0;
+      __syncthreads();
+      for (int i = 0; i < n; ++i) {
+        if (tid == 0) s_cnt = 0;
+        __syncthreads();
+        double best = -1.0;
+        int brow = n;
+        for (int r = i + tid; r < n; r += blockDim.x) {
+          const double av = fabs(A[(size_t)r * n + i]);
+          if (av > best || (av == best && r < brow)) {
+            best = av;
+            brow = r;
           }
-        if (bv < 1e-25) s_sing = 1;
-        s_piv = br;
-        s_aii = fabs(A[(size_t)i * n + i]);
+          if (r > i && av >= 1e-30) rows[atomicAdd(&s_cnt, 1)] = r;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(kFull, best, o);
+          const int orow = __shfl_xor_sync(kFull, brow, o);
+          if (ob > best || (ob == best && orow < brow)) {
+            best = ob;
+            brow = orow;
+          }
+        }
+        if (lane == 0) {
+          red_v[warp] = best;
+          red_r[warp] = brow;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          double bv = red_v[0];
+          int br = red_r[0];
+          for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+            if (red_v[w] > bv || (red_v[w] == bv && red_r[w] < br)) {
+              bv = red_v[w];
+              br = red_r[w];
+            }
+          if (bv < 1e-25) s_sing = 1;
+          s_piv = br;
+          s_aii = fabs(A[(size_t)i * n + i]);
+        }
+        __syncthreads();
+        if (s_sing) break;
+        const int p = s_piv;
+        if (p != i) {
+          for (int c = tid; c < n; c += blockDim.x) {
+            const double t = A[(size_t)i * n + c];
+            A[(size_t)i * n + c] = A[(size_t)p * n + c];
+            A[(size_t)p * n + c] = t;
+          }
+          if (tid == 0) {
+            const double t = b[i];
+            b[i] = b[p];
+            b[p] = t;
+            // row p now holds the old row i: it stays in the list only if its
+            // entry in column i is not negligible
+            if (!(s_aii >= 1e-30))
+              for (int q = 0; q < s_cnt; ++q)
+                if (rows[q] == p) {
+                  rows[q] = rows[s_cnt - 1];
+                  s_cnt--;
+                  break;
+                }
+          }
+        }
+        __syncthreads();
+        const int m = s_cnt;
+        const double piv = A[(size_t)i * n + i];
+        for (int q = tid; q < m; q += blockDim.x) {
+          const int r = rows[q];
+          const double l = A[(size_t)r * n + i] / piv;
+          A[(size_t)r * n + i] = l;
+          lval[q] = l;
+        }
+        __syncthreads();
+        const int w = n - i - 1;
+        for (int e2 = tid; e2 < m * w; e2 += blockDim.x) {
+          const int q = e2 / w, c = i + 1 + (e2 - q * w);
+          A[(size_t)rows[q] * n + c] -= lval[q] * A[(size_t)i * n + c];
+        }
+        __syncthreads();
       }
-      __syncthreads();
-      if (s_sing) break;
-      const int p = s_piv;
-      if (p != i) {
-        for (int c = tid; c < n; c += blockDim.x) {
-          const double t = A[(size_t)i * n + c];
-          A[(size_t)i * n + c] = A[(size_t)p * n + c];
-          A[(size_t)p * n + c] = t;
+      if (!s_sing) {
+        for (int j = 0; j < n; ++j) {  // forward substitution, unit lower
+          const double bj = b[j];
+          for (int r = j + 1 + tid; r < n; r += blockDim.x) b[r] -= A[(size_t)r * n + j] * bj;
+          __syncthreads();
+        }
+        for (int j = n - 1; j >= 0; --j) {  // back substitution
+          if (tid == 0) b[j] /= A[(size_t)j * n + j];
+          __syncthreads();
+          const double xj = b[j];
+          for (int r = tid; r < j; r += blockDim.x) b[r] -= A[(size_t)r * n + j] * xj;
+          __syncthreads();
         }
         if (tid == 0) {
-          const double t = b[i];
-          b[i] = b[p];
-          b[p] = t;
-          // row p now holds the old row i: it stays in the list only if its
-          // entry in column i is not negligible
-          if (!(s_aii >= 1e-30))
-            for (int q = 0; q < s_cnt; ++q)
-              if (rows[q] == p) {
-                rows[q] = rows[s_cnt - 1];
-                s_cnt--;
-                break;
-              }
+          s_ok = 1;
+          if (I.counters) atomicAdd(&I.counters[4], 1ull);
         }
       }
       __syncthreads();
-      const int m = s_cnt;
-      const double piv = A[(size_t)i * n + i];
-      for (int q = tid; q < m; q += blockDim.x) {
-        const int r = rows[q];
-        const double l = A[(size_t)r * n + i] / piv;
-        A[(size_t)r * n + i] = l;
-        lval[q] = l;
-      }
-      __syncthreads();
-      const int w = n - i - 1;
-      for (int e2 = tid; e2 < m * w; e2 += blockDim.x) {
-        const int q = e2 / w, c = i + 1 + (e2 - q * w);
-        A[(size_t)rows[q] * n + c] -= lval[q] * A[(size_t)i * n + c];
-      }
-      __syncthreads();
     }
-    if (!s_sing) {
-      for (int j = 0; j < n; ++j) {  // forward substitution, unit lower
-        const double bj = b[j];
-        for (int r = j + 1 + tid; r < n; r += blockDim.x) b[r] -= A[(size_t)r * n + j] * bj;
-        __syncthreads();
-      }
-      for (int j = n - 1; j >= 0; --j) {  // back substitution
-        if (tid == 0) b[j] /= A[(size_t)j * n + j];
-        __syncthreads();
-        const double xj = b[j];
-        for (int r = tid; r < j; r += blockDim.x) b[r] -= A[(size_t)r * n + j] * xj;
-        __syncthreads();
-      }
-      double* x = I.x + (size_t)inst * n;
-      const double* v = I.v + (size_t)inst * n;
+    if (s_ok) {
       const bool sanitize = (item.act & ACT_LIMIT) != 0;
       for (int i = tid; i < n; i += blockDim.x) {
-        double xi = v[i] + b[i];
+        const size_t o = (size_t)i * ld + g;
+        double xi = I.v[o] + b[i];
         if (sanitize && !isfinite(xi)) xi = 0.0;
-        x[i] = xi;
+        I.x[o] = xi;
       }
       __syncthreads();
       if (tid == 0) {
-        if (sanitize && Tp.n_dio > 0) limit_junctions(Tp, x, v);
-        I.st[inst].rescued += 1;
+        if (sanitize)
+          for (int d = 0; d < Tp.n_dio; ++d) limit_one(Tp, d, I.x, I.v, ld, g);
+        I.st[g].rescued += 1;
         if (I.counters) atomicAdd(&I.counters[3], 1ull);
       }
     } else if (tid == 0) {
-      on_singular(Tp, I, inst);
+      on_singular(Tp, I, g);
+      set_eval_point(I, P, g, I.st[g]);
     }
     __syncthreads();
   }
 }
-#endif  // !KARAM_JIT
 
-#if !defined(KARAM_JIT)
-__global__ void k_tran_start(DevTopo T, DevInst I, int init_caps) {
-  const int inst = blockIdx.x;
-  if (inst >= I.ni) return;
-  InstState s = I.st[inst];
+// Moves every converged instance into the transient at step 1 (capacitor
+// history from the accepted point when init_caps). Thread per instance.
+__global__ void k_tran_start(DevTopo T, DevInst I, JobParams P, int init_caps) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= I.ni) return;
+  InstState s = I.st[g];
   if (s.status != KST_CONVERGED) return;
-  __syncthreads();
-  const double* v = I.v + (size_t)inst * T.n;
-  double* x = I.x + (size_t)inst * T.n;
-  for (int i = threadIdx.x; i < T.n; i += blockDim.x) x[i] = v[i];
-  if (init_caps)
-    for (int c = threadIdx.x; c < T.n_cap; c += blockDim.x) {
-      const int2 tt = T.cap_term[c];
-      const size_t ci = (size_t)inst * T.n_cap + c;
-      I.cap_vp[ci] = (tt.x >= 0 ? v[tt.x] : 0.0) - (tt.y >= 0 ? v[tt.y] : 0.0);
-      I.cap_ip[ci] = 0.0;
-    }
-  double* vtp = I.v_tp + (size_t)inst * T.n;
-  for (int i = threadIdx.x; i < T.n; i += blockDim.x) vtp[i] = v[i];
-  if (threadIdx.x == 0) {
-    if (I.counters) atomicAdd(&I.counters[1], 1ull);
-    s.mode = MODE_TRAN;
-    s.sub = SUB_NR;
-    s.step = 1;
-    s.first = 1;
-    s.it = 0;
-    s.depth = 0;
-    s.frac = 0;
-    s.status = KST_NOCONV;
-    I.st[inst] = s;
+  const size_t ld = I.ld;
+  for (int i = 0; i < T.n; ++i) {
+    const double vi = I.v[i * ld + g];
+    I.x[i * ld + g] = vi;
+    I.v_tp[i * ld + g] = vi;
   }
+  if (init_caps)
+    for (int c = 0; c < T.n_cap; ++c) {
+      const int2 tt = T.cap_term[c];
+      I.cap_vp[c * ld + g] = (tt.x >= 0 ? I.v[tt.x * ld + g] : 0.0) - (tt.y >= 0 ? I.v[tt.y * ld + g] : 0.0);
+      I.cap_ip[c * ld + g] = 0.0;
+    }
+  s.mode = MODE_TRAN;
+  s.sub = SUB_NR;
+  s.step = 1;
+  s.first = 1;
+  s.it = 0;
+  s.depth = 0;
+  s.frac = 0;
+  s.status = KST_NOCONV;
+  I.st[g] = s;
+  set_eval_point(I, P, g, s);
+  reset_reductions(I, g);
 }
-#endif  // !KARAM_JIT
 
-#if !defined(KARAM_JIT)
-__global__ void k_unpermute(const double* vp, const int* perm, double* out, int ni, int n) {
-  const size_t total = (size_t)ni * n;
+// Instance-interleaved permuted voltages -> instance-major node order.
+__global__ void k_unpermute(const double* vp, const int* perm, double* out, int ni, int ld, int n) {
+  const size_t total = (size_t)n * ld;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
        e += (size_t)gridDim.x * blockDim.x) {
-    const size_t inst = e / n;
-    const int p = (int)(e - inst * n);
-    out[inst * n + perm[p]] = vp[e];
+    const int p = (int)(e / ld);
+    const int g = (int)(e - (size_t)p * ld);
+    if (g < ni) out[(size_t)g * n + perm[p]] = vp[e];
   }
 }
-#endif  // !KARAM_JIT
 
+// Interleaves an instance-major [ni][n] host-order block into [n][ld] permuted.
+__global__ void k_interleave(const double* src, const int* perm, double* dst, int ni, int ld, int n) {
+  const size_t total = (size_t)n * ld;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int p = (int)(e / ld);
+    const int g = (int)(e - (size_t)p * ld);
+    dst[e] = g < ni ? src[(size_t)g * n + perm[p]] : 0.0;
+  }
+}
 
 }  // namespace knr
 #endif

@@ -1,16 +1,19 @@
-// nr_types.h -- data layout shared by the host driver, the statically compiled
-// kernels and the kernels compiled at run time for a topology (NVRTC).
-// No standard-library includes: the run-time compiler sees this text as is.
+// nr_types.h -- data layout shared by the host driver and the kernels.
 //
 // All vectors live in the permuted index space of the Min-Fill ordering
-// (position p holds unknown perm[p]); matrices live in the filled L+U pattern
-// of that ordering, row-major. Instance data is instance-major.
+// (position p holds unknown perm[p]). Matrix values live in "value slots":
+// the positions of the filled L+U pattern that the static-pivot elimination
+// can make non-zero (the unsymmetric structure of the stamps plus its fill),
+// numbered row-major.
+//
+// Per-instance data is instance-interleaved: item k of instance i sits at
+// [k * ld + i], ld = instance count rounded up to 32, so a warp that works on
+// one item (a node, a device, a slot) for consecutive instances reads and
+// writes whole 32-byte sectors, and every index load is a broadcast.
 #ifndef KARAM_NR_TYPES_H
 #define KARAM_NR_TYPES_H
 
-#if !defined(__CUDACC_RTC__)
 #include <vector_types.h>
-#endif
 
 // Per-instance status codes and selectors (mirror include/karam.h).
 #define KST_CONVERGED 0
@@ -21,10 +24,15 @@
 #define KTRAN_TRAP 1
 #define KSRC_PULSE 1
 
+// Evaluation + stamping blocks: devices held in shared memory at a time, and
+// items per block.
+#define KES_MAX_DEV 48
+#define KES_MAX_ITEMS 64
+
 enum { MODE_DC = 0, MODE_TRAN = 1, MODE_DONE = 2 };
 enum { SUB_NR = 0, SUB_POLISH = 1 };
 
-// Per-instance solver state (one 104-byte record).
+// Per-instance solver state (one 104-byte record, instance-major).
 struct InstState {
   int mode;       // MODE_*
   int sub;        // SUB_*
@@ -45,13 +53,13 @@ struct InstState {
   double prevF;   // previous accepted KCL residual (damping test)
   double prev_dv; // previous polishing update (stall test)
   double resid;   // last KCL residual seen
-  int rescued;    // linear solves redone by the partial-pivoting rescue
+  int rescued;    // linear solves redone by the rescue path
   int depth;      // transient step halvings in effect (sub-step = h / 2^depth)
   int frac;       // part of the current step done, in units of h / 2^max_halvings
   int halvings;   // transient restarts with a halved step
 };
 
-// One linear solve handed to the partial-pivoting rescue.
+// One linear solve handed to the rescue path.
 struct RescueItem {
   int inst;
   int act;
@@ -60,7 +68,7 @@ struct RescueItem {
 
 // Shared topology tables (device pointers).
 struct DevTopo {
-  int n, nf, n_mos, n_dio, n_res, n_cap, n_vs, n_is;
+  int n, nv, n_mos, n_dio, n_res, n_cap, n_vs, n_is;
   double temp_k;
   const int4* mos_term;     // d g s b (permuted, -1 = ground)
   const double2* mos_geo;   // {W/L, lambda}
@@ -80,45 +88,69 @@ struct DevTopo {
   const double* vs_pulse;   // [n_vs][7] (td tr tf pw per used; v1 v2 per instance)
   const int2* is_term;
   const double* is_amp;
-  const int* jt_off;
-  const int* jt_code;
+  // Jacobian linear part per value slot: R + V stamps pre-summed (jlin) and
+  // capacitor companions (jcap: conductance 2C/h_eff)
   const double* jlin_dc;
   const int* jcap_off;
   const int* jcap_code;
-  const int* ft_off;
-  const int* ft_code;
-  const int4* lu_hdr;       // off, nL, nU, dpos
-  const int* lu_data;       // Lrow[nL] Lpos[nL] Ucol[nU] Upos[nU] T[nL*nU]
-  const int* f_row;         // row of every filled position (permuted)
-  const int* f_colp;        // column of every filled position (permuted)
+  // Evaluation + stamping blocks (see es_blocks in topology.cpp):
+  //   es_block[b] = {item offset, items (-1: hub node walked in device chunks),
+  //                  device offset, devices}
+  //   es_item[k]  = {item (slot s < nv, node nv + i), term offset, terms, 0}
+  //   es_dev      = global device ids (MOSFETs, then n_mos + diode index)
+  //   es_jt       = slot device terms: sign | kind << 24 | local device
+  //   es_ft       = node terms {code, terminal a, terminal b, 0}, device codes
+  //                 carrying the local device; es_fc their coefficients (1/R,
+  //                 source amplitude, 2C, or 0)
+  int n_es_blocks;
+  const int4* es_block;
+  const int4* es_item;
+  const int* es_dev;
+  const int* es_jt;
+  const int4* es_ft;
+  const double* es_fc;
+  // LU program per pivot k: hdr = (off, nL, nU, diagonal slot); data at off =
+  // Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots)
+  const int4* lu_hdr;
+  const int* lu_data;
+  int lu_small;             // 1: every pivot has nL <= 2 and nU <= 2
+  const int4* lu_rec;       // packed pivot records when lu_small (2 int4 per pivot, see
+                            // pack_small_pivots in topology.cpp), else 0
+  const int2* slot_rc;      // (row, col) of every value slot (permuted)
   const int* seed_vs;       // permuted positive node per source (-1 = ground)
   const int* seed_anode;    // permuted anode per netlist diode (-1 = ground)
   int n_seed_anode;
 };
 
-// Per-instance device buffers.
+// Per-instance device buffers ([item][ld] unless noted).
 struct DevInst {
-  int ni;
-  const float* kp;          // [ni][n_mos] SoA order, or 0 = model card
-  const float* vth;         // [ni][n_mos], or 0 = model card
-  const double* vs_dc;      // [ni][n_vs]
-  const double* vs_v1;      // [ni][n_vs]
-  const double* vs_v2;      // [ni][n_vs]
-  double* v;                // [ni][n] accepted point
-  double* x;                // [ni][n] point under evaluation
-  double* F;                // [ni][n] KCL residual at x (device currents, no gmin)
-  double* Fmax;             // [ni]
-  void* J;                  // [ni][nf] Jacobian at x without gmin (float or double)
-  double* cap_vp;           // [ni][n_cap]
-  double* cap_ip;           // [ni][n_cap]
-  double* v_tp;             // [ni][n] voltages at the last accepted time point
+  int ni;                   // instances in the batch
+  int ld;                   // lane stride: ni rounded up to 32
+  const float* kp;          // [n_mos][ld] SoA order, or 0 = model card
+  const float* vth;         // [n_mos][ld], or 0 = model card
+  const double* vs_dc;      // [n_vs][ld]
+  const double* vs_v1;      // [n_vs][ld]
+  const double* vs_v2;      // [n_vs][ld]
+  double* v;                // [n][ld] accepted point
+  double* x;                // [n][ld] point under evaluation
+  double* F;                // [n][ld] KCL residual at x (device currents, no gmin)
+  void* J;                  // [nv][ld] Jacobian value slots at x without gmin (float or double)
+  unsigned long long* red_f;   // [ld] max |F| over nodes (bit pattern of a non-negative double)
+  unsigned long long* red_dv;  // [ld] max |x - v| over nodes (bit pattern)
+  int* red_flags;           // [ld] AND over nodes: bit 0 NR-converged, bit 1 polish-converged
+  double* ev_t;             // [ld] time of the point the next round evaluates
+  double* ev_heff;          // [ld] its companion step: < 0 not live, 0 DC, > 0 transient
+  double* cap_vp;           // [n_cap][ld]
+  double* cap_ip;           // [n_cap][ld]
+  double* v_tp;             // [n][ld] voltages at the last accepted time point
   InstState* st;            // [ni]
-  const double* seed;       // [ni][n] caller guesses (permuted) or 0
+  const double* seed;       // [n][ld] caller guesses (permuted) or 0
   double* rescue_ws;        // [rescue_slots][n][n] dense workspaces
   RescueItem* rescue_list;  // [ni]
   int* rescue_count;
   int rescue_slots;
-  unsigned long long* counters;  // [4]: evaluations DC, evaluations transient, solves, rescues
+  unsigned long long* counters;  // [5]: evaluations DC, evaluations transient, solves,
+                                 // rescues, rescues that needed dense partial pivoting
   double* wave;             // [ni][wave_steps][n_wave] node voltages after each step
   const int* wave_pos;      // permuted positions of the recorded nodes (-1 = ground)
   int n_wave, wave_steps;

@@ -288,35 +288,6 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   };
   for (auto& x : T.trip) x.f = fp(T.iperm[x.row], T.iperm[x.col]);
 
-  // Evaluation gather tables, summation order = triplet order.
-  std::vector<std::vector<int>> jt(nf), jc(nf);
-  T.jlin_dc.assign(nf, 0.0);
-  for (auto& x : T.trip) {
-    switch (x.kind) {
-      case SS_RES: {
-        double g = 1.0 / T.res[x.idx].val;
-        T.jlin_dc[x.f] += x.neg ? -g : g;
-        break;
-      }
-      case SS_VS:
-        T.jlin_dc[x.f] += x.neg ? -1.0e3 : 1.0e3;
-        break;
-      case SS_CAP:
-        jc[x.f].push_back(term(0, x.idx, x.neg));
-        break;
-      case SS_DIO:
-        jt[x.f].push_back(term(JK_DIO_G, x.idx, x.neg));
-        break;
-      case SS_MOS_GDS:
-        jt[x.f].push_back(term(JK_MOS_GDS, x.idx, x.neg));
-        break;
-      case SS_MOS_GM:
-        jt[x.f].push_back(term(JK_MOS_GM, x.idx, x.neg));
-        break;
-      default:
-        break;  // gmb (always 0 in the level-1 kernel) and gmin are not gathered
-    }
-  }
   auto flatten = [](const std::vector<std::vector<int>>& v, std::vector<int>& off,
                     std::vector<int>& code) {
     off.assign(v.size() + 1, 0);
@@ -327,9 +298,6 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
     }
     off[v.size()] = (int)code.size();
   };
-  flatten(jt, T.jt_off, T.jt_code);
-  flatten(jc, T.jcap_off, T.jcap_code);
-
   // KCL gather tables per permuted node: currents leaving the node.
   std::vector<std::vector<int>> ft(n);
   auto two = [&](int n1, int n2, int kind, int idx) {
@@ -390,6 +358,96 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
     for (int i : L)
       for (int j : U) T.lu_data.push_back(fp(i, j));
     T.lu_ops += nl + nl * nu;
+  }
+
+  // Value slots: the filled positions the static-pivot elimination can make
+  // non-zero (every position the program reads or writes), numbered
+  // row-major. The device stores and factors only these.
+  T.f_slot.assign(nf, -1);
+  for (int k = 0; k < n; ++k) {
+    const int off = T.lu_hdr[4 * k], nl = T.lu_hdr[4 * k + 1], nu = T.lu_hdr[4 * k + 2];
+    T.f_slot[T.lu_hdr[4 * k + 3]] = 0;
+    for (int q = off + nl; q < off + 2 * nl; ++q) T.f_slot[T.lu_data[q]] = 0;
+    for (int q = off + 2 * nl + nu; q < off + 2 * nl + 2 * nu + nl * nu; ++q) T.f_slot[T.lu_data[q]] = 0;
+  }
+  T.nv = 0;
+  T.slot_row.clear();
+  T.slot_col.clear();
+  for (int i = 0; i < n; ++i)
+    for (int f = T.f_row_ptr[i]; f < T.f_row_ptr[i + 1]; ++f)
+      if (T.f_slot[f] >= 0) {
+        T.f_slot[f] = T.nv++;
+        T.slot_row.push_back(i);
+        T.slot_col.push_back(T.f_col[f]);
+      }
+  for (int k = 0; k < n; ++k) {
+    const int off = T.lu_hdr[4 * k], nl = T.lu_hdr[4 * k + 1], nu = T.lu_hdr[4 * k + 2];
+    T.lu_hdr[4 * k + 3] = T.f_slot[T.lu_hdr[4 * k + 3]];
+    for (int q = off + nl; q < off + 2 * nl; ++q) T.lu_data[q] = T.f_slot[T.lu_data[q]];
+    for (int q = off + 2 * nl + nu; q < off + 2 * nl + 2 * nu + nl * nu; ++q)
+      T.lu_data[q] = T.f_slot[T.lu_data[q]];
+  }
+
+  // Jacobian gather tables per value slot, summation order = triplet order.
+  std::vector<std::vector<int>> jt(T.nv), jc(T.nv);
+  T.jlin_dc.assign(T.nv, 0.0);
+  for (auto& x : T.trip) {
+    if (x.kind == SS_MOS_GMB || x.kind == SS_GMIN) continue;  // gmb is always 0; gmin is added per solve
+    const int sl = T.f_slot[x.f];
+    require(sl >= 0, "a stamped position is outside the LU structure");
+    switch (x.kind) {
+      case SS_RES: {
+        double g = 1.0 / T.res[x.idx].val;
+        T.jlin_dc[sl] += x.neg ? -g : g;
+        break;
+      }
+      case SS_VS:
+        T.jlin_dc[sl] += x.neg ? -1.0e3 : 1.0e3;
+        break;
+      case SS_CAP:
+        jc[sl].push_back(term(0, x.idx, x.neg));
+        break;
+      case SS_DIO:
+        jt[sl].push_back(term(JK_DIO_G, x.idx, x.neg));
+        break;
+      case SS_MOS_GDS:
+        jt[sl].push_back(term(JK_MOS_GDS, x.idx, x.neg));
+        break;
+      case SS_MOS_GM:
+        jt[sl].push_back(term(JK_MOS_GM, x.idx, x.neg));
+        break;
+      default:
+        break;
+    }
+  }
+  flatten(jt, T.jt_off, T.jt_code);
+  flatten(jc, T.jcap_off, T.jcap_code);
+
+  // Packed pivot records for programs whose pivots all have nL, nU <= 2 (2 int4
+  // per pivot): w0 = diagonal slot | nL << 24 | nU << 28; then 16-bit pairs
+  // (Lrow0, Lrow1), (Lslot0, Lslot1), (Uslot0, Uslot1), (T00, T01), (T10, T11),
+  // (Ucol0, Ucol1), 0.
+  T.lu_small = T.n < 65536 && T.nv < 65536;
+  for (int k = 0; k < n && T.lu_small; ++k)
+    if (T.lu_hdr[4 * k + 1] > 2 || T.lu_hdr[4 * k + 2] > 2) T.lu_small = false;
+  T.lu_rec.clear();
+  if (T.lu_small) {
+    T.lu_rec.assign(8 * (size_t)n, 0);
+    auto pk = [](int lo, int hi) { return (int)((uint32_t)lo | ((uint32_t)hi << 16)); };
+    for (int k = 0; k < n; ++k) {
+      const int off = T.lu_hdr[4 * k], nl = T.lu_hdr[4 * k + 1], nu = T.lu_hdr[4 * k + 2];
+      const int* d = &T.lu_data[off];
+      auto at = [&](int cnt, int base, int i) { return i < cnt ? d[base + i] : 0; };
+      int* w = &T.lu_rec[8 * (size_t)k];
+      w[0] = T.lu_hdr[4 * k + 3] | (nl << 24) | (nu << 28);
+      w[1] = pk(at(nl, 0, 0), at(nl, 0, 1));
+      w[2] = pk(at(nl, nl, 0), at(nl, nl, 1));
+      w[3] = pk(at(nu, 2 * nl + nu, 0), at(nu, 2 * nl + nu, 1));
+      const int tb = 2 * nl + 2 * nu;
+      w[4] = pk(nl > 0 && nu > 0 ? d[tb] : 0, nl > 0 && nu > 1 ? d[tb + 1] : 0);
+      w[5] = pk(nl > 1 && nu > 0 ? d[tb + nu] : 0, nl > 1 && nu > 1 ? d[tb + nu + 1] : 0);
+      w[6] = pk(at(nu, 2 * nl, 0), at(nu, 2 * nl, 1));
+    }
   }
 
   // Junction limiting constants (applyPnJunctionLimits, circuitsim_solver.cpp:118-169):
@@ -542,6 +600,194 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
   return out;
 }
 
+namespace {
+
+// KCL term records (terminals + coefficient per term of ft_code).
+void node_term_records(Topology& T) {
+  T.ft_a.clear();
+  T.ft_b.clear();
+  T.ft_coef.clear();
+  for (int c : T.ft_code) {
+    const int kind = (c >> 24) & 0x7f, idx = c & 0xffffff;
+    int a = -1, b = -1;
+    double coef = 0.0;
+    switch (kind) {
+      case FK_RES:
+        a = T.res_term[2 * idx];
+        b = T.res_term[2 * idx + 1];
+        coef = 1.0 / T.res[idx].val;
+        break;
+      case FK_VS:
+        a = T.vs_term[2 * idx];
+        b = T.vs_term[2 * idx + 1];
+        break;
+      case FK_IS:
+        coef = T.isrc[idx].val;
+        break;
+      case FK_CAP:
+        a = T.cap_term[2 * idx];
+        b = T.cap_term[2 * idx + 1];
+        coef = 2.0 * T.cap[idx].val;
+        break;
+      default:
+        break;
+    }
+    T.ft_a.push_back(a);
+    T.ft_b.push_back(b);
+    T.ft_coef.push_back(coef);
+  }
+}
+
+// Packs the stamp items into evaluation + stamping blocks. Items go in row
+// order (the slots of a row, then its node), so a block covers a stretch of
+// the ordering and the devices it needs are mostly its own; a device shared
+// by two blocks is evaluated by both.
+void es_blocks(Topology& T) {
+  const int n = T.n, nv = T.nv, nm = (int)T.mos.size();
+  T.es_block.clear();
+  T.es_item.clear();
+  T.es_dev.clear();
+  T.es_jt.clear();
+  T.es_ft.clear();
+  T.es_fc.clear();
+  T.es_max_dev = kEsMaxDev;
+  // device of a slot term / node term (-1: none)
+  auto slot_dev = [&](int c) {
+    const int kind = (c >> 24) & 0x7f, idx = c & 0xffffff;
+    return kind == JK_DIO_G ? nm + idx : idx;
+  };
+  auto node_dev = [&](int c) {
+    const int kind = (c >> 24) & 0x7f, idx = c & 0xffffff;
+    if (kind == FK_DIO) return nm + idx;
+    if (kind == FK_MOS) return idx;
+    return -1;
+  };
+  auto item_devs = [&](int it, std::vector<int>& out) {
+    out.clear();
+    if (it < nv) {
+      for (int q = T.jt_off[it]; q < T.jt_off[it + 1]; ++q) out.push_back(slot_dev(T.jt_code[q]));
+    } else {
+      const int i = it - nv;
+      for (int q = T.ft_off[i]; q < T.ft_off[i + 1]; ++q) {
+        const int d = node_dev(T.ft_code[q]);
+        if (d >= 0) out.push_back(d);
+      }
+    }
+  };
+  // item order: row by row, slots then the node
+  std::vector<int> order;
+  {
+    int s = 0;
+    for (int r = 0; r < n; ++r) {
+      while (s < nv && T.slot_row[s] == r) order.push_back(s++);
+      order.push_back(nv + r);
+    }
+  }
+  std::vector<int> cur_items, cur_devs, devs;
+  std::unordered_map<int, int> local;
+  auto emit = [&](const std::vector<int>& items, const std::vector<int>& dlist, bool) {
+    if (items.empty()) return;
+    std::unordered_map<int, int> lid;
+    for (size_t k = 0; k < dlist.size(); ++k) lid[dlist[k]] = (int)k;
+    T.es_block.push_back((int)T.es_item.size() / 4);
+    T.es_block.push_back((int)items.size());
+    T.es_block.push_back((int)T.es_dev.size());
+    T.es_block.push_back((int)dlist.size());
+    T.es_dev.insert(T.es_dev.end(), dlist.begin(), dlist.end());
+    for (int it : items) {
+      T.es_item.push_back(it);
+      if (it < nv) {
+        T.es_item.push_back((int)T.es_jt.size());
+        T.es_item.push_back(T.jt_off[it + 1] - T.jt_off[it]);
+        T.es_item.push_back(0);
+        for (int q = T.jt_off[it]; q < T.jt_off[it + 1]; ++q) {
+          const int c = T.jt_code[q];
+          T.es_jt.push_back((c & int32_t(0xFF000000u)) | lid.at(slot_dev(c)));
+        }
+      } else {
+        const int i = it - nv;
+        T.es_item.push_back((int)T.es_ft.size() / 4);
+        T.es_item.push_back(T.ft_off[i + 1] - T.ft_off[i]);
+        T.es_item.push_back(0);
+        for (int q = T.ft_off[i]; q < T.ft_off[i + 1]; ++q) {
+          const int c = T.ft_code[q];
+          const int d = node_dev(c);
+          T.es_ft.push_back(d >= 0 ? ((c & int32_t(0xFF000000u)) | lid.at(d)) : c);
+          T.es_ft.push_back(T.ft_a[q]);
+          T.es_ft.push_back(T.ft_b[q]);
+          T.es_ft.push_back(0);
+          T.es_fc.push_back(T.ft_coef[q]);
+        }
+      }
+    }
+  };
+  for (int it : order) {
+    item_devs(it, devs);
+    std::vector<int> fresh;
+    for (int d : devs)
+      if (!local.count(d) && std::find(fresh.begin(), fresh.end(), d) == fresh.end()) fresh.push_back(d);
+    std::vector<int> own;  // the item's own distinct devices, in term order
+    for (int d : devs)
+      if (std::find(own.begin(), own.end(), d) == own.end()) own.push_back(d);
+    if ((int)own.size() > kEsMaxDev) {
+      // hub item (node or slot): a block of its own that walks its terms in
+      // chunks of kEsMaxDev device terms, one device per term occurrence, so
+      // the local index grows with the term order
+      emit(cur_items, cur_devs, false);
+      cur_items.clear();
+      cur_devs.clear();
+      local.clear();
+      T.es_block.push_back((int)T.es_item.size() / 4);
+      T.es_block.push_back(-1);
+      T.es_block.push_back((int)T.es_dev.size());
+      T.es_block.push_back((int)devs.size());
+      T.es_item.push_back(it);
+      int occ = 0;
+      if (it < nv) {  // a hub slot, e.g. the supply diagonal
+        T.es_item.push_back((int)T.es_jt.size());
+        T.es_item.push_back(T.jt_off[it + 1] - T.jt_off[it]);
+        T.es_item.push_back(0);
+        for (int q = T.jt_off[it]; q < T.jt_off[it + 1]; ++q) {
+          const int c = T.jt_code[q];
+          T.es_dev.push_back(slot_dev(c));
+          T.es_jt.push_back((c & int32_t(0xFF000000u)) | occ++);
+        }
+        continue;
+      }
+      const int i = it - nv;
+      T.es_item.push_back((int)T.es_ft.size() / 4);
+      T.es_item.push_back(T.ft_off[i + 1] - T.ft_off[i]);
+      T.es_item.push_back(0);
+      for (int q = T.ft_off[i]; q < T.ft_off[i + 1]; ++q) {
+        const int c = T.ft_code[q];
+        const int d = node_dev(c);
+        if (d >= 0) T.es_dev.push_back(d);
+        T.es_ft.push_back(d >= 0 ? ((c & int32_t(0xFF000000u)) | occ++) : c);
+        T.es_ft.push_back(T.ft_a[q]);
+        T.es_ft.push_back(T.ft_b[q]);
+        T.es_ft.push_back(0);
+        T.es_fc.push_back(T.ft_coef[q]);
+      }
+      continue;
+    }
+    if ((int)(cur_devs.size() + fresh.size()) > kEsMaxDev || (int)cur_items.size() >= kEsMaxItems) {
+      emit(cur_items, cur_devs, false);
+      cur_items.clear();
+      cur_devs.clear();
+      local.clear();
+      fresh = own;
+    }
+    for (int d : fresh) {
+      local[d] = (int)cur_devs.size();
+      cur_devs.push_back(d);
+    }
+    cur_items.push_back(it);
+  }
+  emit(cur_items, cur_devs, false);
+}
+
+}  // namespace
+
 Topology build_topology(const karam_netlist* nl) {
   Topology T;
   tensorize(nl, T);
@@ -550,6 +796,8 @@ Topology build_topology(const karam_netlist* nl) {
   std::vector<std::vector<int>> urow;
   symbolic(T, urow);
   device_tables(T, urow);
+  node_term_records(T);
+  es_blocks(T);
   return T;
 }
 

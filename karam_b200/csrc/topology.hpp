@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/karam.h"
+#include "nr_types.h"
 
 namespace karam {
 
@@ -69,18 +70,41 @@ struct Topology {
   int fill_in = 0;
   std::vector<int> f_diag;  // filled position of (k, k)
 
+  // ---- value slots: filled positions the static-pivot elimination can make
+  //      non-zero (the unsymmetric stamp structure + its fill), row-major ----
+  int nv = 0;
+  std::vector<int> f_slot;                   // filled position -> slot (-1: always zero)
+  std::vector<int> slot_row, slot_col;       // permuted (row, col) per slot
+
   // ---- gather tables (permuted space) ----
-  std::vector<int> jt_off, jt_code;          // per filled position
-  std::vector<double> jlin_dc;               // R + V stamps per filled position
-  std::vector<int> jcap_off, jcap_code;      // capacitor stamps per filled position (G = C * scale)
+  std::vector<int> jt_off, jt_code;          // device terms per slot
+  std::vector<double> jlin_dc;               // R + V stamps per slot
+  std::vector<int> jcap_off, jcap_code;      // capacitor stamps per slot (G = 2C / h_eff)
   std::vector<int> ft_off, ft_code;          // per permuted node
 
-  // ---- LU program: per pivot k (off, nL, nU, dpos); data at off =
-  //      Lrow[nL] Lpos[nL] Ucol[nU] Upos[nU] T[nL*nU] (update targets, row-major) ----
+  // ---- LU program: per pivot k (off, nL, nU, diagonal slot); data at off =
+  //      Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots, row-major) ----
   std::vector<int> lu_hdr;   // 4 ints per pivot
   std::vector<int> lu_data;
+  bool lu_small = false;     // every pivot has nL <= 2 and nU <= 2 (and n, nv < 65536)
+  std::vector<int> lu_rec;   // packed pivot records (8 ints per pivot) when lu_small
   int lu_ops = 0;
   int max_d = 0;
+
+  // ---- evaluation + stamping blocks: the stamp items (value slots 0..nv-1,
+  //      nodes nv..nv+n-1) packed in row order into blocks whose devices fit
+  //      one CTA's shared memory; a node with more devices than that forms a
+  //      block of its own that walks its devices in chunks ----
+  std::vector<int> ft_a, ft_b;              // per KCL term: element terminals (permuted, -1 ground)
+  std::vector<double> ft_coef;              // 1/R, source amplitude, 2C or 0
+  std::vector<int> es_block;                // 4 per block: item offset, items, device offset, devices
+  std::vector<int> es_item;                 // 4 per item: item id, term offset, terms, 0
+  std::vector<int> es_dev;                  // global device ids (MOSFETs, then n_mos + diode)
+  std::vector<int> es_jt;                   // slot device terms: sign | kind << 24 | local device
+  std::vector<int> es_ft;                   // node terms: 4 per term {code, a, b, 0}; device codes
+                                            // carry the local device index
+  std::vector<double> es_fc;                // node term coefficients
+  int es_max_dev = 0;                       // devices per chunk (shared-memory budget)
 
   // ---- junction limiting (SoA diode order) ----
   std::vector<double> dio_lim;  // 2 per diode: Vt * T/Tnom, vcrit
@@ -98,6 +122,11 @@ struct Topology {
 
 // Builds the full topology; throws std::runtime_error with a message on bad input.
 Topology build_topology(const karam_netlist* nl);
+
+// Devices one evaluation + stamping CTA holds in shared memory at a time, and
+// items of one evaluation + stamping block (nr_types.h).
+constexpr int kEsMaxDev = KES_MAX_DEV;
+constexpr int kEsMaxItems = KES_MAX_ITEMS;
 
 // Min-Fill on an explicit factor list (exposed for tests of the ordering).
 struct MinFillResult {
