@@ -249,11 +249,10 @@ def run_reference(args, dist):
 
 def eval_stamp_bytes(info, mixed, tran=False):
     """Algorithmic HBM bytes of one evaluation + stamping of one instance
-    (k_eval + k_stamp): KP/VTO read (FP32), the trial point x and the accepted
-    point v read (FP64; v for the convergence test), the Jacobian value slots
-    written (FP32 or FP64), the KCL residual written (FP64), and in transient
-    the capacitor history v_prev read. Device values pass through an
-    L2-resident scratch and are not counted."""
+    (k_es): KP/VTO read (FP32), the trial point x and the accepted point v read
+    (FP64; v for the convergence test), the Jacobian value slots written (FP32
+    or FP64), the KCL residual written (FP64), and in transient the capacitor
+    history v_prev read. Device values live in shared memory only."""
     n, nm, nv, nc = info["n"], info["n_mos"], info["n_slots"], info["n_cap"]
     b = 8 * nm + 8 * n + 8 * n + (4 if mixed else 8) * nv + 8 * n
     return b + (8 * nc if tran else 0)
@@ -368,7 +367,7 @@ def run_karam(args, dist):
         e2e_solves += sum(TRAN_STEPS + 1 for s in st if s["status"] == A.ST_CONVERGED)
     e2e_value = dist.sum(e2e_solves) / dist.max(e2e_t)
 
-    # rooflines: evaluation + stamping (k_eval + k_stamp) and factor/solve
+    # rooflines: evaluation + stamping (k_es) and factor/solve
     # (k_lu), algorithmic bytes per live instance-round over their event time
     peak, peak_kind = measured_peaks()
     es_b = evals_dc * eval_stamp_bytes(info, True) + evals_tran * eval_stamp_bytes(info, True, True)
@@ -377,7 +376,7 @@ def run_karam(args, dist):
     lu_gbs = lu_b / (lu_ms / 1e3) / 1e9 if lu_ms else 0.0
     tot_k = eval_ms + lu_ms + rescue_ms
     kernels = {
-        "k_eval+k_stamp<float>": {"ms_per_step": eval_ms / args.steps, "share": eval_ms / tot_k,
+        "k_es<float>": {"ms_per_step": eval_ms / args.steps, "share": eval_ms / tot_k,
                                   "achieved_gbs": es_gbs, "frac": es_gbs / peak,
                                   "bytes_per_instance_eval": eval_stamp_bytes(info, True, True)},
         "k_lu<float>": {"ms_per_step": lu_ms / args.steps, "share": lu_ms / tot_k,
@@ -385,7 +384,7 @@ def run_karam(args, dist):
                         "bytes_per_instance_round": lu_bytes(info, True), "lanes_per_cta": lanes},
         "k_rescue": {"ms_per_step": rescue_ms / args.steps, "share": rescue_ms / tot_k},
     }
-    dom = "k_lu<float>" if lu_ms >= eval_ms else "k_eval+k_stamp<float>"
+    dom = "k_lu<float>" if lu_ms >= eval_ms else "k_es<float>"
     roofline = {
         "kernel": dom, "bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak,
         "unit": "GB/s", "frac": kernels[dom]["frac"], "peak_source": peak_kind,
@@ -404,178 +403,10 @@ def run_karam(args, dist):
         es_us.append(1e3 * prob.timing()["eval_ms"])
     es_us = statistics.median(es_us[1:])
     es_bytes = ni * eval_stamp_bytes(info, mixed=True)
-    eval_roofline = {"kernel": "k_eval + k_stamp<float>, all instances live", "bound": "hbm",
+    eval_roofline = {"kernel": "k_es<float>, all instances live", "bound": "hbm",
                      "achieved": es_bytes / (es_us / 1e6) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": es_bytes / (es_us / 1e6) / 1e9 / peak, "launch_pair_us": es_us,
                      "algorithmic_bytes": es_bytes}
-
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "MC inverter chain 256 stages + 64 diode clamps, n=322, "
-                               "DC + 200 BE steps of 1 ps", "instances_per_step": count,
-                   "solver": "oracle/_ref: reference sources, solveSparse_LU"
-                   if kind == "reference" else "oracle port (restatement)"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
-                         "sample": sample},
-        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-
-
-def eval_stamp_bytes(info, mixed, tran=False):
-    """Algorithmic HBM bytes of one evaluation + stamping of one instance
-    (k_eval + k_stamp): KP/VTO read (FP32), the trial point x and the accepted
-    point v read (FP64; v for the convergence test), the Jacobian value slots
-    written (FP32 or FP64), the KCL residual written (FP64), and in transient
-    the capacitor history v_prev read. Device values pass through an
-    L2-resident scratch and are not counted."""
-    n, nm, nv, nc = info["n"], info["n_mos"], info["n_slots"], info["n_cap"]
-    b = 8 * nm + 8 * n + 8 * n + (4 if mixed else 8) * nv + 8 * n
-    return b + (8 * nc if tran else 0)
-
-
-def lu_bytes(info, mixed):
-    """Algorithmic HBM bytes of one control-flow + factor/solve pass of one
-    instance (k_lu): the Jacobian value slots and the KCL residual read, x and
-    v read and written back, the state record read and written."""
-    n, nv = info["n"], info["n_slots"]
-    return (4 if mixed else 8) * nv + 8 * n + 4 * 8 * n + 2 * 104
-
-
-def run_karam(args, dist):
-    import karam_b200 as K
-    from karam_b200 import _abi as A
-
-    ni = args.instances
-    nl, inst = workload(ni, dist.rank * ni)
-    ctx = K.Context(dist.local)
-    prob = K.Problem(ctx, nl, max_instances=ni)
-    prob.set_instances(inst)
-    info = prob.info
-
-    flush = None
-    try:
-        import torch
-        if torch.cuda.is_available():
-            flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32,
-                                device=f"cuda:{dist.local}")
-    except Exception:
-        flush = None
-
-    def l2_flush():
-        if flush is not None:
-            flush.zero_()
-            import torch
-            torch.cuda.synchronize()
-
-    def job(opts):
-        prob.run_mc_device(DT, TRAN_STEPS, A.TRAN_BE, opts)
-        t = prob.timing()
-        _, st = prob.read_results()
-        conv = sum(1 for s in st if s["status"] == A.ST_CONVERGED)
-        return t, conv, st
-
-    mixed = K.options(precision=A.PREC_MIXED, max_halvings=MAX_HALVINGS, **POLISH)
-    fp64 = K.options(precision=A.PREC_FP64, max_halvings=MAX_HALVINGS, **POLISH)
-
-    for _ in range(args.warmup):
-        l2_flush()
-        job(mixed)
-
-    clocks = Clocks(dist.local)
-    dist.barrier()
-    clocks.start()
-    tot_ms = 0.0
-    solves = 0
-    eval_ms = lu_ms = rescue_ms = 0.0
-    evals_dc = evals_tran = 0
-    launches = 0
-    rescues = 0
-    rounds = 0
-    conv_min = ni
-    for _ in range(args.steps):
-        l2_flush()
-        t, conv, st = job(mixed)
-        tot_ms += t["job_ms"]
-        solves += conv * (TRAN_STEPS + 1)
-        eval_ms += t["eval_ms"]
-        lu_ms += t["lu_ms"]
-        rescue_ms += t["rescue_ms"]
-        rounds += t["rounds"]
-        evals_dc += t["evals_dc"]
-        evals_tran += t["evals_tran"]
-        rescues += t["rescues"]
-        launches += (t["eval_launches"] + t["lu_launches"] + t["rescue_launches"]
-                     + t["other_launches"])
-        lanes = t["lanes"]
-        conv_min = min(conv_min, conv)
-    clk = clocks.stop()
-    dist.barrier()
-    v_mixed, st_mixed = prob.read_results()
-    t_max = dist.max(tot_ms)
-    all_solves = dist.sum(solves)
-    value = all_solves / (t_max / 1e3)
-
-    # plain FP64 GPU Newton path, same job and timing rules
-    fp_ms = 0.0
-    fp_solves = 0
-    for _ in range(max(1, args.warmup // 3)):
-        job(fp64)
-    for _ in range(args.steps):
-        l2_flush()
-        t, conv, _ = job(fp64)
-        fp_ms += t["job_ms"]
-        fp_solves += conv * (TRAN_STEPS + 1)
-    v_fp64, _ = prob.read_results()
-    fp_value = dist.sum(fp_solves) / (dist.max(fp_ms) / 1e3)
-
-    # end to end through the C ABI with host buffers
-    h2d = inst.mos_kp.nbytes + inst.mos_vto.nbytes
-    d2h = ni * info["n"] * 8 + ni * A.C.sizeof(A.KaramInstanceStats)
-    e2e_t = 0.0
-    e2e_solves = 0
-    for _ in range(args.steps):
-        l2_flush()
-        dist.barrier()
-        t0 = time.perf_counter()
-        v, st = prob.run_mc(inst, DT, TRAN_STEPS, A.TRAN_BE, mixed)
-        e2e_t += time.perf_counter() - t0
-        e2e_solves += sum(TRAN_STEPS + 1 for s in st if s["status"] == A.ST_CONVERGED)
-    e2e_value = dist.sum(e2e_solves) / dist.max(e2e_t)
-
-    # roofline of the dominant kernel: the fused NR round
-    b_dc, b_tran = round_bytes(info)
-    peak, peak_kind = measured_peaks()
-    achieved = (evals_dc * b_dc + evals_tran * b_tran) / (round_ms / 1e3) / 1e9 if round_ms else 0.0
-    roofline = {
-        "kernel": "k_round<float> (evaluation + stamping + control + LU, fused)", "bound": "hbm",
-        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "peak_source": peak_kind,
-        "traffic": profiled_traffic(),
-        "algorithmic_bytes_per_instance_round": {"dc": b_dc, "tran": b_tran},
-        "avg_launch_us": 1e3 * round_ms / rounds if rounds else None,
-        "time_share": round_ms / (round_ms + rescue_ms) if round_ms + rescue_ms > 0 else None,
-        "lanes_per_cta": lanes,
-    }
-
-    # evaluation + stamping alone at full batch (an evaluation-only launch of
-    # k_round writing the Jacobian and residual to HBM), timed with CUDA events
-    v_probe = np.repeat(v_mixed[:1], ni, axis=0) if len(v_mixed) else None
-    es_us = []
-    for _ in range(5):
-        l2_flush()
-        prob.eval_stamp(v_probe, A.PREC_MIXED)
-        es_us.append(1e3 * prob.timing()["round_ms"])
-    es_us = statistics.median(es_us[1:])
-    es_bytes = ni * eval_stamp_bytes(info, mixed=True)
-    eval_roofline = {"kernel": "k_round<float>, evaluation-only launch", "bound": "hbm",
-                     "achieved": es_bytes / (es_us / 1e6) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": es_bytes / (es_us / 1e6) / 1e9 / peak, "launch_us": es_us,
-                     "algorithmic_bytes_per_launch": es_bytes}
 
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": dist.world,
