@@ -287,6 +287,23 @@ KARAM_API int karam_get_lu_program(const karam_problem *p, int32_t *hdr, int32_t
  * capacitor companions of the chosen method with history v_prev = i_prev = 0. */
 KARAM_API int karam_eval_stamp(karam_problem *p, int32_t precision, const double *v,
                                double *jac, double *f);
+/* karam_eval_stamp for callers that cannot allocate device memory at the time
+ * of the call -- code whose GPU memory belongs to its own pool allocator, or
+ * latency-critical loops where cudaMalloc / cudaFree would synchronise the
+ * device. No counterpart in the reference (its evaluation allocates freely).
+ * d_v ([n_instances][n], node order), d_jac ([n_instances][nnz], CSR order,
+ * without the gmin diagonal) and d_f ([n_instances][n]) are DEVICE pointers the
+ * caller owns; the instance parameters are the problem's (karam_set_instances).
+ * Intermediates live in one fixed 16 MiB device array of the library, shared
+ * by every call on a GPU and held until the process exits: a problem whose
+ * batch capacity needs more is rejected with KARAM_E_INVALID and a message.
+ * The array keeps the last call's contents; each call clears what it needs
+ * cleared. Calls that overlap on the GPU (other threads or streams) race on the
+ * array. The first call on a device looks up the array's address, so make it
+ * before any stream capture. Runs on the problem's stream and returns when the
+ * outputs are written. */
+KARAM_API int karam_eval_stamp_noalloc(karam_problem *p, int32_t precision, const double *d_v,
+                                       double *d_jac, double *d_f);
 /* Device-side accounting of the last solve or evaluation call (CUDA events on
  * the problem's stream; counters kept by the kernels). */
 typedef struct karam_timing {

@@ -74,6 +74,8 @@ def lib():
         "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
                                        P(C.c_double)]),
         "karam_last_timing": (C.c_int, [vp, P(A.KaramTiming)]),
+        "karam_eval_stamp_noalloc": (C.c_int, [vp, C.c_int32, C.c_void_p, C.c_void_p,
+                                               C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -13,6 +13,7 @@
 
 #include "../../include/karam.h"
 #include "device.hpp"
+#include "noalloc.hpp"
 #include "topology.hpp"
 
 using namespace karam;
@@ -935,6 +936,33 @@ int karam_eval_stamp(karam_problem* p, int32_t precision, const double* v, doubl
       if (f)
         for (int k = 0; k < n; ++k) f[(size_t)i * n + T.perm[k]] = F[(size_t)k * ld + i];
     }
+    return KARAM_OK;
+  });
+}
+
+int karam_eval_stamp_noalloc(karam_problem* p, int32_t precision, const double* d_v,
+                             double* d_jac, double* d_f) {
+  if (!p || !d_v || !d_jac || !d_f) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    if (precision != KARAM_PREC_FP64 && precision != KARAM_PREC_MIXED)
+      throw std::runtime_error("unknown precision");
+    const Topology& T = p->topo;
+    const size_t need = noalloc_bytes(T.n, T.nv, T.nnz(), p->ld);
+    if (need > kScratchBytes)
+      throw std::runtime_error("karam_eval_stamp_noalloc: this problem needs " +
+                               std::to_string(need) + " bytes of scratch, the fixed maximum is " +
+                               std::to_string(kScratchBytes) +
+                               " (create the problem with fewer max_instances)");
+    ck(cudaSetDevice(p->ctx->device), "cudaSetDevice");
+    const char* err = "";
+    void* scratch = noalloc_scratch(p->ctx->device, &err);
+    if (!scratch) throw CudaError(std::string("cudaGetSymbolAddress: ") + err);
+    cudaStream_t s = p->ctx->stream;
+    ck(noalloc_eval_stamp(scratch, p->dt, dev_inst(p), precision, d_v, p->t_perm.as<int>(),
+                          p->csr_to_slot.data(), T.nnz(), d_jac, d_f, s),
+       "karam_eval_stamp_noalloc launch");
+    ck(cudaStreamSynchronize(s), "karam_eval_stamp_noalloc sync");
     return KARAM_OK;
   });
 }
