@@ -150,7 +150,11 @@ typedef struct karam_solver_opts {
                             0 keeps the reference stopping rule                  */
   double polish_rel;     /* polishing stops once |dv_i| <= polish_rel*|v_i| + polish_abs */
   double polish_abs;     /*   for every node, or when |dv| stops shrinking        */
-  int32_t ir_steps;      /* FP64 refinement steps per FP32 linear solve (mixed)  */
+  double lu_growth_limit; /* a static-pivot solve whose multipliers exceed this goes
+                            to the rescue path (FP64 static pivots, then dense
+                            partial pivoting); 0 = 1e4 in FP32 / 1e10 in FP64;
+                            < 0 = no growth test (tiny or non-finite pivots and
+                            non-finite solutions still go to the rescue)       */
   int32_t seeded;        /* 1: start from the caller's guess at the final GMIN
                             step; fall back to full GMIN stepping if it has not
                             converged after seed_max_iter iterations              */

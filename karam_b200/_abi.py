@@ -56,7 +56,7 @@ class KaramSolverOpts(C.Structure):
         ("precision", C.c_int32), ("max_nr_iter", C.c_int32), ("gmin_steps", C.c_int32),
         ("reltol", C.c_double), ("vntol", C.c_double), ("kcl_shortcut", C.c_double),
         ("kcl_tol", C.c_double), ("polish_max", C.c_int32), ("polish_rel", C.c_double),
-        ("polish_abs", C.c_double), ("ir_steps", C.c_int32), ("seeded", C.c_int32),
+        ("polish_abs", C.c_double), ("lu_growth_limit", C.c_double), ("seeded", C.c_int32),
         ("seed_max_iter", C.c_int32), ("schedule", C.c_int32), ("max_rounds", C.c_int32),
         ("max_halvings", C.c_int32),
     ]

@@ -84,7 +84,8 @@ struct karam_problem {
   DBuf t_mos_term, t_mos_geo, t_mos_pmos, t_dio_term, t_dio_par, t_res_term, t_res_g, t_cap_term,
       t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
-      t_es_jt, t_es_ft, t_es_fc, t_lu_hdr, t_lu_data, t_lu_rec, t_seed_vs, t_seed_anode, t_perm;
+      t_es_jt, t_es_ft, t_es_fc, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
+      t_perm;
   DevTopo dt{};
   // instance buffers, [item][ld] (instance-interleaved)
   int ld = 0;
@@ -226,6 +227,7 @@ void upload_topology(karam_problem* p) {
   upload(p->t_lu_hdr, hdr);
   upload(p->t_lu_data, T.lu_data);
   upload(p->t_lu_rec, T.lu_rec);
+  upload(p->t_lu_rec2, T.lu_rec2);
   upload(p->t_seed_vs, seed_vs);
   upload(p->t_seed_anode, seed_an);
   upload(p->t_perm, T.perm);
@@ -275,6 +277,7 @@ void upload_topology(karam_problem* p) {
   d.lu_data = p->t_lu_data.as<int>();
   d.lu_small = T.lu_small ? 1 : 0;
   d.lu_rec = T.lu_small ? p->t_lu_rec.as<int4>() : nullptr;
+  d.lu_rec2 = T.lu_small ? p->t_lu_rec2.as<int2>() : nullptr;
   d.slot_rc = p->t_slot_rc.as<int2>();
   d.seed_vs = p->t_seed_vs.as<int>();
   d.seed_anode = p->t_seed_anode.as<int>();
@@ -434,6 +437,8 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
   P.seeded = o->seeded;
   P.seed_max_iter = o->seed_max_iter;
   P.max_halvings = o->max_halvings;
+  P.growth32 = o->lu_growth_limit > 0 ? o->lu_growth_limit : (o->lu_growth_limit < 0 ? 1e300 : 1e4);
+  P.growth64 = o->lu_growth_limit > 0 ? o->lu_growth_limit : (o->lu_growth_limit < 0 ? 1e300 : 1e10);
   if (P.max_halvings < 0 || P.max_halvings > 10) throw std::runtime_error("max_halvings must be in 0..10");
   if (P.max_nr_iter < 1 || P.gmin_steps < 1 || P.polish_max < 0)
     throw std::runtime_error("invalid solver options");
@@ -615,7 +620,7 @@ void karam_default_opts(karam_solver_opts* o) {
   o->polish_max = 0;
   o->polish_rel = 0.0;
   o->polish_abs = 0.0;
-  o->ir_steps = 0;
+  o->lu_growth_limit = 0.0;
   o->seeded = 0;
   o->seed_max_iter = 10;
   o->schedule = 0;

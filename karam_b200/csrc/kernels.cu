@@ -17,7 +17,7 @@ namespace {
 // Value slots + right-hand side of L instances, then the packed pivot records.
 size_t round_smem(const DevTopo& T, int L, size_t es) {
   size_t b = es * ((size_t)T.nv + (size_t)T.n) * (size_t)L;
-  if (T.lu_rec) b = ((b + 15) & ~size_t(15)) + 2 * sizeof(int4) * (size_t)T.n;
+  if (T.lu_rec) b = ((b + 15) & ~size_t(15)) + (2 * sizeof(int4) + sizeof(int2)) * (size_t)T.n;
   return b;
 }
 
@@ -54,7 +54,10 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
     const int grid = (ni + L - 1) / L;
     const long slots = (long)per_sm * std::max(1, num_sms);
     const long waves = (grid + slots - 1) / slots;
-    if (best_waves < 0 || waves < best_waves) {
+    // fewest waves; among equals, a grid that reaches every SM (the streaming
+    // phases spread wider and each SM runs more factor chains side by side)
+    const bool fills = grid >= num_sms, best_fills = best.grid >= num_sms;
+    if (best_waves < 0 || waves < best_waves || (waves == best_waves && fills && !best_fills)) {
       best_waves = waves;
       best.L = L;
       best.grid = grid;
@@ -95,7 +98,7 @@ void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const Rou
 
 size_t rescue_smem_bytes(const DevTopo& T) {
   size_t b = sizeof(double) * ((size_t)T.n + (size_t)std::max(T.nv, T.n)) + sizeof(int) * (size_t)T.n;
-  if (T.lu_rec) b += 16 + 2 * sizeof(int4) * (size_t)T.n;
+  if (T.lu_rec) b += 16 + (2 * sizeof(int4) + sizeof(int2)) * (size_t)T.n;
   return b;
 }
 

@@ -15,6 +15,8 @@
 // dense partial pivoting), launched after every round.
 #ifndef KARAM_NR_DEVICE_CUH
 #define KARAM_NR_DEVICE_CUH
+#include <cstdint>
+
 #include "nr_types.h"
 
 namespace knr {
@@ -436,30 +438,18 @@ __device__ __forceinline__ void limit_one(const DevTopo& T, int d, double* x, co
 // L, U, diagonal and target slots are distinct), so a pivot costs about one
 // shared-memory round trip plus the reciprocal; otherwise (rec == 0) a
 // generic loop walks the program in global memory.
-struct SmallPivot {
-  int d, nl, nu, lr0, lr1, ls0, ls1, us0, us1, t00, t01, t10, t11, uc0, uc1;
-};
-
-// Decodes a packed pivot record (see pack_small_pivots in topology.cpp).
-__device__ __forceinline__ SmallPivot decode_pivot(int4 a, int4 b) {
-  SmallPivot q;
-  const unsigned w0 = (unsigned)a.x;
-  q.d = (int)(w0 & 0xffffffu);
-  q.nl = (int)((w0 >> 24) & 15u);
-  q.nu = (int)(w0 >> 28);
-  q.lr0 = a.y & 0xffff;
-  q.lr1 = (int)((unsigned)a.y >> 16);
-  q.ls0 = a.z & 0xffff;
-  q.ls1 = (int)((unsigned)a.z >> 16);
-  q.us0 = a.w & 0xffff;
-  q.us1 = (int)((unsigned)a.w >> 16);
-  q.t00 = b.x & 0xffff;
-  q.t01 = (int)((unsigned)b.x >> 16);
-  q.t10 = b.y & 0xffff;
-  q.t11 = (int)((unsigned)b.y >> 16);
-  q.uc0 = b.z & 0xffff;
-  q.uc1 = (int)((unsigned)b.z >> 16);
-  return q;
+// Stages the pivot records into shared memory with every slot / row offset
+// multiplied by the lane count L (so the factorisation indexes A and y with
+// them directly): rec[2k], rec[2k+1] per pivot, then rec2[k]. Whole CTA.
+__device__ __forceinline__ void stage_pivots(const DevTopo& T, int4* rec, int L) {
+  int2* rec2 = reinterpret_cast<int2*>(rec + 2 * T.n);
+  for (int k = threadIdx.x; k < T.n; k += blockDim.x) {
+    const int4 a = __ldg(&T.lu_rec[2 * k]), b = __ldg(&T.lu_rec[2 * k + 1]);
+    const int2 c = __ldg(&T.lu_rec2[k]);
+    rec[2 * k] = make_int4(a.x, a.y * L, a.z * L, a.w * L);
+    rec[2 * k + 1] = make_int4(b.x * L, b.y * L, b.z * L, b.w * L);
+    rec2[k] = make_int2(c.x * L, c.y * L);
+  }
 }
 
 // Correctly rounded reciprocal (the value of 1 / x).
@@ -473,58 +463,56 @@ __device__ bool lu_solve(T* __restrict__ A, T* __restrict__ y, int L, const DevT
   bool ok = true;
   T lmax = T(0);
   if (rec) {
-    SmallPivot q = decode_pivot(rec[0], rec[1]);
+    // w00, w01, wy0: what the previous pivot wrote to its two targets and to
+    // its L row's right-hand side; a chain pivot (meta bit 8) takes its L
+    // value, second target and L row's right-hand side from them. L values
+    // are not stored: the forward substitution runs inside the elimination
+    // and the back substitution reads only U, so nothing reads them again.
+    const int2* rec2 = reinterpret_cast<const int2*>(rec + 2 * n);
+    T w00 = T(0), w01 = T(0), wy0 = T(0);
+    int4 ra = rec[0], rb = rec[1];
     for (int k = 0; k < n; ++k) {
       const int kn = k + 1 < n ? k + 1 : k;
-      const SmallPivot nq = decode_pivot(rec[2 * kn], rec[2 * kn + 1]);
-      const int nl = q.nl, nu = q.nu;
-      const T piv = A[q.d * L];
+      const int4 na = rec[2 * kn], nb = rec[2 * kn + 1];
+      const bool chain = (ra.x >> 8) & 1;
+      const int nl = ra.x & 15, nu = (ra.x >> 4) & 15;
+      const T piv = A[ra.y];
       const T yk = y[k * L];
-      const T u0 = nu > 0 ? A[q.us0 * L] : T(0);
-      const T u1 = nu > 1 ? A[q.us1 * L] : T(0);
-      const T a0 = nl > 0 ? A[q.ls0 * L] : T(0);
-      const T a1 = nl > 1 ? A[q.ls1 * L] : T(0);
-      const T y0 = nl > 0 ? y[q.lr0 * L] : T(0);
-      const T y1 = nl > 1 ? y[q.lr1 * L] : T(0);
-      const T b00 = (nl > 0 && nu > 0) ? A[q.t00 * L] : T(0);
-      const T b01 = (nl > 0 && nu > 1) ? A[q.t01 * L] : T(0);
-      const T b10 = (nl > 1 && nu > 0) ? A[q.t10 * L] : T(0);
-      const T b11 = (nl > 1 && nu > 1) ? A[q.t11 * L] : T(0);
+      const T u0 = nu > 0 ? A[rb.x] : T(0), u1 = nu > 1 ? A[rb.y] : T(0);
+      const T b00 = (nl > 0 && nu > 0) ? A[rb.z] : T(0);
+      const T a0 = chain ? w00 : (nl > 0 ? A[ra.z] : T(0));
+      const T y0 = chain ? wy0 : (nl > 0 ? y[ra.w] : T(0));
+      const T b01 = chain ? w01 : ((nl > 0 && nu > 1) ? A[rb.w] : T(0));
       ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
       const T r = recip(piv);
-      A[q.d * L] = r;
+      A[ra.y] = r;
       if (nl > 0) {
         const T l = a0 * r;
         lmax = fmax(lmax, fabs(l));
-        A[q.ls0 * L] = l;
-        y[q.lr0 * L] = y0 - l * yk;
-        if (nu > 0) A[q.t00 * L] = b00 - l * u0;
-        if (nu > 1) A[q.t01 * L] = b01 - l * u1;
+        wy0 = y0 - l * yk;
+        if (nu > 0) w00 = b00 - l * u0;
+        if (nu > 1) w01 = b01 - l * u1;
+        y[ra.w] = wy0;
+        if (nu > 0) A[rb.z] = w00;
+        if (nu > 1) A[rb.w] = w01;
       }
-      if (nl > 1) {
-        const T l = a1 * r;
-        lmax = fmax(lmax, fabs(l));
-        A[q.ls1 * L] = l;
-        y[q.lr1 * L] = y1 - l * yk;
-        if (nu > 0) A[q.t10 * L] = b10 - l * u0;
-        if (nu > 1) A[q.t11 * L] = b11 - l * u1;
-      }
-      q = nq;
+      ra = na;
+      rb = nb;
     }
     bool finite = true;
-    q = decode_pivot(rec[2 * (n - 1)], rec[2 * (n - 1) + 1]);
+    T yprev = T(0);  // the unknown the previous back-substitution step solved
     for (int k = n - 1; k >= 0; --k) {
-      const int kn = k > 0 ? k - 1 : 0;
-      const SmallPivot nq = decode_pivot(rec[2 * kn], rec[2 * kn + 1]);
-      const int nu = q.nu;
-      T s = y[k * L];
-      const T r = A[q.d * L];
-      if (nu > 0) s -= A[q.us0 * L] * y[q.uc0 * L];
-      if (nu > 1) s -= A[q.us1 * L] * y[q.uc1 * L];
-      s *= r;
-      y[k * L] = s;
-      finite = finite && isfinite(s);
-      q = nq;
+      const int4 a = rec[2 * k], b = rec[2 * k + 1];
+      const int2 c = rec2[k];
+      const int nu = (a.x >> 4) & 15;
+      const unsigned fb = ((unsigned)a.x >> 9) & 3u;
+      T sv = y[k * L];
+      if (nu > 0) sv -= A[b.x] * ((fb & 1u) ? yprev : y[c.x]);
+      if (nu > 1) sv -= A[b.y] * ((fb & 2u) ? yprev : y[c.y]);
+      sv *= A[a.y];
+      y[k * L] = sv;
+      yprev = sv;
+      finite = finite && isfinite(sv);
     }
     return ok && finite && !(lmax > growth_limit);
   }
@@ -625,8 +613,9 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
 // (linear stamps, capacitor companions, device terms, in stamp order) and the
 // KCL residual of each of its nodes (terms in node order), and folds max |F|,
 // max |x - v| and the convergence flags of its nodes into the instance's
-// reductions with one atomic each. A hub node (more devices than shared memory
-// holds) walks its terms in chunks of KES_MAX_DEV devices.
+// reductions with one atomic each. Hub items (more devices than shared memory
+// holds: the supply node and its diagonal) walk their devices in chunks of
+// KES_MAX_DEV, a group of them sharing one walk.
 template <typename TJ>
 __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
   __shared__ double s_dev[KES_MAX_DEV * 3 * 32];
@@ -695,13 +684,18 @@ __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
         }
       }
   } else {
-    // hub item: devices in chunks of KES_MAX_DEV in term order; warp 0 sums
-    const int4 it = __ldg(&T.es_item[blk.x]);
+    // hub group: -blk.y items (warp w sums item w) over one walk of the
+    // group's devices in chunks of KES_MAX_DEV; each item's device indices
+    // never decrease along its terms, so every sum keeps its term order
+    const int nh = -blk.y;
+    const bool mine = warp < nh && live;
+    int4 it = make_int4(0, 0, 0, 0);
+    if (warp < nh) it = __ldg(&T.es_item[blk.x + warp]);
     const bool slot = it.x < nv;
     int q = it.y;
     const int qe = it.y + it.z;
     double acc = 0.0;
-    if (slot) {
+    if (mine && slot) {
       acc = __ldg(&T.jlin_dc[it.x]);
       if (tran) {
         const int q1 = __ldg(&T.jcap_off[it.x + 1]);
@@ -718,7 +712,7 @@ __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
         for (int k = warp; k < cn; k += 8)
           eval_device(T, I, __ldg(&T.es_dev[blk.z + c0 + k]), g, s_dev + k * 96 + lane);
       __syncthreads();
-      if (warp == 0 && live) {
+      if (mine) {
         if (slot) {
           for (; q < qe; ++q) {  // every slot term is a device term
             const int c = __ldg(&T.es_jt[q]);
@@ -737,11 +731,11 @@ __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
       }
       __syncthreads();
     }
-    if (warp == 0 && live) {
+    if (mine) {
       if (slot) {
         reinterpret_cast<TJ*>(I.J)[(size_t)it.x * ld + g] = (TJ)acc;
       } else {
-        for (; q < qe; ++q) {
+        for (; q < qe; ++q) {  // linear terms after the last device term
           const int4 tm = __ldg(&T.es_ft[q]);
           const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
           acc = tm.x < 0 ? acc - cur : acc + cur;
@@ -908,8 +902,7 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
     } else {
       for (int s = row; s < nv; s += R) A[s * L + lane] = J[(size_t)s * ld + g];
     }
-    if (rec)
-      for (int k = tid; k < 2 * n; k += blockDim.x) rec[k] = __ldg(&Tp.lu_rec[k]);
+    if (rec) stage_pivots(Tp, rec, L);
     cp_async_wait_all();
   }
 
@@ -952,7 +945,7 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
     // 3. factor + solve: one lane per instance
     if (tid < L && (s_act[tid] & ACT_SOLVE)) {
       const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
-      const T growth = sizeof(T) == 8 ? (T)1e10 : (T)1e4;
+      const T growth = sizeof(T) == 8 ? (T)P.growth64 : (T)fmin(P.growth32, 3.0e38);
       s_sing[tid] = lu_solve<T>(A + tid, Y + tid, L, Tp, rec, tiny, growth) ? 0 : 1;
     }
     __syncthreads();
@@ -1049,7 +1042,7 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
   const int total = *I.rescue_count;
   if (blockIdx.x >= total) return;
   if (rec) {
-    for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) rec[k] = __ldg(&Tp.lu_rec[k]);
+    stage_pivots(Tp, rec, 1);
     __syncthreads();
   }
   double* A = I.rescue_ws + (size_t)blockIdx.x * n * n;
@@ -1072,7 +1065,7 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
       __syncthreads();
       for (int i = tid; i < n; i += blockDim.x) As[Tp.lu_hdr[i].w] += gmin;
       __syncthreads();
-      if (tid == 0) s_ok = lu_solve<double>(As, b, 1, Tp, rec, 1e-25, 1e10) ? 1 : 0;
+      if (tid == 0) s_ok = lu_solve<double>(As, b, 1, Tp, rec, 1e-25, P.growth64) ? 1 : 0;
     }
     __syncthreads();
     if (!s_ok) {

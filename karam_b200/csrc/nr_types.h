@@ -26,8 +26,12 @@
 
 // Evaluation + stamping blocks: devices held in shared memory at a time, and
 // items per block.
+#ifndef KES_MAX_DEV
 #define KES_MAX_DEV 48
+#endif
+#ifndef KES_MAX_ITEMS
 #define KES_MAX_ITEMS 64
+#endif
 
 enum { MODE_DC = 0, MODE_TRAN = 1, MODE_DONE = 2 };
 enum { SUB_NR = 0, SUB_POLISH = 1 };
@@ -113,9 +117,10 @@ struct DevTopo {
   // Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots)
   const int4* lu_hdr;
   const int* lu_data;
-  int lu_small;             // 1: every pivot has nL <= 2 and nU <= 2
-  const int4* lu_rec;       // packed pivot records when lu_small (2 int4 per pivot, see
-                            // pack_small_pivots in topology.cpp), else 0
+  int lu_small;             // 1: every pivot has nL <= 1 and nU <= 2
+  const int4* lu_rec;       // pivot records when lu_small (2 int4 per pivot: meta, diagonal,
+                            // Lslot, Lrow | Uslot0, Uslot1, T0, T1; see topology.cpp), else 0
+  const int2* lu_rec2;      // back-substitution columns (Ucol0, Ucol1) per pivot
   const int2* slot_rc;      // (row, col) of every value slot (permuted)
   const int* seed_vs;       // permuted positive node per source (-1 = ground)
   const int* seed_anode;    // permuted anode per netlist diode (-1 = ground)
@@ -168,6 +173,7 @@ struct JobParams {
   int method;
   int seeded, seed_max_iter;
   int max_halvings;  // transient restarts with a halved step (reference: 3)
+  double growth32, growth64;  // static-pivot multiplier limits (FP32 / FP64 solves)
 };
 
 #endif

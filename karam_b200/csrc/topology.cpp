@@ -423,30 +423,77 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   flatten(jt, T.jt_off, T.jt_code);
   flatten(jc, T.jcap_off, T.jcap_code);
 
-  // Packed pivot records for programs whose pivots all have nL, nU <= 2 (2 int4
-  // per pivot): w0 = diagonal slot | nL << 24 | nU << 28; then 16-bit pairs
-  // (Lrow0, Lrow1), (Lslot0, Lslot1), (Uslot0, Uslot1), (T00, T01), (T10, T11),
-  // (Ucol0, Ucol1), 0.
-  T.lu_small = T.n < 65536 && T.nv < 65536;
+  // Pivot records for programs whose pivots all have nL <= 1 and nU <= 2
+  // (chain-like circuits), 8 ints per pivot:
+  //   meta = nL | nU << 4 | chain << 8 | back-forwarding << 9
+  //   then diagonal slot, Lslot0, Lrow0, Uslot0, Uslot1, T00, T01
+  // and 2 ints per pivot for the back substitution: Ucol0, Ucol1 (lu_rec2).
+  // "chain" marks a pivot whose L value and second target are the previous
+  // pivot's targets and whose L row's right-hand side the previous pivot wrote
+  // (so the device keeps them in registers), with no other read touching what
+  // the previous pivot wrote (so its loads may be issued early).
+  // Back-forwarding bit b: Ucol b is the unknown the previous back-substitution
+  // step solved.
+  T.lu_small = T.n < (1 << 24) && T.nv < (1 << 24);
   for (int k = 0; k < n && T.lu_small; ++k)
-    if (T.lu_hdr[4 * k + 1] > 2 || T.lu_hdr[4 * k + 2] > 2) T.lu_small = false;
+    if (T.lu_hdr[4 * k + 1] > 1 || T.lu_hdr[4 * k + 2] > 2) T.lu_small = false;
   T.lu_rec.clear();
+  T.lu_rec2.clear();
   if (T.lu_small) {
     T.lu_rec.assign(8 * (size_t)n, 0);
-    auto pk = [](int lo, int hi) { return (int)((uint32_t)lo | ((uint32_t)hi << 16)); };
+    T.lu_rec2.assign(2 * (size_t)n, 0);
+    struct Piv { int d, nl, nu, lr, ls, us[2], uc[2], t[2]; };
+    std::vector<Piv> pv(n);
     for (int k = 0; k < n; ++k) {
       const int off = T.lu_hdr[4 * k], nl = T.lu_hdr[4 * k + 1], nu = T.lu_hdr[4 * k + 2];
       const int* d = &T.lu_data[off];
-      auto at = [&](int cnt, int base, int i) { return i < cnt ? d[base + i] : 0; };
+      Piv& q = pv[k];
+      q = Piv{};
+      q.d = T.lu_hdr[4 * k + 3];
+      q.nl = nl;
+      q.nu = nu;
+      if (nl > 0) {
+        q.lr = d[0];
+        q.ls = d[1];
+      }
+      for (int b = 0; b < nu; ++b) {
+        q.uc[b] = d[2 * nl + b];
+        q.us[b] = d[2 * nl + nu + b];
+        if (nl > 0) q.t[b] = d[2 * nl + 2 * nu + b];
+      }
+    }
+    for (int k = 0; k < n; ++k) {
+      const Piv& q = pv[k];
+      bool chain = false;
+      if (k > 0 && q.nl == 1 && q.nu == 2) {
+        const Piv& p = pv[k - 1];
+        auto written = [&](int slot) {
+          if (slot == p.d) return true;
+          if (p.nl > 0 && slot == p.ls) return true;
+          for (int b = 0; b < p.nu && p.nl > 0; ++b)
+            if (slot == p.t[b]) return true;
+          return false;
+        };
+        chain = p.nl == 1 && p.nu == 2 && q.ls == p.t[0] && q.t[1] == p.t[1] && q.lr == p.lr &&
+                !written(q.d) && !written(q.us[0]) && !written(q.us[1]) && !written(q.t[0]) &&
+                k != p.lr;
+      }
+      unsigned fb = 0;
+      if (k + 1 < n) {
+        if (q.nu > 0 && q.uc[0] == k + 1) fb |= 1u;
+        if (q.nu > 1 && q.uc[1] == k + 1) fb |= 2u;
+      }
       int* w = &T.lu_rec[8 * (size_t)k];
-      w[0] = T.lu_hdr[4 * k + 3] | (nl << 24) | (nu << 28);
-      w[1] = pk(at(nl, 0, 0), at(nl, 0, 1));
-      w[2] = pk(at(nl, nl, 0), at(nl, nl, 1));
-      w[3] = pk(at(nu, 2 * nl + nu, 0), at(nu, 2 * nl + nu, 1));
-      const int tb = 2 * nl + 2 * nu;
-      w[4] = pk(nl > 0 && nu > 0 ? d[tb] : 0, nl > 0 && nu > 1 ? d[tb + 1] : 0);
-      w[5] = pk(nl > 1 && nu > 0 ? d[tb + nu] : 0, nl > 1 && nu > 1 ? d[tb + nu + 1] : 0);
-      w[6] = pk(at(nu, 2 * nl, 0), at(nu, 2 * nl, 1));
+      w[0] = (int)((unsigned)q.nl | (unsigned)q.nu << 4 | (chain ? 1u : 0u) << 8 | fb << 9);
+      w[1] = q.d;
+      w[2] = q.ls;
+      w[3] = q.lr;
+      w[4] = q.us[0];
+      w[5] = q.us[1];
+      w[6] = q.t[0];
+      w[7] = q.t[1];
+      T.lu_rec2[2 * (size_t)k] = q.uc[0];
+      T.lu_rec2[2 * (size_t)k + 1] = q.uc[1];
     }
   }
 
@@ -685,6 +732,7 @@ void es_blocks(Topology& T) {
   }
   std::vector<int> cur_items, cur_devs, devs;
   std::unordered_map<int, int> local;
+  std::vector<int> hubs;  // items with more devices than one block holds
   auto emit = [&](const std::vector<int>& items, const std::vector<int>& dlist, bool) {
     if (items.empty()) return;
     std::unordered_map<int, int> lid;
@@ -730,44 +778,7 @@ void es_blocks(Topology& T) {
     for (int d : devs)
       if (std::find(own.begin(), own.end(), d) == own.end()) own.push_back(d);
     if ((int)own.size() > kEsMaxDev) {
-      // hub item (node or slot): a block of its own that walks its terms in
-      // chunks of kEsMaxDev device terms, one device per term occurrence, so
-      // the local index grows with the term order
-      emit(cur_items, cur_devs, false);
-      cur_items.clear();
-      cur_devs.clear();
-      local.clear();
-      T.es_block.push_back((int)T.es_item.size() / 4);
-      T.es_block.push_back(-1);
-      T.es_block.push_back((int)T.es_dev.size());
-      T.es_block.push_back((int)devs.size());
-      T.es_item.push_back(it);
-      int occ = 0;
-      if (it < nv) {  // a hub slot, e.g. the supply diagonal
-        T.es_item.push_back((int)T.es_jt.size());
-        T.es_item.push_back(T.jt_off[it + 1] - T.jt_off[it]);
-        T.es_item.push_back(0);
-        for (int q = T.jt_off[it]; q < T.jt_off[it + 1]; ++q) {
-          const int c = T.jt_code[q];
-          T.es_dev.push_back(slot_dev(c));
-          T.es_jt.push_back((c & int32_t(0xFF000000u)) | occ++);
-        }
-        continue;
-      }
-      const int i = it - nv;
-      T.es_item.push_back((int)T.es_ft.size() / 4);
-      T.es_item.push_back(T.ft_off[i + 1] - T.ft_off[i]);
-      T.es_item.push_back(0);
-      for (int q = T.ft_off[i]; q < T.ft_off[i + 1]; ++q) {
-        const int c = T.ft_code[q];
-        const int d = node_dev(c);
-        if (d >= 0) T.es_dev.push_back(d);
-        T.es_ft.push_back(d >= 0 ? ((c & int32_t(0xFF000000u)) | occ++) : c);
-        T.es_ft.push_back(T.ft_a[q]);
-        T.es_ft.push_back(T.ft_b[q]);
-        T.es_ft.push_back(0);
-        T.es_fc.push_back(T.ft_coef[q]);
-      }
+      hubs.push_back(it);  // emitted after the normal blocks, grouped
       continue;
     }
     if ((int)(cur_devs.size() + fresh.size()) > kEsMaxDev || (int)cur_items.size() >= kEsMaxItems) {
@@ -784,6 +795,99 @@ void es_blocks(Topology& T) {
     cur_items.push_back(it);
   }
   emit(cur_items, cur_devs, false);
+
+  // Hub items (the supply node and its diagonal slot): groups of up to 8
+  // share one walk over the union of their devices in chunks of kEsMaxDev
+  // (one warp sums each item). The union is in first-occurrence order; a
+  // group is kept only if every item's device indices never decrease along
+  // its terms (so each item's sum keeps its term order), otherwise each hub
+  // walks its own term occurrences.
+  auto terms_of = [&](int it, std::vector<int>& out) {  // device per term, -1 = linear
+    out.clear();
+    if (it < nv) {
+      for (int q = T.jt_off[it]; q < T.jt_off[it + 1]; ++q) out.push_back(slot_dev(T.jt_code[q]));
+    } else {
+      const int i = it - nv;
+      for (int q = T.ft_off[i]; q < T.ft_off[i + 1]; ++q) out.push_back(node_dev(T.ft_code[q]));
+    }
+  };
+  auto emit_group = [&](const std::vector<int>& items, const std::vector<int>& dlist,
+                        const std::vector<std::vector<int>>& lidx) {
+    T.es_block.push_back((int)T.es_item.size() / 4);
+    T.es_block.push_back(-(int)items.size());
+    T.es_block.push_back((int)T.es_dev.size());
+    T.es_block.push_back((int)dlist.size());
+    T.es_dev.insert(T.es_dev.end(), dlist.begin(), dlist.end());
+    for (size_t m = 0; m < items.size(); ++m) {
+      const int it = items[m];
+      T.es_item.push_back(it);
+      const std::vector<int>& li = lidx[m];
+      if (it < nv) {
+        T.es_item.push_back((int)T.es_jt.size());
+        T.es_item.push_back(T.jt_off[it + 1] - T.jt_off[it]);
+        T.es_item.push_back(0);
+        for (int q = T.jt_off[it], t = 0; q < T.jt_off[it + 1]; ++q, ++t)
+          T.es_jt.push_back((T.jt_code[q] & int32_t(0xFF000000u)) | li[t]);
+      } else {
+        const int i = it - nv;
+        T.es_item.push_back((int)T.es_ft.size() / 4);
+        T.es_item.push_back(T.ft_off[i + 1] - T.ft_off[i]);
+        T.es_item.push_back(0);
+        for (int q = T.ft_off[i], t = 0; q < T.ft_off[i + 1]; ++q, ++t) {
+          const int c = T.ft_code[q];
+          T.es_ft.push_back(li[t] >= 0 ? ((c & int32_t(0xFF000000u)) | li[t]) : c);
+          T.es_ft.push_back(T.ft_a[q]);
+          T.es_ft.push_back(T.ft_b[q]);
+          T.es_ft.push_back(0);
+          T.es_fc.push_back(T.ft_coef[q]);
+        }
+      }
+    }
+  };
+  std::vector<int> tdev;
+  for (size_t h0 = 0; h0 < hubs.size(); h0 += 8) {
+    std::vector<int> items(hubs.begin() + h0, hubs.begin() + std::min(hubs.size(), h0 + 8));
+    std::vector<int> dlist;
+    std::unordered_map<int, int> uid;
+    std::vector<std::vector<int>> lidx(items.size());
+    bool monotone = true;
+    for (size_t m = 0; m < items.size(); ++m) {
+      terms_of(items[m], tdev);
+      int last_chunk = 0;
+      for (int d : tdev) {
+        if (d < 0) {
+          lidx[m].push_back(-1);
+          continue;
+        }
+        auto f = uid.find(d);
+        int id;
+        if (f == uid.end()) {
+          id = (int)dlist.size();
+          uid[d] = id;
+          dlist.push_back(d);
+        } else {
+          id = f->second;
+        }
+        lidx[m].push_back(id);
+        if (id / kEsMaxDev < last_chunk) monotone = false;
+        last_chunk = std::max(last_chunk, id / kEsMaxDev);
+      }
+    }
+    if (monotone) {
+      emit_group(items, dlist, lidx);
+      continue;
+    }
+    for (int it : items) {  // each hub walks its own term occurrences
+      terms_of(it, tdev);
+      std::vector<int> occ;
+      std::vector<std::vector<int>> li(1);
+      for (int d : tdev) {
+        li[0].push_back(d >= 0 ? (int)occ.size() : -1);
+        if (d >= 0) occ.push_back(d);
+      }
+      emit_group({it}, occ, li);
+    }
+  }
 }
 
 }  // namespace

@@ -86,8 +86,9 @@ struct Topology {
   //      Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots, row-major) ----
   std::vector<int> lu_hdr;   // 4 ints per pivot
   std::vector<int> lu_data;
-  bool lu_small = false;     // every pivot has nL <= 2 and nU <= 2 (and n, nv < 65536)
-  std::vector<int> lu_rec;   // packed pivot records (8 ints per pivot) when lu_small
+  bool lu_small = false;     // every pivot has nL <= 1 and nU <= 2
+  std::vector<int> lu_rec;   // pivot records (8 ints per pivot) when lu_small
+  std::vector<int> lu_rec2;  // back-substitution columns (2 ints per pivot) when lu_small
   int lu_ops = 0;
   int max_d = 0;
 
