@@ -480,20 +480,33 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_l
   ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
   // External event records become event-record nodes of the graph (a plain
   // record inside capture would only order work within the capture).
+  // a launch that fails inside the capture is reported by name
+  const char* failed = nullptr;
+  cudaError_t launch_err = cudaSuccess;
+  auto check = [&](const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess && launch_err == cudaSuccess) {
+      launch_err = e;
+      failed = what;
+    }
+  };
   for (int r = 0; r < kRounds; ++r) {
     if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
     if (I.rescue_count) cudaMemsetAsync(I.rescue_count, 0, sizeof(int), s);
     cudaEventRecordWithFlags(ev[4 * r], s, cudaEventRecordExternal);
     launch_eval_stamp(p->dt, I, P, L, prec, s);
+    check("k_es launch");
     cudaEventRecordWithFlags(ev[4 * r + 1], s, cudaEventRecordExternal);
     launch_lu(p->dt, I, P, L, prec, active, s);
+    check("k_lu launch");
     cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
     if (I.rescue_list) launch_rescue(p->dt, I, P, I.rescue_slots, s);
+    check("k_rescue launch");
     cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
   }
-  const cudaError_t launch_err = cudaGetLastError();
-  ck(cudaStreamEndCapture(s, &graph), "end capture");
-  ck(launch_err, "kernel launch in capture");
+  const cudaError_t end_err = cudaStreamEndCapture(s, &graph);
+  ck(launch_err, failed ? failed : "kernel launch in capture");
+  ck(end_err, "end capture");
   struct GraphGuard {
     cudaGraph_t& g;
     cudaGraphExec_t& e;

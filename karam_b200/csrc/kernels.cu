@@ -67,6 +67,9 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
   }
   if (best.L > 0)
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best.smem);
+  const int rsm = (int)rescue_smem_bytes(T);
+  cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+  cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
   return best;
 }
 
