@@ -84,7 +84,7 @@ struct karam_problem {
   DBuf t_mos_term, t_mos_geo, t_mos_pmos, t_dio_term, t_dio_par, t_res_term, t_res_g, t_cap_term,
       t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
-      t_es_jt, t_es_ft, t_es_fc, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
+      t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
       t_perm;
   DevTopo dt{};
   // instance buffers, [item][ld] (instance-interleaved)
@@ -224,6 +224,7 @@ void upload_topology(karam_problem* p) {
   upload(p->t_es_dev, T.es_dev);
   upload(p->t_es_jt, T.es_jt);
   upload(p->t_es_fc, T.es_fc);
+  upload(p->t_es_hub, T.es_hub);
   upload(p->t_lu_hdr, hdr);
   upload(p->t_lu_data, T.lu_data);
   upload(p->t_lu_rec, T.lu_rec);
@@ -273,6 +274,7 @@ void upload_topology(karam_problem* p) {
   d.es_jt = p->t_es_jt.as<int>();
   d.es_ft = p->t_es_ft.as<int4>();
   d.es_fc = p->t_es_fc.as<double>();
+  d.es_hub = p->t_es_hub.as<int>();
   d.lu_hdr = p->t_lu_hdr.as<int4>();
   d.lu_data = p->t_lu_data.as<int>();
   d.lu_small = T.lu_small ? 1 : 0;

@@ -158,41 +158,90 @@ __device__ __forceinline__ void diode_eval(double vdd, double4 par, double& id, 
   gd = fmax(1e-12, gbase);
 }
 
-// Device d (MOSFETs first, then diodes) of instance g at x into out[0..2]
-// (stride 32 doubles): MOSFET gm, gds, ids; diode g, i.
-__device__ __forceinline__ void eval_device(const DevTopo& T, const DevInst& I, int d, int g,
-                                            double* out) {
+// Inputs of one device evaluation: terminal voltages and parameters
+// (MOSFET: vd, vg, vs, KP, VTO, W/L, lambda, sign; diode: v_a - v_c in va,
+// Is, N, Vt in p0..p2).
+struct DevIn {
+  bool mos;
+  double va, vb, vc, p0, p1, p2, p3, sign;
+};
+
+// Loads the inputs of device d (MOSFETs first, then diodes) for instance g.
+// Nothing here depends on an earlier evaluation, so the loads of several
+// devices can be in flight together.
+__device__ __forceinline__ DevIn load_device(const DevTopo& T, const DevInst& I, int d, int g) {
   const size_t ld = I.ld;
   const int nm = T.n_mos;
-  const double* x = I.x;
-  if (d < nm) {
+  const double* __restrict__ x = I.x;
+  DevIn in;
+  in.mos = d < nm;
+  if (in.mos) {
     const int4 tm = __ldg(&T.mos_term[d]);
     const double2 geo = __ldg(&T.mos_geo[d]);
-    const double sign = __ldg(&T.mos_pmos[d]) ? -1.0 : 1.0;
-    double kpm, vthm;
+    in.sign = __ldg(&T.mos_pmos[d]) ? -1.0 : 1.0;
     if (I.kp) {
-      kpm = (double)I.kp[d * ld + g];
-      vthm = (double)I.vth[d * ld + g];
+      in.p0 = (double)__ldg(&I.kp[d * ld + g]);
+      in.p1 = (double)__ldg(&I.vth[d * ld + g]);
     } else {
       const double2 card = __ldg(&T.mos_card[d]);
-      kpm = card.x;
-      vthm = card.y;
+      in.p0 = card.x;
+      in.p1 = card.y;
     }
-    double ids, gm, gds;
-    mosfet_eval(tm.x >= 0 ? x[tm.x * ld + g] : 0.0, tm.y >= 0 ? x[tm.y * ld + g] : 0.0,
-                tm.z >= 0 ? x[tm.z * ld + g] : 0.0, sign, kpm, vthm, geo.x, geo.y, ids, gm, gds);
-    out[0] = gm;
-    out[32] = gds;
-    out[64] = ids;
+    in.p2 = geo.x;
+    in.p3 = geo.y;
+    in.va = tm.x >= 0 ? __ldg(&x[tm.x * ld + g]) : 0.0;
+    in.vb = tm.y >= 0 ? __ldg(&x[tm.y * ld + g]) : 0.0;
+    in.vc = tm.z >= 0 ? __ldg(&x[tm.z * ld + g]) : 0.0;
   } else {
     const int k = d - nm;
     const int2 tt = __ldg(&T.dio_term[k]);
     const double4 par = T.dio_par[k];
+    in.p0 = par.x;
+    in.p1 = par.y;
+    in.p2 = par.z;
+    in.p3 = par.w;
+    in.sign = 0.0;
+    in.va = (tt.x >= 0 ? __ldg(&x[tt.x * ld + g]) : 0.0) - (tt.y >= 0 ? __ldg(&x[tt.y * ld + g]) : 0.0);
+    in.vb = in.vc = 0.0;
+  }
+  return in;
+}
+
+// Evaluates loaded inputs into out[0..2] (stride 32 doubles): MOSFET gm,
+// gds, ids; diode g, i.
+__device__ __forceinline__ void eval_loaded(const DevIn& in, double* out) {
+  if (in.mos) {
+    double ids, gm, gds;
+    mosfet_eval(in.va, in.vb, in.vc, in.sign, in.p0, in.p1, in.p2, in.p3, ids, gm, gds);
+    out[0] = gm;
+    out[32] = gds;
+    out[64] = ids;
+  } else {
     double id, gd;
-    diode_eval((tt.x >= 0 ? x[tt.x * ld + g] : 0.0) - (tt.y >= 0 ? x[tt.y * ld + g] : 0.0), par,
-               id, gd);
+    diode_eval(in.va, make_double4(in.p0, in.p1, in.p2, in.p3), id, gd);
     out[0] = gd;
     out[32] = id;
+  }
+}
+
+__device__ __forceinline__ void eval_device(const DevTopo& T, const DevInst& I, int d, int g,
+                                            double* out) {
+  eval_loaded(load_device(T, I, d, g), out);
+}
+
+// Devices k0 and k0 + 8 of a block's device list for instance g (k < n): both
+// devices' loads are issued before either computes.
+__device__ __forceinline__ void eval_device_pair(const DevTopo& T, const DevInst& I,
+                                                 const int* devs, int k0, int n, int g,
+                                                 double* s_dev, int lane) {
+  const int k1 = k0 + 8;
+  const DevIn a = load_device(T, I, __ldg(&devs[k0]), g);
+  if (k1 < n) {
+    const DevIn b = load_device(T, I, __ldg(&devs[k1]), g);
+    eval_loaded(a, s_dev + k0 * 96 + lane);
+    eval_loaded(b, s_dev + k1 * 96 + lane);
+  } else {
+    eval_loaded(a, s_dev + k0 * 96 + lane);
   }
 }
 
@@ -595,14 +644,14 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
   const int idx = code_idx(tm.x), kind = code_kind(tm.x);
   if (kind >= 4) return sd[(idx - dev_base) * 96 + (kind == 4 ? 32 : 64)];  // diode i / MOSFET ids
   if (kind == 2) return coef;                                                // current source
-  const double va = tm.y >= 0 ? I.x[tm.y * ld + g] : 0.0;
-  const double vb = tm.z >= 0 ? I.x[tm.z * ld + g] : 0.0;
+  const double va = tm.y >= 0 ? __ldg(&I.x[tm.y * ld + g]) : 0.0;
+  const double vb = tm.z >= 0 ? __ldg(&I.x[tm.z * ld + g]) : 0.0;
   if (kind == 0) return coef * (va - vb);                                    // resistor
   if (kind == 1) return 1.0e3 * ((va - vb) - source_value(T, I, g, idx, tran, t));  // Norton V source
   if (!tran) return 0.0;                                                     // capacitor companion
   const size_t ci = (size_t)idx * ld + g;
-  double cur = (coef / heff) * ((va - vb) - I.cap_vp[ci]);
-  if (P.method == KTRAN_TRAP) cur -= I.cap_ip[ci];
+  double cur = (coef / heff) * ((va - vb) - __ldg(&I.cap_vp[ci]));
+  if (P.method == KTRAN_TRAP) cur -= __ldg(&I.cap_ip[ci]);
   return cur;
 }
 
@@ -615,7 +664,7 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
 // max |x - v| and the convergence flags of its nodes into the instance's
 // reductions with one atomic each. Hub items (more devices than shared memory
 // holds: the supply node and its diagonal) walk their devices in chunks of
-// KES_MAX_DEV, a group of them sharing one walk.
+// KES_MAX_DEV, a group of them sharing one walk and all warps sharing the sums.
 template <typename TJ>
 __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
   __shared__ double s_dev[KES_MAX_DEV * 3 * 32];
@@ -649,10 +698,11 @@ __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
   };
   if (blk.y > 0) {
     if (live)
-      for (int k = warp; k < blk.w; k += 8)
-        eval_device(T, I, __ldg(&T.es_dev[blk.z + k]), g, s_dev + k * 96 + lane);
+      for (int k = warp; k < blk.w; k += 16)
+        eval_device_pair(T, I, T.es_dev + blk.z, k, blk.w, g, s_dev, lane);
     __syncthreads();
     if (live)
+#pragma unroll 2
       for (int k = warp; k < blk.y; k += 8) {
         const int4 it = __ldg(&T.es_item[blk.x + k]);
         if (it.x < nv) {
@@ -675,73 +725,89 @@ __global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
           reinterpret_cast<TJ*>(I.J)[(size_t)s * ld + g] = (TJ)acc;
         } else {
           double acc = 0.0;
-          for (int q = it.y; q < it.y + it.z; ++q) {
-            const int4 tm = __ldg(&T.es_ft[q]);
-            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
-            acc = tm.x < 0 ? acc - cur : acc + cur;
+          int q = it.y;
+          const int qe = it.y + it.z;
+          for (; q + 1 < qe; q += 2) {  // two terms' loads in flight, sum in order
+            const int4 t0 = __ldg(&T.es_ft[q]), t1 = __ldg(&T.es_ft[q + 1]);
+            const double c0 = node_term(T, I, P, t0, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
+            const double c1 = node_term(T, I, P, t1, __ldg(&T.es_fc[q + 1]), g, tran, t, heff, sd, 0);
+            acc = t0.x < 0 ? acc - c0 : acc + c0;
+            acc = t1.x < 0 ? acc - c1 : acc + c1;
+          }
+          if (q < qe) {
+            const int4 t0 = __ldg(&T.es_ft[q]);
+            const double c0 = node_term(T, I, P, t0, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
+            acc = t0.x < 0 ? acc - c0 : acc + c0;
           }
           node_done(it.x - nv, acc);
         }
       }
   } else {
-    // hub group: -blk.y items (warp w sums item w) over one walk of the
-    // group's devices in chunks of KES_MAX_DEV; each item's device indices
-    // never decrease along its terms, so every sum keeps its term order
+    // hub group: -blk.y items over one walk of the group's devices in chunks
+    // of KES_MAX_DEV; within a chunk the eight warps sum consecutive slices of
+    // each item's terms, and the per-warp partials are added in warp order at
+    // the end (a fixed order, so results do not vary from run to run)
     const int nh = -blk.y;
-    const bool mine = warp < nh && live;
-    int4 it = make_int4(0, 0, 0, 0);
-    if (warp < nh) it = __ldg(&T.es_item[blk.x + warp]);
-    const bool slot = it.x < nv;
-    int q = it.y;
-    const int qe = it.y + it.z;
-    double acc = 0.0;
-    if (mine && slot) {
-      acc = __ldg(&T.jlin_dc[it.x]);
-      if (tran) {
-        const int q1 = __ldg(&T.jcap_off[it.x + 1]);
-        for (int c = __ldg(&T.jcap_off[it.x]); c < q1; ++c) {
-          const int cc = __ldg(&T.jcap_code[c]);
-          const double gq = (2.0 * __ldg(&T.cap_c[code_idx(cc)])) / heff;
-          acc = cc < 0 ? acc - gq : acc + gq;
-        }
-      }
-    }
-    for (int c0 = 0; c0 < blk.w; c0 += KES_MAX_DEV) {
+    const int nch = (blk.w + KES_MAX_DEV - 1) / KES_MAX_DEV;
+    double acc[KES_MAX_HUBS];
+#pragma unroll
+    for (int m = 0; m < KES_MAX_HUBS; ++m) acc[m] = 0.0;
+    for (int c = 0; c < nch; ++c) {
+      const int c0 = c * KES_MAX_DEV;
       const int cn = min(KES_MAX_DEV, blk.w - c0);
       if (live)
-        for (int k = warp; k < cn; k += 8)
-          eval_device(T, I, __ldg(&T.es_dev[blk.z + c0 + k]), g, s_dev + k * 96 + lane);
+        for (int k = warp; k < cn; k += 16)
+          eval_device_pair(T, I, T.es_dev + blk.z + c0, k, cn, g, s_dev, lane);
       __syncthreads();
-      if (mine) {
-        if (slot) {
-          for (; q < qe; ++q) {  // every slot term is a device term
-            const int c = __ldg(&T.es_jt[q]);
-            if (code_idx(c) >= c0 + cn) break;
-            const double val = sd[(code_idx(c) - c0) * 96 + (code_kind(c) == 0 ? 32 : 0)];
-            acc = c < 0 ? acc - val : acc + val;
-          }
-        } else {
-          for (; q < qe; ++q) {
-            const int4 tm = __ldg(&T.es_ft[q]);
-            if (code_kind(tm.x) >= 4 && code_idx(tm.x) >= c0 + cn) break;
-            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, c0);
-            acc = tm.x < 0 ? acc - cur : acc + cur;
+      if (live)
+#pragma unroll
+        for (int m = 0; m < KES_MAX_HUBS; ++m) {
+          if (m >= nh) break;
+          const int4 it = __ldg(&T.es_item[blk.x + m]);
+          const int lo = __ldg(&T.es_hub[it.w + c]), hi = __ldg(&T.es_hub[it.w + c + 1]);
+          const int q0 = lo + (int)(((long long)(hi - lo) * warp) / 8);
+          const int q1 = lo + (int)(((long long)(hi - lo) * (warp + 1)) / 8);
+          if (it.x < nv) {
+            for (int q = it.y + q0; q < it.y + q1; ++q) {  // every slot term is a device term
+              const int cc = __ldg(&T.es_jt[q]);
+              const double val = sd[(code_idx(cc) - c0) * 96 + (code_kind(cc) == 0 ? 32 : 0)];
+              acc[m] = cc < 0 ? acc[m] - val : acc[m] + val;
+            }
+          } else {
+            for (int q = it.y + q0; q < it.y + q1; ++q) {
+              const int4 tm = __ldg(&T.es_ft[q]);
+              const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, c0);
+              acc[m] = tm.x < 0 ? acc[m] - cur : acc[m] + cur;
+            }
           }
         }
-      }
       __syncthreads();
     }
-    if (mine) {
-      if (slot) {
-        reinterpret_cast<TJ*>(I.J)[(size_t)it.x * ld + g] = (TJ)acc;
-      } else {
-        for (; q < qe; ++q) {  // linear terms after the last device term
-          const int4 tm = __ldg(&T.es_ft[q]);
-          const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
-          acc = tm.x < 0 ? acc - cur : acc + cur;
+    // partials through shared memory (the device values are no longer needed)
+    double* part = s_dev;  // [m][warp][32]
+#pragma unroll
+    for (int m = 0; m < KES_MAX_HUBS; ++m)
+      if (m < nh) part[(m * 8 + warp) * 32 + lane] = acc[m];
+    __syncthreads();
+    if (warp < nh && live) {
+      const int4 it = __ldg(&T.es_item[blk.x + warp]);
+      double sum = 0.0;
+      if (it.x < nv) {
+        sum = __ldg(&T.jlin_dc[it.x]);
+        if (tran) {
+          const int q1 = __ldg(&T.jcap_off[it.x + 1]);
+          for (int c = __ldg(&T.jcap_off[it.x]); c < q1; ++c) {
+            const int cc = __ldg(&T.jcap_code[c]);
+            const double gq = (2.0 * __ldg(&T.cap_c[code_idx(cc)])) / heff;
+            sum = cc < 0 ? sum - gq : sum + gq;
+          }
         }
-        node_done(it.x - nv, acc);
       }
+      for (int w = 0; w < 8; ++w) sum += part[(warp * 8 + w) * 32 + lane];
+      if (it.x < nv)
+        reinterpret_cast<TJ*>(I.J)[(size_t)it.x * ld + g] = (TJ)sum;
+      else
+        node_done(it.x - nv, sum);
     }
   }
   // non-negative doubles order like their bit patterns; NaN sorts above +inf

@@ -32,6 +32,8 @@
 #ifndef KES_MAX_ITEMS
 #define KES_MAX_ITEMS 64
 #endif
+// Hub items (more devices than one block holds) sharing one device walk.
+#define KES_MAX_HUBS 4
 
 enum { MODE_DC = 0, MODE_TRAN = 1, MODE_DONE = 2 };
 enum { SUB_NR = 0, SUB_POLISH = 1 };
@@ -100,7 +102,8 @@ struct DevTopo {
   // Evaluation + stamping blocks (see es_blocks in topology.cpp):
   //   es_block[b] = {item offset, items (-1: hub node walked in device chunks),
   //                  device offset, devices}
-  //   es_item[k]  = {item (slot s < nv, node nv + i), term offset, terms, 0}
+  //   es_item[k]  = {item (slot s < nv, node nv + i), term offset, terms,
+  //                  hub items: offset of the item's chunk bounds in es_hub}
   //   es_dev      = global device ids (MOSFETs, then n_mos + diode index)
   //   es_jt       = slot device terms: sign | kind << 24 | local device
   //   es_ft       = node terms {code, terminal a, terminal b, 0}, device codes
@@ -113,6 +116,7 @@ struct DevTopo {
   const int* es_jt;
   const int4* es_ft;
   const double* es_fc;
+  const int* es_hub;        // hub items: term index where each device chunk starts, then the end
   // LU program per pivot k: hdr = (off, nL, nU, diagonal slot); data at off =
   // Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots)
   const int4* lu_hdr;

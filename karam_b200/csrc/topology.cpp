@@ -697,6 +697,7 @@ void es_blocks(Topology& T) {
   T.es_jt.clear();
   T.es_ft.clear();
   T.es_fc.clear();
+  T.es_hub.clear();
   T.es_max_dev = kEsMaxDev;
   // device of a slot term / node term (-1: none)
   auto slot_dev = [&](int c) {
@@ -795,13 +796,14 @@ void es_blocks(Topology& T) {
     cur_items.push_back(it);
   }
   emit(cur_items, cur_devs, false);
+  const size_t normal_blocks = T.es_block.size();
 
-  // Hub items (the supply node and its diagonal slot): groups of up to 8
-  // share one walk over the union of their devices in chunks of kEsMaxDev
-  // (one warp sums each item). The union is in first-occurrence order; a
-  // group is kept only if every item's device indices never decrease along
-  // its terms (so each item's sum keeps its term order), otherwise each hub
-  // walks its own term occurrences.
+  // Hub items (the supply node and its diagonal slot): groups of up to
+  // kEsMaxHubs share one walk over the union of their devices in chunks of
+  // kEsMaxDev. The union is in first-occurrence order; a group is kept only
+  // if every item's device indices never decrease along its terms (so the
+  // terms of one chunk are contiguous and es_hub can bound them), otherwise
+  // each hub walks its own term occurrences.
   auto terms_of = [&](int it, std::vector<int>& out) {  // device per term, -1 = linear
     out.clear();
     if (it < nv) {
@@ -818,21 +820,38 @@ void es_blocks(Topology& T) {
     T.es_block.push_back((int)T.es_dev.size());
     T.es_block.push_back((int)dlist.size());
     T.es_dev.insert(T.es_dev.end(), dlist.begin(), dlist.end());
+    const int nch = ((int)dlist.size() + kEsMaxDev - 1) / kEsMaxDev;
     for (size_t m = 0; m < items.size(); ++m) {
       const int it = items[m];
       T.es_item.push_back(it);
       const std::vector<int>& li = lidx[m];
+      // term index where each device chunk starts (linear terms go with the
+      // chunk of the device term before them), and the end
+      const int hb = (int)T.es_hub.size();
+      {
+        int c = 0;
+        T.es_hub.push_back(0);
+        for (int t = 0; t < (int)li.size(); ++t)
+          while (li[t] >= 0 && li[t] / kEsMaxDev > c) {
+            T.es_hub.push_back(t);
+            ++c;
+          }
+        while (c < nch) {
+          T.es_hub.push_back((int)li.size());
+          ++c;
+        }
+      }
       if (it < nv) {
         T.es_item.push_back((int)T.es_jt.size());
         T.es_item.push_back(T.jt_off[it + 1] - T.jt_off[it]);
-        T.es_item.push_back(0);
+        T.es_item.push_back(hb);
         for (int q = T.jt_off[it], t = 0; q < T.jt_off[it + 1]; ++q, ++t)
           T.es_jt.push_back((T.jt_code[q] & int32_t(0xFF000000u)) | li[t]);
       } else {
         const int i = it - nv;
         T.es_item.push_back((int)T.es_ft.size() / 4);
         T.es_item.push_back(T.ft_off[i + 1] - T.ft_off[i]);
-        T.es_item.push_back(0);
+        T.es_item.push_back(hb);
         for (int q = T.ft_off[i], t = 0; q < T.ft_off[i + 1]; ++q, ++t) {
           const int c = T.ft_code[q];
           T.es_ft.push_back(li[t] >= 0 ? ((c & int32_t(0xFF000000u)) | li[t]) : c);
@@ -845,8 +864,8 @@ void es_blocks(Topology& T) {
     }
   };
   std::vector<int> tdev;
-  for (size_t h0 = 0; h0 < hubs.size(); h0 += 8) {
-    std::vector<int> items(hubs.begin() + h0, hubs.begin() + std::min(hubs.size(), h0 + 8));
+  for (size_t h0 = 0; h0 < hubs.size(); h0 += kEsMaxHubs) {
+    std::vector<int> items(hubs.begin() + h0, hubs.begin() + std::min(hubs.size(), h0 + kEsMaxHubs));
     std::vector<int> dlist;
     std::unordered_map<int, int> uid;
     std::vector<std::vector<int>> lidx(items.size());
@@ -888,6 +907,8 @@ void es_blocks(Topology& T) {
       emit_group({it}, occ, li);
     }
   }
+  // hub blocks run longest: put them first so the grid starts them first
+  std::rotate(T.es_block.begin(), T.es_block.begin() + normal_blocks, T.es_block.end());
 }
 
 }  // namespace

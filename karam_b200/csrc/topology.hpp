@@ -105,6 +105,8 @@ struct Topology {
   std::vector<int> es_ft;                   // node terms: 4 per term {code, a, b, 0}; device codes
                                             // carry the local device index
   std::vector<double> es_fc;                // node term coefficients
+  std::vector<int> es_hub;                  // per hub item: term index where each device
+                                            // chunk starts, then the end (offset in es_item w)
   int es_max_dev = 0;                       // devices per chunk (shared-memory budget)
 
   // ---- junction limiting (SoA diode order) ----
@@ -128,6 +130,7 @@ Topology build_topology(const karam_netlist* nl);
 // items of one evaluation + stamping block (nr_types.h).
 constexpr int kEsMaxDev = KES_MAX_DEV;
 constexpr int kEsMaxItems = KES_MAX_ITEMS;
+constexpr int kEsMaxHubs = KES_MAX_HUBS;
 
 // Min-Fill on an explicit factor list (exposed for tests of the ordering).
 struct MinFillResult {

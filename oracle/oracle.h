@@ -81,6 +81,14 @@ int oracle_stamp(const karam_netlist *nl, const karam_instances *inst, int32_t i
                  const double *v, double h, int32_t method, const double *cap_vprev,
                  const double *cap_iprev, double t, double *vals, double *rhs);
 
+/* The same stamping pass as oracle_stamp, reporting per CSR value the sum of
+ * the magnitudes of its triplets (abs_vals[nnz]) and their count
+ * (n_terms[nnz]): the scale of the summation error of a value whose terms are
+ * added in another order. */
+int oracle_stamp_abs(const karam_netlist *nl, const karam_instances *inst, int32_t idx,
+                     const double *v, double h, int32_t method, const double *cap_vprev,
+                     const double *cap_iprev, double t, double *abs_vals, int32_t *n_terms);
+
 /* Min-Fill ordering of FactorGraph::fromTensorizedBlock
  * (infrastructure/factor_graph.cpp:9-162, treewidth_analyzer.cpp:14-141).
  * raw[*raw_len] = eliminationOrdering as produced (branch ids included);

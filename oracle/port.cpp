@@ -761,6 +761,29 @@ int oracle_stamp(const karam_netlist* nl, const karam_instances* inst, int32_t i
   });
 }
 
+int oracle_stamp_abs(const karam_netlist* nl, const karam_instances* inst, int32_t idx,
+                     const double* v, double h, int32_t method, const double* cap_vprev,
+                     const double* cap_iprev, double t, double* abs_vals, int32_t* n_terms) {
+  return guarded([&] {
+    Session s(nl, inst, idx);
+    auto& b = s.b;
+    std::vector<double> vv(v, v + b.n), cvp(b.cap_c.size(), 0.0), cip(b.cap_c.size(), 0.0);
+    if (cap_vprev) cvp.assign(cap_vprev, cap_vprev + b.cap_c.size());
+    if (cap_iprev) cip.assign(cap_iprev, cap_iprev + b.cap_c.size());
+    std::vector<double> vl, r;
+    b.stamp(vv, h, method, cvp, cip, t, vl, r);
+    std::fill(abs_vals, abs_vals + vl.size(), 0.0);
+    std::fill(n_terms, n_terms + vl.size(), 0);
+    for (size_t k = 0; k < b.st.r.size(); ++k) {
+      const int at = b.cp.index_of(b.st.r[k], b.st.c[k]);
+      if (at < 0) continue;
+      abs_vals[at] += std::fabs(b.st.v[k]);
+      n_terms[at] += 1;
+    }
+    return 0;
+  });
+}
+
 int oracle_ordering(const karam_netlist* nl, uint32_t* raw, int32_t* raw_len, int32_t* perm) {
   return guarded([&] {
     Session s(nl, nullptr, 0);

@@ -72,6 +72,10 @@ class Oracle:
         L.oracle_stamp.argtypes = [C.POINTER(A.KaramNetlist), C.POINTER(A.KaramInstances), C.c_int32,
                                    _f64p, C.c_double, C.c_int32, _f64p, _f64p, C.c_double,
                                    _f64p, _f64p]
+        if hasattr(L, "oracle_stamp_abs"):  # restatement only
+            L.oracle_stamp_abs.argtypes = [C.POINTER(A.KaramNetlist), C.POINTER(A.KaramInstances),
+                                           C.c_int32, _f64p, C.c_double, C.c_int32, _f64p, _f64p,
+                                           C.c_double, _f64p, _i32p]
         L.oracle_ordering.argtypes = [C.POINTER(A.KaramNetlist), _u32p, _i32p, _i32p]
         L.oracle_symbolic.argtypes = [C.POINTER(A.KaramNetlist), _i32p, _i32p, _i32p, _i32p,
                                       _i32p, C.c_int32]
@@ -139,6 +143,19 @@ class Oracle:
                                    A.ptr(vals, C.c_double), A.ptr(rhs, C.c_double))
         assert rc == 0
         return vals, rhs
+
+    def stamp_abs(self, nl, v, inst=None, idx=0):
+        """Per CSR value: sum of |triplet| and the triplet count of a DC stamp at v."""
+        s = nl.as_struct()
+        rp, col = self.pattern(nl)
+        a = np.zeros(len(col))
+        cnt = np.zeros(len(col), np.int32)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        rc = self.lib.oracle_stamp_abs(C.byref(s), self._inst(inst), idx, A.ptr(v, C.c_double), 0.0,
+                                       A.TRAN_BE, None, None, 0.0, A.ptr(a, C.c_double),
+                                       A.ptr(cnt, C.c_int32))
+        assert rc == 0
+        return a, cnt
 
     def ordering(self, nl):
         s = nl.as_struct()

@@ -3,7 +3,10 @@
 Tolerances (FP64 oracle as truth, both sides polished to the FP64 fixed point):
 node voltages |dv| <= 1e-9 |v| + 1e-12 V; Norton branch currents
 I = 1e3 (V - (v+ - v-)) within 1e-12 A. Jacobian values from the FP64
-evaluation kernel within 4 ulp of the reference stamps.
+evaluation kernel within 4 ulp of the reference stamps where the kernel keeps
+the reference's term order; values with hundreds of terms (the supply node's
+diagonal), whose sums the kernel splits over warps, within twice the
+recursive-summation bound (n - 1) eps sum|t|.
 """
 import numpy as np
 import pytest
@@ -14,6 +17,7 @@ from karam_b200 import circuits
 pytestmark = pytest.mark.gpu
 
 POLISH = dict(polish_max=8)
+KES_MAX_DEV = 48  # devices one evaluation block holds (nr_types.h)
 
 
 def scaled_err(v, v_ref, rel=1e-9, abs_=1e-12):
@@ -39,12 +43,21 @@ def test_eval_stamp_fp64_matches_reference_stamps(product, ctx, port):
     vs = rng.uniform(-0.2, 2.0, size=(3, prob.n))
     jac, f = prob.eval_stamp(vs, A.PREC_FP64)
     rp, col = port.pattern(nl)
+    eps = np.finfo(np.float64).eps
     for i in range(3):
         vals, rhs = port.stamp(nl, vs[i], inst, i)
+        absum, nterms = port.stamp_abs(nl, vs[i], inst, i)
         # the gmin diagonal is not part of the evaluated Jacobian
         scale = np.maximum(np.abs(vals), 1e-300)
         ulp = np.abs(jac[i] - vals) / (np.spacing(scale))
-        assert ulp.max() <= 4, f"Jacobian differs by {ulp.max()} ulp"
+        # values with few terms are summed in the reference's term order
+        few = nterms <= 4 * KES_MAX_DEV
+        assert ulp[few].max() <= 4, f"Jacobian differs by {ulp[few].max()} ulp"
+        # hub values (hundreds of terms, split over warps): within the
+        # recursive-summation bound (n - 1) eps sum|t| of the reordered sum
+        hub = ~few
+        bound = 2 * np.maximum(nterms[hub] - 1, 1) * eps * absum[hub]
+        assert np.all(np.abs(jac[i][hub] - vals[hub]) <= bound)
         # KCL residual: device currents vs J v - rhs of the reference stamps
         jv = np.array([np.dot(vals[rp[r]:rp[r + 1]], vs[i][col[rp[r]:rp[r + 1]]]) for r in range(prob.n)])
         fref = jv - rhs
