@@ -151,7 +151,7 @@ typedef struct karam_solver_opts {
   double polish_rel;     /* polishing stops once |dv_i| <= polish_rel*|v_i| + polish_abs */
   double polish_abs;     /*   for every node, or when |dv| stops shrinking        */
   double lu_growth_limit; /* a static-pivot solve whose multipliers exceed this goes
-                            to the rescue path (FP64 static pivots, then dense
+                            to the rescue path (FP64 static pivots, then
                             partial pivoting); 0 = 1e4 in FP32 / 1e10 in FP64;
                             < 0 = no growth test (tiny or non-finite pivots and
                             non-finite solutions still go to the rescue)       */
@@ -194,7 +194,7 @@ typedef struct karam_instance_stats {
   int32_t gmin_step;    /* GMIN step reached (DC)                                 */
   int32_t seeded_ok;    /* 1 if the seeded start converged without fallback       */
   int32_t rescued;      /* linear solves redone by the rescue path (FP64 static
-                           pivots, then dense partial pivoting) because the
+                           pivots, then partial pivoting) because the
                            static pivots of the working precision were unusable */
   int32_t halvings;     /* transient step halvings after NR failures              */
   int32_t max_step_iters; /* most NR iterations spent on one transient attempt    */
@@ -324,7 +324,7 @@ typedef struct karam_timing {
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */
   int64_t rescues;          /* linear solves redone by the rescue path               */
-  int64_t rescues_dense;    /* of those, the ones that needed dense partial pivoting */
+  int64_t rescues_dense;    /* of those, the ones that needed partial pivoting       */
 } karam_timing;
 KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 

@@ -85,7 +85,7 @@ struct karam_problem {
       t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
       t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
-      t_perm;
+      t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent;
   DevTopo dt{};
   // instance buffers, [item][ld] (instance-interleaved)
   int ld = 0;
@@ -94,6 +94,7 @@ struct karam_problem {
       d_active, r_ws, r_list, r_count, i_vtp, d_counters;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
+  RescuePlan rplan;
   int* h_active = nullptr;  // pinned
 
   // accounting of the last solve call
@@ -235,6 +236,24 @@ void upload_topology(karam_problem* p) {
   std::vector<int2> src;
   for (int s = 0; s < T.nv; ++s) src.push_back(make_int2(T.slot_row[s], T.slot_col[s]));
   upload(p->t_slot_rc, src);
+  // value slots by row (row-major numbering, columns ascending) and by column
+  std::vector<int> slot_ptr(T.n + 1, 0), csc_ptr(T.n + 1, 0);
+  for (int s = 0; s < T.nv; ++s) {
+    slot_ptr[T.slot_row[s] + 1]++;
+    csc_ptr[T.slot_col[s] + 1]++;
+  }
+  for (int i = 0; i < T.n; ++i) {
+    slot_ptr[i + 1] += slot_ptr[i];
+    csc_ptr[i + 1] += csc_ptr[i];
+  }
+  std::vector<int2> csc_ent(T.nv);
+  {
+    std::vector<int> fillp(csc_ptr.begin(), csc_ptr.end() - 1);
+    for (int s = 0; s < T.nv; ++s) csc_ent[fillp[T.slot_col[s]]++] = make_int2(T.slot_row[s], s);
+  }
+  upload(p->t_slot_ptr, slot_ptr);
+  upload(p->t_csc_ptr, csc_ptr);
+  upload(p->t_csc_ent, csc_ent);
 
   DevTopo& d = p->dt;
   d.n = T.n;
@@ -281,6 +300,9 @@ void upload_topology(karam_problem* p) {
   d.lu_rec = T.lu_small ? p->t_lu_rec.as<int4>() : nullptr;
   d.lu_rec2 = T.lu_small ? p->t_lu_rec2.as<int2>() : nullptr;
   d.slot_rc = p->t_slot_rc.as<int2>();
+  d.slot_ptr = p->t_slot_ptr.as<int>();
+  d.csc_ptr = p->t_csc_ptr.as<int>();
+  d.csc_ent = p->t_csc_ent.as<int2>();
   d.seed_vs = p->t_seed_vs.as<int>();
   d.seed_anode = p->t_seed_anode.as<int>();
   d.n_seed_anode = (int)seed_an.size();
@@ -324,14 +346,18 @@ void alloc_instances(karam_problem* p) {
   p->d_counters.alloc(5 * sizeof(unsigned long long));
   ck(cudaEventCreate(&p->ev_job0), "cudaEventCreate");
   ck(cudaEventCreate(&p->ev_job1), "cudaEventCreate");
-  // Partial-pivoting rescue: one dense n x n FP64 workspace per concurrently
-  // running rescue CTA, bounded by a 2 GiB budget.
-  const size_t dense = n * n * sizeof(double);
+  // Partial-pivoting rescue: per concurrently running rescue warp, the U
+  // factor and room for rows with fill (2 n x n FP64), within a 2 GiB budget.
+  p->rplan = plan_rescue(p->dt);
+  p->rplan.ctas_per_sm = rescue_ctas_per_sm(p->dt, p->rplan);
+  const size_t per = 2 * n * n * sizeof(double);
   const size_t budget = size_t(2) << 30;
-  size_t slots = std::min<size_t>({M, (size_t)8 * std::max(1, p->ctx->num_sms), budget / dense});
+  const size_t resident =
+      (size_t)p->rplan.warps * p->rplan.ctas_per_sm * std::max(1, p->ctx->num_sms);
+  size_t slots = std::min<size_t>({M, resident, budget / per});
   p->rescue_slots = (int)slots;
   if (slots > 0) {
-    p->r_ws.alloc(slots * dense);
+    p->r_ws.alloc(slots * per);
     p->r_list.alloc(M * sizeof(RescueItem));
     p->r_count.alloc(sizeof(int));
     ck(cudaMemset(p->r_count.p, 0, sizeof(int)), "memset rescue count");
@@ -502,7 +528,7 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_l
     launch_lu(p->dt, I, P, L, prec, active, s);
     check("k_lu launch");
     cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
-    if (I.rescue_list) launch_rescue(p->dt, I, P, I.rescue_slots, s);
+    if (I.rescue_list) launch_rescue(p->dt, I, P, p->rplan, s);
     check("k_rescue launch");
     cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
   }

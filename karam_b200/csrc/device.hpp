@@ -38,11 +38,21 @@ void launch_eval_stamp(const DevTopo& T, const DevInst& I, const JobParams& P,
 // Control flow + static-pivot factor/solve of every live instance (k_lu).
 void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const RoundLaunch& L,
                int prec, int* active, cudaStream_t s);
-// Rescue of the solves whose static pivots failed (FP64 static, then dense
-// partial pivoting); one CTA per workspace slot.
-void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, int grid,
+// Rescue of the solves whose static pivots failed (FP64 static pivots, then
+// LU with partial pivoting): one warp per solve and workspace slot, `warps`
+// warps per CTA with K dense row buffers each in shared memory.
+struct RescuePlan {
+  int K = 0;
+  int warps = 0;        // 0: the problem is too large for the rescue kernel
+  size_t smem = 0;      // dynamic shared memory per CTA
+  int ctas_per_sm = 0;  // filled by the caller (occupancy)
+};
+RescuePlan plan_rescue(const DevTopo& T);
+// CTAs of the rescue kernel that can be resident per SM (sets its
+// shared-memory limit first; call outside stream capture).
+int rescue_ctas_per_sm(const DevTopo& T, const RescuePlan& R);
+void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const RescuePlan& R,
                    cudaStream_t s);
-size_t rescue_smem_bytes(const DevTopo& T);
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s);
 void interleave(const double* src, const int* perm, double* dst, int ni, int ld, int n,

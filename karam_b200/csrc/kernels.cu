@@ -67,7 +67,7 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
   }
   if (best.L > 0)
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best.smem);
-  const int rsm = (int)rescue_smem_bytes(T);
+  const int rsm = (int)plan_rescue(T).smem;
   cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
   cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
   return best;
@@ -99,18 +99,43 @@ void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const Rou
     k_lu<double><<<L.grid, kRoundThreads, L.smem, s>>>(T, I, P, L.L, active);
 }
 
-size_t rescue_smem_bytes(const DevTopo& T) {
-  size_t b = sizeof(double) * ((size_t)T.n + (size_t)std::max(T.nv, T.n)) + sizeof(int) * (size_t)T.n;
-  if (T.lu_rec) b += 16 + (2 * sizeof(int4) + sizeof(int2)) * (size_t)T.n;
-  return b;
+RescuePlan plan_rescue(const DevTopo& T) {
+  // the opt-in shared-memory limit of one CTA on sm_100 (227 KiB)
+  const size_t limit = 232448;
+  const size_t rec = (T.lu_rec ? rescue_rec_bytes(T.n) : 0) + rescue_tab_bytes(T.n, T.nv);
+  RescuePlan R;
+  for (int K = 2; K >= 0; --K) {
+    if (K > T.n) continue;
+    const size_t wb = rescue_warp_bytes(T.n, T.nv, K);
+    if (rec + wb > limit) continue;
+    R.K = K;
+    R.warps = (int)std::min<size_t>(8, (limit - rec) / wb);
+    R.smem = rec + (size_t)R.warps * wb;
+    break;
+  }
+  return R;
 }
 
-void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, int grid,
+int rescue_ctas_per_sm(const DevTopo& T, const RescuePlan& R) {
+  if (R.warps <= 0) return 0;
+  cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem);
+  cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem);
+  int a = 0, b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_rescue<float>, 32 * R.warps, R.smem) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_rescue<double>, 32 * R.warps, R.smem) !=
+          cudaSuccess)
+    return 0;
+  return std::min(a, b);
+}
+
+void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const RescuePlan& R,
                    cudaStream_t s) {
+  const int grid = (I.rescue_slots + R.warps - 1) / R.warps;
   if (P.precision == KARAM_PREC_MIXED)
-    k_rescue<float><<<grid, 256, rescue_smem_bytes(T), s>>>(T, I, P);
+    k_rescue<float><<<grid, 32 * R.warps, R.smem, s>>>(T, I, P, R.K);
   else
-    k_rescue<double><<<grid, 256, rescue_smem_bytes(T), s>>>(T, I, P);
+    k_rescue<double><<<grid, 32 * R.warps, R.smem, s>>>(T, I, P, R.K);
 }
 
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,

@@ -12,7 +12,7 @@
 //         elimination, back substitution, x = v + dx, and junction limiting
 //         (pnjlim) for DC NR iterations.
 // Solves whose static pivots fail go to k_rescue (FP64 static pivots, then
-// dense partial pivoting), launched after every round.
+// LU with partial pivoting, one warp per solve), launched after every round.
 #ifndef KARAM_NR_DEVICE_CUH
 #define KARAM_NR_DEVICE_CUH
 #include <cstdint>
@@ -1081,196 +1081,474 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
 }
 
 // ---------------------------------------------------------------------------
-// rescue of the solves whose static pivots failed: FP64 static pivots on the
-// Jacobian (working precision, widened), and when those fail too, dense FP64
-// LU with partial pivoting
-// -- the semantics of solveSparse_LU's numeric phase (math/sparse_lu.cpp:216-312)
-// on the permuted system: pivot = largest |a| in the column (ties to the
-// lower row), singular below 1e-25, rows with |a| < 1e-30 skipped. One CTA per
-// solve; the dense matrix in a global workspace slot, vectors in shared memory.
+// rescue of the solves whose static pivots failed, one warp per solve:
+//   level 1 (mixed precision only; the FP64 path already ran it): the static
+//   pivots again, in FP64 on the value slots;
+//   level 2: LU with partial pivoting -- the semantics of solveSparse_LU's
+//   numeric phase (math/sparse_lu.cpp:216-312) on the permuted system: pivot
+//   = largest |a| in the column over the rows not yet pivoted (ties to the
+//   lower position), singular below 1e-25, rows with |a| < 1e-30 not
+//   eliminated (their entry still enters the forward substitution).
+// Level 2 keeps a row in its value slots while every update it receives falls
+// on its slots (always so until a row interchange brings another row's
+// structure into play); a row that would take fill outside them moves to a
+// dense row buffer: a few per warp in shared memory, the rest in the warp's
+// global workspace. The arithmetic is that of the dense elimination: each
+// entry takes a = fma(-l, u, a) in pivot order, and the only terms left out
+// are those with u == 0 (which leave a unchanged); the right-hand side is
+// eliminated with its row, in the order of a forward substitution; U is
+// written densely and solved in the order of a column-oriented back
+// substitution, in blocks of 32 columns.
 // ---------------------------------------------------------------------------
+
+// Bytes of the pivot records staged once per rescue CTA (stage_pivots).
+__host__ __device__ inline size_t rescue_rec_bytes(int n) {
+  return ((size_t)n * (2 * sizeof(int4) + sizeof(int2)) + 15) & ~size_t(15);
+}
+// Bytes of the slot tables staged once per rescue CTA: row and column
+// pointers (n + 1 each), (row, slot) by column and the column of each slot.
+__host__ __device__ inline size_t rescue_tab_bytes(int n, int nv) {
+  return (sizeof(int) * 2 * ((size_t)n + 1) + sizeof(int2) * (size_t)nv + sizeof(int) * (size_t)nv +
+          15) &
+         ~size_t(15);
+}
+// Per-warp shared memory: value slots, right-hand side and K dense row
+// buffers (FP64), then five int arrays of n.
+__host__ __device__ inline size_t rescue_warp_bytes(int n, int nv, int K) {
+  return (sizeof(double) * ((size_t)nv + n + (size_t)K * n) + sizeof(int) * 5 * (size_t)n + 15) &
+         ~size_t(15);
+}
+
+struct RescueTab {
+  const int2* cent;  // [nv] (row, slot) by column
+  const int* cptr;   // [n + 1]
+  const int* sptr;   // [n + 1] first slot of each row
+  const int* scol;   // [nv] column of each slot (ascending within a row)
+};
+
+// Slot of column c in the slot range [s0, s1) of one row, or -1.
+__device__ __forceinline__ int find_slot(const int* __restrict__ scol, int s0, int s1, int c) {
+  int lo = s0, hi = s1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (scol[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < s1 && scol[lo] == c) ? lo : -1;
+}
+
+struct RescueWarp {
+  double* vs;   // [nv] value slots (rows kept in their slots)
+  double* bp;   // [n] right-hand side by row
+  double* fb;   // [K][n] dense row buffers in shared memory
+  double* G;    // [n - K][n] dense row buffers in global memory
+  double* U;    // [n][n] U by position, row-major (upper part)
+  int* pos_of;  // [n] position of each row
+  int* row_at;  // [n] row at each position
+  int* fat_of;  // [n] row buffer of each row, -1 = in its slots
+  int* live;    // rows with a buffer
+  int* stk;     // free buffers (shared-memory ones on top)
+  int K;
+};
+
+__device__ __forceinline__ double* rescue_buf(const RescueWarp& w, int n, int f) {
+  return f < w.K ? w.fb + (size_t)f * n : w.G + (size_t)(f - w.K) * n;
+}
+
+// One step-i elimination of row r (entry a in column i) by the pivot row:
+// prow = its dense buffer, or null when it is in its slots [ps0, ps1); Ui =
+// U row i (dense, already written); top / nlive = buffer stack and live list
+// sizes (warp-uniform).
+__device__ __forceinline__ void rescue_eliminate(const RescueTab& tb, const RescueWarp& w, int n,
+                                                 int i, int r, double a, double piv, double bP,
+                                                 const double* prow, int ps0, int ps1,
+                                                 const double* Ui, int& top, int& nlive,
+                                                 int lane) {
+  if (fabs(a) >= 1e-30) {
+    const double l = a / piv;
+    if (lane == 0) w.bp[r] = fma(-l, bP, w.bp[r]);
+    // a non-finite multiplier turns the structural zeros of the dense
+    // elimination into NaN too (l * 0): update every column from U row i
+    const bool full = !isfinite(l);
+    int fr = w.fat_of[r];
+    double* fbuf;
+    if (fr < 0) {
+      const int s0 = tb.sptr[r], s1 = tb.sptr[r + 1];
+      if (!prow && !full) {
+        // both rows in their slots: in place when the pivot row's nonzero
+        // columns past i are all slots of row r
+        bool in = true;
+        for (int s = ps0 + lane; s < ps1; s += 32) {
+          const int c = tb.scol[s];
+          if (c > i && w.vs[s] != 0.0 && find_slot(tb.scol, s0, s1, c) < 0) in = false;
+        }
+        if (__all_sync(kFull, in)) {
+          for (int s = ps0 + lane; s < ps1; s += 32) {
+            const int c = tb.scol[s];
+            const double u = w.vs[s];
+            if (c > i && u != 0.0) {
+              const int t = find_slot(tb.scol, s0, s1, c);
+              w.vs[t] = fma(-l, u, w.vs[t]);
+            }
+          }
+          __syncwarp();
+          return;
+        }
+      }
+      // row r moves to a dense row buffer
+      fr = w.stk[top - 1];
+      fbuf = rescue_buf(w, n, fr);
+      __syncwarp();
+      if (lane == 0) {
+        w.fat_of[r] = fr;
+        w.live[nlive] = r;
+      }
+      --top;
+      ++nlive;
+      if (prow && !full) {  // (slot value or 0) - l * (pivot row), in one pass
+        for (int c = i + 1 + lane; c < n; c += 32) {
+          const double u = prow[c];
+          fbuf[c] = u != 0.0 ? fma(-l, u, 0.0) : 0.0;
+        }
+        __syncwarp();
+        for (int s = s0 + lane; s < s1; s += 32) {
+          const int c = tb.scol[s];
+          if (c > i) fbuf[c] = fma(-l, prow[c], w.vs[s]);
+        }
+        __syncwarp();
+        return;
+      }
+      for (int c = i + 1 + lane; c < n; c += 32) fbuf[c] = 0.0;
+      __syncwarp();
+      for (int s = s0 + lane; s < s1; s += 32) {
+        const int c = tb.scol[s];
+        if (c > i) fbuf[c] = w.vs[s];
+      }
+      __syncwarp();
+    } else {
+      fbuf = rescue_buf(w, n, fr);
+    }
+    if (full) {
+      for (int c = i + 1 + lane; c < n; c += 32) fbuf[c] = fma(-l, Ui[c], fbuf[c]);
+    } else if (prow) {
+      for (int c = i + 1 + lane; c < n; c += 32) {
+        const double u = prow[c];
+        if (u != 0.0) fbuf[c] = fma(-l, u, fbuf[c]);
+      }
+    } else {
+      for (int s = ps0 + lane; s < ps1; s += 32) {
+        const int c = tb.scol[s];
+        const double u = w.vs[s];
+        if (c > i && u != 0.0) fbuf[c] = fma(-l, u, fbuf[c]);
+      }
+    }
+  } else if (a != 0.0 && lane == 0) {
+    w.bp[r] = fma(-a, bP, w.bp[r]);  // not eliminated; still in the forward substitution
+  }
+  __syncwarp();
+}
+
+// Level 2 on the staged system (vs with gmin on the diagonal, bp). Returns
+// true with the solution by position in vs, false when singular.
+__device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp& w, int n,
+                                          int lane) {
+  for (int r = lane; r < n; r += 32) {
+    w.pos_of[r] = r;
+    w.row_at[r] = r;
+    w.fat_of[r] = -1;
+    w.stk[r] = n - 1 - r;
+  }
+  int top = n, nlive = 0;  // warp-uniform
+  __syncwarp();
+  for (int i = 0; i < n; ++i) {
+    // pivot: rows at positions >= i with an entry in column i; the largest
+    // |a|, ties to the lower position (pos << 16 | row packs both)
+    double best = -1.0;
+    int bkey = 0x7fffffff;
+    const int e0 = tb.cptr[i], e1 = tb.cptr[i + 1];
+    for (int e = e0 + lane; e < e1; e += 32) {
+      const int2 rs = tb.cent[e];
+      const int ps = w.pos_of[rs.x];
+      if (ps >= i && w.fat_of[rs.x] < 0) {
+        const double av = fabs(w.vs[rs.y]);
+        const int key = ps << 16 | rs.x;
+        if (av > best || (av == best && key < bkey)) {
+          best = av;
+          bkey = key;
+        }
+      }
+    }
+    for (int q = lane; q < nlive; q += 32) {
+      const int r = w.live[q];
+      const double av = fabs(rescue_buf(w, n, w.fat_of[r])[i]);
+      const int key = w.pos_of[r] << 16 | r;
+      if (av > best || (av == best && key < bkey)) {
+        best = av;
+        bkey = key;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(kFull, best, o);
+      const int ok = __shfl_xor_sync(kFull, bkey, o);
+      if (ob > best || (ob == best && ok < bkey)) {
+        best = ob;
+        bkey = ok;
+      }
+    }
+    if (best < 1e-25) return false;
+    const int Pr = bkey & 0xffff, bpos = bkey >> 16;
+    const int q = w.row_at[i];
+    const int fP = w.fat_of[Pr];
+    const double* prow = fP >= 0 ? rescue_buf(w, n, fP) : nullptr;
+    const int ps0 = tb.sptr[Pr], ps1 = tb.sptr[Pr + 1];
+    __syncwarp();
+    if (lane == 0) {  // row interchange: positions only
+      w.row_at[bpos] = q;
+      w.pos_of[q] = bpos;
+      w.row_at[i] = Pr;
+      w.pos_of[Pr] = i;
+    }
+    // U row i = the pivot row from column i on
+    double* Ui = w.U + (size_t)i * n;
+    double piv;
+    if (prow) {
+      piv = prow[i];
+      for (int c = i + lane; c < n; c += 32) Ui[c] = prow[c];
+    } else {
+      // the pivot row came from column i's slot list, so that slot exists
+      piv = w.vs[find_slot(tb.scol, ps0, ps1, i)];
+      for (int c = i + lane; c < n; c += 32) Ui[c] = 0.0;
+      __syncwarp();
+      for (int s = ps0 + lane; s < ps1; s += 32) {
+        const int c = tb.scol[s];
+        if (c >= i) Ui[c] = w.vs[s];
+      }
+    }
+    __syncwarp();
+    const double bP = w.bp[Pr];
+    if (!isfinite(bP)) {
+      // the forward substitution's 0 * b of the rows with no entry in
+      // column i gives NaN (the others take theirs in the eliminations)
+      for (int k = i + 1 + lane; k < n; k += 32) {
+        const int r = w.row_at[k];
+        double a;
+        if (w.fat_of[r] >= 0) {
+          a = rescue_buf(w, n, w.fat_of[r])[i];
+        } else {
+          const int t = find_slot(tb.scol, tb.sptr[r], tb.sptr[r + 1], i);
+          a = t >= 0 ? w.vs[t] : 0.0;
+        }
+        if (a == 0.0) w.bp[r] = fma(-a, bP, w.bp[r]);
+      }
+      __syncwarp();
+    }
+    // rows in buffers first (the list only grows below), then rows in slots
+    for (int q0 = 0; q0 < nlive; q0 += 32) {
+      const int qq = q0 + lane;
+      int r = -1;
+      double a = 0.0;
+      if (qq < nlive) {
+        r = w.live[qq];
+        a = rescue_buf(w, n, w.fat_of[r])[i];
+      }
+      unsigned m = __ballot_sync(kFull, qq < nlive && r != Pr && a != 0.0);
+      while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        rescue_eliminate(tb, w, n, i, __shfl_sync(kFull, r, src), __shfl_sync(kFull, a, src), piv,
+                         bP, prow, ps0, ps1, Ui, top, nlive, lane);
+      }
+    }
+    for (int b0 = e0; b0 < e1; b0 += 32) {
+      const int e = b0 + lane;
+      int r = -1;
+      double a = 0.0;
+      bool cand = false;
+      if (e < e1) {
+        const int2 rs = tb.cent[e];
+        r = rs.x;
+        if (r != Pr && w.pos_of[r] >= i && w.fat_of[r] < 0) {
+          a = w.vs[rs.y];
+          cand = a != 0.0;
+        }
+      }
+      unsigned m = __ballot_sync(kFull, cand);
+      while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        rescue_eliminate(tb, w, n, i, __shfl_sync(kFull, r, src), __shfl_sync(kFull, a, src), piv,
+                         bP, prow, ps0, ps1, Ui, top, nlive, lane);
+      }
+    }
+    if (fP >= 0) {  // the pivot row's buffer is free again
+      int qi = -1;
+      for (int q2 = lane; q2 < nlive; q2 += 32)
+        if (w.live[q2] == Pr) qi = q2;
+      qi = __reduce_max_sync(kFull, qi);
+      __syncwarp();
+      if (lane == 0) {
+        w.live[qi] = w.live[nlive - 1];
+        w.stk[top] = fP;
+        w.fat_of[Pr] = -1;
+      }
+      --nlive;
+      ++top;
+      __syncwarp();
+    }
+  }
+
+  // back substitution by position, column-oriented in blocks of 32 columns;
+  // each lane holds its row's part of the block's triangle in registers
+  double* xs = w.vs;
+  for (int k = lane; k < n; k += 32) xs[k] = w.bp[w.row_at[k]];
+  __syncwarp();
+  for (int j1 = n; j1 > 0; j1 -= 32) {
+    const int j0 = j1 > 32 ? j1 - 32 : 0;
+    const int m = j1 - j0;
+    const int k = j0 + lane;
+    double u[32];
+    {
+      const double* Uk = w.U + (size_t)min(k, n - 1) * n + j0;
+#pragma unroll
+      for (int t = 0; t < 32; ++t) u[t] = (t < m && t >= lane) ? Uk[t] : 0.0;
+    }
+    double acc = k < j1 ? xs[k] : 0.0;
+#pragma unroll
+    for (int t = 31; t >= 0; --t) {
+      if (t < m) {
+        if (lane == t) acc = acc / u[t];
+        const double xj = __shfl_sync(kFull, acc, t);
+        if (lane < t) acc = fma(-u[t], xj, acc);
+      }
+    }
+    if (k < j1) xs[k] = acc;
+    __syncwarp();
+    // rows above the block: their 32 updates in descending column order
+    for (int r = lane; r < j0; r += 32) {
+      const double* Ur = w.U + (size_t)r * n + j0;
+      double v[32];
+#pragma unroll
+      for (int t = 0; t < 32; ++t) v[t] = Ur[t];
+      double a2 = xs[r];
+#pragma unroll
+      for (int t = 31; t >= 0; --t) a2 = fma(-v[t], xs[j0 + t], a2);
+      xs[r] = a2;
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
+// K = dense row buffers per warp in shared memory; blockDim.x / 32 warps per
+// CTA, warp w of CTA b owning workspace slot b * warps + w (U and the global
+// row buffers, 2 n^2 doubles). Shared memory: pivot records (when the
+// static-pivot program has them), slot tables, then the warps' areas.
 template <typename TJ>
-__global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams P) {
+__global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams P, int K) {
   extern __shared__ __align__(16) double rs[];
   const int n = Tp.n, nv = Tp.nv;
-  // packed pivot records behind the vectors: rs + n + max(nv, n) doubles, n ints
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const int total = *I.rescue_count;
+  if (blockIdx.x * W >= total) return;
+  unsigned char* base = reinterpret_cast<unsigned char*>(rs);
   int4* rec = nullptr;
   if (Tp.lu_rec) {
-    rec = reinterpret_cast<int4*>(
-        (reinterpret_cast<uintptr_t>(rs + n + max(nv, n)) + sizeof(int) * n + 15) & ~uintptr_t(15));
-  }
-  const size_t ld = I.ld;
-  __shared__ double red_v[8];
-  __shared__ int red_r[8];
-  __shared__ int s_piv, s_cnt, s_sing, s_ok;
-  __shared__ double s_aii;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int total = *I.rescue_count;
-  if (blockIdx.x >= total) return;
-  if (rec) {
+    rec = reinterpret_cast<int4*>(base);
     stage_pivots(Tp, rec, 1);
-    __syncthreads();
+    base += rescue_rec_bytes(n);
   }
-  double* A = I.rescue_ws + (size_t)blockIdx.x * n * n;
-  for (int e = blockIdx.x; e < total; e += gridDim.x) {
+  RescueTab tb;
+  {
+    int2* cent = reinterpret_cast<int2*>(base);
+    int* cptr = reinterpret_cast<int*>(cent + nv);
+    int* sptr = cptr + n + 1;
+    int* scol = sptr + n + 1;
+    for (int e = threadIdx.x; e < nv; e += blockDim.x) {
+      cent[e] = __ldg(&Tp.csc_ent[e]);
+      scol[e] = __ldg(&Tp.slot_rc[e]).y;
+    }
+    for (int e = threadIdx.x; e <= n; e += blockDim.x) {
+      cptr[e] = __ldg(&Tp.csc_ptr[e]);
+      sptr[e] = __ldg(&Tp.slot_ptr[e]);
+    }
+    tb.cent = cent;
+    tb.cptr = cptr;
+    tb.sptr = sptr;
+    tb.scol = scol;
+    base += rescue_tab_bytes(n, nv);
+  }
+  __syncthreads();
+  const int slot = blockIdx.x * W + warp;
+  if (slot >= I.rescue_slots) return;
+  base += (size_t)warp * rescue_warp_bytes(n, nv, K);
+  RescueWarp w;
+  w.vs = reinterpret_cast<double*>(base);
+  w.bp = w.vs + nv;
+  w.fb = w.bp + n;
+  w.pos_of = reinterpret_cast<int*>(w.fb + (size_t)K * n);
+  w.row_at = w.pos_of + n;
+  w.fat_of = w.row_at + n;
+  w.live = w.fat_of + n;
+  w.stk = w.live + n;
+  w.K = K;
+  w.U = I.rescue_ws + (size_t)slot * 2 * n * n;
+  w.G = w.U + (size_t)n * n;
+  const size_t ld = I.ld;
+  const TJ* J = reinterpret_cast<const TJ*>(I.J);
+  for (int e = slot; e < total; e += gridDim.x * W) {
     const RescueItem item = I.rescue_list[e];
     const int g = item.inst;
     const double gmin = item.gmin;
-    const TJ* J = reinterpret_cast<const TJ*>(I.J);
-    double* b = rs;  // n
-    // -- level 1 (mixed precision only; the FP64 path already ran it): static
-    //    pivots in FP64 on the value slots
-    if (tid == 0) s_ok = 0;
+    auto stage = [&]() {
+#pragma unroll 4
+      for (int s = lane; s < nv; s += 32) w.vs[s] = (double)J[(size_t)s * ld + g];
+#pragma unroll 4
+      for (int i = lane; i < n; i += 32) {
+        const size_t o = (size_t)i * ld + g;
+        w.bp[i] = -(I.F[o] + gmin * I.v[o]);
+      }
+      __syncwarp();
+      for (int i = lane; i < n; i += 32) w.vs[__ldg(&Tp.lu_hdr[i]).w] += gmin;
+      __syncwarp();
+    };
+    int ok = 0;
+    const double* sol = w.bp;
     if (P.precision == KPREC_MIXED) {
-      double* As = rs + n;  // nv
-      for (int s = tid; s < nv; s += blockDim.x) As[s] = (double)J[(size_t)s * ld + g];
-      for (int i = tid; i < n; i += blockDim.x) {
-        const size_t o = (size_t)i * ld + g;
-        b[i] = -(I.F[o] + gmin * I.v[o]);
-      }
-      __syncthreads();
-      for (int i = tid; i < n; i += blockDim.x) As[Tp.lu_hdr[i].w] += gmin;
-      __syncthreads();
-      if (tid == 0) s_ok = lu_solve<double>(As, b, 1, Tp, rec, 1e-25, P.growth64) ? 1 : 0;
+      stage();
+      if (lane == 0) ok = lu_solve<double>(w.vs, w.bp, 1, Tp, rec, 1e-25, P.growth64) ? 1 : 0;
+      ok = __shfl_sync(kFull, ok, 0);
+      __syncwarp();
     }
-    __syncthreads();
-    if (!s_ok) {
-      // -- level 2: dense partial pivoting
-      double* lval = rs + n;                          // n
-      int* rows = reinterpret_cast<int*>(lval + n);  // n
-      for (size_t q = tid; q < (size_t)n * n; q += blockDim.x) A[q] = 0.0;
-      __syncthreads();
-      for (int s = tid; s < nv; s += blockDim.x) {
-        const int2 rc = Tp.slot_rc[s];
-        A[(size_t)rc.x * n + rc.y] = (double)J[(size_t)s * ld + g];
+    if (!ok) {
+      stage();
+      if (rescue_pp(tb, w, n, lane)) {
+        ok = 1;
+        sol = w.vs;
+        if (lane == 0 && I.counters) atomicAdd(&I.counters[4], 1ull);
       }
-      for (int i = tid; i < n; i += blockDim.x) {
-        const size_t o = (size_t)i * ld + g;
-        b[i] = -(I.F[o] + gmin * I.v[o]);
-      }
-      __syncthreads();
-      for (int i = tid; i < n; i += blockDim.x) A[(size_t)i * n + i] += gmin;
-      if (tid == 0) s_sing = 0;
-      __syncthreads();
-      for (int i = 0; i < n; ++i) {
-        if (tid == 0) s_cnt = 0;
-        __syncthreads();
-        double best = -1.0;
-        int brow = n;
-        for (int r = i + tid; r < n; r += blockDim.x) {
-          const double av = fabs(A[(size_t)r * n + i]);
-          if (av > best || (av == best && r < brow)) {
-            best = av;
-            brow = r;
-          }
-          if (r > i && av >= 1e-30) rows[atomicAdd(&s_cnt, 1)] = r;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-          const double ob = __shfl_xor_sync(kFull, best, o);
-          const int orow = __shfl_xor_sync(kFull, brow, o);
-          if (ob > best || (ob == best && orow < brow)) {
-            best = ob;
-            brow = orow;
-          }
-        }
-        if (lane == 0) {
-          red_v[warp] = best;
-          red_r[warp] = brow;
-        }
-        __syncthreads();
-        if (tid == 0) {
-          double bv = red_v[0];
-          int br = red_r[0];
-          for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-            if (red_v[w] > bv || (red_v[w] == bv && red_r[w] < br)) {
-              bv = red_v[w];
-              br = red_r[w];
-            }
-          if (bv < 1e-25) s_sing = 1;
-          s_piv = br;
-          s_aii = fabs(A[(size_t)i * n + i]);
-        }
-        __syncthreads();
-        if (s_sing) break;
-        const int p = s_piv;
-        if (p != i) {
-          for (int c = tid; c < n; c += blockDim.x) {
-            const double t = A[(size_t)i * n + c];
-            A[(size_t)i * n + c] = A[(size_t)p * n + c];
-            A[(size_t)p * n + c] = t;
-          }
-          if (tid == 0) {
-            const double t = b[i];
-            b[i] = b[p];
-            b[p] = t;
-            // row p now holds the old row i: it stays in the list only if its
-            // entry in column i is not negligible
-            if (!(s_aii >= 1e-30))
-              for (int q = 0; q < s_cnt; ++q)
-                if (rows[q] == p) {
-                  rows[q] = rows[s_cnt - 1];
-                  s_cnt--;
-                  break;
-                }
-          }
-        }
-        __syncthreads();
-        const int m = s_cnt;
-        const double piv = A[(size_t)i * n + i];
-        for (int q = tid; q < m; q += blockDim.x) {
-          const int r = rows[q];
-          const double l = A[(size_t)r * n + i] / piv;
-          A[(size_t)r * n + i] = l;
-          lval[q] = l;
-        }
-        __syncthreads();
-        const int w = n - i - 1;
-        for (int e2 = tid; e2 < m * w; e2 += blockDim.x) {
-          const int q = e2 / w, c = i + 1 + (e2 - q * w);
-          A[(size_t)rows[q] * n + c] -= lval[q] * A[(size_t)i * n + c];
-        }
-        __syncthreads();
-      }
-      if (!s_sing) {
-        for (int j = 0; j < n; ++j) {  // forward substitution, unit lower
-          const double bj = b[j];
-          for (int r = j + 1 + tid; r < n; r += blockDim.x) b[r] -= A[(size_t)r * n + j] * bj;
-          __syncthreads();
-        }
-        for (int j = n - 1; j >= 0; --j) {  // back substitution
-          if (tid == 0) b[j] /= A[(size_t)j * n + j];
-          __syncthreads();
-          const double xj = b[j];
-          for (int r = tid; r < j; r += blockDim.x) b[r] -= A[(size_t)r * n + j] * xj;
-          __syncthreads();
-        }
-        if (tid == 0) {
-          s_ok = 1;
-          if (I.counters) atomicAdd(&I.counters[4], 1ull);
-        }
-      }
-      __syncthreads();
     }
-    if (s_ok) {
+    if (ok) {
       const bool sanitize = (item.act & ACT_LIMIT) != 0;
-      for (int i = tid; i < n; i += blockDim.x) {
+      for (int i = lane; i < n; i += 32) {
         const size_t o = (size_t)i * ld + g;
-        double xi = I.v[o] + b[i];
+        double xi = I.v[o] + sol[i];
         if (sanitize && !isfinite(xi)) xi = 0.0;
         I.x[o] = xi;
       }
-      __syncthreads();
-      if (tid == 0) {
+      __syncwarp();
+      if (lane == 0) {
         if (sanitize)
           for (int d = 0; d < Tp.n_dio; ++d) limit_one(Tp, d, I.x, I.v, ld, g);
         I.st[g].rescued += 1;
         if (I.counters) atomicAdd(&I.counters[3], 1ull);
       }
-    } else if (tid == 0) {
+    } else if (lane == 0) {
       on_singular(Tp, I, g);
       set_eval_point(I, P, g, I.st[g]);
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 

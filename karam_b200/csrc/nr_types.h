@@ -126,6 +126,9 @@ struct DevTopo {
                             // Lslot, Lrow | Uslot0, Uslot1, T0, T1; see topology.cpp), else 0
   const int2* lu_rec2;      // back-substitution columns (Ucol0, Ucol1) per pivot
   const int2* slot_rc;      // (row, col) of every value slot (permuted)
+  const int* slot_ptr;      // [n + 1] first slot of each row (columns ascending within a row)
+  const int* csc_ptr;       // [n + 1] value slots by column: (row, slot) in csc_ent
+  const int2* csc_ent;
   const int* seed_vs;       // permuted positive node per source (-1 = ground)
   const int* seed_anode;    // permuted anode per netlist diode (-1 = ground)
   int n_seed_anode;
@@ -154,12 +157,12 @@ struct DevInst {
   double* v_tp;             // [n][ld] voltages at the last accepted time point
   InstState* st;            // [ni]
   const double* seed;       // [n][ld] caller guesses (permuted) or 0
-  double* rescue_ws;        // [rescue_slots][n][n] dense workspaces
+  double* rescue_ws;        // [rescue_slots][2][n][n]: U and dense row buffers per rescue warp
   RescueItem* rescue_list;  // [ni]
   int* rescue_count;
-  int rescue_slots;
+  int rescue_slots;         // rescue warps (one workspace each)
   unsigned long long* counters;  // [5]: evaluations DC, evaluations transient, solves,
-                                 // rescues, rescues that needed dense partial pivoting
+                                 // rescues, rescues that needed partial pivoting
   double* wave;             // [ni][wave_steps][n_wave] node voltages after each step
   const int* wave_pos;      // permuted positions of the recorded nodes (-1 = ground)
   int n_wave, wave_steps;
