@@ -63,6 +63,16 @@ extern "C" {
 #define KARAM_TRAN_BE 0    /* backward Euler (Gear1, math/integration_method.h:83-115) */
 #define KARAM_TRAN_TRAP 1  /* trapezoidal (math/integration_method.h:47-81)           */
 
+#define KARAM_SEED_NONE 0   /* plain NR from the reference seed (seedInitialGuess)     */
+#define KARAM_SEED_CALLER 1 /* the caller's guesses (karam_solve_dc seed_v)            */
+#define KARAM_SEED_EMA 2    /* batch statistical seeder, NeuralSeeder::predictSeed
+                               (solvers/neural_seeder.h:100-137): the first
+                               KARAM_SEED_HISTORY instances run plain NR; their
+                               converged DC solutions, each weighted 0.8 per later
+                               one, seed every instance when the mean per-node
+                               confidence 1 / (1 + variance) is at least 0.3       */
+#define KARAM_SEED_HISTORY 8
+
 #define KARAM_SRC_DC 0
 #define KARAM_SRC_PULSE 1  /* PULSE(v1 v2 td tr tf pw per), physics/circuitsim.h:2155-2170 */
 
@@ -155,9 +165,12 @@ typedef struct karam_solver_opts {
                             partial pivoting); 0 = 1e4 in FP32 / 1e10 in FP64;
                             < 0 = no growth test (tiny or non-finite pivots and
                             non-finite solutions still go to the rescue)       */
-  int32_t seeded;        /* 1: start from the caller's guess at the final GMIN
-                            step; fall back to full GMIN stepping if it has not
-                            converged after seed_max_iter iterations              */
+  int32_t seeded;        /* KARAM_SEED_*: a seeded instance starts from its seed at
+                            the final GMIN step and falls back to full GMIN
+                            stepping if it has not converged after seed_max_iter
+                            iterations. KARAM_SEED_CALLER needs karam_solve_dc's
+                            seed_v; KARAM_SEED_EMA applies to batches of more than
+                            KARAM_SEED_HISTORY instances (smaller ones run plain) */
   int32_t seed_max_iter; /* K of the seeded fallback                              */
   int32_t schedule;      /* instances per CTA of the factor/solve kernel (1, 2, 4, ..., 32);
                             0 = chosen from shared memory, occupancy and batch size */

@@ -18,6 +18,10 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 TRAN_BE = 0
 TRAN_TRAP = 1
+SEED_NONE = 0
+SEED_CALLER = 1
+SEED_EMA = 2
+SEED_HISTORY = 8
 SRC_DC = 0
 SRC_PULSE = 1
 MODEL_NMOS = 0

@@ -91,7 +91,7 @@ struct karam_problem {
   int ld = 0;
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
-      d_active, r_ws, r_list, r_count, i_vtp, d_counters;
+      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
@@ -343,6 +343,7 @@ void alloc_instances(karam_problem* p) {
   p->i_vtp.alloc(ld * n * sizeof(double));
   p->i_out.alloc(ld * n * sizeof(double));
   p->d_active.alloc(sizeof(int));
+  p->d_seed_ok.alloc(sizeof(int));
   p->d_counters.alloc(5 * sizeof(unsigned long long));
   ck(cudaEventCreate(&p->ev_job0), "cudaEventCreate");
   ck(cudaEventCreate(&p->ev_job1), "cudaEventCreate");
@@ -355,6 +356,11 @@ void alloc_instances(karam_problem* p) {
   const size_t resident =
       (size_t)p->rplan.warps * p->rplan.ctas_per_sm * std::max(1, p->ctx->num_sms);
   size_t slots = std::min<size_t>({M, resident, budget / per});
+  // whole CTAs: every warp of the grid takes items (item e on CTA e % grid)
+  if (slots >= (size_t)p->rplan.warps)
+    slots -= slots % p->rplan.warps;
+  else if (slots > 0)
+    p->rplan.warps = (int)slots;
   p->rescue_slots = (int)slots;
   if (slots > 0) {
     p->r_ws.alloc(slots * per);
@@ -464,6 +470,9 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
   P.method = method;
   P.seeded = o->seeded;
   P.seed_max_iter = o->seed_max_iter;
+  P.seed_bcast = 0;
+  if (P.seeded < KARAM_SEED_NONE || P.seeded > KARAM_SEED_EMA)
+    throw std::runtime_error("unknown seeded mode");
   P.max_halvings = o->max_halvings;
   P.growth32 = o->lu_growth_limit > 0 ? o->lu_growth_limit : (o->lu_growth_limit < 0 ? 1e300 : 1e4);
   P.growth64 = o->lu_growth_limit > 0 ? o->lu_growth_limit : (o->lu_growth_limit < 0 ? 1e300 : 1e10);
@@ -623,7 +632,9 @@ void end_job(karam_problem* p) {
 
 void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
   DevInst I = dev_inst(p);
-  if (P.seeded && seed_v) {
+  if (P.seeded == KARAM_SEED_EMA) {
+    I.seed = p->i_seed.as<double>();  // written by ema_seed
+  } else if (P.seeded && seed_v) {
     // caller guesses arrive instance-major in node order; the device works
     // instance-interleaved in permuted order
     const int n = p->topo.n;
@@ -642,6 +653,45 @@ void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
   p->t_now = P.n_steps > 0 ? P.n_steps * P.h : 0.0;
   p->tran_h = P.h;
   p->tran_method = P.method;
+}
+
+// KARAM_SEED_EMA: plain DC of the first KARAM_SEED_HISTORY instances, then
+// their statistical seed for the whole batch. Returns the parameters of the
+// batch job: seeded from lane 0 of i_seed, or plain when the batch is too
+// small or the seeder is not confident.
+JobParams ema_seed(karam_problem* p, JobParams P, const karam_solver_opts* opts) {
+  const int N = p->ni;
+  if (N <= KARAM_SEED_HISTORY) {
+    P.seeded = KARAM_SEED_NONE;
+    return P;
+  }
+  JobParams P1 = P;
+  P1.seeded = KARAM_SEED_NONE;
+  P1.n_steps = 0;
+  P1.h = 0.0;
+  p->ni = KARAM_SEED_HISTORY;
+  try {
+    start_job(p, P1, nullptr);
+    run_rounds(p, P1, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
+  } catch (...) {
+    p->ni = N;
+    throw;
+  }
+  p->ni = N;
+  launch_ema_seed(p->dt, dev_inst(p), KARAM_SEED_HISTORY, p->i_seed.as<double>(),
+                  p->d_seed_ok.as<int>(), p->ctx->stream);
+  ck(cudaGetLastError(), "seed launch");
+  p->timing.other_launches += 1;
+  ck(cudaMemcpyAsync(p->h_active, p->d_seed_ok.p, sizeof(int), cudaMemcpyDeviceToHost,
+                     p->ctx->stream),
+     "D2H seed flag");
+  ck(cudaStreamSynchronize(p->ctx->stream), "seed sync");
+  if (*p->h_active) {
+    P.seed_bcast = 1;
+  } else {
+    P.seeded = KARAM_SEED_NONE;
+  }
+  return P;
 }
 
 }  // namespace
@@ -763,8 +813,10 @@ int karam_solve_dc(karam_problem* p, const karam_solver_opts* opts, const double
   return guarded(p->ctx, [&] {
     need_device(p);
     JobParams P = job_params(opts, 0, 0.0, KARAM_TRAN_BE);
-    if (P.seeded && !seed_v) throw std::runtime_error("seeded solve without seed_v");
+    if (P.seeded == KARAM_SEED_CALLER && !seed_v)
+      throw std::runtime_error("seeded solve without seed_v");
     begin_job(p);
+    if (P.seeded == KARAM_SEED_EMA) P = ema_seed(p, P, opts);
     start_job(p, P, seed_v);
     run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
     end_job(p);
@@ -781,8 +833,10 @@ int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double 
   return guarded(p->ctx, [&] {
     need_device(p);
     JobParams P = job_params(opts, n_steps, dt, method);
-    if (P.seeded) throw std::runtime_error("seeded starts need karam_solve_dc");
+    if (P.seeded == KARAM_SEED_CALLER)
+      throw std::runtime_error("caller seeds need karam_solve_dc");
     begin_job(p);
+    if (P.seeded == KARAM_SEED_EMA) P = ema_seed(p, P, opts);
     start_job(p, P, nullptr);
     run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
     end_job(p);

@@ -77,6 +77,11 @@ void launch_init(const DevTopo& T, const DevInst& I, const JobParams& P, cudaStr
   k_init<<<(I.ni + 127) / 128, 128, 0, s>>>(T, I, P);
 }
 
+void launch_ema_seed(const DevTopo& T, const DevInst& I, int W, double* seed, int* ok,
+                     cudaStream_t s) {
+  k_ema_seed<<<1, 256, 0, s>>>(T, I, W, seed, ok);
+}
+
 void launch_tran_start(const DevTopo& T, const DevInst& I, const JobParams& P, int init_caps,
                        cudaStream_t s) {
   k_tran_start<<<(I.ni + 127) / 128, 128, 0, s>>>(T, I, P, init_caps);

@@ -24,6 +24,7 @@ namespace knr {
 constexpr int kRoundThreads = 512;
 constexpr int kMaxLanes = 32;
 constexpr unsigned kFull = 0xffffffffu;
+#define KARAM_SEED_HISTORY_MAX 8  // NeuralSeeder::Config::maxHistory
 
 enum Act : int {
   ACT_SOLVE = 1,
@@ -91,7 +92,8 @@ __global__ void k_init(DevTopo T, DevInst I, JobParams P) {
   const size_t ld = I.ld;
   const bool seeded = P.seeded && I.seed != nullptr;
   if (seeded) {
-    for (int i = 0; i < T.n; ++i) I.v[i * ld + g] = I.seed[i * ld + g];
+    const int sg = P.seed_bcast ? 0 : g;
+    for (int i = 0; i < T.n; ++i) I.v[i * ld + g] = I.seed[i * ld + sg];
   } else {
     reference_seed(T, I, g, I.v);
   }
@@ -111,6 +113,62 @@ __global__ void k_init(DevTopo T, DevInst I, JobParams P) {
   I.red_f[g] = 0ull;
   I.red_dv[g] = 0ull;
   I.red_flags[g] = 3;
+}
+
+// NeuralSeeder::predictSeed (solvers/neural_seeder.h:100-137, confidence
+// :194-219) over the DC solutions of instances 0..W-1 recorded in order, the
+// converged ones only (recordSolution follows a successful solve): snapshot j
+// of m weighs 0.8^(m-1-j); one snapshot is returned as it is; otherwise the
+// weighted mean, kept when the mean over nodes of 1 / (1 + weighted variance)
+// is at least 0.3. Writes the seed to lane 0 of `seed` and *ok. One CTA.
+__global__ void k_ema_seed(DevTopo T, DevInst I, int W, double* seed, int* ok) {
+  __shared__ double wt[KARAM_SEED_HISTORY_MAX];
+  __shared__ int idx[KARAM_SEED_HISTORY_MAX];
+  __shared__ int s_m;
+  __shared__ double s_conf[32];
+  if (threadIdx.x == 0) {
+    int m = 0;
+    for (int j = 0; j < W && j < KARAM_SEED_HISTORY_MAX; ++j) {
+      if (I.st[j].status != KST_CONVERGED) continue;
+      for (int r = 0; r < m; ++r) wt[r] *= 0.8;  // recordSolution ages the history
+      wt[m] = 1.0;
+      idx[m++] = j;
+    }
+    s_m = m;
+  }
+  __syncthreads();
+  const int m = s_m;
+  const size_t ld = I.ld;
+  double conf = 0.0;
+  for (int i = threadIdx.x; i < T.n; i += blockDim.x) {
+    if (m == 0) break;
+    if (m == 1) {
+      seed[i * ld] = I.v[i * ld + idx[0]];
+      continue;
+    }
+    double sum = 0.0, tw = 0.0;
+    for (int r = 0; r < m; ++r) {  // unfused, as the reference's expressions
+      tw += wt[r];
+      sum = __dadd_rn(sum, __dmul_rn(I.v[i * ld + idx[r]], wt[r]));
+    }
+    const double si = sum / tw;
+    double var = 0.0, tw2 = 0.0;
+    for (int r = 0; r < m; ++r) {
+      const double d = I.v[i * ld + idx[r]] - si;
+      var = __dadd_rn(var, __dmul_rn(__dmul_rn(wt[r], d), d));
+      tw2 += wt[r];
+    }
+    conf += 1.0 / (1.0 + (var / tw2) / (1.0 * 1.0));
+    seed[i * ld] = si;
+  }
+  for (int o = 16; o > 0; o >>= 1) conf += __shfl_xor_sync(kFull, conf, o);
+  if ((threadIdx.x & 31) == 0) s_conf[threadIdx.x >> 5] = conf;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += s_conf[w];
+    *ok = m == 1 || (m >= 2 && c / T.n >= 0.3);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1112,10 +1170,12 @@ __host__ __device__ inline size_t rescue_tab_bytes(int n, int nv) {
           15) &
          ~size_t(15);
 }
-// Per-warp shared memory: value slots, right-hand side and K dense row
-// buffers (FP64), then five int arrays of n.
+// Per-warp shared memory: value slots, right-hand side, K dense row buffers
+// and the candidate entries (FP64), then five int arrays of n and the
+// candidate rows.
 __host__ __device__ inline size_t rescue_warp_bytes(int n, int nv, int K) {
-  return (sizeof(double) * ((size_t)nv + n + (size_t)K * n) + sizeof(int) * 5 * (size_t)n + 15) &
+  return (sizeof(double) * ((size_t)nv + n + (size_t)K * n + 32) +
+          sizeof(int) * (5 * (size_t)n + 32) + 15) &
          ~size_t(15);
 }
 
@@ -1150,6 +1210,8 @@ struct RescueWarp {
   int* fat_of;  // [n] row buffer of each row, -1 = in its slots
   int* live;    // rows with a buffer
   int* stk;     // free buffers (shared-memory ones on top)
+  int* cr;      // [32] candidate rows of the current column
+  double* ca;   // [32] their entries
   int K;
 };
 
@@ -1158,13 +1220,13 @@ __device__ __forceinline__ double* rescue_buf(const RescueWarp& w, int n, int f)
 }
 
 // One step-i elimination of row r (entry a in column i) by the pivot row:
-// prow = its dense buffer, or null when it is in its slots [ps0, ps1); Ui =
-// U row i (dense, already written); top / nlive = buffer stack and live list
-// sizes (warp-uniform).
+// prow = its dense buffer, or null when it is in its slots [ps0, ps1); Uc =
+// U row i, already written (column-major: Uc[c * n]); top / nlive = buffer
+// stack and live list sizes (warp-uniform).
 __device__ __forceinline__ void rescue_eliminate(const RescueTab& tb, const RescueWarp& w, int n,
                                                  int i, int r, double a, double piv, double bP,
                                                  const double* prow, int ps0, int ps1,
-                                                 const double* Ui, int& top, int& nlive,
+                                                 const double* Uc, int& top, int& nlive,
                                                  int lane) {
   if (fabs(a) >= 1e-30) {
     const double l = a / piv;
@@ -1231,7 +1293,7 @@ __device__ __forceinline__ void rescue_eliminate(const RescueTab& tb, const Resc
       fbuf = rescue_buf(w, n, fr);
     }
     if (full) {
-      for (int c = i + 1 + lane; c < n; c += 32) fbuf[c] = fma(-l, Ui[c], fbuf[c]);
+      for (int c = i + 1 + lane; c < n; c += 32) fbuf[c] = fma(-l, Uc[(size_t)c * n], fbuf[c]);
     } else if (prow) {
       for (int c = i + 1 + lane; c < n; c += 32) {
         const double u = prow[c];
@@ -1251,7 +1313,9 @@ __device__ __forceinline__ void rescue_eliminate(const RescueTab& tb, const Resc
 }
 
 // Level 2 on the staged system (vs with gmin on the diagonal, bp). Returns
-// true with the solution by position in vs, false when singular.
+// true with the solution by position in vs, false when singular. U is
+// written column-major (U[c * n + r] = u_rc) for a coalesced back
+// substitution.
 __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp& w, int n,
                                           int lane) {
   for (int r = lane; r < n; r += 32) {
@@ -1262,47 +1326,117 @@ __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp&
   }
   int top = n, nlive = 0;  // warp-uniform
   __syncwarp();
+  const unsigned below = (1u << lane) - 1u;
   for (int i = 0; i < n; ++i) {
-    // pivot: rows at positions >= i with an entry in column i; the largest
-    // |a|, ties to the lower position (pos << 16 | row packs both)
+    // 1. candidates: rows at positions >= i with a nonzero entry in column i
+    //    (rows in buffers, then rows in slots), listed in cr / ca while they
+    //    fit; zeros never win the pivot search unless the column is singular
+    int cnt = 0;  // warp-uniform
+    for (int q0 = 0; q0 < nlive; q0 += 32) {
+      const int qq = q0 + lane;
+      int r = -1;
+      double a = 0.0;
+      if (qq < nlive) {
+        r = w.live[qq];
+        a = rescue_buf(w, n, w.fat_of[r])[i];
+      }
+      const bool c = qq < nlive && a != 0.0;
+      const unsigned m = __ballot_sync(kFull, c);
+      if (c) {
+        const int q = cnt + __popc(m & below);
+        if (q < 32) {
+          w.cr[q] = r;
+          w.ca[q] = a;
+        }
+      }
+      cnt += __popc(m);
+    }
+    const int e0 = tb.cptr[i], e1 = tb.cptr[i + 1];
+    for (int b0 = e0; b0 < e1; b0 += 32) {
+      const int e = b0 + lane;
+      int r = -1;
+      double a = 0.0;
+      bool c = false;
+      if (e < e1) {
+        const int2 rs = tb.cent[e];
+        r = rs.x;
+        if (w.pos_of[r] >= i && w.fat_of[r] < 0) {
+          a = w.vs[rs.y];
+          c = a != 0.0;
+        }
+      }
+      const unsigned m = __ballot_sync(kFull, c);
+      if (c) {
+        const int q = cnt + __popc(m & below);
+        if (q < 32) {
+          w.cr[q] = r;
+          w.ca[q] = a;
+        }
+      }
+      cnt += __popc(m);
+    }
+    __syncwarp();
+    // 2. pivot: the largest |a|, ties to the lower position (pos << 16 | row)
     double best = -1.0;
     int bkey = 0x7fffffff;
-    const int e0 = tb.cptr[i], e1 = tb.cptr[i + 1];
-    for (int e = e0 + lane; e < e1; e += 32) {
-      const int2 rs = tb.cent[e];
-      const int ps = w.pos_of[rs.x];
-      if (ps >= i && w.fat_of[rs.x] < 0) {
-        const double av = fabs(w.vs[rs.y]);
-        const int key = ps << 16 | rs.x;
+    if (cnt <= 4) {  // a short list: every lane scans it
+      for (int q = 0; q < cnt; ++q) {
+        const int r = w.cr[q];
+        const double av = fabs(w.ca[q]);
+        const int key = w.pos_of[r] << 16 | r;
         if (av > best || (av == best && key < bkey)) {
           best = av;
           bkey = key;
         }
       }
-    }
-    for (int q = lane; q < nlive; q += 32) {
-      const int r = w.live[q];
-      const double av = fabs(rescue_buf(w, n, w.fat_of[r])[i]);
-      const int key = w.pos_of[r] << 16 | r;
-      if (av > best || (av == best && key < bkey)) {
-        best = av;
-        bkey = key;
+    } else {
+      if (cnt <= 32) {
+        if (lane < cnt) {
+          const int r = w.cr[lane];
+          best = fabs(w.ca[lane]);
+          bkey = w.pos_of[r] << 16 | r;
+        }
+      } else {  // more than the list holds: rescan
+        for (int q = lane; q < nlive; q += 32) {
+          const int r = w.live[q];
+          const double av = fabs(rescue_buf(w, n, w.fat_of[r])[i]);
+          const int key = w.pos_of[r] << 16 | r;
+          if (av > best || (av == best && key < bkey)) {
+            best = av;
+            bkey = key;
+          }
+        }
+        for (int e = e0 + lane; e < e1; e += 32) {
+          const int2 rs = tb.cent[e];
+          const int ps = w.pos_of[rs.x];
+          if (ps >= i && w.fat_of[rs.x] < 0) {
+            const double av = fabs(w.vs[rs.y]);
+            const int key = ps << 16 | rs.x;
+            if (av > best || (av == best && key < bkey)) {
+              best = av;
+              bkey = key;
+            }
+          }
+        }
       }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(kFull, best, o);
-      const int ok = __shfl_xor_sync(kFull, bkey, o);
-      if (ob > best || (ob == best && ok < bkey)) {
-        best = ob;
-        bkey = ok;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(kFull, best, o);
+        const int ok = __shfl_xor_sync(kFull, bkey, o);
+        if (ob > best || (ob == best && ok < bkey)) {
+          best = ob;
+          bkey = ok;
+        }
       }
     }
     if (best < 1e-25) return false;
     const int Pr = bkey & 0xffff, bpos = bkey >> 16;
     const int q = w.row_at[i];
     const int fP = w.fat_of[Pr];
-    const double* prow = fP >= 0 ? rescue_buf(w, n, fP) : nullptr;
+    double* prow = fP >= 0 ? rescue_buf(w, n, fP) : nullptr;
     const int ps0 = tb.sptr[Pr], ps1 = tb.sptr[Pr + 1];
+    // the pivot row came from column i's list, so a slot-resident one has that slot
+    const double piv = prow ? prow[i] : w.vs[find_slot(tb.scol, ps0, ps1, i)];
+    const double bP = w.bp[Pr];
     __syncwarp();
     if (lane == 0) {  // row interchange: positions only
       w.row_at[bpos] = q;
@@ -1310,24 +1444,70 @@ __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp&
       w.row_at[i] = Pr;
       w.pos_of[Pr] = i;
     }
-    // U row i = the pivot row from column i on
-    double* Ui = w.U + (size_t)i * n;
-    double piv;
+    double* Uc = w.U + i;  // U row i: Uc[c * n]
+
+    // 3. the common step of a row interchange chain: the pivot row in a
+    //    buffer and one other candidate, in its slots, eliminated with a
+    //    finite multiplier -- the candidate takes over the pivot row's
+    //    buffer (same values as a fresh buffer)
+    bool fast = false;
+    int fr = -1, s0 = 0, s1 = 0;
+    double fa = 0.0, fl = 0.0;
+    if (prow && cnt == 2 && isfinite(bP)) {
+      fr = w.cr[0] == Pr ? w.cr[1] : w.cr[0];
+      fa = w.cr[0] == Pr ? w.ca[1] : w.ca[0];
+      s0 = tb.sptr[fr];
+      s1 = tb.sptr[fr + 1];
+      if (w.fat_of[fr] < 0 && fabs(fa) >= 1e-30 && s1 - s0 <= 32) {
+        fl = fa / piv;
+        fast = isfinite(fl);
+      }
+    }
+    if (fast) {
+      const double l = fl;
+      if (lane == 0) w.bp[fr] = fma(-l, bP, w.bp[fr]);
+      int sc = -1;
+      double sv = 0.0;
+      if (s0 + lane < s1) {
+        sc = tb.scol[s0 + lane];
+        if (sc > i)
+          sv = fma(-l, prow[sc], w.vs[s0 + lane]);
+        else
+          sc = -1;
+      }
+      __syncwarp();
+      for (int c = i + lane; c < n; c += 32) {
+        const double u = prow[c];
+        Uc[(size_t)c * n] = u;
+        if (c > i) prow[c] = u != 0.0 ? fma(-l, u, 0.0) : 0.0;
+      }
+      __syncwarp();
+      if (sc >= 0) prow[sc] = sv;
+      int qi = -1;
+      for (int q2 = lane; q2 < nlive; q2 += 32)
+        if (w.live[q2] == Pr) qi = q2;
+      qi = __reduce_max_sync(kFull, qi);
+      if (lane == 0) {
+        w.fat_of[fr] = fP;
+        w.fat_of[Pr] = -1;
+        w.live[qi] = fr;
+      }
+      __syncwarp();
+      continue;
+    }
+
+    // 4. general step: U row i, then every other candidate
     if (prow) {
-      piv = prow[i];
-      for (int c = i + lane; c < n; c += 32) Ui[c] = prow[c];
+      for (int c = i + lane; c < n; c += 32) Uc[(size_t)c * n] = prow[c];
     } else {
-      // the pivot row came from column i's slot list, so that slot exists
-      piv = w.vs[find_slot(tb.scol, ps0, ps1, i)];
-      for (int c = i + lane; c < n; c += 32) Ui[c] = 0.0;
+      for (int c = i + lane; c < n; c += 32) Uc[(size_t)c * n] = 0.0;
       __syncwarp();
       for (int s = ps0 + lane; s < ps1; s += 32) {
         const int c = tb.scol[s];
-        if (c >= i) Ui[c] = w.vs[s];
+        if (c >= i) Uc[(size_t)c * n] = w.vs[s];
       }
     }
     __syncwarp();
-    const double bP = w.bp[Pr];
     if (!isfinite(bP)) {
       // the forward substitution's 0 * b of the rows with no entry in
       // column i gives NaN (the others take theirs in the eliminations)
@@ -1344,42 +1524,51 @@ __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp&
       }
       __syncwarp();
     }
-    // rows in buffers first (the list only grows below), then rows in slots
-    for (int q0 = 0; q0 < nlive; q0 += 32) {
-      const int qq = q0 + lane;
-      int r = -1;
-      double a = 0.0;
-      if (qq < nlive) {
-        r = w.live[qq];
-        a = rescue_buf(w, n, w.fat_of[r])[i];
+    if (cnt <= 32) {
+      for (int q2 = 0; q2 < cnt; ++q2) {
+        const int r = w.cr[q2];
+        if (r != Pr)
+          rescue_eliminate(tb, w, n, i, r, w.ca[q2], piv, bP, prow, ps0, ps1, Uc, top, nlive,
+                           lane);
       }
-      unsigned m = __ballot_sync(kFull, qq < nlive && r != Pr && a != 0.0);
-      while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1;
-        rescue_eliminate(tb, w, n, i, __shfl_sync(kFull, r, src), __shfl_sync(kFull, a, src), piv,
-                         bP, prow, ps0, ps1, Ui, top, nlive, lane);
-      }
-    }
-    for (int b0 = e0; b0 < e1; b0 += 32) {
-      const int e = b0 + lane;
-      int r = -1;
-      double a = 0.0;
-      bool cand = false;
-      if (e < e1) {
-        const int2 rs = tb.cent[e];
-        r = rs.x;
-        if (r != Pr && w.pos_of[r] >= i && w.fat_of[r] < 0) {
-          a = w.vs[rs.y];
-          cand = a != 0.0;
+    } else {
+      // rows in buffers first (the list only grows below), then rows in slots
+      for (int q0 = 0; q0 < nlive; q0 += 32) {
+        const int qq = q0 + lane;
+        int r = -1;
+        double a = 0.0;
+        if (qq < nlive) {
+          r = w.live[qq];
+          a = rescue_buf(w, n, w.fat_of[r])[i];
+        }
+        unsigned m = __ballot_sync(kFull, qq < nlive && r != Pr && a != 0.0);
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          rescue_eliminate(tb, w, n, i, __shfl_sync(kFull, r, src), __shfl_sync(kFull, a, src),
+                           piv, bP, prow, ps0, ps1, Uc, top, nlive, lane);
         }
       }
-      unsigned m = __ballot_sync(kFull, cand);
-      while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1;
-        rescue_eliminate(tb, w, n, i, __shfl_sync(kFull, r, src), __shfl_sync(kFull, a, src), piv,
-                         bP, prow, ps0, ps1, Ui, top, nlive, lane);
+      for (int b0 = e0; b0 < e1; b0 += 32) {
+        const int e = b0 + lane;
+        int r = -1;
+        double a = 0.0;
+        bool cand = false;
+        if (e < e1) {
+          const int2 rs = tb.cent[e];
+          r = rs.x;
+          if (r != Pr && w.pos_of[r] >= i && w.fat_of[r] < 0) {
+            a = w.vs[rs.y];
+            cand = a != 0.0;
+          }
+        }
+        unsigned m = __ballot_sync(kFull, cand);
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          rescue_eliminate(tb, w, n, i, __shfl_sync(kFull, r, src), __shfl_sync(kFull, a, src),
+                           piv, bP, prow, ps0, ps1, Uc, top, nlive, lane);
+        }
       }
     }
     if (fP >= 0) {  // the pivot row's buffer is free again
@@ -1409,11 +1598,9 @@ __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp&
     const int m = j1 - j0;
     const int k = j0 + lane;
     double u[32];
-    {
-      const double* Uk = w.U + (size_t)min(k, n - 1) * n + j0;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) u[t] = (t < m && t >= lane) ? Uk[t] : 0.0;
-    }
+    for (int t = 0; t < 32; ++t)
+      u[t] = (t < m && t >= lane) ? w.U[(size_t)(j0 + t) * n + k] : 0.0;
     double acc = k < j1 ? xs[k] : 0.0;
 #pragma unroll
     for (int t = 31; t >= 0; --t) {
@@ -1426,15 +1613,17 @@ __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp&
     if (k < j1) xs[k] = acc;
     __syncwarp();
     // rows above the block: their 32 updates in descending column order
-    for (int r = lane; r < j0; r += 32) {
-      const double* Ur = w.U + (size_t)r * n + j0;
-      double v[32];
+    for (int r0 = 0; r0 < j0; r0 += 32) {
+      const int r = r0 + lane;
+      if (r < j0) {
+        double v[32];
 #pragma unroll
-      for (int t = 0; t < 32; ++t) v[t] = Ur[t];
-      double a2 = xs[r];
+        for (int t = 0; t < 32; ++t) v[t] = w.U[(size_t)(j0 + t) * n + r];
+        double a2 = xs[r];
 #pragma unroll
-      for (int t = 31; t >= 0; --t) a2 = fma(-v[t], xs[j0 + t], a2);
-      xs[r] = a2;
+        for (int t = 31; t >= 0; --t) a2 = fma(-v[t], xs[j0 + t], a2);
+        xs[r] = a2;
+      }
     }
     __syncwarp();
   }
@@ -1451,7 +1640,7 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
   const int n = Tp.n, nv = Tp.nv;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
   const int total = *I.rescue_count;
-  if (blockIdx.x * W >= total) return;
+  if ((int)blockIdx.x >= total) return;  // item e runs on CTA e % grid: one solve per SM first
   unsigned char* base = reinterpret_cast<unsigned char*>(rs);
   int4* rec = nullptr;
   if (Tp.lu_rec) {
@@ -1487,17 +1676,19 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
   w.vs = reinterpret_cast<double*>(base);
   w.bp = w.vs + nv;
   w.fb = w.bp + n;
-  w.pos_of = reinterpret_cast<int*>(w.fb + (size_t)K * n);
+  w.ca = w.fb + (size_t)K * n;
+  w.pos_of = reinterpret_cast<int*>(w.ca + 32);
   w.row_at = w.pos_of + n;
   w.fat_of = w.row_at + n;
   w.live = w.fat_of + n;
   w.stk = w.live + n;
+  w.cr = w.stk + n;
   w.K = K;
   w.U = I.rescue_ws + (size_t)slot * 2 * n * n;
   w.G = w.U + (size_t)n * n;
   const size_t ld = I.ld;
   const TJ* J = reinterpret_cast<const TJ*>(I.J);
-  for (int e = slot; e < total; e += gridDim.x * W) {
+  for (int e = warp * gridDim.x + blockIdx.x; e < total; e += gridDim.x * W) {
     const RescueItem item = I.rescue_list[e];
     const int g = item.inst;
     const double gmin = item.gmin;

@@ -179,6 +179,7 @@ struct JobParams {
   double t0;  // time of step 0 (transient jobs continue from t0)
   int method;
   int seeded, seed_max_iter;
+  int seed_bcast;    // 1: one seed for every instance, in lane 0 of DevInst::seed
   int max_halvings;  // transient restarts with a halved step (reference: 3)
   double growth32, growth64;  // static-pivot multiplier limits (FP32 / FP64 solves)
 };
