@@ -27,6 +27,7 @@ scaling, no collective on the data path); timings are reduced with MAX.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -201,6 +202,21 @@ def workload(n_inst, first):
     return nl, inst
 
 
+@contextlib.contextmanager
+def native_stdout_to_stderr():
+    """The reference library prints start-up notes on the C stdout; send them to
+    stderr so stdout carries only the bench line."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def cpu_sample_run(nl, inst, count, threads):
     """Reference CPU implementation (oracle/_ref when built, else the restatement)
     on `count` instances with `threads` host threads; returns (seconds, solves, kind)."""
@@ -208,11 +224,12 @@ def cpu_sample_run(nl, inst, count, threads):
     kind = "reference" if pyoracle.available("ref") else "port"
     if kind == "port":
         pyoracle.build("port")
-    orc = pyoracle.Oracle("ref" if kind == "reference" else "port")
-    t0 = time.perf_counter()
-    _, st = orc.run_batch(nl, inst, 0, count, dt=DT, n_steps=TRAN_STEPS, n_threads=threads,
-                          linear_solver=pyoracle.LS_SPARSE, max_halvings=MAX_HALVINGS, **POLISH)
-    el = time.perf_counter() - t0
+    with native_stdout_to_stderr():
+        orc = pyoracle.Oracle("ref" if kind == "reference" else "port")
+        t0 = time.perf_counter()
+        _, st = orc.run_batch(nl, inst, 0, count, dt=DT, n_steps=TRAN_STEPS, n_threads=threads,
+                              linear_solver=pyoracle.LS_SPARSE, max_halvings=MAX_HALVINGS, **POLISH)
+        el = time.perf_counter() - t0
     solves = sum(TRAN_STEPS + 1 for s in st if s["converged"])
     return el, solves, kind
 
@@ -490,15 +507,17 @@ def accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64, sample=6):
     kind = "ref" if pyoracle.available("ref") else "port"
     if kind == "port":
         pyoracle.build("port")
-    orc = pyoracle.Oracle(kind)
     idx = [i for i, s in enumerate(st_mixed) if s["status"] == A.ST_CONVERGED][:sample]
     sub = inst.slice(min(idx), max(idx) + 1) if idx else None
     worst = 0.0
     worst_rel = 0.0
     if idx:
-        v_ref, st = orc.run_batch(nl, sub, 0, sub.n, dt=DT, n_steps=TRAN_STEPS,
-                                  n_threads=os.cpu_count() or 1, linear_solver=pyoracle.LS_SPARSE,
-                                  max_halvings=MAX_HALVINGS, polish_max=8)
+        with native_stdout_to_stderr():
+            orc = pyoracle.Oracle(kind)
+            v_ref, st = orc.run_batch(nl, sub, 0, sub.n, dt=DT, n_steps=TRAN_STEPS,
+                                      n_threads=os.cpu_count() or 1,
+                                      linear_solver=pyoracle.LS_SPARSE,
+                                      max_halvings=MAX_HALVINGS, polish_max=8)
         for i in idx:
             r = v_ref[i - min(idx)]
             d = np.abs(v_mixed[i] - r)

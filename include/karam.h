@@ -295,6 +295,12 @@ KARAM_API int karam_get_device_order(const karam_problem *p, int32_t *mos_order,
  * only *data_len is written. */
 KARAM_API int karam_get_lu_program(const karam_problem *p, int32_t *hdr, int32_t *data,
                                    int32_t *data_len, int32_t *slot_rc);
+/* The same program packed as the device's pivot records, for programs whose
+ * pivots all have nL <= 1 and nU <= 2 (else KARAM_E_UNSUPPORTED): rec[8 n] =
+ * (meta, diagonal slot, L slot, L row, U slot 0, U slot 1, target 0, target 1)
+ * with meta = nL | nU << 4 | chain << 8 | back-forwarding << 9;
+ * rec2[2 n] = (U column 0, U column 1). No counterpart in the reference. */
+KARAM_API int karam_get_lu_records(const karam_problem *p, int32_t *rec, int32_t *rec2);
 
 /* ---- single-kernel access for measurement and parity ----------------------
  * Runs the evaluation + stamping kernel once for every instance at the given

@@ -71,6 +71,7 @@ def lib():
         "karam_get_device_order": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
         "karam_get_lu_program": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(C.c_int32),
                                            P(C.c_int32)]),
+        "karam_get_lu_records": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
         "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
                                        P(C.c_double)]),
         "karam_last_timing": (C.c_int, [vp, P(A.KaramTiming)]),
@@ -205,6 +206,18 @@ class Problem:
                                                A.ptr(data, C.c_int32), C.byref(ln),
                                                A.ptr(rc, C.c_int32)))
         return hdr.reshape(n, 4), data[: ln.value], rc.reshape(nv, 2)
+
+    def lu_records(self):
+        """(rec[n, 8], rec2[n, 2]) pivot records of the device's packed schedule,
+        or None when some pivot has nL > 1 or nU > 2."""
+        n = self.n
+        rec = np.zeros(8 * n, np.int32)
+        rec2 = np.zeros(2 * n, np.int32)
+        rc = lib().karam_get_lu_records(self.h, A.ptr(rec, C.c_int32), A.ptr(rec2, C.c_int32))
+        if rc == A.KARAM_E_UNSUPPORTED:
+            return None
+        self._check(rc)
+        return rec.reshape(n, 8), rec2.reshape(n, 2)
 
     # -- batches and solves -------------------------------------------------
     def set_instances(self, inst: Instances | None):

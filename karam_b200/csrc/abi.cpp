@@ -974,6 +974,15 @@ int karam_get_lu_program(const karam_problem* p, int32_t* hdr, int32_t* data, in
   return KARAM_OK;
 }
 
+int karam_get_lu_records(const karam_problem* p, int32_t* rec, int32_t* rec2) {
+  if (!p) return KARAM_E_INVALID;
+  const Topology& T = p->topo;
+  if (!T.lu_small) return KARAM_E_UNSUPPORTED;
+  if (rec) std::copy(T.lu_rec.begin(), T.lu_rec.end(), rec);
+  if (rec2) std::copy(T.lu_rec2.begin(), T.lu_rec2.end(), rec2);
+  return KARAM_OK;
+}
+
 int karam_eval_stamp(karam_problem* p, int32_t precision, const double* v, double* jac, double* f) {
   if (!p || !v) return KARAM_E_INVALID;
   return guarded(p->ctx, [&] {

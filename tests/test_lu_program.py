@@ -80,3 +80,95 @@ def test_program_size_matches_info(product):
     assert ops == prob.info["lu_ops"]
     # chain circuits: every pivot is small (the packed-record schedule applies)
     assert hdr[:, 1].max() <= 2 and hdr[:, 2].max() <= 2
+
+
+def run_records(rec, rec2, vals, rhs):
+    """The device's packed-record schedule: a chain pivot takes its L value,
+    second target and L-row right-hand side from the previous pivot's
+    registers instead of memory; the back substitution takes the unknown the
+    previous step solved from a register where the forwarding bit says so."""
+    A = vals.copy()
+    y = rhs.copy()
+    n = len(rec)
+
+    def load(k):
+        meta, d, ls, lr, us0, us1, t0, t1 = (int(v) for v in rec[k])
+        chain, nl, nu = (meta >> 8) & 1, meta & 15, (meta >> 4) & 15
+        return dict(piv=A[d], yk=y[k], u0=A[us0] if nu > 0 else 0.0,
+                    u1=A[us1] if nu > 1 else 0.0, b00=A[t0] if nl and nu else 0.0,
+                    a0=A[ls] if nl and not chain else 0.0, y0=y[lr] if nl and not chain else 0.0,
+                    b01=A[t1] if nl and nu > 1 and not chain else 0.0)
+
+    w00 = w01 = wy0 = 0.0
+    cur = load(0)
+    for k in range(n):
+        meta, d, ls, lr, us0, us1, t0, t1 = (int(v) for v in rec[k])
+        chain, nl, nu = (meta >> 8) & 1, meta & 15, (meta >> 4) & 15
+        a0 = w00 if chain else cur["a0"]
+        y0 = wy0 if chain else cur["y0"]
+        b01 = w01 if chain else cur["b01"]
+        r = 1.0 / cur["piv"]
+        A[d] = r
+        if nl:
+            l = a0 * r
+            wy0 = y0 - l * cur["yk"]
+            y[lr] = wy0
+            if nu > 0:
+                w00 = cur["b00"] - l * cur["u0"]
+                A[t0] = w00
+            if nu > 1:
+                w01 = b01 - l * cur["u1"]
+                A[t1] = w01
+        if k + 1 < n:
+            cur = load(k + 1)
+
+    def bvals(k):
+        meta, d, ls, lr, us0, us1, t0, t1 = (int(v) for v in rec[k])
+        nu, fb = (meta >> 4) & 15, (meta >> 9) & 3
+        c0, c1 = (int(v) for v in rec2[k])
+        return dict(yk=y[k], u0=A[us0] if nu > 0 else 0.0, u1=A[us1] if nu > 1 else 0.0,
+                    x0=y[c0] if nu > 0 and not fb & 1 else 0.0,
+                    x1=y[c1] if nu > 1 and not fb & 2 else 0.0, r=A[d])
+
+    yprev = 0.0
+    for k in range(n - 1, -1, -1):
+        cur = bvals(k)
+        meta = int(rec[k][0])
+        nu, fb = (meta >> 4) & 15, (meta >> 9) & 3
+        sv = cur["yk"]
+        if nu > 0:
+            sv -= cur["u0"] * (yprev if fb & 1 else cur["x0"])
+        if nu > 1:
+            sv -= cur["u1"] * (yprev if fb & 2 else cur["x1"])
+        sv *= cur["r"]
+        y[k] = sv
+        yprev = sv
+    return y
+
+
+@pytest.mark.parametrize("name", list(ALL))
+def test_packed_records_schedule_solves(product, name):
+    nl = ALL[name]()
+    prob = product.Problem(None, nl)
+    recs = prob.lu_records()
+    if recs is None:
+        pytest.skip("program has pivots beyond the packed-record shape")
+    rec, rec2 = recs
+    hdr, _, rc = prob.lu_program()
+    n, nv = prob.n, prob.info["n_slots"]
+    assert (rec[:, 1] == hdr[:, 3]).all()
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        vals = rng.uniform(-1.0, 1.0, nv)
+        dense = np.zeros((n, n))
+        dense[rc[:, 0], rc[:, 1]] = vals
+        for k in range(n):
+            s = hdr[k, 3]
+            vals[s] = np.sign(vals[s] or 1.0) * (1.0 + np.abs(dense[k]).sum() + np.abs(dense[:, k]).sum())
+        dense[rc[:, 0], rc[:, 1]] = vals
+        rhs = rng.uniform(-1.0, 1.0, n)
+        x = run_records(rec, rec2, vals, rhs)
+        assert np.allclose(x, np.linalg.solve(dense, rhs), rtol=1e-10, atol=1e-12)
+    if name == "config2":
+        # nearly every pivot of the chain circuit keeps the recurrence in registers
+        assert int(((rec[:, 0] >> 8) & 1).sum()) >= n // 2
