@@ -72,6 +72,7 @@ extern "C" {
                                one, seed every instance when the mean per-node
                                confidence 1 / (1 + variance) is at least 0.3       */
 #define KARAM_SEED_HISTORY 8
+#define KARAM_SEED_MLP 3    /* the learned seeder attached by karam_problem_set_seeder */
 
 #define KARAM_SRC_DC 0
 #define KARAM_SRC_PULSE 1  /* PULSE(v1 v2 td tr tf pw per), physics/circuitsim.h:2155-2170 */
@@ -170,7 +171,8 @@ typedef struct karam_solver_opts {
                             stepping if it has not converged after seed_max_iter
                             iterations. KARAM_SEED_CALLER needs karam_solve_dc's
                             seed_v; KARAM_SEED_EMA applies to batches of more than
-                            KARAM_SEED_HISTORY instances (smaller ones run plain) */
+                            KARAM_SEED_HISTORY instances (smaller ones run plain);
+                            KARAM_SEED_MLP needs an attached, trained seeder     */
   int32_t seed_max_iter; /* K of the seeded fallback                              */
   int32_t schedule;      /* instances per CTA of the factor/solve kernel (1, 2, 4, ..., 32);
                             0 = chosen from shared memory, occupancy and batch size */
@@ -301,6 +303,44 @@ KARAM_API int karam_get_lu_program(const karam_problem *p, int32_t *hdr, int32_t
  * with meta = nL | nU << 4 | chain << 8 | back-forwarding << 9;
  * rec2[2 n] = (U column 0, U column 1). No counterpart in the reference. */
 KARAM_API int karam_get_lu_records(const karam_problem *p, int32_t *rec, int32_t *rec2);
+
+/* ---- learned seeder ---------------------------------------------------------
+ * The role of solvers/neural_seeder.h, whose learned model is future work in
+ * the reference. A multilayer perceptron (hidden layers of `width` GELU units,
+ * one linear output layer) maps an instance's device parameters (VTO and KP
+ * of every MOSFET) and source DC values to an initial guess of its node
+ * voltages. It is trained, on the problem's device, on DC solutions that
+ * plain NR produced for the instances of a problem, and serves
+ * opts->seeded = KARAM_SEED_MLP solves of problems with the same topology.
+ * The GEMMs use BF16 weights and activations with FP32 accumulation; master
+ * weights and Adam moments are FP32. Plain NR stays the judge: a seeded
+ * instance that has not converged after seed_max_iter iterations falls back
+ * to full GMIN stepping. No counterpart in the reference. */
+typedef struct karam_seeder karam_seeder;
+KARAM_API int karam_seeder_create(karam_problem *p, int32_t width, int32_t hidden_layers,
+                                  uint64_t init_seed, karam_seeder **out);
+KARAM_API void karam_seeder_destroy(karam_seeder *s);
+/* Adds the DC solutions of the problem's converged instances as training
+ * samples; the problem's last solve must be a DC one (karam_solve_dc, or
+ * karam_run_mc_device with n_steps = 0). *added = samples added. */
+KARAM_API int karam_seeder_add_dc(karam_seeder *s, karam_problem *p, int32_t *added);
+/* Adam on the mean squared error of the normalised voltages (feature and
+ * voltage normalisations taken from the samples at the first call).
+ * *final_loss = mean loss of the last epoch. */
+KARAM_API int karam_seeder_train(karam_seeder *s, int32_t epochs, int32_t batch, float lr,
+                                 uint64_t shuffle_seed, float *final_loss);
+/* Attaches s (NULL detaches) for KARAM_SEED_MLP solves of p; p must have the
+ * topology sizes the seeder was created for, and s must outlive that use. */
+KARAM_API int karam_problem_set_seeder(karam_problem *p, karam_seeder *s);
+/* The seeder's guesses for p's current instances: out_v[n_instances][n],
+ * node order (index 0 = node 1). */
+KARAM_API int karam_seeder_predict(karam_seeder *s, karam_problem *p, double *out_v);
+/* The seeder's GEMM on host buffers, for tests: C[M][N] = op(A) op(B) with
+ * op(A)[m][k] = transA ? A[k * lda + m] : A[m * lda + k] (B likewise),
+ * operands rounded to BF16, FP32 accumulation, on the current device. */
+KARAM_API int karam_seeder_gemm(int32_t M, int32_t N, int32_t K, const float *A, int32_t lda,
+                                int32_t transA, const float *B, int32_t ldb, int32_t transB,
+                                float *C);
 
 /* ---- single-kernel access for measurement and parity ----------------------
  * Runs the evaluation + stamping kernel once for every instance at the given

@@ -72,6 +72,16 @@ def lib():
         "karam_get_lu_program": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(C.c_int32),
                                            P(C.c_int32)]),
         "karam_get_lu_records": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+        "karam_seeder_create": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_uint64, P(vp)]),
+        "karam_seeder_destroy": (None, [vp]),
+        "karam_seeder_add_dc": (C.c_int, [vp, vp, P(C.c_int32)]),
+        "karam_seeder_train": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_float, C.c_uint64,
+                                         P(C.c_float)]),
+        "karam_problem_set_seeder": (C.c_int, [vp, vp]),
+        "karam_seeder_predict": (C.c_int, [vp, vp, P(C.c_double)]),
+        "karam_seeder_gemm": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, P(C.c_float), C.c_int32,
+                                        C.c_int32, P(C.c_float), C.c_int32, C.c_int32,
+                                        P(C.c_float)]),
         "karam_eval_stamp": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
                                        P(C.c_double)]),
         "karam_last_timing": (C.c_int, [vp, P(A.KaramTiming)]),
@@ -282,8 +292,76 @@ class Problem:
                                            A.ptr(jac, C.c_double), A.ptr(f, C.c_double)))
         return jac, f
 
+    def set_seeder(self, seeder):
+        """Attach (or with None detach) the learned seeder used by
+        options(seeded=SEED_MLP)."""
+        self._check(lib().karam_problem_set_seeder(self.h, seeder.h if seeder else None))
+        self._seeder = seeder
+
     def timing(self):
         """Device accounting of the last solve call (karam_timing as a dict)."""
         t = A.KaramTiming()
         self._check(lib().karam_last_timing(self.h, C.byref(t)))
         return {k: getattr(t, k) for k, _ in A.KaramTiming._fields_}
+
+
+class Seeder:
+    """Learned NR seeder (karam_seeder): a BF16 MLP trained on a problem's
+    plain-NR DC solutions; used by solves with options(seeded=SEED_MLP) once
+    attached with Problem.set_seeder."""
+
+    def __init__(self, prob: Problem, width=512, hidden_layers=3, init_seed=1):
+        self.ctx = prob.ctx
+        h = C.c_void_p()
+        rc = lib().karam_seeder_create(prob.h, width, hidden_layers, init_seed, C.byref(h))
+        if rc != A.KARAM_OK:
+            raise KaramError(rc, lib().karam_last_error(self.ctx.h).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != A.KARAM_OK:
+            raise KaramError(rc, lib().karam_last_error(self.ctx.h).decode())
+
+    def add_dc(self, prob: Problem) -> int:
+        """Add the converged DC solutions of prob's last (DC) solve; returns the count."""
+        n = C.c_int32(0)
+        self._check(lib().karam_seeder_add_dc(self.h, prob.h, C.byref(n)))
+        return n.value
+
+    def train(self, epochs=40, batch=256, lr=1e-3, shuffle_seed=0) -> float:
+        loss = C.c_float(0.0)
+        self._check(lib().karam_seeder_train(self.h, epochs, batch, lr, shuffle_seed,
+                                             C.byref(loss)))
+        return loss.value
+
+    def predict(self, prob: Problem) -> np.ndarray:
+        out = np.zeros((prob.ni, prob.n))
+        self._check(lib().karam_seeder_predict(self.h, prob.h, A.ptr(out, C.c_double)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().karam_seeder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bf16_gemm(a: np.ndarray, b: np.ndarray, trans_a=False, trans_b=False) -> np.ndarray:
+    """The seeder's tensor-core GEMM on host arrays: op(a) @ op(b) with BF16
+    operands and FP32 accumulation (op = transpose when the flag is set)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    M, K = (a.shape[1], a.shape[0]) if trans_a else a.shape
+    K2, N = (b.shape[1], b.shape[0]) if trans_b else b.shape
+    assert K == K2
+    c = np.zeros((M, N), np.float32)
+    rc = lib().karam_seeder_gemm(M, N, K, A.ptr(a, C.c_float), a.shape[1], int(trans_a),
+                                 A.ptr(b, C.c_float), b.shape[1], int(trans_b), A.ptr(c, C.c_float))
+    if rc != A.KARAM_OK:
+        raise KaramError(rc, lib().karam_last_error(None).decode())
+    return c

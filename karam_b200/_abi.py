@@ -22,6 +22,7 @@ SEED_NONE = 0
 SEED_CALLER = 1
 SEED_EMA = 2
 SEED_HISTORY = 8
+SEED_MLP = 3
 SRC_DC = 0
 SRC_PULSE = 1
 MODEL_NMOS = 0

@@ -14,6 +14,7 @@
 #include "../../include/karam.h"
 #include "device.hpp"
 #include "noalloc.hpp"
+#include "seeder.hpp"
 #include "topology.hpp"
 
 using namespace karam;
@@ -95,6 +96,8 @@ struct karam_problem {
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
+  karam_seeder* seeder = nullptr;  // KARAM_SEED_MLP (not owned)
+  DBuf i_feat;                     // [ni][n_features] FP32 seeder inputs
   int* h_active = nullptr;  // pinned
 
   // accounting of the last solve call
@@ -106,6 +109,15 @@ struct karam_problem {
     if (h_active) cudaFreeHost(h_active);
     if (ev_job0) cudaEventDestroy(ev_job0);
     if (ev_job1) cudaEventDestroy(ev_job1);
+  }
+};
+
+struct karam_seeder {
+  karam_ctx* ctx = nullptr;
+  karam::Mlp* m = nullptr;
+  int n = 0, n_mos = 0, n_vs = 0, nv = 0;
+  ~karam_seeder() {
+    if (m) karam::mlp_destroy(m);
   }
 };
 
@@ -471,7 +483,7 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
   P.seeded = o->seeded;
   P.seed_max_iter = o->seed_max_iter;
   P.seed_bcast = 0;
-  if (P.seeded < KARAM_SEED_NONE || P.seeded > KARAM_SEED_EMA)
+  if (P.seeded < KARAM_SEED_NONE || P.seeded > KARAM_SEED_MLP)
     throw std::runtime_error("unknown seeded mode");
   P.max_halvings = o->max_halvings;
   P.growth32 = o->lu_growth_limit > 0 ? o->lu_growth_limit : (o->lu_growth_limit < 0 ? 1e300 : 1e4);
@@ -630,10 +642,30 @@ void end_job(karam_problem* p) {
   p->timing.rescues_dense = (int64_t)c[4];
 }
 
+int seeder_features_count(const Topology& T) { return 2 * (int)T.mos.size() + (int)T.vs.size(); }
+
+// KARAM_SEED_MLP: the attached seeder's guess for every instance, written
+// instance-interleaved (permuted order) into i_seed.
+void mlp_seed(karam_problem* p) {
+  karam_seeder* sd = p->seeder;
+  if (!sd) throw std::logic_error("KARAM_SEED_MLP without an attached seeder");
+  if (karam::mlp_samples(sd->m) == 0) throw std::logic_error("the attached seeder is not trained");
+  const int nf = seeder_features_count(p->topo);
+  const size_t bytes = (size_t)std::max(1, p->ni) * nf * sizeof(float);
+  if (p->i_feat.bytes < bytes) p->i_feat.alloc(bytes);
+  cudaStream_t s = p->ctx->stream;
+  karam::seeder_features(p->dt, dev_inst(p), nullptr, p->ni, p->i_feat.as<float>(), nullptr, s);
+  karam::mlp_predict(sd->m, p->i_feat.as<float>(), p->ni, p->i_seed.as<double>(), p->ld, s);
+  p->timing.other_launches += 1;
+}
+
 void start_job(karam_problem* p, const JobParams& P, const double* seed_v) {
   DevInst I = dev_inst(p);
   if (P.seeded == KARAM_SEED_EMA) {
     I.seed = p->i_seed.as<double>();  // written by ema_seed
+  } else if (P.seeded == KARAM_SEED_MLP) {
+    mlp_seed(p);
+    I.seed = p->i_seed.as<double>();
   } else if (P.seeded && seed_v) {
     // caller guesses arrive instance-major in node order; the device works
     // instance-interleaved in permuted order
@@ -1072,6 +1104,134 @@ int karam_eval_stamp_noalloc(karam_problem* p, int32_t precision, const double* 
                           p->csr_to_slot.data(), T.nnz(), d_jac, d_f, s),
        "karam_eval_stamp_noalloc launch");
     ck(cudaStreamSynchronize(s), "karam_eval_stamp_noalloc sync");
+    return KARAM_OK;
+  });
+}
+
+int karam_seeder_create(karam_problem* p, int32_t width, int32_t hidden_layers,
+                        uint64_t init_seed, karam_seeder** out) {
+  if (!p || !out) return KARAM_E_INVALID;
+  *out = nullptr;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    if (width < 1 || width > 8192 || hidden_layers < 0 || hidden_layers > 16)
+      throw std::runtime_error("seeder: width must be in 1..8192 and hidden_layers in 0..16");
+    const Topology& T = p->topo;
+    auto sd = std::make_unique<karam_seeder>();
+    sd->ctx = p->ctx;
+    sd->n = T.n;
+    sd->nv = T.nv;
+    sd->n_mos = (int)T.mos.size();
+    sd->n_vs = (int)T.vs.size();
+    sd->m = karam::mlp_create(seeder_features_count(T), T.n, width, hidden_layers, init_seed,
+                              p->ctx->stream);
+    *out = sd.release();
+    return KARAM_OK;
+  });
+}
+
+void karam_seeder_destroy(karam_seeder* s) { delete s; }
+
+namespace {
+void seeder_matches(const karam_seeder* s, const karam_problem* p) {
+  const Topology& T = p->topo;
+  if (s->ctx != p->ctx || s->n != T.n || s->nv != T.nv || s->n_mos != (int)T.mos.size() ||
+      s->n_vs != (int)T.vs.size())
+    throw std::runtime_error("seeder and problem differ in context or topology sizes");
+}
+}  // namespace
+
+int karam_seeder_add_dc(karam_seeder* s, karam_problem* p, int32_t* added) {
+  if (!s || !p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    seeder_matches(s, p);
+    if (!p->have_dc || p->tran_started)
+      throw std::logic_error("karam_seeder_add_dc needs a DC solve as the problem's last solve");
+    std::vector<InstState> st(p->ni);
+    ck(cudaMemcpy(st.data(), p->i_st.p, st.size() * sizeof(InstState), cudaMemcpyDeviceToHost),
+       "D2H state");
+    std::vector<int> idx;
+    for (int g = 0; g < p->ni; ++g)
+      if (st[g].status == KST_CONVERGED) idx.push_back(g);
+    if (added) *added = (int32_t)idx.size();
+    if (idx.empty()) return KARAM_OK;
+    const int nf = seeder_features_count(p->topo), rows = (int)idx.size();
+    DBuf d_idx, X, Y;
+    d_idx.alloc(idx.size() * sizeof(int));
+    X.alloc((size_t)rows * nf * sizeof(float));
+    Y.alloc((size_t)rows * p->topo.n * sizeof(float));
+    cudaStream_t cs = p->ctx->stream;
+    ck(cudaMemcpyAsync(d_idx.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, cs),
+       "H2D index");
+    karam::seeder_features(p->dt, dev_inst(p), d_idx.as<int>(), rows, X.as<float>(), Y.as<float>(),
+                           cs);
+    karam::mlp_add_samples(s->m, X.as<float>(), Y.as<float>(), rows, cs);
+    ck(cudaStreamSynchronize(cs), "seeder sync");
+    return KARAM_OK;
+  });
+}
+
+int karam_seeder_train(karam_seeder* s, int32_t epochs, int32_t batch, float lr,
+                       uint64_t shuffle_seed, float* final_loss) {
+  if (!s) return KARAM_E_INVALID;
+  return guarded(s->ctx, [&] {
+    ck(cudaSetDevice(s->ctx->device), "cudaSetDevice");
+    const float l = karam::mlp_train(s->m, epochs, batch, lr, shuffle_seed, s->ctx->stream);
+    if (final_loss) *final_loss = l;
+    return KARAM_OK;
+  });
+}
+
+int karam_problem_set_seeder(karam_problem* p, karam_seeder* s) {
+  if (!p) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    if (s) seeder_matches(s, p);
+    p->seeder = s;
+    return KARAM_OK;
+  });
+}
+
+int karam_seeder_predict(karam_seeder* s, karam_problem* p, double* out_v) {
+  if (!s || !p || !out_v) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    seeder_matches(s, p);
+    karam_seeder* keep = p->seeder;
+    p->seeder = s;
+    try {
+      mlp_seed(p);
+    } catch (...) {
+      p->seeder = keep;
+      throw;
+    }
+    p->seeder = keep;
+    const int n = p->topo.n;
+    unpermute(p->i_seed.as<double>(), p->t_perm.as<int>(), p->i_out.as<double>(), p->ni, p->ld,
+              n, p->ctx->stream);
+    ck(cudaMemcpyAsync(out_v, p->i_out.p, (size_t)p->ni * n * sizeof(double),
+                       cudaMemcpyDeviceToHost, p->ctx->stream),
+       "D2H seeds");
+    ck(cudaStreamSynchronize(p->ctx->stream), "seeder sync");
+    return KARAM_OK;
+  });
+}
+
+int karam_seeder_gemm(int32_t M, int32_t N, int32_t K, const float* A, int32_t lda,
+                      int32_t transA, const float* B, int32_t ldb, int32_t transB, float* C) {
+  if (!A || !B || !C || M < 1 || N < 1 || K < 1) return KARAM_E_INVALID;
+  return guarded(nullptr, [&] {
+    const size_t na = transA ? (size_t)K * lda : (size_t)M * lda;
+    const size_t nb = transB ? (size_t)N * ldb : (size_t)K * ldb;
+    DBuf dA, dB, dC;
+    dA.alloc(na * sizeof(float));
+    dB.alloc(nb * sizeof(float));
+    dC.alloc((size_t)M * N * sizeof(float));
+    ck(cudaMemcpy(dA.p, A, na * sizeof(float), cudaMemcpyHostToDevice), "H2D A");
+    ck(cudaMemcpy(dB.p, B, nb * sizeof(float), cudaMemcpyHostToDevice), "H2D B");
+    karam::mlp_gemm(M, N, K, dA.as<float>(), lda, transA, dB.as<float>(), ldb, transB,
+                    dC.as<float>(), N, 0, nullptr);
+    ck(cudaMemcpy(C, dC.p, (size_t)M * N * sizeof(float), cudaMemcpyDeviceToHost), "D2H C");
     return KARAM_OK;
   });
 }

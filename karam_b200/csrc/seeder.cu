@@ -1,0 +1,506 @@
+// seeder.cu -- training and inference kernels of the learned NR seeder (see
+// seeder.hpp). The GEMMs run on the tensor cores through WMMA with BF16
+// operands and FP32 accumulation; the network is small (config 2: 1026 -> 512
+// -> 512 -> 512 -> 322, 1.2 M weights), so a batch of 4096 instances costs a
+// few GFLOP and the kernels are written for clarity: 64 x 64 output tiles,
+// one warp per 32 x 32 quarter, K staged 32 at a time through shared memory
+// with the conversion to BF16 (and any transposition) done while staging.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <mma.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nr_types.h"
+#include "seeder.hpp"
+
+namespace karam {
+
+namespace {
+
+using namespace nvcuda;
+
+constexpr int kTM = 64, kTN = 64, kTK = 32;
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// C[M][N] (+)= op(A)[M][K] op(B)[K][N]; 128 threads, a 64 x 64 tile per CTA.
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const float* __restrict__ A,
+                                              int lda, int tA, const float* __restrict__ B,
+                                              int ldb, int tB, float* __restrict__ C, int ldc,
+                                              int acc) {
+  __shared__ __align__(32) __nv_bfloat16 As[kTM][kTK + 8];
+  __shared__ __align__(32) __nv_bfloat16 Bs[kTK][kTN + 8];
+  __shared__ __align__(32) float Cs[kTM][kTN + 4];
+  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
+  const int warp = threadIdx.x >> 5;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> c[2][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) wmma::fill_fragment(c[i][j], 0.0f);
+  for (int k0 = 0; k0 < K; k0 += kTK) {
+    // stage op(A) and op(B) with the contiguous index running across threads
+    for (int e = threadIdx.x; e < kTM * kTK; e += blockDim.x) {
+      int r, kk;
+      if (tA) {
+        kk = e / kTM;
+        r = e - kk * kTM;
+      } else {
+        r = e / kTK;
+        kk = e - r * kTK;
+      }
+      const int m = m0 + r, k = k0 + kk;
+      float v = 0.0f;
+      if (m < M && k < K) v = tA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
+      As[r][kk] = __float2bfloat16_rn(v);
+    }
+    for (int e = threadIdx.x; e < kTK * kTN; e += blockDim.x) {
+      int kk, cc;
+      if (tB) {
+        cc = e / kTK;
+        kk = e - cc * kTK;
+      } else {
+        kk = e / kTN;
+        cc = e - kk * kTN;
+      }
+      const int k = k0 + kk, n = n0 + cc;
+      float v = 0.0f;
+      if (k < K && n < N) v = tB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n];
+      Bs[kk][cc] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kTK; kk += 16) {
+      wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a[2];
+      wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) wmma::load_matrix_sync(a[i], &As[wm + 16 * i][kk], kTK + 8);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) wmma::load_matrix_sync(b[j], &Bs[kk][wn + 16 * j], kTN + 8);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) wmma::mma_sync(c[i][j], a[i], b[j], c[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      wmma::store_matrix_sync(&Cs[wm + 16 * i][wn + 16 * j], c[i][j], kTN + 4, wmma::mem_row_major);
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTM * kTN; e += blockDim.x) {
+    const int r = e / kTN, cc = e - r * kTN;
+    const int m = m0 + r, n = n0 + cc;
+    if (m < M && n < N) {
+      float* p = C + (size_t)m * ldc + n;
+      *p = acc ? *p + Cs[r][cc] : Cs[r][cc];
+    }
+  }
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678f)) + z * 0.39894228f * expf(-0.5f * z * z);
+}
+
+// Z += b (kept for the backward pass); H = gelu(Z) unless H is null.
+__global__ void k_bias_act(float* Z, const float* b, float* H, int rows, int cols) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const float z = Z[e] + b[e % cols];
+    Z[e] = z;
+    if (H) H[e] = gelu(z);
+  }
+}
+
+__global__ void k_gelu_bwd(float* dH, const float* Z, int rows, int cols) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x)
+    dH[e] *= gelu_d(Z[e]);
+}
+
+// dY = 2 (Y - T) / (rows cols); loss += mean squared error.
+__global__ void k_mse(const float* Y, const float* T, float* dY, int rows, int cols, float* loss) {
+  const size_t n = (size_t)rows * cols;
+  const float s = 1.0f / (float)n;
+  float part = 0.0f;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const float d = Y[e] - T[e];
+    dY[e] = 2.0f * s * d;
+    part += d * d * s;
+  }
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, part);
+}
+
+__global__ void k_colsum(const float* G, int rows, int cols, float* out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; ++r) s += G[(size_t)r * cols + c];
+  out[c] = s;
+}
+
+__global__ void k_adam(float* w, const float* g, float* m, float* v, int n, float lr, float c1,
+                       float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = 0.9f * m[i] + 0.1f * gi;
+  const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + 1e-8f);
+}
+
+// out[r][j] = (src[row(r)][j] - mean[j]) * istd[j], row(r) = idx ? idx[r] : r.
+__global__ void k_norm_rows(const float* src, const int* idx, int rows, int cols,
+                            const float* mean, const float* istd, float* out) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / cols), j = (int)(e - (size_t)r * cols);
+    const int sr = idx ? idx[r] : r;
+    out[e] = (src[(size_t)sr * cols + j] - mean[j]) * istd[j];
+  }
+}
+
+// Column mean and 1 / standard deviation (0 for a constant column).
+__global__ void k_col_stats(const float* X, int rows, int cols, float* mean, float* istd,
+                            float* sd) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  double s = 0.0;
+  for (int r = 0; r < rows; ++r) s += X[(size_t)r * cols + c];
+  const double mu = s / rows;
+  double q = 0.0;
+  for (int r = 0; r < rows; ++r) {
+    const double d = X[(size_t)r * cols + c] - mu;
+    q += d * d;
+  }
+  const double sdv = sqrt(q / rows);
+  mean[c] = (float)mu;
+  istd[c] = sdv > 0.0 ? (float)(1.0 / sdv) : 0.0f;
+  if (sd) sd[c] = (float)sdv;
+}
+
+__global__ void k_denorm(const float* Y, int rows, int cols, const float* mean, const float* sd,
+                         double* out, int out_ld) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / cols), i = (int)(e - (size_t)r * cols);
+    const double v = (double)Y[e] * sd[i] + mean[i];
+    if (out_ld > 0)
+      out[(size_t)i * out_ld + r] = v;
+    else
+      out[e] = v;
+  }
+}
+
+// Uniform(-a, a) from a counter hash (splitmix64), deterministic per seed.
+__global__ void k_init_uniform(float* w, int n, float a, unsigned long long seed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const float u = (float)((z >> 40) * (1.0 / 16777216.0));  // [0, 1)
+  w[i] = (2.0f * u - 1.0f) * a;
+}
+
+int grid_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 4096); }
+
+struct Buf {
+  float* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = count;
+    if (count) ck(cudaMalloc(&p, count * sizeof(float)), "seeder alloc");
+  }
+  ~Buf() {
+    if (p) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+struct Mlp {
+  std::vector<int> dims;  // n_in, width x hidden, n_out
+  int L = 0;              // weight layers
+  std::vector<Buf> W, b, gW, gb, mW, vW, mb, vb;
+  Buf Xs, Ys;  // training samples (raw)
+  int ns = 0;
+  Buf fmean, fistd, tmean, tistd, tsd;
+  bool normed = false;
+  int bcap = 0;
+  std::vector<Buf> act, pre;  // act[0..L-1] inputs of each layer, pre[1..L] pre-activations
+  Buf g1, g2, tgt, loss;
+  int* idx = nullptr;
+  int idx_cap = 0;
+  long step = 0;
+  ~Mlp() {
+    if (idx) cudaFree(idx);
+  }
+};
+
+namespace {
+
+void ensure_batch(Mlp* m, int B) {
+  if (B <= m->bcap) return;
+  int maxd = *std::max_element(m->dims.begin(), m->dims.end());
+  m->act.resize(m->L);
+  m->pre.resize(m->L + 1);
+  for (int l = 0; l < m->L; ++l) m->act[l].alloc((size_t)B * m->dims[l]);
+  for (int l = 1; l <= m->L; ++l) m->pre[l].alloc((size_t)B * m->dims[l]);
+  m->g1.alloc((size_t)B * maxd);
+  m->g2.alloc((size_t)B * maxd);
+  m->tgt.alloc((size_t)B * m->dims[m->L]);
+  m->bcap = B;
+}
+
+void gemm(int M, int N, int K, const float* A, int lda, int tA, const float* B, int ldb, int tB,
+          float* C, int ldc, int acc, cudaStream_t s) {
+  if (M <= 0 || N <= 0) return;
+  const dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM);
+  k_gemm<<<grid, 128, 0, s>>>(M, N, K, A, lda, tA, B, ldb, tB, C, ldc, acc);
+}
+
+// Forward pass of B rows whose normalised inputs are in act[0]; the output
+// (normalised units) is left in pre[L].
+void forward(Mlp* m, int B, cudaStream_t s) {
+  for (int l = 1; l <= m->L; ++l) {
+    const int K = m->dims[l - 1], N = m->dims[l];
+    gemm(B, N, K, m->act[l - 1].p, K, 0, m->W[l - 1].p, N, 0, m->pre[l].p, N, 0, s);
+    const size_t e = (size_t)B * N;
+    k_bias_act<<<grid_for(e), 256, 0, s>>>(m->pre[l].p, m->b[l - 1].p,
+                                           l < m->L ? m->act[l].p : nullptr, B, N);
+  }
+}
+
+}  // namespace
+
+Mlp* mlp_create(int n_in, int n_out, int width, int hidden, uint64_t seed, cudaStream_t s) {
+  if (n_in < 1 || n_out < 1 || width < 1 || hidden < 0 || hidden > 16)
+    throw std::runtime_error("seeder: bad network sizes");
+  Mlp* m = new Mlp;
+  try {
+    m->dims.push_back(n_in);
+    for (int h = 0; h < hidden; ++h) m->dims.push_back(width);
+    m->dims.push_back(n_out);
+    m->L = (int)m->dims.size() - 1;
+    for (auto* v : {&m->W, &m->b, &m->gW, &m->gb, &m->mW, &m->vW, &m->mb, &m->vb}) v->resize(m->L);
+    for (int l = 0; l < m->L; ++l) {
+      const size_t nw = (size_t)m->dims[l] * m->dims[l + 1], nb = m->dims[l + 1];
+      m->W[l].alloc(nw);
+      m->gW[l].alloc(nw);
+      m->mW[l].alloc(nw);
+      m->vW[l].alloc(nw);
+      m->b[l].alloc(nb);
+      m->gb[l].alloc(nb);
+      m->mb[l].alloc(nb);
+      m->vb[l].alloc(nb);
+      // uniform with variance 1 / fan_in (GELU layers) and zero biases
+      const float a = std::sqrt(3.0f / (float)m->dims[l]);
+      k_init_uniform<<<(int)((nw + 255) / 256), 256, 0, s>>>(m->W[l].p, (int)nw, a,
+                                                              seed + 7919ull * (l + 1));
+      ck(cudaMemsetAsync(m->b[l].p, 0, nb * sizeof(float), s), "seeder init");
+      for (Buf* z : {&m->mW[l], &m->vW[l]}) ck(cudaMemsetAsync(z->p, 0, nw * sizeof(float), s), "seeder init");
+      for (Buf* z : {&m->mb[l], &m->vb[l]}) ck(cudaMemsetAsync(z->p, 0, nb * sizeof(float), s), "seeder init");
+    }
+    m->fmean.alloc(n_in);
+    m->fistd.alloc(n_in);
+    m->tmean.alloc(n_out);
+    m->tistd.alloc(n_out);
+    m->tsd.alloc(n_out);
+    m->loss.alloc(1);
+    ck(cudaGetLastError(), "seeder init launch");
+  } catch (...) {
+    delete m;
+    throw;
+  }
+  return m;
+}
+
+void mlp_destroy(Mlp* m) { delete m; }
+int mlp_n_in(const Mlp* m) { return m->dims.front(); }
+int mlp_n_out(const Mlp* m) { return m->dims.back(); }
+int mlp_samples(const Mlp* m) { return m->ns; }
+
+void mlp_add_samples(Mlp* m, const float* dX, const float* dY, int n, cudaStream_t s) {
+  if (n <= 0) return;
+  const int ni = m->dims.front(), no = m->dims.back();
+  const size_t need = (size_t)(m->ns + n);
+  if (need > m->Xs.n / std::max(1, ni)) {
+    size_t cap = std::max<size_t>(need, 2 * (size_t)m->ns);
+    Buf X2, Y2;
+    X2.alloc(cap * ni);
+    Y2.alloc(cap * no);
+    if (m->ns) {
+      ck(cudaMemcpyAsync(X2.p, m->Xs.p, (size_t)m->ns * ni * sizeof(float), cudaMemcpyDeviceToDevice, s), "seeder copy");
+      ck(cudaMemcpyAsync(Y2.p, m->Ys.p, (size_t)m->ns * no * sizeof(float), cudaMemcpyDeviceToDevice, s), "seeder copy");
+    }
+    ck(cudaStreamSynchronize(s), "seeder sync");
+    std::swap(m->Xs.p, X2.p);
+    std::swap(m->Xs.n, X2.n);
+    std::swap(m->Ys.p, Y2.p);
+    std::swap(m->Ys.n, Y2.n);
+  }
+  ck(cudaMemcpyAsync(m->Xs.p + (size_t)m->ns * ni, dX, (size_t)n * ni * sizeof(float),
+                     cudaMemcpyDeviceToDevice, s), "seeder copy");
+  ck(cudaMemcpyAsync(m->Ys.p + (size_t)m->ns * no, dY, (size_t)n * no * sizeof(float),
+                     cudaMemcpyDeviceToDevice, s), "seeder copy");
+  m->ns += n;
+}
+
+float mlp_train(Mlp* m, int epochs, int batch, float lr, uint64_t shuffle_seed, cudaStream_t s) {
+  if (m->ns < 1) throw std::runtime_error("seeder: no training samples");
+  if (epochs < 1 || batch < 1 || !(lr > 0.0f)) throw std::runtime_error("seeder: bad training options");
+  const int ni = m->dims.front(), no = m->dims.back();
+  if (!m->normed) {
+    k_col_stats<<<(ni + 127) / 128, 128, 0, s>>>(m->Xs.p, m->ns, ni, m->fmean.p, m->fistd.p, nullptr);
+    k_col_stats<<<(no + 127) / 128, 128, 0, s>>>(m->Ys.p, m->ns, no, m->tmean.p, m->tistd.p, m->tsd.p);
+    m->normed = true;
+  }
+  const int B = std::min(batch, m->ns);
+  const int nb = m->ns / B;
+  ensure_batch(m, B);
+  if (m->idx_cap < m->ns) {
+    if (m->idx) cudaFree(m->idx);
+    m->idx = nullptr;
+    ck(cudaMalloc(&m->idx, (size_t)m->ns * sizeof(int)), "seeder alloc");
+    m->idx_cap = m->ns;
+  }
+  std::mt19937_64 rng(shuffle_seed);
+  std::vector<int> perm(m->ns);
+  float last = 0.0f;
+  for (int ep = 0; ep < epochs; ++ep) {
+    std::iota(perm.begin(), perm.end(), 0);
+    std::shuffle(perm.begin(), perm.end(), rng);
+    ck(cudaMemcpyAsync(m->idx, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, s), "seeder idx");
+    ck(cudaMemsetAsync(m->loss.p, 0, sizeof(float), s), "seeder loss");
+    for (int q = 0; q < nb; ++q) {
+      const int* bi = m->idx + (size_t)q * B;
+      k_norm_rows<<<grid_for((size_t)B * ni), 256, 0, s>>>(m->Xs.p, bi, B, ni, m->fmean.p, m->fistd.p, m->act[0].p);
+      k_norm_rows<<<grid_for((size_t)B * no), 256, 0, s>>>(m->Ys.p, bi, B, no, m->tmean.p, m->tistd.p, m->tgt.p);
+      forward(m, B, s);
+      float* gc = m->g1.p;
+      float* gn = m->g2.p;
+      k_mse<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[m->L].p, m->tgt.p, gc, B, no, m->loss.p);
+      for (int l = m->L; l >= 1; --l) {
+        const int K = m->dims[l - 1], N = m->dims[l];
+        gemm(K, N, B, m->act[l - 1].p, K, 1, gc, N, 0, m->gW[l - 1].p, N, 0, s);
+        k_colsum<<<(N + 127) / 128, 128, 0, s>>>(gc, B, N, m->gb[l - 1].p);
+        if (l > 1) {
+          gemm(B, K, N, gc, N, 0, m->W[l - 1].p, N, 1, gn, K, 0, s);
+          k_gelu_bwd<<<grid_for((size_t)B * K), 256, 0, s>>>(gn, m->pre[l - 1].p, B, K);
+          std::swap(gc, gn);
+        }
+      }
+      ++m->step;
+      const float c1 = 1.0f - std::pow(0.9f, (float)m->step);
+      const float c2 = 1.0f - std::pow(0.999f, (float)m->step);
+      for (int l = 0; l < m->L; ++l) {
+        const int nw = m->dims[l] * m->dims[l + 1], nbias = m->dims[l + 1];
+        k_adam<<<(nw + 255) / 256, 256, 0, s>>>(m->W[l].p, m->gW[l].p, m->mW[l].p, m->vW[l].p, nw, lr, c1, c2);
+        k_adam<<<(nbias + 255) / 256, 256, 0, s>>>(m->b[l].p, m->gb[l].p, m->mb[l].p, m->vb[l].p, nbias, lr, c1, c2);
+      }
+    }
+    if (ep == epochs - 1) {
+      ck(cudaMemcpyAsync(&last, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s), "seeder loss");
+      ck(cudaStreamSynchronize(s), "seeder sync");
+      last /= (float)std::max(1, nb);
+    }
+  }
+  ck(cudaGetLastError(), "seeder train launch");
+  return last;
+}
+
+void mlp_predict(Mlp* m, const float* dX, int n, double* out, int out_ld, cudaStream_t s) {
+  if (!m->normed) throw std::runtime_error("seeder: not trained");
+  const int ni = m->dims.front(), no = m->dims.back();
+  const int chunk = std::max(m->bcap, std::min(n, 4096));
+  ensure_batch(m, chunk);
+  for (int r0 = 0; r0 < n; r0 += chunk) {
+    const int B = std::min(chunk, n - r0);
+    k_norm_rows<<<grid_for((size_t)B * ni), 256, 0, s>>>(dX + (size_t)r0 * ni, nullptr, B, ni, m->fmean.p,
+                                                         m->fistd.p, m->act[0].p);
+    forward(m, B, s);
+    double* o = out_ld > 0 ? out + r0 : out + (size_t)r0 * no;
+    k_denorm<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[m->L].p, B, no, m->tmean.p, m->tsd.p, o, out_ld);
+  }
+  ck(cudaGetLastError(), "seeder predict launch");
+}
+
+void mlp_gemm(int M, int N, int K, const float* A, int lda, int transA, const float* B, int ldb,
+              int transB, float* C, int ldc, int accumulate, cudaStream_t s) {
+  gemm(M, N, K, A, lda, transA, B, ldb, transB, C, ldc, accumulate, s);
+  ck(cudaGetLastError(), "gemm launch");
+}
+
+}  // namespace karam
+
+// ---------------------------------------------------------------------------
+// features and targets of a problem's instances
+// ---------------------------------------------------------------------------
+namespace karam {
+
+namespace {
+
+// Row r describes instance g = idx ? idx[r] : r: X[r] = (VTO per MOSFET,
+// KP per MOSFET, DC value per source), Y[r] = node voltages (permuted order).
+__global__ void k_features(DevTopo T, DevInst I, const int* idx, int rows, float* X, float* Y) {
+  const int nm = T.n_mos, nf = 2 * T.n_mos + T.n_vs;
+  const size_t ld = I.ld;
+  const size_t nx = (size_t)rows * nf;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nx;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / nf), j = (int)(e - (size_t)r * nf);
+    const int g = idx ? idx[r] : r;
+    float v;
+    if (j < nm)
+      v = I.vth ? I.vth[(size_t)j * ld + g] : (float)T.mos_card[j].y;
+    else if (j < 2 * nm)
+      v = I.kp ? I.kp[(size_t)(j - nm) * ld + g] : (float)T.mos_card[j - nm].x;
+    else
+      v = (float)I.vs_dc[(size_t)(j - 2 * nm) * ld + g];
+    X[e] = v;
+  }
+  if (!Y) return;
+  const size_t ny = (size_t)rows * T.n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ny;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / T.n), i = (int)(e - (size_t)r * T.n);
+    const int g = idx ? idx[r] : r;
+    Y[e] = (float)I.v[(size_t)i * ld + g];
+  }
+}
+
+}  // namespace
+
+void seeder_features(const DevTopo& T, const DevInst& I, const int* idx, int rows, float* X,
+                     float* Y, cudaStream_t s) {
+  const size_t n = (size_t)rows * (2 * T.n_mos + T.n_vs);
+  k_features<<<grid_for(n), 256, 0, s>>>(T, I, idx, rows, X, Y);
+  ck(cudaGetLastError(), "seeder features launch");
+}
+
+}  // namespace karam
