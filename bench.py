@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="instances in the CPU-baseline sample (0 = sized to ~15 s)")
+    ap.add_argument("--seeder-batches", type=int, default=SEEDER_BATCHES,
+                    help="batches of plain-NR DC solutions the learned seeder trains on (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--max-rounds", type=int, default=0,
@@ -330,9 +332,9 @@ def run_karam(args, dist):
     seeder = K.Seeder(prob, width=512, hidden_layers=3, init_seed=1)
     plain_dc = K.options(precision=A.PREC_MIXED, **POLISH)
     n_train = 0
-    for b in range(SEEDER_BATCHES):
+    for b in range(args.seeder_batches):
         prob.set_instances(circuits.mc_instances(
-            nl, ni, first_instance=SEEDER_FIRST + (dist.rank * SEEDER_BATCHES + b) * ni))
+            nl, ni, first_instance=SEEDER_FIRST + (dist.rank * args.seeder_batches + b) * ni))
         prob.solve_dc(plain_dc)
         n_train += seeder.add_dc(prob)
     t_s1 = time.perf_counter()
