@@ -303,6 +303,19 @@ KARAM_API int karam_get_lu_program(const karam_problem *p, int32_t *hdr, int32_t
  * with meta = nL | nU << 4 | chain << 8 | back-forwarding << 9;
  * rec2[2 n] = (U column 0, U column 1). No counterpart in the reference. */
 KARAM_API int karam_get_lu_records(const karam_problem *p, int32_t *rec, int32_t *rec2);
+/* The level schedule of the factor/solve kernel's LU (nested-dissection order
+ * of the Min-Fill unknowns, its own value slots), as one int32 array:
+ * n, n_slots, levels, long-list threshold, then 24 arrays, each as its length
+ * followed by its values: nd_perm, nd_src, nd_diag, lv_piv, lv_piv_ptr,
+ * lv_l_ptr, l_slot, l_piv, lv_ts_ptr, lv_tl_ptr, t_slot, t_off, pr_l, pr_u,
+ * lv_ys_ptr, lv_yl_ptr, y_row, y_off, yp_l, yp_k, bs_off, bs_u, bs_c, and the
+ * same schedule packed as the kernel stages it (empty if it does not fit
+ * 16-bit fields).
+ * With buf NULL (or cap too small) only *len is written; returns
+ * KARAM_E_UNSUPPORTED when the problem has no schedule. No counterpart in the
+ * reference. */
+KARAM_API int karam_get_lu_schedule(const karam_problem *p, int32_t *buf, int64_t cap,
+                                    int64_t *len);
 
 /* ---- learned seeder ---------------------------------------------------------
  * The role of solvers/neural_seeder.h, whose learned model is future work in

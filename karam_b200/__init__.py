@@ -72,6 +72,7 @@ def lib():
         "karam_get_lu_program": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(C.c_int32),
                                            P(C.c_int32)]),
         "karam_get_lu_records": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+        "karam_get_lu_schedule": (C.c_int, [vp, P(C.c_int32), C.c_int64, P(C.c_int64)]),
         "karam_seeder_create": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_uint64, P(vp)]),
         "karam_seeder_destroy": (None, [vp]),
         "karam_seeder_add_dc": (C.c_int, [vp, vp, P(C.c_int32)]),
@@ -228,6 +229,29 @@ class Problem:
             return None
         self._check(rc)
         return rec.reshape(n, 8), rec2.reshape(n, 2)
+
+    _SCHED = ("nd_perm nd_src nd_diag lv_piv lv_piv_ptr lv_l_ptr l_slot l_piv lv_ts_ptr "
+              "lv_tl_ptr t_slot t_off pr_l pr_u lv_ys_ptr lv_yl_ptr y_row y_off yp_l yp_k "
+              "bs_off bs_u bs_c nd_prog").split()
+
+    def lu_schedule(self):
+        """The level schedule of the factor/solve kernel's LU as a dict of arrays
+        (plus n, n_slots, levels, long), or None when the problem has none."""
+        ln = C.c_int64(0)
+        rc = lib().karam_get_lu_schedule(self.h, None, 0, C.byref(ln))
+        if rc == A.KARAM_E_UNSUPPORTED:
+            return None
+        self._check(rc)
+        buf = np.zeros(ln.value, np.int32)
+        self._check(lib().karam_get_lu_schedule(self.h, A.ptr(buf, C.c_int32), ln.value,
+                                                C.byref(ln)))
+        out = dict(n=int(buf[0]), n_slots=int(buf[1]), levels=int(buf[2]), long=int(buf[3]))
+        i = 4
+        for name in self._SCHED:
+            m = int(buf[i])
+            out[name] = buf[i + 1:i + 1 + m].copy()
+            i += 1 + m
+        return out
 
     # -- batches and solves -------------------------------------------------
     def set_instances(self, inst: Instances | None):

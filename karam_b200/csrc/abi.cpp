@@ -87,6 +87,8 @@ struct karam_problem {
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
       t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
       t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent;
+  DBuf t_nd[23];  // level schedule tables, in karam_get_lu_schedule's order
+  DBuf t_nd_prog;  // the packed schedule (padded to whole int4)
   DevTopo dt{};
   // instance buffers, [item][ld] (instance-interleaved)
   int ld = 0;
@@ -312,6 +314,35 @@ void upload_topology(karam_problem* p) {
   d.lu_rec = T.lu_small ? p->t_lu_rec.as<int4>() : nullptr;
   d.lu_rec2 = T.lu_small ? p->t_lu_rec2.as<int2>() : nullptr;
   d.slot_rc = p->t_slot_rc.as<int2>();
+  d.nd_levels = T.nd_levels;
+  d.nd_nv = T.nd_nv;
+  d.nd_S = T.nd_nv | 1;
+  d.nd_SY = T.n | 1;
+  if (T.nd_levels > 0) {
+    const std::vector<int>* tabs[23] = {
+        &T.nd_pos, &T.nd_src, &T.nd_diag, &T.lv_piv, &T.lv_piv_ptr, &T.lv_l_ptr, &T.l_slot,
+        &T.l_piv, &T.lv_ts_ptr, &T.lv_tl_ptr, &T.t_slot, &T.t_off, &T.pr_l, &T.pr_u, &T.lv_ys_ptr,
+        &T.lv_yl_ptr, &T.y_row, &T.y_off, &T.yp_l, &T.yp_k, &T.bs_off, &T.bs_u, &T.bs_c};
+    const int** dst[23] = {&d.nd_pos, &d.nd_src, &d.nd_diag, &d.lv_piv, &d.lv_piv_ptr,
+                           &d.lv_l_ptr, &d.l_slot, &d.l_piv, &d.lv_ts_ptr, &d.lv_tl_ptr,
+                           &d.t_slot, &d.t_off, &d.pr_l, &d.pr_u, &d.lv_ys_ptr, &d.lv_yl_ptr,
+                           &d.y_row, &d.y_off, &d.yp_l, &d.yp_k, &d.bs_off, &d.bs_u, &d.bs_c};
+    for (int t = 0; t < 23; ++t) {
+      std::vector<int> v = *tabs[t];
+      if (v.empty()) v.push_back(0);
+      upload(p->t_nd[t], v);
+      *dst[t] = p->t_nd[t].as<int>();
+    }
+  }
+  d.nd_prog = nullptr;
+  d.nd_prog_len = 0;
+  if (!T.nd_prog.empty()) {
+    std::vector<int> pg = T.nd_prog;
+    pg.resize((pg.size() + 3) / 4 * 4, 0);
+    upload(p->t_nd_prog, pg);
+    d.nd_prog = p->t_nd_prog.as<int>();
+    d.nd_prog_len = (int)pg.size();
+  }
   d.slot_ptr = p->t_slot_ptr.as<int>();
   d.csc_ptr = p->t_csc_ptr.as<int>();
   d.csc_ent = p->t_csc_ent.as<int2>();
@@ -1012,6 +1043,24 @@ int karam_get_lu_records(const karam_problem* p, int32_t* rec, int32_t* rec2) {
   if (!T.lu_small) return KARAM_E_UNSUPPORTED;
   if (rec) std::copy(T.lu_rec.begin(), T.lu_rec.end(), rec);
   if (rec2) std::copy(T.lu_rec2.begin(), T.lu_rec2.end(), rec2);
+  return KARAM_OK;
+}
+
+int karam_get_lu_schedule(const karam_problem* p, int32_t* buf, int64_t cap, int64_t* len) {
+  if (!p || !len) return KARAM_E_INVALID;
+  const Topology& T = p->topo;
+  if (T.nd_levels == 0) return KARAM_E_UNSUPPORTED;
+  std::vector<int32_t> out{T.n, T.nd_nv, T.nd_levels, Topology::kNdLong};
+  for (const std::vector<int>* v :
+       {&T.nd_perm, &T.nd_src, &T.nd_diag, &T.lv_piv, &T.lv_piv_ptr, &T.lv_l_ptr, &T.l_slot,
+        &T.l_piv, &T.lv_ts_ptr, &T.lv_tl_ptr, &T.t_slot, &T.t_off, &T.pr_l, &T.pr_u, &T.lv_ys_ptr,
+        &T.lv_yl_ptr, &T.y_row, &T.y_off, &T.yp_l, &T.yp_k, &T.bs_off, &T.bs_u, &T.bs_c,
+        &T.nd_prog}) {
+    out.push_back((int32_t)v->size());
+    out.insert(out.end(), v->begin(), v->end());
+  }
+  *len = (int64_t)out.size();
+  if (buf && cap >= (int64_t)out.size()) std::copy(out.begin(), out.end(), buf);
   return KARAM_OK;
 }
 

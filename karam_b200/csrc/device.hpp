@@ -12,10 +12,13 @@ namespace karam {
 // Launch geometry of the factor/solve kernel of an NR round: one CTA per tile
 // of L instances.
 struct RoundLaunch {
-  int L = 0;          // lanes (instances) per CTA, a power of two <= 32
+  int L = 0;          // instances per CTA (a power of two <= 32 for the pivot program;
+                      // any count <= 32 for the level schedule, one warp each)
   int grid = 0;       // CTAs
-  size_t smem = 0;    // dynamic shared memory bytes (value slots + right-hand side)
+  size_t smem = 0;    // dynamic shared memory bytes
   int ctas_per_sm = 0;
+  int threads = 0;    // CTA size
+  bool nd = false;    // the level-scheduled kernel (k_lu_nd)
 };
 
 // Lane stride of the instance-interleaved arrays for ni instances.

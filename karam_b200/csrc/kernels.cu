@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/karam.h"
 #include "device.hpp"
@@ -14,8 +15,12 @@ using namespace knr;
 
 namespace {
 
-// Value slots + right-hand side of L instances, then the packed pivot records.
-size_t round_smem(const DevTopo& T, int L, size_t es) {
+// Level schedule: ND slots + right-hand side of L instances; else value slots
+// + right-hand side of L instances, then the packed pivot records.
+size_t round_smem(const DevTopo& T, int L, size_t es, bool nd) {
+  if (nd)
+    return ((es * ((size_t)T.nd_S + (size_t)T.nd_SY) * (size_t)L + 15) & ~size_t(15)) +
+           sizeof(int) * (size_t)T.nd_prog_len;
   size_t b = es * ((size_t)T.nv + (size_t)T.n) * (size_t)L;
   if (T.lu_rec) b = ((b + 15) & ~size_t(15)) + (2 * sizeof(int4) + sizeof(int2)) * (size_t)T.n;
   return b;
@@ -32,12 +37,25 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
                        int want_lanes) {
   const bool mixed = prec == KARAM_PREC_MIXED;
   const size_t es = mixed ? sizeof(float) : sizeof(double);
-  const void* kern = mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>;
   RoundLaunch best;
   long best_waves = -1;
-  for (int L = kMaxLanes; L >= 1; L >>= 1) {
+  // candidates: the level-scheduled kernel with L instance warps (any L up to
+  // its thread limit), then the pivot-program kernel with power-of-two L
+  struct Cand {
+    int L;
+    bool nd;
+  };
+  std::vector<Cand> cands;
+  if (T.nd_prog_len > 0)
+    for (int L = (mixed ? 32 : 16); L >= 1; --L) cands.push_back({L, true});
+  for (int L = kMaxLanes; L >= 1; L >>= 1) cands.push_back({L, false});
+  for (const Cand& c : cands) {
+    const int L = c.L;
     if (want_lanes > 0 && L != want_lanes) continue;
-    const size_t sm = round_smem(T, L, es);
+    const void* kern = c.nd ? (mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>)
+                            : (mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>);
+    const int threads = c.nd ? 32 * L : kRoundThreads;
+    const size_t sm = round_smem(T, L, es, c.nd);
     if (sm > (size_t)max_smem) continue;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
         cudaSuccess) {
@@ -45,8 +63,7 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
       continue;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRoundThreads, sm) !=
-            cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, sm) != cudaSuccess ||
         per_sm < 1) {
       cudaGetLastError();
       continue;
@@ -54,19 +71,31 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
     const int grid = (ni + L - 1) / L;
     const long slots = (long)per_sm * std::max(1, num_sms);
     const long waves = (grid + slots - 1) / slots;
-    // fewest waves; among equals, a grid that reaches every SM (the streaming
-    // phases spread wider and each SM runs more factor chains side by side)
+    // fewest waves; among equals the level schedule, then a grid that
+    // reaches every SM (the streaming phases spread wider)
     const bool fills = grid >= num_sms, best_fills = best.grid >= num_sms;
-    if (best_waves < 0 || waves < best_waves || (waves == best_waves && fills && !best_fills)) {
+    bool better = best_waves < 0 || waves < best_waves;
+    if (!better && waves == best_waves) {
+      if (c.nd != best.nd)
+        better = c.nd;
+      else
+        better = fills && !best_fills;
+    }
+    if (better) {
       best_waves = waves;
       best.L = L;
       best.grid = grid;
       best.smem = sm;
       best.ctas_per_sm = per_sm;
+      best.threads = threads;
+      best.nd = c.nd;
     }
   }
-  if (best.L > 0)
+  if (best.L > 0) {
+    const void* kern = best.nd ? (mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>)
+                               : (mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best.smem);
+  }
   const int rsm = (int)plan_rescue(T).smem;
   cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
   cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
@@ -98,10 +127,16 @@ void launch_eval_stamp(const DevTopo& T, const DevInst& I, const JobParams& P,
 
 void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const RoundLaunch& L,
                int prec, int* active, cudaStream_t s) {
-  if (prec == KARAM_PREC_MIXED)
+  if (L.nd) {
+    if (prec == KARAM_PREC_MIXED)
+      k_lu_nd<float><<<L.grid, L.threads, L.smem, s>>>(T, I, P, L.L, active);
+    else
+      k_lu_nd<double><<<L.grid, L.threads, L.smem, s>>>(T, I, P, L.L, active);
+  } else if (prec == KARAM_PREC_MIXED) {
     k_lu<float><<<L.grid, kRoundThreads, L.smem, s>>>(T, I, P, L.L, active);
-  else
+  } else {
     k_lu<double><<<L.grid, kRoundThreads, L.smem, s>>>(T, I, P, L.L, active);
+  }
 }
 
 RescuePlan plan_rescue(const DevTopo& T) {

@@ -916,19 +916,141 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// 16-bit field i of the packed half-word array at prog[base].
+__device__ __forceinline__ int nd_half(const int* prog, int base, int i) {
+  return (prog[base + (i >> 1)] >> (16 * (i & 1))) & 0xFFFF;
+}
+
+// The static-pivot LU of one instance by one warp on the packed level
+// schedule in shared memory (layout: nd_program in topology.cpp): per level,
+// the pivots' reciprocals, then their L values, then the update targets and
+// right-hand-side rows (lists longer than Topology::kNdLong summed by the
+// whole warp, partials combined in a fixed tree); then the back substitution
+// from the last level down. A and y are this instance's ND slots and
+// right-hand side (ND order); y returns the solution. Same failure tests as
+// lu_solve: tiny or non-finite pivots, non-finite solutions, multipliers
+// above growth_limit.
+template <typename T>
+__device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __restrict__ prog,
+                         T tiny, T growth_limit, int lane) {
+  const int NL = prog[0], lvt = prog[1], tpb = prog[2], ypb = prog[3], bpb = prog[4];
+  bool ok = true;
+  T lmax = T(0);
+  for (int lv = 0; lv < NL; ++lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    const int po = Lt[0], pc = Lt[1], lo = Lt[2], lc = Lt[3];
+    for (int q = lane; q < pc; q += 32) {
+      const int d = prog[po + q];
+      const T piv = A[d];
+      ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
+      A[d] = recip(piv);
+    }
+    __syncwarp();
+    for (int e = lane; e < lc; e += 32) {
+      const int v = prog[lo + e];
+      const int sl = v & 0xFFFF;
+      const T l = A[sl] * A[(v >> 16) & 0xFFFF];
+      A[sl] = l;
+      lmax = fmax(lmax, fabs(l));
+    }
+    __syncwarp();
+    const int to = Lt[4], tsc = Lt[5], tlc = Lt[6];
+    for (int t = lane; t < tsc; t += 32) {
+      const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
+      const int sl = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
+      T acc = A[sl];
+      for (int q = 0; q < c; ++q) {
+        const int pr = prog[off + q];
+        acc -= A[pr & 0xFFFF] * A[(pr >> 16) & 0xFFFF];
+      }
+      A[sl] = acc;
+    }
+    const int yo = Lt[7], ysc = Lt[8], ylc = Lt[9];
+    for (int r = lane; r < ysc; r += 32) {
+      const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
+      const int row = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
+      T acc = y[row];
+      for (int q = 0; q < c; ++q) {
+        const int pr = prog[off + q];
+        acc -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
+      }
+      y[row] = acc;
+    }
+    for (int t = tsc; t < tsc + tlc; ++t) {  // long target lists: the warp sums
+      const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
+      const int c = (h >> 16) & 0xFFFF;
+      T part = T(0);
+      for (int q = lane; q < c; q += 32) {
+        const int pr = prog[off + q];
+        part += A[pr & 0xFFFF] * A[(pr >> 16) & 0xFFFF];
+      }
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) A[h & 0xFFFF] -= part;
+    }
+    for (int r = ysc; r < ysc + ylc; ++r) {  // long right-hand-side rows
+      const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
+      const int c = (h >> 16) & 0xFFFF;
+      T part = T(0);
+      for (int q = lane; q < c; q += 32) {
+        const int pr = prog[off + q];
+        part += A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
+      }
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) y[h & 0xFFFF] -= part;
+    }
+    __syncwarp();
+  }
+  bool finite = true;
+  for (int lv = NL - 1; lv >= 0; --lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    const int bo = Lt[10], bc = Lt[11];
+    for (int q = lane; q < bc; q += 32) {
+      const int a = prog[bo + 2 * q], b = prog[bo + 2 * q + 1];
+      const int k = a & 0xFFFF, d = (a >> 16) & 0xFFFF;
+      const int c = b & 0xFFFF, off = bpb + ((b >> 16) & 0xFFFF);
+      T sv = y[k];
+      for (int j = 0; j < c; ++j) {
+        const int pr = prog[off + j];
+        sv -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
+      }
+      sv *= A[d];
+      y[k] = sv;
+      finite = finite && isfinite(sv);
+    }
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(kFull, lmax, o));
+  ok = __all_sync(kFull, ok);
+  finite = __all_sync(kFull, finite);
+  return ok && finite && !(lmax > growth_limit);
+}
+
 // Control flow + linear solve of a tile of L instances (one CTA): decisions
 // from the reductions of k_es, vector updates, the Jacobian tile staged
 // into shared memory with cp.async, static-pivot LU with the forward
 // substitution fused, x = v + dx, junction limiting, bookkeeping.
-template <typename T>
-__global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, JobParams P, int L,
-                                                      int* active) {
+template <typename T, bool nd>
+__device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, const JobParams& P,
+                                         int L, int* active) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* A = reinterpret_cast<T*>(smem_raw);  // [nv][L]
-  T* Y = A + (size_t)Tp.nv * L;            // [n][L]
-  int4* rec = Tp.lu_rec ? reinterpret_cast<int4*>(
-                              smem_raw + (((size_t)(Tp.nv + Tp.n) * L * sizeof(T) + 15) & ~size_t(15)))
-                        : nullptr;         // [2 n] packed pivot records
+  // level schedule (nd, one warp per instance): A [L][nd_S] ND slots,
+  // Y [L][nd_SY], then the packed schedule; else A [nv][L] value slots,
+  // Y [n][L] and the packed pivot records
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* Y = nd ? A + (size_t)Tp.nd_S * L : A + (size_t)Tp.nv * L;
+  int4* rec = (!nd && Tp.lu_rec)
+                  ? reinterpret_cast<int4*>(
+                        smem_raw + (((size_t)(Tp.nv + Tp.n) * L * sizeof(T) + 15) & ~size_t(15)))
+                  : nullptr;
+  const int* prog =
+      nd ? reinterpret_cast<const int*>(
+               smem_raw + (((size_t)(Tp.nd_S + Tp.nd_SY) * L * sizeof(T) + 15) & ~size_t(15)))
+         : nullptr;
+  if (nd) {  // the packed schedule into shared memory, once per launch
+    int4* dst = reinterpret_cast<int4*>(const_cast<int*>(prog));
+    const int4* srcp = reinterpret_cast<const int4*>(Tp.nd_prog);
+    for (int e = threadIdx.x; e < (Tp.nd_prog_len + 3) / 4; e += blockDim.x) dst[e] = __ldg(&srcp[e]);
+  }
   __shared__ int s_live[kMaxLanes], s_act[kMaxLanes], s_sing[kMaxLanes], s_trev[kMaxLanes];
   __shared__ double s_gmin[kMaxLanes], s_hsub[kMaxLanes];
 
@@ -1005,7 +1127,9 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
         }
         if (a & (ACT_STEP | ACT_TRAN_INIT)) I.v_tp[o] = vi;
       }
-      if (a & ACT_SOLVE) Y[i * L + lane] = (T)(-(I.F[o] + gmin * vi));
+      if (a & ACT_SOLVE)
+        Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane] =
+            (T)(-(I.F[o] + gmin * vi));
     }
     any_solve = (a & ACT_SOLVE) != 0;
   }
@@ -1015,7 +1139,17 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
   if (any_solve) {
     const T* J = reinterpret_cast<const T*>(I.J);
     const int row_bytes = L * (int)sizeof(T);
-    if (row_bytes % 16 == 0) {
+    if (nd) {
+      // gather each instance's ND slots (consecutive threads: consecutive
+      // instances of one slot, so the global reads are contiguous)
+      const int S = Tp.nd_S, total = Tp.nd_nv * L;
+#pragma unroll 4
+      for (int e = tid; e < total; e += blockDim.x) {
+        const int sl = e / L, w = e - sl * L;
+        const int src = nd_half(prog, prog[5], sl);
+        A[w * S + sl] = (src != 0xFFFF && w < cnt) ? J[(size_t)src * ld + base + w] : T(0);
+      }
+    } else if (row_bytes % 16 == 0) {
       const int cpr = row_bytes / 16;  // 16-byte chunks per slot row
       const int chunks = nv * cpr;
       for (int c = tid; c < chunks; c += blockDim.x) {
@@ -1062,14 +1196,26 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
   if (any_solve) {
     if (a & ACT_SOLVE) {
       const T gmin = (T)s_gmin[lane];
-      for (int i = row; i < n; i += R) A[__ldg(&Tp.lu_hdr[i].w) * L + lane] += gmin;
+      if (nd)
+        for (int i = row; i < n; i += R)
+          A[lane * Tp.nd_S + __ldg(&Tp.nd_diag[nd_half(prog, prog[6], i)])] += gmin;
+      else
+        for (int i = row; i < n; i += R) A[__ldg(&Tp.lu_hdr[i].w) * L + lane] += gmin;
     }
     __syncthreads();
 
-    // 3. factor + solve: one lane per instance
-    if (tid < L && (s_act[tid] & ACT_SOLVE)) {
-      const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
-      const T growth = sizeof(T) == 8 ? (T)P.growth64 : (T)fmin(P.growth32, 3.0e38);
+    // 3. factor + solve: one warp per instance on the level schedule, else
+    //    one lane per instance on the pivot program
+    const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
+    const T growth = sizeof(T) == 8 ? (T)P.growth64 : (T)fmin(P.growth32, 3.0e38);
+    if (nd) {
+      const int w = tid >> 5;
+      if (w < L && (s_act[w] & ACT_SOLVE)) {
+        const bool okw = nd_solve<T>(A + (size_t)w * Tp.nd_S, Y + (size_t)w * Tp.nd_SY, prog,
+                                     tiny, growth, tid & 31);
+        if ((tid & 31) == 0) s_sing[w] = okw ? 0 : 1;
+      }
+    } else if (tid < L && (s_act[tid] & ACT_SOLVE)) {
       s_sing[tid] = lu_solve<T>(A + tid, Y + tid, L, Tp, rec, tiny, growth) ? 0 : 1;
     }
     __syncthreads();
@@ -1080,7 +1226,7 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
     if (upd)
       for (int i = row; i < n; i += R) {
         const size_t o = (size_t)i * ld + g;
-        double xi = I.v[o] + (double)Y[i * L + lane];
+        double xi = I.v[o] + (double)Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane];
         if (sanitize && !isfinite(xi)) xi = 0.0;  // SafeUtils::sanitize_vector
         I.x[o] = xi;
       }
@@ -1136,6 +1282,19 @@ __global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, Job
       }
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRoundThreads) k_lu(DevTopo Tp, DevInst I, JobParams P, int L,
+                                                      int* active) {
+  lu_round<T, false>(Tp, I, P, L, active);
+}
+
+// The level-scheduled variant: blockDim = 32 L, one warp per instance.
+template <typename T>
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 1024 : 512)
+    k_lu_nd(DevTopo Tp, DevInst I, JobParams P, int L, int* active) {
+  lu_round<T, true>(Tp, I, P, L, active);
 }
 
 // ---------------------------------------------------------------------------

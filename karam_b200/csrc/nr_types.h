@@ -125,6 +125,21 @@ struct DevTopo {
   const int4* lu_rec;       // pivot records when lu_small (2 int4 per pivot: meta, diagonal,
                             // Lslot, Lrow | Uslot0, Uslot1, T0, T1; see topology.cpp), else 0
   const int2* lu_rec2;      // back-substitution columns (Ucol0, Ucol1) per pivot
+  // level-scheduled LU of the factor/solve kernel (nd_levels > 0): the same
+  // static pivots on a nested-dissection order with its own value slots; one
+  // warp per instance, pivots of a level side by side (tables as in
+  // Topology::nd_*). Per instance in shared memory: nd_S slots, nd_SY
+  // right-hand-side entries (odd strides).
+  int nd_levels, nd_nv, nd_S, nd_SY;
+  const int* nd_pos;        // Min-Fill index -> ND position
+  const int* nd_src;        // ND slot -> Min-Fill value slot (-1: 0)
+  const int* nd_diag;       // ND pivot -> ND slot of its diagonal
+  const int *lv_piv, *lv_piv_ptr, *lv_l_ptr, *l_slot, *l_piv;
+  const int *lv_ts_ptr, *lv_tl_ptr, *t_slot, *t_off, *pr_l, *pr_u;
+  const int *lv_ys_ptr, *lv_yl_ptr, *y_row, *y_off, *yp_l, *yp_k;
+  const int *bs_off, *bs_u, *bs_c;
+  const int* nd_prog;       // the schedule packed for shared memory (nd_program)
+  int nd_prog_len;          // ints (0: the level-scheduled kernel is not used)
   const int2* slot_rc;      // (row, col) of every value slot (permuted)
   const int* slot_ptr;      // [n + 1] first slot of each row (columns ascending within a row)
   const int* csc_ptr;       // [n + 1] value slots by column: (row, slot) in csc_ent

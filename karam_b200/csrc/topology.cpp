@@ -2,6 +2,7 @@
 #include "topology.hpp"
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <map>
 #include <set>
@@ -535,6 +536,324 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   for (auto& c : T.isrc) { T.is_term.push_back(pn(c.n1)); T.is_term.push_back(pn(c.n2)); }
 }
 
+// Level schedule of the factor/solve kernel's LU (Topology::nd_*): the
+// static-pivot elimination of the Min-Fill system in a nested-dissection
+// order, so that pivots with no dependency between them run side by side.
+//  - Order: vertices of degree > 32 (supply hubs) last; the rest by recursive
+//    bisection with the middle BFS level from a pseudo-peripheral vertex as
+//    separator, separators after both halves (deterministic: ties to the
+//    smallest index).
+//  - Structure: the stamped positions and the diagonal, eliminated
+//    unsymmetrically (pivot k fills (i, j) for i in L_k, j in U_k).
+//  - Levels: pivot m depends on k when k's elimination writes row or column
+//    m (m in L_k or U_k); level(m) = 1 + the largest level it depends on.
+//    Within a level no pivot reads what another writes; two pivots updating
+//    the same target are summed in one list, in pivot order.
+void nd_schedule(Topology& T) {
+  const int n = T.n;
+  T.nd_levels = 0;
+  if (n < 2 || n > 20000) return;
+  auto key = [](int r, int c) { return (int64_t(r) << 32) | int64_t(unsigned(c)); };
+  // stamped positions (Min-Fill permuted space)
+  std::vector<std::pair<int, int>> pos;
+  for (const auto& x : T.trip) {
+    const int sl = T.f_slot[x.f];
+    if (sl >= 0) pos.emplace_back(T.slot_row[sl], T.slot_col[sl]);
+  }
+  for (int i = 0; i < n; ++i) pos.emplace_back(i, i);
+  std::vector<std::vector<int>> adj(n);
+  for (auto& q : pos)
+    if (q.first != q.second) {
+      adj[q.first].push_back(q.second);
+      adj[q.second].push_back(q.first);
+    }
+  for (auto& a : adj) {
+    std::sort(a.begin(), a.end());
+    a.erase(std::unique(a.begin(), a.end()), a.end());
+  }
+  std::vector<char> hub(n, 0);
+  for (int i = 0; i < n; ++i) hub[i] = adj[i].size() > 32;
+  std::vector<int> order;
+  order.reserve(n);
+  std::vector<int> mark(n, -1), lev(n, -1);
+  int stamp = 0;
+  // recursive nested dissection on the vertex set `nodes` (sorted)
+  std::function<void(std::vector<int>&)> nd = [&](std::vector<int>& nodes) {
+    if (nodes.size() <= 2) {
+      order.insert(order.end(), nodes.begin(), nodes.end());
+      return;
+    }
+    const int in_set = stamp++;
+    for (int v : nodes) mark[v] = in_set;
+    // components, each from its smallest vertex
+    std::vector<std::vector<int>> comps;
+    const int seen = stamp++;
+    for (int s0 : nodes) {
+      if (mark[s0] != in_set) continue;
+      std::vector<int> comp{s0};
+      mark[s0] = seen;
+      for (size_t h = 0; h < comp.size(); ++h)
+        for (int w : adj[comp[h]])
+          if (mark[w] == in_set) {
+            mark[w] = seen;
+            comp.push_back(w);
+          }
+      std::sort(comp.begin(), comp.end());
+      comps.push_back(std::move(comp));
+    }
+    if (comps.size() > 1) {
+      for (auto& c : comps) nd(c);
+      return;
+    }
+    std::vector<int>& comp = comps[0];
+    const int cur = stamp++;
+    for (int v : comp) mark[v] = cur;
+    auto bfs = [&](int src, std::vector<int>& seq) {
+      seq.clear();
+      seq.push_back(src);
+      const int vis = stamp++;
+      lev[src] = 0;
+      std::vector<int> visited{src};
+      mark[src] = vis;
+      for (size_t h = 0; h < seq.size(); ++h)
+        for (int w : adj[seq[h]])
+          if (mark[w] == cur) {
+            mark[w] = vis;
+            lev[w] = lev[seq[h]] + 1;
+            seq.push_back(w);
+          }
+      for (int v : seq) mark[v] = cur;  // back into the component
+    };
+    std::vector<int> seq;
+    bfs(comp[0], seq);
+    int far = seq[0];
+    for (int v : seq)
+      if (lev[v] > lev[far] || (lev[v] == lev[far] && v < far)) far = v;
+    bfs(far, seq);
+    int L = 0;
+    for (int v : seq) L = std::max(L, lev[v]);
+    if (L < 2) {
+      order.insert(order.end(), comp.begin(), comp.end());
+      return;
+    }
+    const int mid = L / 2;
+    std::vector<int> a, b, sep;
+    for (int v : comp) (lev[v] < mid ? a : (lev[v] > mid ? b : sep)).push_back(v);
+    nd(a);
+    nd(b);
+    order.insert(order.end(), sep.begin(), sep.end());
+  };
+  std::vector<int> rest;
+  for (int i = 0; i < n; ++i)
+    if (!hub[i]) rest.push_back(i);
+  // hubs leave the graph the dissection sees
+  for (int i = 0; i < n; ++i)
+    if (hub[i]) mark[i] = -2;
+  {
+    std::vector<std::vector<int>> adj2(n);
+    for (int i = 0; i < n; ++i)
+      if (!hub[i])
+        for (int w : adj[i])
+          if (!hub[w]) adj2[i].push_back(w);
+    adj.swap(adj2);
+  }
+  nd(rest);
+  for (int i = 0; i < n; ++i)
+    if (hub[i]) order.push_back(i);
+  if ((int)order.size() != n) return;
+  T.nd_perm = order;
+  T.nd_pos.assign(n, 0);
+  for (int p = 0; p < n; ++p) T.nd_pos[order[p]] = p;
+
+  // unsymmetric symbolic elimination in ND order
+  std::vector<std::set<int>> R(n), Cc(n);
+  for (auto& q : pos) {
+    const int r = T.nd_pos[q.first], c = T.nd_pos[q.second];
+    R[r].insert(c);
+    Cc[c].insert(r);
+  }
+  std::vector<std::vector<int>> Lk(n), Uk(n);
+  for (int k = 0; k < n; ++k) {
+    for (auto it = Cc[k].upper_bound(k); it != Cc[k].end(); ++it) Lk[k].push_back(*it);
+    for (auto it = R[k].upper_bound(k); it != R[k].end(); ++it) Uk[k].push_back(*it);
+    for (int i : Lk[k])
+      for (int j : Uk[k])
+        if (R[i].insert(j).second) Cc[j].insert(i);
+  }
+  // ND slots, row-major
+  std::unordered_map<int64_t, int> slot;
+  T.nd_nv = 0;
+  T.nd_src.clear();
+  std::unordered_map<int64_t, int> mf;
+  for (int sl = 0; sl < T.nv; ++sl) mf[key(T.slot_row[sl], T.slot_col[sl])] = sl;
+  for (int r = 0; r < n; ++r)
+    for (int c : R[r]) {
+      slot[key(r, c)] = T.nd_nv++;
+      auto f = mf.find(key(order[r], order[c]));
+      T.nd_src.push_back(f == mf.end() ? -1 : f->second);
+    }
+  auto S = [&](int r, int c) { return slot.at(key(r, c)); };
+  T.nd_diag.assign(n, 0);
+  for (int k = 0; k < n; ++k) T.nd_diag[k] = S(k, k);
+  // levels
+  std::vector<int> level(n, 0);
+  for (int k = 0; k < n; ++k) {
+    for (int m : Lk[k]) level[m] = std::max(level[m], level[k] + 1);
+    for (int m : Uk[k]) level[m] = std::max(level[m], level[k] + 1);
+  }
+  const int NL = 1 + *std::max_element(level.begin(), level.end());
+  std::vector<std::vector<int>> piv(NL);
+  for (int k = 0; k < n; ++k) piv[level[k]].push_back(k);
+  for (auto* v : {&T.lv_piv, &T.lv_piv_ptr, &T.lv_l_ptr, &T.l_slot, &T.l_piv, &T.lv_ts_ptr,
+                  &T.lv_tl_ptr, &T.t_slot, &T.t_off, &T.pr_l, &T.pr_u, &T.lv_ys_ptr, &T.lv_yl_ptr,
+                  &T.y_row, &T.y_off, &T.yp_l, &T.yp_k, &T.bs_off, &T.bs_u, &T.bs_c})
+    v->clear();
+  T.t_off.push_back(0);
+  T.y_off.push_back(0);
+  for (int lv = 0; lv < NL; ++lv) {
+    T.lv_piv_ptr.push_back((int)T.lv_piv.size());
+    T.lv_l_ptr.push_back((int)T.l_slot.size());
+    std::map<int, std::vector<std::pair<int, int>>> tc, yc;  // target slot / row -> pairs
+    for (int k : piv[lv]) {
+      T.lv_piv.push_back(k);
+      for (int i : Lk[k]) {
+        T.l_slot.push_back(S(i, k));
+        T.l_piv.push_back(k);
+        yc[i].emplace_back(S(i, k), k);
+        for (int j : Uk[k]) tc[S(i, j)].emplace_back(S(i, k), S(k, j));
+      }
+    }
+    for (int pass = 0; pass < 2; ++pass) {  // short lists, then long ones
+      (pass ? T.lv_tl_ptr : T.lv_ts_ptr).push_back((int)T.t_slot.size());
+      for (auto& e : tc)
+        if (((int)e.second.size() > Topology::kNdLong) == (pass == 1)) {
+          T.t_slot.push_back(e.first);
+          for (auto& q : e.second) {
+            T.pr_l.push_back(q.first);
+            T.pr_u.push_back(q.second);
+          }
+          T.t_off.push_back((int)T.pr_l.size());
+        }
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      (pass ? T.lv_yl_ptr : T.lv_ys_ptr).push_back((int)T.y_row.size());
+      for (auto& e : yc)
+        if (((int)e.second.size() > Topology::kNdLong) == (pass == 1)) {
+          T.y_row.push_back(e.first);
+          for (auto& q : e.second) {
+            T.yp_l.push_back(q.first);
+            T.yp_k.push_back(q.second);
+          }
+          T.y_off.push_back((int)T.yp_l.size());
+        }
+    }
+  }
+  T.lv_piv_ptr.push_back((int)T.lv_piv.size());
+  T.lv_l_ptr.push_back((int)T.l_slot.size());
+  T.lv_ts_ptr.push_back((int)T.t_slot.size());
+  T.lv_tl_ptr.push_back((int)T.t_slot.size());
+  T.lv_ys_ptr.push_back((int)T.y_row.size());
+  T.lv_yl_ptr.push_back((int)T.y_row.size());
+  T.bs_off.push_back(0);
+  for (int k = 0; k < n; ++k) {
+    for (int j : Uk[k]) {
+      T.bs_u.push_back(S(k, j));
+      T.bs_c.push_back(j);
+    }
+    T.bs_off.push_back((int)T.bs_u.size());
+  }
+  T.nd_levels = NL;
+}
+
+// The level schedule packed into one int array that a CTA stages into shared
+// memory (lo | hi << 16, 16-bit fields):
+//   [0] levels, [1] section offset of the level table, [2] of the target
+//   pairs, [3] of the right-hand-side pairs, [4] of the back-substitution
+//   pairs, [5] of nd_src (two per int, 0xFFFF = none), [6] of nd_pos (two per
+//   int), [7] total ints;
+//   level table, 12 ints per level: offsets and counts of its pivots (diag
+//   slots), L entries (slot | diag << 16), short targets and long targets
+//   (int2: slot | count << 16, first pair), short and long right-hand-side
+//   rows (int2: row | count << 16, first pair), back-substitution pivots
+//   (int2: pivot | diag << 16, count | first pair << 16);
+//   pairs: target (l slot | u slot << 16), right-hand side (l slot | pivot <<
+//   16), back substitution (u slot | column << 16).
+void nd_program(Topology& T) {
+  T.nd_prog.clear();
+  if (T.nd_levels == 0) return;
+  const int NL = T.nd_levels;
+  if (T.nd_nv >= 0xFFFF || T.n >= 0xFFFF || (int)T.pr_l.size() >= 0xFFFF ||
+      (int)T.yp_l.size() >= 0xFFFF || (int)T.bs_u.size() >= 0xFFFF)
+    return;
+  auto pk = [](int lo, int hi) { return (int)((unsigned)lo | ((unsigned)hi << 16)); };
+  std::vector<int> body, tp, yp, bp;
+  std::vector<int> lvt(12 * (size_t)NL);
+  for (int lv = 0; lv < NL; ++lv) {
+    int* L = &lvt[12 * (size_t)lv];
+    L[0] = (int)body.size();
+    for (int q = T.lv_piv_ptr[lv]; q < T.lv_piv_ptr[lv + 1]; ++q) body.push_back(T.nd_diag[T.lv_piv[q]]);
+    L[1] = (int)body.size() - L[0];
+    L[2] = (int)body.size();
+    for (int e = T.lv_l_ptr[lv]; e < T.lv_l_ptr[lv + 1]; ++e)
+      body.push_back(pk(T.l_slot[e], T.nd_diag[T.l_piv[e]]));
+    L[3] = (int)body.size() - L[2];
+    auto items = [&](int a, int b, const std::vector<int>& key, const std::vector<int>& off,
+                     const std::vector<int>& pl, const std::vector<int>& ph, std::vector<int>& pairs,
+                     int* o, int* c) {
+      *o = (int)body.size();
+      for (int t = a; t < b; ++t) {
+        body.push_back(pk(key[t], off[t + 1] - off[t]));
+        body.push_back((int)pairs.size());
+        for (int q = off[t]; q < off[t + 1]; ++q) pairs.push_back(pk(pl[q], ph[q]));
+      }
+      *c = b - a;
+    };
+    items(T.lv_ts_ptr[lv], T.lv_tl_ptr[lv], T.t_slot, T.t_off, T.pr_l, T.pr_u, tp, &L[4], &L[5]);
+    int tl_off;
+    items(T.lv_tl_ptr[lv], T.lv_ts_ptr[lv + 1], T.t_slot, T.t_off, T.pr_l, T.pr_u, tp, &tl_off, &L[6]);
+    items(T.lv_ys_ptr[lv], T.lv_yl_ptr[lv], T.y_row, T.y_off, T.yp_l, T.yp_k, yp, &L[7], &L[8]);
+    int yl_off;
+    items(T.lv_yl_ptr[lv], T.lv_ys_ptr[lv + 1], T.y_row, T.y_off, T.yp_l, T.yp_k, yp, &yl_off, &L[9]);
+    L[10] = (int)body.size();
+    for (int q = T.lv_piv_ptr[lv]; q < T.lv_piv_ptr[lv + 1]; ++q) {
+      const int k = T.lv_piv[q];
+      body.push_back(pk(k, T.nd_diag[k]));
+      body.push_back(pk(T.bs_off[k + 1] - T.bs_off[k], (int)bp.size()));
+      for (int b = T.bs_off[k]; b < T.bs_off[k + 1]; ++b) bp.push_back(pk(T.bs_u[b], T.bs_c[b]));
+    }
+    L[11] = T.lv_piv_ptr[lv + 1] - T.lv_piv_ptr[lv];
+  }
+  if (tp.size() >= 0xFFFF || yp.size() >= 0xFFFF || bp.size() >= 0xFFFF) return;
+  std::vector<int> src((T.nd_nv + 1) / 2), ps((T.n + 1) / 2);
+  for (int i = 0; i < T.nd_nv; ++i) {
+    const unsigned v = T.nd_src[i] < 0 ? 0xFFFFu : (unsigned)T.nd_src[i];
+    src[i / 2] = (int)((unsigned)src[i / 2] | (v << (16 * (i & 1))));
+  }
+  for (int i = 0; i < T.n; ++i)
+    ps[i / 2] = (int)((unsigned)ps[i / 2] | ((unsigned)T.nd_pos[i] << (16 * (i & 1))));
+  std::vector<int>& P = T.nd_prog;
+  P.assign(8, 0);
+  P[0] = NL;
+  P[1] = (int)P.size();
+  P.insert(P.end(), lvt.begin(), lvt.end());
+  const int body_at = (int)P.size();
+  P.insert(P.end(), body.begin(), body.end());
+  // level-table offsets are absolute in the program
+  for (int lv = 0; lv < NL; ++lv)
+    for (int f : {0, 2, 4, 7, 10}) P[P[1] + 12 * lv + f] += body_at;
+  P[2] = (int)P.size();
+  P.insert(P.end(), tp.begin(), tp.end());
+  P[3] = (int)P.size();
+  P.insert(P.end(), yp.begin(), yp.end());
+  P[4] = (int)P.size();
+  P.insert(P.end(), bp.begin(), bp.end());
+  P[5] = (int)P.size();
+  P.insert(P.end(), src.begin(), src.end());
+  P[6] = (int)P.size();
+  P.insert(P.end(), ps.begin(), ps.end());
+  P[7] = (int)P.size();
+}
+
 }  // namespace
 
 // Min-Fill elimination with the reference's choice rule: at every step the
@@ -923,6 +1242,8 @@ Topology build_topology(const karam_netlist* nl) {
   device_tables(T, urow);
   node_term_records(T);
   es_blocks(T);
+  nd_schedule(T);
+  nd_program(T);
   return T;
 }
 

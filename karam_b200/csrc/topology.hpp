@@ -92,6 +92,31 @@ struct Topology {
   int lu_ops = 0;
   int max_d = 0;
 
+  // ---- level-scheduled LU of the factor/solve kernel: the same static-pivot
+  //      elimination on a nested-dissection order of the Min-Fill unknowns
+  //      (hubs last), whose elimination tree is shallow; its own value slots
+  //      ("ND slots", row-major), gathered from the Min-Fill value slots ----
+  int nd_levels = 0;                 // 0: no schedule
+  int nd_nv = 0;
+  std::vector<int> nd_perm, nd_pos;  // ND position -> Min-Fill index, and back
+  std::vector<int> nd_src;           // ND slot -> Min-Fill value slot (-1: starts at 0)
+  std::vector<int> nd_diag;          // ND pivot -> ND slot of its diagonal
+  // per level (CSR offsets lv_*[level .. level + 1]):
+  std::vector<int> lv_piv, lv_piv_ptr;   // pivots
+  std::vector<int> lv_l_ptr, l_slot, l_piv;  // L entries: l = A[slot] * reciprocal of pivot
+  std::vector<int> lv_ts_ptr, lv_tl_ptr;     // update targets, short lists then long lists
+  std::vector<int> t_slot, t_off;            // target slot, its pairs [t_off[t], t_off[t + 1])
+  std::vector<int> pr_l, pr_u;               // pairs: L slot, U slot
+  std::vector<int> lv_ys_ptr, lv_yl_ptr;     // right-hand-side rows, short then long
+  std::vector<int> y_row, y_off;             // row, its pairs [y_off[r], y_off[r + 1])
+  std::vector<int> yp_l, yp_k;               // pairs: L slot, pivot
+  std::vector<int> bs_off, bs_u, bs_c;       // back substitution per pivot: U slots and columns
+  static constexpr int kNdLong = 8;          // longer contribution lists are summed by the warp
+  // The same schedule packed for shared memory (16-bit fields, two per int;
+  // empty when some index does not fit 16 bits): see nd_program in
+  // topology.cpp for the layout.
+  std::vector<int> nd_prog;
+
   // ---- evaluation + stamping blocks: the stamp items (value slots 0..nv-1,
   //      nodes nv..nv+n-1) packed in row order into blocks whose devices fit
   //      one CTA's shared memory; a node with more devices than that forms a

@@ -172,3 +172,135 @@ def test_packed_records_schedule_solves(product, name):
     if name == "config2":
         # nearly every pivot of the chain circuit keeps the recurrence in registers
         assert int(((rec[:, 0] >> 8) & 1).sum()) >= n // 2
+
+
+def run_schedule(sch, vals_nd, rhs_nd):
+    """The level schedule as the factor/solve kernel runs it, one level at a
+    time: pivot reciprocals, L values, update targets and right-hand-side rows,
+    then the back substitution from the last level down."""
+    A = vals_nd.copy()
+    y = rhs_nd.copy()
+    lp, diag = sch["lv_piv_ptr"], sch["nd_diag"]
+    for lv in range(sch["levels"]):
+        piv = sch["lv_piv"][lp[lv]:lp[lv + 1]]
+        A[diag[piv]] = 1.0 / A[diag[piv]]
+        e0, e1 = sch["lv_l_ptr"][lv], sch["lv_l_ptr"][lv + 1]
+        ls = sch["l_slot"][e0:e1]
+        A[ls] = A[ls] * A[diag[sch["l_piv"][e0:e1]]]
+        for t in range(sch["lv_ts_ptr"][lv], sch["lv_ts_ptr"][lv + 1]):
+            q0, q1 = sch["t_off"][t], sch["t_off"][t + 1]
+            A[sch["t_slot"][t]] -= np.dot(A[sch["pr_l"][q0:q1]], A[sch["pr_u"][q0:q1]])
+        for r in range(sch["lv_ys_ptr"][lv], sch["lv_ys_ptr"][lv + 1]):
+            q0, q1 = sch["y_off"][r], sch["y_off"][r + 1]
+            y[sch["y_row"][r]] -= np.dot(A[sch["yp_l"][q0:q1]], y[sch["yp_k"][q0:q1]])
+    for lv in range(sch["levels"] - 1, -1, -1):
+        for k in sch["lv_piv"][lp[lv]:lp[lv + 1]]:
+            b0, b1 = sch["bs_off"][k], sch["bs_off"][k + 1]
+            y[k] = (y[k] - np.dot(A[sch["bs_u"][b0:b1]], y[sch["bs_c"][b0:b1]])) * A[diag[k]]
+    return y
+
+
+@pytest.mark.parametrize("name", list(ALL))
+def test_level_schedule_solves(product, name):
+    nl = ALL[name]()
+    prob = product.Problem(None, nl)
+    sch = prob.lu_schedule()
+    if sch is None:
+        pytest.skip("no level schedule")
+    hdr, _, rc = prob.lu_program()
+    n, nv = prob.n, prob.info["n_slots"]
+    perm = sch["nd_perm"]
+    assert sorted(perm) == list(range(n)) and sch["n"] == n
+    # the long-list threshold splits every level's targets and rows
+    assert (sch["lv_ts_ptr"][1:] >= sch["lv_tl_ptr"][:-1]).all()
+    # no pivot of a level writes what another pivot of the same level reads
+    level = np.zeros(n, int)
+    for lv in range(sch["levels"]):
+        level[sch["lv_piv"][sch["lv_piv_ptr"][lv]:sch["lv_piv_ptr"][lv + 1]]] = lv
+    owner = np.repeat(np.arange(n), np.diff(sch["bs_off"]))
+    assert (level[sch["bs_c"]] > level[owner]).all()  # U columns are solved in later levels
+    rng = np.random.default_rng(9)
+    for _ in range(3):
+        vals = rng.uniform(-1.0, 1.0, nv)
+        dense = np.zeros((n, n))
+        dense[rc[:, 0], rc[:, 1]] = vals
+        for k in range(n):
+            s = hdr[k, 3]
+            vals[s] = np.sign(vals[s] or 1.0) * (1.0 + np.abs(dense[k]).sum() + np.abs(dense[:, k]).sum())
+        dense[rc[:, 0], rc[:, 1]] = vals
+        rhs = rng.uniform(-1.0, 1.0, n)
+        src = sch["nd_src"]
+        vals_nd = np.where(src >= 0, vals[np.maximum(src, 0)], 0.0)
+        y = run_schedule(sch, vals_nd, rhs[perm])
+        x = np.empty(n)
+        x[perm] = y
+        assert np.allclose(x, np.linalg.solve(dense, rhs), rtol=1e-10, atol=1e-12)
+
+
+def run_packed(prog, vals_mf, rhs_mf, n, n_slots):
+    """The packed schedule as the kernel reads it: gather the ND slots and the
+    right-hand side through the packed maps, then run every level."""
+    P = np.asarray(prog, np.int64) & 0xFFFFFFFF
+    lo = lambda v: int(v) & 0xFFFF
+    hi = lambda v: (int(v) >> 16) & 0xFFFF
+    half = lambda base, i: (int(P[base + i // 2]) >> (16 * (i & 1))) & 0xFFFF
+    nl, lvt, tpb, ypb, bpb, srcb, posb = (int(P[i]) for i in range(7))
+    A = np.array([0.0 if half(srcb, s) == 0xFFFF else vals_mf[half(srcb, s)] for s in range(n_slots)])
+    y = np.zeros(n)
+    for i in range(n):
+        y[half(posb, i)] = rhs_mf[i]
+    for lv in range(nl):
+        L = [int(P[lvt + 12 * lv + f]) for f in range(12)]
+        for q in range(L[1]):
+            d = int(P[L[0] + q])
+            A[d] = 1.0 / A[d]
+        for e in range(L[3]):
+            v = P[L[2] + e]
+            A[lo(v)] *= A[hi(v)]
+        for t in range(L[5] + L[6]):
+            h, off = P[L[4] + 2 * t], int(P[L[4] + 2 * t + 1])
+            for q in range(hi(h)):
+                pr = P[tpb + off + q]
+                A[lo(h)] -= A[lo(pr)] * A[hi(pr)]
+        for r in range(L[8] + L[9]):
+            h, off = P[L[7] + 2 * r], int(P[L[7] + 2 * r + 1])
+            for q in range(hi(h)):
+                pr = P[ypb + off + q]
+                y[lo(h)] -= A[lo(pr)] * y[hi(pr)]
+    for lv in range(nl - 1, -1, -1):
+        L = [int(P[lvt + 12 * lv + f]) for f in range(12)]
+        for q in range(L[11]):
+            a, b = P[L[10] + 2 * q], P[L[10] + 2 * q + 1]
+            k, d, cnt, off = lo(a), hi(a), lo(b), hi(b)
+            sv = y[k]
+            for j in range(cnt):
+                pr = P[bpb + off + j]
+                sv -= A[lo(pr)] * y[hi(pr)]
+            y[k] = sv * A[d]
+    x = np.empty(n)
+    for i in range(n):
+        x[i] = y[half(posb, i)]
+    return x
+
+
+@pytest.mark.parametrize("name", list(ALL))
+def test_packed_level_program_solves(product, name):
+    nl = ALL[name]()
+    prob = product.Problem(None, nl)
+    sch = prob.lu_schedule()
+    if sch is None or len(sch["nd_prog"]) == 0:
+        pytest.skip("no packed level program")
+    hdr, _, rc = prob.lu_program()
+    n, nv = prob.n, prob.info["n_slots"]
+    assert int(sch["nd_prog"][7]) == len(sch["nd_prog"])
+    rng = np.random.default_rng(13)
+    vals = rng.uniform(-1.0, 1.0, nv)
+    dense = np.zeros((n, n))
+    dense[rc[:, 0], rc[:, 1]] = vals
+    for k in range(n):
+        s = hdr[k, 3]
+        vals[s] = np.sign(vals[s] or 1.0) * (1.0 + np.abs(dense[k]).sum() + np.abs(dense[:, k]).sum())
+    dense[rc[:, 0], rc[:, 1]] = vals
+    rhs = rng.uniform(-1.0, 1.0, n)
+    x = run_packed(sch["nd_prog"], vals, rhs, n, sch["n_slots"])
+    assert np.allclose(x, np.linalg.solve(dense, rhs), rtol=1e-10, atol=1e-12)
