@@ -912,6 +912,15 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+// Asynchronous copy of one 4- or 8-byte element; with valid = false nothing
+// is read and the destination is zero-filled.
+template <int B>
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(B),
+               "r"(valid ? B : 0)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
@@ -926,13 +935,14 @@ __device__ __forceinline__ int nd_half(const int* prog, int base, int i) {
 // the pivots' reciprocals, then their L values, then the update targets and
 // right-hand-side rows (lists longer than Topology::kNdLong summed by the
 // whole warp, partials combined in a fixed tree); then the back substitution
-// from the last level down. A and y are this instance's ND slots and
-// right-hand side (ND order); y returns the solution. Same failure tests as
+// from the last level down. A and y are this instance's ND slots (without
+// the gmin diagonal, added to each pivot as it is taken) and right-hand side
+// (ND order); y returns the solution. Same failure tests as
 // lu_solve: tiny or non-finite pivots, non-finite solutions, multipliers
 // above growth_limit.
 template <typename T>
 __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __restrict__ prog,
-                         T tiny, T growth_limit, int lane) {
+                         T gmin, T tiny, T growth_limit, int lane) {
   const int NL = prog[0], lvt = prog[1], tpb = prog[2], ypb = prog[3], bpb = prog[4];
   bool ok = true;
   T lmax = T(0);
@@ -941,7 +951,7 @@ __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __rest
     const int po = Lt[0], pc = Lt[1], lo = Lt[2], lc = Lt[3];
     for (int q = lane; q < pc; q += 32) {
       const int d = prog[po + q];
-      const T piv = A[d];
+      const T piv = A[d] + gmin;  // the gmin diagonal joins at the pivot step
       ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
       A[d] = recip(piv);
     }
@@ -1099,37 +1109,65 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
   }
   if (!__syncthreads_or(my_live)) return;
 
+  // 1b. level schedule: the instances' ND slots start streaming into shared
+  //     memory now (asynchronous copies, a warp per slot, a lane per
+  //     instance) and land while the vectors are updated
+  if (nd) {
+    int anys = 0;
+    for (int q = 0; q < L; ++q) anys |= s_act[q] & ACT_SOLVE;
+    const int lw = tid & 31;
+    if (anys && lw < L) {
+      const T* J = reinterpret_cast<const T*>(I.J);
+      const int S = Tp.nd_S, nw = blockDim.x >> 5;
+      T* dst = A + lw * S;
+      const T* srcb = J + base + lw;
+      const bool inst = lw < cnt;
+#pragma unroll 4
+      for (int sl = tid >> 5; sl < Tp.nd_nv; sl += nw) {
+        const int src = nd_half(prog, prog[5], sl);
+        const bool valid = inst && src != 0xFFFF;
+        cp_async_elem<sizeof(T)>(dst + sl, valid ? srcb + (size_t)src * ld : J, valid);
+      }
+    }
+  }
+
   // 2. vector updates and the right-hand side of the instances that solve
   const int a = s_act[lane];
   int any_solve = 0;
   if (a) {
     const double gmin = s_gmin[lane];
+    double* __restrict__ X = I.x;
+    double* __restrict__ V = I.v;
+    double* __restrict__ VT = I.v_tp;
+    const double* __restrict__ F = I.F;
+#pragma unroll 2
     for (int i = row; i < n; i += R) {
       const size_t o = (size_t)i * ld + g;
+      const double fi = F[o];
       double vi;
       if (a & ACT_RESTART) {
-        vi = I.v_tp[o];
-        I.v[o] = vi;
-        I.x[o] = vi;
+        vi = VT[o];
+        V[o] = vi;
+        X[o] = vi;
       } else if (a & ACT_RESEED) {
-        vi = I.v[o];
-        I.x[o] = vi;
+        vi = V[o];
+        X[o] = vi;
       } else {
-        double xi = I.x[o];
-        vi = I.v[o];
+        double xi = X[o];
+        vi = V[o];
         if (a & ACT_DAMP) {
           xi = vi + 0.5 * (xi - vi);
-          I.x[o] = xi;
+          X[o] = xi;
         }
         if (a & ACT_ACCEPT) {
           vi = xi;
-          I.v[o] = vi;
+          V[o] = vi;
         }
-        if (a & (ACT_STEP | ACT_TRAN_INIT)) I.v_tp[o] = vi;
+        if (a & (ACT_STEP | ACT_TRAN_INIT)) VT[o] = vi;
       }
       if (a & ACT_SOLVE)
         Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane] =
-            (T)(-(I.F[o] + gmin * vi));
+            (T)(-(fi + gmin * vi));
     }
     any_solve = (a & ACT_SOLVE) != 0;
   }
@@ -1140,15 +1178,7 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
     const T* J = reinterpret_cast<const T*>(I.J);
     const int row_bytes = L * (int)sizeof(T);
     if (nd) {
-      // gather each instance's ND slots (consecutive threads: consecutive
-      // instances of one slot, so the global reads are contiguous)
-      const int S = Tp.nd_S, total = Tp.nd_nv * L;
-#pragma unroll 4
-      for (int e = tid; e < total; e += blockDim.x) {
-        const int sl = e / L, w = e - sl * L;
-        const int src = nd_half(prog, prog[5], sl);
-        A[w * S + sl] = (src != 0xFFFF && w < cnt) ? J[(size_t)src * ld + base + w] : T(0);
-      }
+      // issued in 1b
     } else if (row_bytes % 16 == 0) {
       const int cpr = row_bytes / 16;  // 16-byte chunks per slot row
       const int chunks = nv * cpr;
@@ -1196,13 +1226,10 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
   if (any_solve) {
     if (a & ACT_SOLVE) {
       const T gmin = (T)s_gmin[lane];
-      if (nd)
-        for (int i = row; i < n; i += R)
-          A[lane * Tp.nd_S + __ldg(&Tp.nd_diag[nd_half(prog, prog[6], i)])] += gmin;
-      else
+      if (!nd)
         for (int i = row; i < n; i += R) A[__ldg(&Tp.lu_hdr[i].w) * L + lane] += gmin;
     }
-    __syncthreads();
+    if (!nd) __syncthreads();
 
     // 3. factor + solve: one warp per instance on the level schedule, else
     //    one lane per instance on the pivot program
@@ -1212,7 +1239,7 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
       const int w = tid >> 5;
       if (w < L && (s_act[w] & ACT_SOLVE)) {
         const bool okw = nd_solve<T>(A + (size_t)w * Tp.nd_S, Y + (size_t)w * Tp.nd_SY, prog,
-                                     tiny, growth, tid & 31);
+                                     (T)s_gmin[w], tiny, growth, tid & 31);
         if ((tid & 31) == 0) s_sing[w] = okw ? 0 : 1;
       }
     } else if (tid < L && (s_act[tid] & ACT_SOLVE)) {
@@ -1223,13 +1250,17 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
     // 4. x = v + dx, then junction limiting level by level
     const bool upd = (a & ACT_SOLVE) && !s_sing[lane];
     const bool sanitize = (a & ACT_LIMIT) != 0;
-    if (upd)
+    if (upd) {
+      double* __restrict__ X = I.x;
+      const double* __restrict__ V = I.v;
+#pragma unroll 2
       for (int i = row; i < n; i += R) {
         const size_t o = (size_t)i * ld + g;
-        double xi = I.v[o] + (double)Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane];
+        double xi = V[o] + (double)Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane];
         if (sanitize && !isfinite(xi)) xi = 0.0;  // SafeUtils::sanitize_vector
-        I.x[o] = xi;
+        X[o] = xi;
       }
+    }
     if (Tp.n_dio > 0) {
       const int lim = upd && sanitize;
       if (__syncthreads_or(lim)) {
