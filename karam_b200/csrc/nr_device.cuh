@@ -724,7 +724,7 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
 // holds: the supply node and its diagonal) walk their devices in chunks of
 // KES_MAX_DEV, a group of them sharing one walk and all warps sharing the sums.
 template <typename TJ>
-__global__ void __launch_bounds__(256) k_es(DevTopo T, DevInst I, JobParams P) {
+__global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P) {
   __shared__ double s_dev[KES_MAX_DEV * 3 * 32];
   __shared__ unsigned long long s_f[8][32], s_dv[8][32];
   __shared__ int s_fl[8][32];
