@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--seeder-batches", type=int, default=SEEDER_BATCHES,
                     help="batches of plain-NR DC solutions the learned seeder trains on (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the config-1 latency and config-5 seeder measurements")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--max-rounds", type=int, default=0,
                     help="stop every job after this many NR rounds (profiling captures of a "
@@ -527,6 +529,9 @@ def run_karam(args, dist):
         "clocks": clk,
     }
 
+    if dist.rank == 0 and dist.world == 1 and not args.no_configs:
+        line["config1"] = config1_latency(ctx)
+        line["config5"] = config5_seeder(ctx)
     if dist.rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
@@ -543,6 +548,113 @@ def run_karam(args, dist):
     seeder.close()
     prob.close()
     ctx.close()
+
+
+def config1_latency(ctx, reps=50):
+    """Config 1: plain FP64 DC operating point of the 32-stage chain (VIN 0.9 V),
+    single instance, no seed, no batching: latency per solve through the C ABI
+    (host wall clock per call, and the device time of the job), NR iterations
+    beside the reference-built oracle's."""
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+    from karam_b200 import circuits
+    from oracle import pyoracle
+    nl = circuits.config1()
+    prob = K.Problem(ctx, nl, max_instances=1)
+    prob.set_instances(None)
+    opts = K.options(precision=A.PREC_FP64)
+    for _ in range(3):
+        prob.solve_dc(opts)
+    wall, dev = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        v, st = prob.solve_dc(opts)
+        wall.append(time.perf_counter() - t0)
+        dev.append(prob.timing()["job_ms"])
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    with native_stdout_to_stderr():
+        v_ref, st_ref = pyoracle.Oracle(kind).solve_dc(nl)
+    prob.close()
+    return {"workload": "32-stage inverter chain, VIN 0.9 V, n=34; plain FP64 DC, 1 instance",
+            "us_per_solve_wall": 1e6 * statistics.median(wall),
+            "us_per_solve_device": 1e3 * statistics.median(dev),
+            "iterations": st[0]["iterations"], "iterations_oracle": st_ref["iterations"],
+            "converged": st[0]["status"] == A.ST_CONVERGED,
+            "max_abs_diff_vs_oracle_v": float(np.max(np.abs(v[0] - v_ref)))}
+
+
+def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10):
+    """Config 5: the learned seeder on the inverter-chain family (256 stages,
+    VIN 0.9 V) with VDD ~ U(1.2, 2.0) and the MC device variation: trained on
+    plain-NR DC solutions of n_train instances, evaluated on n_test held-out
+    instances against a plain start (reference seed + GMIN stepping): NR
+    iterations, solves/s and the fallback rate. VDD draws: numpy PCG64 seeded
+    by the batch's first instance id."""
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+    from karam_b200 import circuits
+    nl = circuits.inverter_chain(stages=256, vdd=1.8, vin=0.9)
+
+    def instances(first, n):
+        inst = circuits.mc_instances(nl, n, first_instance=first)
+        vdd = np.random.default_rng(first).uniform(1.2, 2.0, n)
+        inst.vs_dc = np.stack([vdd, np.full(n, 0.9)], axis=1)
+        return inst
+
+    prob = K.Problem(ctx, nl, max_instances=batch)
+    plain = K.options(precision=A.PREC_MIXED, **POLISH)
+    t0 = time.perf_counter()
+    seeder = K.Seeder(prob, width=512, hidden_layers=3, init_seed=5)
+    added = 0
+    for b in range(n_train // batch):
+        prob.set_instances(instances(2_000_000 + b * batch, batch))
+        prob.solve_dc(plain)
+        added += seeder.add_dc(prob)
+    t1 = time.perf_counter()
+    loss = seeder.train(epochs=epochs, batch=256, lr=1e-3, shuffle_seed=7)
+    t2 = time.perf_counter()
+    prob.set_seeder(seeder)
+    seeded = K.options(precision=A.PREC_MIXED, seeded=A.SEED_MLP, **POLISH)
+    res = {"plain": {"ms": 0.0, "it": [], "conv": 0}, "seeded": {"ms": 0.0, "it": [], "conv": 0}}
+    fallbacks = 0
+    err = []
+    diff = 0.0
+    for b in range(n_test // batch):
+        prob.set_instances(instances(3_000_000 + b * batch, batch))
+        v0, st0 = prob.solve_dc(plain)
+        res["plain"]["ms"] += prob.timing()["job_ms"]
+        guess = seeder.predict(prob)
+        v1, st1 = prob.solve_dc(seeded)
+        res["seeded"]["ms"] += prob.timing()["job_ms"]
+        for k, st in (("plain", st0), ("seeded", st1)):
+            res[k]["it"] += [s["iterations"] + s["polish_iters"] for s in st]
+            res[k]["conv"] += sum(s["status"] == A.ST_CONVERGED for s in st)
+        fallbacks += sum(1 for s in st1 if not s["seeded_ok"])
+        ok = [i for i, (a, c) in enumerate(zip(st0, st1))
+              if a["status"] == A.ST_CONVERGED and c["status"] == A.ST_CONVERGED]
+        err += np.max(np.abs(guess[ok] - v0[ok]), axis=1).tolist()
+        diff = max(diff, float(np.max(np.abs(v1[ok] - v0[ok]) / (1e-9 * np.abs(v0[ok]) + 1e-12))))
+    prob.set_seeder(None)
+    seeder.close()
+    n_out = prob.n
+    prob.close()
+    out = {"workload": "256-stage inverter chain, VIN 0.9 V, VDD ~ U(1.2, 2.0) + MC VTO/KP; DC",
+           "network": f"MLP {2 * len(nl.mos) + len(nl.vsrc)}-512-512-512-{n_out} (GELU), "
+                      "BF16 weights, FP32 accumulation, Adam/MSE",
+           "train_solutions": added, "train_data_s": t1 - t0, "train_s": t2 - t1,
+           "epochs": epochs, "final_loss": loss, "heldout": n_test,
+           "fallback_rate": fallbacks / n_test,
+           "seed_err_median_v": float(np.median(err)), "seed_err_max_v": float(np.max(err)),
+           "max_scaled_diff_seeded_vs_plain": diff,
+           "scaled": "|dv| / (1e-9 |v| + 1e-12 V) over instances converged both ways"}
+    for k in ("plain", "seeded"):
+        it = np.array(res[k]["it"])
+        out[k] = {"solves_per_s": res[k]["conv"] / (res[k]["ms"] / 1e3),
+                  "nr_iterations_mean": float(it.mean()), "nr_iterations_p99": float(np.percentile(it, 99)),
+                  "converged": res[k]["conv"]}
+    return out
 
 
 def accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64, sample=6):
