@@ -180,6 +180,11 @@ typedef struct karam_solver_opts {
   int32_t max_halvings;  /* transient: a step whose NR exhausts max_nr_iter restarts
                             from the last time point with half the step, at most
                             this many times (reference attempt loop: 3)          */
+  int32_t kernel_timing; /* 1: CUDA events around every kernel of every round, summed
+                            into karam_timing's eval_ms / lu_ms / rescue_ms. The
+                            event records slow a round down (B200, config 2:
+                            ~24 us of a ~160 us round), so 0 (the default) leaves
+                            them out and those three fields at 0               */
 } karam_solver_opts;
 
 /* Sizes of the symbolic analysis of a problem. */
@@ -385,13 +390,17 @@ KARAM_API int karam_eval_stamp_noalloc(karam_problem *p, int32_t precision, cons
 typedef struct karam_timing {
   double job_ms;            /* first kernel of the call to its last one             */
   double eval_ms;           /* summed duration of the device evaluation + stamping
-                               launches (one per round)                             */
+                               launches (one per round; solves: 0 unless
+                               opts.kernel_timing)                                   */
   double lu_ms;             /* summed duration of the control flow + factor/solve
-                               launches (one per round)                             */
-  double rescue_ms;         /* summed duration of the rescue launches (one per round) */
+                               launches (one per round; 0 unless opts.kernel_timing) */
+  double rescue_ms;         /* summed duration of the rescue launches (one per round;
+                               0 unless opts.kernel_timing)                          */
   int32_t rounds;           /* NR rounds                                             */
   int32_t eval_launches, lu_launches, rescue_launches, other_launches;
   int32_t lanes;            /* instances per CTA of the factor/solve kernel          */
+  int32_t level_schedule;   /* 1 when the factor/solve kernel ran the level-scheduled
+                               LU (k_lu_nd), 0 for the pivot-record LU (k_lu)         */
   int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */

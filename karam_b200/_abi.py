@@ -63,7 +63,7 @@ class KaramSolverOpts(C.Structure):
         ("kcl_tol", C.c_double), ("polish_max", C.c_int32), ("polish_rel", C.c_double),
         ("polish_abs", C.c_double), ("lu_growth_limit", C.c_double), ("seeded", C.c_int32),
         ("seed_max_iter", C.c_int32), ("schedule", C.c_int32), ("max_rounds", C.c_int32),
-        ("max_halvings", C.c_int32),
+        ("max_halvings", C.c_int32), ("kernel_timing", C.c_int32),
     ]
 
 
@@ -87,7 +87,8 @@ class KaramTiming(C.Structure):
                 ("rescue_ms", C.c_double), ("rounds", C.c_int32), ("eval_launches", C.c_int32),
                 ("lu_launches", C.c_int32), ("rescue_launches", C.c_int32),
                 ("other_launches", C.c_int32),
-                ("lanes", C.c_int32), ("evals_dc", C.c_int64), ("evals_tran", C.c_int64),
+                ("lanes", C.c_int32), ("level_schedule", C.c_int32),
+                ("evals_dc", C.c_int64), ("evals_tran", C.c_int64),
                 ("solves", C.c_int64), ("rescues", C.c_int64),
                 ("rescues_dense", C.c_int64)]
 

@@ -529,14 +529,20 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
   return P;
 }
 
-// Runs NR rounds until every instance is done (or the round budget ends).
-// Rounds (k_eval, k_stamp, k_lu, k_rescue) are captured in a CUDA graph of
-// kRounds rounds with event records between the phases; the last k_lu of the
-// graph counts the live instances into d_active, which is read back after
-// every replay.
-void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_lanes,
+// Runs NR rounds until every instance is done (or opts->max_rounds ends).
+// Rounds (k_es, k_lu, k_rescue) are captured in a CUDA graph of kRounds
+// rounds; the last k_lu of the graph counts the live instances into d_active,
+// which is read back after every replay. k_es resets the rescue counter of its
+// round, so the graph holds kernels only (and one memset per replay). With
+// opts->kernel_timing, event records between the kernels time each of them;
+// they are left out otherwise, since they cost more than the empty launches
+// of a round.
+void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* opts,
                 const DevInst* inst = nullptr) {
   constexpr int kRounds = 16;
+  const int max_rounds = opts ? opts->max_rounds : 0;
+  const int want_lanes = opts ? opts->schedule : 0;
+  const bool timed = opts && opts->kernel_timing;
   cudaStream_t s = p->ctx->stream;
   DevInst I = inst ? *inst : dev_inst(p);
   const int prec = P.precision;
@@ -545,7 +551,8 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_l
     throw std::runtime_error("one instance's matrix does not fit the shared memory of a CTA");
   ck(cudaGetLastError(), "configure kernels");
   p->timing.lanes = L.L;
-  std::vector<cudaEvent_t> ev(4 * kRounds);
+  p->timing.level_schedule = L.nd ? 1 : 0;
+  std::vector<cudaEvent_t> ev(timed ? 4 * kRounds : 0);
   for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
   struct EvGuard {
     std::vector<cudaEvent_t>& v;
@@ -572,17 +579,16 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_l
   };
   for (int r = 0; r < kRounds; ++r) {
     if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
-    if (I.rescue_count) cudaMemsetAsync(I.rescue_count, 0, sizeof(int), s);
-    cudaEventRecordWithFlags(ev[4 * r], s, cudaEventRecordExternal);
+    if (timed) cudaEventRecordWithFlags(ev[4 * r], s, cudaEventRecordExternal);
     launch_eval_stamp(p->dt, I, P, L, prec, s);
     check("k_es launch");
-    cudaEventRecordWithFlags(ev[4 * r + 1], s, cudaEventRecordExternal);
+    if (timed) cudaEventRecordWithFlags(ev[4 * r + 1], s, cudaEventRecordExternal);
     launch_lu(p->dt, I, P, L, prec, active, s);
     check("k_lu launch");
-    cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
+    if (timed) cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
     if (I.rescue_list) launch_rescue(p->dt, I, P, p->rplan, s);
     check("k_rescue launch");
-    cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
+    if (timed) cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
   }
   const cudaError_t end_err = cudaStreamEndCapture(s, &graph);
   ck(launch_err, failed ? failed : "kernel launch in capture");
@@ -602,7 +608,7 @@ void run_rounds(karam_problem* p, const JobParams& P, int max_rounds, int want_l
     ck(cudaGraphLaunch(exec, s), "graph launch");
     ck(cudaMemcpyAsync(p->h_active, active, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
     ck(cudaStreamSynchronize(s), "round sync");
-    for (int r = 0; r < kRounds; ++r) {
+    for (int r = 0; r < kRounds && timed; ++r) {
       float a = 0, b = 0, c = 0;
       ck(cudaEventElapsedTime(&a, ev[4 * r], ev[4 * r + 1]), "event time");
       ck(cudaEventElapsedTime(&b, ev[4 * r + 1], ev[4 * r + 2]), "event time");
@@ -735,7 +741,7 @@ JobParams ema_seed(karam_problem* p, JobParams P, const karam_solver_opts* opts)
   p->ni = KARAM_SEED_HISTORY;
   try {
     start_job(p, P1, nullptr);
-    run_rounds(p, P1, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
+    run_rounds(p, P1, opts);
   } catch (...) {
     p->ni = N;
     throw;
@@ -881,7 +887,7 @@ int karam_solve_dc(karam_problem* p, const karam_solver_opts* opts, const double
     begin_job(p);
     if (P.seeded == KARAM_SEED_EMA) P = ema_seed(p, P, opts);
     start_job(p, P, seed_v);
-    run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
+    run_rounds(p, P, opts);
     end_job(p);
     p->have_dc = true;
     read_voltages(p, out_v);
@@ -901,7 +907,7 @@ int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double 
     begin_job(p);
     if (P.seeded == KARAM_SEED_EMA) P = ema_seed(p, P, opts);
     start_job(p, P, nullptr);
-    run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0);
+    run_rounds(p, P, opts);
     end_job(p);
     p->have_dc = true;
     return KARAM_OK;
@@ -964,7 +970,7 @@ int karam_step_transient(karam_problem* p, const karam_solver_opts* opts, double
     launch_tran_start(p->dt, I, P, p->tran_started ? 0 : 1, p->ctx->stream);
     ck(cudaGetLastError(), "tran start");
     p->timing.other_launches += 1;
-    run_rounds(p, P, opts ? opts->max_rounds : 0, opts ? opts->schedule : 0, &I);
+    run_rounds(p, P, opts, &I);
     end_job(p);
     p->tran_started = true;
     p->tran_h = dt;

@@ -732,6 +732,9 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
   const int g = blockIdx.x * 32 + lane;
   const size_t ld = I.ld;
   const int nv = T.nv;
+  // this round's rescue list starts empty (the previous round's k_rescue has
+  // finished; this round's k_lu appends to it)
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && I.rescue_count) *I.rescue_count = 0;
   const double heff = g < I.ni ? I.ev_heff[g] : -1.0;
   const bool live = heff >= 0.0;
   if (!__syncthreads_or(live)) return;
