@@ -85,7 +85,7 @@ struct karam_problem {
   DBuf t_mos_term, t_mos_geo, t_mos_pmos, t_dio_term, t_dio_par, t_res_term, t_res_g, t_cap_term,
       t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
-      t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
+      t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_es_hubc, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
       t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent;
   DBuf t_nd[23];  // level schedule tables, in karam_get_lu_schedule's order
   DBuf t_nd_prog;  // the packed schedule (padded to whole int4)
@@ -94,7 +94,7 @@ struct karam_problem {
   int ld = 0;
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
-      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok;
+      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
@@ -233,6 +233,7 @@ void upload_topology(karam_problem* p) {
       return o;
     };
     upload(p->t_es_block, int4s(T.es_block));
+    upload(p->t_es_hubc, int4s(T.es_hubc));
     upload(p->t_es_item, int4s(T.es_item));
     upload(p->t_es_ft, int4s(T.es_ft));
   }
@@ -308,6 +309,9 @@ void upload_topology(karam_problem* p) {
   d.es_ft = p->t_es_ft.as<int4>();
   d.es_fc = p->t_es_fc.as<double>();
   d.es_hub = p->t_es_hub.as<int>();
+  d.es_hubc = p->t_es_hubc.as<int4>();
+  d.n_hub_groups = T.n_hub_groups;
+  d.n_hub_rows = T.n_hub_rows;
   d.lu_hdr = p->t_lu_hdr.as<int4>();
   d.lu_data = p->t_lu_data.as<int>();
   d.lu_small = T.lu_small ? 1 : 0;
@@ -374,6 +378,10 @@ void alloc_instances(karam_problem* p) {
   p->i_redfl.alloc(ld * sizeof(int));
   p->i_evt.alloc(ld * sizeof(double));
   p->i_evh.alloc(ld * sizeof(double));
+  p->i_hub_part.alloc(std::max<size_t>(1, ld * (size_t)T.n_hub_rows) * sizeof(double));
+  p->i_hub_cnt.alloc(std::max<size_t>(1, ld / 32 * (size_t)T.n_hub_groups) * sizeof(int));
+  ck(cudaMemset(p->i_hub_cnt.p, 0, std::max<size_t>(1, ld / 32 * (size_t)T.n_hub_groups) * sizeof(int)),
+     "memset hub counters");
   {
     // lanes beyond the batch never evaluate
     std::vector<double> neg(ld, -1.0);
@@ -441,6 +449,8 @@ DevInst dev_inst(karam_problem* p) {
   I.rescue_list = p->rescue_slots > 0 ? p->r_list.as<RescueItem>() : nullptr;
   I.rescue_count = p->rescue_slots > 0 ? p->r_count.as<int>() : nullptr;
   I.rescue_slots = p->rescue_slots;
+  I.hub_part = p->i_hub_part.as<double>();
+  I.hub_cnt = p->i_hub_cnt.as<int>();
   I.counters = p->d_counters.as<unsigned long long>();
   I.wave = nullptr;
   I.wave_pos = nullptr;
@@ -1144,7 +1154,7 @@ int karam_eval_stamp_noalloc(karam_problem* p, int32_t precision, const double* 
     if (precision != KARAM_PREC_FP64 && precision != KARAM_PREC_MIXED)
       throw std::runtime_error("unknown precision");
     const Topology& T = p->topo;
-    const size_t need = noalloc_bytes(T.n, T.nv, T.nnz(), p->ld);
+    const size_t need = noalloc_bytes(T.n, T.nv, T.nnz(), p->ld, T.n_hub_rows, T.n_hub_groups);
     if (need > kScratchBytes)
       throw std::runtime_error("karam_eval_stamp_noalloc: this problem needs " +
                                std::to_string(need) + " bytes of scratch, the fixed maximum is " +

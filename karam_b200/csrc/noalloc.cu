@@ -11,6 +11,7 @@
 // process exits.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -32,9 +33,10 @@ std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
 
 // Lanes of the batch start at a DC point; lanes past it never evaluate; the
-// reductions start neutral.
-__global__ void k_noalloc_init(DevInst I) {
+// reductions start neutral, the hub chunk counters at 0.
+__global__ void k_noalloc_init(DevInst I, int hub_cnt_len) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < hub_cnt_len) I.hub_cnt[g] = 0;
   if (g >= I.ld) return;
   I.ev_t[g] = 0.0;
   I.ev_heff[g] = g < I.ni ? 0.0 : -1.0;
@@ -85,10 +87,11 @@ void* noalloc_scratch(int device, const char** err) {
   return g_addr[device];
 }
 
-size_t noalloc_bytes(int n, int nv, int nnz, int ld) {
+size_t noalloc_bytes(int n, int nv, int nnz, int ld, int hub_rows, int hub_groups) {
   const size_t L = (size_t)ld;
   return up256(8 * (size_t)n * L) * 2 + up256(8 * (size_t)nv * L) + up256(8 * L) * 4 +
-         up256(4 * L) + up256(4 * (size_t)nnz);
+         up256(4 * L) + up256(4 * (size_t)nnz) + up256(8 * (size_t)hub_rows * L) +
+         up256(4 * (size_t)hub_groups * (L / 32));
 }
 
 cudaError_t noalloc_eval_stamp(void* scratch, const DevTopo& T, DevInst I, int prec,
@@ -110,6 +113,9 @@ cudaError_t noalloc_eval_stamp(void* scratch, const DevTopo& T, DevInst I, int p
   auto* rd = reinterpret_cast<unsigned long long*>(take(8 * L));
   int* rfl = reinterpret_cast<int*>(take(4 * L));
   int* csr = reinterpret_cast<int*>(take(4 * (size_t)nnz));
+  double* hub_part = reinterpret_cast<double*>(take(8 * (size_t)T.n_hub_rows * L));
+  const int hub_cnt_len = T.n_hub_groups * (int)(L / 32);
+  int* hub_cnt = reinterpret_cast<int*>(take(4 * (size_t)hub_cnt_len));
   // every instance evaluates a DC point; v is only read for the convergence
   // measures the stamping kernel folds, which this call does not report
   I.x = x;
@@ -124,11 +130,14 @@ cudaError_t noalloc_eval_stamp(void* scratch, const DevTopo& T, DevInst I, int p
   I.seed = nullptr;
   I.counters = nullptr;
   I.wave = nullptr;
+  I.rescue_count = nullptr;
+  I.hub_part = hub_part;
+  I.hub_cnt = hub_cnt;
   cudaError_t e = cudaMemcpyAsync(csr, h_csr_slot, sizeof(int) * (size_t)nnz,
                                   cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   interleave(d_v, perm, x, I.ni, I.ld, T.n, s);
-  k_noalloc_init<<<(I.ld + 255) / 256, 256, 0, s>>>(I);
+  k_noalloc_init<<<(std::max(I.ld, hub_cnt_len) + 255) / 256, 256, 0, s>>>(I, hub_cnt_len);
   JobParams P{};
   P.precision = prec;
   P.reltol = 1e-3;

@@ -17,8 +17,9 @@ constexpr size_t kScratchBytes = size_t(16) << 20;
 void* noalloc_scratch(int device, const char** err);
 
 // Scratch bytes one call needs for a topology of n unknowns, nv value slots,
-// nnz CSR entries and lane stride ld.
-size_t noalloc_bytes(int n, int nv, int nnz, int ld);
+// nnz CSR entries, hub_rows hub chunk partial rows and hub_groups hub groups,
+// at lane stride ld.
+size_t noalloc_bytes(int n, int nv, int nnz, int ld, int hub_rows, int hub_groups);
 
 // Evaluation + stamping of I's instances at d_v ([ni][n], node order, device)
 // into d_jac ([ni][nnz], CSR order) and d_f ([ni][n], node order), every

@@ -721,8 +721,9 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
 // KCL residual of each of its nodes (terms in node order), and folds max |F|,
 // max |x - v| and the convergence flags of its nodes into the instance's
 // reductions with one atomic each. Hub items (more devices than shared memory
-// holds: the supply node and its diagonal) walk their devices in chunks of
-// KES_MAX_DEV, a group of them sharing one walk and all warps sharing the sums.
+// holds: the supply node and its diagonal) have their devices split into
+// chunks of KES_MAX_DEV, one block per chunk; the last chunk block of a tile
+// to finish adds the chunks' sums.
 template <typename TJ>
 __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P) {
   __shared__ double s_dev[KES_MAX_DEV * 3 * 32];
@@ -804,67 +805,83 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
         }
       }
   } else {
-    // hub group: -blk.y items over one walk of the group's devices in chunks
-    // of KES_MAX_DEV; within a chunk the eight warps sum consecutive slices of
-    // each item's terms, and the per-warp partials are added in warp order at
-    // the end (a fixed order, so results do not vary from run to run)
+    // hub chunk block: chunk hc.x of a group of -blk.y hub items. The eight
+    // warps sum consecutive slices of each item's terms of this chunk, and the
+    // warp partials are added in warp order into the chunk's partial row. The
+    // group's chunk block of this tile that finishes last adds the rows in
+    // chunk order to the item's linear part (a fixed order, so results do not
+    // vary from run to run).
     const int nh = -blk.y;
-    const int nch = (blk.w + KES_MAX_DEV - 1) / KES_MAX_DEV;
+    const int4 hc = __ldg(&T.es_hubc[blockIdx.y]);
+    const int c = hc.x, nch = hc.y;
+    const int c0 = c * KES_MAX_DEV;
     double acc[KES_MAX_HUBS];
 #pragma unroll
     for (int m = 0; m < KES_MAX_HUBS; ++m) acc[m] = 0.0;
-    for (int c = 0; c < nch; ++c) {
-      const int c0 = c * KES_MAX_DEV;
-      const int cn = min(KES_MAX_DEV, blk.w - c0);
-      if (live)
-        for (int k = warp; k < cn; k += 16)
-          eval_device_pair(T, I, T.es_dev + blk.z + c0, k, cn, g, s_dev, lane);
-      __syncthreads();
-      if (live)
+    if (live)
+      for (int k = warp; k < blk.w; k += 16)
+        eval_device_pair(T, I, T.es_dev + blk.z, k, blk.w, g, s_dev, lane);
+    __syncthreads();
+    if (live)
 #pragma unroll
-        for (int m = 0; m < KES_MAX_HUBS; ++m) {
-          if (m >= nh) break;
-          const int4 it = __ldg(&T.es_item[blk.x + m]);
-          const int lo = __ldg(&T.es_hub[it.w + c]), hi = __ldg(&T.es_hub[it.w + c + 1]);
-          const int q0 = lo + (int)(((long long)(hi - lo) * warp) / 8);
-          const int q1 = lo + (int)(((long long)(hi - lo) * (warp + 1)) / 8);
-          if (it.x < nv) {
-            for (int q = it.y + q0; q < it.y + q1; ++q) {  // every slot term is a device term
-              const int cc = __ldg(&T.es_jt[q]);
-              const double val = sd[(code_idx(cc) - c0) * 96 + (code_kind(cc) == 0 ? 32 : 0)];
-              acc[m] = cc < 0 ? acc[m] - val : acc[m] + val;
-            }
-          } else {
-            for (int q = it.y + q0; q < it.y + q1; ++q) {
-              const int4 tm = __ldg(&T.es_ft[q]);
-              const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, c0);
-              acc[m] = tm.x < 0 ? acc[m] - cur : acc[m] + cur;
-            }
+      for (int m = 0; m < KES_MAX_HUBS; ++m) {
+        if (m >= nh) break;
+        const int4 it = __ldg(&T.es_item[blk.x + m]);
+        const int lo = __ldg(&T.es_hub[it.w + c]), hi = __ldg(&T.es_hub[it.w + c + 1]);
+        const int q0 = lo + (int)(((long long)(hi - lo) * warp) / 8);
+        const int q1 = lo + (int)(((long long)(hi - lo) * (warp + 1)) / 8);
+        if (it.x < nv) {
+          for (int q = it.y + q0; q < it.y + q1; ++q) {  // every slot term is a device term
+            const int cc = __ldg(&T.es_jt[q]);
+            const double val = sd[(code_idx(cc) - c0) * 96 + (code_kind(cc) == 0 ? 32 : 0)];
+            acc[m] = cc < 0 ? acc[m] - val : acc[m] + val;
+          }
+        } else {
+          for (int q = it.y + q0; q < it.y + q1; ++q) {
+            const int4 tm = __ldg(&T.es_ft[q]);
+            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, c0);
+            acc[m] = tm.x < 0 ? acc[m] - cur : acc[m] + cur;
           }
         }
-      __syncthreads();
-    }
-    // partials through shared memory (the device values are no longer needed)
+      }
+    __syncthreads();
+    // warp partials through shared memory (the device values are no longer needed)
     double* part = s_dev;  // [m][warp][32]
 #pragma unroll
     for (int m = 0; m < KES_MAX_HUBS; ++m)
       if (m < nh) part[(m * 8 + warp) * 32 + lane] = acc[m];
     __syncthreads();
     if (warp < nh && live) {
+      double sum = 0.0;
+      for (int w = 0; w < 8; ++w) sum += part[(warp * 8 + w) * 32 + lane];
+      I.hub_part[(size_t)(hc.w + warp * nch + c) * ld + g] = sum;
+      __threadfence();  // the row is visible before this block counts itself done
+    }
+    __syncthreads();
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+      int* ctr = I.hub_cnt + (size_t)hc.z * (ld / 32) + blockIdx.x;
+      const int done = atomicAdd(ctr, 1);
+      s_last = done == nch - 1;
+      if (done == nch - 1) *ctr = 0;  // every chunk block has counted: ready for the next launch
+    }
+    __syncthreads();
+    if (s_last && warp < nh && live) {
+      __threadfence();
       const int4 it = __ldg(&T.es_item[blk.x + warp]);
       double sum = 0.0;
       if (it.x < nv) {
         sum = __ldg(&T.jlin_dc[it.x]);
         if (tran) {
           const int q1 = __ldg(&T.jcap_off[it.x + 1]);
-          for (int c = __ldg(&T.jcap_off[it.x]); c < q1; ++c) {
-            const int cc = __ldg(&T.jcap_code[c]);
+          for (int q = __ldg(&T.jcap_off[it.x]); q < q1; ++q) {
+            const int cc = __ldg(&T.jcap_code[q]);
             const double gq = (2.0 * __ldg(&T.cap_c[code_idx(cc)])) / heff;
             sum = cc < 0 ? sum - gq : sum + gq;
           }
         }
       }
-      for (int w = 0; w < 8; ++w) sum += part[(warp * 8 + w) * 32 + lane];
+      for (int q = 0; q < nch; ++q) sum += __ldcg(&I.hub_part[(size_t)(hc.w + warp * nch + q) * ld + g]);
       if (it.x < nv)
         reinterpret_cast<TJ*>(I.J)[(size_t)it.x * ld + g] = (TJ)sum;
       else

@@ -100,8 +100,10 @@ struct DevTopo {
   const int* jcap_off;
   const int* jcap_code;
   // Evaluation + stamping blocks (see es_blocks in topology.cpp):
-  //   es_block[b] = {item offset, items (-1: hub node walked in device chunks),
-  //                  device offset, devices}
+  //   es_block[b] = {item offset, items (-h: chunk block of a group of h hub
+  //                  items), device offset, devices}
+  //   es_hubc[b]  = hub chunk blocks: {chunk, chunks of the group, group, first
+  //                 partial row of the group}
   //   es_item[k]  = {item (slot s < nv, node nv + i), term offset, terms,
   //                  hub items: offset of the item's chunk bounds in es_hub}
   //   es_dev      = global device ids (MOSFETs, then n_mos + diode index)
@@ -117,6 +119,8 @@ struct DevTopo {
   const int4* es_ft;
   const double* es_fc;
   const int* es_hub;        // hub items: term index where each device chunk starts, then the end
+  const int4* es_hubc;
+  int n_hub_groups, n_hub_rows;
   // LU program per pivot k: hdr = (off, nL, nU, diagonal slot); data at off =
   // Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots)
   const int4* lu_hdr;
@@ -176,6 +180,8 @@ struct DevInst {
   RescueItem* rescue_list;  // [ni]
   int* rescue_count;
   int rescue_slots;         // rescue warps (one workspace each)
+  double* hub_part;         // [n_hub_rows][ld] hub items' sums per device chunk
+  int* hub_cnt;             // [n_hub_groups][ld / 32] chunk blocks done (0 between launches)
   unsigned long long* counters;  // [5]: evaluations DC, evaluations transient, solves,
                                  // rescues, rescues that needed partial pivoting
   double* wave;             // [ni][wave_steps][n_wave] node voltages after each step

@@ -1017,6 +1017,9 @@ void es_blocks(Topology& T) {
   T.es_ft.clear();
   T.es_fc.clear();
   T.es_hub.clear();
+  T.es_hubc.clear();
+  T.n_hub_groups = 0;
+  T.n_hub_rows = 0;
   T.es_max_dev = kEsMaxDev;
   // device of a slot term / node term (-1: none)
   auto slot_dev = [&](int c) {
@@ -1061,6 +1064,7 @@ void es_blocks(Topology& T) {
     T.es_block.push_back((int)items.size());
     T.es_block.push_back((int)T.es_dev.size());
     T.es_block.push_back((int)dlist.size());
+    for (int k = 0; k < 4; ++k) T.es_hubc.push_back(0);
     T.es_dev.insert(T.es_dev.end(), dlist.begin(), dlist.end());
     for (int it : items) {
       T.es_item.push_back(it);
@@ -1118,11 +1122,14 @@ void es_blocks(Topology& T) {
   const size_t normal_blocks = T.es_block.size();
 
   // Hub items (the supply node and its diagonal slot): groups of up to
-  // kEsMaxHubs share one walk over the union of their devices in chunks of
-  // kEsMaxDev. The union is in first-occurrence order; a group is kept only
-  // if every item's device indices never decrease along its terms (so the
-  // terms of one chunk are contiguous and es_hub can bound them), otherwise
-  // each hub walks its own term occurrences.
+  // kEsMaxHubs share the union of their devices, split into chunks of
+  // kEsMaxDev with one block per chunk. Each chunk block sums the group's
+  // terms of its chunk into partial rows; the last block of the group to
+  // finish (per tile of 32 instances) adds the partials in chunk order. The
+  // union is in first-occurrence order; a group is kept only if every item's
+  // device indices never decrease along its terms (so the terms of one chunk
+  // are contiguous and es_hub can bound them), otherwise each hub forms a
+  // group of its own over its term occurrences.
   auto terms_of = [&](int it, std::vector<int>& out) {  // device per term, -1 = linear
     out.clear();
     if (it < nv) {
@@ -1134,12 +1141,20 @@ void es_blocks(Topology& T) {
   };
   auto emit_group = [&](const std::vector<int>& items, const std::vector<int>& dlist,
                         const std::vector<std::vector<int>>& lidx) {
-    T.es_block.push_back((int)T.es_item.size() / 4);
-    T.es_block.push_back(-(int)items.size());
-    T.es_block.push_back((int)T.es_dev.size());
-    T.es_block.push_back((int)dlist.size());
-    T.es_dev.insert(T.es_dev.end(), dlist.begin(), dlist.end());
     const int nch = ((int)dlist.size() + kEsMaxDev - 1) / kEsMaxDev;
+    for (int c = 0; c < nch; ++c) {
+      T.es_block.push_back((int)T.es_item.size() / 4);
+      T.es_block.push_back(-(int)items.size());
+      T.es_block.push_back((int)T.es_dev.size() + c * kEsMaxDev);
+      T.es_block.push_back(std::min(kEsMaxDev, (int)dlist.size() - c * kEsMaxDev));
+      T.es_hubc.push_back(c);
+      T.es_hubc.push_back(nch);
+      T.es_hubc.push_back(T.n_hub_groups);
+      T.es_hubc.push_back(T.n_hub_rows);
+    }
+    ++T.n_hub_groups;
+    T.n_hub_rows += (int)items.size() * nch;
+    T.es_dev.insert(T.es_dev.end(), dlist.begin(), dlist.end());
     for (size_t m = 0; m < items.size(); ++m) {
       const int it = items[m];
       T.es_item.push_back(it);
@@ -1228,6 +1243,7 @@ void es_blocks(Topology& T) {
   }
   // hub blocks run longest: put them first so the grid starts them first
   std::rotate(T.es_block.begin(), T.es_block.begin() + normal_blocks, T.es_block.end());
+  std::rotate(T.es_hubc.begin(), T.es_hubc.begin() + normal_blocks, T.es_hubc.end());
 }
 
 }  // namespace

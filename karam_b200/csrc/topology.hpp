@@ -119,8 +119,9 @@ struct Topology {
 
   // ---- evaluation + stamping blocks: the stamp items (value slots 0..nv-1,
   //      nodes nv..nv+n-1) packed in row order into blocks whose devices fit
-  //      one CTA's shared memory; a node with more devices than that forms a
-  //      block of its own that walks its devices in chunks ----
+  //      one CTA's shared memory; items with more devices than that (hubs)
+  //      form groups whose devices are split into chunks, one block per
+  //      chunk ----
   std::vector<int> ft_a, ft_b;              // per KCL term: element terminals (permuted, -1 ground)
   std::vector<double> ft_coef;              // 1/R, source amplitude, 2C or 0
   std::vector<int> es_block;                // 4 per block: item offset, items, device offset, devices
@@ -132,7 +133,11 @@ struct Topology {
   std::vector<double> es_fc;                // node term coefficients
   std::vector<int> es_hub;                  // per hub item: term index where each device
                                             // chunk starts, then the end (offset in es_item w)
+  std::vector<int> es_hubc;                 // 4 per block: chunk, chunks of the group, group,
+                                            // first partial row of the group (0s: not a hub block)
   int es_max_dev = 0;                       // devices per chunk (shared-memory budget)
+  int n_hub_groups = 0;                     // hub groups
+  int n_hub_rows = 0;                       // chunk partial rows: sum over groups of items x chunks
 
   // ---- junction limiting (SoA diode order) ----
   std::vector<double> dio_lim;  // 2 per diode: Vt * T/Tnom, vcrit
