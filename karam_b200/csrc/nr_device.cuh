@@ -1082,6 +1082,7 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
     for (int e = threadIdx.x; e < (Tp.nd_prog_len + 3) / 4; e += blockDim.x) dst[e] = __ldg(&srcp[e]);
   }
   __shared__ int s_live[kMaxLanes], s_act[kMaxLanes], s_sing[kMaxLanes], s_trev[kMaxLanes];
+  __shared__ int s_list[kMaxLanes], s_nlist, s_anysolve;
   __shared__ double s_gmin[kMaxLanes], s_hsub[kMaxLanes];
 
   const int n = Tp.n, nv = Tp.nv;
@@ -1093,9 +1094,10 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
   const int cnt = min(L, I.ni - base);
   if (cnt <= 0) return;
 
-  // 1. decisions (thread per lane) from the reductions of k_es
+  // 1. decisions (thread per lane, all in warp 0: L <= 32) from the reductions
+  //    of k_es; the lanes with an action are listed in order
   int my_live = 0;
-  if (tid < L) {
+  if (tid < 32) {
     int a = 0;
     if (tid < cnt) {
       InstState s = I.st[g];
@@ -1123,20 +1125,29 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
         s_hsub[tid] = hs;
       }
     }
-    s_live[tid] = my_live;
-    s_act[tid] = a;
-    s_sing[tid] = 0;
+    if (tid < L) {
+      s_live[tid] = my_live;
+      s_act[tid] = a;
+      s_sing[tid] = 0;
+    }
+    const unsigned acting = __ballot_sync(kFull, a != 0);
+    if (a) s_list[__popc(acting & ((1u << tid) - 1u))] = tid;
+    const unsigned solving = __ballot_sync(kFull, (a & ACT_SOLVE) != 0);
+    if (tid == 0) {
+      s_nlist = __popc(acting);
+      s_anysolve = solving != 0;
+    }
   }
   if (!__syncthreads_or(my_live)) return;
+  const int m = s_nlist;  // instances with an action; the vector phases run over
+                          // (item, listed instance) pairs spread over the CTA
 
   // 1b. level schedule: the instances' ND slots start streaming into shared
   //     memory now (asynchronous copies, a warp per slot, a lane per
   //     instance) and land while the vectors are updated
   if (nd) {
-    int anys = 0;
-    for (int q = 0; q < L; ++q) anys |= s_act[q] & ACT_SOLVE;
     const int lw = tid & 31;
-    if (anys && lw < L) {
+    if (s_anysolve && lw < L) {
       const T* J = reinterpret_cast<const T*>(I.J);
       const int S = Tp.nd_S, nw = blockDim.x >> 5;
       T* dst = A + lw * S;
@@ -1153,45 +1164,45 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
 
   // 2. vector updates and the right-hand side of the instances that solve
   const int a = s_act[lane];
-  int any_solve = 0;
-  if (a) {
-    const double gmin = s_gmin[lane];
+  const int any_solve = s_anysolve;
+  {
     double* __restrict__ X = I.x;
     double* __restrict__ V = I.v;
     double* __restrict__ VT = I.v_tp;
     const double* __restrict__ F = I.F;
 #pragma unroll 2
-    for (int i = row; i < n; i += R) {
-      const size_t o = (size_t)i * ld + g;
+    for (int e = tid; e < m * n; e += blockDim.x) {
+      const int i = e / m, ln = s_list[e - i * m];
+      const int act = s_act[ln];
+      const double gmin = s_gmin[ln];
+      const size_t o = (size_t)i * ld + base + ln;
       const double fi = F[o];
       double vi;
-      if (a & ACT_RESTART) {
+      if (act & ACT_RESTART) {
         vi = VT[o];
         V[o] = vi;
         X[o] = vi;
-      } else if (a & ACT_RESEED) {
+      } else if (act & ACT_RESEED) {
         vi = V[o];
         X[o] = vi;
       } else {
         double xi = X[o];
         vi = V[o];
-        if (a & ACT_DAMP) {
+        if (act & ACT_DAMP) {
           xi = vi + 0.5 * (xi - vi);
           X[o] = xi;
         }
-        if (a & ACT_ACCEPT) {
+        if (act & ACT_ACCEPT) {
           vi = xi;
           V[o] = vi;
         }
-        if (a & (ACT_STEP | ACT_TRAN_INIT)) VT[o] = vi;
+        if (act & (ACT_STEP | ACT_TRAN_INIT)) VT[o] = vi;
       }
-      if (a & ACT_SOLVE)
-        Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane] =
-            (T)(-(fi + gmin * vi));
+      if (act & ACT_SOLVE)
+        Y[nd ? ln * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + ln] = (T)(-(fi + gmin * vi));
     }
-    any_solve = (a & ACT_SOLVE) != 0;
   }
-  any_solve = __syncthreads_or(any_solve);
+  __syncthreads();
 
   // 2b. the Jacobian tile of the solving instances into shared memory
   if (any_solve) {
@@ -1215,17 +1226,20 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
   }
 
   // 2c. capacitor history after a completed (sub-)step, waveform samples
-  if (a & (ACT_TRAN_INIT | ACT_STEP)) {
-    for (int c = row; c < Tp.n_cap; c += R) {
+  for (int e = tid; e < m * Tp.n_cap; e += blockDim.x) {
+    const int c = e / m, ln = s_list[e - c * m];
+    const int act = s_act[ln];
+    if (act & (ACT_TRAN_INIT | ACT_STEP)) {
       const int2 tt = __ldg(&Tp.cap_term[c]);
-      const double vc = (tt.x >= 0 ? I.v[tt.x * ld + g] : 0.0) - (tt.y >= 0 ? I.v[tt.y * ld + g] : 0.0);
-      const size_t ci = (size_t)c * ld + g;
-      if (a & ACT_TRAN_INIT) {
+      const int gl = base + ln;
+      const double vc = (tt.x >= 0 ? I.v[tt.x * ld + gl] : 0.0) - (tt.y >= 0 ? I.v[tt.y * ld + gl] : 0.0);
+      const size_t ci = (size_t)c * ld + gl;
+      if (act & ACT_TRAN_INIT) {
         I.cap_vp[ci] = vc;
         I.cap_ip[ci] = 0.0;
       } else {
         const double C = __ldg(&Tp.cap_c[c]);
-        const double h = s_hsub[lane];
+        const double h = s_hsub[ln];
         const double ic = P.method == KTRAN_TRAP ? (2.0 * C / h) * (vc - I.cap_vp[ci]) - I.cap_ip[ci]
                                                  : (C / h) * (vc - I.cap_vp[ci]);
         I.cap_vp[ci] = vc;
@@ -1267,27 +1281,32 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
     }
     __syncthreads();
 
-    // 4. x = v + dx, then junction limiting level by level
-    const bool upd = (a & ACT_SOLVE) && !s_sing[lane];
-    const bool sanitize = (a & ACT_LIMIT) != 0;
-    if (upd) {
+    // 4. x = v + dx, then junction limiting level by level, over (item,
+    //    listed instance) pairs; only instances whose solve succeeded update
+    {
       double* __restrict__ X = I.x;
       const double* __restrict__ V = I.v;
 #pragma unroll 2
-      for (int i = row; i < n; i += R) {
-        const size_t o = (size_t)i * ld + g;
-        double xi = V[o] + (double)Y[nd ? lane * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + lane];
-        if (sanitize && !isfinite(xi)) xi = 0.0;  // SafeUtils::sanitize_vector
+      for (int e = tid; e < m * n; e += blockDim.x) {
+        const int i = e / m, ln = s_list[e - i * m];
+        const int act = s_act[ln];
+        if (!(act & ACT_SOLVE) || s_sing[ln]) continue;
+        const size_t o = (size_t)i * ld + base + ln;
+        double xi = V[o] + (double)Y[nd ? ln * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + ln];
+        if ((act & ACT_LIMIT) && !isfinite(xi)) xi = 0.0;  // SafeUtils::sanitize_vector
         X[o] = xi;
       }
     }
     if (Tp.n_dio > 0) {
-      const int lim = upd && sanitize;
-      if (__syncthreads_or(lim)) {
+      const int lim_lane = tid < L && (s_act[tid] & ACT_SOLVE) && (s_act[tid] & ACT_LIMIT) && !s_sing[tid];
+      if (__syncthreads_or(lim_lane)) {
         for (int lvl = 0; lvl < Tp.n_dio_levels; ++lvl) {
-          if (lim)
-            for (int d = row; d < Tp.n_dio; d += R)
-              if (__ldg(&Tp.dio_level[d]) == lvl) limit_one(Tp, d, I.x, I.v, ld, g);
+          for (int e = tid; e < m * Tp.n_dio; e += blockDim.x) {
+            const int d = e / m, ln = s_list[e - d * m];
+            const int act = s_act[ln];
+            if ((act & ACT_SOLVE) && (act & ACT_LIMIT) && !s_sing[ln] && __ldg(&Tp.dio_level[d]) == lvl)
+              limit_one(Tp, d, I.x, I.v, ld, base + ln);
+          }
           __syncthreads();
         }
       }

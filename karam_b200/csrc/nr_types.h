@@ -30,7 +30,7 @@
 #define KES_MAX_DEV 48
 #endif
 #ifndef KES_MAX_ITEMS
-#define KES_MAX_ITEMS 64
+#define KES_MAX_ITEMS 96
 #endif
 // Hub items (more devices than one block holds) sharing one device walk.
 #define KES_MAX_HUBS 4

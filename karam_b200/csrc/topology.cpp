@@ -1044,14 +1044,95 @@ void es_blocks(Topology& T) {
       }
     }
   };
-  // item order: row by row, slots then the node
+  // Item order: row by row (the slots of a row, then its node), the rows in
+  // Cuthill-McKee order of the graph in which two rows are adjacent when a
+  // device stamps into both. Consecutive rows then share most of their
+  // devices, so few devices are evaluated by more than one block. Hub rows
+  // (nodes with more devices than a block holds) stay out of the graph; their
+  // slots follow the row of their column, whose devices they need, and the
+  // hub nodes (and the slots in hub columns) come last.
   std::vector<int> order;
   {
-    int s = 0;
+    std::vector<int> dv;
+    std::vector<int> row_first(n + 1, nv);
+    for (int s = nv - 1; s >= 0; --s) row_first[T.slot_row[s]] = s;
+    for (int r = n - 1; r >= 0; --r) row_first[r] = std::min(row_first[r], row_first[r + 1]);
+    std::vector<std::vector<int>> dev_rows;
+    std::vector<char> hub_row(n, 0);
     for (int r = 0; r < n; ++r) {
-      while (s < nv && T.slot_row[s] == r) order.push_back(s++);
-      order.push_back(nv + r);
+      item_devs(nv + r, dv);
+      std::sort(dv.begin(), dv.end());
+      dv.erase(std::unique(dv.begin(), dv.end()), dv.end());
+      if ((int)dv.size() > kEsMaxDev) {
+        hub_row[r] = 1;
+        continue;
+      }
+      for (int d : dv) {
+        if (d >= (int)dev_rows.size()) dev_rows.resize(d + 1);
+        dev_rows[d].push_back(r);
+      }
     }
+    std::vector<std::vector<int>> adj(n);
+    for (const auto& rows : dev_rows)
+      for (int a : rows)
+        for (int b : rows)
+          if (a != b) adj[a].push_back(b);
+    for (auto& a : adj) {
+      std::sort(a.begin(), a.end());
+      a.erase(std::unique(a.begin(), a.end()), a.end());
+    }
+    auto degree_less = [&](int a, int b) {
+      return adj[a].size() != adj[b].size() ? adj[a].size() < adj[b].size() : a < b;
+    };
+    std::vector<int> level(n, -1);
+    auto bfs = [&](int root, std::vector<int>& out) {  // Cuthill-McKee from root
+      out.clear();
+      out.push_back(root);
+      level[root] = 0;
+      for (size_t h = 0; h < out.size(); ++h) {
+        std::vector<int> nb;
+        for (int b : adj[out[h]])
+          if (level[b] < 0) nb.push_back(b);
+        std::sort(nb.begin(), nb.end(), degree_less);
+        for (int b : nb) {
+          level[b] = level[out[h]] + 1;
+          out.push_back(b);
+        }
+      }
+    };
+    std::vector<int> rows, comp;
+    std::vector<char> done(n, 0);
+    for (int r = 0; r < n; ++r) done[r] = hub_row[r];
+    while (true) {
+      int root = -1;
+      for (int r = 0; r < n; ++r)
+        if (!done[r] && (root < 0 || degree_less(r, root))) root = r;
+      if (root < 0) break;
+      // pseudo-peripheral start: the last row of a BFS from the
+      // lowest-degree row of the component
+      bfs(root, comp);
+      const int far = comp.back();
+      for (int r : comp) level[r] = -1;
+      bfs(far, comp);
+      for (int r : comp) {
+        done[r] = 1;
+        rows.push_back(r);
+      }
+    }
+    std::vector<std::vector<int>> hub_slots_of_col(n);
+    for (int s = 0; s < nv; ++s)
+      if (hub_row[T.slot_row[s]] && !hub_row[T.slot_col[s]]) hub_slots_of_col[T.slot_col[s]].push_back(s);
+    for (int r : rows) {
+      for (int s = row_first[r]; s < nv && T.slot_row[s] == r; ++s) order.push_back(s);
+      order.push_back(nv + r);
+      for (int s : hub_slots_of_col[r]) order.push_back(s);
+    }
+    for (int r = 0; r < n; ++r)
+      if (hub_row[r]) {
+        for (int s = row_first[r]; s < nv && T.slot_row[s] == r; ++s)
+          if (hub_row[T.slot_col[s]]) order.push_back(s);
+        order.push_back(nv + r);
+      }
   }
   std::vector<int> cur_items, cur_devs, devs;
   std::unordered_map<int, int> local;
