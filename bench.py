@@ -385,7 +385,8 @@ def run_karam(args, dist):
         launches += (t["eval_launches"] + t["lu_launches"] + t["rescue_launches"]
                      + t["other_launches"])
         lanes = t["lanes"]
-        lu_name = "k_lu_nd<float>" if t["level_schedule"] else "k_lu<float>"
+        lu_name = ["k_lu<float>", "k_lu_nd<float>", "k_lu_big<float, smem>",
+                   "k_lu_big<float, global>"][t["level_schedule"]]
         conv_min = min(conv_min, conv)
     clk = clocks.stop()
     dist.barrier()

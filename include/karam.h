@@ -174,8 +174,12 @@ typedef struct karam_solver_opts {
                             KARAM_SEED_HISTORY instances (smaller ones run plain);
                             KARAM_SEED_MLP needs an attached, trained seeder     */
   int32_t seed_max_iter; /* K of the seeded fallback                              */
-  int32_t schedule;      /* instances per CTA of the factor/solve kernel (1, 2, 4, ..., 32);
-                            0 = chosen from shared memory, occupancy and batch size */
+  int32_t schedule;      /* factor/solve schedule: instances per CTA (1..32; a warp each
+                            on the level schedule, or a lane each on the pivot
+                            program), -1 one CTA per instance with its slots in
+                            shared memory, -2 the same with them in global
+                            memory; 0 = chosen from shared memory, occupancy and
+                            batch size                                          */
   int32_t max_rounds;    /* device round budget per launch (0 = unlimited)        */
   int32_t max_halvings;  /* transient: a step whose NR exhausts max_nr_iter restarts
                             from the last time point with half the step, at most
@@ -399,8 +403,11 @@ typedef struct karam_timing {
   int32_t rounds;           /* NR rounds                                             */
   int32_t eval_launches, lu_launches, rescue_launches, other_launches;
   int32_t lanes;            /* instances per CTA of the factor/solve kernel          */
-  int32_t level_schedule;   /* 1 when the factor/solve kernel ran the level-scheduled
-                               LU (k_lu_nd), 0 for the pivot-record LU (k_lu)         */
+  int32_t level_schedule;   /* factor/solve kernel that ran: 0 pivot-record LU (k_lu),
+                               1 level schedule with a warp per instance (k_lu_nd),
+                               2 level schedule with a CTA per instance and the
+                               instance's slots in shared memory (k_lu_big), 3 the
+                               same with the slots in global memory                  */
   int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */

@@ -194,6 +194,62 @@ def config2():
                           vin_pulse=RAMP_PULSE)
 
 
+GRID_GATE_PULSE = (0.0, 1.8, 0.5e-9, 0.2e-9, 0.2e-9, 2e-9, 5e-9)
+GRID_SIZES = (8, 64)
+
+
+def grid_circuit(N, seed=None, vdd=1.0, gate_pulse=GRID_GATE_PULSE):
+    """N x N resistor grid of the uneven-batch family.
+
+    Node 1 = VDD (``vdd`` volts), node 2 = the loads' gate net (PULSE), grid
+    node (i, j) = 3 + i N + j. Segment resistors are log-uniform in
+    10 ohm..10 kohm, each grid node has 1 pF to ground, the four corners are
+    fed from VDD through 1 ohm pads, 10 % of the nodes carry a diode clamp to
+    ground (anode at ground, IS 1e-14, N 1) and 5 % a level-1 NMOS current
+    load (drain on the node, gate on the pulsed net, W/L 2u/0.18u). The draws
+    come from PortableRNG(seed), seed = BASE_SEED + N by default, so every
+    grid of one size is the same circuit; Monte-Carlo instances vary the
+    loads' KP/VTO.
+    """
+    if N < 2:
+        raise ValueError("grid needs N >= 2")
+    rng = PCG32(np.array([BASE_SEED + N if seed is None else seed], dtype=np.uint64))
+    uniform = lambda: float(rng.next()[0]) / 4294967296.0
+    nl = Netlist()
+    nmod = nl.model("NMOS", A.MODEL_NMOS, NMOS_CARD["kp"], NMOS_CARD["vto"], NMOS_CARD["lam"])
+    VDD, GATE = 1, 2
+    node = lambda i, j: 3 + i * N + j
+    nl.vsource(VDD, 0, vdd)
+    nl.vsource(GATE, 0, gate_pulse[0], pulse=gate_pulse)
+    for i in range(N):
+        for j in range(N):
+            if j + 1 < N:
+                nl.resistor(node(i, j), node(i, j + 1), 10.0 ** (1.0 + 3.0 * uniform()))
+            if i + 1 < N:
+                nl.resistor(node(i, j), node(i + 1, j), 10.0 ** (1.0 + 3.0 * uniform()))
+    for i, j in ((0, 0), (0, N - 1), (N - 1, 0), (N - 1, N - 1)):
+        nl.resistor(VDD, node(i, j), 1.0)
+    for i in range(N):
+        for j in range(N):
+            nl.capacitor(node(i, j), 0, 1e-12)
+    for k in range(N * N):
+        u = uniform()
+        if u < 0.10:
+            nl.diode(0, 3 + k, 1e-14, 1.0)
+        elif u < 0.15:
+            nl.mosfet(3 + k, GATE, 0, 0, nmod, *NMOS_WL)
+    return nl
+
+
+def config3_sizes(n_instances=2048, first_instance=0):
+    """Grid size N ~ U{8..64} of each instance of the uneven batch: one
+    PortableRNG draw per instance, seeded BASE_SEED + 5,000,000 + instance."""
+    ids = np.arange(first_instance, first_instance + n_instances, dtype=np.uint64)
+    rng = PCG32(ids + np.uint64(BASE_SEED + 5_000_000))
+    lo, hi = GRID_SIZES
+    return (lo + (rng.next().astype(np.uint64) % np.uint64(hi - lo + 1))).astype(np.int64)
+
+
 # ---------------------------------------------------------------------------
 # Monte-Carlo sampling (math/portable_rng.h:15-95)
 # ---------------------------------------------------------------------------

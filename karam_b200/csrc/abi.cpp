@@ -94,7 +94,7 @@ struct karam_problem {
   int ld = 0;
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
-      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt;
+      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
@@ -406,9 +406,11 @@ void alloc_instances(karam_problem* p) {
   const size_t budget = size_t(2) << 30;
   const size_t resident =
       (size_t)p->rplan.warps * p->rplan.ctas_per_sm * std::max(1, p->ctx->num_sms);
-  size_t slots = std::min<size_t>({M, resident, budget / per});
+  // no rescue when its slot tables do not fit a CTA's shared memory (large
+  // problems): a failed solve then aborts the step as in the reference
+  size_t slots = p->rplan.warps > 0 ? std::min<size_t>({M, resident, budget / per}) : 0;
   // whole CTAs: every warp of the grid takes items (item e on CTA e % grid)
-  if (slots >= (size_t)p->rplan.warps)
+  if (slots >= (size_t)p->rplan.warps && p->rplan.warps > 0)
     slots -= slots % p->rplan.warps;
   else if (slots > 0)
     p->rplan.warps = (int)slots;
@@ -561,7 +563,12 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
     throw std::runtime_error("one instance's matrix does not fit the shared memory of a CTA");
   ck(cudaGetLastError(), "configure kernels");
   p->timing.lanes = L.L;
-  p->timing.level_schedule = L.nd ? 1 : 0;
+  p->timing.level_schedule = L.big ? 1 + L.big : L.nd ? 1 : 0;
+  if (L.big == 2) {  // the ND slots of every instance in global memory
+    const size_t need = (size_t)p->ni * (size_t)p->dt.nd_S * sizeof(double);
+    if (p->i_luws.bytes < need) p->i_luws.alloc(need);
+    I.lu_ws = p->i_luws.p;
+  }
   std::vector<cudaEvent_t> ev(timed ? 4 * kRounds : 0);
   for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
   struct EvGuard {

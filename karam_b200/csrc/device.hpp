@@ -19,14 +19,19 @@ struct RoundLaunch {
   int ctas_per_sm = 0;
   int threads = 0;    // CTA size
   bool nd = false;    // the level-scheduled kernel (k_lu_nd)
+  int big = 0;        // block per instance on the level schedule (k_lu_big): 1 with the
+                      // ND slots in shared memory, 2 in a global workspace
 };
 
 // Lane stride of the instance-interleaved arrays for ni instances.
 inline int lane_stride(int ni) { return (ni + 31) / 32 * 32; }
 
-// Picks L (or takes `want_lanes` when it is a valid power of two) so the
-// tiles fit shared memory and spread over the SMs in the fewest waves;
-// sets the kernels' shared-memory limits (call outside stream capture).
+// Picks the factor/solve schedule: the kernel kind and L (instances per CTA)
+// so the tiles fit shared memory and spread over the SMs in the fewest waves.
+// want_lanes > 0 asks for that L (warp-per-instance level schedule or pivot
+// program), -1 for the block-per-instance kernel with the ND slots in shared
+// memory, -2 with them in a global workspace; 0 chooses. Sets the kernels'
+// shared-memory limits (call outside stream capture).
 RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num_sms,
                        int want_lanes);
 void launch_init(const DevTopo& T, const DevInst& I, const JobParams& P, cudaStream_t s);

@@ -33,29 +33,56 @@ int grid_for(size_t total, int threads) {
 
 }  // namespace
 
+namespace {
+
+// The factor/solve kernel of a candidate schedule.
+const void* lu_kernel(bool mixed, bool nd, int big) {
+  if (big == 1) return mixed ? (const void*)k_lu_big<float, false> : (const void*)k_lu_big<double, false>;
+  if (big == 2) return mixed ? (const void*)k_lu_big<float, true> : (const void*)k_lu_big<double, true>;
+  if (nd) return mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>;
+  return mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>;
+}
+
+}  // namespace
+
 RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num_sms,
                        int want_lanes) {
   const bool mixed = prec == KARAM_PREC_MIXED;
   const size_t es = mixed ? sizeof(float) : sizeof(double);
   RoundLaunch best;
   long best_waves = -1;
+  int best_rank = -1;
   // candidates: the level-scheduled kernel with L instance warps (any L up to
-  // its thread limit), then the pivot-program kernel with power-of-two L
+  // its thread limit), the block-per-instance kernel on the level schedule
+  // (ND slots in shared memory, or in a global workspace), then the
+  // pivot-program kernel with power-of-two L
   struct Cand {
     int L;
     bool nd;
+    int big;
+    int rank;  // preference among candidates with as few waves
   };
   std::vector<Cand> cands;
   if (T.nd_prog_len > 0)
-    for (int L = (mixed ? 32 : 16); L >= 1; --L) cands.push_back({L, true});
-  for (int L = kMaxLanes; L >= 1; L >>= 1) cands.push_back({L, false});
+    for (int L = (mixed ? 32 : 16); L >= 1; --L) cands.push_back({L, true, 0, 3});
+  if (T.nd_levels > 0) {
+    cands.push_back({1, false, 1, 2});
+    cands.push_back({1, false, 2, 1});
+  }
+  for (int L = kMaxLanes; L >= 1; L >>= 1) cands.push_back({L, false, 0, 0});
   for (const Cand& c : cands) {
     const int L = c.L;
-    if (want_lanes > 0 && L != want_lanes) continue;
-    const void* kern = c.nd ? (mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>)
-                            : (mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>);
-    const int threads = c.nd ? 32 * L : kRoundThreads;
-    const size_t sm = round_smem(T, L, es, c.nd);
+    if (want_lanes > 0 && (c.big || L != want_lanes)) continue;
+    if (want_lanes < 0 && c.big != -want_lanes) continue;
+    const void* kern = lu_kernel(mixed, c.nd, c.big);
+    const int threads = c.big ? kBigThreads : c.nd ? 32 * L : kRoundThreads;
+    size_t sm;
+    if (c.big == 1)
+      sm = es * ((size_t)T.nd_SY + (size_t)T.nd_S);
+    else if (c.big == 2)
+      sm = (es * (size_t)T.nd_SY + 15) & ~size_t(15);
+    else
+      sm = round_smem(T, L, es, c.nd);
     if (sm > (size_t)max_smem) continue;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
         cudaSuccess) {
@@ -71,31 +98,31 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
     const int grid = (ni + L - 1) / L;
     const long slots = (long)per_sm * std::max(1, num_sms);
     const long waves = (grid + slots - 1) / slots;
-    // fewest waves; among equals the level schedule, then a grid that
+    // fewest waves; among equals the preferred kind, then a grid that
     // reaches every SM (the streaming phases spread wider)
     const bool fills = grid >= num_sms, best_fills = best.grid >= num_sms;
     bool better = best_waves < 0 || waves < best_waves;
     if (!better && waves == best_waves) {
-      if (c.nd != best.nd)
-        better = c.nd;
+      if (c.rank != best_rank)
+        better = c.rank > best_rank;
       else
         better = fills && !best_fills;
     }
     if (better) {
       best_waves = waves;
+      best_rank = c.rank;
       best.L = L;
       best.grid = grid;
       best.smem = sm;
       best.ctas_per_sm = per_sm;
       best.threads = threads;
       best.nd = c.nd;
+      best.big = c.big;
     }
   }
-  if (best.L > 0) {
-    const void* kern = best.nd ? (mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>)
-                               : (mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>);
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best.smem);
-  }
+  if (best.L > 0)
+    cudaFuncSetAttribute(lu_kernel(mixed, best.nd, best.big),
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best.smem);
   const int rsm = (int)plan_rescue(T).smem;
   cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
   cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
@@ -127,7 +154,17 @@ void launch_eval_stamp(const DevTopo& T, const DevInst& I, const JobParams& P,
 
 void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const RoundLaunch& L,
                int prec, int* active, cudaStream_t s) {
-  if (L.nd) {
+  if (L.big == 1) {
+    if (prec == KARAM_PREC_MIXED)
+      k_lu_big<float, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+    else
+      k_lu_big<double, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+  } else if (L.big == 2) {
+    if (prec == KARAM_PREC_MIXED)
+      k_lu_big<float, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+    else
+      k_lu_big<double, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+  } else if (L.nd) {
     if (prec == KARAM_PREC_MIXED)
       k_lu_nd<float><<<L.grid, L.threads, L.smem, s>>>(T, I, P, L.L, active);
     else

@@ -23,6 +23,7 @@ namespace knr {
 
 constexpr int kRoundThreads = 512;
 constexpr int kMaxLanes = 32;
+constexpr int kBigThreads = 1024;  // CTA size of the block-per-instance factor/solve kernel
 constexpr unsigned kFull = 0xffffffffu;
 #define KARAM_SEED_HISTORY_MAX 8  // NeuralSeeder::Config::maxHistory
 
@@ -1055,6 +1056,61 @@ __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __rest
   return ok && finite && !(lmax > growth_limit);
 }
 
+// The decision of instance g for this round from the reductions of k_es (the
+// reference control flow as a state machine, `decide`): the state advances,
+// the reductions return to neutral, and a reseed restarts GMIN stepping from
+// the reference seed. Returns the action bits; live = 0 for a finished
+// instance; trev = 1 when this round evaluated a transient point.
+__device__ __forceinline__ int instance_decide(const DevTopo& Tp, const DevInst& I, const JobParams& P,
+                                               int g, int& live, int& trev, double& gm, double& hs) {
+  InstState s = I.st[g];
+  trev = s.mode == MODE_TRAN;
+  live = 0;
+  if (s.mode == MODE_DONE) return 0;
+  live = 1;
+  const unsigned long long fb = I.red_f[g];
+  const double Fm = __longlong_as_double((long long)fb);
+  const double dvm = __longlong_as_double((long long)I.red_dv[g]);
+  const int fl = I.red_flags[g];
+  reset_reductions(I, g);
+  gm = 1e-12;
+  hs = P.h;
+  const int a = decide(s, Fm, fl & 1, (fl & 2) != 0, dvm, P, gm, hs);
+  if (a & ACT_RESEED) {
+    s.g = 0;
+    s.it = 0;
+    s.first = 1;
+    s.damp = 0;
+    s.prevF = 0.0;
+    s.seeded = 0;
+    reference_seed(Tp, I, g, I.v);
+  }
+  I.st[g] = s;
+  return a;
+}
+
+// End of instance g's round: a failed solve goes to the rescue list (or
+// aborts the step when there is none), then the next evaluation point.
+// Returns whether the instance is still live.
+__device__ __forceinline__ int instance_finish(const DevTopo& Tp, const DevInst& I, const JobParams& P,
+                                               int g, int act, int sing, double gmin) {
+  if ((act & ACT_SOLVE) && sing) {
+    if (I.rescue_list) {
+      const int slot = atomicAdd(I.rescue_count, 1);
+      RescueItem it;
+      it.inst = g;
+      it.act = act;
+      it.gmin = gmin;
+      I.rescue_list[slot] = it;
+    } else {
+      on_singular(Tp, I, g);
+    }
+  }
+  const InstState st2 = I.st[g];
+  set_eval_point(I, P, g, st2);
+  return st2.mode != MODE_DONE;
+}
+
 // Control flow + linear solve of a tile of L instances (one CTA): decisions
 // from the reductions of k_es, vector updates, the Jacobian tile staged
 // into shared memory with cp.async, static-pivot LU with the forward
@@ -1100,27 +1156,11 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
   if (tid < 32) {
     int a = 0;
     if (tid < cnt) {
-      InstState s = I.st[g];
-      s_trev[tid] = s.mode == MODE_TRAN;  // what this round evaluated
-      if (s.mode != MODE_DONE) {
-        my_live = 1;
-        const unsigned long long fb = I.red_f[g];
-        const double Fm = __longlong_as_double((long long)fb);
-        const double dvm = __longlong_as_double((long long)I.red_dv[g]);
-        const int fl = I.red_flags[g];
-        reset_reductions(I, g);
-        double gm = 1e-12, hs = P.h;
-        a = decide(s, Fm, fl & 1, (fl & 2) != 0, dvm, P, gm, hs);
-        if (a & ACT_RESEED) {
-          s.g = 0;
-          s.it = 0;
-          s.first = 1;
-          s.damp = 0;
-          s.prevF = 0.0;
-          s.seeded = 0;
-          reference_seed(Tp, I, g, I.v);
-        }
-        I.st[g] = s;
+      int trev = 0;
+      double gm = 1e-12, hs = P.h;
+      a = instance_decide(Tp, I, P, g, my_live, trev, gm, hs);
+      s_trev[tid] = trev;  // what this round evaluated
+      if (my_live) {
         s_gmin[tid] = gm;
         s_hsub[tid] = hs;
       }
@@ -1322,22 +1362,8 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
       const int act = s_act[tid];
       trev = s_trev[tid];
       dcev = !trev;
-      if ((act & ACT_SOLVE) && s_sing[tid]) {
-        if (I.rescue_list) {
-          const int slot = atomicAdd(I.rescue_count, 1);
-          RescueItem it;
-          it.inst = g;
-          it.act = act;
-          it.gmin = s_gmin[tid];
-          I.rescue_list[slot] = it;
-        } else {
-          on_singular(Tp, I, g);
-        }
-      }
-      const InstState st2 = I.st[g];
       solved = (act & ACT_SOLVE) && !s_sing[tid];
-      live = st2.mode != MODE_DONE;
-      set_eval_point(I, P, g, st2);
+      live = instance_finish(Tp, I, P, g, act, s_sing[tid], s_gmin[tid]);
     }
     const int nlive = __popc(__ballot_sync(mask, live));
     const int nsol = __popc(__ballot_sync(mask, solved));
@@ -1365,6 +1391,242 @@ template <typename T>
 __global__ void __launch_bounds__(sizeof(T) == 4 ? 1024 : 512)
     k_lu_nd(DevTopo Tp, DevInst I, JobParams P, int L, int* active) {
   lu_round<T, true>(Tp, I, P, L, active);
+}
+
+// The level schedule solved by a whole CTA for one instance (the
+// block-per-instance schedule): per level the pivots' reciprocals, then the L
+// values, then the update targets and right-hand-side rows, each phase spread
+// over the CTA's threads; target and row lists longer than Topology::kNdLong
+// are summed by one warp with lanes strided and combined in nd_solve's fixed
+// tree, and shorter ones by one thread in order, so the results equal
+// nd_solve's. Tables are read from global memory. A holds the instance's ND
+// slots (shared or global memory), y its right-hand side (ND order) and
+// returns the solution. Same failure tests as nd_solve.
+template <typename T>
+__device__ bool big_solve(T* __restrict__ A, T* __restrict__ y, const DevTopo& Tp, T gmin, T tiny,
+                          T growth_limit) {
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+  bool ok = true, finite = true;
+  T lmax = T(0);
+  for (int lv = 0; lv < Tp.nd_levels; ++lv) {
+    const int p0 = __ldg(&Tp.lv_piv_ptr[lv]), p1 = __ldg(&Tp.lv_piv_ptr[lv + 1]);
+    for (int q = p0 + tid; q < p1; q += bd) {
+      const int d = __ldg(&Tp.nd_diag[__ldg(&Tp.lv_piv[q])]);
+      const T piv = A[d] + gmin;  // the gmin diagonal joins at the pivot step
+      ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
+      A[d] = recip(piv);
+    }
+    __syncthreads();
+    const int e0 = __ldg(&Tp.lv_l_ptr[lv]), e1 = __ldg(&Tp.lv_l_ptr[lv + 1]);
+    for (int e = e0 + tid; e < e1; e += bd) {
+      const int sl = __ldg(&Tp.l_slot[e]);
+      const T l = A[sl] * A[__ldg(&Tp.nd_diag[__ldg(&Tp.l_piv[e])])];
+      A[sl] = l;
+      lmax = fmax(lmax, fabs(l));
+    }
+    __syncthreads();
+    const int t0 = __ldg(&Tp.lv_ts_ptr[lv]), tl = __ldg(&Tp.lv_tl_ptr[lv]), t1 = __ldg(&Tp.lv_ts_ptr[lv + 1]);
+    // two targets per thread in flight (no target of a level is read by
+    // another of the same level), each summed in its own order
+    int t = t0 + tid;
+    for (; t + bd < tl; t += 2 * bd) {
+      const int sa = __ldg(&Tp.t_slot[t]), sb = __ldg(&Tp.t_slot[t + bd]);
+      int qa = __ldg(&Tp.t_off[t]), qb = __ldg(&Tp.t_off[t + bd]);
+      const int qa1 = __ldg(&Tp.t_off[t + 1]), qb1 = __ldg(&Tp.t_off[t + bd + 1]);
+      T acc_a = A[sa], acc_b = A[sb];
+      for (; qa < qa1 && qb < qb1; ++qa, ++qb) {
+        const T la = A[__ldg(&Tp.pr_l[qa])], ua = A[__ldg(&Tp.pr_u[qa])];
+        const T lb = A[__ldg(&Tp.pr_l[qb])], ub = A[__ldg(&Tp.pr_u[qb])];
+        acc_a -= la * ua;
+        acc_b -= lb * ub;
+      }
+      for (; qa < qa1; ++qa) acc_a -= A[__ldg(&Tp.pr_l[qa])] * A[__ldg(&Tp.pr_u[qa])];
+      for (; qb < qb1; ++qb) acc_b -= A[__ldg(&Tp.pr_l[qb])] * A[__ldg(&Tp.pr_u[qb])];
+      A[sa] = acc_a;
+      A[sb] = acc_b;
+    }
+    if (t < tl) {
+      const int sl = __ldg(&Tp.t_slot[t]), q1 = __ldg(&Tp.t_off[t + 1]);
+      T acc = A[sl];
+      for (int q = __ldg(&Tp.t_off[t]); q < q1; ++q) acc -= A[__ldg(&Tp.pr_l[q])] * A[__ldg(&Tp.pr_u[q])];
+      A[sl] = acc;
+    }
+    const int r0 = __ldg(&Tp.lv_ys_ptr[lv]), rl = __ldg(&Tp.lv_yl_ptr[lv]), r1 = __ldg(&Tp.lv_ys_ptr[lv + 1]);
+    for (int r = r0 + tid; r < rl; r += bd) {
+      const int row = __ldg(&Tp.y_row[r]), q1 = __ldg(&Tp.y_off[r + 1]);
+      T acc = y[row];
+      for (int q = __ldg(&Tp.y_off[r]); q < q1; ++q) acc -= A[__ldg(&Tp.yp_l[q])] * y[__ldg(&Tp.yp_k[q])];
+      y[row] = acc;
+    }
+    for (int t = tl + warp; t < t1; t += nw) {  // long target lists: a warp sums
+      const int q0 = __ldg(&Tp.t_off[t]), c = __ldg(&Tp.t_off[t + 1]) - q0;
+      T part = T(0);
+      for (int q = lane; q < c; q += 32) part += A[__ldg(&Tp.pr_l[q0 + q])] * A[__ldg(&Tp.pr_u[q0 + q])];
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) A[__ldg(&Tp.t_slot[t])] -= part;
+    }
+    for (int r = rl + warp; r < r1; r += nw) {  // long right-hand-side rows
+      const int q0 = __ldg(&Tp.y_off[r]), c = __ldg(&Tp.y_off[r + 1]) - q0;
+      T part = T(0);
+      for (int q = lane; q < c; q += 32) part += A[__ldg(&Tp.yp_l[q0 + q])] * y[__ldg(&Tp.yp_k[q0 + q])];
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) y[__ldg(&Tp.y_row[r])] -= part;
+    }
+    __syncthreads();
+  }
+  for (int lv = Tp.nd_levels - 1; lv >= 0; --lv) {
+    const int p0 = __ldg(&Tp.lv_piv_ptr[lv]), p1 = __ldg(&Tp.lv_piv_ptr[lv + 1]);
+    for (int q = p0 + tid; q < p1; q += bd) {
+      const int k = __ldg(&Tp.lv_piv[q]);
+      const int b1 = __ldg(&Tp.bs_off[k + 1]);
+      T sv = y[k];
+      for (int j = __ldg(&Tp.bs_off[k]); j < b1; ++j) sv -= A[__ldg(&Tp.bs_u[j])] * y[__ldg(&Tp.bs_c[j])];
+      sv *= A[__ldg(&Tp.nd_diag[k])];
+      y[k] = sv;
+      finite = finite && isfinite(sv);
+    }
+    __syncthreads();
+  }
+  return __syncthreads_and(ok && finite && !(lmax > growth_limit)) != 0;
+}
+
+// Control flow + linear solve of one instance per CTA on the level schedule
+// (instances whose ND slots do not fit a warp's share of shared memory): the
+// same round as lu_round with every phase spread over the CTA's threads.
+// The ND slots live in dynamic shared memory after the right-hand side
+// (gA = false) or in the instance's slice of I.lu_ws (gA = true, nd_S
+// elements per instance).
+template <typename T, bool gA>
+__global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, JobParams P, int* active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_a, s_live, s_trev, s_sing;
+  __shared__ double s_gmin, s_hsub;
+  const int n = Tp.n, tid = threadIdx.x, g = blockIdx.x;
+  const size_t ld = I.ld;
+  T* Y = reinterpret_cast<T*>(smem_raw);
+  T* A = gA ? reinterpret_cast<T*>(I.lu_ws) + (size_t)g * Tp.nd_S : Y + Tp.nd_SY;
+  if (tid == 0) {
+    int live = 0, trev = 0;
+    double gm = 1e-12, hs = P.h;
+    const int a = g < I.ni ? instance_decide(Tp, I, P, g, live, trev, gm, hs) : 0;
+    s_a = a;
+    s_live = live;
+    s_trev = trev;
+    s_gmin = gm;
+    s_hsub = hs;
+    s_sing = 0;
+  }
+  __syncthreads();
+  if (!s_live) return;
+  const int a = s_a;
+  const double gmin = s_gmin;
+
+  // the instance's ND slots from its Jacobian value slots
+  if (a & ACT_SOLVE) {
+    const T* J = reinterpret_cast<const T*>(I.J);
+    for (int sl = tid; sl < Tp.nd_nv; sl += blockDim.x) {
+      const int src = __ldg(&Tp.nd_src[sl]);
+      A[sl] = src >= 0 ? J[(size_t)src * ld + g] : T(0);
+    }
+  }
+  // vector updates and the right-hand side
+  {
+    double* __restrict__ X = I.x;
+    double* __restrict__ V = I.v;
+    double* __restrict__ VT = I.v_tp;
+    const double* __restrict__ F = I.F;
+    for (int i = tid; i < n; i += blockDim.x) {
+      const size_t o = (size_t)i * ld + g;
+      const double fi = F[o];
+      double vi;
+      if (a & ACT_RESTART) {
+        vi = VT[o];
+        V[o] = vi;
+        X[o] = vi;
+      } else if (a & ACT_RESEED) {
+        vi = V[o];
+        X[o] = vi;
+      } else {
+        double xi = X[o];
+        vi = V[o];
+        if (a & ACT_DAMP) {
+          xi = vi + 0.5 * (xi - vi);
+          X[o] = xi;
+        }
+        if (a & ACT_ACCEPT) {
+          vi = xi;
+          V[o] = vi;
+        }
+        if (a & (ACT_STEP | ACT_TRAN_INIT)) VT[o] = vi;
+      }
+      if (a & ACT_SOLVE) Y[__ldg(&Tp.nd_pos[i])] = (T)(-(fi + gmin * vi));
+    }
+  }
+  __syncthreads();
+  // capacitor history after a completed (sub-)step, waveform samples
+  if (a & (ACT_TRAN_INIT | ACT_STEP)) {
+    for (int c = tid; c < Tp.n_cap; c += blockDim.x) {
+      const int2 tt = __ldg(&Tp.cap_term[c]);
+      const double vc = (tt.x >= 0 ? I.v[tt.x * ld + g] : 0.0) - (tt.y >= 0 ? I.v[tt.y * ld + g] : 0.0);
+      const size_t ci = (size_t)c * ld + g;
+      if (a & ACT_TRAN_INIT) {
+        I.cap_vp[ci] = vc;
+        I.cap_ip[ci] = 0.0;
+      } else {
+        const double C = __ldg(&Tp.cap_c[c]);
+        const double h = s_hsub;
+        const double ic = P.method == KTRAN_TRAP ? (2.0 * C / h) * (vc - I.cap_vp[ci]) - I.cap_ip[ci]
+                                                 : (C / h) * (vc - I.cap_vp[ci]);
+        I.cap_vp[ci] = vc;
+        I.cap_ip[ci] = ic;
+      }
+    }
+  }
+  if ((a & ACT_WAVE) && I.n_wave > 0) {
+    const int done_step = I.st[g].step - 1;  // 1-based step just completed
+    if (done_step >= 1 && done_step <= I.wave_steps)
+      for (int w = tid; w < I.n_wave; w += blockDim.x) {
+        const int q = I.wave_pos[w];
+        I.wave[((size_t)g * I.wave_steps + (done_step - 1)) * I.n_wave + w] = q >= 0 ? I.v[q * ld + g] : 0.0;
+      }
+  }
+  __syncthreads();
+
+  if (a & ACT_SOLVE) {
+    const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
+    const T growth = sizeof(T) == 8 ? (T)P.growth64 : (T)fmin(P.growth32, 3.0e38);
+    const bool ok = big_solve<T>(A, Y, Tp, (T)gmin, tiny, growth);
+    // x = v + dx, then junction limiting level by level
+    if (ok) {
+      for (int i = tid; i < n; i += blockDim.x) {
+        const size_t o = (size_t)i * ld + g;
+        double xi = I.v[o] + (double)Y[__ldg(&Tp.nd_pos[i])];
+        if ((a & ACT_LIMIT) && !isfinite(xi)) xi = 0.0;  // SafeUtils::sanitize_vector
+        I.x[o] = xi;
+      }
+      if ((a & ACT_LIMIT) && Tp.n_dio > 0) {
+        __syncthreads();
+        for (int lvl = 0; lvl < Tp.n_dio_levels; ++lvl) {
+          for (int d = tid; d < Tp.n_dio; d += blockDim.x)
+            if (__ldg(&Tp.dio_level[d]) == lvl) limit_one(Tp, d, I.x, I.v, ld, g);
+          __syncthreads();
+        }
+      }
+    }
+    if (tid == 0) s_sing = ok ? 0 : 1;
+  }
+  __syncthreads();
+
+  // rescue hand-off, next evaluation point, bookkeeping
+  if (tid == 0) {
+    const int sing = s_sing;
+    if (instance_finish(Tp, I, P, g, a, sing, gmin)) atomicAdd(active, 1);
+    if (I.counters) {
+      atomicAdd(&I.counters[s_trev ? 1 : 0], 1ull);
+      if ((a & ACT_SOLVE) && !sing) atomicAdd(&I.counters[2], 1ull);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -180,6 +180,8 @@ struct DevInst {
   RescueItem* rescue_list;  // [ni]
   int* rescue_count;
   int rescue_slots;         // rescue warps (one workspace each)
+  void* lu_ws;              // [ni][nd_S] ND slots of the block-per-instance kernel when they
+                            // live in global memory (float or double), else 0
   double* hub_part;         // [n_hub_rows][ld] hub items' sums per device chunk
   int* hub_cnt;             // [n_hub_groups][ld / 32] chunk blocks done (0 between launches)
   unsigned long long* counters;  // [5]: evaluations DC, evaluations transient, solves,

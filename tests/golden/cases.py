@@ -1,6 +1,7 @@
 """Netlists of the golden fixtures: the two benchmark circuits plus small edge
 cases of the symbolic layer and the NR loop (ragged device mixes, duplicate
-stamp slots, a floating source, a capacitor-only node)."""
+stamp slots, a floating source, a capacitor-only node) and the smallest grid
+of the uneven-batch family."""
 from karam_b200 import circuits
 from karam_b200.circuits import Netlist
 
@@ -55,11 +56,17 @@ def diode_rc():
     return nl
 
 
+def grid8():
+    """8 x 8 resistor grid with diode clamps and pulsed NMOS loads."""
+    return circuits.grid_circuit(8)
+
+
 SMALL = {
     "divider": divider,
     "floating_source": floating_source,
     "parallel_duplicates": parallel_duplicates,
     "diode_rc": diode_rc,
+    "grid8": grid8,
 }
 BENCH = {"config1": circuits.config1, "config2": circuits.config2}
 

@@ -10,7 +10,8 @@ filled pattern of symbolicFactorize, the stamps of stampSoABlock, the NR
 solutions of the oracle driver over those stamps and solveLU_Pivoted /
 solveSparse_LU, and PortableNormalDist draws.
 
-    python tests/golden/make_golden.py      # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py          # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py grid8    # only the named cases
 """
 import os
 import sys
@@ -30,7 +31,8 @@ from karam_b200 import circuits  # noqa: E402
 from oracle import pyoracle  # noqa: E402
 
 POLISH = dict(polish_max=8)
-WAVE_NODES = {"config2": [2, 3, 4, 5, 10, 20, 259], "diode_rc": [1, 2, 3, 4]}
+WAVE_NODES = {"config2": [2, 3, 4, 5, 10, 20, 259], "diode_rc": [1, 2, 3, 4],
+              "grid8": [2, 3, 10, 30, 66]}
 
 
 def probe_voltages(n, seed=11):
@@ -77,15 +79,21 @@ def main():
     ref = pyoracle.Oracle("ref")
 
     seeds = np.array(cases.RNG_SEEDS, np.uint64)
+    if len(sys.argv) > 1:
+        seeds = seeds[:0]
     normals = np.zeros((len(seeds), cases.RNG_COUNT))
     for k, s in enumerate(seeds):
         ref.lib.oracle_ref_normals.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_int32,
                                                C.POINTER(C.c_double)]
         ref.lib.oracle_ref_normals(int(s), 0.0, 1.0, cases.RNG_COUNT,
                                    normals[k].ctypes.data_as(C.POINTER(C.c_double)))
-    np.savez_compressed(os.path.join(HERE, "rng_normals.npz"), seeds=seeds, normals=normals)
+    if len(seeds):
+        np.savez_compressed(os.path.join(HERE, "rng_normals.npz"), seeds=seeds, normals=normals)
 
+    only = set(sys.argv[1:])  # case names to regenerate (default: all)
     for name, make in {**cases.SMALL, **cases.BENCH}.items():
+        if only and name not in only:
+            continue
         nl = make()
         inst = circuits.mc_instances(nl, 2) if name == "config2" else None
         out = symbolic(ref, nl)

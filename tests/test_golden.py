@@ -114,7 +114,7 @@ def test_port_dc_config2(port):
         assert np.allclose(v, g["dc_v"][i], rtol=1e-12, atol=1e-15)
 
 
-@pytest.mark.parametrize("name", ["diode_rc", "config2"])
+@pytest.mark.parametrize("name", ["diode_rc", "grid8", "config2"])
 def test_port_transient(port, name):
     from oracle import pyoracle
     nl, g = ALL[name](), golden(name)

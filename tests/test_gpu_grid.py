@@ -1,0 +1,92 @@
+"""The resistor-grid family of the uneven batch on the GPU: every factor/solve
+schedule (a warp per instance with the level schedule in shared memory, a CTA
+per instance with the instance's slots in shared or global memory) against
+the reference-built fixture and the CPU oracle, and the schedules against
+each other (they run the same level-scheduled elimination in the same order,
+so their results are identical)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from karam_b200 import _abi as A
+from karam_b200 import circuits
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+pytestmark = pytest.mark.gpu
+
+POLISH = dict(polish_max=8)
+KIND = {1: 1, -1: 2, -2: 3}  # schedule option -> karam_timing.level_schedule
+
+
+def scaled_err(v, v_ref, rel=1e-9, abs_=1e-12):
+    return float(np.max(np.abs(v - v_ref) / (rel * np.abs(v_ref) + abs_)))
+
+
+def solve(product, ctx, nl, inst, ni, prec, schedule):
+    prob = product.Problem(ctx, nl, max_instances=ni)
+    prob.set_instances(inst)
+    v, st = prob.solve_dc(product.options(precision=prec, schedule=schedule, **POLISH))
+    return prob, v, st
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+@pytest.mark.parametrize("schedule", [1, -1, -2])
+def test_grid8_dc_matches_reference_fixture(product, ctx, prec, schedule):
+    g = np.load(os.path.join(HERE, "golden", "grid8.npz"))
+    nl = circuits.grid_circuit(8)
+    prob, v, st = solve(product, ctx, nl, None, 1, prec, schedule)
+    assert prob.timing()["level_schedule"] == KIND[schedule]
+    assert st[0]["status"] == A.ST_CONVERGED
+    assert scaled_err(v[0], g["dc_v"]) <= 1.0
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+def test_schedules_give_identical_results(product, ctx, prec):
+    nl = circuits.grid_circuit(10)
+    inst = circuits.mc_instances(nl, 5)
+    out = []
+    for schedule in (1, -1, -2):
+        prob, v, st = solve(product, ctx, nl, inst, 5, prec, schedule)
+        assert prob.timing()["level_schedule"] == KIND[schedule]
+        out.append((v, [s["iterations"] for s in st]))
+    for v, its in out[1:]:
+        assert np.array_equal(v, out[0][0]) and its == out[0][1]
+
+
+@pytest.mark.parametrize("schedule", [0, -2])
+def test_grid24_dc_mc_batch(product, ctx, port, schedule):
+    """578 unknowns: beyond the warp-per-instance program; a CTA per instance."""
+    nl = circuits.grid_circuit(24)
+    ni = 3
+    inst = circuits.mc_instances(nl, ni)
+    prob, v, st = solve(product, ctx, nl, inst, ni, A.PREC_MIXED, schedule)
+    assert prob.timing()["level_schedule"] in (2, 3)
+    for i in range(ni):
+        v_ref, st_ref = port.solve_dc(nl, inst, i, linear_solver=1, **POLISH)
+        assert st_ref["converged"] == 1 and st[i]["status"] == A.ST_CONVERGED
+        assert scaled_err(v[i], v_ref) <= 1.0, (i, scaled_err(v[i], v_ref))
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+def test_grid_trapezoidal_transient(product, ctx, port, prec):
+    nl = circuits.grid_circuit(12)
+    ni, steps, dt = 2, 30, 20e-12
+    inst = circuits.mc_instances(nl, ni)
+    prob = product.Problem(ctx, nl, max_instances=ni)
+    prob.set_instances(inst)
+    opts = product.options(precision=prec, schedule=-1, **POLISH)
+    vdc, st = prob.solve_dc(opts)
+    nodes = [2, 3, 40, 100, 146]
+    v, st, wave = prob.step_transient(dt, steps, A.TRAN_TRAP, opts, wave_nodes=nodes)
+    for i in range(ni):
+        vd_ref, _ = port.solve_dc(nl, inst, i, linear_solver=1, **POLISH)
+        assert scaled_err(vdc[i], vd_ref) <= 1.0
+        v_ref, st_ref, w_ref = port.transient(nl, vd_ref, dt, steps, A.TRAN_TRAP, inst, i,
+                                              wave_nodes=nodes, linear_solver=1, **POLISH)
+        assert st_ref["converged"] == 1 and st[i]["status"] == A.ST_CONVERGED
+        assert scaled_err(v[i], v_ref) <= 1.0
+        assert np.max(np.abs(wave[i] - w_ref)) <= 1e-9 * np.max(np.abs(w_ref)) + 1e-12

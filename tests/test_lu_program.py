@@ -219,9 +219,23 @@ def test_level_schedule_solves(product, name):
         level[sch["lv_piv"][sch["lv_piv_ptr"][lv]:sch["lv_piv_ptr"][lv + 1]]] = lv
     owner = np.repeat(np.arange(n), np.diff(sch["bs_off"]))
     assert (level[sch["bs_c"]] > level[owner]).all()  # U columns are solved in later levels
+    # the ND structure holds every stamped position; Min-Fill slots outside
+    # it are fill of the Min-Fill order that no stamp reaches, zero in every
+    # Jacobian (the evaluation kernel writes them as 0)
+    src = sch["nd_src"]
+    covered = np.zeros(nv, bool)
+    covered[src[src >= 0]] = True
+    _, perm_mf, _ = prob.ordering()
+    iperm = np.empty(n, int)
+    iperm[perm_mf] = np.arange(n)
+    rp, col = prob.pattern()
+    slot_of = {(int(r), int(c)): s for s, (r, c) in enumerate(rc)}
+    for r in range(n):
+        for c in col[rp[r]:rp[r + 1]]:
+            assert covered[slot_of[(iperm[r], iperm[c])]]
     rng = np.random.default_rng(9)
     for _ in range(3):
-        vals = rng.uniform(-1.0, 1.0, nv)
+        vals = np.where(covered, rng.uniform(-1.0, 1.0, nv), 0.0)
         dense = np.zeros((n, n))
         dense[rc[:, 0], rc[:, 1]] = vals
         for k in range(n):
@@ -229,7 +243,6 @@ def test_level_schedule_solves(product, name):
             vals[s] = np.sign(vals[s] or 1.0) * (1.0 + np.abs(dense[k]).sum() + np.abs(dense[:, k]).sum())
         dense[rc[:, 0], rc[:, 1]] = vals
         rhs = rng.uniform(-1.0, 1.0, n)
-        src = sch["nd_src"]
         vals_nd = np.where(src >= 0, vals[np.maximum(src, 0)], 0.0)
         y = run_schedule(sch, vals_nd, rhs[perm])
         x = np.empty(n)
@@ -293,8 +306,11 @@ def test_packed_level_program_solves(product, name):
     hdr, _, rc = prob.lu_program()
     n, nv = prob.n, prob.info["n_slots"]
     assert int(sch["nd_prog"][7]) == len(sch["nd_prog"])
+    src = sch["nd_src"]
+    covered = np.zeros(nv, bool)  # zero outside the ND structure (see above)
+    covered[src[src >= 0]] = True
     rng = np.random.default_rng(13)
-    vals = rng.uniform(-1.0, 1.0, nv)
+    vals = np.where(covered, rng.uniform(-1.0, 1.0, nv), 0.0)
     dense = np.zeros((n, n))
     dense[rc[:, 0], rc[:, 1]] = vals
     for k in range(n):
