@@ -65,7 +65,10 @@ def parse():
                     help="batches of plain-NR DC solutions the learned seeder trains on (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the config-1 latency and config-5 seeder measurements")
+                    help="skip the config-1 latency, config-3 uneven-batch and config-5 seeder "
+                         "measurements")
+    ap.add_argument("--config3-steps", type=int, default=500,
+                    help="trapezoidal steps of the config-3 uneven batch")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--max-rounds", type=int, default=0,
                     help="stop every job after this many NR rounds (profiling captures of a "
@@ -541,6 +544,7 @@ def run_karam(args, dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_configs:
         line["config1"] = config1_latency(ctx)
         line["config5"] = config5_seeder(ctx)
+        line["config3"] = config3_uneven(dist.local, steps=args.config3_steps)
     if dist.rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
@@ -592,6 +596,126 @@ def config1_latency(ctx, reps=50):
             "iterations": st[0]["iterations"], "iterations_oracle": st_ref["iterations"],
             "converged": st[0]["status"] == A.ST_CONVERGED,
             "max_abs_diff_vs_oracle_v": float(np.max(np.abs(v[0] - v_ref)))}
+
+
+CONFIG3_FIRST = 6_000_000  # Monte-Carlo ids of the uneven batch's load parameters
+
+
+def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample=2):
+    """Uneven batch: n_instances N x N resistor grids with N ~ U{8..64}
+    (circuits.config3_sizes), each a DC point then `steps` trapezoidal steps.
+
+    One problem per grid size, each on its own context (stream); the sizes run
+    concurrently from host threads, and each size's factor/solve schedule is
+    the planner's (a warp per instance, or a CTA per instance with the
+    instance's slots in shared or global memory). Timed: the whole batch, wall
+    clock from the first launch to the last result, FP32 LU + FP64
+    refinement against plain FP64. Every size shares one grid (seeded by N);
+    instances vary in their loads' KP/VTO (ids from CONFIG3_FIRST). Accuracy:
+    the smallest instances against the reference-built oracle over the whole
+    transient, which also gives the reference CPU rate on that sample."""
+    import threading
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+    from karam_b200 import circuits
+    sizes = circuits.config3_sizes(n_instances)
+    groups = {}
+    for i, N in enumerate(sizes):
+        groups.setdefault(int(N), []).append(i)
+    t0 = time.perf_counter()
+    probs = []
+    for N, ids in sorted(groups.items()):
+        nl = circuits.grid_circuit(N)
+        draws = [circuits.sample_mos_variation(nl, 1, first_instance=CONFIG3_FIRST + i) for i in ids]
+        inst = circuits.Instances(len(ids), np.concatenate([d[0] for d in draws]),
+                                  np.concatenate([d[1] for d in draws]))
+        ctx = K.Context(device)
+        prob = K.Problem(ctx, nl, max_instances=len(ids))
+        prob.set_instances(inst)
+        probs.append((N, ids, nl, inst, ctx, prob))
+    t_build = time.perf_counter() - t0
+
+    def run(prec, n_steps):
+        opts = K.options(precision=prec, max_halvings=MAX_HALVINGS, **POLISH)
+        errs = []
+
+        def one(prob):
+            try:
+                prob.run_mc_device(dt, n_steps, A.TRAN_TRAP, opts)
+                prob.sync()
+            except Exception as e:  # re-raised below
+                errs.append(e)
+        threads = [threading.Thread(target=one, args=(g[5],)) for g in probs]
+        t = time.perf_counter()
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t
+        if errs:
+            raise errs[0]
+        out = {}
+        conv = 0
+        kinds = {}
+        for N, ids, nl, inst, ctx, prob in probs:
+            v, st = prob.read_results()
+            conv += sum(1 for s in st if s["status"] == A.ST_CONVERGED)
+            k = ["pivot records", "warp per instance", "CTA per instance, shared memory",
+                 "CTA per instance, global memory"][prob.timing()["level_schedule"]]
+            kinds[k] = kinds.get(k, 0) + 1
+            out[N] = (v, st)
+        return wall, conv, kinds, out
+
+    res = {}
+    for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        run(prec, 4)  # warm-up: plans, workspaces, graphs
+        wall, conv, kinds, out = run(prec, steps)
+        res[name] = {"solves_per_s": conv * (steps + 1) / wall, "wall_s": wall,
+                     "converged": conv, "schedules_by_size": kinds, "_out": out}
+    both = []
+    for N, ids, *_ in probs:
+        vm, sm = res["mixed"]["_out"][N]
+        vf, sf = res["fp64"]["_out"][N]
+        for k in range(len(ids)):
+            if sm[k]["status"] == A.ST_CONVERGED and sf[k]["status"] == A.ST_CONVERGED:
+                both.append(float(np.max(np.abs(vm[k] - vf[k]) / (1e-9 * np.abs(vf[k]) + 1e-12))))
+    # the smallest instances against the reference-built oracle
+    from oracle import pyoracle
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    worst, cpu_t, cpu_solves, sample = 0.0, 0.0, 0, []
+    with native_stdout_to_stderr():
+        orc = pyoracle.Oracle(kind)
+        for N, ids, nl, inst, ctx, prob in probs[:oracle_sample]:
+            vm, sm = res["mixed"]["_out"][N]
+            t = time.perf_counter()
+            v_ref, st = orc.run_batch(nl, inst, 0, 1, dt=dt, n_steps=steps, method=A.TRAN_TRAP,
+                                      n_threads=1, linear_solver=pyoracle.LS_SPARSE,
+                                      max_halvings=MAX_HALVINGS, polish_max=8)
+            cpu_t += time.perf_counter() - t
+            if st[0]["converged"] and sm[0]["status"] == A.ST_CONVERGED:
+                cpu_solves += steps + 1
+                worst = max(worst, float(np.max(np.abs(vm[0] - v_ref[0]) /
+                                                (1e-9 * np.abs(v_ref[0]) + 1e-12))))
+            sample.append(f"N={N} (n={prob.n})")
+    for r in res.values():
+        r.pop("_out")
+    return {
+        "workload": f"{n_instances} N x N resistor grids, N ~ U{{8..64}} ({len(groups)} sizes, "
+                    f"n = 66..4098), 1 pF caps, diode clamps at 10 % and pulsed NMOS loads at 5 % "
+                    f"of nodes; DC + {steps} trapezoidal steps of {dt * 1e12:g} ps",
+        "problems": len(groups), "build_s": t_build,
+        "mixed": res["mixed"], "fp64": res["fp64"],
+        "speedup_mixed_vs_fp64": res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"],
+        "max_scaled_diff_mixed_vs_fp64": max(both) if both else None,
+        "max_scaled_err_vs_oracle": worst,
+        "scaled": "|dv| / (1e-9 |v| + 1e-12 V)",
+        "cpu_baseline": {"value": cpu_solves / cpu_t if cpu_t else None, "unit": "solves/s",
+                         "cores": 1, "kind": "reference" if kind == "ref" else "port",
+                         "sample": "one instance of each of the smallest sizes, " + ", ".join(sample)
+                                   + f", full transient, {cpu_t:.1f} s"},
+    }
 
 
 def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10):

@@ -560,7 +560,7 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   const int prec = P.precision;
   RoundLaunch L = plan_round(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms, want_lanes);
   if (L.L < 1)
-    throw std::runtime_error("one instance's matrix does not fit the shared memory of a CTA");
+    throw std::runtime_error(std::string("no factor/solve schedule fits this problem; last: ") + L.why);
   ck(cudaGetLastError(), "configure kernels");
   p->timing.lanes = L.L;
   p->timing.level_schedule = L.big ? 1 + L.big : L.nd ? 1 : 0;

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdint>
 #include <vector>
 
@@ -14,6 +15,21 @@ namespace karam {
 using namespace knr;
 
 namespace {
+
+// the opt-in shared-memory limit of one CTA on sm_100 (227 KiB)
+constexpr int kSmemOptin = 232448;
+
+// Raises a kernel's dynamic shared-memory limit to what the opt-in maximum
+// leaves beside its static shared memory. The limit is process-wide state of
+// the kernel: setting it to this one value for every problem keeps problems
+// planned from several threads from undoing each other's limits.
+cudaError_t open_smem_limit(const void* kern, int max_smem) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              max_smem - (int)fa.sharedSizeBytes);
+}
 
 // Level schedule: ND slots + right-hand side of L instances; else value slots
 // + right-hand side of L instances, then the packed pivot records.
@@ -83,15 +99,24 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
       sm = (es * (size_t)T.nd_SY + 15) & ~size_t(15);
     else
       sm = round_smem(T, L, es, c.nd);
-    if (sm > (size_t)max_smem) continue;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-        cudaSuccess) {
+    auto reject = [&](const char* what) {
+      snprintf(best.why, sizeof(best.why), "%s: %s (kind %d, L %d, %zu B shared)",
+               c.big ? "block per instance" : c.nd ? "warp per instance" : "pivot program", what,
+               c.big, L, sm);
+    };
+    if (sm > (size_t)max_smem) {
+      reject("shared memory");
+      continue;
+    }
+    if (const cudaError_t e = open_smem_limit(kern, max_smem); e != cudaSuccess) {
+      reject(cudaGetErrorString(e));
       cudaGetLastError();
       continue;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, sm) != cudaSuccess ||
-        per_sm < 1) {
+    if (const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, sm);
+        e != cudaSuccess || per_sm < 1) {
+      reject(e != cudaSuccess ? cudaGetErrorString(e) : "no CTA fits an SM");
       cudaGetLastError();
       continue;
     }
@@ -120,12 +145,8 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
       best.big = c.big;
     }
   }
-  if (best.L > 0)
-    cudaFuncSetAttribute(lu_kernel(mixed, best.nd, best.big),
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best.smem);
-  const int rsm = (int)plan_rescue(T).smem;
-  cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-  cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+  open_smem_limit((const void*)k_rescue<float>, max_smem);
+  open_smem_limit((const void*)k_rescue<double>, max_smem);
   return best;
 }
 
@@ -177,8 +198,7 @@ void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const Rou
 }
 
 RescuePlan plan_rescue(const DevTopo& T) {
-  // the opt-in shared-memory limit of one CTA on sm_100 (227 KiB)
-  const size_t limit = 232448;
+  const size_t limit = kSmemOptin;
   const size_t rec = (T.lu_rec ? rescue_rec_bytes(T.n) : 0) + rescue_tab_bytes(T.n, T.nv);
   RescuePlan R;
   for (int K = 2; K >= 0; --K) {
@@ -195,8 +215,8 @@ RescuePlan plan_rescue(const DevTopo& T) {
 
 int rescue_ctas_per_sm(const DevTopo& T, const RescuePlan& R) {
   if (R.warps <= 0) return 0;
-  cudaFuncSetAttribute(k_rescue<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem);
-  cudaFuncSetAttribute(k_rescue<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem);
+  open_smem_limit((const void*)k_rescue<float>, kSmemOptin);
+  open_smem_limit((const void*)k_rescue<double>, kSmemOptin);
   int a = 0, b = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_rescue<float>, 32 * R.warps, R.smem) !=
           cudaSuccess ||
