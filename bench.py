@@ -606,9 +606,9 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample
     (circuits.config3_sizes), each a DC point then `steps` trapezoidal steps.
 
     One problem per grid size, each on its own context (stream); the sizes run
-    concurrently from host threads, and each size's factor/solve schedule is
-    the planner's (a warp per instance, or a CTA per instance with the
-    instance's slots in shared or global memory). Timed: the whole batch, wall
+    concurrently from host threads, and each size's factor/solve schedule (a
+    warp per instance, or a CTA per instance with the instance's slots in
+    shared or global memory) is measured first by karam_tune_schedule. Timed: the whole batch, wall
     clock from the first launch to the last result, FP32 LU + FP64
     refinement against plain FP64. Every size shares one grid (seeded by N);
     instances vary in their loads' KP/VTO (ids from CONFIG3_FIRST). Accuracy:
@@ -668,10 +668,17 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample
 
     res = {}
     for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        # the measured schedule of every size (karam_tune_schedule: 16 DC
+        # rounds per feasible schedule), before timing
+        t = time.perf_counter()
+        for g in probs:
+            g[5].tune_schedule(K.options(precision=prec, max_halvings=MAX_HALVINGS, **POLISH), 16)
+        t_tune = time.perf_counter() - t
         run(prec, 4)  # warm-up: plans, workspaces, graphs
         wall, conv, kinds, out = run(prec, steps)
         res[name] = {"solves_per_s": conv * (steps + 1) / wall, "wall_s": wall,
-                     "converged": conv, "schedules_by_size": kinds, "_out": out}
+                     "converged": conv, "schedules_by_size": kinds, "tune_s": t_tune,
+                     "_out": out}
     both = []
     for N, ids, *_ in probs:
         vm, sm = res["mixed"]["_out"][N]

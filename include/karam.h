@@ -278,6 +278,19 @@ KARAM_API int karam_run_mc(karam_problem *p, const karam_instances *inst,
  * karam_read_results copies the device results back afterwards. */
 KARAM_API int karam_run_mc_device(karam_problem *p, const karam_solver_opts *opts,
                                   double dt, int32_t n_steps, int32_t method);
+/* Measured choice of the factor/solve schedule (the warp-per-instance vs
+ * block-per-instance autotuner; no reference counterpart: the reference
+ * solves one instance at a time). Runs the first `rounds` NR rounds of a DC
+ * job from the reference seed once per feasible schedule (the planner's
+ * choice, a CTA per instance with its slots in shared memory, the same with
+ * them in global memory), timed on the device, and keeps the fastest for this
+ * problem and, process-wide, for problems of the same unknowns, stamp
+ * non-zeros, batch size and precision; solves with opts.schedule == 0 then use
+ * it. *schedule receives it as an opts.schedule value and *best_ms (either may
+ * be null) its trial time. The problem's state afterwards is a trial's: run
+ * the solve again. */
+KARAM_API int karam_tune_schedule(karam_problem *p, const karam_solver_opts *opts, int32_t rounds,
+                                  int32_t *schedule, double *best_ms);
 KARAM_API int karam_read_results(karam_problem *p, double *out_v,
                                  karam_instance_stats *stats);
 /* Blocks until the problem's stream is idle. */

@@ -62,6 +62,8 @@ def lib():
                                    P(A.KaramInstanceStats)]),
         "karam_run_mc_device": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_double, C.c_int32,
                                           C.c_int32]),
+        "karam_tune_schedule": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_int32, P(C.c_int32),
+                                          P(C.c_double)]),
         "karam_read_results": (C.c_int, [vp, P(C.c_double), P(A.KaramInstanceStats)]),
         "karam_sync": (C.c_int, [vp]),
         "karam_get_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
@@ -298,6 +300,16 @@ class Problem:
     def run_mc_device(self, dt=0.0, n_steps=0, method=A.TRAN_BE, opts=None):
         opts = opts or options()
         self._check(lib().karam_run_mc_device(self.h, C.byref(opts), dt, n_steps, method))
+
+    def tune_schedule(self, opts=None, rounds=16):
+        """Measured factor/solve schedule (karam_tune_schedule): returns the
+        opts.schedule value kept for this problem and its trial time (ms)."""
+        opts = opts or options()
+        sch = C.c_int32(0)
+        ms = C.c_double(0.0)
+        self._check(lib().karam_tune_schedule(self.h, C.byref(opts), rounds, C.byref(sch),
+                                              C.byref(ms)))
+        return sch.value, ms.value
 
     def read_results(self, want_stats=True):
         v = np.zeros((self.ni, self.n))

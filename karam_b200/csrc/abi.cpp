@@ -6,8 +6,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -77,6 +80,7 @@ struct karam_problem {
   int ni = 0;
   bool inst_kp = false, inst_vth = false;  // per-instance MOSFET values present
   bool have_dc = false;
+  int tuned[2] = {0, 0};  // measured factor/solve schedule per precision (0 = none)
   bool tran_started = false;  // capacitor history holds a transient in progress
   double t_now = 0.0, tran_h = 0.0;
   int tran_method = KARAM_TRAN_BE;
@@ -541,6 +545,28 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
   return P;
 }
 
+// Measured schedules (karam_tune_schedule), per problem and process-wide by
+// problem shape: unknowns, stamp non-zeros, batch size and precision.
+using TuneKey = std::tuple<int, int, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, int>& tune_cache() {
+  static std::map<TuneKey, int> m;
+  return m;
+}
+TuneKey tune_key(const karam_problem* p, int prec) {
+  return TuneKey{p->topo.n, p->topo.nnz(), p->ni, prec};
+}
+// The schedule option a solve with opts.schedule == 0 uses: the problem's
+// measured choice, else one measured for a problem of the same shape, else 0
+// (the planner's).
+int tuned_schedule(const karam_problem* p, int prec) {
+  const int idx = prec == KARAM_PREC_MIXED ? 1 : 0;
+  if (p->tuned[idx]) return p->tuned[idx];
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  const auto it = tune_cache().find(tune_key(p, prec));
+  return it == tune_cache().end() ? 0 : it->second;
+}
+
 // Runs NR rounds until every instance is done (or opts->max_rounds ends).
 // Rounds (k_es, k_lu, k_rescue) are captured in a CUDA graph of kRounds
 // rounds; the last k_lu of the graph counts the live instances into d_active,
@@ -553,7 +579,8 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
                 const DevInst* inst = nullptr) {
   constexpr int kRounds = 16;
   const int max_rounds = opts ? opts->max_rounds : 0;
-  const int want_lanes = opts ? opts->schedule : 0;
+  int want_lanes = opts ? opts->schedule : 0;
+  if (want_lanes == 0) want_lanes = tuned_schedule(p, P.precision);
   const bool timed = opts && opts->kernel_timing;
   cudaStream_t s = p->ctx->stream;
   DevInst I = inst ? *inst : dev_inst(p);
@@ -927,6 +954,62 @@ int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double 
     run_rounds(p, P, opts);
     end_job(p);
     p->have_dc = true;
+    return KARAM_OK;
+  });
+}
+
+int karam_tune_schedule(karam_problem* p, const karam_solver_opts* opts, int32_t rounds,
+                        int32_t* schedule, double* best_ms) {
+  if (!p || rounds < 1) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    karam_solver_opts o;
+    if (opts)
+      o = *opts;
+    else
+      karam_default_opts(&o);
+    o.max_rounds = rounds;
+    o.kernel_timing = 0;
+    o.seeded = KARAM_SEED_NONE;  // trial rounds from the reference seed
+    const int prec = o.precision;
+    // the feasible schedules: the planner's choice, then a CTA per instance
+    // with the slots in shared or global memory (option values as in
+    // karam_solver_opts.schedule)
+    std::vector<int> cands;
+    for (int want : {0, -1, -2}) {
+      const RoundLaunch L = plan_round(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms, want);
+      cudaGetLastError();
+      if (L.L < 1) continue;
+      const int val = L.big ? -L.big : L.L;
+      if (std::find(cands.begin(), cands.end(), val) == cands.end()) cands.push_back(val);
+    }
+    if (cands.empty()) throw std::runtime_error("no factor/solve schedule fits this problem");
+    int best = cands[0];
+    double best_t = 1e300;
+    for (int c : cands) {
+      o.schedule = c;
+      const JobParams P = job_params(&o, 0, 0.0, KARAM_TRAN_BE);
+      double t = 1e300;
+      for (int rep = 0; rep < 2; ++rep) {  // the first trial builds the graph
+        begin_job(p);
+        start_job(p, P, nullptr);
+        run_rounds(p, P, &o);
+        end_job(p);
+        t = std::min(t, p->timing.job_ms);
+      }
+      if (t < best_t) {
+        best_t = t;
+        best = c;
+      }
+    }
+    p->tuned[prec == KARAM_PREC_MIXED ? 1 : 0] = best;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      tune_cache()[tune_key(p, prec)] = best;
+    }
+    p->have_dc = false;  // the state is a trial's
+    if (schedule) *schedule = best;
+    if (best_ms) *best_ms = best_t;
     return KARAM_OK;
   });
 }

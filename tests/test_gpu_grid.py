@@ -90,3 +90,21 @@ def test_grid_trapezoidal_transient(product, ctx, port, prec):
         assert st_ref["converged"] == 1 and st[i]["status"] == A.ST_CONVERGED
         assert scaled_err(v[i], v_ref) <= 1.0
         assert np.max(np.abs(wave[i] - w_ref)) <= 1e-9 * np.max(np.abs(w_ref)) + 1e-12
+
+
+def test_tuned_schedule_is_used_and_feasible(product, ctx):
+    nl = circuits.grid_circuit(12)
+    ni = 6
+    inst = circuits.mc_instances(nl, ni)
+    prob = product.Problem(ctx, nl, max_instances=ni)
+    prob.set_instances(inst)
+    opts = product.options(precision=A.PREC_MIXED, **POLISH)
+    sch, ms = prob.tune_schedule(opts, rounds=8)
+    assert ms > 0 and (sch in (-1, -2) or 1 <= sch <= 32)
+    v_tuned, st_tuned = prob.solve_dc(opts)  # opts.schedule == 0: the tuned choice
+    kind_tuned = prob.timing()["level_schedule"]
+    v_explicit, st_explicit = prob.solve_dc(product.options(precision=A.PREC_MIXED,
+                                                            schedule=sch, **POLISH))
+    assert prob.timing()["level_schedule"] == kind_tuned
+    assert np.array_equal(v_tuned, v_explicit)
+    assert all(s["status"] == A.ST_CONVERGED for s in st_tuned)
