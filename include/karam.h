@@ -278,6 +278,25 @@ KARAM_API int karam_run_mc(karam_problem *p, const karam_instances *inst,
  * karam_read_results copies the device results back afterwards. */
 KARAM_API int karam_run_mc_device(karam_problem *p, const karam_solver_opts *opts,
                                   double dt, int32_t n_steps, int32_t method);
+/* SPICE netlist front-end (SPICEParser::parse, netlist/spice_parser.cpp:148-262)
+ * for the subset the engine solves: R, C, V (DC, PULSE), I (DC), D, M with
+ * .MODEL NMOS / PMOS (KP, VTO, LAMBDA) and D (IS, N), .TEMP, .OP, .TRAN, .END.
+ * The reference parser's defects are fixed: MOSFET W= / L= are read, diodes
+ * take IS / N from their .MODEL card, model names match case-insensitively,
+ * SIN / SINE are both recognised (and rejected: DC and PULSE sources only),
+ * and the first physical line is the title even when it starts with '*'. Elements the engine cannot solve are errors, not skipped.
+ * karam_spice_parse returns KARAM_E_INVALID with the message (and line) in
+ * err on failure. The netlist stays valid until karam_spice_free. Node names
+ * map to indices 1.. in order of first appearance (ground: 0 / GND / VSS /
+ * GROUND); karam_spice_node returns -1 for an unknown name. */
+typedef struct karam_spice karam_spice;
+KARAM_API int karam_spice_parse(const char *text, karam_spice **out, char *err, int32_t err_len);
+KARAM_API const karam_netlist *karam_spice_netlist(const karam_spice *s);
+KARAM_API int32_t karam_spice_node(const karam_spice *s, const char *name);
+KARAM_API int karam_spice_analysis(const karam_spice *s, int32_t *has_op, int32_t *has_tran,
+                                   double *tran_step, double *tran_stop, double *tran_start);
+KARAM_API void karam_spice_free(karam_spice *s);
+
 /* Measured choice of the factor/solve schedule (the warp-per-instance vs
  * block-per-instance autotuner; no reference counterpart: the reference
  * solves one instance at a time). Runs the first `rounds` NR rounds of a DC

@@ -64,6 +64,12 @@ def lib():
                                           C.c_int32]),
         "karam_tune_schedule": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_int32, P(C.c_int32),
                                           P(C.c_double)]),
+        "karam_spice_parse": (C.c_int, [C.c_char_p, P(vp), C.c_char_p, C.c_int32]),
+        "karam_spice_netlist": (P(A.KaramNetlist), [vp]),
+        "karam_spice_node": (C.c_int32, [vp, C.c_char_p]),
+        "karam_spice_analysis": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(C.c_double),
+                                           P(C.c_double), P(C.c_double)]),
+        "karam_spice_free": (None, [vp]),
         "karam_read_results": (C.c_int, [vp, P(C.c_double), P(A.KaramInstanceStats)]),
         "karam_sync": (C.c_int, [vp]),
         "karam_get_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
@@ -108,6 +114,55 @@ def options(**kw) -> A.KaramSolverOpts:
             raise AttributeError(f"unknown solver option {k}")
         setattr(o, k, v)
     return o
+
+
+class SpiceNetlist:
+    """A SPICE netlist read by the library's front-end (karam_spice_parse);
+    usable wherever a circuits.Netlist is (Problem, the oracle)."""
+
+    def __init__(self, text: str):
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        rc = lib().karam_spice_parse(text.encode(), C.byref(h), err, len(err))
+        if rc != A.KARAM_OK:
+            raise KaramError(rc, err.value.decode())
+        self.h = h
+        self._s = lib().karam_spice_netlist(h).contents
+        self.n_nodes = self._s.n_nodes
+
+    def as_struct(self) -> A.KaramNetlist:
+        return self._s
+
+    def node(self, name: str) -> int:
+        """Node index of a name (0 = ground, -1 = unknown)."""
+        return lib().karam_spice_node(self.h, name.encode())
+
+    def analysis(self):
+        """(.OP given, .TRAN given, tran step, tran stop, tran start)."""
+        op, tr = C.c_int32(0), C.c_int32(0)
+        st, sp, s0 = C.c_double(0), C.c_double(0), C.c_double(0)
+        lib().karam_spice_analysis(self.h, C.byref(op), C.byref(tr), C.byref(st), C.byref(sp),
+                                   C.byref(s0))
+        return bool(op.value), bool(tr.value), st.value, sp.value, s0.value
+
+    @property
+    def n_mos(self):
+        return self._s.n_mos
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().karam_spice_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def parse_spice(text: str) -> SpiceNetlist:
+    return SpiceNetlist(text)
 
 
 class Context:
