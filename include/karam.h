@@ -244,6 +244,17 @@ KARAM_API void karam_default_opts(karam_solver_opts *opts);
 KARAM_API int karam_problem_create(karam_ctx *ctx, const karam_netlist *nl,
                                    int32_t max_instances, karam_problem **out);
 KARAM_API void karam_problem_destroy(karam_problem *p);
+/* Symbolic-analysis cache: karam_problem_create keeps the last 32 analyses by
+ * netlist content (every count, index, value, model name and the
+ * temperature), process-wide, and reuses one for an identical netlist -- the
+ * role of the reference's compiled block / pattern cache keyed by
+ * topologyHash (infrastructure/compiled_block.h:45-88,
+ * solvers/circuitsim_solver.cpp:262-268), which keys on structure alone
+ * because its values are stamped per solve. karam_netlist_hash is a 64-bit
+ * fingerprint of that content. */
+KARAM_API int karam_netlist_hash(const karam_netlist *nl, uint64_t *out);
+KARAM_API int karam_symbolic_cache_info(int32_t *entries, int64_t *hits, int64_t *misses);
+KARAM_API void karam_symbolic_cache_clear(void);
 KARAM_API int karam_problem_info_get(const karam_problem *p, karam_problem_info *out);
 /* Copies per-instance parameters host -> device (the batch to solve next). */
 KARAM_API int karam_set_instances(karam_problem *p, const karam_instances *inst);

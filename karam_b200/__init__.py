@@ -70,6 +70,9 @@ def lib():
         "karam_spice_analysis": (C.c_int, [vp, P(C.c_int32), P(C.c_int32), P(C.c_double),
                                            P(C.c_double), P(C.c_double)]),
         "karam_spice_free": (None, [vp]),
+        "karam_netlist_hash": (C.c_int, [P(A.KaramNetlist), P(C.c_uint64)]),
+        "karam_symbolic_cache_info": (C.c_int, [P(C.c_int32), P(C.c_int64), P(C.c_int64)]),
+        "karam_symbolic_cache_clear": (None, []),
         "karam_read_results": (C.c_int, [vp, P(C.c_double), P(A.KaramInstanceStats)]),
         "karam_sync": (C.c_int, [vp]),
         "karam_get_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
@@ -163,6 +166,26 @@ class SpiceNetlist:
 
 def parse_spice(text: str) -> SpiceNetlist:
     return SpiceNetlist(text)
+
+
+def netlist_hash(nl) -> int:
+    """64-bit fingerprint of a netlist's content (karam_netlist_hash)."""
+    h = C.c_uint64(0)
+    rc = lib().karam_netlist_hash(C.byref(nl.as_struct()), C.byref(h))
+    if rc != A.KARAM_OK:
+        raise KaramError(rc, "netlist hash")
+    return h.value
+
+
+def symbolic_cache_info():
+    """(entries, hits, misses) of the symbolic-analysis cache."""
+    e, h, m = C.c_int32(0), C.c_int64(0), C.c_int64(0)
+    lib().karam_symbolic_cache_info(C.byref(e), C.byref(h), C.byref(m))
+    return e.value, h.value, m.value
+
+
+def symbolic_cache_clear():
+    lib().karam_symbolic_cache_clear()
 
 
 class Context:

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -863,14 +864,137 @@ const char* karam_last_error(const karam_ctx* ctx) {
   return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }
 
+namespace {
+
+// The netlist's content as bytes (every count, index, value, model name and
+// the temperature), the key of the symbolic-analysis cache.
+std::string netlist_bytes(const karam_netlist* nl) {
+  std::string b;
+  auto put = [&](const void* p, size_t n) {
+    if (p && n) b.append(static_cast<const char*>(p), n);
+    const uint64_t len = n;  // lengths keep distinct layouts distinct
+    b.append(reinterpret_cast<const char*>(&len), sizeof(len));
+  };
+  auto ints = [&](const int32_t* p, int n) { put(p, p ? sizeof(int32_t) * (size_t)n : 0); };
+  auto dbls = [&](const double* p, int n) { put(p, p ? sizeof(double) * (size_t)n : 0); };
+  put(&nl->n_nodes, sizeof(nl->n_nodes));
+  put(&nl->temp_k, sizeof(nl->temp_k));
+  const int32_t counts[7] = {nl->n_vsrc, nl->n_isrc, nl->n_res, nl->n_cap, nl->n_dio, nl->n_mos, nl->n_models};
+  put(counts, sizeof(counts));
+  ints(nl->vs_pos, nl->n_vsrc);
+  ints(nl->vs_neg, nl->n_vsrc);
+  dbls(nl->vs_dc, nl->n_vsrc);
+  ints(nl->vs_kind, nl->n_vsrc);
+  dbls(nl->vs_pulse, 7 * nl->n_vsrc);
+  ints(nl->is_pos, nl->n_isrc);
+  ints(nl->is_neg, nl->n_isrc);
+  dbls(nl->is_amp, nl->n_isrc);
+  ints(nl->r_n1, nl->n_res);
+  ints(nl->r_n2, nl->n_res);
+  dbls(nl->r_ohm, nl->n_res);
+  ints(nl->c_n1, nl->n_cap);
+  ints(nl->c_n2, nl->n_cap);
+  dbls(nl->c_farad, nl->n_cap);
+  ints(nl->d_anode, nl->n_dio);
+  ints(nl->d_cathode, nl->n_dio);
+  dbls(nl->d_is, nl->n_dio);
+  dbls(nl->d_n, nl->n_dio);
+  dbls(nl->d_vt, nl->n_dio);
+  ints(nl->d_model, nl->n_dio);
+  ints(nl->m_d, nl->n_mos);
+  ints(nl->m_g, nl->n_mos);
+  ints(nl->m_s, nl->n_mos);
+  ints(nl->m_b, nl->n_mos);
+  dbls(nl->m_w, nl->n_mos);
+  dbls(nl->m_l, nl->n_mos);
+  ints(nl->m_model, nl->n_mos);
+  ints(nl->model_type, nl->n_models);
+  dbls(nl->model_kp, nl->n_models);
+  dbls(nl->model_vto, nl->n_models);
+  dbls(nl->model_lambda, nl->n_models);
+  for (int k = 0; k < nl->n_models; ++k) {
+    const char* nm = nl->model_name && nl->model_name[k] ? nl->model_name[k] : "";
+    put(nm, std::strlen(nm));
+  }
+  return b;
+}
+
+uint64_t fnv1a(const std::string& b) {
+  uint64_t h = 1469598103934665603ull;
+  for (unsigned char c : b) {
+    h ^= c;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Built symbolic analyses by netlist content, most recent first; the role of
+// the reference's compiled-block / pattern cache keyed by topologyHash
+// (infrastructure/compiled_block.h:45-88, solvers/circuitsim_solver.cpp:262-268).
+struct SymbolicCache {
+  static constexpr size_t kEntries = 32;
+  std::mutex mu;
+  std::list<std::pair<std::string, std::shared_ptr<const Topology>>> lru;
+  int64_t hits = 0, misses = 0;
+};
+SymbolicCache& symbolic_cache() {
+  static SymbolicCache c;
+  return c;
+}
+
+Topology cached_topology(const karam_netlist* nl) {
+  const std::string key = netlist_bytes(nl);
+  SymbolicCache& C = symbolic_cache();
+  {
+    std::lock_guard<std::mutex> lock(C.mu);
+    for (auto it = C.lru.begin(); it != C.lru.end(); ++it)
+      if (it->first == key) {
+        C.lru.splice(C.lru.begin(), C.lru, it);
+        ++C.hits;
+        return *C.lru.front().second;
+      }
+    ++C.misses;
+  }
+  auto T = std::make_shared<const Topology>(build_topology(nl));  // outside the lock
+  std::lock_guard<std::mutex> lock(C.mu);
+  C.lru.emplace_front(key, T);
+  if (C.lru.size() > SymbolicCache::kEntries) C.lru.pop_back();
+  return *T;
+}
+
+}  // namespace
+
+int karam_netlist_hash(const karam_netlist* nl, uint64_t* out) {
+  if (!nl || !out) return KARAM_E_INVALID;
+  *out = fnv1a(netlist_bytes(nl));
+  return KARAM_OK;
+}
+
+int karam_symbolic_cache_info(int32_t* entries, int64_t* hits, int64_t* misses) {
+  SymbolicCache& C = symbolic_cache();
+  std::lock_guard<std::mutex> lock(C.mu);
+  if (entries) *entries = (int32_t)C.lru.size();
+  if (hits) *hits = C.hits;
+  if (misses) *misses = C.misses;
+  return KARAM_OK;
+}
+
+void karam_symbolic_cache_clear(void) {
+  SymbolicCache& C = symbolic_cache();
+  std::lock_guard<std::mutex> lock(C.mu);
+  C.lru.clear();
+  C.hits = C.misses = 0;
+}
+
 int karam_problem_create(karam_ctx* ctx, const karam_netlist* nl, int32_t max_instances,
                          karam_problem** out) {
   if (!out) return KARAM_E_INVALID;
   *out = nullptr;
   return guarded(ctx, [&] {
     if (max_instances < 1) throw std::runtime_error("max_instances must be >= 1");
+    if (!nl) throw std::runtime_error("no netlist");
     auto p = std::make_unique<karam_problem>();
-    p->topo = build_topology(nl);
+    p->topo = cached_topology(nl);
     p->max_inst = max_instances;
     if (!ctx) {  // symbolic analysis only
       *out = p.release();
