@@ -389,7 +389,7 @@ def run_karam(args, dist):
                      + t["other_launches"])
         lanes = t["lanes"]
         lu_name = ["k_lu<float>", "k_lu_nd<float>", "k_lu_big<float, smem>",
-                   "k_lu_big<float, global>"][t["level_schedule"]]
+                   "k_lu_big<float, global>", "k_lu_big<float, packed>"][t["level_schedule"]]
         conv_min = min(conv_min, conv)
     clk = clocks.stop()
     dist.barrier()
@@ -661,7 +661,8 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample
             v, st = prob.read_results()
             conv += sum(1 for s in st if s["status"] == A.ST_CONVERGED)
             k = ["pivot records", "warp per instance", "CTA per instance, shared memory",
-                 "CTA per instance, global memory"][prob.timing()["level_schedule"]]
+                 "CTA per instance, global memory",
+                 "CTA per instance, packed program"][prob.timing()["level_schedule"]]
             kinds[k] = kinds.get(k, 0) + 1
             out[N] = (v, st)
         return wall, conv, kinds, out

@@ -178,8 +178,9 @@ typedef struct karam_solver_opts {
                             on the level schedule, or a lane each on the pivot
                             program), -1 one CTA per instance with its slots in
                             shared memory, -2 the same with them in global
-                            memory; 0 = chosen from shared memory, occupancy and
-                            batch size                                          */
+                            memory, -3 one CTA per instance with its slots and
+                            the packed level program in shared memory; 0 =
+                            chosen from shared memory, occupancy and batch size */
   int32_t max_rounds;    /* device round budget per launch (0 = unlimited)        */
   int32_t max_halvings;  /* transient: a step whose NR exhausts max_nr_iter restarts
                             from the last time point with half the step, at most
@@ -312,8 +313,9 @@ KARAM_API void karam_spice_free(karam_spice *s);
  * block-per-instance autotuner; no reference counterpart: the reference
  * solves one instance at a time). Runs the first `rounds` NR rounds of a DC
  * job from the reference seed once per feasible schedule (the planner's
- * choice, a CTA per instance with its slots in shared memory, the same with
- * them in global memory), timed on the device, and keeps the fastest for this
+ * choice, a CTA per instance with its slots and the packed program in shared
+ * memory, with its slots alone there, with them in global memory), timed on
+ * the device, and keeps the fastest for this
  * problem and, process-wide, for problems of the same unknowns, stamp
  * non-zeros, batch size and precision; solves with opts.schedule == 0 then use
  * it. *schedule receives it as an opts.schedule value and *best_ms (either may
@@ -450,12 +452,16 @@ typedef struct karam_timing {
                                1 level schedule with a warp per instance (k_lu_nd),
                                2 level schedule with a CTA per instance and the
                                instance's slots in shared memory (k_lu_big), 3 the
-                               same with the slots in global memory                  */
+                               same with the slots in global memory, 4 a CTA per
+                               instance with slots and packed program in shared
+                               memory                                                */
   int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */
   int64_t rescues;          /* linear solves redone by the rescue path               */
   int64_t rescues_dense;    /* of those, the ones that needed partial pivoting       */
+  int32_t tail_rounds;      /* rounds run with a CTA per live instance over the list of
+                               live instances (once no more are live than SMs)       */
 } karam_timing;
 KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 

@@ -99,7 +99,8 @@ struct karam_problem {
   int ld = 0;
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
-      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws;
+      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws,
+      i_live;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
@@ -576,9 +577,16 @@ int tuned_schedule(const karam_problem* p, int prec) {
 // opts->kernel_timing, event records between the kernels time each of them;
 // they are left out otherwise, since they cost more than the empty launches
 // of a round.
+//
+// Tail: once no more instances are live than the GPU has SMs, a problem on
+// the warp-per-instance level schedule switches to a second graph in which
+// k_lu_big gives each live instance a CTA of its own, over a list of the live
+// instances that the kernel itself refreshes every round (two lists, in turn).
+// k_lu_big runs the same arithmetic as k_lu_nd, so the results do not change;
+// a round with one live instance takes well under half the time.
 void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* opts,
                 const DevInst* inst = nullptr) {
-  constexpr int kRounds = 16;
+  constexpr int kRounds = 16;  // even: the tail rounds alternate between two lists
   const int max_rounds = opts ? opts->max_rounds : 0;
   int want_lanes = opts ? opts->schedule : 0;
   if (want_lanes == 0) want_lanes = tuned_schedule(p, P.precision);
@@ -586,12 +594,18 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   cudaStream_t s = p->ctx->stream;
   DevInst I = inst ? *inst : dev_inst(p);
   const int prec = P.precision;
-  RoundLaunch L = plan_round(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms, want_lanes);
+  const int max_smem = p->ctx->max_smem, num_sms = p->ctx->num_sms;
+  RoundLaunch L = plan_round(p->dt, p->ni, prec, max_smem, num_sms, want_lanes);
   if (L.L < 1)
     throw std::runtime_error(std::string("no factor/solve schedule fits this problem; last: ") + L.why);
   ck(cudaGetLastError(), "configure kernels");
   p->timing.lanes = L.L;
   p->timing.level_schedule = L.big ? 1 + L.big : L.nd ? 1 : 0;
+  RoundLaunch LT;  // the tail's block-per-instance plan (L == 0: no tail switch)
+  if (L.nd && p->ni > num_sms) {  // L.nd: the packed program exists
+    LT = plan_round(p->dt, p->ni, prec, max_smem, num_sms, -3);
+    cudaGetLastError();
+  }
   if (L.big == 2) {  // the ND slots of every instance in global memory
     const size_t need = (size_t)p->ni * (size_t)p->dt.nd_S * sizeof(double);
     if (p->i_luws.bytes < need) p->i_luws.alloc(need);
@@ -607,50 +621,56 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   } eg{ev};
   int* active = p->d_active.as<int>();
 
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-  // External event records become event-record nodes of the graph (a plain
-  // record inside capture would only order work within the capture).
-  // a launch that fails inside the capture is reported by name
-  const char* failed = nullptr;
-  cudaError_t launch_err = cudaSuccess;
-  auto check = [&](const char* what) {
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess && launch_err == cudaSuccess) {
-      launch_err = e;
-      failed = what;
-    }
-  };
-  for (int r = 0; r < kRounds; ++r) {
-    if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
-    if (timed) cudaEventRecordWithFlags(ev[4 * r], s, cudaEventRecordExternal);
-    launch_eval_stamp(p->dt, I, P, L, prec, s);
-    check("k_es launch");
-    if (timed) cudaEventRecordWithFlags(ev[4 * r + 1], s, cudaEventRecordExternal);
-    launch_lu(p->dt, I, P, L, prec, active, s);
-    check("k_lu launch");
-    if (timed) cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
-    if (I.rescue_list) launch_rescue(p->dt, I, P, p->rplan, s);
-    check("k_rescue launch");
-    if (timed) cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
-  }
-  const cudaError_t end_err = cudaStreamEndCapture(s, &graph);
-  ck(launch_err, failed ? failed : "kernel launch in capture");
-  ck(end_err, "end capture");
-  struct GraphGuard {
-    cudaGraph_t& g;
-    cudaGraphExec_t& e;
-    ~GraphGuard() {
+  struct Graph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~Graph() {
       if (e) cudaGraphExecDestroy(e);
       if (g) cudaGraphDestroy(g);
     }
-  } gg{graph, exec};
-  ck(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+  };
+  // kRounds rounds on plan Lp, round r with the instances of Iv[r % 2]
+  auto capture = [&](Graph& G, const RoundLaunch& Lp, const DevInst* Iv) {
+    ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    // External event records become event-record nodes of the graph (a plain
+    // record inside capture would only order work within the capture); a
+    // launch that fails inside the capture is reported by name
+    const char* failed = nullptr;
+    cudaError_t launch_err = cudaSuccess;
+    auto check = [&](const char* what) {
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess && launch_err == cudaSuccess) {
+        launch_err = e;
+        failed = what;
+      }
+    };
+    for (int r = 0; r < kRounds; ++r) {
+      const DevInst& Ir = Iv[r & 1];
+      if (r == kRounds - 1) cudaMemsetAsync(active, 0, sizeof(int), s);
+      if (timed) cudaEventRecordWithFlags(ev[4 * r], s, cudaEventRecordExternal);
+      launch_eval_stamp(p->dt, Ir, P, Lp, prec, s);
+      check("k_es launch");
+      if (timed) cudaEventRecordWithFlags(ev[4 * r + 1], s, cudaEventRecordExternal);
+      launch_lu(p->dt, Ir, P, Lp, prec, active, s);
+      check("k_lu launch");
+      if (timed) cudaEventRecordWithFlags(ev[4 * r + 2], s, cudaEventRecordExternal);
+      if (Ir.rescue_list) launch_rescue(p->dt, Ir, P, p->rplan, s);
+      check("k_rescue launch");
+      if (timed) cudaEventRecordWithFlags(ev[4 * r + 3], s, cudaEventRecordExternal);
+    }
+    const cudaError_t end_err = cudaStreamEndCapture(s, &G.g);
+    ck(launch_err, failed ? failed : "kernel launch in capture");
+    ck(end_err, "end capture");
+    ck(cudaGraphInstantiate(&G.e, G.g, 0), "graph instantiate");
+  };
+  Graph main_g, tail_g;
+  const DevInst Im[2] = {I, I};
+  capture(main_g, L, Im);
+  bool tail = false;
 
   const int budget = max_rounds > 0 ? max_rounds : (1 << 30);
   while (true) {
-    ck(cudaGraphLaunch(exec, s), "graph launch");
+    ck(cudaGraphLaunch(tail ? tail_g.e : main_g.e, s), "graph launch");
     ck(cudaMemcpyAsync(p->h_active, active, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
     ck(cudaStreamSynchronize(s), "round sync");
     for (int r = 0; r < kRounds && timed; ++r) {
@@ -666,7 +686,31 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
     p->timing.lu_launches += kRounds;
     if (I.rescue_list) p->timing.rescue_launches += kRounds;
     p->timing.rounds += kRounds;
+    if (tail) p->timing.tail_rounds += kRounds;
     if (*p->h_active == 0 || p->timing.rounds >= budget) break;
+    if (!tail && LT.L > 0 && *p->h_active <= num_sms) {
+      // lists: [count 0, count 1, pad to 16 B, list 0 [ni], list 1 [ni]]
+      const size_t need = sizeof(int) * (4 + 2 * (size_t)p->ni);
+      if (p->i_live.bytes < need) p->i_live.alloc(need);
+      int* cnt = p->i_live.as<int>();
+      int* list0 = cnt + 4;
+      int* list1 = list0 + p->ni;
+      ck(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), s), "memset live counts");
+      launch_live_list(I, list0, cnt, s);
+      ck(cudaGetLastError(), "k_live_list launch");
+      DevInst It[2] = {I, I};
+      It[0].live_in = list0;
+      It[0].live_in_count = cnt;
+      It[0].live_out = list1;
+      It[0].live_out_count = cnt + 1;
+      It[1].live_in = list1;
+      It[1].live_in_count = cnt + 1;
+      It[1].live_out = list0;
+      It[1].live_out_count = cnt;
+      LT.grid = *p->h_active;  // instances only ever leave the live set
+      capture(tail_g, LT, It);
+      tail = true;
+    }
   }
 }
 
@@ -1097,10 +1141,11 @@ int karam_tune_schedule(karam_problem* p, const karam_solver_opts* opts, int32_t
     o.seeded = KARAM_SEED_NONE;  // trial rounds from the reference seed
     const int prec = o.precision;
     // the feasible schedules: the planner's choice, then a CTA per instance
-    // with the slots in shared or global memory (option values as in
+    // with the slots and the packed program in shared memory, with the slots
+    // alone in shared memory, or in global memory (option values as in
     // karam_solver_opts.schedule)
     std::vector<int> cands;
-    for (int want : {0, -1, -2}) {
+    for (int want : {0, -3, -1, -2}) {
       const RoundLaunch L = plan_round(p->dt, p->ni, prec, p->ctx->max_smem, p->ctx->num_sms, want);
       cudaGetLastError();
       if (L.L < 1) continue;

@@ -36,6 +36,8 @@ inline int lane_stride(int ni) { return (ni + 31) / 32 * 32; }
 RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num_sms,
                        int want_lanes);
 void launch_init(const DevTopo& T, const DevInst& I, const JobParams& P, cudaStream_t s);
+// Lists the instances not yet done into list[0..*count) (*count starts at 0).
+void launch_live_list(const DevInst& I, int* list, int* count, cudaStream_t s);
 // The batch statistical seed from the DC solutions of instances 0..W-1 (lane 0
 // of `seed`); *ok = 1 when it is confident enough to use.
 void launch_ema_seed(const DevTopo& T, const DevInst& I, int W, double* seed, int* ok,

@@ -53,8 +53,12 @@ namespace {
 
 // The factor/solve kernel of a candidate schedule.
 const void* lu_kernel(bool mixed, bool nd, int big) {
-  if (big == 1) return mixed ? (const void*)k_lu_big<float, false> : (const void*)k_lu_big<double, false>;
-  if (big == 2) return mixed ? (const void*)k_lu_big<float, true> : (const void*)k_lu_big<double, true>;
+  if (big == 1)
+    return mixed ? (const void*)k_lu_big<float, false, false> : (const void*)k_lu_big<double, false, false>;
+  if (big == 2)
+    return mixed ? (const void*)k_lu_big<float, true, false> : (const void*)k_lu_big<double, true, false>;
+  if (big == 3)
+    return mixed ? (const void*)k_lu_big<float, false, true> : (const void*)k_lu_big<double, false, true>;
   if (nd) return mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>;
   return mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>;
 }
@@ -82,6 +86,7 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
   if (T.nd_prog_len > 0)
     for (int L = (mixed ? 32 : 16); L >= 1; --L) cands.push_back({L, true, 0, 3});
   if (T.nd_levels > 0) {
+    if (T.nd_prog_len > 0) cands.push_back({1, false, 3, 2});
     cands.push_back({1, false, 1, 2});
     cands.push_back({1, false, 2, 1});
   }
@@ -95,6 +100,9 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
     size_t sm;
     if (c.big == 1)
       sm = es * ((size_t)T.nd_SY + (size_t)T.nd_S);
+    else if (c.big == 3)
+      sm = ((es * ((size_t)T.nd_SY + (size_t)T.nd_S) + 15) & ~size_t(15)) +
+           sizeof(int) * (((size_t)T.nd_prog_len + 3) & ~size_t(3));
     else if (c.big == 2)
       sm = (es * (size_t)T.nd_SY + 15) & ~size_t(15);
     else
@@ -150,6 +158,10 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
   return best;
 }
 
+void launch_live_list(const DevInst& I, int* list, int* count, cudaStream_t s) {
+  k_live_list<<<(I.ni + 255) / 256, 256, 0, s>>>(I, list, count);
+}
+
 void launch_init(const DevTopo& T, const DevInst& I, const JobParams& P, cudaStream_t s) {
   k_init<<<(I.ni + 127) / 128, 128, 0, s>>>(T, I, P);
 }
@@ -177,14 +189,19 @@ void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const Rou
                int prec, int* active, cudaStream_t s) {
   if (L.big == 1) {
     if (prec == KARAM_PREC_MIXED)
-      k_lu_big<float, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+      k_lu_big<float, false, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
     else
-      k_lu_big<double, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+      k_lu_big<double, false, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
   } else if (L.big == 2) {
     if (prec == KARAM_PREC_MIXED)
-      k_lu_big<float, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+      k_lu_big<float, true, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
     else
-      k_lu_big<double, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+      k_lu_big<double, true, false><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+  } else if (L.big == 3) {
+    if (prec == KARAM_PREC_MIXED)
+      k_lu_big<float, false, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+    else
+      k_lu_big<double, false, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
   } else if (L.nd) {
     if (prec == KARAM_PREC_MIXED)
       k_lu_nd<float><<<L.grid, L.threads, L.smem, s>>>(T, I, P, L.L, active);

@@ -734,9 +734,13 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
   const int g = blockIdx.x * 32 + lane;
   const size_t ld = I.ld;
   const int nv = T.nv;
-  // this round's rescue list starts empty (the previous round's k_rescue has
-  // finished; this round's k_lu appends to it)
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && I.rescue_count) *I.rescue_count = 0;
+  // this round's rescue list (and, in tail rounds, its list of instances
+  // still live after it) starts empty: the previous round's k_rescue has
+  // finished, and this round's k_lu appends to them
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    if (I.rescue_count) *I.rescue_count = 0;
+    if (I.live_out_count) *I.live_out_count = 0;
+  }
   const double heff = g < I.ni ? I.ev_heff[g] : -1.0;
   const bool live = heff >= 0.0;
   if (!__syncthreads_or(live)) return;
@@ -1109,6 +1113,103 @@ __device__ __forceinline__ int instance_finish(const DevTopo& Tp, const DevInst&
   const InstState st2 = I.st[g];
   set_eval_point(I, P, g, st2);
   return st2.mode != MODE_DONE;
+}
+
+// nd_solve spread over a whole CTA: the same packed program in shared memory,
+// each phase's items over the CTA's threads, long lists summed by one warp in
+// nd_solve's fixed tree, short ones by one thread in order -- so the result
+// is nd_solve's, bit for bit.
+template <typename T>
+__device__ bool nd_solve_cta(T* __restrict__ A, T* __restrict__ y, const int* __restrict__ prog,
+                             T gmin, T tiny, T growth_limit) {
+  const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+  const int NL = prog[0], lvt = prog[1], tpb = prog[2], ypb = prog[3], bpb = prog[4];
+  bool ok = true;
+  T lmax = T(0);
+  for (int lv = 0; lv < NL; ++lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    const int po = Lt[0], pc = Lt[1], lo = Lt[2], lc = Lt[3];
+    for (int q = tid; q < pc; q += bd) {
+      const int d = prog[po + q];
+      const T piv = A[d] + gmin;
+      ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
+      A[d] = recip(piv);
+    }
+    __syncthreads();
+    for (int e = tid; e < lc; e += bd) {
+      const int v = prog[lo + e];
+      const int sl = v & 0xFFFF;
+      const T l = A[sl] * A[(v >> 16) & 0xFFFF];
+      A[sl] = l;
+      lmax = fmax(lmax, fabs(l));
+    }
+    __syncthreads();
+    const int to = Lt[4], tsc = Lt[5], tlc = Lt[6];
+    for (int t = tid; t < tsc; t += bd) {
+      const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
+      const int sl = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
+      T acc = A[sl];
+      for (int q = 0; q < c; ++q) {
+        const int pr = prog[off + q];
+        acc -= A[pr & 0xFFFF] * A[(pr >> 16) & 0xFFFF];
+      }
+      A[sl] = acc;
+    }
+    const int yo = Lt[7], ysc = Lt[8], ylc = Lt[9];
+    for (int r = tid; r < ysc; r += bd) {
+      const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
+      const int row = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
+      T acc = y[row];
+      for (int q = 0; q < c; ++q) {
+        const int pr = prog[off + q];
+        acc -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
+      }
+      y[row] = acc;
+    }
+    for (int t = tsc + warp; t < tsc + tlc; t += nw) {
+      const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
+      const int c = (h >> 16) & 0xFFFF;
+      T part = T(0);
+      for (int q = lane; q < c; q += 32) {
+        const int pr = prog[off + q];
+        part += A[pr & 0xFFFF] * A[(pr >> 16) & 0xFFFF];
+      }
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) A[h & 0xFFFF] -= part;
+    }
+    for (int r = ysc + warp; r < ysc + ylc; r += nw) {
+      const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
+      const int c = (h >> 16) & 0xFFFF;
+      T part = T(0);
+      for (int q = lane; q < c; q += 32) {
+        const int pr = prog[off + q];
+        part += A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
+      }
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if (lane == 0) y[h & 0xFFFF] -= part;
+    }
+    __syncthreads();
+  }
+  bool finite = true;
+  for (int lv = NL - 1; lv >= 0; --lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    const int bo = Lt[10], bc = Lt[11];
+    for (int q = tid; q < bc; q += bd) {
+      const int a = prog[bo + 2 * q], b = prog[bo + 2 * q + 1];
+      const int k = a & 0xFFFF, d = (a >> 16) & 0xFFFF;
+      const int c = b & 0xFFFF, off = bpb + ((b >> 16) & 0xFFFF);
+      T sv = y[k];
+      for (int j = 0; j < c; ++j) {
+        const int pr = prog[off + j];
+        sv -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
+      }
+      sv *= A[d];
+      y[k] = sv;
+      finite = finite && isfinite(sv);
+    }
+    __syncthreads();
+  }
+  return __syncthreads_and(ok && finite && !(lmax > growth_limit)) != 0;
 }
 
 // Control flow + linear solve of a tile of L instances (one CTA): decisions
@@ -1492,20 +1593,38 @@ __device__ bool big_solve(T* __restrict__ A, T* __restrict__ y, const DevTopo& T
 }
 
 // Control flow + linear solve of one instance per CTA on the level schedule
-// (instances whose ND slots do not fit a warp's share of shared memory): the
-// same round as lu_round with every phase spread over the CTA's threads.
-// The ND slots live in dynamic shared memory after the right-hand side
-// (gA = false) or in the instance's slice of I.lu_ws (gA = true, nd_S
-// elements per instance).
-template <typename T, bool gA>
+// (instances whose ND slots do not fit a warp's share of shared memory, and
+// the last few live instances of a job): the same round as lu_round with
+// every phase spread over the CTA's threads. The ND slots live in dynamic
+// shared memory after the right-hand side (gA = false) or in the instance's
+// slice of I.lu_ws (gA = true, nd_S elements per instance). With packed,
+// the CTA stages the packed program (nd_program) after the slots and solves
+// on it (nd_solve_cta) instead of reading the schedule tables from global
+// memory. With I.live_in, CTA b takes the b-th listed instance and lists it
+// in I.live_out when it stays live.
+template <typename T, bool gA, bool packed>
 __global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, JobParams P, int* active) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_a, s_live, s_trev, s_sing;
   __shared__ double s_gmin, s_hsub;
-  const int n = Tp.n, tid = threadIdx.x, g = blockIdx.x;
+  const int n = Tp.n, tid = threadIdx.x;
+  int g = blockIdx.x;
+  if (I.live_in) {
+    if ((int)blockIdx.x >= *I.live_in_count) return;
+    g = I.live_in[blockIdx.x];
+  }
   const size_t ld = I.ld;
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* A = gA ? reinterpret_cast<T*>(I.lu_ws) + (size_t)g * Tp.nd_S : Y + Tp.nd_SY;
+  const int* prog = nullptr;
+  if (packed) {  // after the slots, on a 16-byte boundary
+    int* dst = reinterpret_cast<int*>(
+        smem_raw + (((size_t)(Tp.nd_SY + Tp.nd_S) * sizeof(T) + 15) & ~size_t(15)));
+    const int4* srcp = reinterpret_cast<const int4*>(Tp.nd_prog);
+    for (int e = tid; e < (Tp.nd_prog_len + 3) / 4; e += blockDim.x)
+      reinterpret_cast<int4*>(dst)[e] = __ldg(&srcp[e]);
+    prog = dst;
+  }
   if (tid == 0) {
     int live = 0, trev = 0;
     double gm = 1e-12, hs = P.h;
@@ -1596,7 +1715,8 @@ __global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, J
   if (a & ACT_SOLVE) {
     const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
     const T growth = sizeof(T) == 8 ? (T)P.growth64 : (T)fmin(P.growth32, 3.0e38);
-    const bool ok = big_solve<T>(A, Y, Tp, (T)gmin, tiny, growth);
+    const bool ok = packed ? nd_solve_cta<T>(A, Y, prog, (T)gmin, tiny, growth)
+                           : big_solve<T>(A, Y, Tp, (T)gmin, tiny, growth);
     // x = v + dx, then junction limiting level by level
     if (ok) {
       for (int i = tid; i < n; i += blockDim.x) {
@@ -1621,12 +1741,21 @@ __global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, J
   // rescue hand-off, next evaluation point, bookkeeping
   if (tid == 0) {
     const int sing = s_sing;
-    if (instance_finish(Tp, I, P, g, a, sing, gmin)) atomicAdd(active, 1);
+    if (instance_finish(Tp, I, P, g, a, sing, gmin)) {
+      atomicAdd(active, 1);
+      if (I.live_out) I.live_out[atomicAdd(I.live_out_count, 1)] = g;
+    }
     if (I.counters) {
       atomicAdd(&I.counters[s_trev ? 1 : 0], 1ull);
       if ((a & ACT_SOLVE) && !sing) atomicAdd(&I.counters[2], 1ull);
     }
   }
+}
+
+// The instances not yet done, listed (any order) for the tail rounds.
+__global__ void k_live_list(DevInst I, int* list, int* count) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < I.ni && I.st[g].mode != MODE_DONE) list[atomicAdd(count, 1)] = g;
 }
 
 // ---------------------------------------------------------------------------

@@ -180,6 +180,10 @@ struct DevInst {
   RescueItem* rescue_list;  // [ni]
   int* rescue_count;
   int rescue_slots;         // rescue warps (one workspace each)
+  const int* live_in;       // tail rounds: the instances live at the start of the round (the
+  const int* live_in_count; // block-per-instance kernel takes CTA b -> live_in[b]), else 0
+  int* live_out;            // ... and the ones still live after it (filled by that kernel;
+  int* live_out_count;      // the count is cleared by the round's k_es)
   void* lu_ws;              // [ni][nd_S] ND slots of the block-per-instance kernel when they
                             // live in global memory (float or double), else 0
   double* hub_part;         // [n_hub_rows][ld] hub items' sums per device chunk

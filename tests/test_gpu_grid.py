@@ -19,7 +19,7 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 pytestmark = pytest.mark.gpu
 
 POLISH = dict(polish_max=8)
-KIND = {1: 1, -1: 2, -2: 3}  # schedule option -> karam_timing.level_schedule
+KIND = {1: 1, -1: 2, -2: 3, -3: 4}  # schedule option -> karam_timing.level_schedule
 
 
 def scaled_err(v, v_ref, rel=1e-9, abs_=1e-12):
@@ -34,7 +34,7 @@ def solve(product, ctx, nl, inst, ni, prec, schedule):
 
 
 @pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
-@pytest.mark.parametrize("schedule", [1, -1, -2])
+@pytest.mark.parametrize("schedule", [1, -1, -2, -3])
 def test_grid8_dc_matches_reference_fixture(product, ctx, prec, schedule):
     g = np.load(os.path.join(HERE, "golden", "grid8.npz"))
     nl = circuits.grid_circuit(8)
@@ -49,7 +49,7 @@ def test_schedules_give_identical_results(product, ctx, prec):
     nl = circuits.grid_circuit(10)
     inst = circuits.mc_instances(nl, 5)
     out = []
-    for schedule in (1, -1, -2):
+    for schedule in (1, -1, -2, -3):
         prob, v, st = solve(product, ctx, nl, inst, 5, prec, schedule)
         assert prob.timing()["level_schedule"] == KIND[schedule]
         out.append((v, [s["iterations"] for s in st]))
@@ -100,7 +100,7 @@ def test_tuned_schedule_is_used_and_feasible(product, ctx):
     prob.set_instances(inst)
     opts = product.options(precision=A.PREC_MIXED, **POLISH)
     sch, ms = prob.tune_schedule(opts, rounds=8)
-    assert ms > 0 and (sch in (-1, -2) or 1 <= sch <= 32)
+    assert ms > 0 and (sch in (-1, -2, -3) or 1 <= sch <= 32)
     v_tuned, st_tuned = prob.solve_dc(opts)  # opts.schedule == 0: the tuned choice
     kind_tuned = prob.timing()["level_schedule"]
     v_explicit, st_explicit = prob.solve_dc(product.options(precision=A.PREC_MIXED,
@@ -108,3 +108,29 @@ def test_tuned_schedule_is_used_and_feasible(product, ctx):
     assert prob.timing()["level_schedule"] == kind_tuned
     assert np.array_equal(v_tuned, v_explicit)
     assert all(s["status"] == A.ST_CONVERGED for s in st_tuned)
+
+
+@pytest.mark.parametrize("prec", [A.PREC_MIXED, A.PREC_FP64])
+def test_tail_switch_keeps_results(product, ctx, prec):
+    """A batch larger than the SM count runs its last rounds with a CTA per
+    live instance over the live list (karam_timing.tail_rounds); the results
+    equal a run on that kernel from the start, and one on the warp kernel."""
+    nl = circuits.config2()
+    ni = 320
+    inst = circuits.mc_instances(nl, ni)
+    prob = product.Problem(ctx, nl, max_instances=ni)
+    prob.set_instances(inst)
+    runs = []
+    for schedule in (0, -1, -3):
+        opts = product.options(precision=prec, schedule=schedule, **POLISH)
+        prob.run_mc_device(1e-12, 20, A.TRAN_BE, opts)
+        t = prob.timing()
+        v, st = prob.read_results()
+        runs.append((t, v, st))
+    (t0, v0, s0), (t1, v1, s1), (t3, v3, s3) = runs
+    assert t0["level_schedule"] == 1 and t0["tail_rounds"] > 0
+    assert t1["level_schedule"] == 2 and t1["tail_rounds"] == 0
+    assert t3["level_schedule"] == 4 and t3["tail_rounds"] == 0
+    assert np.array_equal(v0, v1) and np.array_equal(v0, v3)
+    assert [s["iterations"] for s in s0] == [s["iterations"] for s in s1]
+    assert sum(s["status"] == A.ST_CONVERGED for s in s0) >= ni - 2
