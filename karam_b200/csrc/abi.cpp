@@ -698,6 +698,7 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
       ck(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), s), "memset live counts");
       launch_live_list(I, list0, cnt, s);
       ck(cudaGetLastError(), "k_live_list launch");
+      ++p->timing.other_launches;
       DevInst It[2] = {I, I};
       It[0].live_in = list0;
       It[0].live_in_count = cnt;
