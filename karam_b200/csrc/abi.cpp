@@ -91,7 +91,7 @@ struct karam_problem {
       t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
       t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_es_hubc, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
-      t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent;
+      t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent, t_mos_order;
   DBuf t_nd[23];  // level schedule tables, in karam_get_lu_schedule's order
   DBuf t_nd_prog;  // the packed schedule (padded to whole int4)
   DevTopo dt{};
@@ -100,7 +100,7 @@ struct karam_problem {
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
       d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws,
-      i_live;
+      i_live, i_stage;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
@@ -254,6 +254,7 @@ void upload_topology(karam_problem* p) {
   upload(p->t_seed_vs, seed_vs);
   upload(p->t_seed_anode, seed_an);
   upload(p->t_perm, T.perm);
+  upload(p->t_mos_order, T.mos_order);
   std::vector<int2> src;
   for (int s = 0; s < T.nv; ++s) src.push_back(make_int2(T.slot_row[s], T.slot_col[s]));
   upload(p->t_slot_rc, src);
@@ -472,14 +473,17 @@ void set_instances_impl(karam_problem* p, const karam_instances* inst) {
   int ni = inst ? inst->n_instances : 1;
   if (ni < 1 || ni > p->max_inst) throw std::runtime_error("n_instances out of range");
   const size_t nm = T.mos.size(), nv = T.vs.size(), ld = (size_t)p->ld;
-  // instance-interleaved: item k of instance i at [k * ld + i]
-  std::vector<float> kp(ld * nm, 0.0f), vth(ld * nm, 0.0f);
+  // instance-interleaved: item k of instance i at [k * ld + i]. Per-instance
+  // KP / VTO go to the device as the caller laid them out ([instance][MOSFET],
+  // netlist order) and are interleaved there; model-card values and the
+  // sources are laid out here.
+  const bool dev_kp = inst && inst->mos_kp, dev_vth = inst && inst->mos_vto;
+  std::vector<float> kp(dev_kp ? 0 : ld * nm, 0.0f), vth(dev_vth ? 0 : ld * nm, 0.0f);
   std::vector<double> vdc(ld * nv, 0.0), v1(ld * nv, 0.0), v2(ld * nv, 0.0);
   for (int i = 0; i < ni; ++i) {
-    for (size_t j = 0; j < nm; ++j) {
-      const size_t src = (size_t)i * nm + T.mos_order[j];
-      kp[j * ld + i] = (inst && inst->mos_kp) ? inst->mos_kp[src] : (float)T.mos[j].kp_card;
-      vth[j * ld + i] = (inst && inst->mos_vto) ? inst->mos_vto[src] : (float)T.mos[j].vto_card;
+    for (size_t j = 0; j < nm && !(dev_kp && dev_vth); ++j) {
+      if (!dev_kp) kp[j * ld + i] = (float)T.mos[j].kp_card;
+      if (!dev_vth) vth[j * ld + i] = (float)T.mos[j].vto_card;
     }
     for (size_t s = 0; s < nv; ++s) {
       const auto& V = T.vs[s];
@@ -498,8 +502,24 @@ void set_instances_impl(karam_problem* p, const karam_instances* inst) {
   p->inst_vth = inst && inst->mos_vto;
   cudaStream_t s = p->ctx->stream;
   if (nm) {
-    ck(cudaMemcpyAsync(p->i_kp.p, kp.data(), kp.size() * sizeof(float), cudaMemcpyHostToDevice, s), "H2D kp");
-    ck(cudaMemcpyAsync(p->i_vth.p, vth.data(), vth.size() * sizeof(float), cudaMemcpyHostToDevice, s), "H2D vth");
+    const size_t rows = (size_t)ni * nm;
+    if ((dev_kp || dev_vth) && p->i_stage.bytes < 2 * (size_t)p->max_inst * nm * sizeof(float))
+      p->i_stage.alloc(2 * (size_t)p->max_inst * nm * sizeof(float));
+    float* stage = p->i_stage.as<float>();
+    auto put = [&](bool dev, const float* src, const std::vector<float>& host, DBuf& dst, float* stg,
+                   const char* what) {
+      if (dev) {
+        ck(cudaMemcpyAsync(stg, src, rows * sizeof(float), cudaMemcpyHostToDevice, s), what);
+        interleave_f(stg, p->t_mos_order.as<int>(), dst.as<float>(), ni, (int)ld, (int)nm, s);
+        ck(cudaGetLastError(), "k_interleave_f launch");
+      } else {
+        ck(cudaMemcpyAsync(dst.p, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+           what);
+      }
+    };
+    put(dev_kp, dev_kp ? inst->mos_kp : nullptr, kp, p->i_kp, stage, "H2D kp");
+    put(dev_vth, dev_vth ? inst->mos_vto : nullptr, vth, p->i_vth,
+        stage + (size_t)p->max_inst * nm, "H2D vth");
   }
   if (nv) {
     ck(cudaMemcpyAsync(p->i_vsdc.p, vdc.data(), vdc.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D vs");

@@ -70,6 +70,9 @@ void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const
                    cudaStream_t s);
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s);
+// [ni][n] FP32 per-device parameters (netlist order) into [n][ld] SoA order.
+void interleave_f(const float* src, const int* order, float* dst, int ni, int ld, int n,
+                  cudaStream_t s);
 void interleave(const double* src, const int* perm, double* dst, int ni, int ld, int n,
                 cudaStream_t s);
 

@@ -257,6 +257,11 @@ void unpermute(const double* v_perm, const int* perm, double* out, int ni, int l
   k_unpermute<<<grid_for((size_t)n * ld, 256), 256, 0, s>>>(v_perm, perm, out, ni, ld, n);
 }
 
+void interleave_f(const float* src, const int* order, float* dst, int ni, int ld, int n,
+                  cudaStream_t s) {
+  k_interleave_f<<<grid_for((size_t)n * ld, 256), 256, 0, s>>>(src, order, dst, ni, ld, n);
+}
+
 void interleave(const double* src, const int* perm, double* dst, int ni, int ld, int n,
                 cudaStream_t s) {
   k_interleave<<<grid_for((size_t)n * ld, 256), 256, 0, s>>>(src, perm, dst, ni, ld, n);

@@ -2406,6 +2406,18 @@ __global__ void k_unpermute(const double* vp, const int* perm, double* out, int 
   }
 }
 
+// The same for FP32 per-device parameters: [ni][n] in netlist order into
+// [n][ld] in SoA order (item p takes netlist item order[p]).
+__global__ void k_interleave_f(const float* src, const int* order, float* dst, int ni, int ld, int n) {
+  const size_t total = (size_t)n * ld;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int p = (int)(e / ld);
+    const int g = (int)(e - (size_t)p * ld);
+    dst[e] = g < ni ? src[(size_t)g * n + order[p]] : 0.0f;
+  }
+}
+
 // Interleaves an instance-major [ni][n] host-order block into [n][ld] permuted.
 __global__ void k_interleave(const double* src, const int* perm, double* dst, int ni, int ld, int n) {
   const size_t total = (size_t)n * ld;
