@@ -665,20 +665,71 @@ void nd_schedule(Topology& T) {
   T.nd_pos.assign(n, 0);
   for (int p = 0; p < n; ++p) T.nd_pos[order[p]] = p;
 
-  // unsymmetric symbolic elimination in ND order
-  std::vector<std::set<int>> R(n), Cc(n);
-  for (auto& q : pos) {
-    const int r = T.nd_pos[q.first], c = T.nd_pos[q.second];
-    R[r].insert(c);
-    Cc[c].insert(r);
-  }
-  std::vector<std::vector<int>> Lk(n), Uk(n);
-  for (int k = 0; k < n; ++k) {
-    for (auto it = Cc[k].upper_bound(k); it != Cc[k].end(); ++it) Lk[k].push_back(*it);
-    for (auto it = R[k].upper_bound(k); it != R[k].end(); ++it) Uk[k].push_back(*it);
-    for (int i : Lk[k])
-      for (int j : Uk[k])
-        if (R[i].insert(j).second) Cc[j].insert(i);
+  // unsymmetric symbolic elimination in ND order (rows and columns as bit
+  // rows up to 16384 unknowns, else ordered sets; the same structure either
+  // way), then each row's columns in ascending order
+  std::vector<std::vector<int>> Lk(n), Uk(n), Rrow(n);
+  if (n <= 16384) {
+    const size_t W = ((size_t)n + 63) / 64;
+    std::vector<uint64_t> Rb(W * (size_t)n, 0), Cb(W * (size_t)n, 0);
+    auto set_bit = [&](std::vector<uint64_t>& B, int a, int b) { B[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
+    for (auto& q : pos) {
+      const int r = T.nd_pos[q.first], c = T.nd_pos[q.second];
+      set_bit(Rb, r, c);
+      set_bit(Cb, c, r);
+    }
+    auto above = [&](const std::vector<uint64_t>& B, int k, std::vector<int>& out) {
+      const uint64_t* row = &B[(size_t)k * W];
+      for (size_t q = (size_t)(k + 1) >> 6; q < W; ++q) {
+        uint64_t c = row[q];
+        if (q == ((size_t)(k + 1) >> 6)) c &= ~0ull << ((k + 1) & 63);
+        while (c) {
+          out.push_back((int)(q * 64 + (size_t)__builtin_ctzll(c)));
+          c &= c - 1;
+        }
+      }
+    };
+    std::vector<uint64_t> ub(W);
+    for (int k = 0; k < n; ++k) {
+      above(Cb, k, Lk[k]);
+      above(Rb, k, Uk[k]);
+      if (Uk[k].empty()) continue;
+      std::fill(ub.begin(), ub.end(), 0ull);
+      for (int j : Uk[k]) ub[j >> 6] |= 1ull << (j & 63);
+      const size_t q0 = (size_t)Uk[k].front() >> 6, q1 = (size_t)Uk[k].back() >> 6;
+      for (int i : Lk[k]) {
+        uint64_t* ri = &Rb[(size_t)i * W];
+        for (size_t q = q0; q <= q1; ++q) {
+          uint64_t fresh = ub[q] & ~ri[q];
+          ri[q] |= ub[q];
+          while (fresh) {
+            const int j = (int)(q * 64 + (size_t)__builtin_ctzll(fresh));
+            set_bit(Cb, j, i);
+            fresh &= fresh - 1;
+          }
+        }
+      }
+    }
+    for (int r = 0; r < n; ++r) {  // every column of the row, ascending
+      const uint64_t* row = &Rb[(size_t)r * W];
+      for (size_t q = 0; q < W; ++q)
+        for (uint64_t c = row[q]; c; c &= c - 1) Rrow[r].push_back((int)(q * 64 + (size_t)__builtin_ctzll(c)));
+    }
+  } else {
+    std::vector<std::set<int>> R(n), Cc(n);
+    for (auto& q : pos) {
+      const int r = T.nd_pos[q.first], c = T.nd_pos[q.second];
+      R[r].insert(c);
+      Cc[c].insert(r);
+    }
+    for (int k = 0; k < n; ++k) {
+      for (auto it = Cc[k].upper_bound(k); it != Cc[k].end(); ++it) Lk[k].push_back(*it);
+      for (auto it = R[k].upper_bound(k); it != R[k].end(); ++it) Uk[k].push_back(*it);
+      for (int i : Lk[k])
+        for (int j : Uk[k])
+          if (R[i].insert(j).second) Cc[j].insert(i);
+    }
+    for (int r = 0; r < n; ++r) Rrow[r].assign(R[r].begin(), R[r].end());
   }
   // ND slots, row-major
   std::unordered_map<int64_t, int> slot;
@@ -687,7 +738,7 @@ void nd_schedule(Topology& T) {
   std::unordered_map<int64_t, int> mf;
   for (int sl = 0; sl < T.nv; ++sl) mf[key(T.slot_row[sl], T.slot_col[sl])] = sl;
   for (int r = 0; r < n; ++r)
-    for (int c : R[r]) {
+    for (int c : Rrow[r]) {
       slot[key(r, c)] = T.nd_nv++;
       auto f = mf.find(key(order[r], order[c]));
       T.nd_src.push_back(f == mf.end() ? -1 : f->second);
@@ -890,9 +941,39 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
         adj[a].insert(b);
         adj[b].insert(a);
       }
+  // Adjacency also as bit rows (up to 16384 vertices, 32 MiB): membership
+  // tests become bit tests and a vertex's missing neighbour pairs a sum of
+  // popcounts -- the same integers, so the order and its ties do not change.
+  const bool bits = nv <= 16384;
+  const size_t words = ((size_t)nv + 63) / 64;
+  std::vector<uint64_t> brow(bits ? words * (size_t)nv : 0);
+  auto bset = [&](int a, int b) { brow[(size_t)a * words + (b >> 6)] |= 1ull << (b & 63); };
+  auto bclr = [&](int a, int b) { brow[(size_t)a * words + (b >> 6)] &= ~(1ull << (b & 63)); };
+  auto bhas = [&](int a, int b) { return (brow[(size_t)a * words + (b >> 6)] >> (b & 63)) & 1ull; };
+  if (bits)
+    for (int a = 0; a < nv; ++a)
+      for (int b : adj[a]) bset(a, b);
+  std::vector<uint64_t> mask(bits ? words : 0);
   auto count_fill = [&](int u) {
-    uint32_t c = 0;
     std::vector<int> nb(adj[u].begin(), adj[u].end());
+    if (bits) {
+      // missing pairs = (k (k - 1) - sum over neighbours of their neighbours in N(u)) / 2
+      int lo = nv, hi = -1;
+      for (int w : nb) {
+        mask[w >> 6] |= 1ull << (w & 63);
+        lo = std::min(lo, w >> 6);
+        hi = std::max(hi, w >> 6);
+      }
+      uint64_t inside = 0;
+      for (int w : nb) {
+        const uint64_t* r = &brow[(size_t)w * words];
+        for (int q = lo; q <= hi; ++q) inside += (uint64_t)__builtin_popcountll(r[q] & mask[q]);
+      }
+      for (int w : nb) mask[w >> 6] = 0;
+      const uint64_t k = nb.size();
+      return (uint32_t)((k * (k > 0 ? k - 1 : 0) - inside) / 2);
+    }
+    uint32_t c = 0;
     for (size_t i = 0; i < nb.size(); ++i) {
       const auto& ai = adj[nb[i]];
       for (size_t j = i + 1; j < nb.size(); ++j)
@@ -929,20 +1010,50 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
     maxclique = std::max<uint32_t>(maxclique, (uint32_t)nb.size() + 1);
     nbset.clear();
     nbset.insert(nb.begin(), nb.end());
+    if (bits) {
+      for (int w : nb) mask[w >> 6] |= 1ull << (w & 63);
+      mask[u >> 6] |= 1ull << (u & 63);  // u is no candidate either
+    }
     dec.clear();
     for (size_t i = 0; i < nb.size(); ++i)
       for (size_t j = i + 1; j < nb.size(); ++j) {
         int a = nb[i], b = nb[j];
         if (adj[a].insert(b).second) {
           adj[b].insert(a);
+          if (bits) {
+            bset(a, b);
+            bset(b, a);
+          }
           // vertices outside N(u) adjacent to both a and b lose a missing pair
-          const auto& sa = adj[a].size() <= adj[b].size() ? adj[a] : adj[b];
-          const auto& sb = adj[a].size() <= adj[b].size() ? adj[b] : adj[a];
-          for (int w : sa)
-            if (w != a && w != b && w != u && !nbset.count(w) && sb.count(w)) dec[w]++;
+          if (bits) {
+            const uint64_t* ra = &brow[(size_t)a * words];
+            const uint64_t* rb = &brow[(size_t)b * words];
+            for (size_t q = 0; q < words; ++q) {
+              uint64_t c = ra[q] & rb[q] & ~mask[q];
+              while (c) {
+                dec[(int)(q * 64 + (size_t)__builtin_ctzll(c))]++;
+                c &= c - 1;
+              }
+            }
+          } else {
+            const auto& sa = adj[a].size() <= adj[b].size() ? adj[a] : adj[b];
+            const auto& sb = adj[a].size() <= adj[b].size() ? adj[b] : adj[a];
+            for (int w : sa)
+              if (w != a && w != b && w != u && !nbset.count(w) && sb.count(w)) dec[w]++;
+          }
         }
       }
-    for (int w : nb) adj[w].erase(u);
+    for (int w : nb) {
+      adj[w].erase(u);
+      if (bits) bclr(w, u);
+    }
+    if (bits) {
+      for (int w : nb) {
+        bclr(u, w);
+        mask[w >> 6] = 0;
+      }
+      mask[u >> 6] = 0;
+    }
     adj[u].clear();
     alive[u] = 0;
     for (auto& kv : dec) {
