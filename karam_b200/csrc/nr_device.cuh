@@ -1212,6 +1212,27 @@ __device__ bool nd_solve_cta(T* __restrict__ A, T* __restrict__ y, const int* __
   return __syncthreads_and(ok && finite && !(lmax > growth_limit)) != 0;
 }
 
+// Walks the (item i, listed instance k) pairs e = t, t + step, t + 2 step, ...
+// of an m-wide list (i = e / m, k = e % m) with one division per walk rather
+// than one per pair; m > 0.
+struct PairWalk {
+  int i, k, di, dk, m;
+  __device__ PairWalk(int t, int step, int m_) : m(m_) {
+    i = t / m_;
+    k = t - i * m_;
+    di = step / m_;
+    dk = step - di * m_;
+  }
+  __device__ void next() {
+    k += dk;
+    i += di;
+    if (k >= m) {
+      k -= m;
+      ++i;
+    }
+  }
+};
+
 // Control flow + linear solve of a tile of L instances (one CTA): decisions
 // from the reductions of k_es, vector updates, the Jacobian tile staged
 // into shared memory with cp.async, static-pivot LU with the forward
@@ -1312,8 +1333,8 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
     double* __restrict__ VT = I.v_tp;
     const double* __restrict__ F = I.F;
 #pragma unroll 2
-    for (int e = tid; e < m * n; e += blockDim.x) {
-      const int i = e / m, ln = s_list[e - i * m];
+    for (PairWalk w(tid, blockDim.x, m > 0 ? m : 1); m > 0 && w.i < n; w.next()) {
+      const int i = w.i, ln = s_list[w.k];
       const int act = s_act[ln];
       const double gmin = s_gmin[ln];
       const size_t o = (size_t)i * ld + base + ln;
@@ -1367,8 +1388,8 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
   }
 
   // 2c. capacitor history after a completed (sub-)step, waveform samples
-  for (int e = tid; e < m * Tp.n_cap; e += blockDim.x) {
-    const int c = e / m, ln = s_list[e - c * m];
+  for (PairWalk w(tid, blockDim.x, m > 0 ? m : 1); m > 0 && w.i < Tp.n_cap; w.next()) {
+    const int c = w.i, ln = s_list[w.k];
     const int act = s_act[ln];
     if (act & (ACT_TRAN_INIT | ACT_STEP)) {
       const int2 tt = __ldg(&Tp.cap_term[c]);
@@ -1428,8 +1449,8 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
       double* __restrict__ X = I.x;
       const double* __restrict__ V = I.v;
 #pragma unroll 2
-      for (int e = tid; e < m * n; e += blockDim.x) {
-        const int i = e / m, ln = s_list[e - i * m];
+      for (PairWalk w(tid, blockDim.x, m > 0 ? m : 1); m > 0 && w.i < n; w.next()) {
+        const int i = w.i, ln = s_list[w.k];
         const int act = s_act[ln];
         if (!(act & ACT_SOLVE) || s_sing[ln]) continue;
         const size_t o = (size_t)i * ld + base + ln;
@@ -1442,8 +1463,8 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
       const int lim_lane = tid < L && (s_act[tid] & ACT_SOLVE) && (s_act[tid] & ACT_LIMIT) && !s_sing[tid];
       if (__syncthreads_or(lim_lane)) {
         for (int lvl = 0; lvl < Tp.n_dio_levels; ++lvl) {
-          for (int e = tid; e < m * Tp.n_dio; e += blockDim.x) {
-            const int d = e / m, ln = s_list[e - d * m];
+          for (PairWalk w(tid, blockDim.x, m); w.i < Tp.n_dio; w.next()) {
+            const int d = w.i, ln = s_list[w.k];
             const int act = s_act[ln];
             if ((act & ACT_SOLVE) && (act & ACT_LIMIT) && !s_sing[ln] && __ldg(&Tp.dio_level[d]) == lvl)
               limit_one(Tp, d, I.x, I.v, ld, base + ln);
