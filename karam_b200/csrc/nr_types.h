@@ -32,7 +32,7 @@
 #ifndef KES_MAX_ITEMS
 #define KES_MAX_ITEMS 96
 #endif
-// Hub items (more devices than one block holds) sharing one device walk.
+// Hub items (more devices than one block holds) sharing one group of device chunks.
 #define KES_MAX_HUBS 4
 
 enum { MODE_DC = 0, MODE_TRAN = 1, MODE_DONE = 2 };

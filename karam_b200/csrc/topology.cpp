@@ -1422,7 +1422,7 @@ void es_blocks(Topology& T) {
       emit_group(items, dlist, lidx);
       continue;
     }
-    for (int it : items) {  // each hub walks its own term occurrences
+    for (int it : items) {  // each hub over its own term occurrences
       terms_of(it, tdev);
       std::vector<int> occ;
       std::vector<std::vector<int>> li(1);
