@@ -82,6 +82,8 @@ struct karam_problem {
   bool inst_kp = false, inst_vth = false;  // per-instance MOSFET values present
   bool have_dc = false;
   int tuned[2] = {0, 0};  // measured factor/solve schedule per precision (0 = none)
+  int n_hub_items = 0, n_hub_slot_terms = 0;
+  int max_hub_chunks = 0;  // k_es_one sums hub items of up to 8 chunks
   bool tran_started = false;  // capacitor history holds a transient in progress
   double t_now = 0.0, tran_h = 0.0;
   int tran_method = KARAM_TRAN_BE;
@@ -91,7 +93,8 @@ struct karam_problem {
       t_cap_c, t_mos_card, t_slot_rc, t_dio_lim, t_dio_level, t_vs_term, t_vs_kind, t_vs_pulse,
       t_is_term, t_is_amp, t_jlin, t_jcap_off, t_jcap_code, t_es_block, t_es_item, t_es_dev,
       t_es_jt, t_es_ft, t_es_fc, t_es_hub, t_es_hubc, t_lu_hdr, t_lu_data, t_lu_rec, t_lu_rec2, t_seed_vs, t_seed_anode,
-      t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent, t_mos_order;
+      t_perm, t_slot_ptr, t_csc_ptr, t_csc_ent, t_mos_order, t_jt_off, t_jt_code, t_ft_off, t_ft_code,
+      t_ft_a, t_ft_b, t_ft_coef, t_hub_items;
   DBuf t_nd[23];  // level schedule tables, in karam_get_lu_schedule's order
   DBuf t_nd_prog;  // the packed schedule (padded to whole int4)
   DevTopo dt{};
@@ -255,6 +258,29 @@ void upload_topology(karam_problem* p) {
   upload(p->t_seed_anode, seed_an);
   upload(p->t_perm, T.perm);
   upload(p->t_mos_order, T.mos_order);
+  upload(p->t_jt_off, T.jt_off);
+  upload(p->t_jt_code, T.jt_code);
+  upload(p->t_ft_off, T.ft_off);
+  upload(p->t_ft_code, T.ft_code);
+  upload(p->t_ft_a, T.ft_a);
+  upload(p->t_ft_b, T.ft_b);
+  upload(p->t_ft_coef, T.ft_coef);
+  {
+    // hub items from the chunk-0 block of each hub group
+    std::vector<int4> hubs;
+    p->n_hub_slot_terms = 0;
+    for (size_t b = 0; b < T.es_block.size() / 4; ++b)
+      if (T.es_block[4 * b + 1] < 0 && T.es_hubc[4 * b] == 0)
+        for (int m = 0; m < -T.es_block[4 * b + 1]; ++m) {
+          const int k = T.es_block[4 * b] + m, it = T.es_item[4 * k];
+          hubs.push_back(make_int4(it, T.es_item[4 * k + 3], T.es_hubc[4 * b + 1], p->n_hub_slot_terms));
+          if (it < T.nv) p->n_hub_slot_terms += T.jt_off[it + 1] - T.jt_off[it];
+        }
+    upload(p->t_hub_items, hubs);
+    p->n_hub_items = (int)hubs.size();
+    p->max_hub_chunks = 0;
+    for (const int4& h : hubs) p->max_hub_chunks = std::max(p->max_hub_chunks, h.z);
+  }
   std::vector<int2> src;
   for (int s = 0; s < T.nv; ++s) src.push_back(make_int2(T.slot_row[s], T.slot_col[s]));
   upload(p->t_slot_rc, src);
@@ -317,6 +343,17 @@ void upload_topology(karam_problem* p) {
   d.es_fc = p->t_es_fc.as<double>();
   d.es_hub = p->t_es_hub.as<int>();
   d.es_hubc = p->t_es_hubc.as<int4>();
+  d.jt_off = p->t_jt_off.as<int>();
+  d.jt_code = p->t_jt_code.as<int>();
+  d.ft_off = p->t_ft_off.as<int>();
+  d.ft_code = p->t_ft_code.as<int>();
+  d.ft_a = p->t_ft_a.as<int>();
+  d.ft_b = p->t_ft_b.as<int>();
+  d.ft_coef = p->t_ft_coef.as<double>();
+  d.hub_items = p->t_hub_items.as<int4>();
+  d.n_hub_items = p->n_hub_items;
+  d.n_ft_terms = T.ft_off.empty() ? 0 : T.ft_off.back();
+  d.n_hub_slot_terms = p->n_hub_slot_terms;
   d.n_hub_groups = T.n_hub_groups;
   d.n_hub_rows = T.n_hub_rows;
   d.lu_hdr = p->t_lu_hdr.as<int4>();
@@ -729,6 +766,11 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
       It[1].live_out = list0;
       It[1].live_out_count = cnt;
       LT.grid = *p->h_active;  // instances only ever leave the live set
+      // the per-instance evaluation kernel, when its device values fit the
+      // default 48 KiB of dynamic shared memory and its hubs 8 chunks
+      LT.es_one = p->max_hub_chunks <= 8 &&
+                  sizeof(double) * (3 * (size_t)(p->dt.n_mos + p->dt.n_dio) + (size_t)p->dt.n_ft_terms +
+                                    (size_t)p->dt.n_hub_slot_terms) <= 48 * 1024;
       capture(tail_g, LT, It);
       tail = true;
     }

@@ -21,6 +21,7 @@ struct RoundLaunch {
   bool nd = false;    // the level-scheduled kernel (k_lu_nd)
   int big = 0;        // block per instance on the level schedule (k_lu_big): 1 with the
                       // ND slots in shared memory, 2 in a global workspace
+  bool es_one = false; // evaluation + stamping by k_es_one, one CTA per listed instance
   char why[192] = {};  // when no candidate fits: why the last ones were rejected
 };
 

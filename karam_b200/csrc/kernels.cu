@@ -178,6 +178,15 @@ void launch_tran_start(const DevTopo& T, const DevInst& I, const JobParams& P, i
 
 void launch_eval_stamp(const DevTopo& T, const DevInst& I, const JobParams& P,
                        const RoundLaunch& L, int prec, cudaStream_t s) {
+  if (L.es_one) {  // tail rounds: one CTA per listed live instance
+    const size_t sm =
+        sizeof(double) * (3 * (size_t)(T.n_mos + T.n_dio) + (size_t)T.n_ft_terms + (size_t)T.n_hub_slot_terms);
+    if (prec == KARAM_PREC_MIXED)
+      k_es_one<float><<<L.grid, kBigThreads, sm, s>>>(T, I, P);
+    else
+      k_es_one<double><<<L.grid, kBigThreads, sm, s>>>(T, I, P);
+    return;
+  }
   const dim3 grid((I.ni + 31) / 32, T.n_es_blocks);
   if (prec == KARAM_PREC_MIXED)
     k_es<float><<<grid, 256, 0, s>>>(T, I, P);

@@ -912,6 +912,194 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
   }
 }
 
+// Device evaluation + stamping of one listed live instance per CTA, for the
+// tail rounds (few live instances; I.live_in lists them): the CTA's threads
+// take the instance's devices, then its stamp items, instead of 32 instances
+// in the lanes of every CTA. Slots and nodes sum their terms in the order of
+// k_es, and hub items in k_es's order too (chunk by chunk, the eight warp
+// slices of each chunk in turn, the chunk sums added to the linear part in
+// chunk order), so the results are k_es's. Dynamic shared memory: the
+// device values [3][devices] (gm or diode g, gds or diode i, ids), then every
+// node term's signed value and every hub slot term's signed value, computed
+// side by side before the sums (a - c and a + (-c) round alike).
+template <typename TJ>
+__global__ void __launch_bounds__(kBigThreads) k_es_one(DevTopo T, DevInst I, JobParams P) {
+  extern __shared__ __align__(16) double s_val[];
+  __shared__ unsigned long long s_f[kBigThreads / 32], s_dv[kBigThreads / 32];
+  __shared__ int s_fl[kBigThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (blockIdx.x == 0 && tid == 0) {  // the round's lists start empty, as in k_es
+    if (I.rescue_count) *I.rescue_count = 0;
+    if (I.live_out_count) *I.live_out_count = 0;
+  }
+  if ((int)blockIdx.x >= *I.live_in_count) return;
+  const int g = I.live_in[blockIdx.x];
+  const size_t ld = I.ld;
+  const int nv = T.nv, n = T.n, nm = T.n_mos, nd = T.n_mos + T.n_dio;
+  const double heff = I.ev_heff[g];
+  if (heff < 0.0) return;
+  const bool tran = heff > 0.0;
+  const double t = I.ev_t[g];
+  double* v0 = s_val;           // gm | diode g
+  double* v1 = s_val + nd;      // gds | diode i
+  double* v2 = s_val + 2 * nd;  // ids
+  double* tv = s_val + 3 * nd;  // node terms, signed
+  double* hv = tv + T.n_ft_terms;  // hub slot terms, signed
+  for (int d = tid; d < nd; d += blockDim.x) {
+    const DevIn in = load_device(T, I, d, g);
+    if (in.mos) {
+      double ids, gm, gds;
+      mosfet_eval(in.va, in.vb, in.vc, in.sign, in.p0, in.p1, in.p2, in.p3, ids, gm, gds);
+      v0[d] = gm;
+      v1[d] = gds;
+      v2[d] = ids;
+    } else {
+      double id, gd;
+      diode_eval(in.va, make_double4(in.p0, in.p1, in.p2, in.p3), id, gd);
+      v0[d] = gd;
+      v1[d] = id;
+    }
+  }
+  __syncthreads();
+  // a slot term's device value (codes in global numbering: MOSFET or diode index)
+  auto slot_val = [&](int c) {
+    const int kind = code_kind(c), idx = code_idx(c);
+    return kind == 0 ? v1[idx] : kind == 2 ? v0[nm + idx] : v0[idx];  // gds | diode g | gm
+  };
+  auto node_val = [&](int q) {
+    const int c = __ldg(&T.ft_code[q]), kind = code_kind(c), idx = code_idx(c);
+    if (kind == 4) return v1[nm + idx];  // diode current
+    if (kind == 5) return v2[idx];       // MOSFET ids
+    const int4 tm = make_int4(c, __ldg(&T.ft_a[q]), __ldg(&T.ft_b[q]), 0);
+    return node_term(T, I, P, tm, __ldg(&T.ft_coef[q]), g, tran, t, heff, s_val, 0);
+  };
+  auto slot_base = [&](int s) {  // linear part + capacitor companions
+    double acc = __ldg(&T.jlin_dc[s]);
+    if (tran) {
+      const int q1 = __ldg(&T.jcap_off[s + 1]);
+      for (int q = __ldg(&T.jcap_off[s]); q < q1; ++q) {
+        const int cc = __ldg(&T.jcap_code[q]);
+        const double gq = (2.0 * __ldg(&T.cap_c[code_idx(cc)])) / heff;
+        acc = cc < 0 ? acc - gq : acc + gq;
+      }
+    }
+    return acc;
+  };
+  auto is_hub = [&](int it) {
+    for (int h = 0; h < T.n_hub_items; ++h)
+      if (__ldg(&T.hub_items[h]).x == it) return true;
+    return false;
+  };
+  for (int q = tid; q < T.n_ft_terms; q += blockDim.x) {
+    const double c0 = node_val(q);
+    tv[q] = __ldg(&T.ft_code[q]) < 0 ? -c0 : c0;
+  }
+  for (int h = 0; h < T.n_hub_items; ++h) {
+    const int4 hb = __ldg(&T.hub_items[h]);
+    if (hb.x >= nv) continue;
+    const int qs = __ldg(&T.jt_off[hb.x]), nt = __ldg(&T.jt_off[hb.x + 1]) - qs;
+    for (int q = tid; q < nt; q += blockDim.x) {
+      const int c = __ldg(&T.jt_code[qs + q]);
+      const double val = slot_val(c);
+      hv[hb.w + q] = c < 0 ? -val : val;
+    }
+  }
+  __syncthreads();
+  double fmx = 0.0, dvm = 0.0;
+  bool bad = false;
+  int flags = 3;
+  auto node_done = [&](int i, double f) {
+    const size_t o = (size_t)i * ld + g;
+    I.F[o] = f;
+    if (!isfinite(f)) bad = true;
+    fmx = fmax(fmx, fabs(f));
+    const double xi = I.x[o], vi = I.v[o];
+    const double dd = fabs(xi - vi), m = fmax(fabs(xi), fabs(vi));
+    if (dd > P.reltol * m + P.vntol) flags &= ~1;
+    if (dd > P.polish_rel * m + P.polish_abs) flags &= ~2;
+    dvm = fmax(dvm, dd);
+  };
+  for (int it = tid; it < nv + n; it += blockDim.x) {
+    if (is_hub(it)) continue;
+    if (it < nv) {
+      double acc = slot_base(it);
+      const int q1 = __ldg(&T.jt_off[it + 1]);
+      for (int q = __ldg(&T.jt_off[it]); q < q1; ++q) {
+        const int c = __ldg(&T.jt_code[q]);
+        const double val = slot_val(c);
+        acc = c < 0 ? acc - val : acc + val;
+      }
+      reinterpret_cast<TJ*>(I.J)[(size_t)it * ld + g] = (TJ)acc;
+    } else {
+      const int i = it - nv;
+      double acc = 0.0;
+      const int q1 = __ldg(&T.ft_off[i + 1]);
+      for (int q = __ldg(&T.ft_off[i]); q < q1; ++q) acc += tv[q];
+      node_done(i, acc);
+    }
+  }
+  // hub items, one warp each: lane c * 8 + w sums slice w of chunk c (as the
+  // warps of k_es's chunk blocks do), lane 0 then combines in k_es's order
+  for (int h = warp; h < T.n_hub_items; h += nw) {
+    const int4 hb = __ldg(&T.hub_items[h]);
+    const int it = hb.x, nch = hb.z;
+    const bool slot = it < nv;
+    const int qs = slot ? __ldg(&T.jt_off[it]) : __ldg(&T.ft_off[it - nv]);
+    double part[2] = {0.0, 0.0};  // up to 64 slices per warp: lanes take two
+    for (int r = 0; r < 2; ++r) {
+      const int sl = lane + 32 * r, c = sl >> 3, w = sl & 7;
+      if (c >= nch) continue;
+      const int lo = __ldg(&T.es_hub[hb.y + c]), hi = __ldg(&T.es_hub[hb.y + c + 1]);
+      const int q0 = lo + (int)(((long long)(hi - lo) * w) / 8);
+      const int q1 = lo + (int)(((long long)(hi - lo) * (w + 1)) / 8);
+      const double* src = slot ? hv + hb.w : tv + qs;
+      double acc = 0.0;
+      for (int q = q0; q < q1; ++q) acc += src[q];
+      part[r] = acc;
+    }
+    double sum = slot ? slot_base(it) : 0.0;
+    for (int c = 0; c < nch; ++c) {
+      double pc = 0.0;
+      for (int w = 0; w < 8; ++w) {
+        const int sl = c * 8 + w;
+        pc += __shfl_sync(kFull, part[sl >> 5], sl & 31);
+      }
+      sum += pc;
+    }
+    if (lane == 0) {
+      if (slot)
+        reinterpret_cast<TJ*>(I.J)[(size_t)it * ld + g] = (TJ)sum;
+      else
+        node_done(it - nv, sum);
+    }
+  }
+  // the instance's reductions (one CTA per instance: no other CTA adds to them)
+  for (int o = 16; o > 0; o >>= 1) {
+    fmx = fmax(fmx, __shfl_xor_sync(kFull, fmx, o));
+    dvm = fmax(dvm, __shfl_xor_sync(kFull, dvm, o));
+    flags &= __shfl_xor_sync(kFull, flags, o);
+  }
+  const bool any_bad = __any_sync(kFull, bad);
+  if (lane == 0) {
+    s_f[warp] = any_bad ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(fmx);
+    s_dv[warp] = (unsigned long long)__double_as_longlong(dvm);
+    s_fl[warp] = flags;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long f = s_f[0], dv = s_dv[0];
+    int fl = s_fl[0];
+    for (int w = 1; w < nw; ++w) {
+      f = max(f, s_f[w]);
+      dv = max(dv, s_dv[w]);
+      fl &= s_fl[w];
+    }
+    atomicMax(&I.red_f[g], f);
+    atomicMax(&I.red_dv[g], dv);
+    if (fl != 3) atomicAnd(&I.red_flags[g], fl);
+  }
+}
+
 // Reductions of an instance back to their neutral values.
 __device__ __forceinline__ void reset_reductions(const DevInst& I, int g) {
   I.red_f[g] = 0ull;

@@ -121,6 +121,15 @@ struct DevTopo {
   const int* es_hub;        // hub items: term index where each device chunk starts, then the end
   const int4* es_hubc;
   int n_hub_groups, n_hub_rows;
+  // the stamp terms in global device numbering, for the per-instance
+  // evaluation of tail rounds (k_es_one): slot terms (jt_off [nv + 1],
+  // jt_code), node terms (ft_off [n + 1], ft_code, terminals ft_a / ft_b,
+  // coefficients ft_coef), and the hub items {item, es_hub offset, chunks, 0}
+  const int *jt_off, *jt_code, *ft_off, *ft_code, *ft_a, *ft_b;
+  const double* ft_coef;
+  const int4* hub_items;    // {item, es_hub offset, chunks, offset of a hub slot's terms}
+  int n_hub_items;
+  int n_ft_terms, n_hub_slot_terms;  // node terms in all; terms of the hub slots
   // LU program per pivot k: hdr = (off, nL, nU, diagonal slot); data at off =
   // Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots)
   const int4* lu_hdr;
