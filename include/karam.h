@@ -380,7 +380,7 @@ KARAM_API int karam_get_lu_schedule(const karam_problem *p, int32_t *buf, int64_
  * plain NR produced for the instances of a problem, and serves
  * opts->seeded = KARAM_SEED_MLP solves of problems with the same topology.
  * The GEMMs use BF16 weights and activations with FP32 accumulation; master
- * weights and Adam moments are FP32. Plain NR stays the judge: a seeded
+ * weights and Adam moments are FP32. Plain NR still decides convergence: a seeded
  * instance that has not converged after seed_max_iter iterations falls back
  * to full GMIN stepping. No counterpart in the reference. */
 typedef struct karam_seeder karam_seeder;

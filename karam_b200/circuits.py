@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _abi as A
 
-# Level-1 model cards of the inverter-chain family.
+# Level-1 model cards of the inverter-chain family of the benchmark circuits.
 NMOS_CARD = dict(kp=110e-6, vto=0.7, lam=0.04)
 PMOS_CARD = dict(kp=40e-6, vto=-0.7, lam=0.05)
 NMOS_WL = (2e-6, 0.18e-6)

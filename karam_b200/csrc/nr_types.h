@@ -45,7 +45,7 @@ struct InstState {
   int g;          // GMIN step
   int it;         // NR iterations in the current GMIN step / time step
   int damp;       // damping count of the pending trial point
-  int first;      // 1: x == v, nothing to judge
+  int first;      // 1: x == v, nothing to compare yet
   int step;       // transient output step (1-based)
   int status;     // KST_*
   int iters;      // DC iterations, counted as the reference counts them

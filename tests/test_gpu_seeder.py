@@ -3,7 +3,7 @@
 NeuralSeeder::predictSeed (solvers/neural_seeder.h:100-137) seeds the batch
 from the plain-NR DC solutions of its first KARAM_SEED_HISTORY instances; the
 seeded instances start at the final GMIN step and fall back to full GMIN
-stepping after seed_max_iter iterations. Plain NR judges the result: the
+stepping after seed_max_iter iterations. Plain NR decides the result: the
 seeded solutions must meet the same tolerances against the oracle (node
 voltages |dv| <= 1e-9 |v| + 1e-12 V, Norton branch currents within 1e-12 A).
 """
