@@ -698,10 +698,10 @@ __device__ bool on_singular(const DevTopo& Tp, const DevInst& I, int g) {
 // the CTA's device values sd ([local][3][32] doubles, lane offset applied).
 __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, const JobParams& P,
                                             int4 tm, double coef, int g, bool tran, double t,
-                                            double heff, const double* sd, int dev_base) {
+                                            double heff, const double* sd) {
   const size_t ld = I.ld;
   const int idx = code_idx(tm.x), kind = code_kind(tm.x);
-  if (kind >= 4) return sd[(idx - dev_base) * 96 + (kind == 4 ? 32 : 64)];  // diode i / MOSFET ids
+  if (kind >= 4) return sd[tm.w];  // diode i / MOSFET ids, at the offset the table carries
   if (kind == 2) return coef;                                                // current source
   const double va = tm.y >= 0 ? __ldg(&I.x[tm.y * ld + g]) : 0.0;
   const double vb = tm.z >= 0 ? __ldg(&I.x[tm.z * ld + g]) : 0.0;
@@ -784,9 +784,8 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
             }
           }
           for (int q = it.y; q < it.y + it.z; ++q) {
-            const int c = __ldg(&T.es_jt[q]);
-            const int kind = code_kind(c);  // 0 gds, 1 gm, 2 diode g
-            const double val = sd[code_idx(c) * 96 + (kind == 0 ? 32 : 0)];
+            const int c = __ldg(&T.es_jt[q]);  // sign | offset of the value (gds, gm, diode g)
+            const double val = sd[c & 0x7fffffff];
             acc = c < 0 ? acc - val : acc + val;
           }
           reinterpret_cast<TJ*>(I.J)[(size_t)s * ld + g] = (TJ)acc;
@@ -796,14 +795,14 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
           const int qe = it.y + it.z;
           for (; q + 1 < qe; q += 2) {  // two terms' loads in flight, sum in order
             const int4 t0 = __ldg(&T.es_ft[q]), t1 = __ldg(&T.es_ft[q + 1]);
-            const double c0 = node_term(T, I, P, t0, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
-            const double c1 = node_term(T, I, P, t1, __ldg(&T.es_fc[q + 1]), g, tran, t, heff, sd, 0);
+            const double c0 = node_term(T, I, P, t0, __ldg(&T.es_fc[q]), g, tran, t, heff, sd);
+            const double c1 = node_term(T, I, P, t1, __ldg(&T.es_fc[q + 1]), g, tran, t, heff, sd);
             acc = t0.x < 0 ? acc - c0 : acc + c0;
             acc = t1.x < 0 ? acc - c1 : acc + c1;
           }
           if (q < qe) {
             const int4 t0 = __ldg(&T.es_ft[q]);
-            const double c0 = node_term(T, I, P, t0, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, 0);
+            const double c0 = node_term(T, I, P, t0, __ldg(&T.es_fc[q]), g, tran, t, heff, sd);
             acc = t0.x < 0 ? acc - c0 : acc + c0;
           }
           node_done(it.x - nv, acc);
@@ -819,7 +818,6 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
     const int nh = -blk.y;
     const int4 hc = __ldg(&T.es_hubc[blockIdx.y]);
     const int c = hc.x, nch = hc.y;
-    const int c0 = c * KES_MAX_DEV;
     double acc[KES_MAX_HUBS];
 #pragma unroll
     for (int m = 0; m < KES_MAX_HUBS; ++m) acc[m] = 0.0;
@@ -837,14 +835,14 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
         const int q1 = lo + (int)(((long long)(hi - lo) * (warp + 1)) / 8);
         if (it.x < nv) {
           for (int q = it.y + q0; q < it.y + q1; ++q) {  // every slot term is a device term
-            const int cc = __ldg(&T.es_jt[q]);
-            const double val = sd[(code_idx(cc) - c0) * 96 + (code_kind(cc) == 0 ? 32 : 0)];
+            const int cc = __ldg(&T.es_jt[q]);  // sign | chunk-local offset
+            const double val = sd[cc & 0x7fffffff];
             acc[m] = cc < 0 ? acc[m] - val : acc[m] + val;
           }
         } else {
           for (int q = it.y + q0; q < it.y + q1; ++q) {
             const int4 tm = __ldg(&T.es_ft[q]);
-            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd, c0);
+            const double cur = node_term(T, I, P, tm, __ldg(&T.es_fc[q]), g, tran, t, heff, sd);
             acc[m] = tm.x < 0 ? acc[m] - cur : acc[m] + cur;
           }
         }
@@ -971,7 +969,7 @@ __global__ void __launch_bounds__(kBigThreads) k_es_one(DevTopo T, DevInst I, Jo
     if (kind == 4) return v1[nm + idx];  // diode current
     if (kind == 5) return v2[idx];       // MOSFET ids
     const int4 tm = make_int4(c, __ldg(&T.ft_a[q]), __ldg(&T.ft_b[q]), 0);
-    return node_term(T, I, P, tm, __ldg(&T.ft_coef[q]), g, tran, t, heff, s_val, 0);
+    return node_term(T, I, P, tm, __ldg(&T.ft_coef[q]), g, tran, t, heff, s_val);
   };
   auto slot_base = [&](int s) {  // linear part + capacitor companions
     double acc = __ldg(&T.jlin_dc[s]);

@@ -107,10 +107,11 @@ struct DevTopo {
   //   es_item[k]  = {item (slot s < nv, node nv + i), term offset, terms,
   //                  hub items: offset of the item's chunk bounds in es_hub}
   //   es_dev      = global device ids (MOSFETs, then n_mos + diode index)
-  //   es_jt       = slot device terms: sign | kind << 24 | local device
-  //   es_ft       = node terms {code, terminal a, terminal b, 0}, device codes
-  //                 carrying the local device; es_fc their coefficients (1/R,
-  //                 source amplitude, 2C, or 0)
+  //   es_jt       = slot device terms: sign bit | offset of the term's value
+  //                 in the block's (or chunk's) device values for lane 0
+  //   es_ft       = node terms {code, terminal a, terminal b, value offset of
+  //                 a device term}, device codes carrying the local device;
+  //                 es_fc their coefficients (1/R, source amplitude, 2C, or 0)
   int n_es_blocks;
   const int4* es_block;
   const int4* es_item;

@@ -1115,6 +1115,19 @@ void node_term_records(Topology& T) {
   }
 }
 
+// Shared-memory layout of a block's device values: 96 doubles per device, 32
+// lanes each of {gm or diode g, gds or diode i, MOSFET ids}. A slot term is
+// stored as its sign bit | the offset of its value for lane 0; a node
+// device term keeps its code and carries that offset in its fourth field.
+int es_slot_term(int code, int local_dev) {
+  const int kind = (code >> 24) & 0x7f;  // JK_MOS_GDS, JK_MOS_GM, JK_DIO_G
+  return (code & int32_t(0x80000000u)) | (local_dev * 96 + (kind == JK_MOS_GDS ? 32 : 0));
+}
+int es_node_term_offset(int code, int local_dev) {
+  const int kind = (code >> 24) & 0x7f;  // FK_DIO: diode current, FK_MOS: ids
+  return local_dev * 96 + (kind == FK_DIO ? 32 : 64);
+}
+
 // Packs the stamp items into evaluation + stamping blocks. Items go in row
 // order (the slots of a row, then its node), so a block covers a stretch of
 // the ordering and the devices it needs are mostly its own; a device shared
@@ -1266,7 +1279,7 @@ void es_blocks(Topology& T) {
         T.es_item.push_back(0);
         for (int q = T.jt_off[it]; q < T.jt_off[it + 1]; ++q) {
           const int c = T.jt_code[q];
-          T.es_jt.push_back((c & int32_t(0xFF000000u)) | lid.at(slot_dev(c)));
+          T.es_jt.push_back(es_slot_term(c, lid.at(slot_dev(c))));
         }
       } else {
         const int i = it - nv;
@@ -1279,7 +1292,7 @@ void es_blocks(Topology& T) {
           T.es_ft.push_back(d >= 0 ? ((c & int32_t(0xFF000000u)) | lid.at(d)) : c);
           T.es_ft.push_back(T.ft_a[q]);
           T.es_ft.push_back(T.ft_b[q]);
-          T.es_ft.push_back(0);
+          T.es_ft.push_back(d >= 0 ? es_node_term_offset(c, lid.at(d)) : 0);
           T.es_fc.push_back(T.ft_coef[q]);
         }
       }
@@ -1372,7 +1385,7 @@ void es_blocks(Topology& T) {
         T.es_item.push_back(T.jt_off[it + 1] - T.jt_off[it]);
         T.es_item.push_back(hb);
         for (int q = T.jt_off[it], t = 0; q < T.jt_off[it + 1]; ++q, ++t)
-          T.es_jt.push_back((T.jt_code[q] & int32_t(0xFF000000u)) | li[t]);
+          T.es_jt.push_back(es_slot_term(T.jt_code[q], li[t] % kEsMaxDev));  // chunk-local
       } else {
         const int i = it - nv;
         T.es_item.push_back((int)T.es_ft.size() / 4);
@@ -1383,7 +1396,7 @@ void es_blocks(Topology& T) {
           T.es_ft.push_back(li[t] >= 0 ? ((c & int32_t(0xFF000000u)) | li[t]) : c);
           T.es_ft.push_back(T.ft_a[q]);
           T.es_ft.push_back(T.ft_b[q]);
-          T.es_ft.push_back(0);
+          T.es_ft.push_back(li[t] >= 0 ? es_node_term_offset(c, li[t] % kEsMaxDev) : 0);
           T.es_fc.push_back(T.ft_coef[q]);
         }
       }
