@@ -731,19 +731,25 @@ void nd_schedule(Topology& T) {
     }
     for (int r = 0; r < n; ++r) Rrow[r].assign(R[r].begin(), R[r].end());
   }
-  // ND slots, row-major
-  std::unordered_map<int64_t, int> slot;
-  T.nd_nv = 0;
+  // ND slots, row-major: slot (r, c) = first slot of row r + rank of c among
+  // the row's ascending columns
+  std::vector<int> row_first(n + 1, 0);
+  for (int r = 0; r < n; ++r) row_first[r + 1] = row_first[r] + (int)Rrow[r].size();
+  T.nd_nv = row_first[n];
   T.nd_src.clear();
   std::unordered_map<int64_t, int> mf;
   for (int sl = 0; sl < T.nv; ++sl) mf[key(T.slot_row[sl], T.slot_col[sl])] = sl;
   for (int r = 0; r < n; ++r)
     for (int c : Rrow[r]) {
-      slot[key(r, c)] = T.nd_nv++;
       auto f = mf.find(key(order[r], order[c]));
       T.nd_src.push_back(f == mf.end() ? -1 : f->second);
     }
-  auto S = [&](int r, int c) { return slot.at(key(r, c)); };
+  auto S = [&](int r, int c) {
+    const auto& row = Rrow[r];
+    const auto it = std::lower_bound(row.begin(), row.end(), c);
+    if (it == row.end() || *it != c) throw std::logic_error("level schedule: position outside the structure");
+    return row_first[r] + (int)(it - row.begin());
+  };
   T.nd_diag.assign(n, 0);
   for (int k = 0; k < n; ++k) T.nd_diag[k] = S(k, k);
   // levels
@@ -764,40 +770,56 @@ void nd_schedule(Topology& T) {
   for (int lv = 0; lv < NL; ++lv) {
     T.lv_piv_ptr.push_back((int)T.lv_piv.size());
     T.lv_l_ptr.push_back((int)T.l_slot.size());
-    std::map<int, std::vector<std::pair<int, int>>> tc, yc;  // target slot / row -> pairs
+    // update pairs by target slot and right-hand-side pairs by row, each in
+    // pivot order within its target (a stable sort of the emission order)
+    struct Rec {
+      int key, a, b;
+    };
+    std::vector<Rec> tc, yc;
     for (int k : piv[lv]) {
       T.lv_piv.push_back(k);
       for (int i : Lk[k]) {
-        T.l_slot.push_back(S(i, k));
+        const int sik = S(i, k);
+        T.l_slot.push_back(sik);
         T.l_piv.push_back(k);
-        yc[i].emplace_back(S(i, k), k);
-        for (int j : Uk[k]) tc[S(i, j)].emplace_back(S(i, k), S(k, j));
+        yc.push_back({i, sik, k});
+        if (Uk[k].empty()) continue;
+        // row i holds every column of U_k (fill): walk both ascending lists
+        const auto& row = Rrow[i];
+        size_t p = (size_t)(std::lower_bound(row.begin(), row.end(), Uk[k].front()) - row.begin());
+        for (int j : Uk[k]) {
+          while (p < row.size() && row[p] < j) ++p;
+          if (p == row.size() || row[p] != j) throw std::logic_error("level schedule: fill outside the structure");
+          tc.push_back({row_first[i] + (int)p, sik, S(k, j)});
+        }
       }
     }
-    for (int pass = 0; pass < 2; ++pass) {  // short lists, then long ones
-      (pass ? T.lv_tl_ptr : T.lv_ts_ptr).push_back((int)T.t_slot.size());
-      for (auto& e : tc)
-        if (((int)e.second.size() > Topology::kNdLong) == (pass == 1)) {
-          T.t_slot.push_back(e.first);
-          for (auto& q : e.second) {
-            T.pr_l.push_back(q.first);
-            T.pr_u.push_back(q.second);
+    auto by_key = [](const Rec& x, const Rec& y) { return x.key < y.key; };
+    std::stable_sort(tc.begin(), tc.end(), by_key);
+    std::stable_sort(yc.begin(), yc.end(), by_key);
+    // groups of equal keys in key order: short lists, then long ones
+    auto emit = [&](const std::vector<Rec>& recs, std::vector<int>& keys, std::vector<int>& off,
+                    std::vector<int>& pa, std::vector<int>& pb, std::vector<int>& short_ptr,
+                    std::vector<int>& long_ptr) {
+      for (int pass = 0; pass < 2; ++pass) {
+        (pass ? long_ptr : short_ptr).push_back((int)keys.size());
+        for (size_t g0 = 0; g0 < recs.size();) {
+          size_t g1 = g0;
+          while (g1 < recs.size() && recs[g1].key == recs[g0].key) ++g1;
+          if (((int)(g1 - g0) > Topology::kNdLong) == (pass == 1)) {
+            keys.push_back(recs[g0].key);
+            for (size_t q = g0; q < g1; ++q) {
+              pa.push_back(recs[q].a);
+              pb.push_back(recs[q].b);
+            }
+            off.push_back((int)pa.size());
           }
-          T.t_off.push_back((int)T.pr_l.size());
+          g0 = g1;
         }
-    }
-    for (int pass = 0; pass < 2; ++pass) {
-      (pass ? T.lv_yl_ptr : T.lv_ys_ptr).push_back((int)T.y_row.size());
-      for (auto& e : yc)
-        if (((int)e.second.size() > Topology::kNdLong) == (pass == 1)) {
-          T.y_row.push_back(e.first);
-          for (auto& q : e.second) {
-            T.yp_l.push_back(q.first);
-            T.yp_k.push_back(q.second);
-          }
-          T.y_off.push_back((int)T.yp_l.size());
-        }
-    }
+      }
+    };
+    emit(tc, T.t_slot, T.t_off, T.pr_l, T.pr_u, T.lv_ts_ptr, T.lv_tl_ptr);
+    emit(yc, T.y_row, T.y_off, T.yp_l, T.yp_k, T.lv_ys_ptr, T.lv_yl_ptr);
   }
   T.lv_piv_ptr.push_back((int)T.lv_piv.size());
   T.lv_l_ptr.push_back((int)T.l_slot.size());
