@@ -929,6 +929,18 @@ void nd_program(Topology& T) {
 
 }  // namespace
 
+// Sum of popcount(r[q] & m[q]) over q0 <= q <= q1. On x86-64 it is built with
+// and without the POPCNT instruction, and the loader picks the one the host
+// supports; the generic popcount is several times slower on this loop.
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
+__attribute__((target_clones("popcnt", "default")))
+#endif
+static uint64_t and_popcount(const uint64_t* r, const uint64_t* m, int q0, int q1) {
+  uint64_t s = 0;
+  for (int q = q0; q <= q1; ++q) s += (uint64_t)__builtin_popcountll(r[q] & m[q]);
+  return s;
+}
+
 // Min-Fill elimination with the reference's choice rule: at every step the
 // vertex with the fewest missing neighbour pairs, ties to the smallest id
 // (treewidth_analyzer.cpp:72-102). Instead of rescanning every vertex, fill
@@ -954,46 +966,75 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
     }
   }
   const int nv = (int)ids.size();
-  std::vector<std::unordered_set<int>> adj(nv);
-  for (const auto& f : factors)
-    for (size_t i = 0; i < f.size(); ++i)
-      for (size_t j = i + 1; j < f.size(); ++j) {
-        if (f[i] == f[j]) continue;
-        int a = dense.at(f[i]), b = dense.at(f[j]);
-        adj[a].insert(b);
-        adj[b].insert(a);
-      }
-  // Adjacency also as bit rows (up to 16384 vertices, 32 MiB): membership
-  // tests become bit tests and a vertex's missing neighbour pairs a sum of
-  // popcounts -- the same integers, so the order and its ties do not change.
+  // Adjacency as bit rows when it fits (up to 16384 vertices, 32 MiB), else
+  // hash sets. With bit rows a membership test is a bit test, a vertex's
+  // missing neighbour pairs are a sum of popcounts and its neighbours come out
+  // ascending: the same integers as with the sets, so the order and its ties
+  // do not change. Each row keeps the span of words it has ever occupied, and
+  // every scan of the row stays inside it.
   const bool bits = nv <= 16384;
   const size_t words = ((size_t)nv + 63) / 64;
   std::vector<uint64_t> brow(bits ? words * (size_t)nv : 0);
-  auto bset = [&](int a, int b) { brow[(size_t)a * words + (b >> 6)] |= 1ull << (b & 63); };
-  auto bclr = [&](int a, int b) { brow[(size_t)a * words + (b >> 6)] &= ~(1ull << (b & 63)); };
-  auto bhas = [&](int a, int b) { return (brow[(size_t)a * words + (b >> 6)] >> (b & 63)) & 1ull; };
-  if (bits)
-    for (int a = 0; a < nv; ++a)
-      for (int b : adj[a]) bset(a, b);
+  std::vector<int> rlo(bits ? nv : 0, (int)words), rhi(bits ? nv : 0, -1);
+  std::vector<std::unordered_set<int>> adj(bits ? 0 : nv);
+  auto has = [&](int a, int b) -> bool {
+    if (bits) return (brow[(size_t)a * words + (b >> 6)] >> (b & 63)) & 1ull;
+    return adj[a].count(b) != 0;
+  };
+  auto link = [&](int a, int b) {
+    if (bits) {
+      brow[(size_t)a * words + (b >> 6)] |= 1ull << (b & 63);
+      brow[(size_t)b * words + (a >> 6)] |= 1ull << (a & 63);
+      rlo[a] = std::min(rlo[a], b >> 6);
+      rhi[a] = std::max(rhi[a], b >> 6);
+      rlo[b] = std::min(rlo[b], a >> 6);
+      rhi[b] = std::max(rhi[b], a >> 6);
+    } else {
+      adj[a].insert(b);
+      adj[b].insert(a);
+    }
+  };
+  auto unlink = [&](int a, int b) {
+    if (bits) {
+      brow[(size_t)a * words + (b >> 6)] &= ~(1ull << (b & 63));
+      brow[(size_t)b * words + (a >> 6)] &= ~(1ull << (a & 63));
+    } else {
+      adj[a].erase(b);
+      adj[b].erase(a);
+    }
+  };
+  auto neighbours = [&](int u, std::vector<int>& out) {  // ascending
+    out.clear();
+    if (bits) {
+      const uint64_t* r = &brow[(size_t)u * words];
+      for (int q = rlo[u]; q <= rhi[u]; ++q)
+        for (uint64_t c = r[q]; c; c &= c - 1) out.push_back(q * 64 + __builtin_ctzll(c));
+    } else {
+      out.assign(adj[u].begin(), adj[u].end());
+      std::sort(out.begin(), out.end());
+    }
+  };
+  for (const auto& f : factors)
+    for (size_t i = 0; i < f.size(); ++i)
+      for (size_t j = i + 1; j < f.size(); ++j)
+        if (f[i] != f[j]) link(dense.at(f[i]), dense.at(f[j]));
   std::vector<uint64_t> mask(bits ? words : 0);
-  auto count_fill = [&](int u) {
-    std::vector<int> nb(adj[u].begin(), adj[u].end());
+  std::vector<int> cf_nb;
+  auto count_fill = [&](int u) -> uint32_t {
+    neighbours(u, cf_nb);
+    const std::vector<int>& nb = cf_nb;
+    if (nb.empty()) return 0;
     if (bits) {
       // missing pairs = (k (k - 1) - sum over neighbours of their neighbours in N(u)) / 2
-      int lo = nv, hi = -1;
-      for (int w : nb) {
-        mask[w >> 6] |= 1ull << (w & 63);
-        lo = std::min(lo, w >> 6);
-        hi = std::max(hi, w >> 6);
-      }
+      const int lo = nb.front() >> 6, hi = nb.back() >> 6;
+      for (int w : nb) mask[w >> 6] |= 1ull << (w & 63);
       uint64_t inside = 0;
       for (int w : nb) {
-        const uint64_t* r = &brow[(size_t)w * words];
-        for (int q = lo; q <= hi; ++q) inside += (uint64_t)__builtin_popcountll(r[q] & mask[q]);
+        inside += and_popcount(&brow[(size_t)w * words], mask.data(), std::max(lo, rlo[w]), std::min(hi, rhi[w]));
       }
       for (int w : nb) mask[w >> 6] = 0;
       const uint64_t k = nb.size();
-      return (uint32_t)((k * (k > 0 ? k - 1 : 0) - inside) / 2);
+      return (uint32_t)((k * (k - 1) - inside) / 2);
     }
     uint32_t c = 0;
     for (size_t i = 0; i < nb.size(); ++i) {
@@ -1016,7 +1057,10 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
   uint32_t maxclique = 0;
   std::vector<int> nb, touched;
   std::unordered_set<int> nbset;
-  std::unordered_map<int, uint32_t> dec;
+  std::vector<uint32_t> dec(nv, 0);  // missing pairs each vertex loses this step
+  auto lose = [&](int w) {
+    if (dec[w]++ == 0) touched.push_back(w);
+  };
   while (!pq.empty()) {
     auto top = *pq.begin();
     pq.erase(pq.begin());
@@ -1027,61 +1071,45 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
       if (--ghosts[u] > 0) pq.insert({0u, ids[u]});
       continue;
     }
-    nb.assign(adj[u].begin(), adj[u].end());
-    std::sort(nb.begin(), nb.end());
+    neighbours(u, nb);
     maxclique = std::max<uint32_t>(maxclique, (uint32_t)nb.size() + 1);
-    nbset.clear();
-    nbset.insert(nb.begin(), nb.end());
     if (bits) {
       for (int w : nb) mask[w >> 6] |= 1ull << (w & 63);
       mask[u >> 6] |= 1ull << (u & 63);  // u is no candidate either
+    } else {
+      nbset.clear();
+      nbset.insert(nb.begin(), nb.end());
     }
-    dec.clear();
+    touched.clear();
     for (size_t i = 0; i < nb.size(); ++i)
       for (size_t j = i + 1; j < nb.size(); ++j) {
-        int a = nb[i], b = nb[j];
-        if (adj[a].insert(b).second) {
-          adj[b].insert(a);
-          if (bits) {
-            bset(a, b);
-            bset(b, a);
-          }
-          // vertices outside N(u) adjacent to both a and b lose a missing pair
-          if (bits) {
-            const uint64_t* ra = &brow[(size_t)a * words];
-            const uint64_t* rb = &brow[(size_t)b * words];
-            for (size_t q = 0; q < words; ++q) {
-              uint64_t c = ra[q] & rb[q] & ~mask[q];
-              while (c) {
-                dec[(int)(q * 64 + (size_t)__builtin_ctzll(c))]++;
-                c &= c - 1;
-              }
-            }
-          } else {
-            const auto& sa = adj[a].size() <= adj[b].size() ? adj[a] : adj[b];
-            const auto& sb = adj[a].size() <= adj[b].size() ? adj[b] : adj[a];
-            for (int w : sa)
-              if (w != a && w != b && w != u && !nbset.count(w) && sb.count(w)) dec[w]++;
-          }
+        const int a = nb[i], b = nb[j];
+        if (has(a, b)) continue;
+        link(a, b);
+        // vertices outside N(u) adjacent to both a and b lose a missing pair
+        if (bits) {
+          const uint64_t* ra = &brow[(size_t)a * words];
+          const uint64_t* rb = &brow[(size_t)b * words];
+          const int q1 = std::min(rhi[a], rhi[b]);
+          for (int q = std::max(rlo[a], rlo[b]); q <= q1; ++q)
+            for (uint64_t c = ra[q] & rb[q] & ~mask[q]; c; c &= c - 1) lose(q * 64 + __builtin_ctzll(c));
+        } else {
+          const auto& sa = adj[a].size() <= adj[b].size() ? adj[a] : adj[b];
+          const auto& sb = adj[a].size() <= adj[b].size() ? adj[b] : adj[a];
+          for (int w : sa)
+            if (w != a && w != b && w != u && !nbset.count(w) && sb.count(w)) lose(w);
         }
       }
-    for (int w : nb) {
-      adj[w].erase(u);
-      if (bits) bclr(w, u);
-    }
+    for (int w : nb) unlink(w, u);
     if (bits) {
-      for (int w : nb) {
-        bclr(u, w);
-        mask[w >> 6] = 0;
-      }
+      for (int w : nb) mask[w >> 6] = 0;
       mask[u >> 6] = 0;
     }
-    adj[u].clear();
     alive[u] = 0;
-    for (auto& kv : dec) {
-      int w = kv.first;
+    for (int w : touched) {
       pq.erase({fill[w], ids[w]});
-      fill[w] -= kv.second;
+      fill[w] -= dec[w];
+      dec[w] = 0;
       pq.insert({fill[w], ids[w]});
     }
     for (int w : nb) {
