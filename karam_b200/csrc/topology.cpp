@@ -278,14 +278,13 @@ void symbolic(Topology& T, std::vector<std::vector<int>>& urow) {
 
 void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   const int n = T.n, nf = T.nnz_filled();
-  std::unordered_map<int64_t, int> fpos;
-  fpos.reserve((size_t)nf * 2);
-  for (int i = 0; i < n; ++i)
-    for (int k = T.f_row_ptr[i]; k < T.f_row_ptr[i + 1]; ++k) fpos[key(i, T.f_col[k])] = k;
+  // position of (pr, pc) in the filled CSR: each row's columns ascend
   auto fp = [&](int pr, int pc) {
-    auto it = fpos.find(key(pr, pc));
-    require(it != fpos.end(), "filled pattern misses a position");
-    return it->second;
+    const int* row = T.f_col.data() + T.f_row_ptr[pr];
+    const int* end = T.f_col.data() + T.f_row_ptr[pr + 1];
+    const int* it = std::lower_bound(row, end, pc);
+    require(it != end && *it == pc, "filled pattern misses a position");
+    return (int)(it - T.f_col.data());
   };
   for (auto& x : T.trip) x.f = fp(T.iperm[x.row], T.iperm[x.col]);
 
