@@ -320,8 +320,19 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   // eliminates on the unsymmetric structure of the stamps (gmb stamps, always
   // zero in the level-1 kernel, excluded), which is a subset of the filled
   // pattern, so results equal the full static elimination's.
-  std::vector<std::vector<int>> nzr(n), nzc(n);  // row -> cols, col -> rows (permuted)
+  // Structure as bit rows and columns up to 16384 unknowns, else sorted
+  // vectors (row -> cols, col -> rows, permuted); L and U of a pivot come out
+  // ascending either way.
+  const bool nzbits = n <= 16384;
+  const size_t W = ((size_t)n + 63) / 64;
+  std::vector<uint64_t> nzrb(nzbits ? W * (size_t)n : 0), nzcb(nzbits ? W * (size_t)n : 0);
+  std::vector<std::vector<int>> nzr(nzbits ? 0 : n), nzc(nzbits ? 0 : n);
   auto add_nz = [&](int r, int c) {
+    if (nzbits) {
+      nzrb[(size_t)r * W + (c >> 6)] |= 1ull << (c & 63);
+      nzcb[(size_t)c * W + (r >> 6)] |= 1ull << (r & 63);
+      return;
+    }
     auto& row = nzr[r];
     auto it = std::lower_bound(row.begin(), row.end(), c);
     if (it != row.end() && *it == c) return;
@@ -339,10 +350,24 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   for (int k = 0; k < n; ++k) {
     L.clear();
     U.clear();
-    for (int i : nzc[k])
-      if (i > k) L.push_back(i);
-    for (int j : nzr[k])
-      if (j > k) U.push_back(j);
+    if (nzbits) {
+      auto above = [&](const std::vector<uint64_t>& B, std::vector<int>& out) {
+        const uint64_t* row = &B[(size_t)k * W];
+        const size_t q0 = (size_t)(k + 1) >> 6;
+        for (size_t q = q0; q < W; ++q) {
+          uint64_t c = row[q];
+          if (q == q0) c &= ~0ull << ((k + 1) & 63);
+          for (; c; c &= c - 1) out.push_back((int)(q * 64 + (size_t)__builtin_ctzll(c)));
+        }
+      };
+      above(nzcb, L);
+      above(nzrb, U);
+    } else {
+      for (int i : nzc[k])
+        if (i > k) L.push_back(i);
+      for (int j : nzr[k])
+        if (j > k) U.push_back(j);
+    }
     for (int i : L)
       for (int j : U) add_nz(i, j);
     const int nl = (int)L.size(), nu = (int)U.size();
