@@ -429,8 +429,10 @@ KARAM_API int karam_eval_stamp(karam_problem *p, int32_t precision, const double
  * batch capacity needs more is rejected with KARAM_E_INVALID and a message.
  * The array keeps the last call's contents; each call clears what it needs
  * cleared. Calls that overlap on the GPU (other threads or streams) race on the
- * array. The first call on a device looks up the array's address, so make it
- * before any stream capture. Runs on the problem's stream and returns when the
+ * array. Every call looks up the array's address on the problem's device (no
+ * allocation; the first lookup on a device also loads the library's kernels
+ * there), so make the first call on a device before any stream capture. Runs
+ * on the problem's stream and synchronises it before returning, when the
  * outputs are written. */
 KARAM_API int karam_eval_stamp_noalloc(karam_problem *p, int32_t precision, const double *d_v,
                                        double *d_jac, double *d_f);

@@ -82,6 +82,7 @@ struct karam_problem {
   bool inst_kp = false, inst_vth = false;  // per-instance MOSFET values present
   bool have_dc = false;
   int tuned[2] = {0, 0};  // measured factor/solve schedule per precision (0 = none)
+  uint64_t content_hash = 0;  // karam_netlist_hash of the netlist the problem was made from
   int n_hub_items = 0, n_hub_slot_terms = 0;
   int max_hub_chunks = 0;  // k_es_one sums hub items of up to 8 chunks
   bool tran_started = false;  // capacitor history holds a transient in progress
@@ -605,19 +606,22 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
 }
 
 // Measured schedules (karam_tune_schedule), per problem and process-wide by
-// problem shape: unknowns, stamp non-zeros, batch size and precision.
-using TuneKey = std::tuple<int, int, int, int>;
+// netlist content (karam_netlist_hash), device, batch size and precision: a
+// schedule is reused only for the same topology on the same GPU, since the
+// shared memory a schedule needs depends on the topology and what fits
+// depends on the device.
+using TuneKey = std::tuple<uint64_t, int, int, int>;
 std::mutex g_tune_mu;
 std::map<TuneKey, int>& tune_cache() {
   static std::map<TuneKey, int> m;
   return m;
 }
 TuneKey tune_key(const karam_problem* p, int prec) {
-  return TuneKey{p->topo.n, p->topo.nnz(), p->ni, prec};
+  return TuneKey{p->content_hash, p->ctx ? p->ctx->device : -1, p->ni, prec};
 }
 // The schedule option a solve with opts.schedule == 0 uses: the problem's
-// measured choice, else one measured for a problem of the same shape, else 0
-// (the planner's).
+// measured choice, else one measured for an identical netlist and batch size
+// on the same device, else 0 (the planner's).
 int tuned_schedule(const karam_problem* p, int prec) {
   const int idx = prec == KARAM_PREC_MIXED ? 1 : 0;
   if (p->tuned[idx]) return p->tuned[idx];
@@ -646,13 +650,19 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   constexpr int kRounds = 16;  // even: the tail rounds alternate between two lists
   const int max_rounds = opts ? opts->max_rounds : 0;
   int want_lanes = opts ? opts->schedule : 0;
-  if (want_lanes == 0) want_lanes = tuned_schedule(p, P.precision);
+  const bool from_tuner = want_lanes == 0;
+  if (from_tuner) want_lanes = tuned_schedule(p, P.precision);
   const bool timed = opts && opts->kernel_timing;
   cudaStream_t s = p->ctx->stream;
   DevInst I = inst ? *inst : dev_inst(p);
   const int prec = P.precision;
   const int max_smem = p->ctx->max_smem, num_sms = p->ctx->num_sms;
   RoundLaunch L = plan_round(p->dt, p->ni, prec, max_smem, num_sms, want_lanes);
+  if (L.L < 1 && from_tuner && want_lanes != 0) {
+    // a measured schedule that does not fit here falls back to the planner's choice
+    cudaGetLastError();
+    L = plan_round(p->dt, p->ni, prec, max_smem, num_sms, 0);
+  }
   if (L.L < 1)
     throw std::runtime_error(std::string("no factor/solve schedule fits this problem; last: ") + L.why);
   ck(cudaGetLastError(), "configure kernels");
@@ -1102,6 +1112,7 @@ int karam_problem_create(karam_ctx* ctx, const karam_netlist* nl, int32_t max_in
     if (!nl) throw std::runtime_error("no netlist");
     auto p = std::make_unique<karam_problem>();
     p->topo = cached_topology(nl);
+    p->content_hash = fnv1a(netlist_bytes(nl));
     p->max_inst = max_instances;
     if (!ctx) {  // symbolic analysis only
       *out = p.release();
@@ -1484,7 +1495,7 @@ int karam_eval_stamp_noalloc(karam_problem* p, int32_t precision, const double* 
                                " (create the problem with fewer max_instances)");
     ck(cudaSetDevice(p->ctx->device), "cudaSetDevice");
     const char* err = "";
-    void* scratch = noalloc_scratch(p->ctx->device, &err);
+    void* scratch = noalloc_scratch(&err);
     if (!scratch) throw CudaError(std::string("cudaGetSymbolAddress: ") + err);
     cudaStream_t s = p->ctx->stream;
     ck(noalloc_eval_stamp(scratch, p->dt, dev_inst(p), precision, d_v, p->t_perm.as<int>(),

@@ -13,7 +13,6 @@
 
 #include <algorithm>
 #include <cstdint>
-#include <mutex>
 
 #include "../../include/karam.h"
 #include "device.hpp"
@@ -27,10 +26,6 @@ namespace {
 // kernel: on the host the name stands for a host-side placeholder, not for the
 // device address; the address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
 
 // Lanes of the batch start at a DC point; lanes past it never evaluate; the
 // reductions start neutral, the hub chunk counters at 0.
@@ -69,22 +64,17 @@ size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 
 }  // namespace
 
-void* noalloc_scratch(int device, const char** err) {
-  if (device < 0 || device >= kMaxDevices) {
-    *err = "device index beyond the scratch table";
+// Looked up on every call rather than cached: the lookup allocates nothing
+// and costs little, and an address kept from an earlier context would be
+// stale after a device reset in the same process.
+void* noalloc_scratch(const char** err) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
     return nullptr;
   }
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) {
-      *err = cudaGetErrorString(e);
-      return nullptr;
-    }
-    g_addr[device] = p;
-  }
-  return g_addr[device];
+  return p;
 }
 
 size_t noalloc_bytes(int n, int nv, int nnz, int ld, int hub_rows, int hub_groups) {

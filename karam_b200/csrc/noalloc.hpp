@@ -11,10 +11,10 @@ namespace karam {
 // Size of the library's fixed device scratch array (per GPU, held until exit).
 constexpr size_t kScratchBytes = size_t(16) << 20;
 
-// Device address of the scratch array on `device` (which must be current).
-// The first call per device looks it up with cudaGetSymbolAddress; returns
-// null and sets *err when that fails.
-void* noalloc_scratch(int device, const char** err);
+// Device address of the scratch array on the current device, looked up with
+// cudaGetSymbolAddress on every call; returns null and sets *err when that
+// fails.
+void* noalloc_scratch(const char** err);
 
 // Scratch bytes one call needs for a topology of n unknowns, nv value slots,
 // nnz CSR entries, hub_rows hub chunk partial rows and hub_groups hub groups,

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <functional>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <set>
 #include <stdexcept>
@@ -13,6 +14,18 @@
 
 namespace karam {
 namespace {
+
+// Largest problem (unknowns, or Min-Fill vertices) whose host analysis keeps
+// its structures as bit rows; larger ones use sorted vectors, ordered sets and
+// hash sets. Both give identical tables. KARAM_BITROW_MAX, read once, moves
+// the switch so that tests can run the large-problem code on small cases.
+int bitrow_max() {
+  static const int v = [] {
+    const char* e = std::getenv("KARAM_BITROW_MAX");
+    return e && *e ? std::atoi(e) : 16384;
+  }();
+  return v;
+}
 
 void require(bool ok, const std::string& msg) {
   if (!ok) throw std::runtime_error(msg);
@@ -323,7 +336,7 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   // Structure as bit rows and columns up to 16384 unknowns, else sorted
   // vectors (row -> cols, col -> rows, permuted); L and U of a pivot come out
   // ascending either way.
-  const bool nzbits = n <= 16384;
+  const bool nzbits = n <= bitrow_max();
   const size_t W = ((size_t)n + 63) / 64;
   std::vector<uint64_t> nzrb(nzbits ? W * (size_t)n : 0), nzcb(nzbits ? W * (size_t)n : 0);
   std::vector<std::vector<int>> nzr(nzbits ? 0 : n), nzc(nzbits ? 0 : n);
@@ -693,7 +706,7 @@ void nd_schedule(Topology& T) {
   // rows up to 16384 unknowns, else ordered sets; the same structure either
   // way), then each row's columns in ascending order
   std::vector<std::vector<int>> Lk(n), Uk(n), Rrow(n);
-  if (n <= 16384) {
+  if (n <= bitrow_max()) {
     const size_t W = ((size_t)n + 63) / 64;
     std::vector<uint64_t> Rb(W * (size_t)n, 0), Cb(W * (size_t)n, 0);
     auto set_bit = [&](std::vector<uint64_t>& B, int a, int b) { B[(size_t)a * W + (b >> 6)] |= 1ull << (b & 63); };
@@ -996,7 +1009,7 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
   // ascending: the same integers as with the sets, so the order and its ties
   // do not change. Each row keeps the span of words it has ever occupied, and
   // every scan of the row stays inside it.
-  const bool bits = nv <= 16384;
+  const bool bits = nv <= bitrow_max();
   const size_t words = ((size_t)nv + 63) / 64;
   std::vector<uint64_t> brow(bits ? words * (size_t)nv : 0);
   std::vector<int> rlo(bits ? nv : 0, (int)words), rhi(bits ? nv : 0, -1);

@@ -9,7 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_TREE = "/root/reference"
+REFERENCE_TREE = os.environ.get("KARAM_REFERENCE_TREE", "/root/reference")
 
 
 def pytest_configure(config):

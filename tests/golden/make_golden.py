@@ -73,7 +73,7 @@ def stats_arr(st):
 
 
 def main():
-    if not os.path.isdir("/root/reference"):
+    if not os.path.isdir(os.environ.get("KARAM_REFERENCE_TREE", "/root/reference")):
         sys.exit("the reference tree is needed to build the reference oracle")
     pyoracle.build("ref")
     ref = pyoracle.Oracle("ref")
