@@ -224,7 +224,26 @@ typedef struct karam_instance_stats {
   int32_t halvings;     /* transient step halvings after NR failures              */
   int32_t max_step_iters; /* most NR iterations spent on one transient attempt    */
   double residual;      /* final max KCL residual [A]                             */
+  /* DC convergence diagnostics (SolverStats, infrastructure/simtrace.h:86-104;
+   * filled as CircuitSim::solveDC fills them, solvers/circuitsim_solver.cpp:408-443, 516) */
+  int32_t failure_type; /* KARAM_FAIL_*: ConvergenceEngine::classifyFailure on the
+                           DC history (solvers/convergence_engine.h:26-87); set
+                           for converged solves too, as the reference does       */
+  int32_t stagnation;   /* SolverStats::stagnationDetected                        */
+  int32_t divergence;   /* SolverStats::divergenceDetected                        */
+  int32_t history_len;  /* DC NR iterations recorded (convergenceHistory.size())  */
 } karam_instance_stats;
+
+/* ConvergenceFailureType (infrastructure/simtrace.h:39-47), same order. */
+#define KARAM_FAIL_NONE 0
+#define KARAM_FAIL_SINGULAR_MATRIX 1
+#define KARAM_FAIL_DIVERGENCE 2
+#define KARAM_FAIL_LIMIT_CYCLE 3
+#define KARAM_FAIL_SLOW_CONVERGENCE 4
+#define KARAM_FAIL_FLOATING_NODE_INDUCED 5
+#define KARAM_FAIL_EXPONENTIAL_OVERFLOW 6
+/* Length of the per-instance ring of DC convergence history records. */
+#define KARAM_HISTORY_MAX 16
 
 typedef struct karam_ctx karam_ctx;
 typedef struct karam_problem karam_problem;
@@ -325,6 +344,15 @@ KARAM_API int karam_tune_schedule(karam_problem *p, const karam_solver_opts *opt
                                   int32_t *schedule, double *best_ms);
 KARAM_API int karam_read_results(karam_problem *p, double *out_v,
                                  karam_instance_stats *stats);
+/* The DC convergence history of one instance after a solve: the last
+ * KARAM_HISTORY_MAX (or fewer) records, oldest first -- per NR iteration its
+ * max KCL residual [A] and max |v_new - v_old| [V], the residualNorm and
+ * maxVoltageDelta of the reference's ConvergenceStep (infrastructure/
+ * simtrace.h:30-37, filled at solvers/circuitsim_solver.cpp:408-425). *len
+ * receives the count; residual and max_dv (both null, or both KARAM_HISTORY_MAX
+ * long) receive the records. */
+KARAM_API int karam_get_history(karam_problem *p, int32_t instance, double *residual,
+                                double *max_dv, int32_t *len);
 /* Blocks until the problem's stream is idle. */
 KARAM_API int karam_sync(karam_problem *p);
 

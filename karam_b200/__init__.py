@@ -74,6 +74,8 @@ def lib():
         "karam_symbolic_cache_info": (C.c_int, [P(C.c_int32), P(C.c_int64), P(C.c_int64)]),
         "karam_symbolic_cache_clear": (None, []),
         "karam_read_results": (C.c_int, [vp, P(C.c_double), P(A.KaramInstanceStats)]),
+        "karam_get_history": (C.c_int, [vp, C.c_int32, P(C.c_double), P(C.c_double),
+                                        P(C.c_int32)]),
         "karam_sync": (C.c_int, [vp]),
         "karam_get_pattern": (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
         "karam_get_stamp_map": (C.c_int, [vp, P(C.c_int32)]),
@@ -394,6 +396,16 @@ class Problem:
         st = (A.KaramInstanceStats * self.ni)() if want_stats else None
         self._check(lib().karam_read_results(self.h, A.ptr(v, C.c_double), st))
         return v, (self._stats(st) if want_stats else None)
+
+    def history(self, instance):
+        """(residual[m], max_dv[m]) of the instance's last m <= HISTORY_MAX DC NR
+        iterations, oldest first (karam_get_history)."""
+        f = np.zeros(A.HISTORY_MAX)
+        dv = np.zeros(A.HISTORY_MAX)
+        m = C.c_int32(0)
+        self._check(lib().karam_get_history(self.h, instance, A.ptr(f, C.c_double),
+                                            A.ptr(dv, C.c_double), C.byref(m)))
+        return f[: m.value], dv[: m.value]
 
     def sync(self):
         self._check(lib().karam_sync(self.h))

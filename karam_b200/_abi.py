@@ -13,6 +13,10 @@ ST_NOCONV = 1
 ST_SINGULAR = 2
 ST_NAN = 3
 ST_TIMEOUT = 4
+# ConvergenceFailureType (include/karam.h KARAM_FAIL_*)
+FAIL_NONE, FAIL_SINGULAR_MATRIX, FAIL_DIVERGENCE, FAIL_LIMIT_CYCLE = 0, 1, 2, 3
+FAIL_SLOW_CONVERGENCE, FAIL_FLOATING_NODE_INDUCED, FAIL_EXPONENTIAL_OVERFLOW = 4, 5, 6
+HISTORY_MAX = 16
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -79,7 +83,9 @@ class KaramInstanceStats(C.Structure):
                 ("polish_iters", C.c_int32), ("damped", C.c_int32),
                 ("gmin_step", C.c_int32), ("seeded_ok", C.c_int32),
                 ("rescued", C.c_int32), ("halvings", C.c_int32),
-                ("max_step_iters", C.c_int32), ("residual", C.c_double)]
+                ("max_step_iters", C.c_int32), ("residual", C.c_double),
+                ("failure_type", C.c_int32), ("stagnation", C.c_int32),
+                ("divergence", C.c_int32), ("history_len", C.c_int32)]
 
 
 class KaramTiming(C.Structure):

@@ -104,7 +104,7 @@ struct karam_problem {
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
       d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws,
-      i_live, i_stage;
+      i_live, i_stage, i_hist;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
   int rescue_slots = 0;
   RescuePlan rplan;
@@ -435,6 +435,7 @@ void alloc_instances(karam_problem* p) {
   p->i_cvp.alloc(std::max<size_t>(1, ld * T.cap.size()) * sizeof(double));
   p->i_cip.alloc(std::max<size_t>(1, ld * T.cap.size()) * sizeof(double));
   p->i_st.alloc(M * sizeof(InstState));
+  p->i_hist.alloc(ld * 2 * KHIST_LEN * sizeof(double));
   p->i_seed.alloc(ld * n * sizeof(double));
   p->i_vtp.alloc(ld * n * sizeof(double));
   p->i_out.alloc(ld * n * sizeof(double));
@@ -491,6 +492,7 @@ DevInst dev_inst(karam_problem* p) {
   I.cap_ip = p->i_cip.as<double>();
   I.v_tp = p->i_vtp.as<double>();
   I.st = p->i_st.as<InstState>();
+  I.hist = p->i_hist.as<double>();
   I.seed = nullptr;
   I.rescue_ws = p->rescue_slots > 0 ? p->r_ws.as<double>() : nullptr;
   I.rescue_list = p->rescue_slots > 0 ? p->r_list.as<RescueItem>() : nullptr;
@@ -787,10 +789,53 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   }
 }
 
+// The recorded DC convergence history of instance g, oldest first (the last
+// KHIST_LEN iterations): residuals into f, max |dv| into dv; returns the count.
+int history_of(const std::vector<double>& hist, int ld, const InstState& s, int g, double* f,
+               double* dv) {
+  const int m = std::min(s.hist_n, KHIST_LEN);
+  for (int j = 0; j < m; ++j) {
+    const int k = (s.hist_n - m + j) % KHIST_LEN;
+    f[j] = hist[(size_t)(2 * k) * ld + g];
+    dv[j] = hist[(size_t)(2 * k + 1) * ld + g];
+  }
+  return m;
+}
+
+// ConvergenceEngine::classifyFailure (solvers/convergence_engine.h:26-87) on
+// an instance's DC history: singular > exponential overflow (a step above
+// 100 V anywhere in the history) > divergence (the residual rose over each of
+// the last 5 iterations) > limit cycle (the residual changed direction in more
+// than 60 % of the iterations) > slow convergence (less than a 50 % reduction
+// over the last 10). Like the reference, it classifies converged solves too.
+// The device keeps the whole-history quantities as running counts, and the
+// last KHIST_LEN residuals, which cover the 5- and 10-iteration windows.
+int classify_failure(const InstState& s, const double* f, int m) {
+  if (s.hflags & KHF_SINGULAR) return KARAM_FAIL_SINGULAR_MATRIX;
+  if (s.hist_n == 0) return KARAM_FAIL_NONE;
+  if (s.hflags & KHF_OVERFLOW) return KARAM_FAIL_EXPONENTIAL_OVERFLOW;
+  if (s.hist_n >= 5) {
+    bool rising = true;
+    for (int j = m - 4; j < m; ++j)
+      if (!(f[j] > f[j - 1])) rising = false;
+    if (rising) return KARAM_FAIL_DIVERGENCE;
+  }
+  if (s.hist_n >= 4 && (double)s.dir_changes / (double)(s.hist_n - 2) > 0.6)
+    return KARAM_FAIL_LIMIT_CYCLE;
+  if (s.hist_n >= 10) {
+    const double first = f[m - 10], last = f[m - 1];
+    if (first > 0.0 && last > 0.5 * first) return KARAM_FAIL_SLOW_CONVERGENCE;
+  }
+  return KARAM_FAIL_NONE;
+}
+
 void read_stats(karam_problem* p, karam_instance_stats* stats, bool dc_only) {
   if (!stats) return;
   std::vector<InstState> st(p->ni);
   ck(cudaMemcpy(st.data(), p->i_st.p, st.size() * sizeof(InstState), cudaMemcpyDeviceToHost), "D2H state");
+  std::vector<double> hist((size_t)p->ld * 2 * KHIST_LEN);
+  ck(cudaMemcpy(hist.data(), p->i_hist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost),
+     "D2H history");
   for (int i = 0; i < p->ni; ++i) {
     const InstState& s = st[i];
     karam_instance_stats& o = stats[i];
@@ -804,6 +849,12 @@ void read_stats(karam_problem* p, karam_instance_stats* stats, bool dc_only) {
     o.halvings = s.halvings;
     o.max_step_iters = s.max_step_it;
     o.residual = s.resid;
+    double f[KHIST_LEN], dv[KHIST_LEN];
+    const int m = history_of(hist, p->ld, s, i, f, dv);
+    o.failure_type = classify_failure(s, f, m);
+    o.stagnation = (s.hflags & KHF_STAGNATION) ? 1 : 0;
+    o.divergence = (s.hflags & KHF_DIVERGENCE) ? 1 : 0;
+    o.history_len = s.hist_n;
   }
 }
 
@@ -1253,6 +1304,31 @@ int karam_tune_schedule(karam_problem* p, const karam_solver_opts* opts, int32_t
     p->have_dc = false;  // the state is a trial's
     if (schedule) *schedule = best;
     if (best_ms) *best_ms = best_t;
+    return KARAM_OK;
+  });
+}
+
+int karam_get_history(karam_problem* p, int32_t instance, double* residual, double* max_dv,
+                      int32_t* len) {
+  if (!p || !len || (!residual) != (!max_dv)) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    if (instance < 0 || instance >= p->ni) throw std::runtime_error("instance out of range");
+    ck(cudaStreamSynchronize(p->ctx->stream), "sync");
+    InstState s;
+    ck(cudaMemcpy(&s, p->i_st.as<InstState>() + instance, sizeof(s), cudaMemcpyDeviceToHost),
+       "D2H state");
+    std::vector<double> hist((size_t)p->ld * 2 * KHIST_LEN);
+    ck(cudaMemcpy(hist.data(), p->i_hist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost),
+       "D2H history");
+    double f[KHIST_LEN], dv[KHIST_LEN];
+    const int m = history_of(hist, p->ld, s, instance, f, dv);
+    *len = m;
+    if (residual)
+      for (int j = 0; j < m; ++j) {
+        residual[j] = f[j];
+        max_dv[j] = dv[j];
+      }
     return KARAM_OK;
   });
 }

@@ -358,6 +358,26 @@ __device__ int start_polish(InstState& s, double& gmin_out) {
   return ACT_SOLVE;
 }
 
+// Convergence history of a DC NR iteration whose final trial point has KCL
+// residual F and moved the nodes by at most dv (before s.prevF, the previous
+// iteration's residual, is replaced): the stagnation and divergence flags of
+// circuitsim_solver.cpp:427-443 and the running counts classifyFailure
+// (solvers/convergence_engine.h:26-87) needs. The (F, dv) pair itself goes
+// to the instance's history ring (instance_decide).
+__device__ __forceinline__ void record_iteration(InstState& s, double F, double dv,
+                                                 const JobParams& P) {
+  if (s.it > 0 && fabs(s.prevF - F) < 1e-15 && F > P.kcl_tol) s.hflags |= KHF_STAGNATION;
+  if (s.hist_n >= 2 && F > s.h1 && s.h1 > s.h2) s.hflags |= KHF_DIVERGENCE;
+  if (s.hist_n >= 2) {
+    const double pd = s.h1 - s.h2, cd = F - s.h1;
+    if ((pd > 0.0 && cd < 0.0) || (pd < 0.0 && cd > 0.0)) s.dir_changes++;
+  }
+  if (dv > 100.0) s.hflags |= KHF_OVERFLOW;
+  s.h2 = s.h1;
+  s.h1 = F;
+  s.hist_n++;
+}
+
 // One decision of the NR control flow for the trial point x whose KCL
 // residual is F (vconv / pok / dv compare x against the accepted point v).
 __device__ int decide(InstState& s, double F, bool vconv, bool pok, double dv,
@@ -384,6 +404,7 @@ __device__ int decide(InstState& s, double F, bool vconv, bool pok, double dv,
         return ACT_DAMP;
       }
       s.damp = 0;
+      record_iteration(s, F, dv, P);
       s.prevF = F;
       const double tol = (s.g == G - 1) ? P.kcl_tol : 1.0;
       const bool conv = (F < P.kcl_shortcut) || (vconv && !(F > tol));
@@ -671,7 +692,10 @@ __device__ bool lu_solve(T* __restrict__ A, T* __restrict__ y, int L, const DevT
 // Returns false when the instance stopped.
 __device__ bool on_singular(const DevTopo& Tp, const DevInst& I, int g) {
   InstState s = I.st[g];
-  if (s.mode == MODE_DC && s.sub == SUB_NR) s.iters += 2 * (s.it + 1);
+  if (s.mode == MODE_DC && s.sub == SUB_NR) {
+    s.iters += 2 * (s.it + 1);
+    s.hflags |= KHF_SINGULAR;
+  }
   bool alive = false;
   if (s.mode == MODE_DC && s.sub == SUB_NR && s.seeded) {
     reference_seed(Tp, I, g, I.v);
@@ -1265,7 +1289,13 @@ __device__ __forceinline__ int instance_decide(const DevTopo& Tp, const DevInst&
   reset_reductions(I, g);
   gm = 1e-12;
   hs = P.h;
+  const int h0 = s.hist_n;
   const int a = decide(s, Fm, fl & 1, (fl & 2) != 0, dvm, P, gm, hs);
+  if (s.hist_n != h0 && I.hist) {
+    const size_t k = (size_t)(h0 % KHIST_LEN) * 2;
+    I.hist[k * I.ld + g] = Fm;
+    I.hist[(k + 1) * I.ld + g] = dvm;
+  }
   if (a & ACT_RESEED) {
     s.g = 0;
     s.it = 0;

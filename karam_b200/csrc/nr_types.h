@@ -38,7 +38,7 @@
 enum { MODE_DC = 0, MODE_TRAN = 1, MODE_DONE = 2 };
 enum { SUB_NR = 0, SUB_POLISH = 1 };
 
-// Per-instance solver state (one 104-byte record, instance-major).
+// Per-instance solver state (one record per instance, instance-major).
 struct InstState {
   int mode;       // MODE_*
   int sub;        // SUB_*
@@ -63,7 +63,24 @@ struct InstState {
   int depth;      // transient step halvings in effect (sub-step = h / 2^depth)
   int frac;       // part of the current step done, in units of h / 2^max_halvings
   int halvings;   // transient restarts with a halved step
+  // convergence history of the DC NR iterations (ConvergenceStep records of
+  // CircuitSim::solveDC, circuitsim_solver.cpp:408-443): the last
+  // KHIST_LEN (residual, max |dv|) pairs sit in DevInst::hist; these are the
+  // running quantities classifyFailure and the stagnation / divergence flags
+  // need over the whole history
+  int hist_n;       // iterations recorded
+  int dir_changes;  // residual direction changes between consecutive iterations
+  int hflags;       // KHF_* bits
+  int pad_;
+  double h1, h2;    // the last two recorded residuals (h1 most recent)
 };
+
+// InstState::hflags
+#define KHF_STAGNATION 1  // residual plateaued without converging
+#define KHF_DIVERGENCE 2  // three consecutive increases of the residual
+#define KHF_SINGULAR 4    // a DC linear solve failed for good
+#define KHF_OVERFLOW 8    // some iteration moved a node by more than 100 V
+#define KHIST_LEN 16
 
 // One linear solve handed to the rescue path.
 struct RescueItem {
@@ -200,6 +217,7 @@ struct DevInst {
   int* hub_cnt;             // [n_hub_groups][ld / 32] chunk blocks done (0 between launches)
   unsigned long long* counters;  // [5]: evaluations DC, evaluations transient, solves,
                                  // rescues, rescues that needed partial pivoting
+  double* hist;             // [KHIST_LEN][2][ld] ring of (residual, max |dv|) per DC iteration
   double* wave;             // [ni][wave_steps][n_wave] node voltages after each step
   const int* wave_pos;      // permuted positions of the recorded nodes (-1 = ground)
   int n_wave, wave_steps;

@@ -176,6 +176,52 @@ struct Driver {
 
   Driver(B& be, const oracle_opts& oo) : b(be), o(oo) {}
 
+  // DC convergence history (ConvergenceStep records, circuitsim_solver.cpp:
+  // 408-425): residual and max |v_new - v_old| of every DC NR iteration, and
+  // the stagnation / divergence flags of :427-443.
+  std::vector<double> h_res, h_dv;
+  bool h_stag = false, h_div = false, h_sing = false;
+
+  void record(int it, double prev_kcl, double kcl, const std::vector<double>& x,
+              const std::vector<double>& v) {
+    double md = 0.0;
+    for (int i = 0; i < b.n; ++i) md = std::max(md, std::fabs(x[i] - v[i]));
+    h_res.push_back(kcl);
+    h_dv.push_back(md);
+    if (it > 0 && std::fabs(prev_kcl - kcl) < 1e-15 && kcl > o.kcl_tol) h_stag = true;
+    const size_t z = h_res.size();
+    if (z >= 3 && h_res[z - 1] > h_res[z - 2] && h_res[z - 2] > h_res[z - 3]) h_div = true;
+  }
+
+  // ConvergenceEngine::classifyFailure (solvers/convergence_engine.h:26-87),
+  // numbered as ConvergenceFailureType (infrastructure/simtrace.h:39-47).
+  int classify() const {
+    if (h_sing) return 1;
+    const size_t z = h_res.size();
+    if (z == 0) return 0;
+    for (double d : h_dv)
+      if (d > 100.0) return 6;
+    if (z >= 5) {
+      bool up = true;
+      for (size_t i = z - 4; i < z; ++i)
+        if (h_res[i] <= h_res[i - 1]) up = false;
+      if (up) return 2;
+    }
+    if (z >= 4) {
+      int ch = 0;
+      for (size_t i = 2; i < z; ++i) {
+        const double pd = h_res[i - 1] - h_res[i - 2], cd = h_res[i] - h_res[i - 1];
+        if ((pd > 0 && cd < 0) || (pd < 0 && cd > 0)) ch++;
+      }
+      if ((double)ch / (double)(z - 2) > 0.6) return 3;
+    }
+    if (z >= 10) {
+      const double a = h_res[z - 10], c = h_res.back();
+      if (a > 0.0 && c > 0.5 * a) return 4;
+    }
+    return 0;
+  }
+
   void add_gmin(std::vector<double>& v, double gmin) {
     for (int i = 0; i < b.n; ++i) v[b.pat.diag[i]] += gmin;
   }
@@ -270,6 +316,7 @@ struct Driver {
         if (!newton_point(v, gmin, 0.0, 0, 0.0, x)) {
           final_kcl = 1e9;
           st->singular = 1;
+          h_sing = true;
           st->iterations += it + 1;
           break;
         }
@@ -288,6 +335,7 @@ struct Driver {
             st->damped++;
           }
         }
+        record(it, final_kcl, kcl, x, v);
         final_kcl = kcl;
         double tol = (g == G - 1) ? o.kcl_tol : 1.0;
         if (check_convergence(o, x, v, kcl, tol)) {
@@ -354,6 +402,9 @@ struct Driver {
 
   int solve_dc(const double* v0, std::vector<double>& v, oracle_stats* st) {
     std::memset(st, 0, sizeof(*st));
+    h_res.clear();
+    h_dv.clear();
+    h_stag = h_div = h_sing = false;
     v.assign(b.n, 0.0);
     bool conv = false;
     if (o.seeded && v0) {
@@ -381,6 +432,10 @@ struct Driver {
     st->converged = conv ? 1 : 0;
     if (conv) polish(v, 0.0, 0, 0.0, st);
     final_residual(v, 0.0, 0, 0.0, st);
+    st->failure_type = classify();
+    st->stagnation = h_stag ? 1 : 0;
+    st->divergence = h_div ? 1 : 0;
+    st->history_len = (int32_t)h_res.size();
     return 0;
   }
 

@@ -51,6 +51,11 @@ typedef struct oracle_stats {
   int32_t seeded_ok;
   int32_t max_step_iters; /* transient: most NR iterations of one step */
   double residual;       /* final max |KCL| [A] */
+  /* DC convergence diagnostics of CircuitSim::solveDC (circuitsim_solver.cpp:408-443, 516) */
+  int32_t failure_type;  /* ConvergenceEngine::classifyFailure over the whole DC history */
+  int32_t stagnation;
+  int32_t divergence;
+  int32_t history_len;
 } oracle_stats;
 
 /* Fills o with the reference constants; polish off, dense solver. */

@@ -39,7 +39,9 @@ class OracleStats(C.Structure):
                 ("polish_iters", C.c_int32), ("damped", C.c_int32),
                 ("gmin_step", C.c_int32), ("singular", C.c_int32),
                 ("seeded_ok", C.c_int32), ("max_step_iters", C.c_int32),
-                ("residual", C.c_double)]
+                ("residual", C.c_double), ("failure_type", C.c_int32),
+                ("stagnation", C.c_int32), ("divergence", C.c_int32),
+                ("history_len", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

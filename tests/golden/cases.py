@@ -70,5 +70,14 @@ SMALL = {
 }
 BENCH = {"config1": circuits.config1, "config2": circuits.config2}
 
+# Larger grids of the uneven-batch family (n = 258, 1026, 4098 unknowns), where
+# the level schedules run a CTA per instance. Each fixture holds the symbolic
+# layer, DC solutions of two Monte-Carlo instances and a trapezoidal waveform
+# of instance 0 (GRID_TRAN), all from the reference-built library.
+GRIDS = {"grid16": 16, "grid32": 32, "grid64": 64}
+GRID_TRAN = dict(dt=40e-12, steps=20, max_halvings=6)  # the gate ramp: steps 13-18
+GRID_WAVE = {16: [3, 50, 130, 200, 258], 32: [3, 200, 530, 900, 1026],
+             64: [3, 900, 2050, 3500, 4098]}
+
 RNG_SEEDS = (circuits.BASE_SEED, circuits.BASE_SEED + 1, circuits.BASE_SEED + 4095, 1)
 RNG_COUNT = 64

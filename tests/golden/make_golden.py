@@ -12,6 +12,7 @@ solveSparse_LU, and PortableNormalDist draws.
 
     python tests/golden/make_golden.py          # rewrites tests/golden/*.npz
     python tests/golden/make_golden.py grid8    # only the named cases
+    python tests/golden/make_golden.py grid64   # a large grid (minutes: dense-workspace LU)
 """
 import os
 import sys
@@ -67,6 +68,33 @@ def stamps(ref, nl, inst=None):
     return out
 
 
+def grid_fixture(ref, name, N):
+    """Symbolic layer, probe stamps, DC of MC instances 0 and 1 and a
+    trapezoidal waveform of instance 0 on the N x N grid, from the reference
+    build; the linear solves use solveSparse_LU on the translated ordering."""
+    nl = circuits.grid_circuit(N)
+    inst = circuits.mc_instances(nl, 2)
+    out = symbolic(ref, nl)
+    out.update(stamps(ref, nl, inst))
+    out["mc_kp"], out["mc_vto"] = inst.mos_kp, inst.mos_vto
+    vs, sts = [], []
+    for i in range(2):
+        v, st = ref.solve_dc(nl, inst, i, linear_solver=pyoracle.LS_SPARSE, **POLISH)
+        vs.append(v)
+        sts.append(stats_arr(st))
+    out["dc_v"], out["dc_stats"] = np.array(vs), np.array(sts)
+    tr = cases.GRID_TRAN
+    wave_nodes = cases.GRID_WAVE[N]
+    vt, st, wave = ref.transient(nl, vs[0], tr["dt"], tr["steps"], A.TRAN_TRAP, inst, 0,
+                                 wave_nodes=wave_nodes, linear_solver=pyoracle.LS_SPARSE,
+                                 max_halvings=tr["max_halvings"], **POLISH)
+    out["tran_v"], out["tran_stats"], out["tran_wave"] = vt, stats_arr(st), wave
+    out["tran_wave_nodes"] = np.array(wave_nodes, np.int32)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "n =", nl.n_nodes, "nnz =", len(out["col_tran"]), "dc stats",
+          out["dc_stats"].tolist(), "tran stats", out["tran_stats"].tolist(), flush=True)
+
+
 def stats_arr(st):
     keys = ("converged", "iterations", "polish_iters", "damped", "gmin_step", "singular")
     return np.array([st[k] for k in keys], np.int64)
@@ -91,6 +119,10 @@ def main():
         np.savez_compressed(os.path.join(HERE, "rng_normals.npz"), seeds=seeds, normals=normals)
 
     only = set(sys.argv[1:])  # case names to regenerate (default: all)
+    for name, N in cases.GRIDS.items():
+        if only and name not in only:
+            continue
+        grid_fixture(ref, name, N)
     for name, make in {**cases.SMALL, **cases.BENCH}.items():
         if only and name not in only:
             continue

@@ -157,3 +157,53 @@ def test_product_symbolic(product, name):
     assert prob.info["fill_in"] == int(g["fill_in"])
     mo, do = prob.device_order()
     assert np.array_equal(mo, g["mos_order"]) and np.array_equal(do, g["dio_order"])
+
+
+# ---------------------------------------------------------------------------
+# larger grids of the uneven-batch family: bit-exact symbolic layer of the
+# product, and the restatement's solutions, against the reference build
+# ---------------------------------------------------------------------------
+def grid_case(name):
+    N = cases.GRIDS[name]
+    g = golden(name)
+    nl = circuits.grid_circuit(N)
+    return nl, g, circuits.Instances(2, g["mc_kp"], g["mc_vto"])
+
+
+@pytest.mark.parametrize("name", list(cases.GRIDS))
+def test_product_symbolic_grids(product, name):
+    nl, g, inst = grid_case(name)
+    assert np.array_equal(inst.mos_kp, circuits.mc_instances(nl, 2).mos_kp)
+    prob = product.Problem(None, nl)
+    rp, col = prob.pattern()
+    assert np.array_equal(rp, g["rp_tran"]) and np.array_equal(col, g["col_tran"])
+    assert np.array_equal(prob.stamp_map(), g["stamp_map"])
+    raw, perm, tw = prob.ordering()
+    assert np.array_equal(raw, g["raw_order"]) and np.array_equal(perm, g["perm_translated"])
+    assert tw == int(g["treewidth"])
+    frp, fcol = prob.filled_pattern()
+    assert np.array_equal(frp, g["f_row_ptr"]) and np.array_equal(fcol, g["f_col"])
+    assert prob.info["fill_in"] == int(g["fill_in"])
+    mo, do = prob.device_order()
+    assert np.array_equal(mo, g["mos_order"]) and np.array_equal(do, g["dio_order"])
+
+
+@pytest.mark.parametrize("name", ["grid16", "grid32"])
+def test_port_grids(port, name):
+    from oracle import pyoracle
+    nl, g, inst = grid_case(name)
+    raw, perm, tw = port.ordering(nl)
+    assert np.array_equal(raw, g["raw_order"]) and np.array_equal(perm, g["perm_translated"])
+    vals, rhs = port.stamp(nl, g["probe_v"], inst, 0)
+    assert np.array_equal(vals, g["stamp_dc_vals"]) and np.array_equal(rhs, g["stamp_dc_rhs"])
+    for i in range(2):
+        v, st = port.solve_dc(nl, inst, i, linear_solver=pyoracle.LS_SPARSE, polish_max=8)
+        assert np.array_equal(stats_arr(st), g["dc_stats"][i])
+        assert np.allclose(v, g["dc_v"][i], rtol=1e-12, atol=1e-15)
+    if name == "grid16":
+        tr = cases.GRID_TRAN
+        v, st, wave = port.transient(nl, g["dc_v"][0], tr["dt"], tr["steps"], A.TRAN_TRAP, inst, 0,
+                                     wave_nodes=g["tran_wave_nodes"], linear_solver=pyoracle.LS_SPARSE,
+                                     max_halvings=tr["max_halvings"], polish_max=8)
+        assert np.array_equal(stats_arr(st), g["tran_stats"])
+        assert np.allclose(wave, g["tran_wave"], rtol=1e-12, atol=1e-15)

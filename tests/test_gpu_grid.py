@@ -134,3 +134,36 @@ def test_tail_switch_keeps_results(product, ctx, prec):
     assert np.array_equal(v0, v1) and np.array_equal(v0, v3)
     assert [s["iterations"] for s in s0] == [s["iterations"] for s in s1]
     assert sum(s["status"] == A.ST_CONVERGED for s in s0) >= ni - 2
+
+
+# The larger grids against their reference-built fixtures (tests/golden/
+# grid16/32/64.npz): DC of two Monte-Carlo instances and a trapezoidal waveform
+# across the gate ramp. Slots in shared memory where they fit (FP32 slots up to
+# grid 32, FP64 up to grid 16), in global memory everywhere.
+LARGE = [("grid16", -1, A.PREC_FP64), ("grid16", -1, A.PREC_MIXED), ("grid16", -2, A.PREC_MIXED),
+         ("grid32", -1, A.PREC_MIXED), ("grid32", -2, A.PREC_FP64), ("grid32", -2, A.PREC_MIXED),
+         ("grid64", -2, A.PREC_FP64), ("grid64", -2, A.PREC_MIXED)]
+
+
+@pytest.mark.parametrize("name,schedule,prec", LARGE)
+def test_large_grid_matches_reference_fixture(product, ctx, name, schedule, prec):
+    import cases
+    g = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    nl = circuits.grid_circuit(cases.GRIDS[name])
+    inst = circuits.Instances(2, g["mc_kp"], g["mc_vto"])
+    tr = cases.GRID_TRAN
+    prob = product.Problem(ctx, nl, max_instances=2)
+    prob.set_instances(inst)
+    opts = product.options(precision=prec, schedule=schedule, max_halvings=tr["max_halvings"],
+                           **POLISH)
+    v, st = prob.solve_dc(opts)
+    assert prob.timing()["level_schedule"] == KIND[schedule]
+    for i in range(2):
+        assert st[i]["status"] == A.ST_CONVERGED
+        assert scaled_err(v[i], g["dc_v"][i]) <= 1.0, (i, scaled_err(v[i], g["dc_v"][i]))
+    nodes = [int(x) for x in g["tran_wave_nodes"]]
+    vt, st, wave = prob.step_transient(tr["dt"], tr["steps"], A.TRAN_TRAP, opts, wave_nodes=nodes)
+    assert st[0]["status"] == A.ST_CONVERGED
+    assert scaled_err(vt[0], g["tran_v"]) <= 1.0, scaled_err(vt[0], g["tran_v"])
+    w_ref = g["tran_wave"]
+    assert np.max(np.abs(wave[0] - w_ref)) <= 1e-9 * np.max(np.abs(w_ref)) + 1e-12
