@@ -1181,12 +1181,19 @@ __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __rest
   const int NL = prog[0], lvt = prog[1], tpb = prog[2], ypb = prog[3], bpb = prog[4];
   bool ok = true;
   T lmax = T(0);
+  // the gmin diagonal joins before the elimination, as the reference's
+  // addDiagonalConditioning (physics/circuitsim.h:2857) precedes its LU
+  for (int lv = 0; lv < NL; ++lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    for (int q = lane; q < Lt[1]; q += 32) A[prog[Lt[0] + q]] += gmin;
+  }
+  __syncwarp();
   for (int lv = 0; lv < NL; ++lv) {
     const int* Lt = prog + lvt + 12 * lv;
     const int po = Lt[0], pc = Lt[1], lo = Lt[2], lc = Lt[3];
     for (int q = lane; q < pc; q += 32) {
       const int d = prog[po + q];
-      const T piv = A[d] + gmin;  // the gmin diagonal joins at the pivot step
+      const T piv = A[d];
       ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
       A[d] = recip(piv);
     }
@@ -1342,12 +1349,17 @@ __device__ bool nd_solve_cta(T* __restrict__ A, T* __restrict__ y, const int* __
   const int NL = prog[0], lvt = prog[1], tpb = prog[2], ypb = prog[3], bpb = prog[4];
   bool ok = true;
   T lmax = T(0);
+  for (int lv = 0; lv < NL; ++lv) {  // the gmin diagonal, before the elimination
+    const int* Lt = prog + lvt + 12 * lv;
+    for (int q = tid; q < Lt[1]; q += bd) A[prog[Lt[0] + q]] += gmin;
+  }
+  __syncthreads();
   for (int lv = 0; lv < NL; ++lv) {
     const int* Lt = prog + lvt + 12 * lv;
     const int po = Lt[0], pc = Lt[1], lo = Lt[2], lc = Lt[3];
     for (int q = tid; q < pc; q += bd) {
       const int d = prog[po + q];
-      const T piv = A[d] + gmin;
+      const T piv = A[d];
       ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
       A[d] = recip(piv);
     }
@@ -1747,11 +1759,14 @@ __device__ bool big_solve(T* __restrict__ A, T* __restrict__ y, const DevTopo& T
   const int lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
   bool ok = true, finite = true;
   T lmax = T(0);
+  // the gmin diagonal, before the elimination (addDiagonalConditioning)
+  for (int q = tid; q < Tp.n; q += bd) A[__ldg(&Tp.nd_diag[q])] += gmin;
+  __syncthreads();
   for (int lv = 0; lv < Tp.nd_levels; ++lv) {
     const int p0 = __ldg(&Tp.lv_piv_ptr[lv]), p1 = __ldg(&Tp.lv_piv_ptr[lv + 1]);
     for (int q = p0 + tid; q < p1; q += bd) {
       const int d = __ldg(&Tp.nd_diag[__ldg(&Tp.lv_piv[q])]);
-      const T piv = A[d] + gmin;  // the gmin diagonal joins at the pivot step
+      const T piv = A[d];
       ok = ok && isfinite(piv) && !(fabs(piv) < tiny);
       A[d] = recip(piv);
     }
