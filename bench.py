@@ -389,7 +389,8 @@ def run_karam(args, dist):
                      + t["other_launches"])
         lanes = t["lanes"]
         lu_name = ["k_lu<float>", "k_lu_nd<float>", "k_lu_big<float, smem>",
-                   "k_lu_big<float, global>", "k_lu_big<float, packed>"][t["level_schedule"]]
+                   "k_lu_big<float, global>", "k_lu_big<float, packed>",
+                   "k_persist<float>"][t["level_schedule"]]
         conv_min = min(conv_min, conv)
     clk = clocks.stop()
     dist.barrier()
@@ -575,24 +576,46 @@ def config1_latency(ctx, reps=50):
     nl = circuits.config1()
     prob = K.Problem(ctx, nl, max_instances=1)
     prob.set_instances(None)
-    opts = K.options(precision=A.PREC_FP64)
-    for _ in range(3):
-        prob.solve_dc(opts)
-    wall, dev = [], []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        v, st = prob.solve_dc(opts)
-        wall.append(time.perf_counter() - t0)
-        dev.append(prob.timing()["job_ms"])
+
+    def timed(schedule):
+        opts = K.options(precision=A.PREC_FP64, schedule=schedule)
+        for _ in range(3):
+            prob.solve_dc(opts)
+        wall, dev = [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            v, st = prob.solve_dc(opts)
+            wall.append(time.perf_counter() - t0)
+            dev.append(prob.timing()["job_ms"])
+        return v, st, 1e6 * statistics.median(wall), 1e3 * statistics.median(dev), prob.timing()
+
+    # the default schedule (the persistent kernel: every round in one launch)
+    # and the round-per-launch graph of the block-per-instance kernels
+    v, st, wall, dev, t = timed(0)
+    vg, stg, wall_g, dev_g, _ = timed(-3)
     kind = "ref" if pyoracle.available("ref") else "port"
     if kind == "port":
         pyoracle.build("port")
     with native_stdout_to_stderr():
-        v_ref, st_ref = pyoracle.Oracle(kind).solve_dc(nl)
+        orc = pyoracle.Oracle(kind)
+        v_ref, st_ref = orc.solve_dc(nl)
+        cpu = []
+        for _ in range(20):  # the reference CPU path, one host thread, same run
+            t0 = time.perf_counter()
+            orc.solve_dc(nl)
+            cpu.append(time.perf_counter() - t0)
     prob.close()
     return {"workload": "32-stage inverter chain, VIN 0.9 V, n=34; plain FP64 DC, 1 instance",
-            "us_per_solve_wall": 1e6 * statistics.median(wall),
-            "us_per_solve_device": 1e3 * statistics.median(dev),
+            "us_per_solve_wall": wall, "us_per_solve_device": dev,
+            "schedule": "persistent CTA (all NR rounds in one launch)" if t["level_schedule"] == 5
+                        else f"level_schedule {t['level_schedule']}",
+            "rounds": t["rounds"],
+            "graph_rounds": {"us_per_solve_wall": wall_g, "us_per_solve_device": dev_g,
+                             "schedule": "CUDA graph of per-round launches (CTA per instance, packed)",
+                             "identical_result": bool(np.array_equal(v, vg))},
+            "cpu_reference": {"us_per_solve": 1e6 * statistics.median(cpu), "cores": 1,
+                              "kind": "reference" if kind == "ref" else "port",
+                              "sample": "20 solves of the same DC, one host thread"},
             "iterations": st[0]["iterations"], "iterations_oracle": st_ref["iterations"],
             "converged": st[0]["status"] == A.ST_CONVERGED,
             "max_abs_diff_vs_oracle_v": float(np.max(np.abs(v[0] - v_ref)))}
@@ -662,7 +685,8 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample
             conv += sum(1 for s in st if s["status"] == A.ST_CONVERGED)
             k = ["pivot records", "warp per instance", "CTA per instance, shared memory",
                  "CTA per instance, global memory",
-                 "CTA per instance, packed program"][prob.timing()["level_schedule"]]
+                 "CTA per instance, packed program",
+                 "persistent CTA per instance"][prob.timing()["level_schedule"]]
             kinds[k] = kinds.get(k, 0) + 1
             out[N] = (v, st)
         return wall, conv, kinds, out

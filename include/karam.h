@@ -179,8 +179,14 @@ typedef struct karam_solver_opts {
                             program), -1 one CTA per instance with its slots in
                             shared memory, -2 the same with them in global
                             memory, -3 one CTA per instance with its slots and
-                            the packed level program in shared memory; 0 =
-                            chosen from shared memory, occupancy and batch size */
+                            the packed level program in shared memory, -4 the
+                            persistent kernel: one CTA per instance running all
+                            of its rounds in one launch (the code of -3); 0 =
+                            chosen from shared memory, occupancy and batch size
+                            (-4 for batches no larger than the SM count where it
+                            fits). Batches larger than the SM count switch to
+                            -4 for their last rounds, once no more instances
+                            are live than SMs, unless kernel_timing is set     */
   int32_t max_rounds;    /* device round budget per launch (0 = unlimited)        */
   int32_t max_halvings;  /* transient: a step whose NR exhausts max_nr_iter restarts
                             from the last time point with half the step, at most
@@ -333,11 +339,11 @@ KARAM_API void karam_spice_free(karam_spice *s);
  * solves one instance at a time). Runs the first `rounds` NR rounds of a DC
  * job from the reference seed once per feasible schedule (the planner's
  * choice, a CTA per instance with its slots and the packed program in shared
- * memory, with its slots alone there, with them in global memory), timed on
- * the device, and keeps the fastest for this
- * problem and, process-wide, for problems of the same unknowns, stamp
- * non-zeros, batch size and precision; solves with opts.schedule == 0 then use
- * it. *schedule receives it as an opts.schedule value and *best_ms (either may
+ * memory, with its slots alone there, with them in global memory, the
+ * persistent kernel), timed on the device, and keeps the fastest for this
+ * problem and, process-wide, for problems made from an identical netlist with
+ * the same batch size and precision on the same device; solves with
+ * opts.schedule == 0 then use it. *schedule receives it as an opts.schedule value and *best_ms (either may
  * be null) its trial time. The problem's state afterwards is a trial's: run
  * the solve again. */
 KARAM_API int karam_tune_schedule(karam_problem *p, const karam_solver_opts *opts, int32_t rounds,
@@ -484,7 +490,8 @@ typedef struct karam_timing {
                                instance's slots in shared memory (k_lu_big), 3 the
                                same with the slots in global memory, 4 a CTA per
                                instance with slots and packed program in shared
-                               memory                                                */
+                               memory, 5 the persistent kernel (all rounds of an
+                               instance in one launch, the code of 4)                */
   int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */
@@ -492,6 +499,8 @@ typedef struct karam_timing {
   int64_t rescues_dense;    /* of those, the ones that needed partial pivoting       */
   int32_t tail_rounds;      /* rounds run with a CTA per live instance over the list of
                                live instances (once no more are live than SMs)       */
+  int32_t persistent_rounds; /* rounds run inside the persistent per-instance kernel
+                               (every remaining round of an instance in one launch) */
 } karam_timing;
 KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 

@@ -96,7 +96,8 @@ class KaramTiming(C.Structure):
                 ("lanes", C.c_int32), ("level_schedule", C.c_int32),
                 ("evals_dc", C.c_int64), ("evals_tran", C.c_int64),
                 ("solves", C.c_int64), ("rescues", C.c_int64),
-                ("rescues_dense", C.c_int64), ("tail_rounds", C.c_int32)]
+                ("rescues_dense", C.c_int64), ("tail_rounds", C.c_int32),
+                ("persistent_rounds", C.c_int32)]
 
 
 def ptr(arr, ctype):

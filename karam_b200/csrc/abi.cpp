@@ -439,7 +439,7 @@ void alloc_instances(karam_problem* p) {
   p->i_seed.alloc(ld * n * sizeof(double));
   p->i_vtp.alloc(ld * n * sizeof(double));
   p->i_out.alloc(ld * n * sizeof(double));
-  p->d_active.alloc(sizeof(int));
+  p->d_active.alloc(2 * sizeof(int));  // live instances; most rounds of a persistent launch
   p->d_seed_ok.alloc(sizeof(int));
   p->d_counters.alloc(5 * sizeof(unsigned long long));
   ck(cudaEventCreate(&p->ev_job0), "cudaEventCreate");
@@ -467,7 +467,7 @@ void alloc_instances(karam_problem* p) {
     p->r_count.alloc(sizeof(int));
     ck(cudaMemset(p->r_count.p, 0, sizeof(int)), "memset rescue count");
   }
-  ck(cudaMallocHost(&p->h_active, sizeof(int)), "cudaMallocHost");
+  ck(cudaMallocHost(&p->h_active, 2 * sizeof(int)), "cudaMallocHost");
 }
 
 DevInst dev_inst(karam_problem* p) {
@@ -659,7 +659,8 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   DevInst I = inst ? *inst : dev_inst(p);
   const int prec = P.precision;
   const int max_smem = p->ctx->max_smem, num_sms = p->ctx->num_sms;
-  RoundLaunch L = plan_round(p->dt, p->ni, prec, max_smem, num_sms, want_lanes);
+  // the per-round graph's plan (the planner's choice under the persistent option)
+  RoundLaunch L = plan_round(p->dt, p->ni, prec, max_smem, num_sms, want_lanes == -4 ? 0 : want_lanes);
   if (L.L < 1 && from_tuner && want_lanes != 0) {
     // a measured schedule that does not fit here falls back to the planner's choice
     cudaGetLastError();
@@ -675,6 +676,42 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
     LT = plan_round(p->dt, p->ni, prec, max_smem, num_sms, -3);
     cudaGetLastError();
   }
+  // The persistent per-instance kernel runs an instance's remaining rounds in
+  // one launch with the code of the per-instance round kernels: for batches
+  // no larger than the SM count (opts.schedule 0 or -4) and for the tail once
+  // no more instances are live than SMs. Each CTA rescues its own failed
+  // solves, so the rescue workspace must have a slot per CTA.
+  const int want = want_lanes;  // after the measured choice
+  size_t psm = 0;
+  if (!timed && p->max_hub_chunks <= 8) {
+    psm = plan_persist(p->dt, prec, p->rplan, max_smem);
+    cudaGetLastError();
+  }
+  auto persist_fits = [&](int grid) {
+    return psm > 0 && (p->rescue_slots == 0 || p->rescue_slots >= grid);
+  };
+  const int budget = max_rounds > 0 ? max_rounds : (1 << 30);
+  int* active = p->d_active.as<int>();
+  // all rounds of every instance in one launch
+  auto run_persist = [&](const DevInst& Ip, int grid, int rounds_left, bool is_tail) {
+    ck(cudaMemsetAsync(active, 0, 2 * sizeof(int), s), "memset active");
+    launch_persist(p->dt, Ip, P, prec, grid, psm, rounds_left, p->rplan.K, active, active + 1, s);
+    ck(cudaGetLastError(), "k_persist launch");
+    ck(cudaMemcpyAsync(p->h_active, active, 2 * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
+    ck(cudaStreamSynchronize(s), "persistent sync");
+    ++p->timing.other_launches;
+    p->timing.rounds += p->h_active[1];
+    p->timing.persistent_rounds += p->h_active[1];
+    if (is_tail) p->timing.tail_rounds += p->h_active[1];
+  };
+  if (want == -4 && !persist_fits(p->ni))
+    throw std::runtime_error("the persistent per-instance schedule does not fit this problem");
+  if (want == -4 || (want == 0 && p->ni <= num_sms && persist_fits(p->ni))) {
+    p->timing.lanes = 1;
+    p->timing.level_schedule = 5;
+    run_persist(I, p->ni, budget, false);
+    return;
+  }
   if (L.big == 2) {  // the ND slots of every instance in global memory
     const size_t need = (size_t)p->ni * (size_t)p->dt.nd_S * sizeof(double);
     if (p->i_luws.bytes < need) p->i_luws.alloc(need);
@@ -688,7 +725,6 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
       for (auto e : v) cudaEventDestroy(e);
     }
   } eg{ev};
-  int* active = p->d_active.as<int>();
 
   struct Graph {
     cudaGraph_t g = nullptr;
@@ -737,7 +773,6 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   capture(main_g, L, Im);
   bool tail = false;
 
-  const int budget = max_rounds > 0 ? max_rounds : (1 << 30);
   while (true) {
     ck(cudaGraphLaunch(tail ? tail_g.e : main_g.e, s), "graph launch");
     ck(cudaMemcpyAsync(p->h_active, active, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
@@ -778,6 +813,13 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
       It[1].live_out = list0;
       It[1].live_out_count = cnt;
       LT.grid = *p->h_active;  // instances only ever leave the live set
+      if (persist_fits(LT.grid)) {  // the remaining rounds of every live instance in one launch
+        DevInst Ip = I;
+        Ip.live_in = list0;
+        Ip.live_in_count = cnt;
+        run_persist(Ip, LT.grid, budget - p->timing.rounds, true);
+        break;
+      }
       // the per-instance evaluation kernel, when its device values fit the
       // default 48 KiB of dynamic shared memory and its hubs 8 chunks
       LT.es_one = p->max_hub_chunks <= 8 &&
@@ -1277,6 +1319,10 @@ int karam_tune_schedule(karam_problem* p, const karam_solver_opts* opts, int32_t
       const int val = L.big ? -L.big : L.L;
       if (std::find(cands.begin(), cands.end(), val) == cands.end()) cands.push_back(val);
     }
+    if (p->max_hub_chunks <= 8 && (p->rescue_slots == 0 || p->rescue_slots >= p->ni) &&
+        plan_persist(p->dt, prec, p->rplan, p->ctx->max_smem) > 0)
+      cands.push_back(-4);
+    cudaGetLastError();
     if (cands.empty()) throw std::runtime_error("no factor/solve schedule fits this problem");
     int best = cands[0];
     double best_t = 1e300;

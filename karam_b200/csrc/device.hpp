@@ -69,6 +69,20 @@ RescuePlan plan_rescue(const DevTopo& T);
 int rescue_ctas_per_sm(const DevTopo& T, const RescuePlan& R);
 void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const RescuePlan& R,
                    cudaStream_t s);
+// Dynamic shared memory of the persistent per-instance kernel (k_persist) for
+// precision prec and rescue plan R, or 0 when the problem cannot use it: it
+// needs the packed level program, and its phases (evaluation + stamping of
+// one instance, the packed factor/solve, a rescue warp) must each fit one
+// CTA's shared memory. Sets the kernel's shared-memory limit (call outside
+// stream capture).
+size_t plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_smem);
+// Every remaining NR round of each listed instance (or of instances
+// 0 .. grid - 1 when I.live_in is null) in one launch of `grid` CTAs, at most
+// max_rounds rounds each; *active receives the instances still live and
+// *rounds_max the most rounds one instance ran.
+void launch_persist(const DevTopo& T, const DevInst& I, const JobParams& P, int prec, int grid,
+                    size_t smem, int max_rounds, int K, int* active, int* rounds_max,
+                    cudaStream_t s);
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s);
 // [ni][n] FP32 per-device parameters (netlist order) into [n][ld] SoA order.

@@ -261,6 +261,40 @@ void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const
     k_rescue<double><<<grid, 32 * R.warps, R.smem, s>>>(T, I, P, R.K);
 }
 
+size_t plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_smem) {
+  if (T.nd_prog_len <= 0 || T.nd_levels <= 0) return 0;
+  const size_t es = prec == KARAM_PREC_MIXED ? sizeof(float) : sizeof(double);
+  const size_t ev = sizeof(double) * (3 * (size_t)(T.n_mos + T.n_dio) + (size_t)T.n_ft_terms +
+                                      (size_t)T.n_hub_slot_terms);
+  const size_t lu = ((es * ((size_t)T.nd_SY + (size_t)T.nd_S) + 15) & ~size_t(15)) +
+                    sizeof(int) * (((size_t)T.nd_prog_len + 3) & ~size_t(3));
+  const size_t rs = R.warps > 0 ? (T.lu_rec ? rescue_rec_bytes(T.n) : 0) + rescue_tab_bytes(T.n, T.nv) +
+                                      rescue_warp_bytes(T.n, T.nv, R.K)
+                                : 0;
+  const size_t sm = std::max({ev, lu, rs});
+  const void* kern = prec == KARAM_PREC_MIXED ? (const void*)k_persist<float> : (const void*)k_persist<double>;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (sm + fa.sharedSizeBytes > (size_t)max_smem) return 0;
+  if (open_smem_limit(kern, max_smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return std::max<size_t>(sm, 16);
+}
+
+void launch_persist(const DevTopo& T, const DevInst& I, const JobParams& P, int prec, int grid,
+                    size_t smem, int max_rounds, int K, int* active, int* rounds_max,
+                    cudaStream_t s) {
+  if (prec == KARAM_PREC_MIXED)
+    k_persist<float><<<grid, kPersistThreads, smem, s>>>(T, I, P, max_rounds, K, active, rounds_max);
+  else
+    k_persist<double><<<grid, kPersistThreads, smem, s>>>(T, I, P, max_rounds, K, active, rounds_max);
+}
+
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s) {
   k_unpermute<<<grid_for((size_t)n * ld, 256), 256, 0, s>>>(v_perm, perm, out, ni, ld, n);

@@ -944,18 +944,13 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
 // device values [3][devices] (gm or diode g, gds or diode i, ids), then every
 // node term's signed value and every hub slot term's signed value, computed
 // side by side before the sums (a - c and a + (-c) round alike).
+// The body of k_es_one for instance g, by the whole CTA (s_val: the dynamic
+// shared memory described above; s_f, s_dv, s_fl: one entry per warp).
 template <typename TJ>
-__global__ void __launch_bounds__(kBigThreads) k_es_one(DevTopo T, DevInst I, JobParams P) {
-  extern __shared__ __align__(16) double s_val[];
-  __shared__ unsigned long long s_f[kBigThreads / 32], s_dv[kBigThreads / 32];
-  __shared__ int s_fl[kBigThreads / 32];
+__device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobParams& P, int g,
+                                double* s_val, unsigned long long* s_f, unsigned long long* s_dv,
+                                int* s_fl) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  if (blockIdx.x == 0 && tid == 0) {  // the round's lists start empty, as in k_es
-    if (I.rescue_count) *I.rescue_count = 0;
-    if (I.live_out_count) *I.live_out_count = 0;
-  }
-  if ((int)blockIdx.x >= *I.live_in_count) return;
-  const int g = I.live_in[blockIdx.x];
   const size_t ld = I.ld;
   const int nv = T.nv, n = T.n, nm = T.n_mos, nd = T.n_mos + T.n_dio;
   const double heff = I.ev_heff[g];
@@ -1120,6 +1115,19 @@ __global__ void __launch_bounds__(kBigThreads) k_es_one(DevTopo T, DevInst I, Jo
     atomicMax(&I.red_dv[g], dv);
     if (fl != 3) atomicAnd(&I.red_flags[g], fl);
   }
+}
+
+template <typename TJ>
+__global__ void __launch_bounds__(kBigThreads) k_es_one(DevTopo T, DevInst I, JobParams P) {
+  extern __shared__ __align__(16) double s_val[];
+  __shared__ unsigned long long s_f[kBigThreads / 32], s_dv[kBigThreads / 32];
+  __shared__ int s_fl[kBigThreads / 32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {  // the round's lists start empty, as in k_es
+    if (I.rescue_count) *I.rescue_count = 0;
+    if (I.live_out_count) *I.live_out_count = 0;
+  }
+  if ((int)blockIdx.x >= *I.live_in_count) return;
+  es_one_instance<TJ>(T, I, P, I.live_in[blockIdx.x], s_val, s_f, s_dv, s_fl);
 }
 
 // Reductions of an instance back to their neutral values.
@@ -1854,17 +1862,23 @@ __device__ bool big_solve(T* __restrict__ A, T* __restrict__ y, const DevTopo& T
 // on it (nd_solve_cta) instead of reading the schedule tables from global
 // memory. With I.live_in, CTA b takes the b-th listed instance and lists it
 // in I.live_out when it stays live.
+// What the body of k_lu_big leaves for its caller (shared memory).
+struct LuShared {
+  int a, live, trev, sing;
+  double gmin, hsub;
+};
+
+// The body of k_lu_big for instance g, by the whole CTA: the decision, the
+// vector updates, the factor/solve and x = v + dx with junction limiting.
+// sh receives the action bits, whether the instance was live, whether it
+// evaluated a transient point, whether the static pivots failed, and the
+// gmin of the solve.
 template <typename T, bool gA, bool packed>
-__global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, JobParams P, int* active) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int s_a, s_live, s_trev, s_sing;
-  __shared__ double s_gmin, s_hsub;
+__device__ void lu_big_instance(const DevTopo& Tp, const DevInst& I, const JobParams& P, int g,
+                                unsigned char* smem_raw, LuShared& sh) {
+  int &s_a = sh.a, &s_live = sh.live, &s_trev = sh.trev, &s_sing = sh.sing;
+  double &s_gmin = sh.gmin, &s_hsub = sh.hsub;
   const int n = Tp.n, tid = threadIdx.x;
-  int g = blockIdx.x;
-  if (I.live_in) {
-    if ((int)blockIdx.x >= *I.live_in_count) return;
-    g = I.live_in[blockIdx.x];
-  }
   const size_t ld = I.ld;
   T* Y = reinterpret_cast<T*>(smem_raw);
   T* A = gA ? reinterpret_cast<T*>(I.lu_ws) + (size_t)g * Tp.nd_S : Y + Tp.nd_SY;
@@ -1989,16 +2003,28 @@ __global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, J
     if (tid == 0) s_sing = ok ? 0 : 1;
   }
   __syncthreads();
+}
 
+template <typename T, bool gA, bool packed>
+__global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, JobParams P, int* active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ LuShared sh;
+  int g = blockIdx.x;
+  if (I.live_in) {
+    if ((int)blockIdx.x >= *I.live_in_count) return;
+    g = I.live_in[blockIdx.x];
+  }
+  lu_big_instance<T, gA, packed>(Tp, I, P, g, smem_raw, sh);
+  if (!sh.live) return;
   // rescue hand-off, next evaluation point, bookkeeping
-  if (tid == 0) {
-    const int sing = s_sing;
-    if (instance_finish(Tp, I, P, g, a, sing, gmin)) {
+  if (threadIdx.x == 0) {
+    const int a = sh.a, sing = sh.sing;
+    if (instance_finish(Tp, I, P, g, a, sing, sh.gmin)) {
       atomicAdd(active, 1);
       if (I.live_out) I.live_out[atomicAdd(I.live_out_count, 1)] = g;
     }
     if (I.counters) {
-      atomicAdd(&I.counters[s_trev ? 1 : 0], 1ull);
+      atomicAdd(&I.counters[sh.trev ? 1 : 0], 1ull);
       if ((a & ACT_SOLVE) && !sing) atomicAdd(&I.counters[2], 1ull);
     }
   }
@@ -2506,44 +2532,42 @@ __device__ __forceinline__ bool rescue_pp(const RescueTab& tb, const RescueWarp&
 // CTA, warp w of CTA b owning workspace slot b * warps + w (U and the global
 // row buffers, 2 n^2 doubles). Shared memory: pivot records (when the
 // static-pivot program has them), slot tables, then the warps' areas.
-template <typename TJ>
-__global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams P, int K) {
-  extern __shared__ __align__(16) double rs[];
+// Stages the rescue's shared tables (the pivot records when the problem has
+// them, the slot tables) at base, by the whole CTA; returns the first byte
+// after them. The caller synchronises before using them.
+__device__ unsigned char* rescue_setup(const DevTopo& Tp, unsigned char* base, int4*& rec,
+                                       RescueTab& tb) {
   const int n = Tp.n, nv = Tp.nv;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
-  const int total = *I.rescue_count;
-  if ((int)blockIdx.x >= total) return;  // item e runs on CTA e % grid: one solve per SM first
-  unsigned char* base = reinterpret_cast<unsigned char*>(rs);
-  int4* rec = nullptr;
+  rec = nullptr;
   if (Tp.lu_rec) {
     rec = reinterpret_cast<int4*>(base);
     stage_pivots(Tp, rec, 1);
     base += rescue_rec_bytes(n);
   }
-  RescueTab tb;
-  {
-    int2* cent = reinterpret_cast<int2*>(base);
-    int* cptr = reinterpret_cast<int*>(cent + nv);
-    int* sptr = cptr + n + 1;
-    int* scol = sptr + n + 1;
-    for (int e = threadIdx.x; e < nv; e += blockDim.x) {
-      cent[e] = __ldg(&Tp.csc_ent[e]);
-      scol[e] = __ldg(&Tp.slot_rc[e]).y;
-    }
-    for (int e = threadIdx.x; e <= n; e += blockDim.x) {
-      cptr[e] = __ldg(&Tp.csc_ptr[e]);
-      sptr[e] = __ldg(&Tp.slot_ptr[e]);
-    }
-    tb.cent = cent;
-    tb.cptr = cptr;
-    tb.sptr = sptr;
-    tb.scol = scol;
-    base += rescue_tab_bytes(n, nv);
+  int2* cent = reinterpret_cast<int2*>(base);
+  int* cptr = reinterpret_cast<int*>(cent + nv);
+  int* sptr = cptr + n + 1;
+  int* scol = sptr + n + 1;
+  for (int e = threadIdx.x; e < nv; e += blockDim.x) {
+    cent[e] = __ldg(&Tp.csc_ent[e]);
+    scol[e] = __ldg(&Tp.slot_rc[e]).y;
   }
-  __syncthreads();
-  const int slot = blockIdx.x * W + warp;
-  if (slot >= I.rescue_slots) return;
-  base += (size_t)warp * rescue_warp_bytes(n, nv, K);
+  for (int e = threadIdx.x; e <= n; e += blockDim.x) {
+    cptr[e] = __ldg(&Tp.csc_ptr[e]);
+    sptr[e] = __ldg(&Tp.slot_ptr[e]);
+  }
+  tb.cent = cent;
+  tb.cptr = cptr;
+  tb.sptr = sptr;
+  tb.scol = scol;
+  return base + rescue_tab_bytes(n, nv);
+}
+
+// The rescue warp's buffers at base (shared memory, rescue_warp_bytes) and
+// workspace slot `slot` of I.rescue_ws.
+__device__ RescueWarp rescue_warp(const DevTopo& Tp, const DevInst& I, unsigned char* base, int K,
+                                  int slot) {
+  const int n = Tp.n, nv = Tp.nv;
   RescueWarp w;
   w.vs = reinterpret_cast<double*>(base);
   w.bp = w.vs + nv;
@@ -2558,60 +2582,156 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
   w.K = K;
   w.U = I.rescue_ws + (size_t)slot * 2 * n * n;
   w.G = w.U + (size_t)n * n;
+  return w;
+}
+
+// Rescue of instance g's failed linear solve (action bits act, gmin) by one
+// warp: FP64 static pivots first (mixed precision), then the LU with partial
+// pivoting. On success x = v + dx (sanitised and junction-limited for DC NR
+// iterations) and the instance's rescue count grows; otherwise the
+// singular-matrix branch of the control flow runs.
+template <typename TJ>
+__device__ void rescue_item(const DevTopo& Tp, const DevInst& I, const JobParams& P,
+                            const RescueTab& tb, const RescueWarp& w, const int4* rec, int g,
+                            int act, double gmin, int lane) {
+  const int n = Tp.n, nv = Tp.nv;
   const size_t ld = I.ld;
   const TJ* J = reinterpret_cast<const TJ*>(I.J);
-  for (int e = warp * gridDim.x + blockIdx.x; e < total; e += gridDim.x * W) {
-    const RescueItem item = I.rescue_list[e];
-    const int g = item.inst;
-    const double gmin = item.gmin;
-    auto stage = [&]() {
+  auto stage = [&]() {
 #pragma unroll 4
-      for (int s = lane; s < nv; s += 32) w.vs[s] = (double)J[(size_t)s * ld + g];
+    for (int s = lane; s < nv; s += 32) w.vs[s] = (double)J[(size_t)s * ld + g];
 #pragma unroll 4
-      for (int i = lane; i < n; i += 32) {
-        const size_t o = (size_t)i * ld + g;
-        w.bp[i] = -(I.F[o] + gmin * I.v[o]);
-      }
-      __syncwarp();
-      for (int i = lane; i < n; i += 32) w.vs[__ldg(&Tp.lu_hdr[i]).w] += gmin;
-      __syncwarp();
-    };
-    int ok = 0;
-    const double* sol = w.bp;
-    if (P.precision == KPREC_MIXED) {
-      stage();
-      if (lane == 0) ok = lu_solve<double>(w.vs, w.bp, 1, Tp, rec, 1e-25, P.growth64) ? 1 : 0;
-      ok = __shfl_sync(kFull, ok, 0);
-      __syncwarp();
-    }
-    if (!ok) {
-      stage();
-      if (rescue_pp(tb, w, n, lane)) {
-        ok = 1;
-        sol = w.vs;
-        if (lane == 0 && I.counters) atomicAdd(&I.counters[4], 1ull);
-      }
-    }
-    if (ok) {
-      const bool sanitize = (item.act & ACT_LIMIT) != 0;
-      for (int i = lane; i < n; i += 32) {
-        const size_t o = (size_t)i * ld + g;
-        double xi = I.v[o] + sol[i];
-        if (sanitize && !isfinite(xi)) xi = 0.0;
-        I.x[o] = xi;
-      }
-      __syncwarp();
-      if (lane == 0) {
-        if (sanitize)
-          for (int d = 0; d < Tp.n_dio; ++d) limit_one(Tp, d, I.x, I.v, ld, g);
-        I.st[g].rescued += 1;
-        if (I.counters) atomicAdd(&I.counters[3], 1ull);
-      }
-    } else if (lane == 0) {
-      on_singular(Tp, I, g);
-      set_eval_point(I, P, g, I.st[g]);
+    for (int i = lane; i < n; i += 32) {
+      const size_t o = (size_t)i * ld + g;
+      w.bp[i] = -(I.F[o] + gmin * I.v[o]);
     }
     __syncwarp();
+    for (int i = lane; i < n; i += 32) w.vs[__ldg(&Tp.lu_hdr[i]).w] += gmin;
+    __syncwarp();
+  };
+  int ok = 0;
+  const double* sol = w.bp;
+  if (P.precision == KPREC_MIXED) {
+    stage();
+    if (lane == 0) ok = lu_solve<double>(w.vs, w.bp, 1, Tp, rec, 1e-25, P.growth64) ? 1 : 0;
+    ok = __shfl_sync(kFull, ok, 0);
+    __syncwarp();
+  }
+  if (!ok) {
+    stage();
+    if (rescue_pp(tb, w, n, lane)) {
+      ok = 1;
+      sol = w.vs;
+      if (lane == 0 && I.counters) atomicAdd(&I.counters[4], 1ull);
+    }
+  }
+  if (ok) {
+    const bool sanitize = (act & ACT_LIMIT) != 0;
+    for (int i = lane; i < n; i += 32) {
+      const size_t o = (size_t)i * ld + g;
+      double xi = I.v[o] + sol[i];
+      if (sanitize && !isfinite(xi)) xi = 0.0;
+      I.x[o] = xi;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      if (sanitize)
+        for (int d = 0; d < Tp.n_dio; ++d) limit_one(Tp, d, I.x, I.v, ld, g);
+      I.st[g].rescued += 1;
+      if (I.counters) atomicAdd(&I.counters[3], 1ull);
+    }
+  } else if (lane == 0) {
+    on_singular(Tp, I, g);
+    set_eval_point(I, P, g, I.st[g]);
+  }
+  __syncwarp();
+}
+
+template <typename TJ>
+__global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams P, int K) {
+  extern __shared__ __align__(16) double rs[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const int total = *I.rescue_count;
+  if ((int)blockIdx.x >= total) return;  // item e runs on CTA e % grid: one solve per SM first
+  int4* rec;
+  RescueTab tb;
+  unsigned char* base = rescue_setup(Tp, reinterpret_cast<unsigned char*>(rs), rec, tb);
+  __syncthreads();
+  const int slot = blockIdx.x * W + warp;
+  if (slot >= I.rescue_slots) return;
+  const RescueWarp w = rescue_warp(Tp, I, base + (size_t)warp * rescue_warp_bytes(Tp.n, Tp.nv, K), K, slot);
+  for (int e = warp * gridDim.x + blockIdx.x; e < total; e += gridDim.x * W) {
+    const RescueItem item = I.rescue_list[e];
+    rescue_item<TJ>(Tp, I, P, tb, w, rec, item.inst, item.act, item.gmin, lane);
+  }
+}
+
+// Threads of the persistent per-instance kernel.
+constexpr int kPersistThreads = 512;
+
+// Every remaining NR round of one instance per CTA, inside one launch: the
+// rounds k_es_one + k_lu_big (packed program and slots in shared memory) +
+// k_rescue would run one launch each, with the same device code, so the
+// results are theirs bit for bit. An instance whose static pivots fail is
+// rescued by the CTA's warp 0 in workspace slot blockIdx.x. The CTA stops when
+// its instance is done or after max_rounds rounds; it then adds 1 to *active
+// if the instance is still live, and raises *rounds_max to the rounds it ran.
+// Instances: I.live_in[0 .. *I.live_in_count) when listed, else 0 .. ni - 1.
+// Dynamic shared memory: the largest of the three phases' needs (they run one
+// after another).
+template <typename T>
+__global__ void __launch_bounds__(kPersistThreads) k_persist(DevTopo Tp, DevInst I, JobParams P,
+                                                             int max_rounds, int K, int* active,
+                                                             int* rounds_max) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned long long s_f[kPersistThreads / 32], s_dv[kPersistThreads / 32];
+  __shared__ int s_fl[kPersistThreads / 32];
+  __shared__ LuShared sh;
+  __shared__ int s_rescue;
+  int g = blockIdx.x;
+  if (I.live_in) {
+    if ((int)blockIdx.x >= *I.live_in_count) return;
+    g = I.live_in[blockIdx.x];
+  }
+  if (g >= I.ni) return;
+  const int tid = threadIdx.x;
+  int r = 0;
+  bool live = I.ev_heff[g] >= 0.0;
+  for (; r < max_rounds && live; ++r) {
+    es_one_instance<T>(Tp, I, P, g, reinterpret_cast<double*>(smem_raw), s_f, s_dv, s_fl);
+    __syncthreads();
+    lu_big_instance<T, false, true>(Tp, I, P, g, smem_raw, sh);
+    if (!sh.live) break;
+    const int a = sh.a, sing = (a & ACT_SOLVE) ? sh.sing : 0;
+    if (tid == 0) {
+      s_rescue = sing && I.rescue_ws != nullptr && (int)blockIdx.x < I.rescue_slots;
+      if (s_rescue)
+        set_eval_point(I, P, g, I.st[g]);  // as instance_finish does before its hand-off
+      else
+        instance_finish(Tp, I, P, g, a, sing, sh.gmin);
+      if (I.counters) {
+        atomicAdd(&I.counters[sh.trev ? 1 : 0], 1ull);
+        if ((a & ACT_SOLVE) && !sing) atomicAdd(&I.counters[2], 1ull);
+      }
+    }
+    __syncthreads();
+    if (s_rescue) {
+      int4* rec;
+      RescueTab tb;
+      unsigned char* base = rescue_setup(Tp, smem_raw, rec, tb);
+      __syncthreads();
+      if (tid < 32) {
+        const RescueWarp w = rescue_warp(Tp, I, base, K, blockIdx.x);
+        rescue_item<T>(Tp, I, P, tb, w, rec, g, a, sh.gmin, tid);
+      }
+      __syncthreads();
+    }
+    live = I.ev_heff[g] >= 0.0;
+    __syncthreads();  // every thread has read the next evaluation point
+  }
+  if (tid == 0) {
+    if (I.st[g].mode != MODE_DONE) atomicAdd(active, 1);
+    atomicMax(rounds_max, r);
   }
 }
 

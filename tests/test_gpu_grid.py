@@ -19,7 +19,7 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 pytestmark = pytest.mark.gpu
 
 POLISH = dict(polish_max=8)
-KIND = {1: 1, -1: 2, -2: 3, -3: 4}  # schedule option -> karam_timing.level_schedule
+KIND = {1: 1, -1: 2, -2: 3, -3: 4, -4: 5}  # schedule option -> karam_timing.level_schedule
 
 
 def scaled_err(v, v_ref, rel=1e-9, abs_=1e-12):
@@ -64,7 +64,7 @@ def test_grid24_dc_mc_batch(product, ctx, port, schedule):
     ni = 3
     inst = circuits.mc_instances(nl, ni)
     prob, v, st = solve(product, ctx, nl, inst, ni, A.PREC_MIXED, schedule)
-    assert prob.timing()["level_schedule"] in (2, 3)
+    assert prob.timing()["level_schedule"] in (2, 3, 5)
     for i in range(ni):
         v_ref, st_ref = port.solve_dc(nl, inst, i, linear_solver=1, **POLISH)
         assert st_ref["converged"] == 1 and st[i]["status"] == A.ST_CONVERGED
@@ -100,7 +100,7 @@ def test_tuned_schedule_is_used_and_feasible(product, ctx):
     prob.set_instances(inst)
     opts = product.options(precision=A.PREC_MIXED, **POLISH)
     sch, ms = prob.tune_schedule(opts, rounds=8)
-    assert ms > 0 and (sch in (-1, -2, -3) or 1 <= sch <= 32)
+    assert ms > 0 and (sch in (-1, -2, -3, -4) or 1 <= sch <= 32)
     v_tuned, st_tuned = prob.solve_dc(opts)  # opts.schedule == 0: the tuned choice
     kind_tuned = prob.timing()["level_schedule"]
     v_explicit, st_explicit = prob.solve_dc(product.options(precision=A.PREC_MIXED,
