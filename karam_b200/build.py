@@ -14,8 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libkaram_b200.so")
-SOURCES = ["kernels.cu", "topology.cpp", "abi.cpp", "noalloc.cu", "seeder.cu", "spice.cpp"]
-HEADERS = ["device.hpp", "topology.hpp", "nr_types.h", "nr_device.cuh", "noalloc.hpp", "seeder.hpp"]
+SOURCES = ["kernels.cu", "topology.cpp", "abi.cpp", "noalloc.cu", "seeder.cu", "tc_gemm.cu", "spice.cpp"]
+HEADERS = ["device.hpp", "topology.hpp", "nr_types.h", "nr_device.cuh", "noalloc.hpp", "seeder.hpp",
+           "tc_gemm.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,16 +1,15 @@
 // seeder.cu -- training and inference kernels of the learned NR seeder (see
-// seeder.hpp). The GEMMs run on the tensor cores through WMMA with BF16
-// operands and FP32 accumulation; the network is small (config 2: 1026 -> 512
-// -> 512 -> 512 -> 322, 1.2 M weights), so a batch of 4096 instances costs a
-// few GFLOP and the kernels are written for clarity: 64 x 64 output tiles,
-// one warp per 32 x 32 quarter, K staged 32 at a time through shared memory
-// with the conversion to BF16 (and any transposition) done while staging.
+// seeder.hpp). The GEMMs run on the tcgen05 tensor cores (tc_gemm.cu) with
+// BF16 operands staged by TMA and FP32 accumulation in tensor memory; each
+// operand is first converted to a K-major BF16 copy, transposed where the
+// product needs it. The network is small (config 2: 1026 -> 512 -> 512 ->
+// 512 -> 322, 1.2 M weights), so a batch of 4096 instances costs a few GFLOP.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
-#include <mma.h>
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <stdexcept>
@@ -19,95 +18,14 @@
 
 #include "nr_types.h"
 #include "seeder.hpp"
+#include "tc_gemm.hpp"
 
 namespace karam {
 
 namespace {
 
-using namespace nvcuda;
-
-constexpr int kTM = 64, kTN = 64, kTK = 32;
-
 void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-// C[M][N] (+)= op(A)[M][K] op(B)[K][N]; 128 threads, a 64 x 64 tile per CTA.
-__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const float* __restrict__ A,
-                                              int lda, int tA, const float* __restrict__ B,
-                                              int ldb, int tB, float* __restrict__ C, int ldc,
-                                              int acc) {
-  __shared__ __align__(32) __nv_bfloat16 As[kTM][kTK + 8];
-  __shared__ __align__(32) __nv_bfloat16 Bs[kTK][kTN + 8];
-  __shared__ __align__(32) float Cs[kTM][kTN + 4];
-  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
-  const int warp = threadIdx.x >> 5;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> c[2][2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 2; ++j) wmma::fill_fragment(c[i][j], 0.0f);
-  for (int k0 = 0; k0 < K; k0 += kTK) {
-    // stage op(A) and op(B) with the contiguous index running across threads
-    for (int e = threadIdx.x; e < kTM * kTK; e += blockDim.x) {
-      int r, kk;
-      if (tA) {
-        kk = e / kTM;
-        r = e - kk * kTM;
-      } else {
-        r = e / kTK;
-        kk = e - r * kTK;
-      }
-      const int m = m0 + r, k = k0 + kk;
-      float v = 0.0f;
-      if (m < M && k < K) v = tA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
-      As[r][kk] = __float2bfloat16_rn(v);
-    }
-    for (int e = threadIdx.x; e < kTK * kTN; e += blockDim.x) {
-      int kk, cc;
-      if (tB) {
-        cc = e / kTK;
-        kk = e - cc * kTK;
-      } else {
-        kk = e / kTN;
-        cc = e - kk * kTN;
-      }
-      const int k = k0 + kk, n = n0 + cc;
-      float v = 0.0f;
-      if (k < K && n < N) v = tB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n];
-      Bs[kk][cc] = __float2bfloat16_rn(v);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kTK; kk += 16) {
-      wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a[2];
-      wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b[2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) wmma::load_matrix_sync(a[i], &As[wm + 16 * i][kk], kTK + 8);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) wmma::load_matrix_sync(b[j], &Bs[kk][wn + 16 * j], kTN + 8);
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) wmma::mma_sync(c[i][j], a[i], b[j], c[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-      wmma::store_matrix_sync(&Cs[wm + 16 * i][wn + 16 * j], c[i][j], kTN + 4, wmma::mem_row_major);
-  __syncthreads();
-  for (int e = threadIdx.x; e < kTM * kTN; e += blockDim.x) {
-    const int r = e / kTN, cc = e - r * kTN;
-    const int m = m0 + r, n = n0 + cc;
-    if (m < M && n < N) {
-      float* p = C + (size_t)m * ldc + n;
-      *p = acc ? *p + Cs[r][cc] : Cs[r][cc];
-    }
-  }
 }
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678f)); }
@@ -241,6 +159,37 @@ struct Buf {
   }
 };
 
+// BF16 copies of a GEMM's operands and its kernel's error flag.
+struct GemmWs {
+  __nv_bfloat16* a = nullptr;
+  __nv_bfloat16* b = nullptr;
+  size_t na = 0, nb = 0;
+  int* err = nullptr;
+  void need(size_t ea, size_t eb) {
+    if (ea > na) {
+      if (a) cudaFree(a);
+      a = nullptr;
+      ck(cudaMalloc(&a, ea * sizeof(__nv_bfloat16)), "seeder gemm workspace");
+      na = ea;
+    }
+    if (eb > nb) {
+      if (b) cudaFree(b);
+      b = nullptr;
+      ck(cudaMalloc(&b, eb * sizeof(__nv_bfloat16)), "seeder gemm workspace");
+      nb = eb;
+    }
+    if (!err) {
+      ck(cudaMalloc(&err, sizeof(int)), "seeder gemm flag");
+      ck(cudaMemset(err, 0, sizeof(int)), "seeder gemm flag");
+    }
+  }
+  ~GemmWs() {
+    if (a) cudaFree(a);
+    if (b) cudaFree(b);
+    if (err) cudaFree(err);
+  }
+};
+
 }  // namespace
 
 struct Mlp {
@@ -257,6 +206,7 @@ struct Mlp {
   int* idx = nullptr;
   int idx_cap = 0;
   long step = 0;
+  GemmWs ws;
   ~Mlp() {
     if (idx) cudaFree(idx);
   }
@@ -277,11 +227,29 @@ void ensure_batch(Mlp* m, int B) {
   m->bcap = B;
 }
 
+// C[M][N] (+)= op(A)[M][K] op(B)[K][N] for FP32 matrices: both operands
+// become K-major BF16 copies (A as [M][K], B as [N][K]; rows padded to a
+// multiple of 8 values for the TMA strides), then the tcgen05 GEMM.
 void gemm(int M, int N, int K, const float* A, int lda, int tA, const float* B, int ldb, int tB,
-          float* C, int ldc, int acc, cudaStream_t s) {
+          float* C, int ldc, int acc, GemmWs& ws, cudaStream_t s) {
   if (M <= 0 || N <= 0) return;
-  const dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM);
-  k_gemm<<<grid, 128, 0, s>>>(M, N, K, A, lda, tA, B, ldb, tB, C, ldc, acc);
+  const int kp = (K + 7) & ~7;
+  ws.need((size_t)M * kp, (size_t)N * kp);
+  to_bf16(A, lda, tA, M, K, ws.a, kp, s);       // A[m][k] = op(A)
+  to_bf16(B, ldb, tB ? 0 : 1, N, K, ws.b, kp, s);  // B[n][k] = op(B)[k][n]
+  ck(tc_gemm_bf16(M, N, K, ws.a, kp, ws.b, kp, C, ldc, acc, ws.err, s), "tcgen05 gemm launch");
+}
+
+// Synchronises s and reports a GEMM whose bounded waits gave up.
+void check_gemm(GemmWs& ws, cudaStream_t s) {
+  if (!ws.err) return;
+  int e = 0;
+  ck(cudaMemcpyAsync(&e, ws.err, sizeof(int), cudaMemcpyDeviceToHost, s), "gemm flag");
+  ck(cudaStreamSynchronize(s), "gemm sync");
+  if (e) {
+    cudaMemsetAsync(ws.err, 0, sizeof(int), s);
+    throw std::runtime_error("seeder GEMM: a bounded wait of the tensor-core kernel gave up");
+  }
 }
 
 // Forward pass of B rows whose normalised inputs are in act[0]; the output
@@ -289,7 +257,7 @@ void gemm(int M, int N, int K, const float* A, int lda, int tA, const float* B, 
 void forward(Mlp* m, int B, cudaStream_t s) {
   for (int l = 1; l <= m->L; ++l) {
     const int K = m->dims[l - 1], N = m->dims[l];
-    gemm(B, N, K, m->act[l - 1].p, K, 0, m->W[l - 1].p, N, 0, m->pre[l].p, N, 0, s);
+    gemm(B, N, K, m->act[l - 1].p, K, 0, m->W[l - 1].p, N, 0, m->pre[l].p, N, 0, m->ws, s);
     const size_t e = (size_t)B * N;
     k_bias_act<<<grid_for(e), 256, 0, s>>>(m->pre[l].p, m->b[l - 1].p,
                                            l < m->L ? m->act[l].p : nullptr, B, N);
@@ -407,10 +375,10 @@ float mlp_train(Mlp* m, int epochs, int batch, float lr, uint64_t shuffle_seed, 
       k_mse<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[m->L].p, m->tgt.p, gc, B, no, m->loss.p);
       for (int l = m->L; l >= 1; --l) {
         const int K = m->dims[l - 1], N = m->dims[l];
-        gemm(K, N, B, m->act[l - 1].p, K, 1, gc, N, 0, m->gW[l - 1].p, N, 0, s);
+        gemm(K, N, B, m->act[l - 1].p, K, 1, gc, N, 0, m->gW[l - 1].p, N, 0, m->ws, s);
         k_colsum<<<(N + 127) / 128, 128, 0, s>>>(gc, B, N, m->gb[l - 1].p);
         if (l > 1) {
-          gemm(B, K, N, gc, N, 0, m->W[l - 1].p, N, 1, gn, K, 0, s);
+          gemm(B, K, N, gc, N, 0, m->W[l - 1].p, N, 1, gn, K, 0, m->ws, s);
           k_gelu_bwd<<<grid_for((size_t)B * K), 256, 0, s>>>(gn, m->pre[l - 1].p, B, K);
           std::swap(gc, gn);
         }
@@ -431,6 +399,7 @@ float mlp_train(Mlp* m, int epochs, int batch, float lr, uint64_t shuffle_seed, 
     }
   }
   ck(cudaGetLastError(), "seeder train launch");
+  check_gemm(m->ws, s);
   return last;
 }
 
@@ -452,8 +421,12 @@ void mlp_predict(Mlp* m, const float* dX, int n, double* out, int out_ld, cudaSt
 
 void mlp_gemm(int M, int N, int K, const float* A, int lda, int transA, const float* B, int ldb,
               int transB, float* C, int ldc, int accumulate, cudaStream_t s) {
-  gemm(M, N, K, A, lda, transA, B, ldb, transB, C, ldc, accumulate, s);
+  static std::mutex mu;
+  static GemmWs* ws = new GemmWs;  // kept for the process: the standalone entry point's workspace
+  std::lock_guard<std::mutex> lock(mu);
+  gemm(M, N, K, A, lda, transA, B, ldb, transB, C, ldc, accumulate, *ws, s);
   ck(cudaGetLastError(), "gemm launch");
+  check_gemm(*ws, s);
 }
 
 }  // namespace karam

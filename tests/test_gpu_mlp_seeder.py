@@ -26,11 +26,15 @@ def bf16(x):
     return u.astype(np.uint32).view(np.float32)
 
 
+@pytest.mark.parametrize("shape", [(67, 45, 130), (300, 260, 1030), (4, 512, 8)])
 @pytest.mark.parametrize("ta", [False, True])
 @pytest.mark.parametrize("tb", [False, True])
-def test_bf16_gemm_matches_reference(product, ctx, ta, tb):
+def test_bf16_gemm_matches_reference(product, ctx, ta, tb, shape):
+    """The tcgen05 GEMM (TMA-staged BF16 operands, FP32 accumulation in tensor
+    memory): several output tiles, K blocks beyond the ring of stages, ragged
+    edges in M, N and K, every operand orientation."""
     rng = np.random.default_rng(11)
-    M, N, K = 67, 45, 130
+    M, N, K = shape
     a = rng.standard_normal((K, M) if ta else (M, K)).astype(np.float32)
     b = rng.standard_normal((N, K) if tb else (K, N)).astype(np.float32)
     c = product.bf16_gemm(a, b, trans_a=ta, trans_b=tb)
