@@ -50,6 +50,7 @@ SEEDER_EPOCHS = 30
 MAX_HALVINGS = 6
 METRIC = "solves/sec at <=1e-9 rel err: seeded mixed-precision vs plain FP64 NR, 1xB200"
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
 
 
 def parse():
@@ -82,6 +83,8 @@ def parse():
 class Dist:
     def __init__(self, want_gpus):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        if self.world > 1 and want_gpus not in (1, self.world):
+            raise SystemExit(f"--gpus {want_gpus} under a launcher of {self.world} ranks")
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
@@ -176,13 +179,15 @@ class Clocks:
                 "reasons": sorted(reasons)}
 
 
-def measured_peaks():
+def measured_peaks(kind="hbm"):
+    """(peak, "measured" | "fallback"): the HBM copy bandwidth in GB/s, or with
+    kind="bf16" the burst cuBLAS BF16 GEMM rate in TFLOP/s."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
             d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
+        return float(d["bf16_tflops" if kind == "bf16" else "hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
-        return FALLBACK_HBM_GBS, "fallback"
+        return (FALLBACK_BF16_TFLOPS if kind == "bf16" else FALLBACK_HBM_GBS), "fallback"
 
 
 def profiled_traffic(kernel):
@@ -545,9 +550,12 @@ def run_karam(args, dist):
     if dist.rank == 0 and dist.world == 1 and not args.no_configs:
         line["config1"] = config1_latency(ctx)
         line["config5"] = config5_seeder(ctx)
+        # the 32-stage family of the same method (130 features), a smaller training set
+        line["config5_32stage"] = config5_seeder(ctx, n_train=40960, n_test=8192, stages=32)
         line["config3"] = config3_uneven(dist.local, steps=args.config3_steps)
     if dist.rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64)
+        line["outcomes"] = outcome_check(nl, inst, st_mixed, st_fp64)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         count = args.cpu_sample or threads * 2
@@ -624,7 +632,7 @@ def config1_latency(ctx, reps=50):
 CONFIG3_FIRST = 6_000_000  # Monte-Carlo ids of the uneven batch's load parameters
 
 
-def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample=2):
+def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sizes=(8, 9, 16)):
     """Uneven batch: n_instances N x N resistor grids with N ~ U{8..64}
     (circuits.config3_sizes), each a DC point then `steps` trapezoidal steps.
 
@@ -717,19 +725,34 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample
     if kind == "port":
         pyoracle.build("port")
     worst, cpu_t, cpu_solves, sample = 0.0, 0.0, 0, []
+    by_size = {}
     with native_stdout_to_stderr():
         orc = pyoracle.Oracle(kind)
-        for N, ids, nl, inst, ctx, prob in probs[:oracle_sample]:
-            vm, sm = res["mixed"]["_out"][N]
+        # one instance of each sampled size over the whole transient, the sizes
+        # side by side on host threads (the oracle releases the interpreter)
+        chosen = [g for g in probs if g[0] in oracle_sizes]
+        outs = {}
+
+        def one(g):
+            N, ids, nl, inst, ctx, prob = g
             t = time.perf_counter()
-            v_ref, st = orc.run_batch(nl, inst, 0, 1, dt=dt, n_steps=steps, method=A.TRAN_TRAP,
-                                      n_threads=1, linear_solver=pyoracle.LS_SPARSE,
-                                      max_halvings=MAX_HALVINGS, polish_max=8)
-            cpu_t += time.perf_counter() - t
+            outs[N] = orc.run_batch(nl, inst, 0, 1, dt=dt, n_steps=steps, method=A.TRAN_TRAP,
+                                    n_threads=1, linear_solver=pyoracle.LS_SPARSE,
+                                    max_halvings=MAX_HALVINGS, polish_max=8) + (time.perf_counter() - t,)
+        threads = [threading.Thread(target=one, args=(g,)) for g in chosen]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        for N, ids, nl, inst, ctx, prob in chosen:
+            v_ref, st, secs = outs[N]
+            vm, sm = res["mixed"]["_out"][N]
+            cpu_t += secs
             if st[0]["converged"] and sm[0]["status"] == A.ST_CONVERGED:
                 cpu_solves += steps + 1
-                worst = max(worst, float(np.max(np.abs(vm[0] - v_ref[0]) /
-                                                (1e-9 * np.abs(v_ref[0]) + 1e-12))))
+                e = float(np.max(np.abs(vm[0] - v_ref[0]) / (1e-9 * np.abs(v_ref[0]) + 1e-12)))
+                worst = max(worst, e)
+                by_size[N] = e
             sample.append(f"N={N} (n={prob.n})")
     for r in res.values():
         r.pop("_out")
@@ -742,25 +765,67 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sample
         "speedup_mixed_vs_fp64": res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"],
         "max_scaled_diff_mixed_vs_fp64": max(both) if both else None,
         "max_scaled_err_vs_oracle": worst,
+        "scaled_err_vs_oracle_by_size": by_size,
+        "fixture_check": grid_fixture_check(device),
         "scaled": "|dv| / (1e-9 |v| + 1e-12 V)",
         "cpu_baseline": {"value": cpu_solves / cpu_t if cpu_t else None, "unit": "solves/s",
                          "cores": 1, "kind": "reference" if kind == "ref" else "port",
-                         "sample": "one instance of each of the smallest sizes, " + ", ".join(sample)
-                                   + f", full transient, {cpu_t:.1f} s"},
+                         "sample": "one instance of each of the sizes " + ", ".join(sample)
+                                   + f", full transient, {cpu_t:.1f} s of CPU time (one thread each)"},
     }
 
 
-def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10):
-    """Config 5: the learned seeder on the inverter-chain family (256 stages,
-    VIN 0.9 V) with VDD ~ U(1.2, 2.0) and the MC device variation: trained on
-    plain-NR DC solutions of n_train instances, evaluated on n_test held-out
-    instances against a plain start (reference seed + GMIN stepping): NR
-    iterations, solves/s and the fallback rate. VDD draws: numpy PCG64 seeded
-    by the batch's first instance id."""
+def grid_fixture_check(device):
+    """The larger grids of the family (16 x 16, 32 x 32, 64 x 64) against the
+    fixtures generated from the reference-built library (tests/golden/gridN.npz:
+    DC of two Monte-Carlo instances, then 20 trapezoidal steps of 40 ps over
+    the gate ramp for instance 0), mixed precision on the default schedule:
+    max |dv| / (1e-9 |v| + 1e-12 V) of the DC points, the final point and the
+    recorded waveform."""
     import karam_b200 as K
     from karam_b200 import _abi as A
     from karam_b200 import circuits
-    nl = circuits.inverter_chain(stages=256, vdd=1.8, vin=0.9)
+    out = {}
+    ctx = K.Context(device)
+    for N in (16, 32, 64):
+        path = os.path.join(ROOT, "tests", "golden", f"grid{N}.npz")
+        if not os.path.exists(path):
+            continue
+        g = np.load(path)
+        nl = circuits.grid_circuit(N)
+        prob = K.Problem(ctx, nl, max_instances=2)
+        prob.set_instances(circuits.Instances(2, g["mc_kp"], g["mc_vto"]))
+        opts = K.options(precision=A.PREC_MIXED, max_halvings=6, **POLISH)
+        v, st = prob.solve_dc(opts)
+        sc = lambda a, b: float(np.max(np.abs(a - b) / (1e-9 * np.abs(b) + 1e-12)))
+        dc = max(sc(v[i], g["dc_v"][i]) for i in range(2))
+        nodes = [int(x) for x in g["tran_wave_nodes"]]
+        vt, stt, wave = prob.step_transient(40e-12, 20, A.TRAN_TRAP, opts, wave_nodes=nodes)
+        out[f"N={N}"] = {"n": prob.n, "dc": dc, "final": sc(vt[0], g["tran_v"]),
+                         "wave_max_abs_v": float(np.max(np.abs(wave[0] - g["tran_wave"]))),
+                         "converged": bool(st[0]["status"] == A.ST_CONVERGED and
+                                           stt[0]["status"] == A.ST_CONVERGED)}
+        prob.close()
+    ctx.close()
+    return out
+
+
+def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10, stages=256,
+                   oracle_sample=16):
+    """Config 5: the learned seeder on the inverter-chain family (`stages`
+    stages, VIN 0.9 V) with VDD ~ U(1.2, 2.0) and the MC device variation:
+    trained on plain-NR DC solutions of n_train instances, evaluated on n_test
+    held-out instances against a plain start (reference seed + GMIN stepping):
+    NR iterations, solves/s and the fallback rate; the inference's tcgen05
+    GEMM throughput inside the timed jobs; and, on oracle_sample instances the
+    plain GPU NR failed and as many it converged, whether the reference-built
+    oracle (FP64, sparse LU) reaches the same outcome. VDD draws: numpy PCG64
+    seeded by the batch's first instance id."""
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+    from karam_b200 import circuits
+    from oracle import pyoracle
+    nl = circuits.inverter_chain(stages=stages, vdd=1.8, vin=0.9)
 
     def instances(first, n):
         inst = circuits.mc_instances(nl, n, first_instance=first)
@@ -786,13 +851,19 @@ def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10):
     fallbacks = 0
     err = []
     diff = 0.0
+    seed_ms = 0.0
+    failed, passed = [], []  # (batch first id, index) of plain-NR outcomes, for the oracle check
     for b in range(n_test // batch):
-        prob.set_instances(instances(3_000_000 + b * batch, batch))
+        first = 3_000_000 + b * batch
+        prob.set_instances(instances(first, batch))
         v0, st0 = prob.solve_dc(plain)
         res["plain"]["ms"] += prob.timing()["job_ms"]
+        failed += [(first, i) for i, s in enumerate(st0) if s["status"] != A.ST_CONVERGED]
+        passed += [(first, i) for i, s in enumerate(st0) if s["status"] == A.ST_CONVERGED]
         guess = seeder.predict(prob)
         v1, st1 = prob.solve_dc(seeded)
         res["seeded"]["ms"] += prob.timing()["job_ms"]
+        seed_ms += prob.timing()["seed_ms"]
         for k, st in (("plain", st0), ("seeded", st1)):
             res[k]["it"] += [s["iterations"] + s["polish_iters"] for s in st]
             res[k]["conv"] += sum(s["status"] == A.ST_CONVERGED for s in st)
@@ -805,9 +876,43 @@ def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10):
     seeder.close()
     n_out = prob.n
     prob.close()
-    out = {"workload": "256-stage inverter chain, VIN 0.9 V, VDD ~ U(1.2, 2.0) + MC VTO/KP; DC",
-           "network": f"MLP {2 * len(nl.mos) + len(nl.vsrc)}-512-512-512-{n_out} (GELU), "
+    dims = [2 * len(nl.mos) + len(nl.vsrc), 512, 512, 512, n_out]
+    flops_per_row = 2.0 * sum(a * b for a, b in zip(dims[:-1], dims[1:]))
+    peak = measured_peaks(kind="bf16")[0]
+    jobs = n_test // batch
+    inf_tflops = flops_per_row * batch / (seed_ms / jobs / 1e3) / 1e12 if seed_ms else None
+    train_tflops = 3.0 * flops_per_row * added * epochs / (t2 - t1) / 1e12
+    # the plain outcome against the reference-built oracle on a sample of the
+    # failures and of the converged instances
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    agree = {"gpu_failed": 0, "oracle_failed_too": 0, "gpu_converged": 0, "oracle_converged_too": 0}
+    pick = np.random.default_rng(5)
+    with native_stdout_to_stderr():
+        orc = pyoracle.Oracle(kind)
+        for group, key, okey in ((failed, "gpu_failed", "oracle_failed_too"),
+                                 (passed, "gpu_converged", "oracle_converged_too")):
+            if not group:
+                continue
+            sel = [group[j] for j in pick.choice(len(group), min(oracle_sample, len(group)), replace=False)]
+            for first, i in sel:
+                inst1 = instances(first, batch).slice(i, i + 1)
+                _, st = orc.run_batch(nl, inst1, 0, 1, n_threads=1, linear_solver=pyoracle.LS_SPARSE, **POLISH)
+                agree[key] += 1
+                agree[okey] += int(bool(st[0]["converged"]) == (key == "gpu_converged"))
+    out = {"workload": f"{stages}-stage inverter chain, VIN 0.9 V, VDD ~ U(1.2, 2.0) + MC VTO/KP; DC",
+           "network": f"MLP {dims[0]}-512-512-512-{n_out} (GELU), "
                       "BF16 weights, FP32 accumulation, Adam/MSE",
+           "inference": {"ms_per_batch": seed_ms / jobs if jobs else None, "batch": batch,
+                         "gflop_per_batch": flops_per_row * batch / 1e9,
+                         "tflops": inf_tflops, "frac_of_bf16_peak": inf_tflops / peak if inf_tflops else None,
+                         "peak_tflops": peak,
+                         "timed": "features + four tcgen05 GEMM layers + activations, CUDA events in the job"},
+           "training_tflops": train_tflops,
+           "plain_outcome_vs_oracle": {**agree, "oracle": kind,
+                                       "sample": f"{oracle_sample} plain-NR failures and {oracle_sample} "
+                                                 "converged instances, FP64 sparse LU"},
            "train_solutions": added, "train_data_s": t1 - t0, "train_s": t2 - t1,
            "epochs": epochs, "final_loss": loss, "heldout": n_test,
            "fallback_rate": fallbacks / n_test,
@@ -859,8 +964,75 @@ def accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64, sample=6):
             "scaled": "|dv| / (1e-9 |v| + 1e-12 V); <= 1 meets the 1e-9 relative bar"}
 
 
+def outcome_check(nl, inst, st_mixed, st_fp64, converged_sample=16):
+    """Which instances fail, and whether the reference-built oracle (FP64,
+    sparse LU, plain GMIN stepping) fails on the same ones: every instance the
+    plain FP64 GPU arm did not converge, plus as many it converged (seeded
+    draw), each run DC + the full BE transient on its own host thread."""
+    import threading
+    from karam_b200 import _abi as A
+    from oracle import pyoracle
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    fail64 = [i for i, s in enumerate(st_fp64) if s["status"] != A.ST_CONVERGED]
+    failmx = [i for i, s in enumerate(st_mixed) if s["status"] != A.ST_CONVERGED]
+    conv = [i for i, s in enumerate(st_fp64) if s["status"] == A.ST_CONVERGED]
+    pick = np.random.default_rng(3)
+    conv = sorted(pick.choice(conv, min(converged_sample, len(conv)), replace=False).tolist())
+    res = {}
+    with native_stdout_to_stderr():
+        orc = pyoracle.Oracle(kind)
+
+        def one(i):
+            _, st = orc.run_batch(nl, inst.slice(i, i + 1), 0, 1, dt=DT, n_steps=TRAN_STEPS,
+                                  n_threads=1, linear_solver=pyoracle.LS_SPARSE,
+                                  max_halvings=MAX_HALVINGS, polish_max=8)
+            res[i] = bool(st[0]["converged"])
+        ids = sorted(set(fail64) | set(failmx) | set(conv))
+        for k in range(0, len(ids), os.cpu_count() or 1):
+            threads = [threading.Thread(target=one, args=(i,)) for i in ids[k:k + (os.cpu_count() or 1)]]
+            for th in threads:
+                th.start()
+            for th in threads:
+                th.join()
+    return {"failed_fp64_arm": fail64, "failed_headline_arm": failmx,
+            "oracle_failed": [i for i in ids if not res[i]],
+            "fp64_arm_agrees_with_oracle": sum(res[i] == (st_fp64[i]["status"] == A.ST_CONVERGED)
+                                               for i in ids),
+            "checked": len(ids), "oracle": kind,
+            "sample": f"every instance either GPU arm failed plus {len(conv)} the FP64 arm converged; "
+                      "DC + full BE transient each"}
+
+
+def spawn_ranks(n):
+    """`--gpus n` outside a launcher: start n local ranks through
+    torch.distributed.run (rendezvous on 127.0.0.1) and return their exit
+    code. Refuses rather than measure fewer GPUs than asked for."""
+    import socket
+    import subprocess
+    try:
+        import torch
+        visible = torch.cuda.device_count()
+    except Exception:
+        visible = 0
+    if visible < n:
+        print(json.dumps({"metric": METRIC, "error": f"--gpus {n} needs {n} visible GPUs, "
+                          f"{visible} are visible"}), flush=True)
+        return 2
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__),
+           *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     dist = Dist(args.gpus)
     try:
         if args.impl == "reference":

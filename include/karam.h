@@ -501,6 +501,8 @@ typedef struct karam_timing {
                                live instances (once no more are live than SMs)       */
   int32_t persistent_rounds; /* rounds run inside the persistent per-instance kernel
                                (every remaining round of an instance in one launch) */
+  double seed_ms;           /* the learned seeder's inference inside the job (features,
+                               the MLP's tcgen05 GEMMs and activations), 0 without it */
 } karam_timing;
 KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 

@@ -105,7 +105,8 @@ struct karam_problem {
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
       d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws,
       i_live, i_stage, i_hist;
-  cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr;
+  cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr, ev_seed0 = nullptr, ev_seed1 = nullptr;
+  bool seed_timed = false;  // ev_seed0 / ev_seed1 bracket this job's seeder inference
   int rescue_slots = 0;
   RescuePlan rplan;
   karam_seeder* seeder = nullptr;  // KARAM_SEED_MLP (not owned)
@@ -121,6 +122,8 @@ struct karam_problem {
     if (h_active) cudaFreeHost(h_active);
     if (ev_job0) cudaEventDestroy(ev_job0);
     if (ev_job1) cudaEventDestroy(ev_job1);
+    if (ev_seed0) cudaEventDestroy(ev_seed0);
+    if (ev_seed1) cudaEventDestroy(ev_seed1);
   }
 };
 
@@ -444,6 +447,8 @@ void alloc_instances(karam_problem* p) {
   p->d_counters.alloc(5 * sizeof(unsigned long long));
   ck(cudaEventCreate(&p->ev_job0), "cudaEventCreate");
   ck(cudaEventCreate(&p->ev_job1), "cudaEventCreate");
+  ck(cudaEventCreate(&p->ev_seed0), "cudaEventCreate");
+  ck(cudaEventCreate(&p->ev_seed1), "cudaEventCreate");
   // Partial-pivoting rescue: per concurrently running rescue warp, the U
   // factor and room for rows with fill (2 n x n FP64), within a 2 GiB budget.
   p->rplan = plan_rescue(p->dt);
@@ -915,6 +920,7 @@ void read_voltages(karam_problem* p, double* out_v) {
 // first kernel of a solve call; end_job records the end event and reads back.
 void begin_job(karam_problem* p) {
   p->timing = karam_timing{};
+  p->seed_timed = false;
   ck(cudaMemsetAsync(p->d_counters.p, 0, 5 * sizeof(unsigned long long), p->ctx->stream), "memset counters");
   ck(cudaEventRecord(p->ev_job0, p->ctx->stream), "event record");
 }
@@ -927,6 +933,11 @@ void end_job(karam_problem* p) {
   float ms = 0;
   ck(cudaEventElapsedTime(&ms, p->ev_job0, p->ev_job1), "job time");
   p->timing.job_ms = ms;
+  if (p->seed_timed) {
+    float sms = 0;
+    ck(cudaEventElapsedTime(&sms, p->ev_seed0, p->ev_seed1), "seeder time");
+    p->timing.seed_ms = sms;
+  }
   p->timing.evals_dc = (int64_t)c[0];
   p->timing.evals_tran = (int64_t)c[1];
   p->timing.solves = (int64_t)c[2];
@@ -946,8 +957,11 @@ void mlp_seed(karam_problem* p) {
   const size_t bytes = (size_t)std::max(1, p->ni) * nf * sizeof(float);
   if (p->i_feat.bytes < bytes) p->i_feat.alloc(bytes);
   cudaStream_t s = p->ctx->stream;
+  ck(cudaEventRecord(p->ev_seed0, s), "event record");
   karam::seeder_features(p->dt, dev_inst(p), nullptr, p->ni, p->i_feat.as<float>(), nullptr, s);
   karam::mlp_predict(sd->m, p->i_feat.as<float>(), p->ni, p->i_seed.as<double>(), p->ld, s);
+  ck(cudaEventRecord(p->ev_seed1, s), "event record");
+  p->seed_timed = true;
   p->timing.other_launches += 1;
 }
 

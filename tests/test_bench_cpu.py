@@ -35,3 +35,18 @@ def test_reference_arm_prints_one_json_line():
     assert rec["impl"] == "reference" and rec["unit"] == "solves/s" and rec["value"] > 0
     assert rec["cpu_baseline"]["kind"] in ("reference", "port")
     assert rec["e2e"]["h2d_bytes_per_step"] == 0
+
+
+@pytest.mark.timeout(300)
+def test_multi_gpu_request_without_gpus_is_refused():
+    """`--gpus N` outside a launcher starts N ranks itself; with fewer visible
+    GPUs than asked for it refuses (exit 2, an error line) instead of
+    measuring fewer GPUs."""
+    env = dict(os.environ)
+    env.pop("WORLD_SIZE", None)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2",
+                          "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+    assert out.returncode == 2
+    rec = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][0])
+    assert "2 visible GPUs" in rec["error"]
