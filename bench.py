@@ -889,6 +889,7 @@ def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10, sta
         pyoracle.build("port")
     agree = {"gpu_failed": 0, "oracle_failed_too": 0, "gpu_converged": 0, "oracle_converged_too": 0}
     pick = np.random.default_rng(5)
+    fail_sel = []
     with native_stdout_to_stderr():
         orc = pyoracle.Oracle(kind)
         for group, key, okey in ((failed, "gpu_failed", "oracle_failed_too"),
@@ -901,6 +902,21 @@ def config5_seeder(ctx, n_train=200704, n_test=16384, batch=4096, epochs=10, sta
                 _, st = orc.run_batch(nl, inst1, 0, 1, n_threads=1, linear_solver=pyoracle.LS_SPARSE, **POLISH)
                 agree[key] += 1
                 agree[okey] += int(bool(st[0]["converged"]) == (key == "gpu_converged"))
+                if key == "gpu_failed":
+                    fail_sel.append((inst1, bool(st[0]["converged"])))
+    # the same failures of the mixed-precision plain start, solved again on the
+    # GPU in FP64: does the outcome follow the precision or the algorithm?
+    if fail_sel:
+        sub_inst = circuits.Instances(len(fail_sel), np.concatenate([x.mos_kp for x, _ in fail_sel]),
+                                      np.concatenate([x.mos_vto for x, _ in fail_sel]),
+                                      np.concatenate([x.vs_dc for x, _ in fail_sel]))
+        p64 = K.Problem(ctx, nl, max_instances=len(fail_sel))
+        p64.set_instances(sub_inst)
+        _, st64 = p64.solve_dc(K.options(precision=A.PREC_FP64, **POLISH))
+        p64.close()
+        agree["fp64_gpu_converged"] = sum(s["status"] == A.ST_CONVERGED for s in st64)
+        agree["fp64_gpu_agrees_with_oracle"] = sum((s["status"] == A.ST_CONVERGED) == oc
+                                                   for s, (_, oc) in zip(st64, fail_sel))
     out = {"workload": f"{stages}-stage inverter chain, VIN 0.9 V, VDD ~ U(1.2, 2.0) + MC VTO/KP; DC",
            "network": f"MLP {dims[0]}-512-512-512-{n_out} (GELU), "
                       "BF16 weights, FP32 accumulation, Adam/MSE",
