@@ -636,15 +636,18 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sizes=
     """Uneven batch: n_instances N x N resistor grids with N ~ U{8..64}
     (circuits.config3_sizes), each a DC point then `steps` trapezoidal steps.
 
-    One problem per grid size, each on its own context (stream); the sizes run
-    concurrently from host threads, and each size's factor/solve schedule (a
-    warp per instance, or a CTA per instance with the instance's slots in
-    shared or global memory) is measured first by karam_tune_schedule. Timed: the whole batch, wall
-    clock from the first launch to the last result, FP32 LU + FP64
-    refinement against plain FP64. Every size shares one grid (seeded by N);
-    instances vary in their loads' KP/VTO (ids from CONFIG3_FIRST). Accuracy:
-    the smallest instances against the reference-built oracle over the whole
-    transient, which also gives the reference CPU rate on that sample."""
+    One problem per grid size. Headline (mixed / fp64): every size in ONE
+    launch of the multi-problem persistent kernel (karam_run_mc_multi, one
+    CTA per instance, the largest grids first), wall clock of the call and the
+    device time of the job. For comparison (per_size_streams): each size on
+    its own context (stream) from host threads, each size's factor/solve
+    schedule measured first by karam_tune_schedule; the two must give the
+    same results (the schedules run the same elimination in the same order).
+    FP32 LU + FP64 refinement against plain FP64. Every size shares one grid
+    (seeded by N); instances vary in their loads' KP/VTO (ids from
+    CONFIG3_FIRST). Accuracy: one instance of each sampled size against the
+    reference-built oracle over the whole transient, which also gives the
+    reference CPU rate on that sample."""
     import threading
     import karam_b200 as K
     from karam_b200 import _abi as A
@@ -699,7 +702,7 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sizes=
             out[N] = (v, st)
         return wall, conv, kinds, out
 
-    res = {}
+    streams = {}
     for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
         # the measured schedule of every size (karam_tune_schedule: 16 DC
         # rounds per feasible schedule), before timing
@@ -709,9 +712,49 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sizes=
         t_tune = time.perf_counter() - t
         run(prec, 4)  # warm-up: plans, workspaces, graphs
         wall, conv, kinds, out = run(prec, steps)
+        streams[name] = {"solves_per_s": conv * (steps + 1) / wall, "wall_s": wall,
+                         "converged": conv, "schedules_by_size": kinds, "tune_s": t_tune,
+                         "_out": out}
+    # the same batch again as one launch, the per-size contexts freed first
+    for g in probs:
+        g[5].close()
+        g[4].close()
+    shared_ctx = K.Context(device)
+    multi = []
+    for N, ids, nl, inst, _, _ in probs:
+        mp = K.Problem(shared_ctx, nl, max_instances=len(ids))
+        mp.set_instances(inst)
+        multi.append(mp)
+
+    def run_one_launch(prec, n_steps):
+        opts = K.options(precision=prec, max_halvings=MAX_HALVINGS, **POLISH)
+        t = time.perf_counter()
+        K.run_mc_multi(multi, dt, n_steps, A.TRAN_TRAP, opts)
+        wall = time.perf_counter() - t
+        out, conv = {}, 0
+        for (N, *_), mp in zip(probs, multi):
+            v, st = mp.read_results()
+            conv += sum(1 for s in st if s["status"] == A.ST_CONVERGED)
+            out[N] = (v, st)
+        return wall, multi[0].timing(), conv, out
+
+    res = {}
+    for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        run_one_launch(prec, 4)  # warm-up: plans, workspaces
+        wall, tm, conv, out = run_one_launch(prec, steps)
+        same = all(np.array_equal(out[N][0], streams[name]["_out"][N][0]) and
+                   [s["status"] for s in out[N][1]] == [s["status"] for s in streams[name]["_out"][N][1]]
+                   for N in out)
         res[name] = {"solves_per_s": conv * (steps + 1) / wall, "wall_s": wall,
-                     "converged": conv, "schedules_by_size": kinds, "tune_s": t_tune,
-                     "_out": out}
+                     "device_ms": tm["job_ms"],
+                     "solves_per_s_device": conv * (steps + 1) / (tm["job_ms"] * 1e-3),
+                     "rounds_max": tm["rounds"], "converged": conv, "launches": 1,
+                     "equals_per_size_streams": bool(same), "_out": out}
+        streams[name].pop("_out")
+        res[name]["per_size_streams"] = streams[name]
+    for mp in multi:
+        mp.close()
+    shared_ctx.close()
     both = []
     for N, ids, *_ in probs:
         vm, sm = res["mixed"]["_out"][N]

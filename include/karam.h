@@ -315,6 +315,25 @@ KARAM_API int karam_run_mc(karam_problem *p, const karam_instances *inst,
  * karam_read_results copies the device results back afterwards. */
 KARAM_API int karam_run_mc_device(karam_problem *p, const karam_solver_opts *opts,
                                   double dt, int32_t n_steps, int32_t method);
+/* One launch over problems of different circuits and sizes (an uneven batch;
+ * the reference runs such jobs one after another, MonteCarloRunner::run,
+ * infrastructure/monte_carlo.h:18-127): karam_run_mc_device of every problem
+ * (same context, unseeded, same opts / dt / n_steps / method) as ONE launch of
+ * the persistent per-instance kernel, one CTA per instance of every problem
+ * (the problems with the most LU work per instance on the first CTAs), each
+ * problem on the first factor/solve layout that fits a CTA (packed level
+ * program and slots in shared memory; slots in shared memory; slots in a
+ * global workspace). Results per problem through karam_read_results; each
+ * problem's karam_timing holds the whole launch (job_ms, rounds = the most
+ * rounds any instance ran, level_schedule 5). A problem's rescues share its
+ * rescue workspace slots (a CTA takes a free one for each rescue, waiting up
+ * to about 8 s of GPU clock; a solve that finds none is singular and the call
+ * returns KARAM_E_CUDA after the job, results still readable). KARAM_E_INVALID
+ * with a message naming the problem when one does not fit (evaluation or
+ * factor data beyond a CTA's shared memory). */
+KARAM_API int karam_run_mc_multi(karam_problem *const *probs, int32_t n_probs,
+                                 const karam_solver_opts *opts, double dt, int32_t n_steps,
+                                 int32_t method);
 /* SPICE netlist front-end (SPICEParser::parse, netlist/spice_parser.cpp:148-262)
  * for the subset the engine solves: R, C, V (DC, PULSE), I (DC), D, M with
  * .MODEL NMOS / PMOS (KP, VTO, LAMBDA) and D (IS, N), .TEMP, .OP, .TRAN, .END.
@@ -503,6 +522,9 @@ typedef struct karam_timing {
                                (every remaining round of an instance in one launch) */
   double seed_ms;           /* the learned seeder's inference inside the job (features,
                                the MLP's tcgen05 GEMMs and activations), 0 without it */
+  int32_t resident_instances; /* instances whose state the persistent kernel kept in
+                               shared memory for its whole launch                   */
+  int32_t reserved_;
 } karam_timing;
 KARAM_API int karam_last_timing(const karam_problem *p, karam_timing *out);
 

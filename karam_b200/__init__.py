@@ -62,6 +62,8 @@ def lib():
                                    P(A.KaramInstanceStats)]),
         "karam_run_mc_device": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_double, C.c_int32,
                                           C.c_int32]),
+        "karam_run_mc_multi": (C.c_int, [P(vp), C.c_int32, P(A.KaramSolverOpts), C.c_double,
+                                         C.c_int32, C.c_int32]),
         "karam_tune_schedule": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_int32, P(C.c_int32),
                                           P(C.c_double)]),
         "karam_spice_parse": (C.c_int, [C.c_char_p, P(vp), C.c_char_p, C.c_int32]),
@@ -429,6 +431,18 @@ class Problem:
         t = A.KaramTiming()
         self._check(lib().karam_last_timing(self.h, C.byref(t)))
         return {k: getattr(t, k) for k, _ in A.KaramTiming._fields_}
+
+
+def run_mc_multi(problems, dt=0.0, n_steps=0, method=A.TRAN_BE, opts=None):
+    """karam_run_mc_multi: the device-resident job of every problem (one
+    context, instances already set) in one persistent launch; results per
+    problem through Problem.read_results()."""
+    opts = opts or options()
+    if not problems:
+        raise ValueError("no problems")
+    hs = (C.c_void_p * len(problems))(*[p.h for p in problems])
+    rc = lib().karam_run_mc_multi(hs, len(problems), C.byref(opts), dt, n_steps, method)
+    problems[0]._check(rc)
 
 
 class Seeder:

@@ -97,7 +97,8 @@ class KaramTiming(C.Structure):
                 ("evals_dc", C.c_int64), ("evals_tran", C.c_int64),
                 ("solves", C.c_int64), ("rescues", C.c_int64),
                 ("rescues_dense", C.c_int64), ("tail_rounds", C.c_int32),
-                ("persistent_rounds", C.c_int32), ("seed_ms", C.c_double)]
+                ("persistent_rounds", C.c_int32), ("seed_ms", C.c_double),
+                ("resident_instances", C.c_int32), ("reserved_", C.c_int32)]
 
 
 def ptr(arr, ctype):

@@ -358,6 +358,7 @@ void upload_topology(karam_problem* p) {
   d.n_hub_items = p->n_hub_items;
   d.n_ft_terms = T.ft_off.empty() ? 0 : T.ft_off.back();
   d.n_hub_slot_terms = p->n_hub_slot_terms;
+  d.n_jt_terms = T.jt_off.empty() ? 0 : T.jt_off.back();
   d.n_hub_groups = T.n_hub_groups;
   d.n_hub_rows = T.n_hub_rows;
   d.lu_hdr = p->t_lu_hdr.as<int4>();
@@ -687,26 +688,27 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
   // no more instances are live than SMs. Each CTA rescues its own failed
   // solves, so the rescue workspace must have a slot per CTA.
   const int want = want_lanes;  // after the measured choice
-  size_t psm = 0;
+  PersistPlan pplan;
   if (!timed && p->max_hub_chunks <= 8) {
-    psm = plan_persist(p->dt, prec, p->rplan, max_smem);
+    pplan = plan_persist(p->dt, prec, p->rplan, max_smem);
     cudaGetLastError();
   }
   auto persist_fits = [&](int grid) {
-    return psm > 0 && (p->rescue_slots == 0 || p->rescue_slots >= grid);
+    return pplan.smem > 0 && (p->rescue_slots == 0 || p->rescue_slots >= grid);
   };
   const int budget = max_rounds > 0 ? max_rounds : (1 << 30);
   int* active = p->d_active.as<int>();
   // all rounds of every instance in one launch
   auto run_persist = [&](const DevInst& Ip, int grid, int rounds_left, bool is_tail) {
     ck(cudaMemsetAsync(active, 0, 2 * sizeof(int), s), "memset active");
-    launch_persist(p->dt, Ip, P, prec, grid, psm, rounds_left, p->rplan.K, active, active + 1, s);
+    launch_persist(p->dt, Ip, P, prec, grid, pplan, rounds_left, p->rplan.K, active, active + 1, s);
     ck(cudaGetLastError(), "k_persist launch");
     ck(cudaMemcpyAsync(p->h_active, active, 2 * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H active");
     ck(cudaStreamSynchronize(s), "persistent sync");
     ++p->timing.other_launches;
     p->timing.rounds += p->h_active[1];
     p->timing.persistent_rounds += p->h_active[1];
+    if (pplan.resident_at > 0) p->timing.resident_instances += grid;
     if (is_tail) p->timing.tail_rounds += p->h_active[1];
   };
   if (want == -4 && !persist_fits(p->ni))
@@ -1307,6 +1309,98 @@ int karam_run_mc_device(karam_problem* p, const karam_solver_opts* opts, double 
   });
 }
 
+int karam_run_mc_multi(karam_problem* const* probs, int32_t n_probs, const karam_solver_opts* opts,
+                       double dt, int32_t n_steps, int32_t method) {
+  if (!probs || n_probs < 1) return KARAM_E_INVALID;
+  for (int j = 0; j < n_probs; ++j)
+    if (!probs[j] || probs[j]->ctx != probs[0]->ctx) return KARAM_E_INVALID;
+  karam_ctx* ctx = probs[0]->ctx;
+  return guarded(ctx, [&] {
+    for (int j = 0; j < n_probs; ++j) need_device(probs[j]);
+    const JobParams P = job_params(opts, n_steps, dt, method);
+    if (P.seeded != KARAM_SEED_NONE) throw std::runtime_error("karam_run_mc_multi runs unseeded jobs only");
+    const int prec = P.precision;
+    cudaStream_t s = ctx->stream;
+    // one table entry per problem, CTA ranges back to back, the costliest
+    // instances (most LU operations per factorisation) first: CTAs start in
+    // index order, so the longest ones do not trail the launch
+    std::vector<int> order(n_probs);
+    for (int j = 0; j < n_probs; ++j) order[j] = j;
+    auto cost = [&](int j) { return (double)probs[j]->topo.lu_ops + (double)probs[j]->topo.nnz(); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    std::vector<PersistJob> jobs(n_probs);
+    std::vector<size_t> lock_off(n_probs);
+    std::vector<char> resident(n_probs, 0);
+    size_t smem = 16, n_locks = 0;
+    int grid = 0;
+    for (int q = 0; q < n_probs; ++q) {
+      const int j = order[q];
+      karam_problem* p = probs[j];
+      const PersistPlan plan = plan_persist_job(p->dt, prec, p->rplan, ctx->max_smem);
+      cudaGetLastError();
+      if (plan.smem == 0 || p->max_hub_chunks > 8)
+        throw std::runtime_error("problem " + std::to_string(j) +
+                                 " does not fit the multi-problem persistent kernel");
+      PersistJob& J = jobs[q];
+      std::memset(&J, 0, sizeof(J));
+      J.T = p->dt;
+      J.I = dev_inst(p);
+      J.P = P;
+      J.K = p->rplan.K;
+      J.I.rescue_list = nullptr;  // no hand-off: a solve with no rescue slot is singular
+      J.cta0 = grid;
+      J.variant = plan.variant;
+      J.resident_at = plan.resident_at;
+      J.slot_values = plan.slot_values;
+      resident[j] = plan.resident_at > 0;
+      lock_off[q] = n_locks;
+      n_locks += p->rescue_slots;
+      if (plan.variant == 2) {
+        const size_t need = (size_t)p->ni * (size_t)p->dt.nd_S * sizeof(double);
+        if (p->i_luws.bytes < need) p->i_luws.alloc(need);
+        J.I.lu_ws = p->i_luws.p;
+      }
+      smem = std::max(smem, plan.smem);
+      grid += p->ni;
+    }
+    // [active, rounds_max, slot timeouts, pad, slot locks...]
+    DBuf words;
+    words.alloc((4 + n_locks) * sizeof(int));
+    int* d_words = words.as<int>();
+    for (int j = 0; j < n_probs; ++j) jobs[j].slot_lock = d_words + 4 + lock_off[j];
+    DBuf table;
+    upload(table, jobs);
+    ck(cudaMemsetAsync(d_words, 0, words.bytes, s), "memset launch words");
+    for (int j = 0; j < n_probs; ++j) begin_job(probs[j]);
+    for (int j = 0; j < n_probs; ++j) start_job(probs[j], P, nullptr);
+    if (grid > 0) {
+      const int budget = opts && opts->max_rounds > 0 ? opts->max_rounds : (1 << 30);
+      launch_persist_multi(table.as<PersistJob>(), n_probs, prec, grid, smem, budget, d_words,
+                           d_words + 1, d_words + 2, s);
+      ck(cudaGetLastError(), "k_persist_multi launch");
+    }
+    int h_words[4] = {0, 0, 0, 0};
+    ck(cudaMemcpyAsync(h_words, d_words, sizeof(h_words), cudaMemcpyDeviceToHost, s), "D2H active");
+    ck(cudaStreamSynchronize(s), "persistent sync");
+    for (int j = 0; j < n_probs; ++j) {
+      karam_problem* p = probs[j];
+      p->timing.lanes = 1;
+      p->timing.level_schedule = 5;
+      p->timing.rounds = h_words[1];
+      p->timing.persistent_rounds = h_words[1];
+      p->timing.resident_instances = resident[j] ? p->ni : 0;
+      p->timing.other_launches += j == 0 ? 1 : 0;
+      end_job(p);
+      p->have_dc = true;
+    }
+    if (h_words[2] > 0)
+      throw CudaError(std::to_string(h_words[2]) +
+                      " solves found no free rescue workspace slot in time; their instances "
+                      "report KARAM_ST_SINGULAR");
+    return KARAM_OK;
+  });
+}
+
 int karam_tune_schedule(karam_problem* p, const karam_solver_opts* opts, int32_t rounds,
                         int32_t* schedule, double* best_ms) {
   if (!p || rounds < 1) return KARAM_E_INVALID;
@@ -1334,7 +1428,7 @@ int karam_tune_schedule(karam_problem* p, const karam_solver_opts* opts, int32_t
       if (std::find(cands.begin(), cands.end(), val) == cands.end()) cands.push_back(val);
     }
     if (p->max_hub_chunks <= 8 && (p->rescue_slots == 0 || p->rescue_slots >= p->ni) &&
-        plan_persist(p->dt, prec, p->rplan, p->ctx->max_smem) > 0)
+        plan_persist(p->dt, prec, p->rplan, p->ctx->max_smem).smem > 0)
       cands.push_back(-4);
     cudaGetLastError();
     if (cands.empty()) throw std::runtime_error("no factor/solve schedule fits this problem");

@@ -69,20 +69,46 @@ RescuePlan plan_rescue(const DevTopo& T);
 int rescue_ctas_per_sm(const DevTopo& T, const RescuePlan& R);
 void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const RescuePlan& R,
                    cudaStream_t s);
-// Dynamic shared memory of the persistent per-instance kernel (k_persist) for
-// precision prec and rescue plan R, or 0 when the problem cannot use it: it
-// needs the packed level program, and its phases (evaluation + stamping of
-// one instance, the packed factor/solve, a rescue warp) must each fit one
-// CTA's shared memory. Sets the kernel's shared-memory limit (call outside
-// stream capture).
-size_t plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_smem);
+// The persistent kernels' launch plan for one problem: variant = where the
+// factor/solve keeps its data (0 packed level program and ND slots in shared
+// memory, 1 slots in shared memory, 2 slots in a global workspace of
+// ni * nd_S values; PersistJob::variant); resident_at > 0: the byte offset in
+// dynamic shared memory from which each instance's state is kept there for
+// the whole launch (resident_in), when it fits beside the phases;
+// smem = the dynamic shared memory, 0 when nothing fits.
+struct PersistPlan {
+  size_t smem = 0;
+  int variant = -1;
+  int resident_at = 0;
+  int slot_values = 0;  // 1: the evaluation keeps every slot term's value in shared memory
+};
+// The plan of the persistent per-instance kernel (k_persist) for precision
+// prec and rescue plan R (smem 0 when the problem cannot use it): it needs
+// the packed level program, and its phases (evaluation + stamping of one
+// instance, the packed factor/solve, a rescue warp) must each fit one CTA's
+// shared memory. Sets the kernel's shared-memory limit (call outside stream
+// capture).
+PersistPlan plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_smem);
 // Every remaining NR round of each listed instance (or of instances
 // 0 .. grid - 1 when I.live_in is null) in one launch of `grid` CTAs, at most
 // max_rounds rounds each; *active receives the instances still live and
 // *rounds_max the most rounds one instance ran.
 void launch_persist(const DevTopo& T, const DevInst& I, const JobParams& P, int prec, int grid,
-                    size_t smem, int max_rounds, int K, int* active, int* rounds_max,
+                    const PersistPlan& plan, int max_rounds, int K, int* active, int* rounds_max,
                     cudaStream_t s);
+// The first variant (0, 1, 2) whose phases each fit one CTA's shared memory
+// next to the multi-problem kernel's static shared memory. Sets the kernel's
+// shared-memory limit (call outside stream capture).
+PersistPlan plan_persist_job(const DevTopo& T, int prec, const RescuePlan& R, int max_smem);
+// Every remaining NR round of every instance of n_jobs problems (jobs: a
+// device array sorted by cta0, the first at 0, the CTA ranges back to back
+// and covering grid CTAs) in one launch, at most max_rounds rounds each, with
+// smem bytes of dynamic shared memory (the largest job's PersistPlan::smem);
+// *active and *rounds_max as for launch_persist, over all jobs;
+// *slot_timeouts counts solves that found no free rescue slot in time.
+void launch_persist_multi(const PersistJob* jobs, int n_jobs, int prec, int grid, size_t smem,
+                          int max_rounds, int* active, int* rounds_max, int* slot_timeouts,
+                          cudaStream_t s);
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s);
 // [ni][n] FP32 per-device parameters (netlist order) into [n][ld] SoA order.

@@ -261,8 +261,36 @@ void launch_rescue(const DevTopo& T, const DevInst& I, const JobParams& P, const
     k_rescue<double><<<grid, 32 * R.warps, R.smem, s>>>(T, I, P, R.K);
 }
 
-size_t plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_smem) {
-  if (T.nd_prog_len <= 0 || T.nd_levels <= 0) return 0;
+// The persistent plan's shared memory beyond the phases' minimum sm (lu, rs:
+// the factor/solve's and the rescue's needs): the slot-term values of the
+// evaluation and the instance's resident state, each when it fits, the
+// values first.
+static void fill_persist_smem(PersistPlan& plan, const DevTopo& T, size_t es, size_t sm, size_t lu, size_t rs,
+                       size_t static_smem, int max_smem) {
+  const size_t room = (size_t)max_smem - static_smem;
+  const size_t ev_jv = sizeof(double) * (3 * (size_t)(T.n_mos + T.n_dio) + (size_t)T.n_ft_terms +
+                                         (size_t)T.n_hub_slot_terms + (size_t)T.n_jt_terms);
+  const size_t sm_jv = (std::max({ev_jv, lu, rs, size_t(16)}) + 15) & ~size_t(15);
+  const size_t res = resident_layout(T, es).total;
+  plan.slot_values = 0;
+  plan.resident_at = 0;
+  plan.smem = sm;
+  if (sm_jv + res <= room) {
+    plan.slot_values = 1;
+    plan.resident_at = (int)sm_jv;
+    plan.smem = sm_jv + res;
+  } else if (sm + res <= room) {
+    plan.resident_at = (int)sm;
+    plan.smem = sm + res;
+  } else if (sm_jv <= room) {
+    plan.slot_values = 1;
+    plan.smem = sm_jv;
+  }
+}
+
+PersistPlan plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_smem) {
+  PersistPlan plan;
+  if (T.nd_prog_len <= 0 || T.nd_levels <= 0) return plan;
   const size_t es = prec == KARAM_PREC_MIXED ? sizeof(float) : sizeof(double);
   const size_t ev = sizeof(double) * (3 * (size_t)(T.n_mos + T.n_dio) + (size_t)T.n_ft_terms +
                                       (size_t)T.n_hub_slot_terms);
@@ -271,28 +299,83 @@ size_t plan_persist(const DevTopo& T, int prec, const RescuePlan& R, int max_sme
   const size_t rs = R.warps > 0 ? (T.lu_rec ? rescue_rec_bytes(T.n) : 0) + rescue_tab_bytes(T.n, T.nv) +
                                       rescue_warp_bytes(T.n, T.nv, R.K)
                                 : 0;
-  const size_t sm = std::max({ev, lu, rs});
+  const size_t sm = (std::max({ev, lu, rs, size_t(16)}) + 15) & ~size_t(15);
   const void* kern = prec == KARAM_PREC_MIXED ? (const void*)k_persist<float> : (const void*)k_persist<double>;
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
     cudaGetLastError();
-    return 0;
+    return plan;
   }
-  if (sm + fa.sharedSizeBytes > (size_t)max_smem) return 0;
+  if (sm + fa.sharedSizeBytes > (size_t)max_smem) return plan;
   if (open_smem_limit(kern, max_smem) != cudaSuccess) {
     cudaGetLastError();
-    return 0;
+    return plan;
   }
-  return std::max<size_t>(sm, 16);
+  plan.variant = 0;
+  fill_persist_smem(plan, T, es, sm, lu, rs, fa.sharedSizeBytes, max_smem);
+  return plan;
 }
 
 void launch_persist(const DevTopo& T, const DevInst& I, const JobParams& P, int prec, int grid,
-                    size_t smem, int max_rounds, int K, int* active, int* rounds_max,
+                    const PersistPlan& plan, int max_rounds, int K, int* active, int* rounds_max,
                     cudaStream_t s) {
   if (prec == KARAM_PREC_MIXED)
-    k_persist<float><<<grid, kPersistThreads, smem, s>>>(T, I, P, max_rounds, K, active, rounds_max);
+    k_persist<float><<<grid, kPersistThreads, plan.smem, s>>>(T, I, P, max_rounds, K, active, rounds_max,
+                                                              plan.resident_at, plan.slot_values);
   else
-    k_persist<double><<<grid, kPersistThreads, smem, s>>>(T, I, P, max_rounds, K, active, rounds_max);
+    k_persist<double><<<grid, kPersistThreads, plan.smem, s>>>(T, I, P, max_rounds, K, active, rounds_max,
+                                                               plan.resident_at, plan.slot_values);
+}
+
+PersistPlan plan_persist_job(const DevTopo& T, int prec, const RescuePlan& R, int max_smem) {
+  PersistPlan plan;
+  if (T.nd_levels <= 0) return plan;
+  const bool mixed = prec == KARAM_PREC_MIXED;
+  const size_t es = mixed ? sizeof(float) : sizeof(double);
+  const size_t ev = sizeof(double) * (3 * (size_t)(T.n_mos + T.n_dio) + (size_t)T.n_ft_terms +
+                                      (size_t)T.n_hub_slot_terms);
+  const size_t rs = R.warps > 0 ? (T.lu_rec ? rescue_rec_bytes(T.n) : 0) + rescue_tab_bytes(T.n, T.nv) +
+                                      rescue_warp_bytes(T.n, T.nv, R.K)
+                                : 0;
+  const void* kern = mixed ? (const void*)k_persist_multi<float> : (const void*)k_persist_multi<double>;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+    cudaGetLastError();
+    return plan;
+  }
+  const size_t slots = es * ((size_t)T.nd_SY + (size_t)T.nd_S);
+  for (int v = 0; v < 3; ++v) {
+    size_t lu;
+    if (v == 0) {
+      if (T.nd_prog_len <= 0) continue;
+      lu = ((slots + 15) & ~size_t(15)) + sizeof(int) * (((size_t)T.nd_prog_len + 3) & ~size_t(3));
+    } else if (v == 1) {
+      lu = slots;
+    } else {
+      lu = (es * (size_t)T.nd_SY + 15) & ~size_t(15);
+    }
+    const size_t sm = (std::max({ev, lu, rs, size_t(16)}) + 15) & ~size_t(15);
+    if (sm + fa.sharedSizeBytes > (size_t)max_smem) continue;
+    if (open_smem_limit(kern, max_smem) != cudaSuccess) {
+      cudaGetLastError();
+      return plan;
+    }
+    plan.variant = v;
+    fill_persist_smem(plan, T, es, sm, lu, rs, fa.sharedSizeBytes, max_smem);
+    return plan;
+  }
+  return plan;
+}
+
+void launch_persist_multi(const PersistJob* jobs, int n_jobs, int prec, int grid, size_t smem,
+                          int max_rounds, int* active, int* rounds_max, int* slot_timeouts,
+                          cudaStream_t s) {
+  if (prec == KARAM_PREC_MIXED)
+    k_persist_multi<float><<<grid, kPersistThreads, smem, s>>>(jobs, n_jobs, max_rounds, active,
+                                                               rounds_max, slot_timeouts);
+  else
+    k_persist_multi<double><<<grid, kPersistThreads, smem, s>>>(jobs, n_jobs, max_rounds, active,
+                                                                rounds_max, slot_timeouts);
 }
 
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,

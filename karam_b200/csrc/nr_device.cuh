@@ -225,9 +225,21 @@ struct DevIn {
   double va, vb, vc, p0, p1, p2, p3, sign;
 };
 
+// A load of an instance buffer: through the read-only data cache when the
+// buffer is known to be in global memory (G), else a plain load (the
+// persistent kernels may keep the instance's state in shared memory).
+template <bool G, typename V>
+__device__ __forceinline__ V ld_in(const V* p) {
+  if constexpr (G)
+    return __ldg(p);
+  else
+    return *p;
+}
+
 // Loads the inputs of device d (MOSFETs first, then diodes) for instance g.
 // Nothing here depends on an earlier evaluation, so the loads of several
 // devices can be in flight together.
+template <bool G = true>
 __device__ __forceinline__ DevIn load_device(const DevTopo& T, const DevInst& I, int d, int g) {
   const size_t ld = I.ld;
   const int nm = T.n_mos;
@@ -239,8 +251,8 @@ __device__ __forceinline__ DevIn load_device(const DevTopo& T, const DevInst& I,
     const double2 geo = __ldg(&T.mos_geo[d]);
     in.sign = __ldg(&T.mos_pmos[d]) ? -1.0 : 1.0;
     if (I.kp) {
-      in.p0 = (double)__ldg(&I.kp[d * ld + g]);
-      in.p1 = (double)__ldg(&I.vth[d * ld + g]);
+      in.p0 = (double)ld_in<G>(&I.kp[d * ld + g]);
+      in.p1 = (double)ld_in<G>(&I.vth[d * ld + g]);
     } else {
       const double2 card = __ldg(&T.mos_card[d]);
       in.p0 = card.x;
@@ -248,9 +260,9 @@ __device__ __forceinline__ DevIn load_device(const DevTopo& T, const DevInst& I,
     }
     in.p2 = geo.x;
     in.p3 = geo.y;
-    in.va = tm.x >= 0 ? __ldg(&x[tm.x * ld + g]) : 0.0;
-    in.vb = tm.y >= 0 ? __ldg(&x[tm.y * ld + g]) : 0.0;
-    in.vc = tm.z >= 0 ? __ldg(&x[tm.z * ld + g]) : 0.0;
+    in.va = tm.x >= 0 ? ld_in<G>(&x[tm.x * ld + g]) : 0.0;
+    in.vb = tm.y >= 0 ? ld_in<G>(&x[tm.y * ld + g]) : 0.0;
+    in.vc = tm.z >= 0 ? ld_in<G>(&x[tm.z * ld + g]) : 0.0;
   } else {
     const int k = d - nm;
     const int2 tt = __ldg(&T.dio_term[k]);
@@ -260,7 +272,7 @@ __device__ __forceinline__ DevIn load_device(const DevTopo& T, const DevInst& I,
     in.p2 = par.z;
     in.p3 = par.w;
     in.sign = 0.0;
-    in.va = (tt.x >= 0 ? __ldg(&x[tt.x * ld + g]) : 0.0) - (tt.y >= 0 ? __ldg(&x[tt.y * ld + g]) : 0.0);
+    in.va = (tt.x >= 0 ? ld_in<G>(&x[tt.x * ld + g]) : 0.0) - (tt.y >= 0 ? ld_in<G>(&x[tt.y * ld + g]) : 0.0);
     in.vb = in.vc = 0.0;
   }
   return in;
@@ -720,6 +732,7 @@ __device__ bool on_singular(const DevTopo& Tp, const DevInst& I, int g) {
 // ---------------------------------------------------------------------------
 // One KCL term of record q (es_ft / es_fc) for instance g; device terms read
 // the CTA's device values sd ([local][3][32] doubles, lane offset applied).
+template <bool G = true>
 __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, const JobParams& P,
                                             int4 tm, double coef, int g, bool tran, double t,
                                             double heff, const double* sd) {
@@ -727,14 +740,14 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
   const int idx = code_idx(tm.x), kind = code_kind(tm.x);
   if (kind >= 4) return sd[tm.w];  // diode i / MOSFET ids, at the offset the table carries
   if (kind == 2) return coef;                                                // current source
-  const double va = tm.y >= 0 ? __ldg(&I.x[tm.y * ld + g]) : 0.0;
-  const double vb = tm.z >= 0 ? __ldg(&I.x[tm.z * ld + g]) : 0.0;
+  const double va = tm.y >= 0 ? ld_in<G>(&I.x[tm.y * ld + g]) : 0.0;
+  const double vb = tm.z >= 0 ? ld_in<G>(&I.x[tm.z * ld + g]) : 0.0;
   if (kind == 0) return coef * (va - vb);                                    // resistor
   if (kind == 1) return 1.0e3 * ((va - vb) - source_value(T, I, g, idx, tran, t));  // Norton V source
   if (!tran) return 0.0;                                                     // capacitor companion
   const size_t ci = (size_t)idx * ld + g;
-  double cur = (coef / heff) * ((va - vb) - __ldg(&I.cap_vp[ci]));
-  if (P.method == KTRAN_TRAP) cur -= __ldg(&I.cap_ip[ci]);
+  double cur = (coef / heff) * ((va - vb) - ld_in<G>(&I.cap_vp[ci]));
+  if (P.method == KTRAN_TRAP) cur -= ld_in<G>(&I.cap_ip[ci]);
   return cur;
 }
 
@@ -943,13 +956,15 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
 // chunk order), so the results are k_es's. Dynamic shared memory: the
 // device values [3][devices] (gm or diode g, gds or diode i, ids), then every
 // node term's signed value and every hub slot term's signed value, computed
-// side by side before the sums (a - c and a + (-c) round alike).
+// side by side before the sums (a - c and a + (-c) round alike); with
+// slot_values also every slot term's signed value, so the slot sums read
+// consecutive values instead of gathering them term by term.
 // The body of k_es_one for instance g, by the whole CTA (s_val: the dynamic
 // shared memory described above; s_f, s_dv, s_fl: one entry per warp).
-template <typename TJ>
+template <typename TJ, bool G = true>
 __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobParams& P, int g,
                                 double* s_val, unsigned long long* s_f, unsigned long long* s_dv,
-                                int* s_fl) {
+                                int* s_fl, bool slot_values = false) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const size_t ld = I.ld;
   const int nv = T.nv, n = T.n, nm = T.n_mos, nd = T.n_mos + T.n_dio;
@@ -962,8 +977,9 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
   double* v2 = s_val + 2 * nd;  // ids
   double* tv = s_val + 3 * nd;  // node terms, signed
   double* hv = tv + T.n_ft_terms;  // hub slot terms, signed
+  double* jv = hv + T.n_hub_slot_terms;  // with slot_values: every slot term, signed
   for (int d = tid; d < nd; d += blockDim.x) {
-    const DevIn in = load_device(T, I, d, g);
+    const DevIn in = load_device<G>(T, I, d, g);
     if (in.mos) {
       double ids, gm, gds;
       mosfet_eval(in.va, in.vb, in.vc, in.sign, in.p0, in.p1, in.p2, in.p3, ids, gm, gds);
@@ -979,16 +995,17 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
   }
   __syncthreads();
   // a slot term's device value (codes in global numbering: MOSFET or diode index)
-  auto slot_val = [&](int c) {
+  auto slot_val = [&](int c) {  // one load from a selected address: loads of several terms overlap
     const int kind = code_kind(c), idx = code_idx(c);
-    return kind == 0 ? v1[idx] : kind == 2 ? v0[nm + idx] : v0[idx];  // gds | diode g | gm
+    const double* src = kind == 0 ? v1 + idx : kind == 2 ? v0 + nm + idx : v0 + idx;  // gds | diode g | gm
+    return *src;
   };
   auto node_val = [&](int q) {
     const int c = __ldg(&T.ft_code[q]), kind = code_kind(c), idx = code_idx(c);
     if (kind == 4) return v1[nm + idx];  // diode current
     if (kind == 5) return v2[idx];       // MOSFET ids
     const int4 tm = make_int4(c, __ldg(&T.ft_a[q]), __ldg(&T.ft_b[q]), 0);
-    return node_term(T, I, P, tm, __ldg(&T.ft_coef[q]), g, tran, t, heff, s_val);
+    return node_term<G>(T, I, P, tm, __ldg(&T.ft_coef[q]), g, tran, t, heff, s_val);
   };
   auto slot_base = [&](int s) {  // linear part + capacitor companions
     double acc = __ldg(&T.jlin_dc[s]);
@@ -1011,6 +1028,12 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
     const double c0 = node_val(q);
     tv[q] = __ldg(&T.ft_code[q]) < 0 ? -c0 : c0;
   }
+  if (slot_values)
+    for (int q = tid; q < T.n_jt_terms; q += blockDim.x) {
+      const int c = __ldg(&T.jt_code[q]);
+      const double val = slot_val(c);
+      jv[q] = c < 0 ? -val : val;
+    }
   for (int h = 0; h < T.n_hub_items; ++h) {
     const int4 hb = __ldg(&T.hub_items[h]);
     if (hb.x >= nv) continue;
@@ -1041,7 +1064,24 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
     if (it < nv) {
       double acc = slot_base(it);
       const int q1 = __ldg(&T.jt_off[it + 1]);
-      for (int q = __ldg(&T.jt_off[it]); q < q1; ++q) {
+      int q = __ldg(&T.jt_off[it]);
+      if (slot_values)  // the signed values side by side: a - v and a + (-v) round alike
+        for (; q < q1; ++q) acc += jv[q];
+      // eight terms' codes and values fetched together, then added in term
+      // order (a - v and a + (-v) round alike): the loads overlap, the sum
+      // is the sequential one
+      for (; q + 8 <= q1; q += 8) {
+        double sv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int c = __ldg(&T.jt_code[q + k]);
+          const double val = slot_val(c);
+          sv[k] = c < 0 ? -val : val;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc += sv[k];
+      }
+      for (; q < q1; ++q) {
         const int c = __ldg(&T.jt_code[q]);
         const double val = slot_val(c);
         acc = c < 0 ? acc - val : acc + val;
@@ -1385,6 +1425,7 @@ __device__ bool nd_solve_cta(T* __restrict__ A, T* __restrict__ y, const int* __
       const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
       const int sl = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
       T acc = A[sl];
+#pragma unroll 4
       for (int q = 0; q < c; ++q) {
         const int pr = prog[off + q];
         acc -= A[pr & 0xFFFF] * A[(pr >> 16) & 0xFFFF];
@@ -1396,6 +1437,7 @@ __device__ bool nd_solve_cta(T* __restrict__ A, T* __restrict__ y, const int* __
       const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
       const int row = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
       T acc = y[row];
+#pragma unroll 4
       for (int q = 0; q < c; ++q) {
         const int pr = prog[off + q];
         acc -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
@@ -1435,6 +1477,7 @@ __device__ bool nd_solve_cta(T* __restrict__ A, T* __restrict__ y, const int* __
       const int k = a & 0xFFFF, d = (a >> 16) & 0xFFFF;
       const int c = b & 0xFFFF, off = bpb + ((b >> 16) & 0xFFFF);
       T sv = y[k];
+#pragma unroll 4
       for (int j = 0; j < c; ++j) {
         const int pr = prog[off + j];
         sv -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
@@ -2669,62 +2712,96 @@ __global__ void __launch_bounds__(256) k_rescue(DevTopo Tp, DevInst I, JobParams
 // Threads of the persistent per-instance kernel.
 constexpr int kPersistThreads = 512;
 
-// Every remaining NR round of one instance per CTA, inside one launch: the
-// rounds k_es_one + k_lu_big (packed program and slots in shared memory) +
-// k_rescue would run one launch each, with the same device code, so the
-// results are theirs bit for bit. An instance whose static pivots fail is
-// rescued by the CTA's warp 0 in workspace slot blockIdx.x. The CTA stops when
-// its instance is done or after max_rounds rounds; it then adds 1 to *active
-// if the instance is still live, and raises *rounds_max to the rounds it ran.
-// Instances: I.live_in[0 .. *I.live_in_count) when listed, else 0 .. ni - 1.
-// Dynamic shared memory: the largest of the three phases' needs (they run one
-// after another).
-template <typename T>
-__global__ void __launch_bounds__(kPersistThreads) k_persist(DevTopo Tp, DevInst I, JobParams P,
-                                                             int max_rounds, int K, int* active,
-                                                             int* rounds_max) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ unsigned long long s_f[kPersistThreads / 32], s_dv[kPersistThreads / 32];
-  __shared__ int s_fl[kPersistThreads / 32];
-  __shared__ LuShared sh;
-  __shared__ int s_rescue;
-  int g = blockIdx.x;
-  if (I.live_in) {
-    if ((int)blockIdx.x >= *I.live_in_count) return;
-    g = I.live_in[blockIdx.x];
+// Static shared memory of the persistent kernels' rounds.
+struct PersistShared {
+  unsigned long long f[kPersistThreads / 32], dv[kPersistThreads / 32];
+  int fl[kPersistThreads / 32];
+  LuShared lu;
+  int rescue;
+  int slot;  // rescue workspace slot of this round's rescue
+};
+
+// Cycles a CTA waits for a free rescue workspace slot (about 8 s of SM
+// clock) before it gives the solve up as singular.
+constexpr long long kSlotWaitCycles = 1ll << 34;
+
+// A free slot of the shared rescue workspace (slot_lock[k] == 0 -> 1), tried
+// from k = first upward, cyclically; -1 (and *timeouts + 1) when none came free
+// within kSlotWaitCycles. Holders release theirs after their rescue, and a
+// rescue waits on nothing, so every held slot comes free.
+__device__ __forceinline__ int acquire_slot(int* slot_lock, int n_slots, int first, int* timeouts) {
+  const long long t0 = clock64();
+  for (int k = first % n_slots;; k = k + 1 == n_slots ? 0 : k + 1) {
+    if (atomicCAS(&slot_lock[k], 0, 1) == 0) {
+      __threadfence();
+      return k;
+    }
+    if (clock64() - t0 > kSlotWaitCycles) {
+      if (timeouts) atomicAdd(timeouts, 1);
+      return -1;
+    }
   }
-  if (g >= I.ni) return;
+}
+
+// Every remaining NR round of instance g by the whole CTA: the rounds
+// k_es_one + k_lu_big<T, gA, packed> + k_rescue would run one launch each,
+// with the same device code, so the results are theirs bit for bit. An
+// instance whose static pivots fail is rescued by the CTA's warp 0: in
+// workspace slot `slot` when slot_lock is null, else in a slot taken from
+// the shared pool slot_lock[0 .. I.rescue_slots) for that rescue (a solve
+// that finds no slot within kSlotWaitCycles counts in *slot_timeouts and is
+// treated as singular). Stops when the instance is done or after max_rounds
+// rounds; then thread 0 adds 1 to *active if the instance is still live and
+// raises *rounds_max to the rounds it ran. Dynamic shared memory: the
+// largest of the three phases' needs (they run one after another).
+template <typename T, bool gA, bool packed>
+__device__ void persist_instance(const DevTopo& Tp, const DevInst& I, const JobParams& P, int g,
+                                 int slot, int K, int max_rounds, unsigned char* smem_raw,
+                                 PersistShared& S, int* active, int* rounds_max,
+                                 int* slot_lock = nullptr, int* slot_timeouts = nullptr,
+                                 bool slot_values = false) {
   const int tid = threadIdx.x;
   int r = 0;
   bool live = I.ev_heff[g] >= 0.0;
   for (; r < max_rounds && live; ++r) {
-    es_one_instance<T>(Tp, I, P, g, reinterpret_cast<double*>(smem_raw), s_f, s_dv, s_fl);
+    es_one_instance<T, false>(Tp, I, P, g, reinterpret_cast<double*>(smem_raw), S.f, S.dv, S.fl,
+                              slot_values);
     __syncthreads();
-    lu_big_instance<T, false, true>(Tp, I, P, g, smem_raw, sh);
-    if (!sh.live) break;
-    const int a = sh.a, sing = (a & ACT_SOLVE) ? sh.sing : 0;
+    lu_big_instance<T, gA, packed>(Tp, I, P, g, smem_raw, S.lu);
+    if (!S.lu.live) break;
+    const int a = S.lu.a, sing = (a & ACT_SOLVE) ? S.lu.sing : 0;
     if (tid == 0) {
-      s_rescue = sing && I.rescue_ws != nullptr && (int)blockIdx.x < I.rescue_slots;
-      if (s_rescue)
+      int rs = -1;
+      if (sing && I.rescue_ws != nullptr) {
+        if (!slot_lock)
+          rs = slot < I.rescue_slots ? slot : -1;
+        else if (I.rescue_slots > 0)
+          rs = acquire_slot(slot_lock, I.rescue_slots, slot, slot_timeouts);
+      }
+      S.rescue = rs >= 0;
+      S.slot = rs;
+      if (S.rescue)
         set_eval_point(I, P, g, I.st[g]);  // as instance_finish does before its hand-off
       else
-        instance_finish(Tp, I, P, g, a, sing, sh.gmin);
+        instance_finish(Tp, I, P, g, a, sing, S.lu.gmin);
       if (I.counters) {
-        atomicAdd(&I.counters[sh.trev ? 1 : 0], 1ull);
+        atomicAdd(&I.counters[S.lu.trev ? 1 : 0], 1ull);
         if ((a & ACT_SOLVE) && !sing) atomicAdd(&I.counters[2], 1ull);
       }
     }
     __syncthreads();
-    if (s_rescue) {
+    if (S.rescue) {
       int4* rec;
       RescueTab tb;
       unsigned char* base = rescue_setup(Tp, smem_raw, rec, tb);
       __syncthreads();
       if (tid < 32) {
-        const RescueWarp w = rescue_warp(Tp, I, base, K, blockIdx.x);
-        rescue_item<T>(Tp, I, P, tb, w, rec, g, a, sh.gmin, tid);
+        const RescueWarp w = rescue_warp(Tp, I, base, K, S.slot);
+        rescue_item<T>(Tp, I, P, tb, w, rec, g, a, S.lu.gmin, tid);
+        if (slot_lock) __threadfence();  // the workspace writes before the slot's release
       }
       __syncthreads();
+      if (tid == 0 && slot_lock) atomicExch(&slot_lock[S.slot], 0);
     }
     live = I.ev_heff[g] >= 0.0;
     __syncthreads();  // every thread has read the next evaluation point
@@ -2732,6 +2809,260 @@ __global__ void __launch_bounds__(kPersistThreads) k_persist(DevTopo Tp, DevInst
   if (tid == 0) {
     if (I.st[g].mode != MODE_DONE) atomicAdd(active, 1);
     atomicMax(rounds_max, r);
+  }
+}
+
+// Byte offsets of one instance's state in shared memory (resident_in),
+// each region on a 16-byte boundary; es = the Jacobian value size.
+struct ResidentLayout {
+  size_t v, x, F, vtp, cvp, cip, vsdc, v1, v2, hist, scal, st, J, kp, vth, total;
+};
+__host__ __device__ inline ResidentLayout resident_layout(const DevTopo& T, size_t es) {
+  ResidentLayout L{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o += (bytes + 15) & ~size_t(15);
+    return at;
+  };
+  const size_t n = (size_t)T.n, nc = (size_t)T.n_cap, ns = (size_t)T.n_vs;
+  L.v = take(8 * n);
+  L.x = take(8 * n);
+  L.F = take(8 * n);
+  L.vtp = take(8 * n);
+  L.cvp = take(8 * nc);
+  L.cip = take(8 * nc);
+  L.vsdc = take(8 * ns);
+  L.v1 = take(8 * ns);
+  L.v2 = take(8 * ns);
+  L.hist = take(8 * 2 * KHIST_LEN);
+  L.scal = take(8 * 5);  // ev_t, ev_heff, red_f, red_dv, red_flags
+  L.st = take(sizeof(InstState));
+  L.J = take(es * (size_t)T.nv);
+  L.kp = take(4 * (size_t)T.n_mos);
+  L.vth = take(4 * (size_t)T.n_mos);
+  L.total = o;
+  return L;
+}
+
+// The state of instance g in shared memory for a persistent CTA: the CTA
+// copies the instance's vectors, Jacobian slots, parameters, history and
+// state word from the batch's interleaved arrays into `base` (laid out by
+// resident_layout), and thread 0 makes R a one-instance view of the copy
+// (instance 0, lane stride 1); resident_out writes the mutable part back.
+// persist_instance on R runs the arithmetic it would run on the batch's
+// arrays, on the same values, so the results are the same bit for bit; only
+// the latency of the state changes. Needs a barrier before R is used.
+template <typename T>
+__device__ void resident_in(const DevTopo& Tp, const DevInst& I, int g, unsigned char* base,
+                            DevInst& R) {
+  const ResidentLayout L = resident_layout(Tp, sizeof(T));
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const size_t ld = I.ld;
+  double* v = reinterpret_cast<double*>(base + L.v);
+  double* x = reinterpret_cast<double*>(base + L.x);
+  double* F = reinterpret_cast<double*>(base + L.F);
+  double* vtp = reinterpret_cast<double*>(base + L.vtp);
+  double* cvp = reinterpret_cast<double*>(base + L.cvp);
+  double* cip = reinterpret_cast<double*>(base + L.cip);
+  double* vsdc = reinterpret_cast<double*>(base + L.vsdc);
+  double* v1 = reinterpret_cast<double*>(base + L.v1);
+  double* v2 = reinterpret_cast<double*>(base + L.v2);
+  double* hist = reinterpret_cast<double*>(base + L.hist);
+  double* scal = reinterpret_cast<double*>(base + L.scal);
+  InstState* st = reinterpret_cast<InstState*>(base + L.st);
+  T* Jr = reinterpret_cast<T*>(base + L.J);
+  float* kp = reinterpret_cast<float*>(base + L.kp);
+  float* vth = reinterpret_cast<float*>(base + L.vth);
+  const T* Jg = reinterpret_cast<const T*>(I.J);
+  if (tid == 0) {
+    R = I;
+    R.ni = 1;
+    R.ld = 1;
+    R.v = v;
+    R.x = x;
+    R.F = F;
+    R.v_tp = vtp;
+    R.cap_vp = cvp;
+    R.cap_ip = cip;
+    R.vs_dc = vsdc;
+    R.vs_v1 = v1;
+    R.vs_v2 = v2;
+    R.hist = hist;
+    R.ev_t = scal;
+    R.ev_heff = scal + 1;
+    R.red_f = reinterpret_cast<unsigned long long*>(scal + 2);
+    R.red_dv = reinterpret_cast<unsigned long long*>(scal + 3);
+    R.red_flags = reinterpret_cast<int*>(scal + 4);
+    R.st = st;
+    R.J = Jr;
+    R.kp = I.kp ? kp : nullptr;
+    R.vth = I.vth ? vth : nullptr;
+    R.seed = nullptr;
+    R.live_in = nullptr;
+    R.live_in_count = nullptr;
+    R.live_out = nullptr;
+    R.live_out_count = nullptr;
+    R.hub_part = nullptr;
+    R.hub_cnt = nullptr;
+    R.lu_ws = I.lu_ws ? reinterpret_cast<unsigned char*>(I.lu_ws) + (size_t)g * Tp.nd_S * sizeof(T)
+                      : nullptr;
+    R.wave = I.wave ? I.wave + (size_t)g * I.wave_steps * I.n_wave : nullptr;
+    scal[0] = I.ev_t[g];
+    scal[1] = I.ev_heff[g];
+    reinterpret_cast<unsigned long long*>(scal)[2] = I.red_f[g];
+    reinterpret_cast<unsigned long long*>(scal)[3] = I.red_dv[g];
+    *reinterpret_cast<int*>(scal + 4) = I.red_flags[g];
+    *st = I.st[g];
+  }
+  for (int i = tid; i < Tp.n; i += bd) {
+    const size_t o = (size_t)i * ld + g;
+    v[i] = I.v[o];
+    x[i] = I.x[o];
+    F[i] = I.F[o];
+    vtp[i] = I.v_tp[o];
+  }
+  for (int c = tid; c < Tp.n_cap; c += bd) {
+    cvp[c] = I.cap_vp[(size_t)c * ld + g];
+    cip[c] = I.cap_ip[(size_t)c * ld + g];
+  }
+  for (int k = tid; k < Tp.n_vs; k += bd) {
+    vsdc[k] = I.vs_dc[(size_t)k * ld + g];
+    v1[k] = I.vs_v1[(size_t)k * ld + g];
+    v2[k] = I.vs_v2[(size_t)k * ld + g];
+  }
+  for (int k = tid; k < 2 * KHIST_LEN; k += bd) hist[k] = I.hist[(size_t)k * ld + g];
+  for (int k = tid; k < Tp.nv; k += bd) Jr[k] = Jg[(size_t)k * ld + g];
+  for (int k = tid; k < Tp.n_mos; k += bd) {
+    if (I.kp) kp[k] = I.kp[(size_t)k * ld + g];
+    if (I.vth) vth[k] = I.vth[(size_t)k * ld + g];
+  }
+}
+
+template <typename T>
+__device__ void resident_out(const DevTopo& Tp, const DevInst& I, int g, const unsigned char* base) {
+  const ResidentLayout L = resident_layout(Tp, sizeof(T));
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const size_t ld = I.ld;
+  const double* v = reinterpret_cast<const double*>(base + L.v);
+  const double* x = reinterpret_cast<const double*>(base + L.x);
+  const double* F = reinterpret_cast<const double*>(base + L.F);
+  const double* vtp = reinterpret_cast<const double*>(base + L.vtp);
+  const double* cvp = reinterpret_cast<const double*>(base + L.cvp);
+  const double* cip = reinterpret_cast<const double*>(base + L.cip);
+  const double* hist = reinterpret_cast<const double*>(base + L.hist);
+  const double* scal = reinterpret_cast<const double*>(base + L.scal);
+  const InstState* st = reinterpret_cast<const InstState*>(base + L.st);
+  const T* Jr = reinterpret_cast<const T*>(base + L.J);
+  for (int i = tid; i < Tp.n; i += bd) {
+    const size_t o = (size_t)i * ld + g;
+    I.v[o] = v[i];
+    I.x[o] = x[i];
+    I.F[o] = F[i];
+    I.v_tp[o] = vtp[i];
+  }
+  for (int c = tid; c < Tp.n_cap; c += bd) {
+    I.cap_vp[(size_t)c * ld + g] = cvp[c];
+    I.cap_ip[(size_t)c * ld + g] = cip[c];
+  }
+  for (int k = tid; k < 2 * KHIST_LEN; k += bd) I.hist[(size_t)k * ld + g] = hist[k];
+  T* Jw = reinterpret_cast<T*>(I.J);
+  for (int k = tid; k < Tp.nv; k += bd) Jw[(size_t)k * ld + g] = Jr[k];
+  if (tid == 0) {
+    I.ev_t[g] = scal[0];
+    I.ev_heff[g] = scal[1];
+    I.red_f[g] = reinterpret_cast<const unsigned long long*>(scal)[2];
+    I.red_dv[g] = reinterpret_cast<const unsigned long long*>(scal)[3];
+    I.red_flags[g] = *reinterpret_cast<const int*>(scal + 4);
+    I.st[g] = *st;
+  }
+}
+
+// One instance per CTA, all its remaining rounds in one launch (packed
+// program, slots in shared memory; rescue slot blockIdx.x). Instances:
+// I.live_in[0 .. *I.live_in_count) when listed, else 0 .. ni - 1.
+// With resident_at > 0 the instance's state lives in shared memory from
+// that byte offset on (resident_in / resident_out); either way the rounds
+// read the instance's buffers through a view R in shared memory. With
+// slot_values the evaluation keeps every slot term's value in shared memory
+// (es_one_instance).
+template <typename T>
+__global__ void __launch_bounds__(kPersistThreads) k_persist(DevTopo Tp, DevInst I, JobParams P,
+                                                             int max_rounds, int K, int* active,
+                                                             int* rounds_max, int resident_at,
+                                                             int slot_values) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PersistShared S;
+  __shared__ DevInst R;
+  int g = blockIdx.x;
+  if (I.live_in) {
+    if ((int)blockIdx.x >= *I.live_in_count) return;
+    g = I.live_in[blockIdx.x];
+  }
+  if (g >= I.ni) return;
+  if (resident_at > 0)
+    resident_in<T>(Tp, I, g, smem_raw + resident_at, R);
+  else if (threadIdx.x == 0)
+    R = I;
+  __syncthreads();
+  persist_instance<T, false, true>(Tp, R, P, resident_at > 0 ? 0 : g, blockIdx.x, K, max_rounds,
+                                   smem_raw, S, active, rounds_max, nullptr, nullptr, slot_values != 0);
+  if (resident_at > 0) {
+    __syncthreads();
+    resident_out<T>(Tp, I, g, smem_raw + resident_at);
+  }
+}
+
+// Several problems of different sizes in one persistent launch: CTA b runs
+// instance b - cta0 of the job whose CTA range holds b (jobs sorted by cta0,
+// the first at 0), with that job's factor/solve variant. The job's tables
+// are copied into shared memory once; a problem's rescues share its
+// workspace slots through the job's slot_lock pool. Dynamic shared memory:
+// the largest job's need.
+template <typename T>
+__global__ void __launch_bounds__(kPersistThreads) k_persist_multi(const PersistJob* __restrict__ jobs,
+                                                                   int n_jobs, int max_rounds,
+                                                                   int* active, int* rounds_max,
+                                                                   int* slot_timeouts) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PersistShared S;
+  __shared__ __align__(16) PersistJob J;
+  __shared__ DevInst R;
+  const int b = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;  // the last job with cta0 <= b
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&jobs[mid].cta0) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  static_assert(sizeof(PersistJob) % 4 == 0, "job copy by words");
+  const int* src = reinterpret_cast<const int*>(&jobs[lo]);
+  int* dst = reinterpret_cast<int*>(&J);
+  for (int e = threadIdx.x; e < (int)(sizeof(PersistJob) / 4); e += blockDim.x) dst[e] = __ldg(&src[e]);
+  __syncthreads();
+  const int g = b - J.cta0;
+  if (g < 0 || g >= J.I.ni) return;
+  const int res = J.resident_at;
+  if (res > 0)
+    resident_in<T>(J.T, J.I, g, smem_raw + res, R);
+  else if (threadIdx.x == 0)
+    R = J.I;
+  __syncthreads();
+  const int gl = res > 0 ? 0 : g;
+  if (J.variant == 0)
+    persist_instance<T, false, true>(J.T, R, J.P, gl, g, J.K, max_rounds, smem_raw, S, active,
+                                     rounds_max, J.slot_lock, slot_timeouts, J.slot_values != 0);
+  else if (J.variant == 1)
+    persist_instance<T, false, false>(J.T, R, J.P, gl, g, J.K, max_rounds, smem_raw, S, active,
+                                      rounds_max, J.slot_lock, slot_timeouts, J.slot_values != 0);
+  else
+    persist_instance<T, true, false>(J.T, R, J.P, gl, g, J.K, max_rounds, smem_raw, S, active,
+                                     rounds_max, J.slot_lock, slot_timeouts, J.slot_values != 0);
+  if (res > 0) {
+    __syncthreads();
+    resident_out<T>(J.T, J.I, g, smem_raw + res);
   }
 }
 

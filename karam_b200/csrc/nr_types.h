@@ -148,6 +148,7 @@ struct DevTopo {
   const int4* hub_items;    // {item, es_hub offset, chunks, offset of a hub slot's terms}
   int n_hub_items;
   int n_ft_terms, n_hub_slot_terms;  // node terms in all; terms of the hub slots
+  int n_jt_terms, pad_jt_;           // slot terms in all
   // LU program per pivot k: hdr = (off, nL, nU, diagonal slot); data at off =
   // Lrow[nL] Lslot[nL] Ucol[nU] Uslot[nU] T[nL*nU] (update target slots)
   const int4* lu_hdr;
@@ -237,6 +238,28 @@ struct JobParams {
   int seed_bcast;    // 1: one seed for every instance, in lane 0 of DevInst::seed
   int max_halvings;  // transient restarts with a halved step (reference: 3)
   double growth32, growth64;  // static-pivot multiplier limits (FP32 / FP64 solves)
+};
+
+// One problem of a multi-problem persistent launch (k_persist_multi): CTAs
+// cta0 .. cta0 + I.ni - 1 of the launch run this problem's instances 0 ..
+// I.ni - 1. variant: where the factor/solve keeps its ND slots and program --
+// 0 packed program and slots in shared memory, 1 slots in shared memory and
+// the schedule tables in global memory, 2 slots in I.lu_ws (global memory).
+// K: the rescue workspace's column stride. resident_at: > 0 when each
+// instance's state lives in the CTA's dynamic shared memory from that byte
+// offset on. slot_lock: one word per rescue workspace slot (I.rescue_slots of
+// them, 0 = free), the pool this problem's rescues take their slots from.
+struct PersistJob {
+  DevTopo T;
+  DevInst I;
+  JobParams P;
+  int K;
+  int cta0;
+  int variant;
+  int resident_at;
+  int slot_values;  // 1: the evaluation keeps every slot term's value in shared memory
+  int pad_;
+  int* slot_lock;
 };
 
 #endif

@@ -69,3 +69,33 @@ def test_round_budget_stops_persistent_kernel(product, ctx):
     prob.set_instances(None)
     _, st = prob.solve_dc(product.options(precision=A.PREC_FP64, schedule=-4, max_rounds=10))
     assert st[0]["status"] == A.ST_TIMEOUT and prob.timing()["rounds"] == 10
+
+
+@pytest.mark.parametrize("prec", [A.PREC_MIXED, A.PREC_FP64])
+def test_uneven_batch_in_one_launch_equals_per_problem_runs(product, ctx, prec):
+    """Grids of three sizes (8 x 8 and 16 x 16 fit the packed program in shared
+    memory, 40 x 40 keeps its slots in global memory) and a config-2 batch:
+    DC + 10 trapezoidal steps of all four problems in ONE k_persist_multi
+    launch equal each problem's own per-round run bit for bit."""
+    specs = [(circuits.grid_circuit(8), 3), (circuits.grid_circuit(16), 2),
+             (circuits.grid_circuit(40), 2), (circuits.config2(), 4)]
+    dt, steps = 20e-12, 10
+    opts = product.options(precision=prec, **POLISH)
+    probs = []
+    for nl, ni in specs:
+        p = product.Problem(ctx, nl, max_instances=ni)
+        p.set_instances(circuits.mc_instances(nl, ni))
+        probs.append(p)
+    product.run_mc_multi(probs, dt, steps, A.TRAN_TRAP, opts)
+    multi = [p.read_results() for p in probs]
+    t = probs[0].timing()
+    assert t["level_schedule"] == 5 and t["persistent_rounds"] == t["rounds"] > 0
+    for p, (v_m, st_m) in zip(probs, multi):
+        p.run_mc_device(dt, steps, A.TRAN_TRAP,
+                        product.options(precision=prec, schedule=-2, **POLISH))
+        v, st = p.read_results()
+        assert np.array_equal(v_m, v)
+        assert stats_key(st_m) == stats_key(st)
+        assert sum(s["status"] == A.ST_CONVERGED for s in st) >= len(st) - 1
+    for p in probs:
+        p.close()
