@@ -553,6 +553,7 @@ def run_karam(args, dist):
         # the 32-stage family of the same method (130 features), a smaller training set
         line["config5_32stage"] = config5_seeder(ctx, n_train=40960, n_test=8192, stages=32)
         line["config3"] = config3_uneven(dist.local, steps=args.config3_steps)
+        line["ac"] = ac_sweep_leg(ctx)
     if dist.rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64)
         line["outcomes"] = outcome_check(nl, inst, st_mixed, st_fp64)
@@ -570,6 +571,61 @@ def run_karam(args, dist):
     seeder.close()
     prob.close()
     ctx.close()
+
+
+def ac_sweep_leg(ctx, n_instances=4096, n_points=16, f_start=1e6, f_stop=1e12, input_node=2,
+                 oracle_sample=4):
+    """Small-signal AC sweep (karam_ac_sweep) of the config-2 Monte-Carlo batch
+    at its DC points: each instance's Y(jw) = the FP64 NR Jacobian at its DC
+    point + jwC, driven at the chain's input, over n_points log-spaced
+    frequencies; one CTA per (instance, frequency) factors Y on the static
+    pivots in complex FP64. Timed: the call (device time of the Jacobian
+    evaluation + the sweep, and wall time with the copies back). Accuracy: the
+    first instances against the oracle's sweep (dense complex LU with partial
+    pivoting) at the same DC points, which also gives the CPU rate on that
+    sample (the oracle's restatement of the reference's dense solve, one thread)."""
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+    from karam_b200 import circuits
+    from oracle import pyoracle
+    nl = circuits.config2()
+    inst = circuits.mc_instances(nl, n_instances)
+    prob = K.Problem(ctx, nl, max_instances=n_instances)
+    prob.set_instances(inst)
+    v, st = prob.solve_dc(K.options(precision=A.PREC_MIXED, **POLISH))
+    conv = [i for i in range(n_instances) if st[i]["status"] == A.ST_CONVERGED]
+    prob.ac_sweep(f_start, f_stop, n_points, input_node)  # warm-up
+    t = time.perf_counter()
+    f, x, status = prob.ac_sweep(f_start, f_stop, n_points, input_node)
+    wall = time.perf_counter() - t
+    dev_ms = prob.timing()["job_ms"]
+    ok_points = int(np.sum(status == A.ST_CONVERGED))
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    worst, cpu_t = 0.0, 0.0
+    with native_stdout_to_stderr():
+        orc = pyoracle.Oracle(kind)
+        for i in conv[:oracle_sample]:
+            t0 = time.perf_counter()
+            x_ref, _ = orc.ac(nl, v[i], f_start, f_stop, n_points, input_node, inst=inst, idx=i)
+            cpu_t += time.perf_counter() - t0
+            worst = max(worst, float(np.max(np.abs(x[i] - x_ref) / (1e-9 * np.abs(x_ref) + 1e-12))))
+    prob.close()
+    n_done = min(oracle_sample, len(conv))
+    return {
+        "workload": f"config-2 MC batch ({n_instances} instances, n = {nl.n_nodes}) at its DC points, "
+                    f"{n_points} log-spaced points {f_start:g}..{f_stop:g} Hz, input node {input_node}",
+        "points_per_s": ok_points / wall, "points_per_s_device": ok_points / (dev_ms * 1e-3),
+        "wall_ms": wall * 1e3, "device_ms": dev_ms, "points_ok": ok_points,
+        "points": n_instances * n_points, "dc_converged": len(conv),
+        "max_scaled_err_vs_oracle": worst,
+        "scaled": "|dv| / (1e-9 |v| + 1e-12 V) on complex node voltages",
+        "cpu_baseline": {"value": n_done * n_points / cpu_t if cpu_t else None, "unit": "points/s",
+                         "cores": 1, "kind": "reference" if kind == "ref" else "port",
+                         "sample": f"{n_done} instances x {n_points} points, dense complex LU "
+                                   f"(solveComplexLU_Sparse), {cpu_t:.2f} s"},
+    }
 
 
 def config1_latency(ctx, reps=50):

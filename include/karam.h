@@ -334,6 +334,28 @@ KARAM_API int karam_run_mc_device(karam_problem *p, const karam_solver_opts *opt
 KARAM_API int karam_run_mc_multi(karam_problem *const *probs, int32_t n_probs,
                                  const karam_solver_opts *opts, double dt, int32_t n_steps,
                                  int32_t method);
+/* Small-signal AC sweep of every instance at its DC operating point, after a
+ * DC-only solve (karam_solve_dc): the analysis of ACSolver::solveAC_Sparse
+ * (solvers/ac_solver.h:711-773), which the reference runs per netlist with a
+ * dense complex LU (math/linalg.h:993-1078). Y(jw) = the NR Jacobian at the
+ * DC point (every device conductance from the instance's own models) + jwC +
+ * 1e-12 on every diagonal, with input_node (1-based; 0 = none) driven through
+ * 1e6 S at `amplitude` volts; n_points log-spaced frequencies from f_start to
+ * f_stop by the reference's formula (freqs_out[n_points] when non-NULL). One
+ * CTA per (instance, frequency) factors Y on the problem's static pivots and
+ * level schedule in complex FP64 and solves it. out_re / out_im:
+ * [n_instances][n_points][n] node voltages (node i at index i - 1). status
+ * [n_instances][n_points] (may be NULL): KARAM_ST_CONVERGED, KARAM_ST_SINGULAR
+ * when a static pivot failed, or the instance's DC status when its DC did not
+ * converge. Unlike the reference's admittance build, MOSFETs are linearised
+ * with their own KP / VTO / LAMBDA and PMOS sign (ac_solver.h:688-696 uses
+ * fixed NMOS values) and diode conductance keeps the DC floor of 1e-12 S (the
+ * reference's AC build floors at 1e-15). KARAM_E_UNSUPPORTED when the problem
+ * has no packed level program or its complex slots exceed one CTA's shared
+ * memory; KARAM_E_STATE without a DC-only solve. */
+KARAM_API int karam_ac_sweep(karam_problem *p, double f_start, double f_stop, int32_t n_points,
+                             int32_t input_node, double amplitude, double *freqs_out,
+                             double *out_re, double *out_im, int32_t *status);
 /* SPICE netlist front-end (SPICEParser::parse, netlist/spice_parser.cpp:148-262)
  * for the subset the engine solves: R, C, V (DC, PULSE), I (DC), D, M with
  * .MODEL NMOS / PMOS (KP, VTO, LAMBDA) and D (IS, N), .TEMP, .OP, .TRAN, .END.

@@ -64,6 +64,8 @@ def lib():
                                           C.c_int32]),
         "karam_run_mc_multi": (C.c_int, [P(vp), C.c_int32, P(A.KaramSolverOpts), C.c_double,
                                          C.c_int32, C.c_int32]),
+        "karam_ac_sweep": (C.c_int, [vp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double,
+                                     P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int32)]),
         "karam_tune_schedule": (C.c_int, [vp, P(A.KaramSolverOpts), C.c_int32, P(C.c_int32),
                                           P(C.c_double)]),
         "karam_spice_parse": (C.c_int, [C.c_char_p, P(vp), C.c_char_p, C.c_int32]),
@@ -382,6 +384,19 @@ class Problem:
     def run_mc_device(self, dt=0.0, n_steps=0, method=A.TRAN_BE, opts=None):
         opts = opts or options()
         self._check(lib().karam_run_mc_device(self.h, C.byref(opts), dt, n_steps, method))
+
+    def ac_sweep(self, f_start, f_stop, n_points, input_node, amplitude=1.0):
+        """Small-signal AC sweep at every instance's DC point (karam_ac_sweep):
+        (frequencies[n_points], complex voltages [ni][n_points][n],
+        status [ni][n_points])."""
+        f = np.zeros(n_points)
+        re = np.zeros((self.ni, n_points, self.n))
+        im = np.zeros((self.ni, n_points, self.n))
+        st = np.zeros((self.ni, n_points), np.int32)
+        self._check(lib().karam_ac_sweep(self.h, f_start, f_stop, n_points, input_node, amplitude,
+                                         A.ptr(f, C.c_double), A.ptr(re, C.c_double),
+                                         A.ptr(im, C.c_double), A.ptr(st, C.c_int32)))
+        return f, re + 1j * im, st
 
     def tune_schedule(self, opts=None, rounds=16):
         """Measured factor/solve schedule (karam_tune_schedule): returns the

@@ -1643,6 +1643,102 @@ int karam_get_lu_schedule(const karam_problem* p, int32_t* buf, int64_t cap, int
   return KARAM_OK;
 }
 
+int karam_ac_sweep(karam_problem* p, double f_start, double f_stop, int32_t n_points,
+                   int32_t input_node, double amplitude, double* freqs_out, double* out_re,
+                   double* out_im, int32_t* status) {
+  if (!p || n_points < 1 || !out_re || !out_im) return KARAM_E_INVALID;
+  return guarded(p->ctx, [&] {
+    need_device(p);
+    if (!p->have_dc || p->tran_started)
+      throw std::logic_error("karam_ac_sweep needs a DC operating point (a DC-only solve first)");
+    const Topology& T = p->topo;
+    const int n = T.n, ni = p->ni;
+    const size_t ld = (size_t)p->ld;
+    if (input_node < 0 || input_node > n) throw std::runtime_error("input node out of range");
+    int stage = 0;
+    const size_t smem = plan_ac(p->dt, p->ctx->max_smem, &stage);
+    cudaGetLastError();
+    if (smem == 0) {
+      set_err(p->ctx, "AC needs the packed level program and its complex slots in one CTA's shared memory");
+      return KARAM_E_UNSUPPORTED;
+    }
+    // log-spaced frequencies, ACSolver::solveAC_Sparse's formula (ac_solver.h:724-729)
+    std::vector<double> f(n_points), w(n_points);
+    const double lo = std::log10(std::max(f_start, 1e-3));
+    const double hi = std::log10(std::max(f_stop, f_start + 1.0));
+    for (int k = 0; k < n_points; ++k) {
+      f[k] = std::pow(10.0, lo + (hi - lo) * k / std::max(n_points - 1, 1));
+      w[k] = 2.0 * M_PI * f[k];
+    }
+    if (freqs_out) std::copy(f.begin(), f.end(), freqs_out);
+    cudaStream_t s = p->ctx->stream;
+    // the FP64 Jacobian of every instance at its DC point
+    ck(cudaMemcpyAsync(p->i_x.p, p->i_v.p, (size_t)n * ld * sizeof(double), cudaMemcpyDeviceToDevice, s),
+       "copy v");
+    std::vector<double> evh(ld, -1.0), evt(ld, 0.0);
+    std::fill(evh.begin(), evh.begin() + ni, 0.0);
+    ck(cudaMemcpyAsync(p->i_evh.p, evh.data(), ld * sizeof(double), cudaMemcpyHostToDevice, s), "H2D ev");
+    ck(cudaMemcpyAsync(p->i_evt.p, evt.data(), ld * sizeof(double), cudaMemcpyHostToDevice, s), "H2D ev");
+    JobParams P = job_params(nullptr, 0, 0.0, KARAM_TRAN_BE);
+    P.precision = KARAM_PREC_FP64;
+    DevInst I = dev_inst(p);
+    const RoundLaunch L = plan_round(p->dt, ni, KARAM_PREC_FP64, p->ctx->max_smem, p->ctx->num_sms, 0);
+    if (L.L < 1) throw std::runtime_error(std::string("no evaluation schedule fits: ") + L.why);
+    DBuf d_w, d_re, d_im, d_st;
+    d_w.alloc((size_t)n_points * sizeof(double));
+    const size_t npts = (size_t)ni * n_points;
+    d_re.alloc(npts * n * sizeof(double));
+    d_im.alloc(npts * n * sizeof(double));
+    d_st.alloc(npts * sizeof(int));
+    ck(cudaMemcpyAsync(d_w.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s), "H2D omega");
+    p->timing = karam_timing{};
+    ck(cudaEventRecord(p->ev_job0, s), "event record");
+    launch_eval_stamp(p->dt, I, P, L, KARAM_PREC_FP64, s);
+    ck(cudaGetLastError(), "eval launch");
+    AcParams A{};
+    A.omega = d_w.as<double>();
+    A.n_points = n_points;
+    A.in_pos = input_node > 0 ? T.iperm[input_node - 1] : -1;
+    A.in_slot = A.in_pos >= 0 ? T.lu_hdr[4 * A.in_pos + 3] : -1;
+    A.stage_prog = stage;
+    A.g_in = 1e6;  // the excitation's Norton conductance (ac_solver.h:751-763)
+    A.rhs_in = 1e6 * amplitude;
+    A.gmin = 1e-12;
+    A.tiny = 1e-25;
+    A.growth = P.growth64;
+    A.perm = p->t_perm.as<int>();
+    A.out_re = d_re.as<double>();
+    A.out_im = d_im.as<double>();
+    A.status = d_st.as<int>();
+    launch_ac(p->dt, I, A, smem, s);
+    ck(cudaGetLastError(), "k_ac launch");
+    ck(cudaEventRecord(p->ev_job1, s), "event record");
+    ck(cudaMemcpyAsync(out_re, d_re.p, npts * n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ac");
+    ck(cudaMemcpyAsync(out_im, d_im.p, npts * n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ac");
+    std::vector<int> st_ac(npts);
+    ck(cudaMemcpyAsync(st_ac.data(), d_st.p, npts * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H status");
+    std::vector<InstState> st(ni);
+    ck(cudaMemcpyAsync(st.data(), p->i_st.p, ni * sizeof(InstState), cudaMemcpyDeviceToHost, s), "D2H state");
+    // every instance's evaluation point back to "done"
+    std::fill(evh.begin(), evh.end(), -1.0);
+    ck(cudaMemcpyAsync(p->i_evh.p, evh.data(), ld * sizeof(double), cudaMemcpyHostToDevice, s), "H2D ev");
+    ck(cudaStreamSynchronize(s), "ac sync");
+    float ms = 0;
+    ck(cudaEventElapsedTime(&ms, p->ev_job0, p->ev_job1), "ac time");
+    p->timing.job_ms = ms;
+    p->timing.eval_launches = 1;
+    p->timing.other_launches = 1;
+    if (status)
+      for (int g = 0; g < ni; ++g) {
+        // an instance whose DC point did not converge reports that status
+        const int dc = st[g].mode == MODE_DONE ? st[g].status : KARAM_ST_TIMEOUT;
+        for (int k = 0; k < n_points; ++k)
+          status[(size_t)g * n_points + k] = dc != KARAM_ST_CONVERGED ? dc : st_ac[(size_t)g * n_points + k];
+      }
+    return KARAM_OK;
+  });
+}
+
 int karam_eval_stamp(karam_problem* p, int32_t precision, const double* v, double* jac, double* f) {
   if (!p || !v) return KARAM_E_INVALID;
   return guarded(p->ctx, [&] {

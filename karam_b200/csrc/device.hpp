@@ -109,6 +109,13 @@ PersistPlan plan_persist_job(const DevTopo& T, int prec, const RescuePlan& R, in
 void launch_persist_multi(const PersistJob* jobs, int n_jobs, int prec, int grid, size_t smem,
                           int max_rounds, int* active, int* rounds_max, int* slot_timeouts,
                           cudaStream_t s);
+// Dynamic shared memory of the AC kernel (k_ac), or 0 when the problem has
+// no packed level program or its complex ND slots do not fit one CTA;
+// *stage_prog = 1 when the program fits beside them. Sets the kernel's
+// shared-memory limit (call outside stream capture).
+size_t plan_ac(const DevTopo& T, int max_smem, int* stage_prog);
+// One CTA per (frequency, instance): grid A.n_points x I.ni.
+void launch_ac(const DevTopo& T, const DevInst& I, const AcParams& A, size_t smem, cudaStream_t s);
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s);
 // [ni][n] FP32 per-device parameters (netlist order) into [n][ld] SoA order.

@@ -378,6 +378,33 @@ void launch_persist_multi(const PersistJob* jobs, int n_jobs, int prec, int grid
                                                                 rounds_max, slot_timeouts);
 }
 
+size_t plan_ac(const DevTopo& T, int max_smem, int* stage_prog) {
+  *stage_prog = 0;
+  if (T.nd_prog_len <= 0 || T.nd_levels <= 0) return 0;
+  const size_t slots = sizeof(double2) * ((size_t)T.nd_SY + (size_t)T.nd_S);
+  const size_t prog = sizeof(int) * (((size_t)T.nd_prog_len + 3) & ~size_t(3));
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k_ac) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  const size_t room = (size_t)max_smem - fa.sharedSizeBytes;
+  if (slots > room) return 0;
+  if (open_smem_limit((const void*)k_ac, max_smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (slots + prog <= room) {
+    *stage_prog = 1;
+    return slots + prog;
+  }
+  return std::max<size_t>(slots, 16);
+}
+
+void launch_ac(const DevTopo& T, const DevInst& I, const AcParams& A, size_t smem, cudaStream_t s) {
+  k_ac<<<dim3(A.n_points, I.ni), 256, smem, s>>>(T, I, A);
+}
+
 void unpermute(const double* v_perm, const int* perm, double* out, int ni, int ld, int n,
                cudaStream_t s) {
   k_unpermute<<<grid_for((size_t)n * ld, 256), 256, 0, s>>>(v_perm, perm, out, ni, ld, n);

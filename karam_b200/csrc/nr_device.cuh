@@ -3066,6 +3066,185 @@ __global__ void __launch_bounds__(kPersistThreads) k_persist_multi(const Persist
   }
 }
 
+// ---------------------------------------------------------------------------
+// Small-signal AC: complex static-pivot LU on the packed level program
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_recip(double2 a) {
+  const double den = a.x * a.x + a.y * a.y;
+  return make_double2(a.x / den, -a.y / den);
+}
+__device__ __forceinline__ double c_abs(double2 a) { return hypot(a.x, a.y); }
+
+// nd_solve_cta in complex arithmetic: the same packed program (ND slots A,
+// right-hand side y in ND positions, gmin on every diagonal first), pivots
+// replaced by their reciprocals, multipliers, target updates, forward and back
+// substitution level by level. False when a pivot is non-finite or below
+// tiny in magnitude, a solution value is non-finite, or a multiplier exceeds
+// growth_limit in magnitude.
+__device__ bool nd_solve_cta_c(double2* __restrict__ A, double2* __restrict__ y,
+                               const int* __restrict__ prog, double gmin, double tiny,
+                               double growth_limit) {
+  const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+  const int NL = prog[0], lvt = prog[1], tpb = prog[2], ypb = prog[3], bpb = prog[4];
+  bool ok = true;
+  double lmax = 0.0;
+  for (int lv = 0; lv < NL; ++lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    for (int q = tid; q < Lt[1]; q += bd) A[prog[Lt[0] + q]].x += gmin;
+  }
+  __syncthreads();
+  for (int lv = 0; lv < NL; ++lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    const int po = Lt[0], pc = Lt[1], lo = Lt[2], lc = Lt[3];
+    for (int q = tid; q < pc; q += bd) {
+      const int d = prog[po + q];
+      const double2 piv = A[d];
+      const double m = c_abs(piv);
+      ok = ok && isfinite(m) && !(m < tiny);
+      A[d] = c_recip(piv);
+    }
+    __syncthreads();
+    for (int e = tid; e < lc; e += bd) {
+      const int v = prog[lo + e];
+      const int sl = v & 0xFFFF;
+      const double2 l = c_mul(A[sl], A[(v >> 16) & 0xFFFF]);
+      A[sl] = l;
+      lmax = fmax(lmax, c_abs(l));
+    }
+    __syncthreads();
+    const int to = Lt[4], tsc = Lt[5], tlc = Lt[6];
+    for (int t = tid; t < tsc; t += bd) {
+      const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
+      const int sl = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
+      double2 acc = A[sl];
+      for (int q = 0; q < c; ++q) {
+        const int pr = prog[off + q];
+        acc = c_sub(acc, c_mul(A[pr & 0xFFFF], A[(pr >> 16) & 0xFFFF]));
+      }
+      A[sl] = acc;
+    }
+    const int yo = Lt[7], ysc = Lt[8], ylc = Lt[9];
+    for (int r = tid; r < ysc; r += bd) {
+      const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
+      const int row = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
+      double2 acc = y[row];
+      for (int q = 0; q < c; ++q) {
+        const int pr = prog[off + q];
+        acc = c_sub(acc, c_mul(A[pr & 0xFFFF], y[(pr >> 16) & 0xFFFF]));
+      }
+      y[row] = acc;
+    }
+    for (int t = tsc + warp; t < tsc + tlc; t += nw) {
+      const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
+      const int c = (h >> 16) & 0xFFFF;
+      double2 part = make_double2(0.0, 0.0);
+      for (int q = lane; q < c; q += 32) {
+        const int pr = prog[off + q];
+        part = c_add(part, c_mul(A[pr & 0xFFFF], A[(pr >> 16) & 0xFFFF]));
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        part.x += __shfl_xor_sync(kFull, part.x, o);
+        part.y += __shfl_xor_sync(kFull, part.y, o);
+      }
+      if (lane == 0) A[h & 0xFFFF] = c_sub(A[h & 0xFFFF], part);
+    }
+    for (int r = ysc + warp; r < ysc + ylc; r += nw) {
+      const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
+      const int c = (h >> 16) & 0xFFFF;
+      double2 part = make_double2(0.0, 0.0);
+      for (int q = lane; q < c; q += 32) {
+        const int pr = prog[off + q];
+        part = c_add(part, c_mul(A[pr & 0xFFFF], y[(pr >> 16) & 0xFFFF]));
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        part.x += __shfl_xor_sync(kFull, part.x, o);
+        part.y += __shfl_xor_sync(kFull, part.y, o);
+      }
+      if (lane == 0) y[h & 0xFFFF] = c_sub(y[h & 0xFFFF], part);
+    }
+    __syncthreads();
+  }
+  bool finite = true;
+  for (int lv = NL - 1; lv >= 0; --lv) {
+    const int* Lt = prog + lvt + 12 * lv;
+    const int bo = Lt[10], bc = Lt[11];
+    for (int q = tid; q < bc; q += bd) {
+      const int a = prog[bo + 2 * q], b = prog[bo + 2 * q + 1];
+      const int k = a & 0xFFFF, d = (a >> 16) & 0xFFFF;
+      const int c = b & 0xFFFF, off = bpb + ((b >> 16) & 0xFFFF);
+      double2 sv = y[k];
+      for (int j = 0; j < c; ++j) {
+        const int pr = prog[off + j];
+        sv = c_sub(sv, c_mul(A[pr & 0xFFFF], y[(pr >> 16) & 0xFFFF]));
+      }
+      sv = c_mul(sv, A[d]);
+      y[k] = sv;
+      finite = finite && isfinite(sv.x) && isfinite(sv.y);
+    }
+    __syncthreads();
+  }
+  return __syncthreads_and(ok && finite && !(lmax > growth_limit)) != 0;
+}
+
+// One AC point per CTA: blockIdx.x = frequency k, blockIdx.y = instance g.
+// Y(j w) from the instance's FP64 Jacobian value slots at its DC point (I.J,
+// lane g), plus j w C over each slot's capacitor terms (the transient
+// companions' lists), the input node's excitation conductance, and gmin on
+// every diagonal inside the solve. Dynamic shared memory: the right-hand side
+// [nd_SY] and the ND slots [nd_S] as double2, then (stage_prog) the packed
+// program.
+__global__ void __launch_bounds__(256) k_ac(DevTopo Tp, DevInst I, AcParams A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int k = blockIdx.x, g = blockIdx.y, tid = threadIdx.x, bd = blockDim.x;
+  if (k >= A.n_points || g >= I.ni) return;
+  double2* Y = reinterpret_cast<double2*>(smem_raw);
+  double2* S = Y + Tp.nd_SY;
+  const int* prog = Tp.nd_prog;
+  if (A.stage_prog) {
+    int* dst = reinterpret_cast<int*>(S + Tp.nd_S);
+    const int4* srcp = reinterpret_cast<const int4*>(Tp.nd_prog);
+    for (int e = tid; e < (Tp.nd_prog_len + 3) / 4; e += bd) reinterpret_cast<int4*>(dst)[e] = __ldg(&srcp[e]);
+    prog = dst;
+  }
+  const double w = A.omega[k];
+  const size_t ld = I.ld;
+  const double* J = reinterpret_cast<const double*>(I.J);
+  for (int sl = tid; sl < Tp.nd_S; sl += bd) {
+    double2 a = make_double2(0.0, 0.0);
+    const int src = sl < Tp.nd_nv ? __ldg(&Tp.nd_src[sl]) : -1;
+    if (src >= 0) {
+      double c = 0.0;
+      const int q1 = __ldg(&Tp.jcap_off[src + 1]);
+      for (int q = __ldg(&Tp.jcap_off[src]); q < q1; ++q) {
+        const int cc = __ldg(&Tp.jcap_code[q]);
+        const double C = __ldg(&Tp.cap_c[code_idx(cc)]);
+        c = cc < 0 ? c - C : c + C;
+      }
+      a.x = J[(size_t)src * ld + g] + (src == A.in_slot ? A.g_in : 0.0);
+      a.y = w * c;
+    }
+    S[sl] = a;
+  }
+  for (int i = tid; i < Tp.nd_SY; i += bd) Y[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  if (tid == 0 && A.in_pos >= 0) Y[__ldg(&Tp.nd_pos[A.in_pos])] = make_double2(A.rhs_in, 0.0);
+  __syncthreads();
+  const bool ok = nd_solve_cta_c(S, Y, prog, A.gmin, A.tiny, A.growth);
+  const size_t base = ((size_t)g * A.n_points + k) * (size_t)Tp.n;
+  for (int i = tid; i < Tp.n; i += bd) {
+    const double2 v = ok ? Y[__ldg(&Tp.nd_pos[i])] : make_double2(0.0, 0.0);
+    const size_t o = base + __ldg(&A.perm[i]);
+    A.out_re[o] = v.x;
+    A.out_im[o] = v.y;
+  }
+  if (tid == 0) A.status[(size_t)g * A.n_points + k] = ok ? KST_CONVERGED : KST_SINGULAR;
+}
+
 // Moves every converged instance into the transient at step 1 (capacitor
 // history from the accepted point when init_caps). Thread per instance.
 __global__ void k_tran_start(DevTopo T, DevInst I, JobParams P, int init_caps) {

@@ -262,4 +262,23 @@ struct PersistJob {
   int* slot_lock;
 };
 
+// One small-signal AC sweep (k_ac): CTA (k, g) solves Y(j omega[k]) x = b for
+// instance g. in_slot: value slot of the input node's diagonal, which gets
+// g_in; in_pos: the input node's Min-Fill index, whose right-hand side is
+// rhs_in (both -1 without excitation). Results go to out_re / out_im
+// [ni][n_points][n] in node order (perm: Min-Fill index -> node index) and
+// status [ni][n_points]. stage_prog: the packed level program is copied into
+// shared memory after the slots (else read from global memory).
+struct AcParams {
+  const double* omega;
+  int n_points;
+  int in_slot, in_pos;
+  int stage_prog;
+  double g_in, rhs_in, gmin, tiny, growth;
+  const int* perm;
+  double* out_re;
+  double* out_im;
+  int* status;
+};
+
 #endif

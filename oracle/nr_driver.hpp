@@ -527,4 +527,60 @@ struct Driver {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Small-signal AC (ACSolver::solveAC_Sparse, solvers/ac_solver.h:711-773)
+// ---------------------------------------------------------------------------
+
+// Log-spaced sweep frequencies, solveAC_Sparse's formula (ac_solver.h:724-729).
+inline std::vector<double> ac_frequencies(double f_start, double f_stop, int n_points) {
+  std::vector<double> f(n_points > 0 ? n_points : 0);
+  const double lo = std::log10(std::max(f_start, 1e-3));
+  const double hi = std::log10(std::max(f_stop, f_start + 1.0));
+  for (int i = 0; i < n_points; ++i)
+    f[i] = std::pow(10.0, lo + (hi - lo) * i / std::max(n_points - 1, 1));
+  return f;
+}
+
+// Position of (r, c) in the pattern's row r, or -1.
+inline int csr_at(const Csr& p, int r, int c) {
+  for (int q = p.row_ptr[r]; q < p.row_ptr[r + 1]; ++q)
+    if (p.col[q] == c) return q;
+  return -1;
+}
+
+// Y(jw) on the stamp pattern p at one frequency w: the real part is the NR
+// Jacobian at the DC point (jac, without gmin) plus 1e-12 on every diagonal
+// (the conditioning of ac_solver.h:701-702) plus the excitation's 1e6 at the
+// input node's diagonal (ac_solver.h:751-763); the imaginary part is w C from
+// each capacitor's four stamps (ac_solver.h:658-660). rhs_re: 1e6 * amplitude
+// at the input node. Nodes are 1-based, 0 = ground.
+inline void ac_matrix(const Csr& p, const std::vector<double>& jac, const std::vector<int>& cap_n1,
+                      const std::vector<int>& cap_n2, const std::vector<double>& cap_c, double w,
+                      int input_node, double amplitude, std::vector<double>& re,
+                      std::vector<double>& im, std::vector<double>& rhs_re) {
+  const int n = p.n;
+  re = jac;
+  im.assign(jac.size(), 0.0);
+  rhs_re.assign(n, 0.0);
+  auto add_im = [&](int a, int b, double y) {
+    if (a <= 0 || b <= 0) return;
+    const int q = csr_at(p, a - 1, b - 1);
+    if (q >= 0) im[q] += y;
+  };
+  for (size_t k = 0; k < cap_c.size(); ++k) {
+    const double y = w * cap_c[k];
+    const int a = cap_n1[k], b = cap_n2[k];
+    add_im(a, a, y);
+    add_im(a, b, -y);
+    add_im(b, a, -y);
+    add_im(b, b, y);
+  }
+  for (int i = 0; i < n; ++i) re[p.diag[i]] += 1e-12;
+  if (input_node > 0 && input_node <= n) {
+    const double g_large = 1e6;
+    re[p.diag[input_node - 1]] += g_large;
+    rhs_re[input_node - 1] += g_large * amplitude;
+  }
+}
+
 }  // namespace oracle

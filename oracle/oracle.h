@@ -135,6 +135,22 @@ int oracle_run_batch(const karam_netlist *nl, const karam_instances *inst, int32
                      int32_t i1, const oracle_opts *opts, double dt, int32_t n_steps,
                      int32_t method, int32_t n_threads, double *v_out, oracle_stats *st);
 
+/* Small-signal AC sweep at the DC point v_dc[n] of instance idx
+ * (ACSolver::solveAC_Sparse, solvers/ac_solver.h:711-773): n_points
+ * log-spaced frequencies from f_start to f_stop (its formula), and at each
+ * Y(jw) x = b solved by LU with partial pivoting on the complex magnitude
+ * (solveComplexLU_Sparse, math/linalg.h:993-1078), with the input node
+ * driven through 1e6 S at amplitude volts. rule 1: Y = the NR Jacobian at
+ * v_dc (the stamps of physics/circuitsim.h:2413-2751, device conductances of
+ * the instance's own models) + jwC + 1e-12 on every diagonal. rule 0
+ * (reference build only): the reference's own admittance build
+ * (buildAdmittanceMatrixSparse, ac_solver.h:618-704). out_re / out_im
+ * [n_points][n]. Returns the number of points whose matrix was singular. */
+int oracle_ac(const karam_netlist *nl, const karam_instances *inst, int32_t idx,
+              const double *v_dc, double f_start, double f_stop, int32_t n_points,
+              int32_t input_node, double amplitude, int32_t rule, double *out_re,
+              double *out_im);
+
 #ifdef __cplusplus
 }
 #endif

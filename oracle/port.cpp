@@ -687,6 +687,85 @@ int guarded(F f) {
   }
 }
 
+// solveComplexLU_Sparse (math/linalg.h:993-1078) restated: the CSR values
+// into a dense row-major matrix, LU with partial pivoting on the complex
+// magnitude (hypot; on equal magnitudes the earlier row), rows swapped with
+// the right-hand side, multipliers by complex division over |d|^2, forward
+// substitution with the unit lower factor, back substitution. Returns false
+// when a pivot's magnitude is below 1e-25 (rank deficient).
+bool complex_lu_solve(const oracle::Csr& p, const std::vector<double>& vre,
+                      const std::vector<double>& vim, const std::vector<double>& rre,
+                      const std::vector<double>& rim, std::vector<double>& xre,
+                      std::vector<double>& xim) {
+  const int n = p.n;
+  xre.assign(n, 0.0);
+  xim.assign(n, 0.0);
+  if (n == 0) return true;
+  std::vector<double> Are((size_t)n * n, 0.0), Aim((size_t)n * n, 0.0);
+  for (int r = 0; r < n; ++r)
+    for (int q = p.row_ptr[r]; q < p.row_ptr[r + 1]; ++q) {
+      Are[(size_t)r * n + p.col[q]] = vre[q];
+      Aim[(size_t)r * n + p.col[q]] = vim[q];
+    }
+  std::vector<double> bre(rre), bim(rim);
+  for (int i = 0; i < n; ++i) {
+    double best = 0.0;
+    int row = i;
+    for (int k = i; k < n; ++k) {
+      const double mag = std::hypot(Are[(size_t)k * n + i], Aim[(size_t)k * n + i]);
+      if (mag > best) {
+        best = mag;
+        row = k;
+      } else if (mag == best && k < row) {
+        row = k;
+      }
+    }
+    if (best < 1e-25) return false;
+    if (row != i) {
+      for (int k = 0; k < n; ++k) {
+        std::swap(Are[(size_t)i * n + k], Are[(size_t)row * n + k]);
+        std::swap(Aim[(size_t)i * n + k], Aim[(size_t)row * n + k]);
+      }
+      std::swap(bre[i], bre[row]);
+      std::swap(bim[i], bim[row]);
+    }
+    const double dre = Are[(size_t)i * n + i], dim = Aim[(size_t)i * n + i];
+    const double den = dre * dre + dim * dim;
+    for (int j = i + 1; j < n; ++j) {
+      const double ar = Are[(size_t)j * n + i], ai = Aim[(size_t)j * n + i];
+      const double fre = (ar * dre + ai * dim) / den;
+      const double fim = (ai * dre - ar * dim) / den;
+      Are[(size_t)j * n + i] = fre;
+      Aim[(size_t)j * n + i] = fim;
+      for (int k = i + 1; k < n; ++k) {
+        Are[(size_t)j * n + k] -= fre * Are[(size_t)i * n + k] - fim * Aim[(size_t)i * n + k];
+        Aim[(size_t)j * n + k] -= fre * Aim[(size_t)i * n + k] + fim * Are[(size_t)i * n + k];
+      }
+    }
+  }
+  std::vector<double> yre(n), yim(n);
+  for (int i = 0; i < n; ++i) {
+    yre[i] = bre[i];
+    yim[i] = bim[i];
+    for (int j = 0; j < i; ++j) {
+      yre[i] -= Are[(size_t)i * n + j] * yre[j] - Aim[(size_t)i * n + j] * yim[j];
+      yim[i] -= Are[(size_t)i * n + j] * yim[j] + Aim[(size_t)i * n + j] * yre[j];
+    }
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double sre = yre[i], sim = yim[i];
+    for (int j = i + 1; j < n; ++j) {
+      sre -= Are[(size_t)i * n + j] * xre[j] - Aim[(size_t)i * n + j] * xim[j];
+      sim -= Are[(size_t)i * n + j] * xim[j] + Aim[(size_t)i * n + j] * xre[j];
+    }
+    const double dre = Are[(size_t)i * n + i], dim = Aim[(size_t)i * n + i];
+    const double den = dre * dre + dim * dim;
+    xre[i] = (sre * dre + sim * dim) / den;
+    xim[i] = (sim * dre - sre * dim) / den;
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -886,6 +965,33 @@ int oracle_run_batch(const karam_netlist* nl, const karam_instances* inst, int32
     }
     for (auto& th : pool) th.join();
     return 0;
+  });
+}
+
+int oracle_ac(const karam_netlist* nl, const karam_instances* inst, int32_t idx, const double* v_dc,
+              double f_start, double f_stop, int32_t n_points, int32_t input_node, double amplitude,
+              int32_t rule, double* out_re, double* out_im) {
+  return guarded([&] {
+    if (rule != 1) throw std::runtime_error("the port restates the Jacobian rule (1) only");
+    Session s(nl, inst, idx);
+    auto& b = s.b;
+    std::vector<double> v(v_dc, v_dc + b.n), z(b.cap_c.size(), 0.0), jac, rhs;
+    b.stamp(v, 0.0, KARAM_TRAN_BE, z, z, 0.0, jac, rhs);
+    const std::vector<double> f = oracle::ac_frequencies(f_start, f_stop, n_points);
+    int singular = 0;
+    std::vector<double> re, im, rre, rim(b.n, 0.0), xre, xim;
+    for (int k = 0; k < n_points; ++k) {
+      oracle::ac_matrix(b.pat, jac, b.cap_n1, b.cap_n2, b.cap_c, 2.0 * M_PI * f[k], input_node,
+                        amplitude, re, im, rre);
+      if (!complex_lu_solve(b.pat, re, im, rre, rim, xre, xim)) {
+        ++singular;
+        std::fill(xre.begin(), xre.end(), 0.0);
+        std::fill(xim.begin(), xim.end(), 0.0);
+      }
+      std::copy(xre.begin(), xre.end(), out_re + (size_t)k * b.n);
+      std::copy(xim.begin(), xim.end(), out_im + (size_t)k * b.n);
+    }
+    return singular;
   });
 }
 

@@ -94,6 +94,9 @@ class Oracle:
                                        C.c_int32, C.c_int32, C.POINTER(OracleOpts), C.c_double,
                                        C.c_int32, C.c_int32, C.c_int32, _f64p,
                                        C.POINTER(OracleStats)]
+        L.oracle_ac.argtypes = [C.POINTER(A.KaramNetlist), C.POINTER(A.KaramInstances), C.c_int32,
+                                _f64p, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double,
+                                C.c_int32, _f64p, _f64p]
 
     def opts(self, **kw):
         o = OracleOpts()
@@ -201,6 +204,20 @@ class Oracle:
                                       A.ptr(v0a, C.c_double), A.ptr(v, C.c_double), C.byref(st))
         assert rc == 0
         return v, st.as_dict()
+
+    def ac(self, nl, v_dc, f_start, f_stop, n_points, input_node, amplitude=1.0, inst=None, idx=0,
+           rule=1):
+        """Small-signal AC sweep at the DC point v_dc (oracle_ac): complex node
+        voltages [n_points][n] and the number of singular points."""
+        s = nl.as_struct()
+        v = np.ascontiguousarray(v_dc, np.float64)
+        re = np.zeros((n_points, s.n_nodes))
+        im = np.zeros((n_points, s.n_nodes))
+        rc = self.lib.oracle_ac(C.byref(s), self._inst(inst), idx, A.ptr(v, C.c_double), f_start,
+                                f_stop, n_points, input_node, amplitude, rule,
+                                A.ptr(re, C.c_double), A.ptr(im, C.c_double))
+        assert rc >= 0, rc
+        return re + 1j * im, rc
 
     def transient(self, nl, v_start, dt, n_steps, method=A.TRAN_BE, inst=None, idx=0,
                   wave_nodes=None, **opt):

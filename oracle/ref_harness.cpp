@@ -19,6 +19,7 @@
 #include "acutesim_engine/infrastructure/treewidth_analyzer.h"
 #include "acutesim_engine/math/sparse_lu.h"
 #include "acutesim_engine/math/portable_rng.h"
+#include "acutesim_engine/solvers/ac_solver.h"
 
 #include <algorithm>
 #include <cmath>
@@ -522,6 +523,50 @@ int oracle_ref_normals(uint64_t seed, double mean, double sd, int32_t count, dou
   acutesim::math::PortableNormalDist dist(mean, sd);
   for (int32_t i = 0; i < count; ++i) out[i] = dist(rng);
   return 0;
+}
+
+int oracle_ac(const karam_netlist* nl, const karam_instances* inst, int32_t idx, const double* v_dc,
+              double f_start, double f_stop, int32_t n_points, int32_t input_node, double amplitude,
+              int32_t rule, double* out_re, double* out_im) {
+  return guarded([&] {
+    Session s(nl, inst, idx);
+    auto& b = s.b;
+    const int n = b.n;
+    std::vector<double> v(v_dc, v_dc + n);
+    int singular = 0;
+    if (rule == 0) {  // the reference's sweep as it stands
+      ACSolver::ACResult r =
+          ACSolver::solveAC_Sparse(b.net, v, f_start, f_stop, n_points, input_node, amplitude);
+      for (int k = 0; k < n_points; ++k)
+        for (int i = 0; i < n; ++i) {
+          out_re[(size_t)k * n + i] = r.nodeVoltages[k][i].real();
+          out_im[(size_t)k * n + i] = r.nodeVoltages[k][i].imag();
+        }
+      return 0;
+    }
+    // the NR Jacobian of the reference's stamps at the DC point, solved by
+    // the reference's complex LU
+    std::vector<double> z(b.cap_c.size(), 0.0), jac, rhs;
+    b.stamp(v, 0.0, KARAM_TRAN_BE, z, z, 0.0, jac, rhs);
+    const std::vector<double> f = oracle::ac_frequencies(f_start, f_stop, n_points);
+    std::vector<double> re, im, rre, rim(n, 0.0);
+    for (int k = 0; k < n_points; ++k) {
+      oracle::ac_matrix(b.pat, jac, b.cap_n1, b.cap_n2, b.cap_c, 2.0 * M_PI * f[k], input_node,
+                        amplitude, re, im, rre);
+      ComplexCsr Y;
+      Y.rows = Y.cols = n;
+      Y.nnz = (int)b.pat.col.size();
+      Y.row_pointer = b.pat.row_ptr;
+      Y.col_indices = b.pat.col;
+      Y.values_real = re;
+      Y.values_imag = im;
+      ComplexSolverResult sol = solveComplexLU_Sparse(Y, rre, rim);
+      if (sol.rankDeficient && !sol.converged) ++singular;
+      std::copy(sol.solution_real.begin(), sol.solution_real.end(), out_re + (size_t)k * n);
+      std::copy(sol.solution_imag.begin(), sol.solution_imag.end(), out_im + (size_t)k * n);
+    }
+    return singular;
+  });
 }
 
 }  // extern "C"

@@ -61,6 +61,30 @@ def grid8():
     return circuits.grid_circuit(8)
 
 
+def rc_ladder_diodes():
+    """RC ladder from a 1 V source with forward-biased diode clamps at every
+    fourth node and 1 pF to ground everywhere: no MOSFETs and no diode near
+    its conductance floor, so the reference's own AC admittance build and the
+    NR-Jacobian rule coincide (the AC pinning case)."""
+    nl = Netlist()
+    nl.vsource(1, 0, 1.0)
+    for k in range(1, 12):
+        nl.resistor(k, k + 1, 1e3)
+    for k in range(1, 13):
+        nl.capacitor(k, 0, 1e-12)
+    for k in (4, 8, 12):
+        nl.diode(k, 0, 1e-14, 1.0)
+    return nl
+
+
+# AC sweeps of the fixtures: (netlist, input node, f_start, f_stop, points)
+AC_CASES = {
+    "rc_ladder_diodes": (rc_ladder_diodes, 1, 1e3, 1e11, 17),
+    "diode_rc": (diode_rc, 1, 1e6, 1e13, 15),
+    "grid8": (grid8, 1, 1e5, 1e11, 13),
+    "config2": (circuits.config2, 2, 1e6, 1e12, 13),
+}
+
 SMALL = {
     "divider": divider,
     "floating_source": floating_source,

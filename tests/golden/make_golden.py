@@ -8,11 +8,13 @@ Every array comes from reference code: the stamp pattern and slot map
 tensorizeNetlist, the Min-Fill ordering (FactorGraph + TreewidthAnalyzer), the
 filled pattern of symbolicFactorize, the stamps of stampSoABlock, the NR
 solutions of the oracle driver over those stamps and solveLU_Pivoted /
-solveSparse_LU, and PortableNormalDist draws.
+solveSparse_LU, PortableNormalDist draws, and AC sweeps solved by
+solveComplexLU_Sparse (and by ACSolver::solveAC_Sparse as it stands).
 
     python tests/golden/make_golden.py          # rewrites tests/golden/*.npz
     python tests/golden/make_golden.py grid8    # only the named cases
     python tests/golden/make_golden.py grid64   # a large grid (minutes: dense-workspace LU)
+    python tests/golden/make_golden.py ac_grid8 # one AC sweep fixture (ac_<case>)
 """
 import os
 import sys
@@ -95,6 +97,25 @@ def grid_fixture(ref, name, N):
           out["dc_stats"].tolist(), "tran stats", out["tran_stats"].tolist(), flush=True)
 
 
+def ac_fixture(ref, name):
+    """Small-signal AC sweep at a DC point, from the reference build: the
+    NR-Jacobian rule (the reference's stamps at the DC point + jwC, solved by
+    the reference's solveComplexLU_Sparse) and the reference's own admittance
+    build (ACSolver::solveAC_Sparse as it stands)."""
+    make, node, f0, f1, npts = cases.AC_CASES[name]
+    nl = make()
+    inst = circuits.mc_instances(nl, 2) if nl.n_mos else None
+    v, st = ref.solve_dc(nl, inst, 0, linear_solver=pyoracle.LS_SPARSE, **POLISH)
+    x1, s1 = ref.ac(nl, v, f0, f1, npts, node, inst=inst, idx=0, rule=1)
+    x0, _ = ref.ac(nl, v, f0, f1, npts, node, inst=inst, idx=0, rule=0)
+    out = dict(v_dc=v, dc_stats=stats_arr(st), x_rule1=x1, x_rule0=x0, singular=np.int64(s1),
+               sweep=np.array([f0, f1, npts, node], np.float64))
+    if inst is not None:
+        out["mc_kp"], out["mc_vto"] = inst.mos_kp, inst.mos_vto
+    np.savez_compressed(os.path.join(HERE, f"ac_{name}.npz"), **out)
+    print(f"ac_{name}", "n =", nl.n_nodes, "dc", stats_arr(st).tolist(), "singular", s1, flush=True)
+
+
 def stats_arr(st):
     keys = ("converged", "iterations", "polish_iters", "damped", "gmin_step", "singular")
     return np.array([st[k] for k in keys], np.int64)
@@ -119,6 +140,10 @@ def main():
         np.savez_compressed(os.path.join(HERE, "rng_normals.npz"), seeds=seeds, normals=normals)
 
     only = set(sys.argv[1:])  # case names to regenerate (default: all)
+    for name in cases.AC_CASES:
+        if only and f"ac_{name}" not in only:
+            continue
+        ac_fixture(ref, name)
     for name, N in cases.GRIDS.items():
         if only and name not in only:
             continue
