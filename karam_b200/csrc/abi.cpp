@@ -170,13 +170,6 @@ int guarded(karam_ctx* c, F f) {
   }
 }
 
-// Up to this many unknowns, the block-per-instance kernels factor and solve
-// on the packed program with one warp (nd_solve, __syncwarp between phases)
-// instead of the whole CTA (nd_solve_cta): the levels are a few items wide,
-// and the barriers of a 512-thread CTA cost more than the work. The two give
-// the same results bit for bit.
-constexpr int kWarpSolveMaxN = 96;
-
 void upload_topology(karam_problem* p) {
   const Topology& T = p->topo;
   std::vector<int4> mt;
@@ -396,7 +389,6 @@ void upload_topology(karam_problem* p) {
   }
   d.nd_prog = nullptr;
   d.nd_prog_len = 0;
-  d.nd_warp_solve = T.n <= kWarpSolveMaxN ? 1 : 0;
   if (!T.nd_prog.empty()) {
     std::vector<int> pg = T.nd_prog;
     pg.resize((pg.size() + 3) / 4 * 4, 0);

@@ -2024,15 +2024,8 @@ __device__ void lu_big_instance(const DevTopo& Tp, const DevInst& I, const JobPa
   if (a & ACT_SOLVE) {
     const T tiny = sizeof(T) == 8 ? (T)1e-25 : (T)1e-30;
     const T growth = sizeof(T) == 8 ? (T)P.growth64 : (T)fmin(P.growth32, 3.0e38);
-    bool ok;
-    if (packed && Tp.nd_warp_solve) {  // warp 0 alone; the barrier publishes its result
-      bool w = false;
-      if (tid < 32) w = nd_solve<T>(A, Y, prog, (T)gmin, tiny, growth, tid);
-      ok = __syncthreads_or(tid == 0 && w) != 0;
-    } else {
-      ok = packed ? nd_solve_cta<T>(A, Y, prog, (T)gmin, tiny, growth)
-                  : big_solve<T>(A, Y, Tp, (T)gmin, tiny, growth);
-    }
+    const bool ok = packed ? nd_solve_cta<T>(A, Y, prog, (T)gmin, tiny, growth)
+                           : big_solve<T>(A, Y, Tp, (T)gmin, tiny, growth);
     // x = v + dx, then junction limiting level by level
     if (ok) {
       for (int i = tid; i < n; i += blockDim.x) {

@@ -172,8 +172,6 @@ struct DevTopo {
   const int *bs_off, *bs_u, *bs_c;
   const int* nd_prog;       // the schedule packed for shared memory (nd_program)
   int nd_prog_len;          // ints (0: the level-scheduled kernel is not used)
-  int nd_warp_solve;        // 1: block-per-instance kernels run the packed factor/solve on
-                            // one warp (small problems: its levels are a few items wide)
   const int2* slot_rc;      // (row, col) of every value slot (permuted)
   const int* slot_ptr;      // [n + 1] first slot of each row (columns ascending within a row)
   const int* csc_ptr;       // [n + 1] value slots by column: (row, slot) in csc_ent
