@@ -28,7 +28,7 @@ void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678f)); }
+__device__ __forceinline__ float gelu(float z) { return seeder_gelu(z); }
 __device__ __forceinline__ float gelu_d(float z) {
   return 0.5f * (1.0f + erff(z * 0.70710678f)) + z * 0.39894228f * expf(-0.5f * z * z);
 }
@@ -98,6 +98,18 @@ __global__ void k_norm_rows(const float* src, const int* idx, int rows, int cols
   }
 }
 
+// k_norm_rows into a K-major BF16 operand [rows][ld] (the first layer's A):
+// the same FP32 arithmetic, rounded to BF16 as the GEMM's operand copy would.
+__global__ void k_norm_rows_bf16(const float* src, int rows, int cols, const float* mean,
+                                 const float* istd, __nv_bfloat16* out, int ld) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / cols), j = (int)(e - (size_t)r * cols);
+    out[(size_t)r * ld + j] = __float2bfloat16_rn((src[(size_t)r * cols + j] - mean[j]) * istd[j]);
+  }
+}
+
 // Column mean and 1 / standard deviation (0 for a constant column).
 __global__ void k_col_stats(const float* X, int rows, int cols, float* mean, float* istd,
                             float* sd) {
@@ -159,6 +171,30 @@ struct Buf {
   }
 };
 
+struct BBuf {  // device BF16 array
+  __nv_bfloat16* p = nullptr;
+  size_t n = 0;
+  void need(size_t count) {
+    if (count <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = count;
+    ck(cudaMalloc(&p, count * sizeof(__nv_bfloat16)), "seeder alloc");
+  }
+  BBuf() = default;
+  BBuf(const BBuf&) = delete;
+  BBuf& operator=(const BBuf&) = delete;
+  BBuf(BBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  ~BBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+inline int pad8(int k) { return (k + 7) & ~7; }
+
 // BF16 copies of a GEMM's operands and its kernel's error flag.
 struct GemmWs {
   __nv_bfloat16* a = nullptr;
@@ -182,6 +218,13 @@ struct GemmWs {
       ck(cudaMalloc(&err, sizeof(int)), "seeder gemm flag");
       ck(cudaMemset(err, 0, sizeof(int)), "seeder gemm flag");
     }
+  }
+  int* err_flag() {
+    if (!err) {
+      ck(cudaMalloc(&err, sizeof(int)), "seeder gemm flag");
+      ck(cudaMemset(err, 0, sizeof(int)), "seeder gemm flag");
+    }
+    return err;
   }
   ~GemmWs() {
     if (a) cudaFree(a);
@@ -207,6 +250,10 @@ struct Mlp {
   int idx_cap = 0;
   long step = 0;
   GemmWs ws;
+  // inference: K-major BF16 weights ([N][pad8(K)] per layer, converted again
+  // when training has changed them) and BF16 activations ([rows][pad8(K)])
+  std::vector<BBuf> wbf, abf;
+  long wbf_step = -1;
   ~Mlp() {
     if (idx) cudaFree(idx);
   }
@@ -403,18 +450,53 @@ float mlp_train(Mlp* m, int epochs, int batch, float lr, uint64_t shuffle_seed, 
   return last;
 }
 
+// Inference: the first layer's input normalised straight into BF16, then one
+// tcgen05 GEMM per layer whose epilogue adds the bias and applies GELU while
+// writing the next layer's BF16 operand (the last layer writes FP32). The
+// values are those of the training forward pass (the same FP32 bias add and
+// GELU, rounded to BF16 where that pass converts its activations).
 void mlp_predict(Mlp* m, const float* dX, int n, double* out, int out_ld, cudaStream_t s) {
   if (!m->normed) throw std::runtime_error("seeder: not trained");
-  const int ni = m->dims.front(), no = m->dims.back();
+  const int ni = m->dims.front(), no = m->dims.back(), L = m->L;
   const int chunk = std::max(m->bcap, std::min(n, 4096));
   ensure_batch(m, chunk);
+  if ((int)m->wbf.size() != L) {
+    m->wbf.clear();
+    m->abf.clear();
+    for (int l = 0; l < L; ++l) {
+      m->wbf.emplace_back();
+      m->abf.emplace_back();
+    }
+    m->wbf_step = -1;
+  }
+  if (m->wbf_step != m->step) {
+    for (int l = 0; l < L; ++l) {
+      const int K = m->dims[l], N = m->dims[l + 1];
+      m->wbf[l].need((size_t)N * pad8(K));
+      to_bf16(m->W[l].p, N, 1, N, K, m->wbf[l].p, pad8(K), s);  // B[n][k] = W[k][n]
+    }
+    m->wbf_step = m->step;
+  }
+  for (int l = 0; l < L; ++l) m->abf[l].need((size_t)chunk * pad8(m->dims[l]));
   for (int r0 = 0; r0 < n; r0 += chunk) {
     const int B = std::min(chunk, n - r0);
-    k_norm_rows<<<grid_for((size_t)B * ni), 256, 0, s>>>(dX + (size_t)r0 * ni, nullptr, B, ni, m->fmean.p,
-                                                         m->fistd.p, m->act[0].p);
-    forward(m, B, s);
+    k_norm_rows_bf16<<<grid_for((size_t)B * ni), 256, 0, s>>>(dX + (size_t)r0 * ni, B, ni, m->fmean.p,
+                                                              m->fistd.p, m->abf[0].p, pad8(ni));
+    for (int l = 1; l <= L; ++l) {
+      const int K = m->dims[l - 1], N = m->dims[l];
+      TcEpilogue ep;
+      ep.bias = m->b[l - 1].p;
+      if (l < L) {
+        ep.gelu = 1;
+        ep.out_bf16 = m->abf[l].p;
+        ep.ld_out = pad8(N);
+      }
+      ck(tc_gemm_bf16(B, N, K, m->abf[l - 1].p, pad8(K), m->wbf[l - 1].p, pad8(K),
+                      l < L ? nullptr : m->pre[L].p, N, 0, m->ws.err_flag(), s, &ep),
+         "tcgen05 gemm launch");
+    }
     double* o = out_ld > 0 ? out + r0 : out + (size_t)r0 * no;
-    k_denorm<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[m->L].p, B, no, m->tmean.p, m->tsd.p, o, out_ld);
+    k_denorm<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[L].p, B, no, m->tmean.p, m->tsd.p, o, out_ld);
   }
   ck(cudaGetLastError(), "seeder predict launch");
 }

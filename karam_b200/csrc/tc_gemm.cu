@@ -132,7 +132,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 __global__ void __launch_bounds__(128) k_gemm_tc(const __grid_constant__ CUtensorMap ta,
                                                  const __grid_constant__ CUtensorMap tb, int M,
                                                  int N, int K, float* __restrict__ C, int ldc,
-                                                 int acc, int* err) {
+                                                 int acc, int* err, TcEpilogue ep) {
   extern __shared__ unsigned char tc_raw[];
   const uint32_t pad = (1024u - (sm_addr(tc_raw) & 1023u)) & 1023u;
   TcSmem* S = reinterpret_cast<TcSmem*>(tc_raw + pad);
@@ -207,8 +207,27 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __grid_constant__ CUtenso
       float v[32];
       tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       if (row >= M) continue;
-      float* crow = C + (size_t)row * ldc + n0 + c0;
       const int nv = N - (n0 + c0);
+      if (nv <= 0) continue;
+      if (ep.bias)
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += j < nv ? __ldg(&ep.bias[n0 + c0 + j]) : 0.0f;
+      if (ep.out_bf16) {
+        __nv_bfloat16* orow = ep.out_bf16 + (size_t)row * ep.ld_out + n0 + c0;
+        if (nv >= 32) {  // 16-byte stores: ld_out and the column offset are multiples of 8
+#pragma unroll
+          for (int j = 0; j < 32; j += 8) {
+            __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16_rn(ep.gelu ? seeder_gelu(v[j + q]) : v[j + q]);
+            *reinterpret_cast<uint4*>(orow + j) = *reinterpret_cast<const uint4*>(h);
+          }
+        } else {
+          for (int j = 0; j < nv; ++j) orow[j] = __float2bfloat16_rn(ep.gelu ? seeder_gelu(v[j]) : v[j]);
+        }
+      }
+      if (!C) continue;
+      float* crow = C + (size_t)row * ldc + n0 + c0;
       if (vec && nv >= 32) {
 #pragma unroll
         for (int j = 0; j < 32; j += 4) {
@@ -298,10 +317,14 @@ bool kmajor_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int K, in
 
 cudaError_t tc_gemm_bf16(int M, int N, int K, const __nv_bfloat16* A, int lda,
                          const __nv_bfloat16* B, int ldb, float* C, int ldc, int acc, int* err,
-                         cudaStream_t s) {
+                         cudaStream_t s, const TcEpilogue* ep) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  const TcEpilogue e = ep ? *ep : TcEpilogue{};
+  if (e.out_bf16 && ((e.ld_out & 7) || (reinterpret_cast<uintptr_t>(e.out_bf16) & 15)))
+    return cudaErrorInvalidValue;  // the epilogue's 16-byte stores
+  if (!C && !e.out_bf16) return cudaErrorInvalidValue;
   if (K <= 0) {  // an empty sum
-    if (acc) return cudaSuccess;
+    if (acc || e.bias || e.out_bf16) return cudaErrorInvalidValue;
     return cudaMemset2DAsync(C, (size_t)ldc * sizeof(float), 0, (size_t)N * sizeof(float), M, s);
   }
   if ((lda & 7) || (ldb & 7) || (reinterpret_cast<uintptr_t>(A) & 15) ||
@@ -317,7 +340,7 @@ cudaError_t tc_gemm_bf16(int M, int N, int K, const __nv_bfloat16* A, int lda,
   });
   if (ea != cudaSuccess) return ea;
   const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
-  k_gemm_tc<<<grid, 128, smem, s>>>(ta, tb, M, N, K, C, ldc, acc, err);
+  k_gemm_tc<<<grid, 128, smem, s>>>(ta, tb, M, N, K, C, ldc, acc, err, e);
   return cudaGetLastError();
 }
 
