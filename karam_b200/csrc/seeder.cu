@@ -74,16 +74,38 @@ __global__ void k_colsum(const float* G, int rows, int cols, float* out) {
   out[c] = s;
 }
 
-__global__ void k_adam(float* w, const float* g, float* m, float* v, int n, float lr, float c1,
-                       float c2) {
+// Adam update of n parameters for one training step: the step's bias
+// corrections c1, c2 come from the epoch's table c12[2 q], c12[2 q + 1], q =
+// ctr[0] the step within the epoch (so a captured step replays unchanged).
+__global__ void k_adam_step(float* w, const float* g, float* m, float* v, int n, float lr,
+                            const float* c12, const int* ctr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int q = *ctr;
+  const float c1 = c12[2 * q], c2 = c12[2 * q + 1];
   const float gi = g[i];
   const float mi = 0.9f * m[i] + 0.1f * gi;
   const float vi = 0.999f * v[i] + 0.001f * gi * gi;
   m[i] = mi;
   v[i] = vi;
   w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + 1e-8f);
+}
+
+// The step within the epoch advances (the last kernel of a captured step).
+__global__ void k_step_advance(int* ctr) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctr[0] += 1;
+}
+
+// k_norm_rows over the batch of step ctr[0]: rows idx[ctr[0] * B + r].
+__global__ void k_norm_rows_step(const float* src, const int* idx, const int* ctr, int B, int cols,
+                                 const float* mean, const float* istd, float* out) {
+  const int* bi = idx + (size_t)(*ctr) * B;
+  const size_t n = (size_t)B * cols;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / cols), j = (int)(e - (size_t)r * cols);
+    out[e] = (src[(size_t)bi[r] * cols + j] - mean[j]) * istd[j];
+  }
 }
 
 // out[r][j] = (src[row(r)][j] - mean[j]) * istd[j], row(r) = idx ? idx[r] : r.
@@ -254,7 +276,12 @@ struct Mlp {
   // when training has changed them) and BF16 activations ([rows][pad8(K)])
   std::vector<BBuf> wbf, abf;
   long wbf_step = -1;
+  // training: the step counter of a captured step and the epoch's Adam
+  // bias-correction table
+  Buf c12;
+  int* ctr = nullptr;
   ~Mlp() {
+    if (ctr) cudaFree(ctr);
     if (idx) cudaFree(idx);
   }
 };
@@ -404,44 +431,90 @@ float mlp_train(Mlp* m, int epochs, int batch, float lr, uint64_t shuffle_seed, 
     ck(cudaMalloc(&m->idx, (size_t)m->ns * sizeof(int)), "seeder alloc");
     m->idx_cap = m->ns;
   }
+  if (!m->ctr) {
+    ck(cudaMalloc(&m->ctr, 2 * sizeof(int)), "seeder alloc");
+    ck(cudaMemset(m->ctr, 0, 2 * sizeof(int)), "seeder alloc");
+  }
+  if (m->c12.n < 2 * (size_t)nb) m->c12.alloc(2 * (size_t)nb);
+  // One training step: the batch of step ctr[0] normalised, forward, MSE,
+  // backward, Adam with the step's bias corrections, ctr[0] + 1. Its launches
+  // read every varying value from device memory, so the step is captured once
+  // into a CUDA graph and replayed (the first step of a call runs eagerly:
+  // it sizes the GEMM workspace before the capture).
+  auto train_step = [&]() {
+    k_norm_rows_step<<<grid_for((size_t)B * ni), 256, 0, s>>>(m->Xs.p, m->idx, m->ctr, B, ni, m->fmean.p,
+                                                              m->fistd.p, m->act[0].p);
+    k_norm_rows_step<<<grid_for((size_t)B * no), 256, 0, s>>>(m->Ys.p, m->idx, m->ctr, B, no, m->tmean.p,
+                                                              m->tistd.p, m->tgt.p);
+    forward(m, B, s);
+    float* gc = m->g1.p;
+    float* gn = m->g2.p;
+    k_mse<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[m->L].p, m->tgt.p, gc, B, no, m->loss.p);
+    for (int l = m->L; l >= 1; --l) {
+      const int K = m->dims[l - 1], N = m->dims[l];
+      gemm(K, N, B, m->act[l - 1].p, K, 1, gc, N, 0, m->gW[l - 1].p, N, 0, m->ws, s);
+      k_colsum<<<(N + 127) / 128, 128, 0, s>>>(gc, B, N, m->gb[l - 1].p);
+      if (l > 1) {
+        gemm(B, K, N, gc, N, 0, m->W[l - 1].p, N, 1, gn, K, 0, m->ws, s);
+        k_gelu_bwd<<<grid_for((size_t)B * K), 256, 0, s>>>(gn, m->pre[l - 1].p, B, K);
+        std::swap(gc, gn);
+      }
+    }
+    for (int l = 0; l < m->L; ++l) {
+      const int nw = m->dims[l] * m->dims[l + 1], nbias = m->dims[l + 1];
+      k_adam_step<<<(nw + 255) / 256, 256, 0, s>>>(m->W[l].p, m->gW[l].p, m->mW[l].p, m->vW[l].p, nw, lr,
+                                                   m->c12.p, m->ctr);
+      k_adam_step<<<(nbias + 255) / 256, 256, 0, s>>>(m->b[l].p, m->gb[l].p, m->mb[l].p, m->vb[l].p, nbias,
+                                                      lr, m->c12.p, m->ctr);
+    }
+    k_step_advance<<<1, 32, 0, s>>>(m->ctr);
+  };
+  struct GraphGuard {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~GraphGuard() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+    }
+  } graph;
   std::mt19937_64 rng(shuffle_seed);
   std::vector<int> perm(m->ns);
+  std::vector<float> c12(2 * (size_t)nb);
   float last = 0.0f;
   for (int ep = 0; ep < epochs; ++ep) {
     std::iota(perm.begin(), perm.end(), 0);
     std::shuffle(perm.begin(), perm.end(), rng);
+    for (int q = 0; q < nb; ++q) {  // Adam's bias corrections of the epoch's steps
+      const long st = m->step + 1 + q;
+      c12[2 * q] = 1.0f - std::pow(0.9f, (float)st);
+      c12[2 * q + 1] = 1.0f - std::pow(0.999f, (float)st);
+    }
     ck(cudaMemcpyAsync(m->idx, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, s), "seeder idx");
+    ck(cudaMemcpyAsync(m->c12.p, c12.data(), c12.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+       "seeder adam table");
+    ck(cudaMemsetAsync(m->ctr, 0, sizeof(int), s), "seeder step");
     ck(cudaMemsetAsync(m->loss.p, 0, sizeof(float), s), "seeder loss");
-    for (int q = 0; q < nb; ++q) {
-      const int* bi = m->idx + (size_t)q * B;
-      k_norm_rows<<<grid_for((size_t)B * ni), 256, 0, s>>>(m->Xs.p, bi, B, ni, m->fmean.p, m->fistd.p, m->act[0].p);
-      k_norm_rows<<<grid_for((size_t)B * no), 256, 0, s>>>(m->Ys.p, bi, B, no, m->tmean.p, m->tistd.p, m->tgt.p);
-      forward(m, B, s);
-      float* gc = m->g1.p;
-      float* gn = m->g2.p;
-      k_mse<<<grid_for((size_t)B * no), 256, 0, s>>>(m->pre[m->L].p, m->tgt.p, gc, B, no, m->loss.p);
-      for (int l = m->L; l >= 1; --l) {
-        const int K = m->dims[l - 1], N = m->dims[l];
-        gemm(K, N, B, m->act[l - 1].p, K, 1, gc, N, 0, m->gW[l - 1].p, N, 0, m->ws, s);
-        k_colsum<<<(N + 127) / 128, 128, 0, s>>>(gc, B, N, m->gb[l - 1].p);
-        if (l > 1) {
-          gemm(B, K, N, gc, N, 0, m->W[l - 1].p, N, 1, gn, K, 0, m->ws, s);
-          k_gelu_bwd<<<grid_for((size_t)B * K), 256, 0, s>>>(gn, m->pre[l - 1].p, B, K);
-          std::swap(gc, gn);
-        }
-      }
-      ++m->step;
-      const float c1 = 1.0f - std::pow(0.9f, (float)m->step);
-      const float c2 = 1.0f - std::pow(0.999f, (float)m->step);
-      for (int l = 0; l < m->L; ++l) {
-        const int nw = m->dims[l] * m->dims[l + 1], nbias = m->dims[l + 1];
-        k_adam<<<(nw + 255) / 256, 256, 0, s>>>(m->W[l].p, m->gW[l].p, m->mW[l].p, m->vW[l].p, nw, lr, c1, c2);
-        k_adam<<<(nbias + 255) / 256, 256, 0, s>>>(m->b[l].p, m->gb[l].p, m->mb[l].p, m->vb[l].p, nbias, lr, c1, c2);
+    int q = 0;
+    if (!graph.e) {
+      train_step();  // eager: sizes the workspace
+      ck(cudaGetLastError(), "seeder train launch");
+      q = 1;
+      if (nb > 1) {
+        ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "seeder capture");
+        train_step();
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ce = cudaStreamEndCapture(s, &graph.g);
+        ck(le, "seeder step launch in capture");
+        ck(ce, "seeder end capture");
+        ck(cudaGraphInstantiate(&graph.e, graph.g, 0), "seeder graph instantiate");
       }
     }
+    for (; q < nb; ++q) ck(cudaGraphLaunch(graph.e, s), "seeder graph launch");
+    m->step += nb;
+    // the host copies above read pageable buffers that the next epoch rewrites
+    ck(cudaStreamSynchronize(s), "seeder epoch sync");
     if (ep == epochs - 1) {
-      ck(cudaMemcpyAsync(&last, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s), "seeder loss");
-      ck(cudaStreamSynchronize(s), "seeder sync");
+      ck(cudaMemcpy(&last, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost), "seeder loss");
       last /= (float)std::max(1, nb);
     }
   }
