@@ -480,8 +480,13 @@ def run_karam(args, dist):
         "kernel": dom, "bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak,
         "unit": "GB/s", "frac": kernels[dom]["frac"], "peak_source": peak_kind,
         "traffic": profiled_traffic(dom),
+        "traffic_source": "ncu capture of one full-batch DC round (dram__bytes_read + write), "
+                          "profiles/round_kernels_config2.md",
         "algorithmic_bytes_per_full_launch": ni * (lu_bytes(info, True) if dom == lu_name
                                                    else eval_stamp_bytes(info, True, True)),
+        "algorithmic_bytes_model": "transient round (capacitor history read); achieved uses it",
+        "algorithmic_bytes_per_full_launch_dc": ni * (lu_bytes(info, True) if dom == lu_name
+                                                      else eval_stamp_bytes(info, True, False)),
         "avg_launch_us": 1e3 * (lu_ms if dom == lu_name else eval_ms) / rounds_k,
     }
 

@@ -196,6 +196,18 @@ typedef struct karam_solver_opts {
                             event records slow a round down (B200, config 2:
                             ~24 us of a ~160 us round), so 0 (the default) leaves
                             them out and those three fields at 0               */
+  double lte_reltol;     /* transient step control by local truncation error: a
+                            converged sub-step of size h whose accepted point x
+                            leaves, at some node, the linear extrapolation
+                            p = v1 + (h / h1) (v1 - v2) from the two previous
+                            accepted points (v1 after a sub-step of size h1) by
+                            more than lte_reltol * max(|x|, |v1|) + lte_abstol
+                            is redone from v1 with half the step, as an NR
+                            failure is, while max_halvings allows (then it is
+                            accepted). The first sub-step of a transient has no
+                            predictor and is not tested. 0 (the default): off,
+                            the reference's fixed-step behaviour              */
+  double lte_abstol;     /* [V], with lte_reltol                                  */
 } karam_solver_opts;
 
 /* Sizes of the symbolic analysis of a problem. */
@@ -238,6 +250,9 @@ typedef struct karam_instance_stats {
   int32_t stagnation;   /* SolverStats::stagnationDetected                        */
   int32_t divergence;   /* SolverStats::divergenceDetected                        */
   int32_t history_len;  /* DC NR iterations recorded (convergenceHistory.size())  */
+  int32_t lte_rejects;  /* transient sub-steps redone by the LTE test (opts.lte_reltol;
+                           counted in halvings too)                              */
+  int32_t reserved_;
 } karam_instance_stats;
 
 /* ConvergenceFailureType (infrastructure/simtrace.h:39-47), same order. */

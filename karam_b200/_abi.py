@@ -68,6 +68,7 @@ class KaramSolverOpts(C.Structure):
         ("polish_abs", C.c_double), ("lu_growth_limit", C.c_double), ("seeded", C.c_int32),
         ("seed_max_iter", C.c_int32), ("schedule", C.c_int32), ("max_rounds", C.c_int32),
         ("max_halvings", C.c_int32), ("kernel_timing", C.c_int32),
+        ("lte_reltol", C.c_double), ("lte_abstol", C.c_double),
     ]
 
 
@@ -85,7 +86,8 @@ class KaramInstanceStats(C.Structure):
                 ("rescued", C.c_int32), ("halvings", C.c_int32),
                 ("max_step_iters", C.c_int32), ("residual", C.c_double),
                 ("failure_type", C.c_int32), ("stagnation", C.c_int32),
-                ("divergence", C.c_int32), ("history_len", C.c_int32)]
+                ("divergence", C.c_int32), ("history_len", C.c_int32),
+                ("lte_rejects", C.c_int32), ("reserved_", C.c_int32)]
 
 
 class KaramTiming(C.Structure):

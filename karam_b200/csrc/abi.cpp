@@ -103,7 +103,7 @@ struct karam_problem {
   int ld = 0;
   DBuf i_kp, i_vth, i_vsdc, i_v1, i_v2, i_v, i_x, i_F, i_J, i_cvp, i_cip, i_st, i_seed, i_out,
       i_redf, i_reddv, i_redfl, i_evt, i_evh,
-      d_active, r_ws, r_list, r_count, i_vtp, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws,
+      d_active, r_ws, r_list, r_count, i_vtp, i_vtpp, i_evl, d_counters, d_seed_ok, i_hub_part, i_hub_cnt, i_luws,
       i_live, i_stage, i_hist;
   cudaEvent_t ev_job0 = nullptr, ev_job1 = nullptr, ev_seed0 = nullptr, ev_seed1 = nullptr;
   bool seed_timed = false;  // ev_seed0 / ev_seed1 bracket this job's seeder inference
@@ -442,6 +442,8 @@ void alloc_instances(karam_problem* p) {
   p->i_hist.alloc(ld * 2 * KHIST_LEN * sizeof(double));
   p->i_seed.alloc(ld * n * sizeof(double));
   p->i_vtp.alloc(ld * n * sizeof(double));
+  p->i_vtpp.alloc(ld * n * sizeof(double));
+  upload(p->i_evl, std::vector<double>(ld, -1.0));
   p->i_out.alloc(ld * n * sizeof(double));
   p->d_active.alloc(2 * sizeof(int));  // live instances; most rounds of a persistent launch
   p->d_seed_ok.alloc(sizeof(int));
@@ -497,6 +499,8 @@ DevInst dev_inst(karam_problem* p) {
   I.cap_vp = p->i_cvp.as<double>();
   I.cap_ip = p->i_cip.as<double>();
   I.v_tp = p->i_vtp.as<double>();
+  I.v_tpp = p->i_vtpp.as<double>();
+  I.ev_lte = p->i_evl.as<double>();
   I.st = p->i_st.as<InstState>();
   I.hist = p->i_hist.as<double>();
   I.seed = nullptr;
@@ -592,6 +596,8 @@ JobParams job_params(const karam_solver_opts* o, int n_steps, double h, int meth
   P.polish_max = o->polish_max;
   P.polish_rel = o->polish_rel;
   P.polish_abs = o->polish_abs;
+  P.lte_rel = o->lte_reltol > 0.0 ? o->lte_reltol : 0.0;
+  P.lte_abs = o->lte_abstol;
   P.n_steps = n_steps;
   P.h = h;
   P.method = method;
@@ -904,6 +910,7 @@ void read_stats(karam_problem* p, karam_instance_stats* stats, bool dc_only) {
     o.stagnation = (s.hflags & KHF_STAGNATION) ? 1 : 0;
     o.divergence = (s.hflags & KHF_DIVERGENCE) ? 1 : 0;
     o.history_len = s.hist_n;
+    o.lte_rejects = s.lte_rejects;
   }
 }
 
@@ -1051,6 +1058,8 @@ void karam_default_opts(karam_solver_opts* o) {
   o->polish_max = 0;
   o->polish_rel = 0.0;
   o->polish_abs = 0.0;
+  o->lte_reltol = 0.0;
+  o->lte_abstol = 0.0;
   o->lu_growth_limit = 0.0;
   o->seeded = 0;
   o->seed_max_iter = 10;

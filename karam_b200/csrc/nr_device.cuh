@@ -111,9 +111,10 @@ __global__ void k_init(DevTopo T, DevInst I, JobParams P) {
   I.st[g] = s;
   I.ev_t[g] = 0.0;
   I.ev_heff[g] = 0.0;
+  if (I.ev_lte) I.ev_lte[g] = -1.0;
   I.red_f[g] = 0ull;
   I.red_dv[g] = 0ull;
-  I.red_flags[g] = 3;
+  I.red_flags[g] = 7;
 }
 
 // NeuralSeeder::predictSeed (solvers/neural_seeder.h:100-137, confidence
@@ -236,6 +237,16 @@ __device__ __forceinline__ V ld_in(const V* p) {
     return *p;
 }
 
+// The LTE test of one node at the candidate point x of a transient sub-step:
+// the linear extrapolation p = v_tp + r (v_tp - v_tpp) from the two previous
+// accepted points (r = sub-step / previous sub-step) must lie within
+// lte_rel * max(|x|, |v_tp|) + lte_abs of x.
+__device__ __forceinline__ bool lte_node_ok(double x, double vt, double vq, double r,
+                                            const JobParams& P) {
+  const double p = vt + r * (vt - vq);
+  return !(fabs(x - p) > P.lte_rel * fmax(fabs(x), fabs(vt)) + P.lte_abs);
+}
+
 // Loads the inputs of device d (MOSFETs first, then diodes) for instance g.
 // Nothing here depends on an earlier evaluation, so the loads of several
 // devices can be in flight together.
@@ -331,6 +342,7 @@ __device__ int dc_done(InstState& s, const JobParams& P) {
     s.step = 1;
     s.first = 1;
     s.it = 0;
+    s.hprev = 0.0;
     return ACT_TRAN_INIT;
   }
   s.mode = MODE_DONE;
@@ -344,6 +356,7 @@ __device__ int step_done(InstState& s, const JobParams& P, double& hsub) {
   const int units = 1 << P.max_halvings;
   const int size = units >> s.depth;
   hsub = P.h * size / units;
+  s.hprev = hsub;
   s.frac += size;
   s.sub = SUB_NR;
   s.first = 1;
@@ -360,6 +373,24 @@ __device__ int step_done(InstState& s, const JobParams& P, double& hsub) {
     }
   }
   return a;
+}
+
+// A converged transient sub-step passes the LTE test (lte_ok: every node of
+// the accepted point lies within lte_rel * max(|x|, |v_tp|) + lte_abs of the
+// linear extrapolation from the two previous accepted points) or is redone
+// from the last accepted point with half the step while halvings remain; at
+// the last halving it is accepted as it is.
+__device__ int accept_substep(InstState& s, const JobParams& P, bool lte_ok, double& hsub) {
+  if (!lte_ok && P.lte_rel > 0.0 && s.depth < P.max_halvings) {
+    s.depth++;
+    s.halvings++;
+    s.lte_rejects++;
+    s.sub = SUB_NR;
+    s.it = 0;
+    s.first = 1;
+    return ACT_RESTART;
+  }
+  return ACT_ACCEPT | step_done(s, P, hsub);
 }
 
 __device__ int start_polish(InstState& s, double& gmin_out) {
@@ -392,7 +423,7 @@ __device__ __forceinline__ void record_iteration(InstState& s, double F, double 
 
 // One decision of the NR control flow for the trial point x whose KCL
 // residual is F (vconv / pok / dv compare x against the accepted point v).
-__device__ int decide(InstState& s, double F, bool vconv, bool pok, double dv,
+__device__ int decide(InstState& s, double F, bool vconv, bool pok, bool lte_ok, double dv,
                       const JobParams& P, double& gmin_out, double& hsub) {
   const int G = P.gmin_steps;
   if (s.mode == MODE_DONE) return 0;
@@ -472,7 +503,7 @@ __device__ int decide(InstState& s, double F, bool vconv, bool pok, double dv,
       s.tran_iters += s.it;
       if (s.it > s.max_step_it) s.max_step_it = s.it;
       if (P.polish_max > 0) return ACT_ACCEPT | start_polish(s, gmin_out);
-      return ACT_ACCEPT | step_done(s, P, hsub);
+      return accept_substep(s, P, lte_ok, hsub);
     }
     if (s.it >= P.max_nr_iter) {
       // attempt loop of CircuitSim::stepTransient (circuitsim_solver.cpp:587-660)
@@ -495,8 +526,7 @@ __device__ int decide(InstState& s, double F, bool vconv, bool pok, double dv,
   s.polish++;
   s.pol_cnt++;
   const bool stalled = s.prev_dv >= 0.0 && dv > 0.5 * s.prev_dv;
-  if (pok || dv == 0.0 || stalled || s.pol_cnt >= P.polish_max)
-    return ACT_ACCEPT | step_done(s, P, hsub);
+  if (pok || dv == 0.0 || stalled || s.pol_cnt >= P.polish_max) return accept_substep(s, P, lte_ok, hsub);
   s.prev_dv = dv;
   gmin_out = 1e-12;
   return ACT_ACCEPT | ACT_SOLVE;
@@ -784,10 +814,11 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
   const int4 blk = __ldg(&T.es_block[blockIdx.y]);  // item off, items, device off, devices
   const bool tran = heff > 0.0;
   const double t = live ? I.ev_t[g] : 0.0;
+  const double lr = live && I.ev_lte ? I.ev_lte[g] : -1.0;
   const double* sd = s_dev + lane;
   double fmx = 0.0, dvm = 0.0;
   bool bad = false;
-  int flags = 3, node_seen = 0;
+  int flags = 7, node_seen = 0;
   auto node_done = [&](int i, double f) {
     const size_t o = (size_t)i * ld + g;
     I.F[o] = f;
@@ -797,6 +828,7 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
     const double dd = fabs(xi - vi), m = fmax(fabs(xi), fabs(vi));
     if (dd > P.reltol * m + P.vntol) flags &= ~1;
     if (dd > P.polish_rel * m + P.polish_abs) flags &= ~2;
+    if (lr >= 0.0 && !lte_node_ok(xi, I.v_tp[o], I.v_tpp[o], lr, P)) flags &= ~4;
     dvm = fmax(dvm, dd);
     node_seen = 1;
   };
@@ -943,7 +975,7 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
     }
     atomicMax(&I.red_f[g], f);
     atomicMax(&I.red_dv[g], d);
-    if (fl != 3) atomicAnd(&I.red_flags[g], fl);
+    if (fl != 7) atomicAnd(&I.red_flags[g], fl);
   }
 }
 
@@ -972,6 +1004,7 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
   if (heff < 0.0) return;
   const bool tran = heff > 0.0;
   const double t = I.ev_t[g];
+  const double lr = I.ev_lte ? I.ev_lte[g] : -1.0;
   double* v0 = s_val;           // gm | diode g
   double* v1 = s_val + nd;      // gds | diode i
   double* v2 = s_val + 2 * nd;  // ids
@@ -1047,7 +1080,7 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
   __syncthreads();
   double fmx = 0.0, dvm = 0.0;
   bool bad = false;
-  int flags = 3;
+  int flags = 7;
   auto node_done = [&](int i, double f) {
     const size_t o = (size_t)i * ld + g;
     I.F[o] = f;
@@ -1057,6 +1090,7 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
     const double dd = fabs(xi - vi), m = fmax(fabs(xi), fabs(vi));
     if (dd > P.reltol * m + P.vntol) flags &= ~1;
     if (dd > P.polish_rel * m + P.polish_abs) flags &= ~2;
+    if (lr >= 0.0 && !lte_node_ok(xi, I.v_tp[o], I.v_tpp[o], lr, P)) flags &= ~4;
     dvm = fmax(dvm, dd);
   };
   for (int it = tid; it < nv + n; it += blockDim.x) {
@@ -1153,7 +1187,7 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
     }
     atomicMax(&I.red_f[g], f);
     atomicMax(&I.red_dv[g], dv);
-    if (fl != 3) atomicAnd(&I.red_flags[g], fl);
+    if (fl != 7) atomicAnd(&I.red_flags[g], fl);
   }
 }
 
@@ -1174,7 +1208,7 @@ __global__ void __launch_bounds__(kBigThreads) k_es_one(DevTopo T, DevInst I, Jo
 __device__ __forceinline__ void reset_reductions(const DevInst& I, int g) {
   I.red_f[g] = 0ull;
   I.red_dv[g] = 0ull;
-  I.red_flags[g] = 3;
+  I.red_flags[g] = 7;
 }
 
 // Evaluation point of the next round from the instance's state.
@@ -1183,12 +1217,18 @@ __device__ __forceinline__ void set_eval_point(const DevInst& I, const JobParams
   if (st.mode == MODE_DONE) {
     I.ev_heff[g] = -1.0;
     I.ev_t[g] = 0.0;
+    if (I.ev_lte) I.ev_lte[g] = -1.0;
     return;
   }
   double t, heff;
   eval_point(st, P, t, heff);
   I.ev_t[g] = t;
   I.ev_heff[g] = heff;
+  if (I.ev_lte) {  // the LTE predictor's step ratio, when the test applies to this point
+    const int units = 1 << P.max_halvings;
+    const double hsub = P.h * (units >> st.depth) / units;
+    I.ev_lte[g] = st.mode == MODE_TRAN && P.lte_rel > 0.0 && st.hprev > 0.0 ? hsub / st.hprev : -1.0;
+  }
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -1345,7 +1385,7 @@ __device__ __forceinline__ int instance_decide(const DevTopo& Tp, const DevInst&
   gm = 1e-12;
   hs = P.h;
   const int h0 = s.hist_n;
-  const int a = decide(s, Fm, fl & 1, (fl & 2) != 0, dvm, P, gm, hs);
+  const int a = decide(s, Fm, fl & 1, (fl & 2) != 0, (fl & 4) != 0, dvm, P, gm, hs);
   if (s.hist_n != h0 && I.hist) {
     const size_t k = (size_t)(h0 % KHIST_LEN) * 2;
     I.hist[k * I.ld + g] = Fm;
@@ -1637,7 +1677,10 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
           vi = xi;
           V[o] = vi;
         }
-        if (act & (ACT_STEP | ACT_TRAN_INIT)) VT[o] = vi;
+        if (act & (ACT_STEP | ACT_TRAN_INIT)) {
+          if (I.v_tpp) I.v_tpp[o] = (act & ACT_TRAN_INIT) ? vi : VT[o];  // the LTE predictor's older point
+          VT[o] = vi;
+        }
       }
       if (act & ACT_SOLVE)
         Y[nd ? ln * Tp.nd_SY + nd_half(prog, prog[6], i) : i * L + ln] = (T)(-(fi + gmin * vi));
@@ -1986,7 +2029,10 @@ __device__ void lu_big_instance(const DevTopo& Tp, const DevInst& I, const JobPa
           vi = xi;
           V[o] = vi;
         }
-        if (a & (ACT_STEP | ACT_TRAN_INIT)) VT[o] = vi;
+        if (a & (ACT_STEP | ACT_TRAN_INIT)) {
+          if (I.v_tpp) I.v_tpp[o] = (a & ACT_TRAN_INIT) ? vi : VT[o];  // the LTE predictor's older point
+          VT[o] = vi;
+        }
       }
       if (a & ACT_SOLVE) Y[__ldg(&Tp.nd_pos[i])] = (T)(-(fi + gmin * vi));
     }
@@ -2815,7 +2861,7 @@ __device__ void persist_instance(const DevTopo& Tp, const DevInst& I, const JobP
 // Byte offsets of one instance's state in shared memory (resident_in),
 // each region on a 16-byte boundary; es = the Jacobian value size.
 struct ResidentLayout {
-  size_t v, x, F, vtp, cvp, cip, vsdc, v1, v2, hist, scal, st, J, kp, vth, total;
+  size_t v, x, F, vtp, vtpp, cvp, cip, vsdc, v1, v2, hist, scal, st, J, kp, vth, total;
 };
 __host__ __device__ inline ResidentLayout resident_layout(const DevTopo& T, size_t es) {
   ResidentLayout L{};
@@ -2830,13 +2876,14 @@ __host__ __device__ inline ResidentLayout resident_layout(const DevTopo& T, size
   L.x = take(8 * n);
   L.F = take(8 * n);
   L.vtp = take(8 * n);
+  L.vtpp = take(8 * n);
   L.cvp = take(8 * nc);
   L.cip = take(8 * nc);
   L.vsdc = take(8 * ns);
   L.v1 = take(8 * ns);
   L.v2 = take(8 * ns);
   L.hist = take(8 * 2 * KHIST_LEN);
-  L.scal = take(8 * 5);  // ev_t, ev_heff, red_f, red_dv, red_flags
+  L.scal = take(8 * 6);  // ev_t, ev_heff, red_f, red_dv, red_flags, ev_lte
   L.st = take(sizeof(InstState));
   L.J = take(es * (size_t)T.nv);
   L.kp = take(4 * (size_t)T.n_mos);
@@ -2863,6 +2910,7 @@ __device__ void resident_in(const DevTopo& Tp, const DevInst& I, int g, unsigned
   double* x = reinterpret_cast<double*>(base + L.x);
   double* F = reinterpret_cast<double*>(base + L.F);
   double* vtp = reinterpret_cast<double*>(base + L.vtp);
+  double* vtpp = reinterpret_cast<double*>(base + L.vtpp);
   double* cvp = reinterpret_cast<double*>(base + L.cvp);
   double* cip = reinterpret_cast<double*>(base + L.cip);
   double* vsdc = reinterpret_cast<double*>(base + L.vsdc);
@@ -2883,6 +2931,8 @@ __device__ void resident_in(const DevTopo& Tp, const DevInst& I, int g, unsigned
     R.x = x;
     R.F = F;
     R.v_tp = vtp;
+    R.v_tpp = I.v_tpp ? vtpp : nullptr;
+    R.ev_lte = I.ev_lte ? scal + 5 : nullptr;
     R.cap_vp = cvp;
     R.cap_ip = cip;
     R.vs_dc = vsdc;
@@ -2913,6 +2963,7 @@ __device__ void resident_in(const DevTopo& Tp, const DevInst& I, int g, unsigned
     reinterpret_cast<unsigned long long*>(scal)[2] = I.red_f[g];
     reinterpret_cast<unsigned long long*>(scal)[3] = I.red_dv[g];
     *reinterpret_cast<int*>(scal + 4) = I.red_flags[g];
+    scal[5] = I.ev_lte ? I.ev_lte[g] : -1.0;
     *st = I.st[g];
   }
   for (int i = tid; i < Tp.n; i += bd) {
@@ -2921,6 +2972,7 @@ __device__ void resident_in(const DevTopo& Tp, const DevInst& I, int g, unsigned
     x[i] = I.x[o];
     F[i] = I.F[o];
     vtp[i] = I.v_tp[o];
+    if (I.v_tpp) vtpp[i] = I.v_tpp[o];
   }
   for (int c = tid; c < Tp.n_cap; c += bd) {
     cvp[c] = I.cap_vp[(size_t)c * ld + g];
@@ -2948,6 +3000,7 @@ __device__ void resident_out(const DevTopo& Tp, const DevInst& I, int g, const u
   const double* x = reinterpret_cast<const double*>(base + L.x);
   const double* F = reinterpret_cast<const double*>(base + L.F);
   const double* vtp = reinterpret_cast<const double*>(base + L.vtp);
+  const double* vtpp = reinterpret_cast<const double*>(base + L.vtpp);
   const double* cvp = reinterpret_cast<const double*>(base + L.cvp);
   const double* cip = reinterpret_cast<const double*>(base + L.cip);
   const double* hist = reinterpret_cast<const double*>(base + L.hist);
@@ -2960,6 +3013,7 @@ __device__ void resident_out(const DevTopo& Tp, const DevInst& I, int g, const u
     I.x[o] = x[i];
     I.F[o] = F[i];
     I.v_tp[o] = vtp[i];
+    if (I.v_tpp) I.v_tpp[o] = vtpp[i];
   }
   for (int c = tid; c < Tp.n_cap; c += bd) {
     I.cap_vp[(size_t)c * ld + g] = cvp[c];
@@ -2974,6 +3028,7 @@ __device__ void resident_out(const DevTopo& Tp, const DevInst& I, int g, const u
     I.red_f[g] = reinterpret_cast<const unsigned long long*>(scal)[2];
     I.red_dv[g] = reinterpret_cast<const unsigned long long*>(scal)[3];
     I.red_flags[g] = *reinterpret_cast<const int*>(scal + 4);
+    if (I.ev_lte) I.ev_lte[g] = scal[5];
     I.st[g] = *st;
   }
 }
@@ -3257,7 +3312,9 @@ __global__ void k_tran_start(DevTopo T, DevInst I, JobParams P, int init_caps) {
     const double vi = I.v[i * ld + g];
     I.x[i * ld + g] = vi;
     I.v_tp[i * ld + g] = vi;
+    if (init_caps && I.v_tpp) I.v_tpp[i * ld + g] = vi;
   }
+  if (init_caps) s.hprev = 0.0;  // a fresh transient: no previous sub-step for the LTE test
   if (init_caps)
     for (int c = 0; c < T.n_cap; ++c) {
       const int2 tt = T.cap_term[c];

@@ -71,8 +71,9 @@ struct InstState {
   int hist_n;       // iterations recorded
   int dir_changes;  // residual direction changes between consecutive iterations
   int hflags;       // KHF_* bits
-  int pad_;
+  int lte_rejects;  // transient sub-steps redone because the LTE test failed
   double h1, h2;    // the last two recorded residuals (h1 most recent)
+  double hprev;     // size of the last accepted transient sub-step (0: none yet)
 };
 
 // InstState::hflags
@@ -202,6 +203,9 @@ struct DevInst {
   double* cap_vp;           // [n_cap][ld]
   double* cap_ip;           // [n_cap][ld]
   double* v_tp;             // [n][ld] voltages at the last accepted time point
+  double* v_tpp;            // [n][ld] ... and at the accepted point before it (LTE predictor)
+  double* ev_lte;           // [ld] LTE predictor ratio of the point the next round evaluates:
+                            // sub-step / previous sub-step, < 0 when no LTE test applies
   InstState* st;            // [ni]
   const double* seed;       // [n][ld] caller guesses (permuted) or 0
   double* rescue_ws;        // [rescue_slots][2][n][n]: U and dense row buffers per rescue warp
@@ -238,6 +242,7 @@ struct JobParams {
   int seed_bcast;    // 1: one seed for every instance, in lane 0 of DevInst::seed
   int max_halvings;  // transient restarts with a halved step (reference: 3)
   double growth32, growth64;  // static-pivot multiplier limits (FP32 / FP64 solves)
+  double lte_rel, lte_abs;    // transient LTE test tolerances (lte_rel 0: no test)
 };
 
 // One problem of a multi-problem persistent launch (k_persist_multi): CTAs

@@ -481,7 +481,8 @@ struct Driver {
       return node > 0 ? vv[node - 1] : 0.0;
     };
     for (size_t i = 0; i < nc; ++i) cvp[i] = vnode(v, b.cap_n1[i]) - vnode(v, b.cap_n2[i]);
-    std::vector<double> guess;
+    std::vector<double> guess, v_prev = v;  // v_prev: the accepted point before v
+    double h_prev = 0.0;                     // size of the last accepted sub-step
     st->converged = 1;
     const int H = o.max_halvings, units = 1 << H;
     const double unit = dt / units;
@@ -503,9 +504,29 @@ struct Driver {
             break;
           }
           depth++;
+          st->halvings++;
           continue;
         }
         polish(guess, h, method, t, st);
+        // LTE step control (the product's documented rule, karam_solver_opts
+        // lte_reltol): the accepted point against the linear extrapolation
+        // from the two previous accepted points; a failing sub-step is redone
+        // with half the step while halvings remain
+        if (o.lte_rel > 0.0 && h_prev > 0.0 && depth < H) {
+          const double r = h / h_prev;
+          bool ok = true;
+          for (int i = 0; i < b.n && ok; ++i) {
+            const double p = v[i] + r * (v[i] - v_prev[i]);
+            if (std::fabs(guess[i] - p) > o.lte_rel * std::fmax(std::fabs(guess[i]), std::fabs(v[i])) + o.lte_abs)
+              ok = false;
+          }
+          if (!ok) {
+            depth++;
+            st->halvings++;
+            st->lte_rejects++;
+            continue;
+          }
+        }
         // capacitor history, circuitsim_solver.cpp:669-699
         for (size_t i = 0; i < nc; ++i) {
           double vc = vnode(guess, b.cap_n1[i]) - vnode(guess, b.cap_n2[i]);
@@ -515,7 +536,9 @@ struct Driver {
           cvp[i] = vc;
           cip[i] = ic;
         }
+        v_prev = v;
         v = guess;
+        h_prev = h;
         frac += size;
       }
       if (st->converged && wave_out && n_wave > 0)

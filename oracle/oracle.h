@@ -39,6 +39,9 @@ typedef struct oracle_opts {
   int32_t seed_max_iter; /* fall back to full GMIN stepping after this many */
   int32_t max_halvings;  /* transient step halvings after NR failure (3 = the
                             reference's 4 attempts, circuitsim_solver.cpp:583) */
+  double lte_rel, lte_abs; /* LTE step control of the product's transient (the
+                            linear-extrapolation test of karam_solver_opts
+                            lte_reltol / lte_abstol); lte_rel 0 = off */
 } oracle_opts;
 
 typedef struct oracle_stats {
@@ -56,6 +59,8 @@ typedef struct oracle_stats {
   int32_t stagnation;
   int32_t divergence;
   int32_t history_len;
+  int32_t halvings;      /* transient sub-steps redone with half the step */
+  int32_t lte_rejects;   /* ... of those, by the LTE test */
 } oracle_stats;
 
 /* Fills o with the reference constants; polish off, dense solver. */

@@ -31,7 +31,7 @@ class OracleOpts(C.Structure):
                 ("polish_max", C.c_int32), ("polish_rel", C.c_double),
                 ("polish_abs", C.c_double), ("linear_solver", C.c_int32),
                 ("seeded", C.c_int32), ("seed_max_iter", C.c_int32),
-                ("max_halvings", C.c_int32)]
+                ("max_halvings", C.c_int32), ("lte_rel", C.c_double), ("lte_abs", C.c_double)]
 
 
 class OracleStats(C.Structure):
@@ -41,7 +41,8 @@ class OracleStats(C.Structure):
                 ("seeded_ok", C.c_int32), ("max_step_iters", C.c_int32),
                 ("residual", C.c_double), ("failure_type", C.c_int32),
                 ("stagnation", C.c_int32), ("divergence", C.c_int32),
-                ("history_len", C.c_int32)]
+                ("history_len", C.c_int32), ("halvings", C.c_int32),
+                ("lte_rejects", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

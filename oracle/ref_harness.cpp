@@ -348,6 +348,8 @@ void oracle_default_opts(oracle_opts* o) {
   o->seeded = 0;
   o->seed_max_iter = 10;
   o->max_halvings = 3;
+  o->lte_rel = 0.0;
+  o->lte_abs = 0.0;
 }
 
 int oracle_tensorize(const karam_netlist* nl, int32_t* mos_order, int32_t* dio_order) {

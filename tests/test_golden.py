@@ -242,3 +242,22 @@ def test_ac_rule_equals_reference_build_where_they_coincide():
     assert scaled(g) < 1e-3  # the same stamps, summed in another order
     g, *_ = ac_inputs("config2")
     assert scaled(g) > 1.0
+
+
+def test_lte_step_control_in_the_oracle(port, ref):
+    """The LTE rule of the transient (the product's documented step control)
+    runs in the oracle driver over both backends: over the gate ramp of the
+    8 x 8 grid it redoes sub-steps, the restatement and the reference-built
+    stamps take the same decisions and reach the same waveform, and with the
+    rule off no step is halved."""
+    nl = circuits.grid_circuit(8)
+    v, _ = port.solve_dc(nl, polish_max=8)
+    kw = dict(wave_nodes=[3, 10, 30], max_halvings=6, polish_max=8)
+    vp, sp, wp = port.transient(nl, v, 40e-12, 20, A.TRAN_TRAP, lte_rel=1e-3, lte_abs=1e-4, **kw)
+    vr, sr, wr = ref.transient(nl, v, 40e-12, 20, A.TRAN_TRAP, lte_rel=1e-3, lte_abs=1e-4, **kw)
+    assert sp["converged"] == sr["converged"] == 1
+    assert sp["lte_rejects"] == sr["lte_rejects"] > 0
+    assert sp["halvings"] == sr["halvings"] and sp["iterations"] == sr["iterations"]
+    assert np.max(np.abs(wp - wr)) <= 1e-9 * np.max(np.abs(wr)) + 1e-12
+    _, s0, _ = port.transient(nl, v, 40e-12, 20, A.TRAN_TRAP, **kw)
+    assert s0["lte_rejects"] == 0 and s0["halvings"] == 0
