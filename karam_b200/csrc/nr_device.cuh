@@ -814,7 +814,7 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
   const int4 blk = __ldg(&T.es_block[blockIdx.y]);  // item off, items, device off, devices
   const bool tran = heff > 0.0;
   const double t = live ? I.ev_t[g] : 0.0;
-  const double lr = live && I.ev_lte ? I.ev_lte[g] : -1.0;
+  const double lr = P.lte_rel > 0.0 && live && I.ev_lte ? I.ev_lte[g] : -1.0;
   const double* sd = s_dev + lane;
   double fmx = 0.0, dvm = 0.0;
   bool bad = false;
@@ -1004,7 +1004,7 @@ __device__ void es_one_instance(const DevTopo& T, const DevInst& I, const JobPar
   if (heff < 0.0) return;
   const bool tran = heff > 0.0;
   const double t = I.ev_t[g];
-  const double lr = I.ev_lte ? I.ev_lte[g] : -1.0;
+  const double lr = P.lte_rel > 0.0 && I.ev_lte ? I.ev_lte[g] : -1.0;
   double* v0 = s_val;           // gm | diode g
   double* v1 = s_val + nd;      // gds | diode i
   double* v2 = s_val + 2 * nd;  // ids
@@ -1217,17 +1217,23 @@ __device__ __forceinline__ void set_eval_point(const DevInst& I, const JobParams
   if (st.mode == MODE_DONE) {
     I.ev_heff[g] = -1.0;
     I.ev_t[g] = 0.0;
-    if (I.ev_lte) I.ev_lte[g] = -1.0;
+    if (I.ev_lte && P.lte_rel > 0.0) I.ev_lte[g] = -1.0;
     return;
   }
   double t, heff;
   eval_point(st, P, t, heff);
   I.ev_t[g] = t;
   I.ev_heff[g] = heff;
-  if (I.ev_lte) {  // the LTE predictor's step ratio, when the test applies to this point
-    const int units = 1 << P.max_halvings;
-    const double hsub = P.h * (units >> st.depth) / units;
-    I.ev_lte[g] = st.mode == MODE_TRAN && P.lte_rel > 0.0 && st.hprev > 0.0 ? hsub / st.hprev : -1.0;
+  // the LTE predictor's step ratio, when the test applies to this point (with
+  // the test off the ratio is never read: it stays as k_init set it)
+  if (I.ev_lte && P.lte_rel > 0.0) {
+    if (st.mode == MODE_TRAN && st.hprev > 0.0) {
+      const int units = 1 << P.max_halvings;
+      const double hsub = P.h * (units >> st.depth) / units;
+      I.ev_lte[g] = hsub / st.hprev;
+    } else {
+      I.ev_lte[g] = -1.0;
+    }
   }
 }
 
