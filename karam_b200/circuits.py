@@ -241,6 +241,55 @@ def grid_circuit(N, seed=None, vdd=1.0, gate_pulse=GRID_GATE_PULSE):
     return nl
 
 
+MESH_GATE_PULSE = (0.0, 1.0, 0.1e-9, 0.05e-9, 0.05e-9, 0.4e-9, 1e-9)  # 1 ns period
+
+
+def power_grid_mesh(N, seed=None, vdd=1.0, pad_pitch=64, load_fraction=20_000 / 1_048_576,
+                    gate_pulse=MESH_GATE_PULSE):
+    """N x N power-grid mesh of the large single-instance family (the
+    1024 x 1024 mesh at N = 1024; smaller N are tiles of the same
+    construction).
+
+    Node 1 = VDD (``vdd`` volts), node 2 = the loads' gate net (PULSE, 1 ns
+    period), mesh node (i, j) = 3 + i N + j. Segment resistors are uniform in
+    0.1..1 ohm, each mesh node has 10 fF to ground, every pad_pitch-th border
+    node (the corners included) is fed from VDD through 1 ohm, and a fraction
+    load_fraction of the nodes (20 k of 1 M at full size), drawn at random,
+    carries a level-1 NMOS load (drain on the node, gate on the pulsed net,
+    W/L 2u/0.18u). Draws come from PortableRNG(seed), seed = BASE_SEED +
+    10,000,000 + N by default.
+    """
+    if N < 2:
+        raise ValueError("mesh needs N >= 2")
+    rng = PCG32(np.array([BASE_SEED + 10_000_000 + N if seed is None else seed], dtype=np.uint64))
+    uniform = lambda: float(rng.next()[0]) / 4294967296.0
+    nl = Netlist()
+    nmod = nl.model("NMOS", A.MODEL_NMOS, NMOS_CARD["kp"], NMOS_CARD["vto"], NMOS_CARD["lam"])
+    VDD, GATE = 1, 2
+    node = lambda i, j: 3 + i * N + j
+    nl.vsource(VDD, 0, vdd)
+    nl.vsource(GATE, 0, gate_pulse[0], pulse=gate_pulse)
+    for i in range(N):
+        for j in range(N):
+            if j + 1 < N:
+                nl.resistor(node(i, j), node(i, j + 1), 0.1 + 0.9 * uniform())
+            if i + 1 < N:
+                nl.resistor(node(i, j), node(i + 1, j), 0.1 + 0.9 * uniform())
+    border = set()
+    for k in range(0, N, pad_pitch):
+        border.update({(0, k), (N - 1, k), (k, 0), (k, N - 1)})
+    border.update({(0, N - 1), (N - 1, 0), (N - 1, N - 1)})
+    for i, j in sorted(border):
+        nl.resistor(VDD, node(i, j), 1.0)
+    for i in range(N):
+        for j in range(N):
+            nl.capacitor(node(i, j), 0, 10e-15)
+    for k in range(N * N):
+        if uniform() < load_fraction:
+            nl.mosfet(3 + k, GATE, 0, 0, nmod, *NMOS_WL)
+    return nl
+
+
 def config3_sizes(n_instances=2048, first_instance=0):
     """Grid size N ~ U{8..64} of each instance of the uneven batch: one
     PortableRNG draw per instance, seeded BASE_SEED + 5,000,000 + instance."""

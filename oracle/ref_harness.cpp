@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <iostream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -322,6 +323,14 @@ struct Session {
 
 template <class F>
 int guarded(F f) {
+  // The reference reports clamps and singular pivots on std::cerr; formatting
+  // those messages inside this library crashed the host process, so its
+  // diagnostics are silenced here (the results are returned, not printed).
+  static const bool quiet = [] {
+    std::cerr.setstate(std::ios::badbit);
+    return true;
+  }();
+  (void)quiet;
   try {
     return f();
   } catch (const std::exception& e) {
