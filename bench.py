@@ -559,6 +559,7 @@ def run_karam(args, dist):
         line["config5_32stage"] = config5_seeder(ctx, n_train=40960, n_test=8192, stages=32)
         line["config3"] = config3_uneven(dist.local, steps=args.config3_steps)
         line["ac"] = ac_sweep_leg(ctx)
+        line["config4_tile"] = config4_tile(ctx)
     if dist.rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy_check(nl, inst, v_mixed, v_fp64, st_mixed, st_fp64)
         line["outcomes"] = outcome_check(nl, inst, st_mixed, st_fp64)
@@ -576,6 +577,75 @@ def run_karam(args, dist):
     seeder.close()
     prob.close()
     ctx.close()
+
+
+def config4_tile(ctx, N=64, steps=1000, dt=1e-12, n_check=32, check_steps=150):
+    """Tiles of the large single-instance workload (circuits.power_grid_mesh):
+    one N x N mesh, DC then `steps` backward-Euler steps of `dt`, FP32 LU +
+    FP64 refinement against plain FP64 on the GPU (the level-scheduled
+    kernels; the 1024 x 1024 mesh itself needs the supernodal solver, which is
+    not built). Accuracy and the CPU rate: an n_check x n_check tile, DC +
+    check_steps steps, GPU mixed precision against the reference-built oracle
+    (sparse LU), one thread."""
+    import karam_b200 as K
+    from karam_b200 import _abi as A
+    from karam_b200 import circuits
+    from oracle import pyoracle
+    out = {"workload": f"{N} x {N} power-grid mesh tile (0.1-1 ohm segments, 10 fF caps, VDD pads every "
+                       f"64 border nodes, pulsed NMOS loads at 1.9 % of nodes); DC + {steps} BE steps of "
+                       f"{dt * 1e12:g} ps, one instance"}
+    nl = circuits.power_grid_mesh(N)
+    prob = K.Problem(ctx, nl, max_instances=1)
+    prob.set_instances(None)
+    out["n"] = nl.n_nodes
+    for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        opts = K.options(precision=prec, **POLISH)
+        prob.run_mc_device(dt, 4, A.TRAN_BE, opts)  # warm-up
+        t = time.perf_counter()
+        prob.run_mc_device(dt, steps, A.TRAN_BE, opts)
+        wall = time.perf_counter() - t
+        tm = prob.timing()
+        _, st = prob.read_results()
+        out[name] = {"solves_per_s": (steps + 1) / wall if st[0]["status"] == A.ST_CONVERGED else 0.0,
+                     "wall_s": wall, "device_ms": tm["job_ms"], "rounds": tm["rounds"],
+                     "iterations": st[0]["iterations"], "converged": st[0]["status"] == A.ST_CONVERGED,
+                     "schedule": lu_name_of(tm)}
+    prob.close()
+    out["speedup_mixed_vs_fp64"] = (out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+                                    if out["fp64"]["solves_per_s"] else None)
+    # accuracy and the CPU rate on a smaller tile
+    nl = circuits.power_grid_mesh(n_check)
+    prob = K.Problem(ctx, nl, max_instances=1)
+    prob.set_instances(None)
+    nodes = [3, 3 + n_check * n_check // 2 + n_check // 2, nl.n_nodes]
+    opts = K.options(precision=A.PREC_MIXED, **POLISH)
+    prob.solve_dc(opts)
+    v, st, wave = prob.step_transient(dt, check_steps, A.TRAN_BE, opts, wave_nodes=nodes)
+    prob.close()
+    kind = "ref" if pyoracle.available("ref") else "port"
+    if kind == "port":
+        pyoracle.build("port")
+    with native_stdout_to_stderr():
+        orc = pyoracle.Oracle(kind)
+        t = time.perf_counter()
+        vd, sd = orc.solve_dc(nl, linear_solver=pyoracle.LS_SPARSE, **POLISH)
+        vt, stt, w_ref = orc.transient(nl, vd, dt, check_steps, A.TRAN_BE, wave_nodes=nodes,
+                                       linear_solver=pyoracle.LS_SPARSE, **POLISH)
+        cpu_t = time.perf_counter() - t
+    out["check"] = {"tile": f"{n_check} x {n_check} (n = {nl.n_nodes}), DC + {check_steps} steps, mixed",
+                    "max_scaled_err_vs_oracle": float(np.max(np.abs(v[0] - vt) / (1e-9 * np.abs(vt) + 1e-12))),
+                    "max_abs_wave_diff_v": float(np.max(np.abs(wave[0] - w_ref)))}
+    out["cpu_baseline"] = {"value": (check_steps + 1) / cpu_t, "unit": "solves/s", "cores": 1,
+                           "kind": "reference" if kind == "ref" else "port",
+                           "sample": f"the {n_check} x {n_check} tile, DC + {check_steps} steps, sparse LU "
+                                     f"(solveSparse_LU with the Min-Fill ordering), {cpu_t:.1f} s"}
+    return out
+
+
+def lu_name_of(tm):
+    return ["pivot records", "warp per instance", "CTA per instance, shared memory",
+            "CTA per instance, global memory", "CTA per instance, packed program",
+            "persistent CTA per instance"][tm["level_schedule"]]
 
 
 def ac_sweep_leg(ctx, n_instances=4096, n_points=16, f_start=1e6, f_stop=1e12, input_node=2,
