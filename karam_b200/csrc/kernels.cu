@@ -189,9 +189,9 @@ void launch_eval_stamp(const DevTopo& T, const DevInst& I, const JobParams& P,
   }
   const dim3 grid((I.ni + 31) / 32, T.n_es_blocks);
   if (prec == KARAM_PREC_MIXED)
-    k_es<float><<<grid, 256, 0, s>>>(T, I, P);
+    (P.lte_rel > 0.0 ? k_es<float, true> : k_es<float, false>)<<<grid, 256, 0, s>>>(T, I, P);
   else
-    k_es<double><<<grid, 256, 0, s>>>(T, I, P);
+    (P.lte_rel > 0.0 ? k_es<double, true> : k_es<double, false>)<<<grid, 256, 0, s>>>(T, I, P);
 }
 
 void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const RoundLaunch& L,

@@ -356,7 +356,7 @@ __device__ int step_done(InstState& s, const JobParams& P, double& hsub) {
   const int units = 1 << P.max_halvings;
   const int size = units >> s.depth;
   hsub = P.h * size / units;
-  s.hprev = hsub;
+  s.hprev = P.lte_rel > 0.0 ? hsub : 0.0;  // with the LTE test off no predictor is kept
   s.frac += size;
   s.sub = SUB_NR;
   s.first = 1;
@@ -792,7 +792,9 @@ __device__ __forceinline__ double node_term(const DevTopo& T, const DevInst& I, 
 // holds: the supply node and its diagonal) have their devices split into
 // chunks of KES_MAX_DEV, one block per chunk; the last chunk block of a tile
 // to finish adds the chunks' sums.
-template <typename TJ>
+// kLte: the transient LTE test is on (P.lte_rel > 0); the kernel without it
+// carries none of its code.
+template <typename TJ, bool kLte>
 __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P) {
   __shared__ double s_dev[KES_MAX_DEV * 3 * 32];
   __shared__ unsigned long long s_f[8][32], s_dv[8][32];
@@ -814,7 +816,7 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
   const int4 blk = __ldg(&T.es_block[blockIdx.y]);  // item off, items, device off, devices
   const bool tran = heff > 0.0;
   const double t = live ? I.ev_t[g] : 0.0;
-  const double lr = P.lte_rel > 0.0 && live && I.ev_lte ? I.ev_lte[g] : -1.0;
+  const double lr = kLte && live && I.ev_lte ? I.ev_lte[g] : -1.0;
   const double* sd = s_dev + lane;
   double fmx = 0.0, dvm = 0.0;
   bool bad = false;
@@ -828,7 +830,7 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
     const double dd = fabs(xi - vi), m = fmax(fabs(xi), fabs(vi));
     if (dd > P.reltol * m + P.vntol) flags &= ~1;
     if (dd > P.polish_rel * m + P.polish_abs) flags &= ~2;
-    if (lr >= 0.0 && !lte_node_ok(xi, I.v_tp[o], I.v_tpp[o], lr, P)) flags &= ~4;
+    if (kLte && lr >= 0.0 && !lte_node_ok(xi, I.v_tp[o], I.v_tpp[o], lr, P)) flags &= ~4;
     dvm = fmax(dvm, dd);
     node_seen = 1;
   };
@@ -1684,7 +1686,8 @@ __device__ __forceinline__ void lu_round(const DevTopo& Tp, const DevInst& I, co
           V[o] = vi;
         }
         if (act & (ACT_STEP | ACT_TRAN_INIT)) {
-          if (I.v_tpp) I.v_tpp[o] = (act & ACT_TRAN_INIT) ? vi : VT[o];  // the LTE predictor's older point
+          if (P.lte_rel > 0.0 && I.v_tpp)  // the LTE predictor's older point
+            I.v_tpp[o] = (act & ACT_TRAN_INIT) ? vi : VT[o];
           VT[o] = vi;
         }
       }
@@ -2036,7 +2039,8 @@ __device__ void lu_big_instance(const DevTopo& Tp, const DevInst& I, const JobPa
           V[o] = vi;
         }
         if (a & (ACT_STEP | ACT_TRAN_INIT)) {
-          if (I.v_tpp) I.v_tpp[o] = (a & ACT_TRAN_INIT) ? vi : VT[o];  // the LTE predictor's older point
+          if (P.lte_rel > 0.0 && I.v_tpp)  // the LTE predictor's older point
+            I.v_tpp[o] = (a & ACT_TRAN_INIT) ? vi : VT[o];
           VT[o] = vi;
         }
       }
@@ -3318,7 +3322,7 @@ __global__ void k_tran_start(DevTopo T, DevInst I, JobParams P, int init_caps) {
     const double vi = I.v[i * ld + g];
     I.x[i * ld + g] = vi;
     I.v_tp[i * ld + g] = vi;
-    if (init_caps && I.v_tpp) I.v_tpp[i * ld + g] = vi;
+    if (init_caps && P.lte_rel > 0.0 && I.v_tpp) I.v_tpp[i * ld + g] = vi;
   }
   if (init_caps) s.hprev = 0.0;  // a fresh transient: no previous sub-step for the LTE test
   if (init_caps)
