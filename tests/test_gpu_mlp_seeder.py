@@ -111,3 +111,44 @@ def test_mlp_seed_needs_a_trained_seeder(product, ctx):
     other = product.Problem(ctx, circuits.config2(), max_instances=1)
     with pytest.raises(product.KaramError):
         other.set_seeder(seeder)
+
+
+def _vdd_family(nl, first, n):
+    """Config 5's instances: the chain's MC device variation and VDD ~ U(1.2, 2.0)."""
+    inst = circuits.mc_instances(nl, n, first_instance=first)
+    vdd = np.random.default_rng(first).uniform(1.2, 2.0, n)
+    inst.vs_dc = np.stack([vdd, np.full(n, 0.9)], axis=1)
+    return inst
+
+
+def test_mlp_seeder_on_the_vdd_family_matches_oracle(product, ctx, port):
+    """Config 5's family (the 256-stage chain, VIN 0.9 V, VDD ~ U(1.2, 2.0) and
+    the MC variation): a seeder trained on plain-NR solutions of 2048
+    instances seeds 32 held-out ones: the seeded solves converge on at least
+    as many instances as plain NR, in fewer iterations on average, and where
+    the oracle (FP64, sparse LU) converges too they reach its solution within
+    the tolerance. (Outcomes of plain NR on this family depend on the
+    precision: the bench compares them with the oracle's separately.)"""
+    nl = circuits.inverter_chain(stages=256, vdd=1.8, vin=0.9)
+    plain = product.options(precision=A.PREC_MIXED, **POLISH)
+    train = _vdd_family(nl, 2_000_000, 2048)
+    ptrain, _, _ = _dc_batch(product, ctx, nl, train, plain)
+    seeder = product.Seeder(ptrain, width=256, hidden_layers=2, init_seed=5)
+    assert seeder.add_dc(ptrain) > 1000
+    seeder.train(epochs=20, batch=128, lr=1e-3, shuffle_seed=7)
+    held = _vdd_family(nl, 3_000_000, 32)
+    prob, v_plain, st_plain = _dc_batch(product, ctx, nl, held, plain)
+    prob.set_seeder(seeder)
+    v, st = prob.solve_dc(product.options(precision=A.PREC_MIXED, seeded=A.SEED_MLP, **POLISH))
+    conv = lambda sts: sum(s["status"] == A.ST_CONVERGED for s in sts)
+    assert conv(st) >= conv(st_plain)
+    checked = 0
+    for i in range(0, held.n, 4):
+        v_ref, st_ref = port.solve_dc(nl, held, i, linear_solver=1, **POLISH)
+        if st_ref["converged"] and st[i]["status"] == A.ST_CONVERGED:
+            assert scaled_err(v[i], v_ref) <= 1.0, (i, scaled_err(v[i], v_ref))
+            checked += 1
+    assert checked >= 4
+    assert np.mean([s["iterations"] for s in st]) < np.mean([s["iterations"] for s in st_plain])
+    prob.set_seeder(None)
+    seeder.close()
