@@ -854,6 +854,7 @@ __global__ void __launch_bounds__(256, 4) k_es(DevTopo T, DevInst I, JobParams P
               acc = c < 0 ? acc - gq : acc + gq;
             }
           }
+#pragma unroll 4
           for (int q = it.y; q < it.y + it.z; ++q) {
             const int c = __ldg(&T.es_jt[q]);  // sign | offset of the value (gds, gm, diode g)
             const double val = sd[c & 0x7fffffff];
