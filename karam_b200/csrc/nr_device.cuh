@@ -1308,6 +1308,7 @@ __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __rest
       const int h = prog[to + 2 * t], off = tpb + prog[to + 2 * t + 1];
       const int sl = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
       T acc = A[sl];
+#pragma unroll 4
       for (int q = 0; q < c; ++q) {
         const int pr = prog[off + q];
         acc -= A[pr & 0xFFFF] * A[(pr >> 16) & 0xFFFF];
@@ -1319,6 +1320,7 @@ __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __rest
       const int h = prog[yo + 2 * r], off = ypb + prog[yo + 2 * r + 1];
       const int row = h & 0xFFFF, c = (h >> 16) & 0xFFFF;
       T acc = y[row];
+#pragma unroll 4
       for (int q = 0; q < c; ++q) {
         const int pr = prog[off + q];
         acc -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
@@ -1358,6 +1360,7 @@ __device__ bool nd_solve(T* __restrict__ A, T* __restrict__ y, const int* __rest
       const int k = a & 0xFFFF, d = (a >> 16) & 0xFFFF;
       const int c = b & 0xFFFF, off = bpb + ((b >> 16) & 0xFFFF);
       T sv = y[k];
+#pragma unroll 4
       for (int j = 0; j < c; ++j) {
         const int pr = prog[off + j];
         sv -= A[pr & 0xFFFF] * y[(pr >> 16) & 0xFFFF];
