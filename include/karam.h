@@ -345,7 +345,8 @@ KARAM_API int karam_run_mc_device(karam_problem *p, const karam_solver_opts *opt
  * to about 8 s of GPU clock; a solve that finds none is singular and the call
  * returns KARAM_E_CUDA after the job, results still readable). KARAM_E_INVALID
  * with a message naming the problem when one does not fit (evaluation or
- * factor data beyond a CTA's shared memory). */
+ * factor data beyond a CTA's shared memory), and for a problem listed twice or
+ * problems of different contexts. */
 KARAM_API int karam_run_mc_multi(karam_problem *const *probs, int32_t n_probs,
                                  const karam_solver_opts *opts, double dt, int32_t n_steps,
                                  int32_t method);

@@ -1323,6 +1323,11 @@ int karam_run_mc_multi(karam_problem* const* probs, int32_t n_probs, const karam
   if (!probs || n_probs < 1) return KARAM_E_INVALID;
   for (int j = 0; j < n_probs; ++j)
     if (!probs[j] || probs[j]->ctx != probs[0]->ctx) return KARAM_E_INVALID;
+  {  // each problem once: its buffers are its instances' state for the launch
+    std::vector<const karam_problem*> seen(probs, probs + n_probs);
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return KARAM_E_INVALID;
+  }
   karam_ctx* ctx = probs[0]->ctx;
   return guarded(ctx, [&] {
     for (int j = 0; j < n_probs; ++j) need_device(probs[j]);

@@ -99,3 +99,26 @@ def test_uneven_batch_in_one_launch_equals_per_problem_runs(product, ctx, prec):
         assert sum(s["status"] == A.ST_CONVERGED for s in st) >= len(st) - 1
     for p in probs:
         p.close()
+
+
+def test_multi_launch_argument_errors(product, ctx):
+    nl = circuits.config1()
+    p = product.Problem(ctx, nl, max_instances=1)
+    p.set_instances(None)
+    with pytest.raises(product.KaramError) as e:
+        product.run_mc_multi([p, p], 0.0, 0, A.TRAN_BE, product.options())
+    assert e.value.code == A.KARAM_E_INVALID
+    ctx2 = product.Context(0)
+    q = product.Problem(ctx2, nl, max_instances=1)
+    q.set_instances(None)
+    with pytest.raises(product.KaramError) as e:
+        product.run_mc_multi([p, q], 0.0, 0, A.TRAN_BE, product.options())
+    assert e.value.code == A.KARAM_E_INVALID
+    # one problem alone in the multi launch equals its own persistent solve
+    product.run_mc_multi([p], 0.0, 0, A.TRAN_BE, product.options(precision=A.PREC_FP64))
+    v1, s1 = p.read_results()
+    v2, s2 = p.solve_dc(product.options(precision=A.PREC_FP64, schedule=-4))
+    assert np.array_equal(v1, v2) and stats_key(s1) == stats_key(s2)
+    q.close()
+    ctx2.close()
+    p.close()
