@@ -966,27 +966,190 @@ void nd_program(Topology& T) {
 
 }  // namespace
 
-// Sum of popcount(r[q] & m[q]) over q0 <= q <= q1. On x86-64 it is built with
-// and without the POPCNT instruction, and the loader picks the one the host
-// supports; the generic popcount is several times slower on this loop.
-#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
-__attribute__((target_clones("popcnt", "default")))
-#endif
-static uint64_t and_popcount(const uint64_t* r, const uint64_t* m, int q0, int q1) {
-  uint64_t s = 0;
-  for (int q = q0; q <= q1; ++q) s += (uint64_t)__builtin_popcountll(r[q] & m[q]);
-  return s;
+// Min-Fill on sparse adjacency. Adjacency is a sorted vector per vertex and
+// membership tests go through stamp arrays, so memory and time follow the
+// graph's size, not n^2. Fill counts are updated from the elimination's new
+// edges instead of being recounted. With u eliminated, K = N(u), and for a
+// neighbour w: A = N(w) \ {u}, C = the vertices of K that become new
+// neighbours of w (w's new edges), E_A = the new edges with both ends in A,
+//   fill'(w) = fill(w) - |A \ K| - E_A + sum over c in C of |(A \ K) \ N(c)|
+// (the pairs (u, y) leave, new edges inside A stop being missing, and each new
+// neighbour c is missing exactly the old neighbours outside K it is not
+// adjacent to). Every vertex outside K and u loses one missing pair per new
+// edge with both ends among its neighbours. Integer counts, so the order is
+// the recount's, ties included.
+static MinFillResult min_fill_sparse(const std::vector<std::vector<uint32_t>>& factors,
+                                     const std::unordered_map<uint32_t, int>& dense,
+                                     const std::vector<uint32_t>& ids, std::vector<int> extra,
+                                     size_t n_listed) {
+  const int nv = (int)ids.size();
+  std::vector<std::vector<int>> adj(nv);
+  for (const auto& f : factors)
+    for (size_t i = 0; i < f.size(); ++i)
+      for (size_t j = i + 1; j < f.size(); ++j)
+        if (f[i] != f[j]) {
+          const int a = dense.at(f[i]), b = dense.at(f[j]);
+          adj[a].push_back(b);
+          adj[b].push_back(a);
+        }
+  for (auto& r : adj) {
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+  }
+  // stamp arrays: mark[x] == g tags x in the current set
+  std::vector<uint32_t> in_k(nv, 0), mark(nv, 0);
+  uint32_t gk = 0, gm = 0;
+  std::vector<uint32_t> fill(nv, 0);
+  for (int u = 0; u < nv; ++u) {
+    ++gm;
+    for (int x : adj[u]) mark[x] = gm;
+    uint64_t inside = 0;
+    for (int x : adj[u])
+      for (int y : adj[x]) inside += mark[y] == gm;
+    const uint64_t k = adj[u].size();
+    fill[u] = (uint32_t)((k * (k - 1) - inside) / 2);
+  }
+  std::set<std::pair<uint32_t, uint32_t>> pq;  // (fill, id)
+  for (int u = 0; u < nv; ++u) pq.insert({fill[u], ids[u]});
+  std::vector<char> alive(nv, 1);
+  std::vector<int> ghosts(nv, 0);
+  MinFillResult out;
+  out.ordering.reserve(n_listed);
+  uint32_t maxclique = 0;
+  std::vector<int> nb, touched, merged;
+  std::vector<std::vector<int>> partners;  // per position in nb: new neighbours, ascending
+  std::vector<uint32_t> dec(nv, 0);
+  std::vector<uint32_t> newfill;
+  while (!pq.empty()) {
+    auto top = *pq.begin();
+    pq.erase(pq.begin());
+    const int u = dense.at(top.second);
+    out.ordering.push_back(top.second);
+    if (!alive[u]) {  // repeated listing: isolated by now
+      maxclique = std::max<uint32_t>(maxclique, 1);
+      if (--ghosts[u] > 0) pq.insert({0u, ids[u]});
+      continue;
+    }
+    nb = adj[u];
+    const int k = (int)nb.size();
+    maxclique = std::max<uint32_t>(maxclique, (uint32_t)k + 1);
+    ++gk;
+    in_k[u] = gk;
+    for (int w : nb) in_k[w] = gk;
+    // new edges: for each a in K, the members of K \ {a} it is not adjacent to
+    if ((int)partners.size() < k) partners.resize(k);
+    for (int i = 0; i < k; ++i) {
+      const int a = nb[i];
+      auto& pa = partners[i];
+      pa.clear();
+      const auto& ra = adj[a];
+      size_t p = 0;
+      for (int j = 0; j < k; ++j) {
+        const int b = nb[j];
+        if (b == a) continue;
+        while (p < ra.size() && ra[p] < b) ++p;
+        if (p == ra.size() || ra[p] != b) pa.push_back(b);
+      }
+    }
+    // vertices outside K and u adjacent to both ends of a new edge
+    touched.clear();
+    for (int i = 0; i < k; ++i) {
+      const int a = nb[i];
+      for (int b : partners[i]) {
+        if (b < a) continue;
+        const auto& ra = adj[a];
+        const auto& rb = adj[b];
+        size_t p = 0, q = 0;
+        while (p < ra.size() && q < rb.size()) {
+          if (ra[p] < rb[q]) {
+            ++p;
+          } else if (rb[q] < ra[p]) {
+            ++q;
+          } else {
+            const int w = ra[p];
+            if (in_k[w] != gk && dec[w]++ == 0) touched.push_back(w);
+            ++p;
+            ++q;
+          }
+        }
+      }
+    }
+    // neighbours of u: the update rule above, on the old adjacency
+    newfill.assign(k, 0);
+    for (int i = 0; i < k; ++i) {
+      const int w = nb[i];
+      ++gm;
+      int64_t out_k = 0;  // |A \ K|
+      for (int x : adj[w]) {
+        mark[x] = gm;
+        out_k += in_k[x] != gk;
+      }
+      int64_t e_a = 0;
+      for (int j = 0; j < k; ++j) {
+        const int a = nb[j];
+        if (a == w || mark[a] != gm) continue;
+        for (int b : partners[j])
+          if (b > a && b != w && mark[b] == gm) ++e_a;
+      }
+      int64_t cross = 0;
+      for (int c : partners[i]) {
+        int64_t seen = 0;
+        for (int x : adj[c]) seen += mark[x] == gm && in_k[x] != gk;
+        cross += out_k - seen;
+      }
+      newfill[i] = (uint32_t)((int64_t)fill[w] - out_k - e_a + cross);
+    }
+    // new adjacency: N(a) \ {u} merged with a's new neighbours
+    for (int i = 0; i < k; ++i) {
+      const int a = nb[i];
+      const auto& ra = adj[a];
+      const auto& pa = partners[i];
+      merged.clear();
+      merged.reserve(ra.size() + pa.size());
+      size_t p = 0, q = 0;
+      while (p < ra.size() || q < pa.size()) {
+        if (q == pa.size() || (p < ra.size() && ra[p] < pa[q])) {
+          if (ra[p] != u) merged.push_back(ra[p]);
+          ++p;
+        } else {
+          merged.push_back(pa[q++]);
+        }
+      }
+      adj[a].swap(merged);
+    }
+    adj[u].clear();
+    adj[u].shrink_to_fit();
+    alive[u] = 0;
+    for (int w : touched) {
+      pq.erase({fill[w], ids[w]});
+      fill[w] -= dec[w];
+      dec[w] = 0;
+      pq.insert({fill[w], ids[w]});
+    }
+    for (int i = 0; i < k; ++i) {
+      const int w = nb[i];
+      pq.erase({fill[w], ids[w]});
+      fill[w] = newfill[i];
+      pq.insert({fill[w], ids[w]});
+    }
+    if (extra[u] > 0) {
+      ghosts[u] = extra[u];
+      pq.insert({0u, ids[u]});
+      extra[u] = 0;
+    }
+  }
+  out.treewidth = maxclique > 0 ? (int)maxclique - 1 : 0;
+  return out;
 }
 
 // Min-Fill elimination with the reference's choice rule: at every step the
 // vertex with the fewest missing neighbour pairs, ties to the smallest id
 // (treewidth_analyzer.cpp:72-102). Instead of rescanning every vertex, fill
 // counts live in an ordered set keyed (fill, id) and only vertices whose
-// neighbourhood changed are updated: the eliminated vertex's neighbours are
-// recounted, and every other vertex adjacent to both ends of a new fill edge
-// loses one missing pair. A variable id listed twice (the reference's branch
-// id that equals the node count) is eliminated twice, the second time as an
-// isolated vertex, which is what the reference's map-keyed adjacency does.
+// neighbourhood changed are updated (min_fill_sparse above). A variable id
+// listed twice (the reference's branch id that equals the node count) is
+// eliminated twice, the second time as an isolated vertex, which is what the
+// reference's map-keyed adjacency does.
 MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
                        const std::vector<uint32_t>& variables) {
   std::unordered_map<uint32_t, int> dense;
@@ -1002,166 +1165,7 @@ MinFillResult min_fill(const std::vector<std::vector<uint32_t>>& factors,
       extra[it->second]++;
     }
   }
-  const int nv = (int)ids.size();
-  // Adjacency as bit rows when it fits (up to 16384 vertices, 32 MiB), else
-  // hash sets. With bit rows a membership test is a bit test, a vertex's
-  // missing neighbour pairs are a sum of popcounts and its neighbours come out
-  // ascending: the same integers as with the sets, so the order and its ties
-  // do not change. Each row keeps the span of words it has ever occupied, and
-  // every scan of the row stays inside it.
-  const bool bits = nv <= bitrow_max();
-  const size_t words = ((size_t)nv + 63) / 64;
-  std::vector<uint64_t> brow(bits ? words * (size_t)nv : 0);
-  std::vector<int> rlo(bits ? nv : 0, (int)words), rhi(bits ? nv : 0, -1);
-  std::vector<std::unordered_set<int>> adj(bits ? 0 : nv);
-  auto has = [&](int a, int b) -> bool {
-    if (bits) return (brow[(size_t)a * words + (b >> 6)] >> (b & 63)) & 1ull;
-    return adj[a].count(b) != 0;
-  };
-  auto link = [&](int a, int b) {
-    if (bits) {
-      brow[(size_t)a * words + (b >> 6)] |= 1ull << (b & 63);
-      brow[(size_t)b * words + (a >> 6)] |= 1ull << (a & 63);
-      rlo[a] = std::min(rlo[a], b >> 6);
-      rhi[a] = std::max(rhi[a], b >> 6);
-      rlo[b] = std::min(rlo[b], a >> 6);
-      rhi[b] = std::max(rhi[b], a >> 6);
-    } else {
-      adj[a].insert(b);
-      adj[b].insert(a);
-    }
-  };
-  auto unlink = [&](int a, int b) {
-    if (bits) {
-      brow[(size_t)a * words + (b >> 6)] &= ~(1ull << (b & 63));
-      brow[(size_t)b * words + (a >> 6)] &= ~(1ull << (a & 63));
-    } else {
-      adj[a].erase(b);
-      adj[b].erase(a);
-    }
-  };
-  auto neighbours = [&](int u, std::vector<int>& out) {  // ascending
-    out.clear();
-    if (bits) {
-      const uint64_t* r = &brow[(size_t)u * words];
-      for (int q = rlo[u]; q <= rhi[u]; ++q)
-        for (uint64_t c = r[q]; c; c &= c - 1) out.push_back(q * 64 + __builtin_ctzll(c));
-    } else {
-      out.assign(adj[u].begin(), adj[u].end());
-      std::sort(out.begin(), out.end());
-    }
-  };
-  for (const auto& f : factors)
-    for (size_t i = 0; i < f.size(); ++i)
-      for (size_t j = i + 1; j < f.size(); ++j)
-        if (f[i] != f[j]) link(dense.at(f[i]), dense.at(f[j]));
-  std::vector<uint64_t> mask(bits ? words : 0);
-  std::vector<int> cf_nb;
-  auto count_fill = [&](int u) -> uint32_t {
-    neighbours(u, cf_nb);
-    const std::vector<int>& nb = cf_nb;
-    if (nb.empty()) return 0;
-    if (bits) {
-      // missing pairs = (k (k - 1) - sum over neighbours of their neighbours in N(u)) / 2
-      const int lo = nb.front() >> 6, hi = nb.back() >> 6;
-      for (int w : nb) mask[w >> 6] |= 1ull << (w & 63);
-      uint64_t inside = 0;
-      for (int w : nb) {
-        inside += and_popcount(&brow[(size_t)w * words], mask.data(), std::max(lo, rlo[w]), std::min(hi, rhi[w]));
-      }
-      for (int w : nb) mask[w >> 6] = 0;
-      const uint64_t k = nb.size();
-      return (uint32_t)((k * (k - 1) - inside) / 2);
-    }
-    uint32_t c = 0;
-    for (size_t i = 0; i < nb.size(); ++i) {
-      const auto& ai = adj[nb[i]];
-      for (size_t j = i + 1; j < nb.size(); ++j)
-        if (!ai.count(nb[j])) ++c;
-    }
-    return c;
-  };
-  std::vector<uint32_t> fill(nv);
-  std::set<std::pair<uint32_t, uint32_t>> pq;  // (fill, id)
-  for (int u = 0; u < nv; ++u) {
-    fill[u] = count_fill(u);
-    pq.insert({fill[u], ids[u]});
-  }
-  std::vector<char> alive(nv, 1);
-  std::vector<int> ghosts(nv, 0);
-  MinFillResult out;
-  out.ordering.reserve(variables.size());
-  uint32_t maxclique = 0;
-  std::vector<int> nb, touched;
-  std::unordered_set<int> nbset;
-  std::vector<uint32_t> dec(nv, 0);  // missing pairs each vertex loses this step
-  auto lose = [&](int w) {
-    if (dec[w]++ == 0) touched.push_back(w);
-  };
-  while (!pq.empty()) {
-    auto top = *pq.begin();
-    pq.erase(pq.begin());
-    int u = dense.at(top.second);
-    out.ordering.push_back(top.second);
-    if (!alive[u]) {  // repeated listing: isolated by now
-      maxclique = std::max<uint32_t>(maxclique, 1);
-      if (--ghosts[u] > 0) pq.insert({0u, ids[u]});
-      continue;
-    }
-    neighbours(u, nb);
-    maxclique = std::max<uint32_t>(maxclique, (uint32_t)nb.size() + 1);
-    if (bits) {
-      for (int w : nb) mask[w >> 6] |= 1ull << (w & 63);
-      mask[u >> 6] |= 1ull << (u & 63);  // u is no candidate either
-    } else {
-      nbset.clear();
-      nbset.insert(nb.begin(), nb.end());
-    }
-    touched.clear();
-    for (size_t i = 0; i < nb.size(); ++i)
-      for (size_t j = i + 1; j < nb.size(); ++j) {
-        const int a = nb[i], b = nb[j];
-        if (has(a, b)) continue;
-        link(a, b);
-        // vertices outside N(u) adjacent to both a and b lose a missing pair
-        if (bits) {
-          const uint64_t* ra = &brow[(size_t)a * words];
-          const uint64_t* rb = &brow[(size_t)b * words];
-          const int q1 = std::min(rhi[a], rhi[b]);
-          for (int q = std::max(rlo[a], rlo[b]); q <= q1; ++q)
-            for (uint64_t c = ra[q] & rb[q] & ~mask[q]; c; c &= c - 1) lose(q * 64 + __builtin_ctzll(c));
-        } else {
-          const auto& sa = adj[a].size() <= adj[b].size() ? adj[a] : adj[b];
-          const auto& sb = adj[a].size() <= adj[b].size() ? adj[b] : adj[a];
-          for (int w : sa)
-            if (w != a && w != b && w != u && !nbset.count(w) && sb.count(w)) lose(w);
-        }
-      }
-    for (int w : nb) unlink(w, u);
-    if (bits) {
-      for (int w : nb) mask[w >> 6] = 0;
-      mask[u >> 6] = 0;
-    }
-    alive[u] = 0;
-    for (int w : touched) {
-      pq.erase({fill[w], ids[w]});
-      fill[w] -= dec[w];
-      dec[w] = 0;
-      pq.insert({fill[w], ids[w]});
-    }
-    for (int w : nb) {
-      pq.erase({fill[w], ids[w]});
-      fill[w] = count_fill(w);
-      pq.insert({fill[w], ids[w]});
-    }
-    if (extra[u] > 0) {
-      ghosts[u] = extra[u];
-      pq.insert({0u, ids[u]});
-      extra[u] = 0;
-    }
-  }
-  out.treewidth = maxclique > 0 ? (int)maxclique - 1 : 0;
-  return out;
+  return min_fill_sparse(factors, dense, ids, std::move(extra), variables.size());
 }
 
 namespace {
