@@ -579,14 +579,15 @@ def run_karam(args, dist):
     ctx.close()
 
 
-def config4_tile(ctx, N=64, steps=1000, dt=1e-12, n_check=32, check_steps=150):
+def config4_tile(ctx, N=64, steps=1000, dt=1e-12, n_check=32, check_steps=150, big_N=128, big_steps=100):
     """Tiles of the large single-instance workload (circuits.power_grid_mesh):
     one N x N mesh, DC then `steps` backward-Euler steps of `dt`, FP32 LU +
     FP64 refinement against plain FP64 on the GPU (the level-scheduled
     kernels; the 1024 x 1024 mesh itself needs the supernodal solver, which is
     not built). Accuracy and the CPU rate: an n_check x n_check tile, DC +
     check_steps steps, GPU mixed precision against the reference-built oracle
-    (sparse LU), one thread."""
+    (sparse LU), one thread. Then a big_N x big_N tile, DC + big_steps steps,
+    with the oracle's KCL residual as its accuracy check."""
     import karam_b200 as K
     from karam_b200 import _abi as A
     from karam_b200 import circuits
@@ -639,6 +640,37 @@ def config4_tile(ctx, N=64, steps=1000, dt=1e-12, n_check=32, check_steps=150):
                            "kind": "reference" if kind == "ref" else "port",
                            "sample": f"the {n_check} x {n_check} tile, DC + {check_steps} steps, sparse LU "
                                      f"(solveSparse_LU with the Min-Fill ordering), {cpu_t:.1f} s"}
+    # a 128 x 128 tile: the largest the level-scheduled kernels take; its
+    # accuracy is the oracle's KCL residual at the DC point and the last step
+    # (the oracle's own solve is a dense LU at this size)
+    nl = circuits.power_grid_mesh(big_N)
+    t = time.perf_counter()
+    prob = K.Problem(ctx, nl, max_instances=1)
+    analysis_s = time.perf_counter() - t
+    prob.set_instances(None)
+    big = {"tile": f"{big_N} x {big_N} (n = {nl.n_nodes}), DC + {big_steps} BE steps of {dt * 1e12:g} ps",
+           "host_analysis_s": analysis_s}
+    for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        opts = K.options(precision=prec, **POLISH)
+        prob.run_mc_device(dt, 2, A.TRAN_BE, opts)  # warm-up
+        t = time.perf_counter()
+        prob.run_mc_device(dt, big_steps, A.TRAN_BE, opts)
+        wall = time.perf_counter() - t
+        tm = prob.timing()
+        _, st = prob.read_results()
+        big[name] = {"solves_per_s": (big_steps + 1) / wall if st[0]["status"] == A.ST_CONVERGED else 0.0,
+                     "wall_s": wall, "device_ms": tm["job_ms"], "rounds": tm["rounds"],
+                     "iterations": st[0]["iterations"], "converged": st[0]["status"] == A.ST_CONVERGED,
+                     "schedule": lu_name_of(tm)}
+    vdc, _ = prob.solve_dc(K.options(precision=A.PREC_MIXED, **POLISH))
+    nodes = np.arange(1, nl.n_nodes + 1, dtype=np.int32)
+    v, _, wave = prob.step_transient(dt, 2, A.TRAN_BE, K.options(precision=A.PREC_MIXED, **POLISH),
+                                     wave_nodes=nodes)
+    prob.close()
+    with native_stdout_to_stderr():
+        big["kcl_residual_dc"] = orc.kcl_residual(nl, vdc[0])
+        big["kcl_residual_step2"] = orc.kcl_residual(nl, v[0], h=dt, v_prev=wave[0][0], t=2 * dt)
+    out["tile128"] = big
     return out
 
 

@@ -220,6 +220,27 @@ class Oracle:
         assert rc >= 0, rc
         return re + 1j * im, rc
 
+    def kcl_residual(self, nl, v, inst=None, idx=0, h=0.0, v_prev=None, t=0.0):
+        """Scaled KCL residual of v: the stamp at v (a DC stamp when h == 0,
+        else a backward-Euler step of h from v_prev at time t) gives the
+        Newton system J x = rhs whose fixed point is a solution, so r = J v -
+        rhs is the node current imbalance (branch equations for sources).
+        Returns max_i |r_i| / (sum_j |J_ij v_j| + |rhs_i|): about 1e-13 at a
+        converged point, and about half the relative error of a perturbed one.
+        Needs no factorisation, so it checks problems the oracle's own solve
+        is too slow for."""
+        rp, col = self.pattern(nl)
+        cvp = None
+        if v_prev is not None:
+            vn = np.concatenate([[0.0], np.asarray(v_prev, np.float64)])
+            cvp = np.array([vn[a] - vn[b] for a, b, _ in nl.cap])
+        vals, rhs = self.stamp(nl, v, inst, idx, h=h, method=A.TRAN_BE, cap_vprev=cvp, t=t)
+        v = np.asarray(v, np.float64)
+        rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+        r = np.bincount(rows, vals * v[col], minlength=len(v)) - rhs
+        scale = np.bincount(rows, np.abs(vals * v[col]), minlength=len(v)) + np.abs(rhs)
+        return float(np.max(np.abs(r) / (scale + 1e-300)))
+
     def transient(self, nl, v_start, dt, n_steps, method=A.TRAN_BE, inst=None, idx=0,
                   wave_nodes=None, **opt):
         s = nl.as_struct()

@@ -261,3 +261,27 @@ def test_lte_step_control_in_the_oracle(port, ref):
     assert np.max(np.abs(wp - wr)) <= 1e-9 * np.max(np.abs(wr)) + 1e-12
     _, s0, _ = port.transient(nl, v, 40e-12, 20, A.TRAN_TRAP, **kw)
     assert s0["lte_rejects"] == 0 and s0["halvings"] == 0
+
+
+def test_kcl_residual_check_in_the_oracle(port):
+    """The residual check the large mesh tiles are held to (Oracle.kcl_residual)
+    accepts the oracle's own converged DC point and every backward-Euler step
+    across the gates' edge of a 16 x 16 mesh tile (all nodes recorded per
+    step), and rejects a point moved by 1e-6 relative, a step checked
+    against the wrong previous point and one checked at the wrong time."""
+    nl = circuits.power_grid_mesh(16)
+    vd, st = port.solve_dc(nl, linear_solver=1, polish_max=8)
+    assert st["converged"] == 1 and port.kcl_residual(nl, vd) < 1e-11
+    assert port.kcl_residual(nl, vd * (1 + 1e-6)) > 1e-7
+    dt, steps = 5e-12, 30
+    _, s1, w = port.transient(nl, vd, dt, steps, A.TRAN_BE, wave_nodes=np.arange(1, nl.n_nodes + 1),
+                              linear_solver=1, polish_max=8)
+    assert s1["converged"] == 1 and s1["halvings"] == 0
+    prev = vd
+    for k in range(steps):
+        assert port.kcl_residual(nl, w[k], h=dt, v_prev=prev, t=(k + 1) * dt) < 1e-11
+        prev = w[k]
+    assert np.max(np.abs(w[-1] - vd)) > 1e-3  # the loads switched on
+    # the capacitor currents are small beside the 0.1-1 ohm segment currents
+    assert port.kcl_residual(nl, w[-1], h=dt, v_prev=vd, t=steps * dt) > 1e-9
+    assert port.kcl_residual(nl, w[-1], h=dt, v_prev=w[-2], t=dt) > 1e-7

@@ -3,8 +3,10 @@
 the border every 64 nodes, pulsed NMOS loads with a 1 ns period) at tile size
 on the GPU: a 32 x 32 tile (1026 unknowns), DC then 150 backward-Euler steps
 of 1 ps across the gates' first edge, in FP64 and in mixed precision, against
-the oracle's sparse LU. The full 1024 x 1024 mesh needs the supernodal
-solver, which is not built; this checks the family's circuit and values."""
+the oracle's sparse LU; and a 128 x 128 tile (16386 unknowns) held to the
+oracle's KCL residual at every step. The full 1024 x 1024 mesh needs the
+supernodal solver, which is not built; this checks the family's circuit and
+values."""
 import functools
 
 import numpy as np
@@ -54,4 +56,34 @@ def test_mesh_tile_dc_and_transient_match_oracle(product, ctx, port, prec):
         assert np.max(np.abs(wave[i] - w_ref)) <= 1e-9 * np.max(np.abs(w_ref)) + 1e-12
     # the loads switch on during the window: the supply droops at the far node
     assert np.min(wave[0][:, -1]) < np.max(wave[0][:, -1])
+    prob.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+def test_mesh_128_tile_satisfies_kcl_at_every_step(product, ctx, port, prec):
+    """A 128 x 128 tile (16386 unknowns) of the same family: ordered by the
+    sparse Min-Fill and factored by the block-per-instance kernel with its
+    slots in global memory. The oracle's own solve (a dense LU at this size)
+    is too slow, so the DC point and every backward-Euler step across the
+    gates' edge, with all nodes recorded, are held to the oracle's KCL
+    residual (Oracle.kcl_residual: ~1e-13 at a converged point, ~5e-7 for a
+    1e-6 relative error, ~1.5e-8 for a step taken from the wrong previous
+    point)."""
+    n_side, dt, steps = 128, 5e-12, 30
+    nl = circuits.power_grid_mesh(n_side)
+    prob = product.Problem(ctx, nl, max_instances=1)
+    prob.set_instances(None)
+    opts = product.options(precision=prec, **POLISH)
+    vdc, st = prob.solve_dc(opts)
+    assert st[0]["status"] == A.ST_CONVERGED
+    assert port.kcl_residual(nl, vdc[0]) < 1e-9
+    nodes = np.arange(1, nl.n_nodes + 1, dtype=np.int32)
+    v, stt, wave = prob.step_transient(dt, steps, A.TRAN_BE, opts, wave_nodes=nodes)
+    assert stt[0]["status"] == A.ST_CONVERGED and stt[0]["halvings"] == 0
+    prev = vdc[0]
+    for k in range(steps):
+        assert port.kcl_residual(nl, wave[0][k], h=dt, v_prev=prev, t=(k + 1) * dt) < 1e-9, k
+        prev = wave[0][k]
+    assert np.array_equal(wave[0][-1], v[0])
+    assert np.max(np.abs(v[0] - vdc[0])) > 1e-3  # the loads switched on
     prob.close()
