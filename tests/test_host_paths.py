@@ -1,9 +1,10 @@
 """The host symbolic analysis keeps its structures as bit rows up to a size
-limit (16384 unknowns) and in sorted vectors, ordered sets and hash sets
-beyond it. Both representations must give identical orderings, filled
-patterns, LU programs, level schedules and stamp maps. KARAM_BITROW_MAX moves
-the limit, so the large-problem code runs here on small cases in a child
-process and its tables are compared with the default path's. CPU only."""
+limit (16384 unknowns) and in sorted vectors and ordered sets beyond it (the
+Min-Fill ordering has one sparse path at every size). Both representations
+must give identical orderings, filled patterns, LU programs, level schedules
+and stamp maps. KARAM_BITROW_MAX moves the limit, so the large-problem code
+runs here on small cases in a child process and its tables are compared with
+the default path's. CPU only."""
 import os
 import pickle
 import subprocess
