@@ -2,6 +2,8 @@
 cases of the symbolic layer and the NR loop (ragged device mixes, duplicate
 stamp slots, a floating source, a capacitor-only node) and the smallest grid
 of the uneven-batch family."""
+import numpy as np
+
 from karam_b200 import circuits
 from karam_b200.circuits import Netlist
 
@@ -99,6 +101,19 @@ BENCH = {"config1": circuits.config1, "config2": circuits.config2}
 # layer, DC solutions of two Monte-Carlo instances and a trapezoidal waveform
 # of instance 0 (GRID_TRAN), all from the reference-built library.
 GRIDS = {"grid16": 16, "grid32": 32, "grid64": 64}
+# tiles of the power-grid mesh whose Min-Fill ordering (and, where the
+# reference's symbolic factorization finishes in a minute, filled pattern)
+# is pinned to the reference build
+MESH_ORDERINGS = {"mesh64": 64, "mesh128": 128}
+MESH_FILLED = ("mesh64",)
+
+
+def filled_digest(row_ptr, col):
+    """sha256 of a filled pattern's int32 row pointers and columns."""
+    import hashlib
+    h = hashlib.sha256(np.ascontiguousarray(row_ptr, np.int32).tobytes())
+    h.update(np.ascontiguousarray(col, np.int32).tobytes())
+    return h.hexdigest()
 GRID_TRAN = dict(dt=40e-12, steps=20, max_halvings=6)  # the gate ramp: steps 13-18
 GRID_WAVE = {16: [3, 50, 130, 200, 258], 32: [3, 200, 530, 900, 1026],
              64: [3, 900, 2050, 3500, 4098]}

@@ -15,6 +15,7 @@ solveComplexLU_Sparse (and by ACSolver::solveAC_Sparse as it stands).
     python tests/golden/make_golden.py grid8    # only the named cases
     python tests/golden/make_golden.py grid64   # a large grid (minutes: dense-workspace LU)
     python tests/golden/make_golden.py ac_grid8 # one AC sweep fixture (ac_<case>)
+    python tests/golden/make_golden.py mesh128  # a mesh tile's ordering (14 min: the reference's Min-Fill)
 """
 import os
 import sys
@@ -97,6 +98,21 @@ def grid_fixture(ref, name, N):
           out["dc_stats"].tolist(), "tran stats", out["tran_stats"].tolist(), flush=True)
 
 
+def mesh_ordering_fixture(ref, name, N):
+    """Min-Fill ordering of an N x N power-grid mesh tile from the reference
+    build (its ordering rescans every vertex per step: about 20 s at N = 64,
+    14 min at N = 128), with the filled pattern's digest where it is cheap."""
+    nl = circuits.power_grid_mesh(N)
+    raw, perm, tw = ref.ordering(nl)
+    out = dict(raw_order=raw, perm_translated=perm, treewidth=np.int32(tw), n=np.int32(nl.n_nodes))
+    if name in cases.MESH_FILLED:
+        sym = ref.symbolic(nl)
+        out["filled_sha256"] = np.array(cases.filled_digest(sym["row_ptr"], sym["col"]))
+        out["fill_in"] = np.int32(sym["fill_in"])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "n =", nl.n_nodes, "treewidth", tw)
+
+
 def ac_fixture(ref, name):
     """Small-signal AC sweep at a DC point, from the reference build: the
     NR-Jacobian rule (the reference's stamps at the DC point + jwC, solved by
@@ -148,6 +164,10 @@ def main():
         if only and name not in only:
             continue
         grid_fixture(ref, name, N)
+    for name, N in cases.MESH_ORDERINGS.items():
+        if only and name not in only:
+            continue
+        mesh_ordering_fixture(ref, name, N)
     for name, make in {**cases.SMALL, **cases.BENCH}.items():
         if only and name not in only:
             continue

@@ -285,3 +285,23 @@ def test_kcl_residual_check_in_the_oracle(port):
     # the capacitor currents are small beside the 0.1-1 ohm segment currents
     assert port.kcl_residual(nl, w[-1], h=dt, v_prev=vd, t=steps * dt) > 1e-9
     assert port.kcl_residual(nl, w[-1], h=dt, v_prev=w[-2], t=dt) > 1e-7
+
+
+@pytest.mark.parametrize("name", list(cases.MESH_ORDERINGS))
+def test_product_ordering_mesh_tiles(product, name):
+    """The product's Min-Fill (sparse adjacency, incremental fill counts) on
+    power-grid mesh tiles equals the reference build's ordering bit for bit:
+    64 x 64 (n = 4098) with its filled pattern, and 128 x 128 (n = 16386),
+    whose fixture took the reference's own Min-Fill about 14 minutes."""
+    g = golden(name)
+    nl = circuits.power_grid_mesh(cases.MESH_ORDERINGS[name])
+    assert nl.n_nodes == int(g["n"])
+    prob = product.Problem(None, nl)
+    raw, perm, tw = prob.ordering()
+    assert np.array_equal(raw, g["raw_order"]) and np.array_equal(perm, g["perm_translated"])
+    assert tw == int(g["treewidth"])
+    if "filled_sha256" in g:
+        frp, fcol = prob.filled_pattern()
+        assert cases.filled_digest(frp, fcol) == str(g["filled_sha256"])
+        assert prob.info["fill_in"] == int(g["fill_in"])
+    prob.close()
