@@ -395,7 +395,7 @@ def run_karam(args, dist):
         lanes = t["lanes"]
         lu_name = ["k_lu<float>", "k_lu_nd<float>", "k_lu_big<float, smem>",
                    "k_lu_big<float, global>", "k_lu_big<float, packed>",
-                   "k_persist<float>"][t["level_schedule"]]
+                   "k_persist<float>", "k_lu_big<float, global, global y>"][t["level_schedule"]]
         conv_min = min(conv_min, conv)
     clk = clocks.stop()
     dist.barrier()
@@ -677,7 +677,8 @@ def config4_tile(ctx, N=64, steps=1000, dt=1e-12, n_check=32, check_steps=150, b
 def lu_name_of(tm):
     return ["pivot records", "warp per instance", "CTA per instance, shared memory",
             "CTA per instance, global memory", "CTA per instance, packed program",
-            "persistent CTA per instance"][tm["level_schedule"]]
+            "persistent CTA per instance",
+            "CTA per instance, global memory, solve vector in global memory"][tm["level_schedule"]]
 
 
 def ac_sweep_leg(ctx, n_instances=4096, n_points=16, f_start=1e6, f_stop=1e12, input_node=2,
@@ -860,7 +861,9 @@ def config3_uneven(device, n_instances=2048, steps=500, dt=10e-12, oracle_sizes=
             k = ["pivot records", "warp per instance", "CTA per instance, shared memory",
                  "CTA per instance, global memory",
                  "CTA per instance, packed program",
-                 "persistent CTA per instance"][prob.timing()["level_schedule"]]
+                 "persistent CTA per instance",
+                 "CTA per instance, global memory, solve vector in global memory"][
+                     prob.timing()["level_schedule"]]
             kinds[k] = kinds.get(k, 0) + 1
             out[N] = (v, st)
         return wall, conv, kinds, out

@@ -181,7 +181,10 @@ typedef struct karam_solver_opts {
                             memory, -3 one CTA per instance with its slots and
                             the packed level program in shared memory, -4 the
                             persistent kernel: one CTA per instance running all
-                            of its rounds in one launch (the code of -3); 0 =
+                            of its rounds in one launch (the code of -3), -5 one
+                            CTA per instance with its slots and its solve vector
+                            in global memory (taken by 0 only where -2 does not
+                            fit shared memory); 0 =
                             chosen from shared memory, occupancy and batch size
                             (-4 for batches no larger than the SM count where it
                             fits). Batches larger than the SM count switch to
@@ -548,7 +551,9 @@ typedef struct karam_timing {
                                same with the slots in global memory, 4 a CTA per
                                instance with slots and packed program in shared
                                memory, 5 the persistent kernel (all rounds of an
-                               instance in one launch, the code of 4)                */
+                               instance in one launch, the code of 4), 6 a CTA per
+                               instance with slots and solve vector in global
+                               memory                                                 */
   int64_t evals_dc;         /* instance evaluations in DC mode (live instances summed over rounds) */
   int64_t evals_tran;       /* instance evaluations in transient mode                */
   int64_t solves;           /* linear solves by the static-pivot LU                  */

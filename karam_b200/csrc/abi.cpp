@@ -682,7 +682,7 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
     throw std::runtime_error(std::string("no factor/solve schedule fits this problem; last: ") + L.why);
   ck(cudaGetLastError(), "configure kernels");
   p->timing.lanes = L.L;
-  p->timing.level_schedule = L.big ? 1 + L.big : L.nd ? 1 : 0;
+  p->timing.level_schedule = L.big == 5 ? 6 : L.big ? 1 + L.big : L.nd ? 1 : 0;
   RoundLaunch LT;  // the tail's block-per-instance plan (L == 0: no tail switch)
   if (L.nd && p->ni > num_sms) {  // L.nd: the packed program exists
     LT = plan_round(p->dt, p->ni, prec, max_smem, num_sms, -3);
@@ -725,8 +725,9 @@ void run_rounds(karam_problem* p, const JobParams& P, const karam_solver_opts* o
     run_persist(I, p->ni, budget, false);
     return;
   }
-  if (L.big == 2) {  // the ND slots of every instance in global memory
-    const size_t need = (size_t)p->ni * (size_t)p->dt.nd_S * sizeof(double);
+  if (L.big == 2 || L.big == 5) {  // the ND slots of every instance in global memory
+    const size_t per = (size_t)p->dt.nd_S + (L.big == 5 ? (size_t)p->dt.nd_SY : 0);  // 5: + the solve vector
+    const size_t need = (size_t)p->ni * per * sizeof(double);
     if (p->i_luws.bytes < need) p->i_luws.alloc(need);
     I.lu_ws = p->i_luws.p;
   }

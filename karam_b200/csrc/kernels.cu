@@ -59,6 +59,9 @@ const void* lu_kernel(bool mixed, bool nd, int big) {
     return mixed ? (const void*)k_lu_big<float, true, false> : (const void*)k_lu_big<double, true, false>;
   if (big == 3)
     return mixed ? (const void*)k_lu_big<float, false, true> : (const void*)k_lu_big<double, false, true>;
+  if (big == 5)
+    return mixed ? (const void*)k_lu_big<float, true, false, true>
+                 : (const void*)k_lu_big<double, true, false, true>;
   if (nd) return mixed ? (const void*)k_lu_nd<float> : (const void*)k_lu_nd<double>;
   return mixed ? (const void*)k_lu<float> : (const void*)k_lu<double>;
 }
@@ -89,12 +92,15 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
     if (T.nd_prog_len > 0) cands.push_back({1, false, 3, 2});
     cands.push_back({1, false, 1, 2});
     cands.push_back({1, false, 2, 1});
+    cands.push_back({1, false, 5, 1});  // taken only where kind 2 does not fit
   }
   for (int L = kMaxLanes; L >= 1; L >>= 1) cands.push_back({L, false, 0, 0});
+  bool big2_fits = false;
   for (const Cand& c : cands) {
     const int L = c.L;
     if (want_lanes > 0 && (c.big || L != want_lanes)) continue;
     if (want_lanes < 0 && c.big != -want_lanes) continue;
+    if (c.big == 5 && want_lanes == 0 && big2_fits) continue;
     const void* kern = lu_kernel(mixed, c.nd, c.big);
     const int threads = c.big ? kBigThreads : c.nd ? 32 * L : kRoundThreads;
     size_t sm;
@@ -105,6 +111,8 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
            sizeof(int) * (((size_t)T.nd_prog_len + 3) & ~size_t(3));
     else if (c.big == 2)
       sm = (es * (size_t)T.nd_SY + 15) & ~size_t(15);
+    else if (c.big == 5)
+      sm = 0;
     else
       sm = round_smem(T, L, es, c.nd);
     auto reject = [&](const char* what) {
@@ -128,6 +136,7 @@ RoundLaunch plan_round(const DevTopo& T, int ni, int prec, int max_smem, int num
       cudaGetLastError();
       continue;
     }
+    if (c.big == 2) big2_fits = true;
     const int grid = (ni + L - 1) / L;
     const long slots = (long)per_sm * std::max(1, num_sms);
     const long waves = (grid + slots - 1) / slots;
@@ -211,6 +220,11 @@ void launch_lu(const DevTopo& T, const DevInst& I, const JobParams& P, const Rou
       k_lu_big<float, false, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
     else
       k_lu_big<double, false, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+  } else if (L.big == 5) {
+    if (prec == KARAM_PREC_MIXED)
+      k_lu_big<float, true, false, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
+    else
+      k_lu_big<double, true, false, true><<<L.grid, L.threads, L.smem, s>>>(T, I, P, active);
   } else if (L.nd) {
     if (prec == KARAM_PREC_MIXED)
       k_lu_nd<float><<<L.grid, L.threads, L.smem, s>>>(T, I, P, L.L, active);

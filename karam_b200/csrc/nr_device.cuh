@@ -1956,7 +1956,9 @@ __device__ bool big_solve(T* __restrict__ A, T* __restrict__ y, const DevTopo& T
 // the last few live instances of a job): the same round as lu_round with
 // every phase spread over the CTA's threads. The ND slots live in dynamic
 // shared memory after the right-hand side (gA = false) or in the instance's
-// slice of I.lu_ws (gA = true, nd_S elements per instance). With packed,
+// slice of I.lu_ws (gA = true, nd_S elements per instance); with gY the
+// right-hand side goes to I.lu_ws as well, for systems whose n values do not
+// fit shared memory. With packed,
 // the CTA stages the packed program (nd_program) after the slots and solves
 // on it (nd_solve_cta) instead of reading the schedule tables from global
 // memory. With I.live_in, CTA b takes the b-th listed instance and lists it
@@ -1972,14 +1974,18 @@ struct LuShared {
 // sh receives the action bits, whether the instance was live, whether it
 // evaluated a transient point, whether the static pivots failed, and the
 // gmin of the solve.
-template <typename T, bool gA, bool packed>
+template <typename T, bool gA, bool packed, bool gY = false>
 __device__ void lu_big_instance(const DevTopo& Tp, const DevInst& I, const JobParams& P, int g,
                                 unsigned char* smem_raw, LuShared& sh) {
+  static_assert(!gY || (gA && !packed), "the solve vector goes to global memory only beside global slots");
   int &s_a = sh.a, &s_live = sh.live, &s_trev = sh.trev, &s_sing = sh.sing;
   double &s_gmin = sh.gmin, &s_hsub = sh.hsub;
   const int n = Tp.n, tid = threadIdx.x;
   const size_t ld = I.ld;
-  T* Y = reinterpret_cast<T*>(smem_raw);
+  // gY: the solve vector in global memory too, after every instance's slots
+  // (I.lu_ws holds ni * (nd_S + nd_SY) elements)
+  T* Y = gY ? reinterpret_cast<T*>(I.lu_ws) + (size_t)I.ni * Tp.nd_S + (size_t)g * Tp.nd_SY
+            : reinterpret_cast<T*>(smem_raw);
   T* A = gA ? reinterpret_cast<T*>(I.lu_ws) + (size_t)g * Tp.nd_S : Y + Tp.nd_SY;
   const int* prog = nullptr;
   if (packed) {  // after the slots, on a 16-byte boundary
@@ -2108,7 +2114,7 @@ __device__ void lu_big_instance(const DevTopo& Tp, const DevInst& I, const JobPa
   __syncthreads();
 }
 
-template <typename T, bool gA, bool packed>
+template <typename T, bool gA, bool packed, bool gY = false>
 __global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, JobParams P, int* active) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ LuShared sh;
@@ -2117,7 +2123,7 @@ __global__ void __launch_bounds__(kBigThreads) k_lu_big(DevTopo Tp, DevInst I, J
     if ((int)blockIdx.x >= *I.live_in_count) return;
     g = I.live_in[blockIdx.x];
   }
-  lu_big_instance<T, gA, packed>(Tp, I, P, g, smem_raw, sh);
+  lu_big_instance<T, gA, packed, gY>(Tp, I, P, g, smem_raw, sh);
   if (!sh.live) return;
   // rescue hand-off, next evaluation point, bookkeeping
   if (threadIdx.x == 0) {

@@ -589,7 +589,9 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
 void nd_schedule(Topology& T) {
   const int n = T.n;
   T.nd_levels = 0;
-  if (n < 2 || n > 20000) return;
+  // past ~7e4 unknowns the host build takes minutes and one CTA per instance
+  // is the wrong shape for the factorization
+  if (n < 2 || n > 70000) return;
   auto key = [](int r, int c) { return (int64_t(r) << 32) | int64_t(unsigned(c)); };
   // stamped positions (Min-Fill permuted space)
   std::vector<std::pair<int, int>> pos;

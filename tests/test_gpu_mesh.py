@@ -87,3 +87,48 @@ def test_mesh_128_tile_satisfies_kcl_at_every_step(product, ctx, port, prec):
     assert np.array_equal(wave[0][-1], v[0])
     assert np.max(np.abs(v[0] - vdc[0])) > 1e-3  # the loads switched on
     prob.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED])
+def test_global_solve_vector_schedule_equals_shared_one(product, ctx, prec):
+    """Schedule -5 (a CTA per instance, slots and solve vector in global
+    memory) runs the arithmetic of -2 (slots in global memory, solve vector
+    in shared memory) bit for bit: a 16 x 16 mesh tile alone and a 12 x 12
+    grid with 3 Monte Carlo instances, DC + 20 backward-Euler steps."""
+    for nl, ni in ((circuits.power_grid_mesh(16), 1), (circuits.grid_circuit(12), 3)):
+        out = []
+        for sched in (-2, -5):
+            prob = product.Problem(ctx, nl, max_instances=ni)
+            prob.set_instances(circuits.mc_instances(nl, ni) if ni > 1 else None)
+            prob.run_mc_device(5e-12, 20, A.TRAN_BE, product.options(precision=prec, schedule=sched, **POLISH))
+            v, st = prob.read_results()
+            out.append((v, [(s["status"], s["iterations"], s["halvings"]) for s in st],
+                        prob.timing()["level_schedule"]))
+            prob.close()
+        assert out[0][2] == 3 and out[1][2] == 6
+        assert all(s[0] == A.ST_CONVERGED for s in out[0][1])
+        assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+def test_mesh_256_tile_satisfies_kcl(product, ctx, port):
+    """A 256 x 256 tile (65538 unknowns): its solve vector no longer fits
+    shared memory, so the planner takes schedule -5. DC and 4 backward-Euler
+    steps of 5 ps in mixed precision, all nodes recorded, held to the
+    oracle's KCL residual."""
+    n_side, dt, steps = 256, 5e-12, 4
+    nl = circuits.power_grid_mesh(n_side)
+    prob = product.Problem(ctx, nl, max_instances=1)
+    prob.set_instances(None)
+    opts = product.options(precision=A.PREC_MIXED, **POLISH)
+    vdc, st = prob.solve_dc(opts)
+    assert prob.timing()["level_schedule"] == 6
+    assert st[0]["status"] == A.ST_CONVERGED
+    assert port.kcl_residual(nl, vdc[0]) < 1e-9
+    nodes = np.arange(1, nl.n_nodes + 1, dtype=np.int32)
+    v, stt, wave = prob.step_transient(dt, steps, A.TRAN_BE, opts, wave_nodes=nodes)
+    assert stt[0]["status"] == A.ST_CONVERGED and stt[0]["halvings"] == 0
+    prev = vdc[0]
+    for k in range(steps):
+        assert port.kcl_residual(nl, wave[0][k], h=dt, v_prev=prev, t=(k + 1) * dt) < 1e-9, k
+        prev = wave[0][k]
+    prob.close()
