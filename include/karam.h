@@ -288,8 +288,9 @@ KARAM_API void karam_default_opts(karam_solver_opts *opts);
 KARAM_API int karam_problem_create(karam_ctx *ctx, const karam_netlist *nl,
                                    int32_t max_instances, karam_problem **out);
 KARAM_API void karam_problem_destroy(karam_problem *p);
-/* Symbolic-analysis cache: karam_problem_create keeps the last 32 analyses by
- * netlist content (every count, index, value, model name and the
+/* Symbolic-analysis cache: karam_problem_create keeps the last 32 analyses
+ * (at most 8 GiB of their fill-sized tables together; a larger one is not
+ * kept) by netlist content (every count, index, value, model name and the
  * temperature), process-wide, and reuses one for an identical netlist -- the
  * role of the reference's compiled block / pattern cache keyed by
  * topologyHash (infrastructure/compiled_block.h:45-88,

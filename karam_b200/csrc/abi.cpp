@@ -1169,10 +1169,30 @@ uint64_t fnv1a(const std::string& b) {
 // (infrastructure/compiled_block.h:45-88, solvers/circuitsim_solver.cpp:262-268).
 struct SymbolicCache {
   static constexpr size_t kEntries = 32;
+  static constexpr size_t kBytes = size_t(8) << 30;  // tables kept across entries
+  struct Entry {
+    std::string key;
+    std::shared_ptr<const Topology> topo;
+    size_t bytes;
+  };
   std::mutex mu;
-  std::list<std::pair<std::string, std::shared_ptr<const Topology>>> lru;
+  std::list<Entry> lru;
+  size_t bytes = 0;
   int64_t hits = 0, misses = 0;
 };
+
+// Host bytes of a built analysis, counted over the tables that grow with the
+// fill and the level schedule (the rest is linear in the netlist): several GB
+// for a 256 x 256 mesh tile.
+size_t topology_bytes(const Topology& T) {
+  size_t b = T.trip.size() * sizeof(Triplet);
+  for (const std::vector<int>* v :
+       {&T.f_col, &T.f_slot, &T.slot_row, &T.slot_col, &T.jt_code, &T.lu_data, &T.lu_rec, &T.nd_src,
+        &T.l_slot, &T.l_piv, &T.t_slot, &T.t_off, &T.pr_l, &T.pr_u, &T.y_row, &T.y_off, &T.yp_l, &T.yp_k,
+        &T.bs_u, &T.bs_c, &T.nd_prog, &T.es_item, &T.es_jt, &T.es_ft})
+    b += v->size() * sizeof(int);
+  return b;
+}
 SymbolicCache& symbolic_cache() {
   static SymbolicCache c;
   return c;
@@ -1184,17 +1204,25 @@ Topology cached_topology(const karam_netlist* nl) {
   {
     std::lock_guard<std::mutex> lock(C.mu);
     for (auto it = C.lru.begin(); it != C.lru.end(); ++it)
-      if (it->first == key) {
+      if (it->key == key) {
         C.lru.splice(C.lru.begin(), C.lru, it);
         ++C.hits;
-        return *C.lru.front().second;
+        return *C.lru.front().topo;
       }
     ++C.misses;
   }
   auto T = std::make_shared<const Topology>(build_topology(nl));  // outside the lock
+  const size_t tb = topology_bytes(*T);
+  if (tb > SymbolicCache::kBytes) return *T;  // larger than the whole budget: not kept
   std::lock_guard<std::mutex> lock(C.mu);
-  C.lru.emplace_front(key, T);
-  if (C.lru.size() > SymbolicCache::kEntries) C.lru.pop_back();
+  for (const auto& e : C.lru)
+    if (e.key == key) return *T;  // another thread kept the same analysis meanwhile
+  C.lru.push_front({key, T, tb});
+  C.bytes += tb;
+  while (C.lru.size() > SymbolicCache::kEntries || C.bytes > SymbolicCache::kBytes) {
+    C.bytes -= C.lru.back().bytes;
+    C.lru.pop_back();
+  }
   return *T;
 }
 
@@ -1219,6 +1247,7 @@ void karam_symbolic_cache_clear(void) {
   SymbolicCache& C = symbolic_cache();
   std::lock_guard<std::mutex> lock(C.mu);
   C.lru.clear();
+  C.bytes = 0;
   C.hits = C.misses = 0;
 }
 
