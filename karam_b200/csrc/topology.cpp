@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <functional>
+#include <iterator>
 #include <cmath>
 #include <cstdlib>
 #include <map>
@@ -359,7 +360,7 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
   T.lu_data.clear();
   T.lu_ops = 0;
   T.max_d = 0;
-  std::vector<int> L, U;
+  std::vector<int> L, U, merged;
   for (int k = 0; k < n; ++k) {
     L.clear();
     U.clear();
@@ -381,8 +382,21 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
       for (int j : nzr[k])
         if (j > k) U.push_back(j);
     }
-    for (int i : L)
-      for (int j : U) add_nz(i, j);
+    if (nzbits) {
+      for (int i : L)
+        for (int j : U) add_nz(i, j);
+    } else {  // L and U ascend: one sorted union per row and per column
+      for (int i : L) {
+        merged.clear();
+        std::set_union(nzr[i].begin(), nzr[i].end(), U.begin(), U.end(), std::back_inserter(merged));
+        nzr[i].swap(merged);
+      }
+      for (int j : U) {
+        merged.clear();
+        std::set_union(nzc[j].begin(), nzc[j].end(), L.begin(), L.end(), std::back_inserter(merged));
+        nzc[j].swap(merged);
+      }
+    }
     const int nl = (int)L.size(), nu = (int)U.size();
     T.max_d = std::max({T.max_d, nl, nu});
     T.lu_hdr[4 * k + 0] = (int)T.lu_data.size();
@@ -393,8 +407,18 @@ void device_tables(Topology& T, const std::vector<std::vector<int>>& urow) {
     for (int i : L) T.lu_data.push_back(fp(i, k));
     for (int j : U) T.lu_data.push_back(j);
     for (int j : U) T.lu_data.push_back(fp(k, j));
-    for (int i : L)
-      for (int j : U) T.lu_data.push_back(fp(i, j));
+    // positions of (i, j), j in U, by one walk along row i's filled columns
+    // (U ascends and lies in them)
+    const int* fcol = T.f_col.data();
+    for (int i : L) {
+      const int* end = fcol + T.f_row_ptr[i + 1];
+      const int* it = nu ? std::lower_bound(fcol + T.f_row_ptr[i], end, U.front()) : end;
+      for (int j : U) {
+        while (it != end && *it < j) ++it;
+        require(it != end && *it == j, "filled pattern misses a position");
+        T.lu_data.push_back((int)(it - fcol));
+      }
+    }
     T.lu_ops += nl + nl * nu;
   }
 
