@@ -729,7 +729,7 @@ void nd_schedule(Topology& T) {
   for (int p = 0; p < n; ++p) T.nd_pos[order[p]] = p;
 
   // unsymmetric symbolic elimination in ND order (rows and columns as bit
-  // rows up to 16384 unknowns, else ordered sets; the same structure either
+  // rows up to 16384 unknowns, else sorted vectors; the same structure either
   // way), then each row's columns in ascending order
   std::vector<std::vector<int>> Lk(n), Uk(n), Rrow(n);
   if (n <= bitrow_max()) {
@@ -778,21 +778,34 @@ void nd_schedule(Topology& T) {
       for (size_t q = 0; q < W; ++q)
         for (uint64_t c = row[q]; c; c &= c - 1) Rrow[r].push_back((int)(q * 64 + (size_t)__builtin_ctzll(c)));
     }
-  } else {
-    std::vector<std::set<int>> R(n), Cc(n);
+  } else {  // sorted vectors; pivot k's fill is one sorted union per row and per column
+    std::vector<std::vector<int>> R(n), Cc(n);
     for (auto& q : pos) {
       const int r = T.nd_pos[q.first], c = T.nd_pos[q.second];
-      R[r].insert(c);
-      Cc[c].insert(r);
+      R[r].push_back(c);
+      Cc[c].push_back(r);
     }
+    for (auto* v : {&R, &Cc})
+      for (auto& x : *v) {
+        std::sort(x.begin(), x.end());
+        x.erase(std::unique(x.begin(), x.end()), x.end());
+      }
+    std::vector<int> merged;
     for (int k = 0; k < n; ++k) {
-      for (auto it = Cc[k].upper_bound(k); it != Cc[k].end(); ++it) Lk[k].push_back(*it);
-      for (auto it = R[k].upper_bound(k); it != R[k].end(); ++it) Uk[k].push_back(*it);
-      for (int i : Lk[k])
-        for (int j : Uk[k])
-          if (R[i].insert(j).second) Cc[j].insert(i);
+      Lk[k].assign(std::upper_bound(Cc[k].begin(), Cc[k].end(), k), Cc[k].end());
+      Uk[k].assign(std::upper_bound(R[k].begin(), R[k].end(), k), R[k].end());
+      for (int i : Lk[k]) {
+        merged.clear();
+        std::set_union(R[i].begin(), R[i].end(), Uk[k].begin(), Uk[k].end(), std::back_inserter(merged));
+        R[i].swap(merged);
+      }
+      for (int j : Uk[k]) {
+        merged.clear();
+        std::set_union(Cc[j].begin(), Cc[j].end(), Lk[k].begin(), Lk[k].end(), std::back_inserter(merged));
+        Cc[j].swap(merged);
+      }
     }
-    for (int r = 0; r < n; ++r) Rrow[r].assign(R[r].begin(), R[r].end());
+    for (int r = 0; r < n; ++r) Rrow[r].swap(R[r]);
   }
   // ND slots, row-major: slot (r, c) = first slot of row r + rank of c among
   // the row's ascending columns
