@@ -1357,11 +1357,17 @@ void es_blocks(Topology& T) {
     std::vector<int> rows, comp;
     std::vector<char> done(n, 0);
     for (int r = 0; r < n; ++r) done[r] = hub_row[r];
+    // each component starts at its lowest-degree row (ties to the smallest
+    // index): the first row not yet done in one sorted list
+    std::vector<int> by_degree;
+    for (int r = 0; r < n; ++r)
+      if (!done[r]) by_degree.push_back(r);
+    std::sort(by_degree.begin(), by_degree.end(), degree_less);
+    size_t next_root = 0;
     while (true) {
-      int root = -1;
-      for (int r = 0; r < n; ++r)
-        if (!done[r] && (root < 0 || degree_less(r, root))) root = r;
-      if (root < 0) break;
+      while (next_root < by_degree.size() && done[by_degree[next_root]]) ++next_root;
+      if (next_root == by_degree.size()) break;
+      const int root = by_degree[next_root];
       // pseudo-peripheral start: the last row of a BFS from the
       // lowest-degree row of the component
       bfs(root, comp);
